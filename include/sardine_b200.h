@@ -1,0 +1,362 @@
+/*
+ * sardine_b200.h — C ABI of the B200 (sm_100a) implementation of SARdine's
+ * data-parallel hot path: sigma0 LUT calibration with NESZ, TOPS midpoint
+ * deburst, IW merge, backward Range-Doppler terrain correction and the
+ * SpeckleKernel filters.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (sd_status).  Status codes map
+ *    one-to-one onto the Rust error variants of the function each entry point
+ *    replaces; sd_last_error() returns the formatted message of the last
+ *    failure on a context.  Nothing here aborts the process.
+ *  - Times are int64 microseconds since an arbitrary common epoch.  The
+ *    reference keeps chrono DateTime values but only ever uses whole-
+ *    microsecond differences of them (Duration::num_microseconds), so this is
+ *    lossless for annotation times (which carry microseconds).
+ *  - Array pointers may be host memory (pageable or pinned) or device memory
+ *    of the context's device; the library detects which and stages host
+ *    buffers itself.  With device pointers the call enqueues on the
+ *    context's stream and returns after the stream has finished, unless the
+ *    entry point says otherwise.
+ *  - A context is not thread-safe: use one context per host thread.
+ *
+ * Reference paths cited as file:line are relative to the SARdine repository
+ * (sardine/src/...).
+ */
+#ifndef SARDINE_B200_H
+#define SARDINE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SD_ABI_VERSION 1
+
+/* ── Status codes ─────────────────────────────────────────────────────── */
+typedef enum sd_status {
+    SD_OK = 0,
+    SD_ERR_INVALID_ARGUMENT = 1,
+    SD_ERR_CUDA = 2,
+    SD_ERR_OUT_OF_MEMORY = 3,
+    SD_ERR_INTERNAL = 4,
+    SD_ERR_TIMEOUT = 5,
+    SD_ERR_BUSY = 6,
+    /* TerrainCorrectionError (terrain_correction.rs:45-67) */
+    SD_ERR_TC_ORBIT = 10,          /* OrbitError::OutsideOrbitWindow / InsufficientCoverage */
+    SD_ERR_TC_DEM = 11,
+    SD_ERR_TC_NO_GRID_POINTS = 12,
+    SD_ERR_TC_NO_SUBSWATHS = 13,
+    SD_ERR_TC_CONFIG = 14,
+    SD_ERR_TC_PROJECTION = 15,
+    /* SpeckleError (speckle.rs:96-108) */
+    SD_ERR_SPECKLE_DIMENSION_MISMATCH = 20,
+    SD_ERR_SPECKLE_BAD_WINDOW = 21,
+    SD_ERR_SPECKLE_BAD_ENL = 22,
+    SD_ERR_SPECKLE_BAD_DAMPING = 23,
+    /* CalibrationError (apply_calibration.rs:64-84) */
+    SD_ERR_CAL_NO_CALIBRATION_VECTORS = 30,
+    SD_ERR_CAL_NO_NOISE_RANGE_VECTORS = 31,
+    SD_ERR_CAL_LUT_RANGE_INSUFFICIENT = 32,
+    /* DeburstError (deburst.rs:56-121) */
+    SD_ERR_DEBURST_NO_BURSTS = 40,
+    SD_ERR_DEBURST_BURST_COUNT_MISMATCH = 41,
+    SD_ERR_DEBURST_TIFF_TOO_SMALL = 42,
+    SD_ERR_DEBURST_EMPTY_VALID_WINDOW = 43,
+    SD_ERR_DEBURST_INVALID_OVERLAP = 44,
+    SD_ERR_DEBURST_IMPLAUSIBLE_OVERLAP = 45,
+    /* MergeError (merge_subswaths.rs:62-81) */
+    SD_ERR_MERGE_EMPTY_INPUTS = 50,
+    SD_ERR_MERGE_INCONSISTENT_PIXEL_SPACING = 51,
+    SD_ERR_MERGE_EMPTY_SWATH = 52
+} sd_status;
+
+/* ── Enumerations mirroring the reference's enums ─────────────────────── */
+/* ResamplingKernel (pipeline_options.rs:75-90) */
+enum { SD_RESAMPLE_BILINEAR = 0, SD_RESAMPLE_BICUBIC = 1, SD_RESAMPLE_LANCZOS3 = 2 };
+/* OutputCrs (output_crs.rs:70-96); LAEA and WebMercator are not supported */
+enum { SD_CRS_WGS84 = 0, SD_CRS_UTM_NORTH = 1, SD_CRS_UTM_SOUTH = 2 };
+/* DemSource implementations understood by the device path */
+enum {
+    SD_DEM_GEOGRAPHIC = 0,   /* one Glo30-style tile: dem.rs:351-371 semantics */
+    SD_DEM_PROJECTED_UTM = 1 /* projected grid: forward UTM, then the same grid semantics */
+};
+/* GeoidModel (geoid.rs:342-402): Zero, or a 73x144 2.5-degree undulation grid */
+enum { SD_GEOID_ZERO = 0, SD_GEOID_GRID = 1 };
+/* SpeckleFilter (speckle.rs:61-91) */
+enum {
+    SD_SPECKLE_BOXCAR = 0, SD_SPECKLE_LEE = 1, SD_SPECKLE_FROST = 2,
+    SD_SPECKLE_GAMMA_MAP = 3, SD_SPECKLE_REFINED_LEE = 4
+};
+/* Terrain-correction precision mode */
+enum {
+    SD_PRECISION_FP64 = 0,  /* reproduces the reference arithmetic (default) */
+    SD_PRECISION_SPLIT = 1  /* FP64 orbit/anchor + FP32 bulk, error reported */
+};
+/* mask_code (terrain_correction.rs:346-376) */
+enum {
+    SD_MASK_VALID = 0, SD_MASK_OUTSIDE_FOOTPRINT = 1, SD_MASK_DEM_MISSING = 2,
+    SD_MASK_NON_CONVERGED = 3, SD_MASK_DEGENERATE_GEOMETRY = 4, SD_MASK_SHADOW = 5,
+    SD_MASK_LAYOVER = 6, SD_MASK_FORESHORTENING = 7, SD_MASK_NOISE_MASKED = 8,
+    SD_MASK_DEM_NEIGHBOUR_MISSING = 9
+};
+#define SD_NEWTON_ITER_HIST_SIZE 16  /* NEWTON_ITER_HIST_SIZE, terrain_correction.rs:96 */
+
+/* ── Data contracts ───────────────────────────────────────────────────── */
+
+/* StateVector (types.rs:142); time as int64 us. */
+typedef struct sd_state_vector {
+    int64_t time_us;
+    double position_m[3];
+    double velocity_m_s[3];
+} sd_state_vector;
+
+/* RadarImage (pipeline_options.rs:100-135) as implemented by MergedSigma0
+ * (terrain_correction.rs:888-928; merge_subswaths.rs:106-162). */
+typedef struct sd_radar_image {
+    const float *data;   /* lines x samples, row-major, NaN = nodata */
+    const float *nesz;   /* same shape, or NULL (nesz_at -> None)    */
+    uint64_t lines;
+    uint64_t samples;
+    int64_t azimuth_start_time_us;
+    double near_slant_range_time_s;
+    double range_pixel_spacing_m;
+} sd_radar_image;
+
+/* The parts of SceneMetadata (types.rs:406) the terrain correction reads. */
+typedef struct sd_scene {
+    double azimuth_time_interval_s;  /* scene.sub_swaths[0].azimuth_time_interval_s */
+    int32_t n_sub_swaths;            /* 0 -> TerrainCorrectionError::NoSubSwaths */
+    double min_lat_deg, max_lat_deg, min_lon_deg, max_lon_deg; /* bounding_box */
+    const sd_state_vector *state_vectors; /* orbit.state_vectors, sorted by time */
+    uint64_t n_state_vectors;
+} sd_scene;
+
+/* DemSource (dem.rs:829-842).  (origin_y, origin_x) is the centre of pixel
+ * (0,0): latitude/longitude in degrees for SD_DEM_GEOGRAPHIC, northing/easting
+ * in metres for SD_DEM_PROJECTED_UTM.  Row 0 is the northern edge. */
+typedef struct sd_dem {
+    int32_t kind;
+    int32_t utm_zone;    /* SD_DEM_PROJECTED_UTM only */
+    int32_t utm_south;   /* SD_DEM_PROJECTED_UTM only */
+    int32_t _pad;
+    const float *data;   /* height x width, row-major, NaN = void */
+    uint64_t width;
+    uint64_t height;
+    double origin_y;
+    double origin_x;
+    double pixel_size;
+} sd_dem;
+
+/* GeoidModel (geoid.rs:342-402). */
+typedef struct sd_geoid {
+    int32_t kind;                 /* SD_GEOID_ZERO or SD_GEOID_GRID */
+    int32_t _pad;
+    const float *undulations_m;   /* 73 x 144, row 0 = 90N, col 0 = 0E */
+} sd_geoid;
+
+/* GeolocationGridPoint (types.rs:171): the two fields the terrain correction
+ * uses to seed its azimuth-time guess (terrain_correction.rs:1080-1137).
+ * Pass the points of IW2, or of the first sub-swath when IW2 is absent. */
+typedef struct sd_geo_grid_point {
+    int64_t azimuth_time_us;
+    double latitude_deg;
+} sd_geo_grid_point;
+
+/* TerrainCorrectionConfig (terrain_correction.rs:100-236) plus the two
+ * environment knobs the reference reads inside terrain_correction
+ * (SARDINE_TC_PROJECTOR_ANCHORS, default 256; SARDINE_TC_ROW_CHUNK, which
+ * only schedules CPU work and is accepted and ignored here). */
+typedef struct sd_tc_config {
+    double pixel_spacing;        /* pixel_spacing_deg, in CRS units */
+    int32_t crs;                 /* SD_CRS_* */
+    int32_t utm_zone;            /* 1..60 for UTM CRSs */
+    int32_t max_newton_iterations;
+    int32_t flatten;
+    double newton_tolerance_s;
+    int32_t compute_lia;
+    int32_t resampling;          /* SD_RESAMPLE_* */
+    float noise_floor_margin_db; /* -INFINITY disables NESZ masking */
+    int32_t projector_anchors;   /* >= 1 */
+    int32_t precision;           /* SD_PRECISION_* */
+    int32_t _pad;
+} sd_tc_config;
+
+/* GeocodedImage (terrain_correction.rs:238-307) without the rasters. */
+typedef struct sd_geocoded_info {
+    uint64_t rows, cols;
+    double origin_lat_deg, origin_lon_deg; /* top-left corner, CRS units */
+    double pixel_spacing;
+    double geotransform[6];
+    uint64_t total_pixel_count;
+    uint64_t valid_pixel_count;
+    uint64_t dem_missing_count;
+    uint64_t outside_footprint_count;
+    uint64_t non_converged_count;
+    uint64_t degenerate_geometry_count;
+    uint64_t flat_masked_count;
+    uint64_t noise_masked_count;
+    uint64_t newton_iter_histogram[SD_NEWTON_ITER_HIST_SIZE];
+} sd_geocoded_info;
+
+/* CalibrationVector / NoiseRangeVector (calibration.rs:38-82): one LUT row. */
+typedef struct sd_lut_vector {
+    int32_t line;
+    int32_t _pad;
+    const uint32_t *pixels;  /* ascending */
+    const float *values;
+    uint64_t n;
+} sd_lut_vector;
+
+/* NoiseAzimuthVector (calibration.rs:86-96); n == 0 means absent. */
+typedef struct sd_noise_azimuth {
+    const int32_t *lines;
+    const float *values;
+    uint64_t n;
+} sd_noise_azimuth;
+
+/* BurstEntry (types.rs:351). */
+typedef struct sd_burst {
+    int64_t azimuth_time_us;
+    uint64_t burst_index;
+    uint64_t first_line, last_line;
+    uint64_t first_valid_sample, last_valid_sample;
+} sd_burst;
+
+/* The SubSwathMetadata (types.rs:281) fields deburst/merge read. */
+typedef struct sd_subswath {
+    uint64_t burst_count;
+    uint64_t lines_per_burst;
+    double azimuth_time_interval_s;
+    double range_pixel_spacing_m;
+    double slant_range_time_s;
+} sd_subswath;
+
+/* One IW sub-swath as fed to the fused calibrate+deburst+merge path:
+ * the measurement raster (what SlcReader::read_burst_raw would return),
+ * its metadata, bursts and LUTs. */
+typedef struct sd_swath_input {
+    const int16_t *slc_iq;        /* tiff_height x tiff_width x [I,Q] */
+    uint64_t tiff_width, tiff_height;
+    sd_subswath sw;
+    const sd_burst *bursts;       /* sorted by burst_index */
+    uint64_t n_bursts;
+    const sd_lut_vector *cal;     /* sigmaNought vectors */
+    uint64_t n_cal;
+    const sd_lut_vector *noise_range;
+    uint64_t n_noise_range;
+    sd_noise_azimuth noise_azimuth;
+} sd_swath_input;
+
+/* MergedSigma0 metadata (merge_subswaths.rs:106-162). */
+typedef struct sd_merged_info {
+    uint64_t lines, samples;
+    double near_slant_range_time_s;
+    double range_pixel_spacing_s;
+    double range_pixel_spacing_m;
+    uint32_t cal_lut_extrapolation_gap_px;
+    uint32_t noise_lut_extrapolation_gap_px;
+    int64_t azimuth_start_time_us;
+    /* per-swath layout, for diagnostics and the split/serving paths */
+    int32_t n_swaths;
+    int32_t _pad;
+    int64_t swath_out_offset[8];
+    uint64_t swath_seam[8];
+    uint64_t swath_lines[8];
+    uint64_t swath_valid_offset[8];
+} sd_merged_info;
+
+typedef struct sd_ctx sd_ctx;
+
+/* ── Context ──────────────────────────────────────────────────────────── */
+int sd_abi_version(void);
+int sd_ctx_create(int device, sd_ctx **out);
+void sd_ctx_destroy(sd_ctx *ctx);
+const char *sd_last_error(const sd_ctx *ctx);
+/* Number of this library's kernels launched on the context since creation. */
+uint64_t sd_kernel_launches(const sd_ctx *ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that interleave work. */
+void *sd_ctx_stream(sd_ctx *ctx);
+
+/* ── Speckle ──────────────────────────────────────────────────────────────
+ * Replaces SpeckleKernel::apply / apply_speckle_filter (speckle.rs:131-180,
+ * 586-603).  window is ignored for SD_SPECKLE_REFINED_LEE (fixed 7x7);
+ * enl is used by Lee, Gamma-MAP and Refined Lee, damping by Frost. */
+int sd_speckle(sd_ctx *ctx, const float *data, uint64_t data_len, uint64_t cols,
+               uint64_t rows, int32_t kind, uint64_t window, float enl,
+               float damping, float *out);
+
+/* ── Deburst ──────────────────────────────────────────────────────────────
+ * compute_overlap_lines (deburst.rs:172-210). */
+int sd_compute_overlap_lines(sd_ctx *ctx, const sd_burst *burst_k,
+                             const sd_burst *burst_k1, double ati_s,
+                             uint64_t lines_per_burst, uint64_t *overlap);
+/* Output shape of deburst_subswath without running it. */
+int sd_deburst_plan(sd_ctx *ctx, const sd_subswath *sw, const sd_burst *bursts,
+                    uint64_t n_bursts, uint64_t tiff_height, uint64_t *lines,
+                    uint64_t *samples, uint64_t *valid_sample_offset);
+/* deburst_subswath (deburst.rs:230-344) over an in-memory measurement raster.
+ * out_iq: lines x samples x [I,Q] int16. */
+int sd_deburst_subswath(sd_ctx *ctx, const int16_t *slc_iq, uint64_t tiff_width,
+                        uint64_t tiff_height, const sd_subswath *sw,
+                        const sd_burst *bursts, uint64_t n_bursts, int16_t *out_iq);
+
+/* ── Calibration ──────────────────────────────────────────────────────────
+ * apply_calibration (apply_calibration.rs:374-572). */
+int sd_apply_calibration(sd_ctx *ctx, const int16_t *deburst_iq, uint64_t lines,
+                         uint64_t samples, uint64_t valid_sample_offset,
+                         const sd_lut_vector *cal, uint64_t n_cal,
+                         const sd_lut_vector *noise_range, uint64_t n_noise_range,
+                         const sd_noise_azimuth *noise_azimuth,
+                         uint64_t tiff_line_origin, float *out_sigma0,
+                         float *out_nesz, uint32_t *cal_gap_px,
+                         uint32_t *noise_gap_px);
+
+/* ── Merge ────────────────────────────────────────────────────────────────
+ * merge_subswaths (merge_subswaths.rs:207-450) over n calibrated swaths,
+ * given in IW1 < IW2 < IW3 order.  sigma0[i]/nesz[i] are lines[i] x
+ * samples[i].  Call with out_data == NULL to only fill *info. */
+int sd_merge_subswaths(sd_ctx *ctx, int32_t n, const float *const *sigma0,
+                       const float *const *nesz, const uint64_t *lines,
+                       const uint64_t *samples, const uint64_t *valid_sample_offset,
+                       const uint32_t *cal_gap_px, const uint32_t *noise_gap_px,
+                       const sd_subswath *sw, const int64_t *azimuth_start_time_us,
+                       float *out_data, float *out_nesz, sd_merged_info *info);
+
+/* ── Fused calibrate + deburst + merge ────────────────────────────────────
+ * The per-IW chain of prepare_merged_scene (scene_prep.rs:598-699): deburst,
+ * apply_calibration with tiff_line_origin = bursts[0].first_line, then
+ * merge_subswaths, in one gather kernel per swath writing straight into the
+ * merged rasters.  Call with out_data == NULL to only fill *info. */
+int sd_calibrate_deburst_merge(sd_ctx *ctx, int32_t n_swaths,
+                               const sd_swath_input *swaths, float *out_data,
+                               float *out_nesz, sd_merged_info *info);
+
+/* ── Terrain correction ───────────────────────────────────────────────────
+ * Output grid of terrain_correction (terrain_correction.rs:1174-1216,
+ * 1297-1320) without running it: fills rows, cols, origin, geotransform. */
+int sd_tc_output_grid(sd_ctx *ctx, const sd_scene *scene, const sd_tc_config *cfg,
+                      sd_geocoded_info *info);
+/* terrain_correction (terrain_correction.rs:1245-1836).  out_data is
+ * rows x cols f32; out_cos_lia / out_mask are filled when cfg->compute_lia
+ * (otherwise they may be NULL).  In SD_PRECISION_SPLIT mode, out_err (may be
+ * NULL) receives per-pixel geolocation error estimates in pixels. */
+int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image,
+                          const sd_scene *scene, const sd_dem *dem,
+                          const sd_geoid *geoid, const sd_geo_grid_point *grid,
+                          uint64_t n_grid, const sd_tc_config *cfg,
+                          float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                          sd_geocoded_info *info);
+
+/* ── Diagnostics ──────────────────────────────────────────────────────────
+ * Runs an FP64 FMA-chain kernel for about `iters` dependent FMAs per thread
+ * over the whole device and returns the achieved FP64 TFLOP/s. */
+int sd_measure_fp64_peak(sd_ctx *ctx, int32_t iters, double *tflops);
+int sd_measure_fp32_peak(sd_ctx *ctx, int32_t iters, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SARDINE_B200_H */

@@ -1,0 +1,376 @@
+"""sardine_b200 — B200 (sm_100a) implementation of SARdine's hot path.
+
+The functions here mirror the reference's Rust API for the path (same names,
+argument meaning and error variants) and call the CUDA library through its
+C ABI (include/sardine_b200.h):
+
+==============================  ============================================
+reference                       here
+==============================  ============================================
+terrain_correction              terrain_correction(merged, scene, dem, grids, config)
+apply_calibration               apply_calibration(deburst, cal, noise, tiff_line_origin)
+deburst_subswath                deburst_subswath(slc_iq, sw, bursts)
+compute_overlap_lines           compute_overlap_lines(burst_k, burst_k1, ati_s, lines_per_burst)
+merge_subswaths                 merge_subswaths(inputs)
+prepare_merged_scene (core)     calibrate_deburst_merge(swaths)
+apply_speckle_filter            apply_speckle_filter(data, cols, rows, filter)
+SpeckleKernel                   SpeckleKernel / GpuSpeckleKernel
+==============================  ============================================
+
+Arrays may be numpy (host) or torch CUDA tensors (device resident); results
+come back in the same kind of container as the main input.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Any, List, Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from . import types as T
+from ._lib import Context, default_context, lib
+from .types import (BoundingBox, BurstEntry, CalibrationVector, DeburstArray, DemGrid,
+                    GeocodedImage, GeoidModel, GeolocationGridPoint, MergedSigma0, NoiseAzimuthVector,
+                    NoiseRangeVector, OrbitData, OutputCrs, ResamplingKernel, SceneMetadata,
+                    Sigma0Array, SpeckleFilter, SubSwathMetadata, SwathCalibration, SwathInput,
+                    SwathNoise, TerrainCorrectionConfig)
+
+__all__ = [
+    "terrain_correction", "apply_calibration", "deburst_subswath", "compute_overlap_lines",
+    "merge_subswaths", "calibrate_deburst_merge", "apply_speckle_filter", "SpeckleKernel",
+    "GpuSpeckleKernel", "SardineError", "TerrainCorrectionError", "SpeckleError",
+    "CalibrationError", "DeburstError", "MergeError", "Context", "default_context",
+    "tc_output_grid",
+] + [n for n in dir(T) if n[:1].isupper()]
+
+
+# ── errors (one class per reference error enum; .kind = variant name) ──────
+class SardineError(RuntimeError):
+    def __init__(self, code: int, kind: str, message: str):
+        super().__init__(f"{kind}: {message}" if message else kind)
+        self.code = code
+        self.kind = kind
+
+
+class TerrainCorrectionError(SardineError):
+    """terrain_correction.rs:45-67"""
+
+
+class SpeckleError(SardineError):
+    """speckle.rs:96-108"""
+
+
+class CalibrationError(SardineError):
+    """apply_calibration.rs:64-84"""
+
+
+class DeburstError(SardineError):
+    """deburst.rs:56-121"""
+
+
+class MergeError(SardineError):
+    """merge_subswaths.rs:62-81"""
+
+
+_KINDS = {
+    _abi.SD_ERR_TC_ORBIT: (TerrainCorrectionError, "Orbit"),
+    _abi.SD_ERR_TC_DEM: (TerrainCorrectionError, "Dem"),
+    _abi.SD_ERR_TC_NO_GRID_POINTS: (TerrainCorrectionError, "NoGridPoints"),
+    _abi.SD_ERR_TC_NO_SUBSWATHS: (TerrainCorrectionError, "NoSubSwaths"),
+    _abi.SD_ERR_TC_CONFIG: (TerrainCorrectionError, "Config"),
+    _abi.SD_ERR_TC_PROJECTION: (TerrainCorrectionError, "Projection"),
+    _abi.SD_ERR_SPECKLE_DIMENSION_MISMATCH: (SpeckleError, "DimensionMismatch"),
+    _abi.SD_ERR_SPECKLE_BAD_WINDOW: (SpeckleError, "BadWindow"),
+    _abi.SD_ERR_SPECKLE_BAD_ENL: (SpeckleError, "BadEnl"),
+    _abi.SD_ERR_SPECKLE_BAD_DAMPING: (SpeckleError, "BadDamping"),
+    _abi.SD_ERR_CAL_NO_CALIBRATION_VECTORS: (CalibrationError, "NoCalibrationVectors"),
+    _abi.SD_ERR_CAL_NO_NOISE_RANGE_VECTORS: (CalibrationError, "NoNoiseRangeVectors"),
+    _abi.SD_ERR_CAL_LUT_RANGE_INSUFFICIENT: (CalibrationError, "LutRangeInsufficient"),
+    _abi.SD_ERR_DEBURST_NO_BURSTS: (DeburstError, "NoBursts"),
+    _abi.SD_ERR_DEBURST_BURST_COUNT_MISMATCH: (DeburstError, "BurstCountMismatch"),
+    _abi.SD_ERR_DEBURST_TIFF_TOO_SMALL: (DeburstError, "TiffTooSmall"),
+    _abi.SD_ERR_DEBURST_EMPTY_VALID_WINDOW: (DeburstError, "EmptyValidWindow"),
+    _abi.SD_ERR_DEBURST_INVALID_OVERLAP: (DeburstError, "InvalidOverlap"),
+    _abi.SD_ERR_DEBURST_IMPLAUSIBLE_OVERLAP: (DeburstError, "ImplausibleOverlap"),
+    _abi.SD_ERR_MERGE_EMPTY_INPUTS: (MergeError, "EmptyInputs"),
+    _abi.SD_ERR_MERGE_INCONSISTENT_PIXEL_SPACING: (MergeError, "InconsistentPixelSpacing"),
+    _abi.SD_ERR_MERGE_EMPTY_SWATH: (MergeError, "EmptySwath"),
+}
+
+
+def _check(ctx: Context, rc: int, default_cls=SardineError):
+    if rc == 0:
+        return
+    cls, kind = _KINDS.get(rc, (default_cls, {
+        _abi.SD_ERR_INVALID_ARGUMENT: "InvalidArgument", _abi.SD_ERR_CUDA: "Cuda",
+        _abi.SD_ERR_OUT_OF_MEMORY: "OutOfMemory", _abi.SD_ERR_INTERNAL: "Internal",
+        _abi.SD_ERR_TIMEOUT: "Timeout", _abi.SD_ERR_BUSY: "Busy"}.get(rc, f"Status{rc}")))
+    raise cls(rc, kind, ctx.last_error())
+
+
+# ── containers ─────────────────────────────────────────────────────────────
+def _is_torch_cuda(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+def _empty_like_kind(ref, shape, dtype: str):
+    if _is_torch_cuda(ref):
+        import torch
+        tdt = {"f4": torch.float32, "u1": torch.uint8, "i2": torch.int16}[dtype]
+        return torch.empty(shape, dtype=tdt, device=ref.device)
+    return np.empty(shape, dtype={"f4": np.float32, "u1": np.uint8, "i2": np.int16}[dtype])
+
+
+def _prep(a, dtype):
+    """numpy arrays are made contiguous with the right dtype; torch tensors must already be."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return np.ascontiguousarray(a, dtype=dtype)
+    return a.contiguous()
+
+
+def _ctx(ctx: Optional[Context]) -> Context:
+    return ctx if ctx is not None else default_context(int(os.environ.get("SARDINE_B200_DEVICE", "0")))
+
+
+def _anchors_from_env() -> int:
+    """SARDINE_TC_PROJECTOR_ANCHORS (terrain_correction.rs:1328-1351)."""
+    s = os.environ.get("SARDINE_TC_PROJECTOR_ANCHORS")
+    if s is None:
+        return 256
+    try:
+        v = int(s)
+        if v < 0:
+            raise ValueError
+    except ValueError:
+        raise TerrainCorrectionError(_abi.SD_ERR_TC_CONFIG, "Config",
+                                     f"SARDINE_TC_PROJECTOR_ANCHORS={s!r} is not a non-negative integer")
+    return v
+
+
+# ── terrain correction ─────────────────────────────────────────────────────
+def tc_output_grid(scene: SceneMetadata, config: TerrainCorrectionConfig,
+                   ctx: Optional[Context] = None) -> _abi.GeocodedInfo:
+    ctx = _ctx(ctx)
+    keep = T._Keep()
+    sc = T.scene_to_c(scene, keep)
+    cfg = config.to_c(256)
+    info = _abi.GeocodedInfo()
+    _check(ctx, lib().sd_tc_output_grid(ctx.handle, C.byref(sc), C.byref(cfg), C.byref(info)),
+           TerrainCorrectionError)
+    return info
+
+
+def terrain_correction(merged: MergedSigma0, scene: SceneMetadata, dem: DemGrid, grids,
+                       config: TerrainCorrectionConfig, ctx: Optional[Context] = None,
+                       out=None) -> GeocodedImage:
+    """terrain_correction (terrain_correction.rs:1245-1836) on the GPU.
+
+    `grids` is a sequence of (sub-swath id, geolocation points); the LUT uses
+    IW2's points, else the first sub-swath's.  `out` may supply preallocated
+    (data, cos_lia, mask) buffers of the output-grid shape."""
+    ctx = _ctx(ctx)
+    keep = T._Keep()
+    merged_data = _prep(merged.data, np.float32)
+    nesz = _prep(merged.nesz, np.float32) if merged.nesz is not None else None
+    img = _abi.RadarImage(T.ptr(merged_data), T.ptr(nesz), merged.lines, merged.samples,
+                          int(merged.azimuth_start_time_us), merged.near_slant_range_time_s,
+                          merged.range_pixel_spacing_m)
+    sc = T.scene_to_c(scene, keep)
+    dem_data = _prep(dem.data, np.float32)
+    d = _abi.Dem(dem.kind, dem.utm_zone, int(dem.utm_south), 0, T.ptr(dem_data),
+                 dem_data.shape[1], dem_data.shape[0], dem.origin_y, dem.origin_x, dem.pixel_size)
+    geo = config.geoid.to_c(keep)
+    pts = T.pick_lut_grid(grids)
+    g = T.grid_to_c(pts)
+    anchors = _anchors_from_env()
+    cfg = config.to_c(anchors)
+    info = _abi.GeocodedInfo()
+    if len(pts) > 0 and config.pixel_spacing_deg > 0 and scene.sub_swaths:
+        _check(ctx, lib().sd_tc_output_grid(ctx.handle, C.byref(sc), C.byref(cfg), C.byref(info)),
+               TerrainCorrectionError)
+    rows, cols = int(info.rows), int(info.cols)
+    if out is not None:
+        data, cos, mask = out
+    else:
+        data = _empty_like_kind(merged_data, (rows, cols), "f4")
+        cos = _empty_like_kind(merged_data, (rows, cols), "f4") if config.compute_lia else None
+        mask = _empty_like_kind(merged_data, (rows, cols), "u1") if config.compute_lia else None
+    rc = lib().sd_terrain_correction(ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo),
+                                     g, len(pts), C.byref(cfg), T.ptr(data), T.ptr(cos), T.ptr(mask),
+                                     C.byref(info))
+    _check(ctx, rc, TerrainCorrectionError)
+    return GeocodedImage.from_info(info, config.crs, data, cos, mask)
+
+
+# ── deburst / calibration / merge ──────────────────────────────────────────
+def compute_overlap_lines(burst_k: BurstEntry, burst_k1: BurstEntry, ati_s: float,
+                          lines_per_burst: int, ctx: Optional[Context] = None) -> int:
+    """compute_overlap_lines (deburst.rs:172-210)."""
+    ctx = _ctx(ctx)
+    a, b = burst_k.to_c(), burst_k1.to_c()
+    ov = C.c_uint64()
+    _check(ctx, lib().sd_compute_overlap_lines(ctx.handle, C.byref(a), C.byref(b), ati_s,
+                                               lines_per_burst, C.byref(ov)), DeburstError)
+    return int(ov.value)
+
+
+def deburst_subswath(slc_iq, sw: SubSwathMetadata, bursts: Sequence[BurstEntry],
+                     ctx: Optional[Context] = None) -> DeburstArray:
+    """deburst_subswath (deburst.rs:230-344).  `slc_iq` is the measurement
+    raster (tiff_height, tiff_width, 2) int16 — what BurstReader reads."""
+    ctx = _ctx(ctx)
+    slc_iq = _prep(slc_iq, np.int16)
+    h, w = int(slc_iq.shape[0]), int(slc_iq.shape[1])
+    swc = sw.to_c()
+    bc = T.bursts_to_c(bursts)
+    lines, samples, off = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    _check(ctx, lib().sd_deburst_plan(ctx.handle, C.byref(swc), bc, len(bursts), h, C.byref(lines),
+                                      C.byref(samples), C.byref(off)), DeburstError)
+    out = _empty_like_kind(slc_iq, (lines.value, samples.value, 2), "i2")
+    _check(ctx, lib().sd_deburst_subswath(ctx.handle, T.ptr(slc_iq), w, h, C.byref(swc), bc,
+                                          len(bursts), T.ptr(out)), DeburstError)
+    return DeburstArray(out, int(lines.value), int(samples.value), int(off.value))
+
+
+def apply_calibration(deburst: DeburstArray, cal: SwathCalibration, noise: SwathNoise,
+                      tiff_line_origin: int, ctx: Optional[Context] = None) -> Sigma0Array:
+    """apply_calibration (apply_calibration.rs:374-572)."""
+    ctx = _ctx(ctx)
+    keep = T._Keep()
+    cv = T.lut_vectors_to_c(cal.vectors, keep, "sigma_nought")
+    nv = T.lut_vectors_to_c(noise.range_vectors, keep, "noise_range_lut")
+    na = T.noise_azimuth_to_c(noise, keep)
+    iq = _prep(deburst.data, np.int16)
+    out = _empty_like_kind(iq, (deburst.lines, deburst.samples), "f4")
+    nesz = _empty_like_kind(iq, (deburst.lines, deburst.samples), "f4")
+    cg, ng = C.c_uint32(), C.c_uint32()
+    rc = lib().sd_apply_calibration(ctx.handle, T.ptr(iq), deburst.lines, deburst.samples,
+                                    deburst.valid_sample_offset, cv, len(cal.vectors), nv,
+                                    len(noise.range_vectors), C.byref(na), tiff_line_origin,
+                                    T.ptr(out), T.ptr(nesz), C.byref(cg), C.byref(ng))
+    _check(ctx, rc, CalibrationError)
+    return Sigma0Array(out, deburst.lines, deburst.samples, deburst.valid_sample_offset,
+                       int(cg.value), int(ng.value), nesz)
+
+
+def merge_subswaths(inputs: Sequence[SwathInput], ctx: Optional[Context] = None) -> MergedSigma0:
+    """merge_subswaths (merge_subswaths.rs:207-450); inputs in IW1 < IW2 < IW3 order."""
+    ctx = _ctx(ctx)
+    n = len(inputs)
+    m = max(1, n)
+    arrs = [(_prep(i.sigma0.data, np.float32), _prep(i.sigma0.nesz, np.float32)) for i in inputs]
+    sig = (C.c_void_p * m)(*[T.ptr(a[0]) for a in arrs])
+    nes = (C.c_void_p * m)(*[T.ptr(a[1]) for a in arrs])
+    u64 = lambda vals: (C.c_uint64 * m)(*vals)
+    lines = u64([i.sigma0.lines for i in inputs])
+    samples = u64([i.sigma0.samples for i in inputs])
+    voff = u64([i.sigma0.valid_sample_offset for i in inputs])
+    cg = (C.c_uint32 * m)(*[i.sigma0.cal_lut_extrapolation_gap_px for i in inputs])
+    ng = (C.c_uint32 * m)(*[i.sigma0.noise_lut_extrapolation_gap_px for i in inputs])
+    sw = (_abi.SubSwath * m)(*[i.swath.to_c() for i in inputs])
+    az = (C.c_int64 * m)(*[int(i.azimuth_start_time_us) for i in inputs])
+    info = _abi.MergedInfo()
+    _check(ctx, lib().sd_merge_subswaths(ctx.handle, n, sig, nes, lines, samples, voff, cg, ng, sw,
+                                         az, None, None, C.byref(info)), MergeError)
+    ref = arrs[0][0]
+    out = _empty_like_kind(ref, (info.lines, info.samples), "f4")
+    onz = _empty_like_kind(ref, (info.lines, info.samples), "f4")
+    _check(ctx, lib().sd_merge_subswaths(ctx.handle, n, sig, nes, lines, samples, voff, cg, ng, sw,
+                                         az, T.ptr(out), T.ptr(onz), C.byref(info)), MergeError)
+    return _merged_from_info(info, out, onz)
+
+
+def _merged_from_info(info: _abi.MergedInfo, out, onz) -> MergedSigma0:
+    return MergedSigma0(out, int(info.lines), int(info.samples), info.near_slant_range_time_s,
+                        info.range_pixel_spacing_s, info.range_pixel_spacing_m,
+                        int(info.cal_lut_extrapolation_gap_px),
+                        int(info.noise_lut_extrapolation_gap_px), onz,
+                        int(info.azimuth_start_time_us))
+
+
+def swath_inputs_to_c(swaths, keep: T._Keep):
+    """ctypes array of sd_swath_input for calibrate_deburst_merge."""
+    arr = (_abi.SwathInput * max(1, len(swaths)))()
+    for k, s in enumerate(swaths):
+        slc = keep.add(_prep(s.slc, np.int16))
+        bc = keep.add(T.bursts_to_c(s.bursts))
+        cv = keep.add(T.lut_vectors_to_c(s.cal.vectors, keep, "sigma_nought"))
+        nv = keep.add(T.lut_vectors_to_c(s.noise.range_vectors, keep, "noise_range_lut"))
+        na = T.noise_azimuth_to_c(s.noise, keep)
+        arr[k].slc_iq = T.ptr(slc)
+        arr[k].tiff_width = int(slc.shape[1])
+        arr[k].tiff_height = int(slc.shape[0])
+        arr[k].sw = s.sw.to_c()
+        arr[k].bursts = C.addressof(bc)
+        arr[k].n_bursts = len(s.bursts)
+        arr[k].cal = C.addressof(cv)
+        arr[k].n_cal = len(s.cal.vectors)
+        arr[k].noise_range = C.addressof(nv)
+        arr[k].n_noise_range = len(s.noise.range_vectors)
+        arr[k].noise_azimuth = na
+    return arr
+
+
+def calibrate_deburst_merge(swaths, ctx: Optional[Context] = None, out=None) -> MergedSigma0:
+    """The per-IW deburst -> apply_calibration(tiff_line_origin =
+    bursts[0].first_line) -> merge_subswaths chain of prepare_merged_scene
+    (scene_prep.rs:598-699), fused into one pass per swath on the GPU.
+    `swaths`: objects with .slc (raster), .sw, .bursts, .cal, .noise."""
+    ctx = _ctx(ctx)
+    keep = T._Keep()
+    arr = swath_inputs_to_c(swaths, keep)
+    info = _abi.MergedInfo()
+    _check(ctx, lib().sd_calibrate_deburst_merge(ctx.handle, len(swaths), arr, None, None,
+                                                 C.byref(info)), MergeError)
+    ref = swaths[0].slc
+    if out is None:
+        out = (_empty_like_kind(ref, (info.lines, info.samples), "f4"),
+               _empty_like_kind(ref, (info.lines, info.samples), "f4"))
+    _check(ctx, lib().sd_calibrate_deburst_merge(ctx.handle, len(swaths), arr, T.ptr(out[0]),
+                                                 T.ptr(out[1]), C.byref(info)), MergeError)
+    return _merged_from_info(info, out[0], out[1])
+
+
+# ── speckle ────────────────────────────────────────────────────────────────
+def apply_speckle_filter(data, cols: int, rows: int, filter: SpeckleFilter,
+                         ctx: Optional[Context] = None):
+    """apply_speckle_filter (speckle.rs:131-180): returns a new array of the
+    same shape; NaN is nodata."""
+    ctx = _ctx(ctx)
+    data = _prep(data, np.float32)
+    n = T.numel(data)
+    out = _empty_like_kind(data, tuple(data.shape), "f4")
+    rc = lib().sd_speckle(ctx.handle, T.ptr(data), n, cols, rows, filter.kind, filter.window,
+                          filter.enl, filter.damping, T.ptr(out))
+    _check(ctx, rc, SpeckleError)
+    return out
+
+
+class SpeckleKernel:
+    """The SpeckleKernel trait (speckle.rs:586-603)."""
+
+    def apply(self, data, cols: int, rows: int):
+        raise NotImplementedError
+
+
+class GpuSpeckleKernel(SpeckleKernel):
+    """SpeckleKernel implemented by the sm_100a filters."""
+
+    def __init__(self, filter: SpeckleFilter, ctx: Optional[Context] = None):
+        self.filter = filter
+        self.ctx = ctx
+
+    def apply(self, data, cols: int, rows: int):
+        return apply_speckle_filter(data, cols, rows, self.filter, self.ctx)
+
+
+def apply_speckle_step(data, cols: int, rows: int, kernel: Optional[SpeckleKernel]):
+    """apply_speckle_step (run.rs:108-123): replaces the buffer when a kernel
+    is given."""
+    if kernel is None:
+        return data
+    return kernel.apply(data, cols, rows)

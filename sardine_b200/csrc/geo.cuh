@@ -1,0 +1,391 @@
+// geo.cuh — geometry primitives of the terrain correction, written once for
+// host and device.  Every function reproduces the reference's arithmetic
+// operation by operation (IEEE f64/f32, left-to-right, no contraction: the
+// library is compiled with --fmad=false), so that integer outcomes (masks,
+// microsecond azimuth times, iteration counts) match the reference.
+//
+// Reference files: sardine/src/geodesy.rs, orbit.rs, dem.rs, geoid.rs,
+// terrain_correction.rs, output_crs.rs.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+
+#include "../../include/sardine_b200.h"
+
+#if defined(__CUDACC__)
+#define SD_HD __host__ __device__ __forceinline__
+#else
+#define SD_HD inline
+#endif
+
+namespace sd {
+
+constexpr double kPi = 3.14159265358979323846;  // std::f64::consts::PI
+constexpr double WGS84_A = 6378137.0;           // geodesy.rs:13
+constexpr double WGS84_F = 1.0 / 298.257223563; // geodesy.rs:16
+constexpr double WGS84_E2 = 2.0 * WGS84_F - WGS84_F * WGS84_F;  // geodesy.rs:22
+constexpr double SPEED_OF_LIGHT = 299792458.0;  // types.rs:11
+
+// Rust `x as i64` (saturating, NaN -> 0).
+SD_HD int64_t f2i64(double x) {
+  if (x != x) return 0;
+  if (x >= 9223372036854775807.0) return INT64_MAX;
+  if (x <= -9223372036854775808.0) return INT64_MIN;
+  return (int64_t)x;
+}
+// Rust `x as usize` (saturating at 0).
+SD_HD uint64_t f2u64(double x) {
+  if (x != x || x <= 0.0) return 0;
+  if (x >= 18446744073709551615.0) return UINT64_MAX;
+  return (uint64_t)x;
+}
+SD_HD double clampd(double x, double lo, double hi) {
+  if (x < lo) x = lo;
+  if (x > hi) x = hi;
+  return x;
+}
+SD_HD int64_t clampi(int64_t x, int64_t lo, int64_t hi) { return x < lo ? lo : (x > hi ? hi : x); }
+SD_HD float maxf_nan(float a, float b) {  // f32::max
+  return (a != a) ? b : ((b != b) ? a : (a > b ? a : b));
+}
+SD_HD double maxd_nan(double a, double b) {
+  return (a != a) ? b : ((b != b) ? a : (a > b ? a : b));
+}
+
+struct V3 {
+  double x, y, z;
+};
+SD_HD double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+SD_HD double norm3(V3 v) { return sqrt(dot3(v, v)); }
+SD_HD V3 sub3(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+SD_HD V3 cross3(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+SD_HD V3 normalize3(V3 v) {
+  double n = norm3(v);
+  if (n == 0.0) return {0.0, 0.0, 0.0};
+  return {v.x / n, v.y / n, v.z / n};
+}
+
+// geodetic_to_ecef (geodesy.rs:38-55)
+SD_HD V3 geodetic_to_ecef(double lat_deg, double lon_deg, double h) {
+  double lat = lat_deg * kPi / 180.0;
+  double lon = lon_deg * kPi / 180.0;
+  double sin_lat = sin(lat), cos_lat = cos(lat);
+  double sin_lon = sin(lon), cos_lon = cos(lon);
+  double n = WGS84_A / sqrt(1.0 - WGS84_E2 * sin_lat * sin_lat);
+  return {(n + h) * cos_lat * cos_lon, (n + h) * cos_lat * sin_lon,
+          (n * (1.0 - WGS84_E2) + h) * sin_lat};
+}
+
+// ── UTM: transverse Mercator by Krueger's n-series to sixth order, as given
+// by C. F. F. Karney (2011), J. Geodesy 85:475-485, eqs. 7-11, 14, 19-21, 35,
+// 36.  (The reference delegates UTM to the proj4rs crate.)
+struct Utm {
+  int32_t zone;
+  int32_t south;
+  double lon0;  // central meridian, radians
+  double k0A;
+  double e, e2m;
+  double alp[7], bet[7];
+};
+
+inline Utm make_utm(int zone, bool south) {
+  Utm u{};
+  u.zone = zone;
+  u.south = south ? 1 : 0;
+  u.lon0 = (double)((zone - 1) * 6 - 180 + 3) * (kPi / 180.0);
+  const double f = WGS84_F;
+  const double n = f / (2.0 - f);
+  const double n2 = n * n, n3 = n2 * n, n4 = n3 * n, n5 = n4 * n, n6 = n5 * n;
+  const double A = WGS84_A / (1.0 + n) * (1.0 + n2 / 4.0 + n4 / 64.0 + n6 / 256.0);
+  u.k0A = 0.9996 * A;
+  u.e = std::sqrt(f * (2.0 - f));
+  u.e2m = 1.0 - f * (2.0 - f);
+  u.alp[0] = 0.0;
+  u.alp[1] = n / 2.0 - 2.0 * n2 / 3.0 + 5.0 * n3 / 16.0 + 41.0 * n4 / 180.0 - 127.0 * n5 / 288.0 + 7891.0 * n6 / 37800.0;
+  u.alp[2] = 13.0 * n2 / 48.0 - 3.0 * n3 / 5.0 + 557.0 * n4 / 1440.0 + 281.0 * n5 / 630.0 - 1983433.0 * n6 / 1935360.0;
+  u.alp[3] = 61.0 * n3 / 240.0 - 103.0 * n4 / 140.0 + 15061.0 * n5 / 26880.0 + 167603.0 * n6 / 181440.0;
+  u.alp[4] = 49561.0 * n4 / 161280.0 - 179.0 * n5 / 168.0 + 6601661.0 * n6 / 7257600.0;
+  u.alp[5] = 34729.0 * n5 / 80640.0 - 3418889.0 * n6 / 1995840.0;
+  u.alp[6] = 212378941.0 * n6 / 319334400.0;
+  u.bet[0] = 0.0;
+  u.bet[1] = n / 2.0 - 2.0 * n2 / 3.0 + 37.0 * n3 / 96.0 - n4 / 360.0 - 81.0 * n5 / 512.0 + 96199.0 * n6 / 604800.0;
+  u.bet[2] = n2 / 48.0 + n3 / 15.0 - 437.0 * n4 / 1440.0 + 46.0 * n5 / 105.0 - 1118711.0 * n6 / 3870720.0;
+  u.bet[3] = 17.0 * n3 / 480.0 - 37.0 * n4 / 840.0 - 209.0 * n5 / 4480.0 + 5569.0 * n6 / 90720.0;
+  u.bet[4] = 4397.0 * n4 / 161280.0 - 11.0 * n5 / 504.0 - 830251.0 * n6 / 7257600.0;
+  u.bet[5] = 4583.0 * n5 / 161280.0 - 108847.0 * n6 / 3991680.0;
+  u.bet[6] = 20648693.0 * n6 / 638668800.0;
+  return u;
+}
+
+SD_HD double adjlon(double lam) {
+  while (lam > kPi) lam -= 2.0 * kPi;
+  while (lam < -kPi) lam += 2.0 * kPi;
+  return lam;
+}
+
+// sum_{j=1..6} c[j] sin(2 j zeta), zeta = xi + i eta  (complex Chebyshev recurrence)
+SD_HD void krueger_sum(const double *c, double xi, double eta, double *re, double *im) {
+  double s1 = sin(2.0 * xi), c1 = cos(2.0 * xi);
+  double sh1 = sinh(2.0 * eta), ch1 = cosh(2.0 * eta);
+  double sr = s1 * ch1, si = c1 * sh1;
+  double cr = c1 * ch1, ci = -s1 * sh1;
+  double pr = 0.0, pi = 0.0, qr = sr, qi = si, ar = 0.0, ai = 0.0;
+  for (int j = 1; j <= 6; ++j) {
+    ar += c[j] * qr;
+    ai += c[j] * qi;
+    double nr = 2.0 * (cr * qr - ci * qi) - pr;
+    double ni = 2.0 * (cr * qi + ci * qr) - pi;
+    pr = qr; pi = qi; qr = nr; qi = ni;
+  }
+  *re = ar;
+  *im = ai;
+}
+
+SD_HD double taupf(double tau, double e) {
+  double tau1 = hypot(1.0, tau);
+  double sig = sinh(e * atanh(e * tau / tau1));
+  return hypot(1.0, sig) * tau - sig * tau1;
+}
+
+SD_HD double tauf(double taup, double e, double e2m) {
+  double tau = taup / e2m;
+  for (int i = 0; i < 6; ++i) {
+    double taupa = taupf(tau, e);
+    double dtau = (taup - taupa) * (1.0 + e2m * tau * tau) / (e2m * hypot(1.0, tau) * hypot(1.0, taupa));
+    tau += dtau;
+    double lim = fabs(tau) > 1.0 ? fabs(tau) : 1.0;
+    if (!(fabs(dtau) >= 1e-15 * lim)) break;
+  }
+  return tau;
+}
+
+// lon/lat in degrees -> easting/northing (Projector::lonlat_to_xy, output_crs.rs:301-315)
+SD_HD void utm_lonlat_to_xy(const Utm &u, double lon_deg, double lat_deg, double *x, double *y) {
+  double lam = adjlon(lon_deg * (kPi / 180.0) - u.lon0);
+  double tau = tan(lat_deg * (kPi / 180.0));
+  double taup = taupf(tau, u.e);
+  double cl = cos(lam);
+  double xip = atan2(taup, cl);
+  double etap = asinh(sin(lam) / hypot(taup, cl));
+  double sr, si;
+  krueger_sum(u.alp, xip, etap, &sr, &si);
+  *x = 500000.0 + u.k0A * (etap + si);
+  *y = (u.south ? 10000000.0 : 0.0) + u.k0A * (xip + sr);
+}
+
+// easting/northing -> lon/lat in degrees (Projector::xy_to_lonlat, output_crs.rs:318-340)
+SD_HD void utm_xy_to_lonlat(const Utm &u, double x, double y, double *lon_deg, double *lat_deg) {
+  double xi = (y - (u.south ? 10000000.0 : 0.0)) / u.k0A;
+  double eta = (x - 500000.0) / u.k0A;
+  double sr, si;
+  krueger_sum(u.bet, xi, eta, &sr, &si);
+  double xip = xi - sr, etap = eta - si;
+  double s = sinh(etap), c = cos(xip);
+  double taup = sin(xip) / hypot(s, c);
+  double tau = tauf(taup, u.e, u.e2m);
+  *lat_deg = atan(tau) * (180.0 / kPi);
+  *lon_deg = adjlon(atan2(s, c) + u.lon0) * (180.0 / kPi);
+}
+
+// ── DEM: DemSource::elevation_at for one grid (dem.rs:351-409, 694-723) ────
+struct DemView {
+  const float *data;
+  uint64_t width, height;
+  double origin_y, origin_x, pixel_size;
+  int32_t kind;
+  Utm utm;
+};
+
+// returns false for Err(OutOfBounds); *h = NaN for voids.
+SD_HD bool dem_elevation(const DemView &d, double lat_deg, double lon_deg, float *h) {
+  double row_f, col_f;
+  if (d.kind == SD_DEM_GEOGRAPHIC) {
+    double lon_norm = lon_deg >= 180.0 ? lon_deg - 360.0 : lon_deg;
+    row_f = (d.origin_y - lat_deg) / d.pixel_size;
+    col_f = (lon_norm - d.origin_x) / d.pixel_size;
+  } else {
+    double x, y;
+    utm_lonlat_to_xy(d.utm, lon_deg, lat_deg, &x, &y);
+    row_f = (d.origin_y - y) / d.pixel_size;
+    col_f = (x - d.origin_x) / d.pixel_size;
+  }
+  double max_row = (double)(d.height - 1);
+  double max_col = (double)(d.width - 1);
+  if (row_f < -0.5 || row_f > max_row + 0.5 || col_f < -0.5 || col_f > max_col + 0.5) return false;
+  row_f = clampd(row_f, 0.0, max_row);
+  col_f = clampd(col_f, 0.0, max_col);
+  // bilinear_on_grid (dem.rs:385-409)
+  uint64_t max_rc = d.height - 1;
+  uint64_t r0 = f2u64(row_f);
+  uint64_t rlim = max_rc == 0 ? 0 : max_rc - 1;
+  if (r0 > rlim) r0 = rlim;
+  uint64_t c0 = f2u64(col_f);
+  uint64_t clim = d.width < 2 ? 0 : d.width - 2;
+  if (c0 > clim) c0 = clim;
+  uint64_t r1 = r0 + 1, c1 = c0 + 1;
+  double dr = row_f - (double)r0;
+  double dc = col_f - (double)c0;
+#if defined(__CUDA_ARCH__)
+  float v00 = __ldg(&d.data[r0 * d.width + c0]), v01 = __ldg(&d.data[r0 * d.width + c1]);
+  float v10 = __ldg(&d.data[r1 * d.width + c0]), v11 = __ldg(&d.data[r1 * d.width + c1]);
+#else
+  float v00 = d.data[r0 * d.width + c0], v01 = d.data[r0 * d.width + c1];
+  float v10 = d.data[r1 * d.width + c0], v11 = d.data[r1 * d.width + c1];
+#endif
+  if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) {
+    *h = NAN;
+    return true;
+  }
+  double v = (double)v00 * (1.0 - dr) * (1.0 - dc) + (double)v01 * (1.0 - dr) * dc +
+             (double)v10 * dr * (1.0 - dc) + (double)v11 * dr * dc;
+  *h = (float)v;
+  return true;
+}
+
+// ── geoid (geoid.rs:220-251) ───────────────────────────────────────────────
+SD_HD double geoid_undulation(const float *g, double lat_deg, double lon_deg) {
+  if (g == nullptr) return 0.0;
+  const uint64_t NLAT = 73, NLON = 144;
+  double lon = fmod(lon_deg, 360.0);
+  if (lon < 0.0) lon += 360.0;
+  double row_f = (90.0 - clampd(lat_deg, -90.0, 90.0)) / 2.5;
+  double col_f = lon / 2.5;
+  uint64_t r0 = f2u64(row_f);
+  if (r0 > NLAT - 2) r0 = NLAT - 2;
+  uint64_t r1 = r0 + 1;
+  uint64_t c0 = f2u64(col_f) % NLON;
+  uint64_t c1 = (c0 + 1) % NLON;
+  double dr = row_f - (double)r0;
+  double dc = col_f - (double)c0;
+  double v00 = g[r0 * NLON + c0], v01 = g[r0 * NLON + c1];
+  double v10 = g[r1 * NLON + c0], v11 = g[r1 * NLON + c1];
+  dc = clampd(dc, 0.0, 1.0);
+  return v00 * (1.0 - dr) * (1.0 - dc) + v01 * (1.0 - dr) * dc + v10 * dr * (1.0 - dc) + v11 * dr * dc;
+}
+
+// ── orbit: 8-point Lagrange position/velocity/acceleration (orbit.rs:498-596)
+struct OrbitState {
+  V3 pos, vel, acc;
+};
+enum { ORB_OK = 0, ORB_INSUFFICIENT = 1, ORB_OUTSIDE = 2 };
+
+SD_HD int orbit_eval(const sd_state_vector *svs, uint64_t n, int64_t t, OrbitState *o) {
+  if (n < 8) return ORB_INSUFFICIENT;
+  if (t < svs[0].time_us || t > svs[n - 1].time_us) return ORB_OUTSIDE;
+  const int64_t t_ref = svs[0].time_us;
+  const double t_sec = (double)(t - t_ref) / 1e6;
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) / 2;
+    if (svs[mid].time_us <= t) lo = mid + 1; else hi = mid;
+  }
+  const uint64_t centre = lo - 1;
+  const uint64_t start = centre < 4 ? 0 : (centre + 4 >= n ? n - 8 : centre - 3);
+  double times[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) times[i] = (double)(svs[start + i].time_us - t_ref) / 1e6;
+  double rdiff[8];
+  double total = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    double diff = t_sec - times[j];
+    rdiff[j] = 0.0;
+    if (fabs(diff) > 1e-9) {
+      rdiff[j] = 1.0 / diff;
+      total += rdiff[j];
+    }
+  }
+  double p0 = 0, p1 = 0, p2 = 0, v0 = 0, v1 = 0, v2 = 0, a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double basis = 1.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      if (j != k) basis *= (t_sec - times[j]) / (times[k] - times[j]);
+    double db = basis * (total - rdiff[k]);
+    const sd_state_vector &sv = svs[start + k];
+    p0 += basis * sv.position_m[0];
+    p1 += basis * sv.position_m[1];
+    p2 += basis * sv.position_m[2];
+    v0 += basis * sv.velocity_m_s[0];
+    v1 += basis * sv.velocity_m_s[1];
+    v2 += basis * sv.velocity_m_s[2];
+    a0 += db * sv.velocity_m_s[0];
+    a1 += db * sv.velocity_m_s[1];
+    a2 += db * sv.velocity_m_s[2];
+  }
+  o->pos = {p0, p1, p2};
+  o->vel = {v0, v1, v2};
+  o->acc = {a0, a1, a2};
+  return ORB_OK;
+}
+
+// One Newton step of solve_zero_doppler (terrain_correction.rs:1030-1067).
+// Returns 0 = converged (|delta| < tol), 1 = step (t advanced), 2 = degenerate.
+SD_HD int zd_step(V3 target, const OrbitState &s, double tol, double *delta_out) {
+  V3 r = sub3(target, s.pos);
+  double f = dot3(r, s.vel);
+  double v_sq = dot3(s.vel, s.vel);
+  double f_prime = -v_sq + dot3(r, s.acc);
+  if (fabs(f_prime) < 1.0) return 2;
+  double delta = -f / f_prime;
+  *delta_out = delta;
+  if (fabs(delta) < tol) return 0;
+  return 1;
+}
+
+// ── resampling kernels (terrain_correction.rs:770-983) ─────────────────────
+SD_HD double keys_weight(double t) {
+  t = fabs(t);
+  if (t < 1.0) return 1.5 * t * t * t - 2.5 * t * t + 1.0;
+  if (t < 2.0) return -0.5 * t * t * t + 2.5 * t * t - 4.0 * t + 2.0;
+  return 0.0;
+}
+
+SD_HD double lanczos_weight(double x) {
+  double ax = fabs(x);
+  if (ax < 1e-10) return 1.0;
+  if (ax < 3.0) {
+    double px = kPi * x;
+    double pxa = kPi * x / 3.0;
+    return sin(px) * sin(pxa) / (px * pxa);
+  }
+  return 0.0;
+}
+
+// ── terrain geometry (terrain_correction.rs:576-651) ───────────────────────
+enum { GEOM_VALID = 0, GEOM_FORESHORTENING = 1, GEOM_LAYOVER = 2, GEOM_SHADOW = 3 };
+
+SD_HD double flat_cell_area(double lat, double lon, double sp) {
+  V3 fe = geodetic_to_ecef(lat, lon + sp, 0.0);
+  V3 fw = geodetic_to_ecef(lat, lon - sp, 0.0);
+  V3 fn = geodetic_to_ecef(lat + sp, lon, 0.0);
+  V3 fs = geodetic_to_ecef(lat - sp, lon, 0.0);
+  return norm3(cross3(sub3(fe, fw), sub3(fn, fs)));
+}
+
+SD_HD int terrain_geometry(double lat, double lon, double he, double hw, double hn, double hs,
+                           V3 sat, V3 target, double sp, double flat_area, double *w_out,
+                           double *cos_lia_out) {
+  V3 pe = geodetic_to_ecef(lat, lon + sp, he);
+  V3 pw = geodetic_to_ecef(lat, lon - sp, hw);
+  V3 pn = geodetic_to_ecef(lat + sp, lon, hn);
+  V3 ps = geodetic_to_ecef(lat - sp, lon, hs);
+  V3 normal = cross3(sub3(pe, pw), sub3(pn, ps));
+  V3 look = normalize3(sub3(sat, target));
+  double local_proj = dot3(normal, look);
+  if (local_proj <= 0.0) return GEOM_SHADOW;
+  double area = norm3(normal);
+  if (area == 0.0) return GEOM_SHADOW;
+  *cos_lia_out = clampd(local_proj / area, 0.0, 1.0);
+  double w = local_proj / flat_area;
+  *w_out = w;
+  if (w < 0.05) return GEOM_FORESHORTENING;
+  if (w > 2.0) return GEOM_LAYOVER;
+  return GEOM_VALID;
+}
+
+}  // namespace sd

@@ -1,0 +1,142 @@
+// runtime.cu — context lifecycle, error reporting and staging.
+#include "runtime.cuh"
+
+namespace sd {
+
+int set_error(sd_ctx *ctx, int code, const char *fmt, ...) {
+  if (ctx) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return code;
+}
+
+int scratch(sd_ctx *ctx, const char *name, size_t bytes, void **out) {
+  if (bytes == 0) bytes = 16;
+  auto &b = ctx->scratch[name];
+  if (b.bytes < bytes) {
+    if (b.p) {
+      cudaStreamSynchronize(ctx->stream);
+      cudaFree(b.p);
+      b.p = nullptr;
+      b.bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      b.p = nullptr;
+      return set_error(ctx, SD_ERR_OUT_OF_MEMORY, "scratch '%s': cudaMalloc(%zu) failed: %s",
+                       name, bytes, cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+  }
+  *out = b.p;
+  return SD_OK;
+}
+
+bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int stage_in(sd_ctx *ctx, const char *name, const void *p, size_t bytes, const void **dev) {
+  if (!p) {
+    *dev = nullptr;
+    return SD_OK;
+  }
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return SD_OK;
+  }
+  void *d = nullptr;
+  SD_TRY(scratch(ctx, name, bytes, &d));
+  SD_CUDA(ctx, cudaMemcpyAsync(d, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  *dev = d;
+  return SD_OK;
+}
+
+int stage_out(sd_ctx *ctx, const char *name, void *p, size_t bytes, void **dev) {
+  if (!p) {
+    *dev = nullptr;
+    return SD_OK;
+  }
+  if (is_device_ptr(p)) {
+    *dev = p;
+    return SD_OK;
+  }
+  return scratch(ctx, name, bytes, dev);
+}
+
+int finish_out(sd_ctx *ctx, void *user, const void *dev, size_t bytes) {
+  if (!user || user == dev || bytes == 0) return SD_OK;
+  SD_CUDA(ctx, cudaMemcpyAsync(user, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return SD_OK;
+}
+
+int sync(sd_ctx *ctx) {
+  SD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SD_OK;
+}
+
+}  // namespace sd
+
+extern "C" {
+
+int sd_abi_version(void) { return SD_ABI_VERSION; }
+
+int sd_ctx_create(int device, sd_ctx **out) {
+  if (!out) return SD_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return SD_ERR_CUDA;
+  }
+  if (device < 0 || device >= n) return SD_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return SD_ERR_CUDA;
+  sd_ctx *c = new sd_ctx();
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaMalloc(&c->d_flags, 64 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&c->d_counters, 64 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    sd_ctx_destroy(c);
+    return SD_ERR_CUDA;
+  }
+  *out = c;
+  return SD_OK;
+}
+
+void sd_ctx_destroy(sd_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto &kv : ctx->scratch)
+    if (kv.second.p) cudaFree(kv.second.p);
+  for (void *p : ctx->pinned) cudaFreeHost(p);
+  if (ctx->d_flags) cudaFree(ctx->d_flags);
+  if (ctx->d_counters) cudaFree(ctx->d_counters);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char *sd_last_error(const sd_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+uint64_t sd_kernel_launches(const sd_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+void *sd_ctx_stream(sd_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// runtime.cuh — context, scratch memory and host/device staging shared by the
+// entry points of libsardine_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/sardine_b200.h"
+
+struct sd_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string last_error;
+  uint64_t launches = 0;
+  struct Buf {
+    void *p = nullptr;
+    size_t bytes = 0;
+  };
+  std::unordered_map<std::string, Buf> scratch;  // grow-only named device buffers
+  std::vector<void *> pinned;                    // grow-only pinned staging buffers
+  int *d_flags = nullptr;                        // device-side error words
+  unsigned long long *d_counters = nullptr;      // device-side counters (64 slots)
+};
+
+namespace sd {
+
+int set_error(sd_ctx *ctx, int code, const char *fmt, ...);
+
+#define SD_CUDA(ctx, call)                                                               \
+  do {                                                                                   \
+    cudaError_t e__ = (call);                                                            \
+    if (e__ != cudaSuccess)                                                              \
+      return ::sd::set_error((ctx), e__ == cudaErrorMemoryAllocation ? SD_ERR_OUT_OF_MEMORY \
+                                                                     : SD_ERR_CUDA,      \
+                             "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e__),    \
+                             __FILE__, __LINE__);                                        \
+  } while (0)
+
+#define SD_LAUNCHED(ctx)                                                                  \
+  do {                                                                                   \
+    (ctx)->launches++;                                                                   \
+    cudaError_t e__ = cudaGetLastError();                                                \
+    if (e__ != cudaSuccess)                                                              \
+      return ::sd::set_error((ctx), SD_ERR_CUDA, "kernel launch failed: %s (%s:%d)",     \
+                             cudaGetErrorString(e__), __FILE__, __LINE__);               \
+  } while (0)
+
+#define SD_TRY(expr)            \
+  do {                          \
+    int r__ = (expr);           \
+    if (r__ != SD_OK) return r__; \
+  } while (0)
+
+// Named grow-only device scratch buffer.
+int scratch(sd_ctx *ctx, const char *name, size_t bytes, void **out);
+template <class T>
+int scratch_t(sd_ctx *ctx, const char *name, size_t count, T **out) {
+  void *p = nullptr;
+  int rc = scratch(ctx, name, count * sizeof(T), &p);
+  *out = (T *)p;
+  return rc;
+}
+
+// True when `p` is device (or managed) memory usable by kernels on ctx->device.
+bool is_device_ptr(const void *p);
+
+// Input view: device pointer to `bytes` of data, staged through scratch
+// `name` when the caller passed host memory.
+int stage_in(sd_ctx *ctx, const char *name, const void *p, size_t bytes, const void **dev);
+// Output view: a device buffer for `bytes`; after the kernels run call
+// finish_out to copy back when the caller passed host memory.
+int stage_out(sd_ctx *ctx, const char *name, void *p, size_t bytes, void **dev);
+int finish_out(sd_ctx *ctx, void *user, const void *dev, size_t bytes);
+int sync(sd_ctx *ctx);
+
+inline unsigned grid_for(size_t n, unsigned block) {
+  size_t g = (n + block - 1) / block;
+  return (unsigned)(g == 0 ? 1 : g);
+}
+
+}  // namespace sd

@@ -1,0 +1,911 @@
+// tc.cu — backward Range-Doppler terrain correction on sm_100a.
+//
+// Replaces terrain_correction (sardine/src/terrain_correction.rs:1245-1836).
+//
+// The reference walks each output row column by column: the Newton
+// zero-Doppler solve of column c starts from the converged azimuth time of
+// the previous converged column (1443, 1580), moves in whole microseconds
+// truncated toward zero (1067) and stops BEFORE applying a sub-tolerance
+// step (1045-1065).  The converged time therefore depends on the seed, and a
+// 1 us difference moves the sample by ~5e-4 azimuth line.  This file
+// reproduces that chain exactly while keeping the work data-parallel:
+//
+//  K1 k_orbit_table   FP64 Lagrange state (pos, vel, acc, |v|^2) at every
+//                     microsecond of the span the scene needs (80 B each), so
+//                     a Newton iteration is one table read instead of an
+//                     8-point Lagrange evaluation with 64 divisions.
+//  K2 k_row_*         per-row set-up: UTM anchors (output_crs.rs:364-417),
+//                     latitude seed, LUT guess, flat-cell area, and a coarse
+//                     azimuth-time model (17 knots per row).
+//  K3 k_geo           per pixel: DEM, geoid, target ECEF; the reference
+//                     iteration from the model time gives one converged time
+//                     t*; the set F = {t : |delta(t)| < tol} of possible
+//                     converged times is {t*-1, t*, t*+1} filtered.
+//  K4 k_cand          per pixel: the reference iteration from every seed in
+//                     F of the left neighbour (the only seeds the chain can
+//                     hand it), encoded as an index into its own F.
+//  K5 k_scan          per row: walks the columns selecting the precomputed
+//                     outcome that matches the actual seed (a byte compare per
+//                     pixel); any seed outside the precomputed set runs the
+//                     reference iteration in place.
+//  K6 k_out           per pixel: slant range, footprint test, resampling,
+//                     Small-2011 geometry, mask, NESZ, counters, histogram.
+#include <algorithm>
+#include <limits>
+
+#include "geo.cuh"
+#include "runtime.cuh"
+
+namespace sd {
+namespace {
+
+enum : uint8_t { ST_CONV = 0, ST_NONCONV = 1, ST_DEGEN = 2, ST_ORBIT = 3, ST_DEMMISS = 4 };
+enum : uint8_t { RF_DEM_MISSING = 1, RF_HAS_F = 2 };
+constexpr uint8_t CODE_NONE = 0xFF;
+constexpr int KNOTS = 17;
+constexpr int kCounters = 8;  // valid, dem, outside, nonconv, degen, flat, noise, spare
+
+struct Rec {       // 16 B per pixel
+  int64_t base;    // F members are base + k for mask bit k
+  uint8_t mask;
+  uint8_t flags;
+  uint8_t pad[6];
+};
+
+struct OrbitDev {
+  const sd_state_vector *svs;
+  uint64_t n;
+  const double2 *tab;  // 5 double2 per microsecond
+  int64_t tab_t0;
+  int64_t tab_n;
+};
+
+__device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
+  int64_t i = t - o.tab_t0;
+  if (i >= 0 && i < o.tab_n) {
+    const double2 *e = o.tab + 5 * i;
+    double2 a = __ldg(e), b = __ldg(e + 1), c = __ldg(e + 2), d = __ldg(e + 3), f = __ldg(e + 4);
+    s->pos = {a.x, a.y, b.x};
+    s->vel = {b.y, c.x, c.y};
+    s->acc = {d.x, d.y, f.x};
+    *vsq = f.y;
+    return ORB_OK;
+  }
+  int rc = orbit_eval(o.svs, o.n, t, s);
+  if (rc == ORB_OK) *vsq = dot3(s->vel, s->vel);
+  return rc;
+}
+
+struct ZdRes {
+  uint8_t st;
+  int64_t t;
+  int it;
+};
+
+// solve_zero_doppler (terrain_correction.rs:1010-1073), bit-exact.
+__device__ ZdRes newton(const OrbitDev &o, V3 P, int64_t seed, int max_iter, double tol) {
+  int64_t t = seed;
+  for (int i = 0; i < max_iter; ++i) {
+    OrbitState s;
+    double vsq;
+    if (orbit_at(o, t, &s, &vsq) != ORB_OK) return {ST_ORBIT, t, i};
+    V3 r = sub3(P, s.pos);
+    double f = dot3(r, s.vel);
+    double fp = -vsq + dot3(r, s.acc);
+    if (fabs(fp) < 1.0) return {ST_DEGEN, t, i};
+    double delta = -f / fp;
+    if (fabs(delta) < tol) return {ST_CONV, t, i + 1};
+    t = t + f2i64(delta * 1e6);
+  }
+  return {ST_NONCONV, t, max_iter};
+}
+
+// True when the reference iteration seeded at t converges there immediately.
+__device__ bool fixed_point(const OrbitDev &o, V3 P, int64_t t, double tol) {
+  OrbitState s;
+  double vsq;
+  if (orbit_at(o, t, &s, &vsq) != ORB_OK) return false;
+  V3 r = sub3(P, s.pos);
+  double f = dot3(r, s.vel);
+  double fp = -vsq + dot3(r, s.acc);
+  if (fabs(fp) < 1.0) return false;
+  double delta = -f / fp;
+  return fabs(delta) < tol;
+}
+
+struct TcDev {
+  // output grid
+  uint64_t rows, cols;
+  double lat_north, lon_west, sp, step_deg;
+  int utm;
+  Utm proj;
+  // anchors (UTM)
+  const double *ax;   // n_pts
+  const double *alon; // rows * n_pts
+  const double *alat;
+  int n_anchors, n_pts;
+  // LUT
+  const double *lut_lat;
+  const int64_t *lut_t;
+  int lut_n;
+  // rows
+  int64_t *row_guess;
+  double *row_flat;
+  int64_t *knot_t;
+  // scene
+  OrbitDev orb;
+  DemView dem;
+  const float *geoid;
+  const float *img;
+  const float *nesz;
+  uint64_t lines, samples;
+  int64_t az_start;
+  double ati, near_range, rps;
+  int max_iter;
+  double tol;
+  int flatten, compute_lia, need_geom, resampling, nesz_mask;
+  float nesz_factor;
+  // per-pixel scratch
+  double *px, *py, *pz;
+  Rec *rec;
+  uint32_t *codes;
+  int64_t *tsol;
+  uint8_t *stit;
+  // outputs
+  float *out;
+  float *cos_lia;
+  uint8_t *mask;
+  int *flags;
+  unsigned long long *counters;
+  unsigned long long *trange;  // [0] = min, [1] = max (biased by 2^63)
+};
+
+__device__ __forceinline__ double row_y(const TcDev &p, uint64_t r) {
+  return p.lat_north - ((double)r + 0.5) * p.sp;
+}
+
+// Output pixel centre in lon/lat: direct for WGS84, project_row anchors for
+// UTM (output_crs.rs:383-415).
+__device__ void pixel_lonlat(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat) {
+  if (!p.utm) {
+    *lon = p.lon_west + ((double)c + 0.5) * p.sp;
+    *lat = row_y(p, r);
+    return;
+  }
+  const double x_start = p.lon_west + 0.5 * p.sp;
+  const double x = x_start + (double)c * p.sp;
+  const int na = p.n_anchors;
+  // segment: smallest s with s == na-1 or x <= ax[s+1]
+  double anchor_dx = p.ax[1] - p.ax[0];
+  int g = 0;
+  if (anchor_dx > 0.0) {
+    double q = floor((x - x_start) / anchor_dx);
+    g = q < 0.0 ? 0 : (q > (double)(na - 1) ? na - 1 : (int)q);
+  }
+  while (g > 0 && x <= p.ax[g]) g--;
+  while (g + 1 < na && x > p.ax[g + 1]) g++;
+  const double x0 = p.ax[g], x1 = p.ax[g + 1];
+  const double *lo = p.alon + r * p.n_pts, *la = p.alat + r * p.n_pts;
+  double t = (x1 == x0) ? 0.0 : (x - x0) / (x1 - x0);
+  *lon = lo[g] + t * (lo[g + 1] - lo[g]);
+  *lat = la[g] + t * (la[g + 1] - la[g]);
+}
+
+// guess_azimuth_time (terrain_correction.rs:1107-1137)
+__device__ int64_t guess_time(const TcDev &p, double lat) {
+  if (p.lut_n == 1) return p.lut_t[0];
+  int lo = 0, hi = p.lut_n;
+  while (lo < hi) {
+    int mid = lo + (hi - lo) / 2;
+    double v = p.lut_lat[mid];
+    if (v < lat) lo = mid + 1;
+    else if (v > lat) hi = mid;
+    else return p.lut_t[mid];
+  }
+  if (lo == 0) return p.lut_t[0];
+  if (lo >= p.lut_n) return p.lut_t[p.lut_n - 1];
+  double frac = (lat - p.lut_lat[lo - 1]) / (p.lut_lat[lo] - p.lut_lat[lo - 1]);
+  double dt_us = (double)(p.lut_t[lo] - p.lut_t[lo - 1]);
+  return p.lut_t[lo - 1] + f2i64(frac * dt_us);
+}
+
+// ── K1 ─────────────────────────────────────────────────────────────────────
+__global__ void k_orbit_table(const sd_state_vector *svs, uint64_t n, int64_t t0, int64_t cnt,
+                              double2 *tab) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  OrbitState s;
+  orbit_eval(svs, n, t0 + i, &s);  // range is inside the state-vector window
+  double2 *e = tab + 5 * i;
+  e[0] = make_double2(s.pos.x, s.pos.y);
+  e[1] = make_double2(s.pos.z, s.vel.x);
+  e[2] = make_double2(s.vel.y, s.vel.z);
+  e[3] = make_double2(s.acc.x, s.acc.y);
+  e[4] = make_double2(s.acc.z, dot3(s.vel, s.vel));
+}
+
+// ── K2 ─────────────────────────────────────────────────────────────────────
+__global__ void k_row_anchors(TcDev p) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t total = p.rows * (uint64_t)p.n_pts;
+  if (i >= total) return;
+  uint64_t r = i / p.n_pts, a = i % p.n_pts;
+  double lon, lat;
+  utm_xy_to_lonlat(p.proj, p.ax[a], row_y(p, r), &lon, &lat);
+  ((double *)p.alon)[i] = lon;
+  ((double *)p.alat)[i] = lat;
+}
+
+__global__ void k_row_setup(TcDev p) {
+  uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.rows) return;
+  const double y = row_y(p, r);
+  double lat_seed = y;
+  if (p.utm) {
+    double mid_x = p.lon_west + ((double)p.cols / 2.0) * p.sp;
+    double lo;
+    utm_xy_to_lonlat(p.proj, mid_x, y, &lo, &lat_seed);
+  }
+  p.row_guess[r] = guess_time(p, lat_seed);
+  if (p.need_geom) {
+    double ref_lon;
+    if (p.utm) {
+      double la;
+      pixel_lonlat(p, r, p.cols / 2, &ref_lon, &la);
+    } else {
+      ref_lon = p.lon_west + ((double)p.cols / 2.0) * p.sp;
+    }
+    p.row_flat[r] = flat_cell_area(lat_seed, ref_lon, p.step_deg);
+  }
+}
+
+__device__ __forceinline__ uint64_t knot_col(const TcDev &p, int j) {
+  return p.cols <= 1 ? 0 : (uint64_t)j * (p.cols - 1) / (KNOTS - 1);
+}
+
+// Coarse azimuth-time model: the reference iteration at KNOTS columns per
+// row with the geoid surface (h = 0 orthometric).  Only a seed predictor.
+__global__ void k_row_model(TcDev p) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.rows * KNOTS) return;
+  uint64_t r = i / KNOTS;
+  int j = (int)(i % KNOTS);
+  uint64_t c = knot_col(p, j);
+  double lon, lat;
+  pixel_lonlat(p, r, c, &lon, &lat);
+  V3 P = geodetic_to_ecef(lat, lon, geoid_undulation(p.geoid, lat, lon));
+  ZdRes z = newton(p.orb, P, p.row_guess[r], 40, 1e-6);
+  if (z.st == ST_CONV) {
+    p.knot_t[i] = z.t;
+    unsigned long long b = (unsigned long long)z.t ^ 0x8000000000000000ull;
+    atomicMin(&p.trange[0], b);
+    atomicMax(&p.trange[1], b);
+  } else {
+    p.knot_t[i] = INT64_MIN;
+  }
+}
+
+__device__ int64_t predicted_time(const TcDev &p, uint64_t r, uint64_t c) {
+  const int64_t *k = p.knot_t + r * KNOTS;
+  if (p.cols <= 1) return k[0] != INT64_MIN ? k[0] : p.row_guess[r];
+  int j = (int)((c * (KNOTS - 1)) / (p.cols - 1));
+  if (j >= KNOTS - 1) j = KNOTS - 2;
+  uint64_t c0 = knot_col(p, j), c1 = knot_col(p, j + 1);
+  int64_t t0 = k[j], t1 = k[j + 1];
+  if (t0 == INT64_MIN && t1 == INT64_MIN) return p.row_guess[r];
+  if (t0 == INT64_MIN) return t1;
+  if (t1 == INT64_MIN || c1 == c0) return t0;
+  double f = (double)(c - c0) / (double)(c1 - c0);
+  return t0 + (int64_t)llrint(f * (double)(t1 - t0));
+}
+
+// ── K3 ─────────────────────────────────────────────────────────────────────
+__global__ void __launch_bounds__(256) k_geo(TcDev p, int fast) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.rows * p.cols) return;
+  uint64_t r = i / p.cols, c = i % p.cols;
+  double lon, lat;
+  pixel_lonlat(p, r, c, &lon, &lat);
+  float hf;
+  Rec rec;
+  rec.base = 0;
+  rec.mask = 0;
+  rec.flags = 0;
+  if (!dem_elevation(p.dem, lat, lon, &hf) || !isfinite(hf)) {
+    rec.flags = RF_DEM_MISSING;
+    p.rec[i] = rec;
+    return;
+  }
+  double h_ell = (double)hf + geoid_undulation(p.geoid, lat, lon);
+  V3 P = geodetic_to_ecef(lat, lon, h_ell);
+  p.px[i] = P.x;
+  p.py[i] = P.y;
+  p.pz[i] = P.z;
+  if (fast) {
+    ZdRes z = newton(p.orb, P, predicted_time(p, r, c), 40, p.tol);
+    if (z.st == ST_CONV) {
+      rec.base = z.t - 1;
+      rec.mask = 2 | (fixed_point(p.orb, P, z.t - 1, p.tol) ? 1 : 0) |
+                 (fixed_point(p.orb, P, z.t + 1, p.tol) ? 4 : 0);
+      rec.flags = RF_HAS_F;
+    }
+  }
+  p.rec[i] = rec;
+}
+
+// ── K4 ─────────────────────────────────────────────────────────────────────
+__global__ void __launch_bounds__(256) k_cand(TcDev p) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.rows * p.cols) return;
+  uint64_t c = i % p.cols;
+  uint32_t codes = 0xFFFFFFFFu;
+  Rec me = p.rec[i];
+  if (c > 0 && (me.flags & RF_HAS_F)) {
+    Rec lf = p.rec[i - 1];
+    if (lf.flags & RF_HAS_F) {
+      V3 P = {p.px[i], p.py[i], p.pz[i]};
+      for (int k = 0; k < 3; ++k) {
+        if (!((lf.mask >> k) & 1)) continue;
+        ZdRes z = newton(p.orb, P, lf.base + k, p.max_iter, p.tol);
+        uint32_t code = CODE_NONE;
+        int it = z.it > 15 ? 15 : z.it;
+        if (z.st == ST_CONV) {
+          int64_t d = z.t - me.base;
+          if (d >= 0 && d <= 2 && ((me.mask >> d) & 1)) code = (uint32_t)d | ((uint32_t)it << 4);
+        } else if (z.st == ST_NONCONV || z.st == ST_DEGEN) {
+          code = 3u | ((uint32_t)z.st << 2) | ((uint32_t)it << 4);
+        }
+        codes = (codes & ~(0xFFu << (8 * k))) | (code << (8 * k));
+      }
+    }
+  }
+  p.codes[i] = codes;
+}
+
+// ── K5 ─────────────────────────────────────────────────────────────────────
+__global__ void __launch_bounds__(128) k_scan(TcDev p) {
+  uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.rows) return;
+  int64_t s = p.row_guess[r];
+  int64_t prev_base = 0;
+  uint8_t prev_mask = 0;
+  const uint64_t base_i = r * p.cols;
+  for (uint64_t c = 0; c < p.cols; ++c) {
+    const uint64_t i = base_i + c;
+    Rec rec = p.rec[i];
+    if (rec.flags & RF_DEM_MISSING) {
+      p.stit[i] = ST_DEMMISS;
+      prev_mask = 0;
+      continue;
+    }
+    uint32_t code = CODE_NONE;
+    if (prev_mask && (rec.flags & RF_HAS_F)) {
+      int64_t k = s - prev_base;
+      if (k >= 0 && k <= 2 && ((prev_mask >> k) & 1)) code = (p.codes[i] >> (8 * k)) & 0xFFu;
+    }
+    uint8_t st;
+    int it;
+    int64_t t;
+    if (code != CODE_NONE) {
+      it = (int)(code >> 4);
+      if ((code & 3u) != 3u) {
+        st = ST_CONV;
+        t = rec.base + (int64_t)(code & 3u);
+      } else {
+        st = (uint8_t)((code >> 2) & 3u);
+        t = s;
+      }
+    } else {
+      V3 P = {p.px[i], p.py[i], p.pz[i]};
+      ZdRes z = newton(p.orb, P, s, p.max_iter, p.tol);
+      st = z.st;
+      t = z.t;
+      it = z.it > 15 ? 15 : z.it;
+    }
+    p.tsol[i] = t;
+    p.stit[i] = (uint8_t)(st | (it << 4));
+    if (st == ST_CONV) s = t;
+    if (st == ST_ORBIT) atomicOr(&p.flags[0], 1);
+    prev_base = rec.base;
+    prev_mask = (rec.flags & RF_HAS_F) ? rec.mask : 0;
+  }
+}
+
+// ── K6 ─────────────────────────────────────────────────────────────────────
+__device__ __forceinline__ float ldf(const float *p, int64_t i) { return __ldg(p + i); }
+
+__device__ float sample_bilinear(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+  int64_t max_line = nl == 0 ? 0 : (int64_t)nl - 1;
+  int64_t max_sample = ns == 0 ? 0 : (int64_t)ns - 1;
+  int64_t l0 = clampi(f2i64(floor(line)), 0, max_line);
+  int64_t l1 = l0 + 1 < max_line ? l0 + 1 : max_line;
+  int64_t s0 = clampi(f2i64(floor(sample)), 0, max_sample);
+  int64_t s1 = s0 + 1 < max_sample ? s0 + 1 : max_sample;
+  double dl = line - (double)l0;
+  double ds = sample - (double)s0;
+  float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
+  float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
+  if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
+  double w00 = (1.0 - dl) * (1.0 - ds);
+  double w01 = (1.0 - dl) * ds;
+  double w10 = dl * (1.0 - ds);
+  double w11 = dl * ds;
+  return (float)((double)v00 * w00 + (double)v01 * w01 + (double)v10 * w10 + (double)v11 * w11);
+}
+
+__device__ float sample_bicubic(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
+  double dl = line - (double)lf, ds = sample - (double)sf;
+  double ws[4];
+  int64_t cols[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ws[k] = keys_weight((double)(k - 1) - ds);
+    cols[k] = clampi(sf + k - 1, 0, max_s);
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int li = -1; li <= 2; ++li) {
+    int64_t row = clampi(lf + li, 0, max_l);
+    double wl = keys_weight((double)li - dl);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) return NAN;
+      acc += (double)v * wl * ws[k];
+    }
+  }
+  return (float)acc;
+}
+
+__device__ float sample_lanczos(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
+  double ws[6];
+  int64_t cols[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    ws[k] = lanczos_weight(sample - (double)(sf + k - 2));
+    cols[k] = clampi(sf + k - 2, 0, max_s);
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int li = -2; li <= 3; ++li) {
+    int64_t row = clampi(lf + li, 0, max_l);
+    double wl = lanczos_weight(line - (double)(lf + li));
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) return NAN;
+      acc += (double)v * wl * ws[k];
+    }
+  }
+  return (float)acc;
+}
+
+template <int KERNEL>
+__global__ void __launch_bounds__(256) k_out(TcDev p) {
+  __shared__ unsigned int s_cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
+  for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
+  __syncthreads();
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < p.rows * p.cols) {
+    uint64_t r = i / p.cols, c = i % p.cols;
+    uint8_t code = p.stit[i];
+    uint8_t st = code & 15;
+    int it = code >> 4;
+    float outv = NAN, cosv = NAN;
+    uint8_t m = SD_MASK_OUTSIDE_FOOTPRINT;
+    int counter = -1;
+    if (st == ST_DEMMISS) {
+      m = SD_MASK_DEM_MISSING;
+      counter = 1;
+    } else if (st == ST_NONCONV) {
+      m = SD_MASK_NON_CONVERGED;
+      counter = 3;
+    } else if (st == ST_DEGEN) {
+      m = SD_MASK_DEGENERATE_GEOMETRY;
+      counter = 4;
+    } else if (st == ST_CONV) {
+      atomicAdd(&s_cnt[kCounters + it], 1u);
+      const int64_t t = p.tsol[i];
+      OrbitState s;
+      double vsq;
+      orbit_at(p.orb, t, &s, &vsq);
+      V3 P = {p.px[i], p.py[i], p.pz[i]};
+      double slant = norm3(sub3(P, s.pos));
+      double dt = (double)(t - p.az_start) / 1e6;
+      double line = dt / p.ati;
+      double sample = (slant - p.near_range) / p.rps;
+      do {
+        if (line < -0.5 || line > ((double)p.lines - 0.5) || sample < -0.5 ||
+            sample > ((double)p.samples - 0.5)) {
+          counter = 2;
+          break;
+        }
+        float sigma0 = KERNEL == SD_RESAMPLE_BICUBIC   ? sample_bicubic(p.img, p.lines, p.samples, line, sample)
+                       : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos(p.img, p.lines, p.samples, line, sample)
+                                                        : sample_bilinear(p.img, p.lines, p.samples, line, sample);
+        if (sigma0 != sigma0) {
+          counter = 2;
+          break;
+        }
+        if (p.need_geom) {
+          double lon, lat;
+          pixel_lonlat(p, r, c, &lon, &lat);
+          const double sd = p.step_deg;
+          float he, hw, hn, hs;
+          bool ok = dem_elevation(p.dem, lat, lon + sd, &he);
+          ok = dem_elevation(p.dem, lat, lon - sd, &hw) && ok;
+          ok = dem_elevation(p.dem, lat + sd, lon, &hn) && ok;
+          ok = dem_elevation(p.dem, lat - sd, lon, &hs) && ok;
+          ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
+          if (!ok) {
+            m = SD_MASK_DEM_NEIGHBOUR_MISSING;
+            if (p.flatten) {
+              counter = 5;
+              break;
+            }
+          } else {
+            double w = 0.0, cl = 0.0;
+            int g = terrain_geometry(lat, lon, (double)he, (double)hw, (double)hn, (double)hs, s.pos,
+                                     P, sd, p.row_flat[r], &w, &cl);
+            if (g == GEOM_VALID) {
+              cosv = (float)cl;
+              if (p.flatten) sigma0 /= (float)w;
+            } else if (g == GEOM_FORESHORTENING || g == GEOM_LAYOVER) {
+              cosv = (float)cl;
+              m = g == GEOM_LAYOVER ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING;
+              if (p.flatten) {
+                counter = 5;
+                break;
+              }
+            } else {
+              m = SD_MASK_SHADOW;
+              if (p.flatten) {
+                counter = 5;
+                break;
+              }
+            }
+          }
+        }
+        if (p.nesz_mask) {
+          float nz = sample_bilinear(p.nesz, p.lines, p.samples, line, sample);
+          if (nz == nz) {
+            float thr = nz * p.nesz_factor;
+            if (sigma0 <= thr) {
+              m = SD_MASK_NOISE_MASKED;
+              counter = 6;
+              break;
+            }
+          }
+        }
+        outv = sigma0;
+        m = SD_MASK_VALID;
+        counter = 0;
+      } while (0);
+      if (counter == 2) {
+        m = SD_MASK_OUTSIDE_FOOTPRINT;
+        cosv = NAN;
+      }
+      if (counter == 5 && !p.compute_lia) cosv = NAN;
+    }
+    if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
+    p.out[i] = outv;
+    if (p.compute_lia) {
+      p.cos_lia[i] = cosv;
+      p.mask[i] = m;
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
+    if (s_cnt[k]) atomicAdd(&p.counters[k], (unsigned long long)s_cnt[k]);
+}
+
+}  // namespace
+
+// ── host side ─────────────────────────────────────────────────────────────
+int tc_output_grid_host(const sd_scene *scene, const sd_tc_config *cfg, sd_geocoded_info *info) {
+  std::memset(info, 0, sizeof(*info));
+  if (!(cfg->pixel_spacing > 0.0)) return SD_ERR_TC_CONFIG;
+  const double sp = cfg->pixel_spacing;
+  double n, s, w, e;
+  if (cfg->crs == SD_CRS_WGS84) {
+    n = std::ceil(scene->max_lat_deg / sp) * sp;
+    s = std::floor(scene->min_lat_deg / sp) * sp;
+    w = std::floor(scene->min_lon_deg / sp) * sp;
+    e = std::ceil(scene->max_lon_deg / sp) * sp;
+  } else if (cfg->crs == SD_CRS_UTM_NORTH || cfg->crs == SD_CRS_UTM_SOUTH) {
+    if (cfg->utm_zone < 1 || cfg->utm_zone > 60) return SD_ERR_TC_PROJECTION;
+    Utm u = make_utm(cfg->utm_zone, cfg->crs == SD_CRS_UTM_SOUTH);
+    const double corners[4][2] = {{scene->min_lon_deg, scene->min_lat_deg},
+                                  {scene->min_lon_deg, scene->max_lat_deg},
+                                  {scene->max_lon_deg, scene->min_lat_deg},
+                                  {scene->max_lon_deg, scene->max_lat_deg}};
+    double xmin = INFINITY, xmax = -INFINITY, ymin = INFINITY, ymax = -INFINITY;
+    for (auto &cn : corners) {
+      double x, y;
+      utm_lonlat_to_xy(u, cn[0], cn[1], &x, &y);
+      if (x < xmin) xmin = x;
+      if (x > xmax) xmax = x;
+      if (y < ymin) ymin = y;
+      if (y > ymax) ymax = y;
+    }
+    n = std::ceil(ymax / sp) * sp;
+    s = std::floor(ymin / sp) * sp;
+    w = std::floor(xmin / sp) * sp;
+    e = std::ceil(xmax / sp) * sp;
+  } else {
+    return SD_ERR_TC_PROJECTION;
+  }
+  uint64_t rows = f2u64(std::round((n - s) / sp));
+  uint64_t cols = f2u64(std::round((e - w) / sp));
+  info->rows = rows;
+  info->cols = cols;
+  info->origin_lat_deg = n;
+  info->origin_lon_deg = w;
+  info->pixel_spacing = sp;
+  info->geotransform[0] = w;
+  info->geotransform[1] = sp;
+  info->geotransform[3] = n;
+  info->geotransform[5] = -sp;
+  info->total_pixel_count = rows * cols;
+  if (rows == 0 || cols == 0) return SD_ERR_TC_CONFIG;
+  return SD_OK;
+}
+
+}  // namespace sd
+
+using namespace sd;
+
+extern "C" int sd_tc_output_grid(sd_ctx *ctx, const sd_scene *scene, const sd_tc_config *cfg,
+                                 sd_geocoded_info *info) {
+  if (!scene || !cfg || !info) return SD_ERR_INVALID_ARGUMENT;
+  int rc = tc_output_grid_host(scene, cfg, info);
+  if (rc != SD_OK) set_error(ctx, rc, "output grid is empty or the CRS is invalid");
+  return rc;
+}
+
+extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene,
+                                     const sd_dem *dem, const sd_geoid *geoid,
+                                     const sd_geo_grid_point *grid, uint64_t n_grid,
+                                     const sd_tc_config *cfg, float *out_data, float *out_cos_lia,
+                                     uint8_t *out_mask, sd_geocoded_info *info) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!image || !scene || !dem || !geoid || !cfg || !info || !out_data)
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null argument");
+  if (cfg->compute_lia && (!out_cos_lia || !out_mask))
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "compute_lia needs cos_lia and mask buffers");
+  SD_CUDA(ctx, cudaSetDevice(ctx->device));
+  // argument checks in the reference's order (terrain_correction.rs:1262-1283)
+  if (n_grid == 0) return set_error(ctx, SD_ERR_TC_NO_GRID_POINTS, "no geolocation grid points provided");
+  if (!(cfg->pixel_spacing > 0.0)) return set_error(ctx, SD_ERR_TC_CONFIG, "pixel spacing must be positive");
+  if (scene->n_sub_swaths <= 0)
+    return set_error(ctx, SD_ERR_TC_NO_SUBSWATHS, "scene has no subswaths — cannot derive radar geometry");
+  const double ati = scene->azimuth_time_interval_s;
+  if (!std::isfinite(ati) || ati <= 0.0)
+    return set_error(ctx, SD_ERR_TC_CONFIG, "invalid azimuth_time_interval_s in subswath metadata: %g", ati);
+  // build_azimuth_time_lut (1080-1104): stable sort by latitude, keep first of near-duplicates
+  std::vector<std::pair<double, int64_t>> lut;
+  for (uint64_t k = 0; k < n_grid; ++k) lut.push_back({grid[k].latitude_deg, grid[k].azimuth_time_us});
+  std::stable_sort(lut.begin(), lut.end(), [](auto &a, auto &b) { return a.first < b.first; });
+  std::vector<double> lut_lat;
+  std::vector<int64_t> lut_t;
+  for (auto &pt : lut) {
+    if (!lut_lat.empty() && std::fabs(pt.first - lut_lat.back()) < 1e-6) continue;
+    lut_lat.push_back(pt.first);
+    lut_t.push_back(pt.second);
+  }
+  if (lut_lat.empty()) return set_error(ctx, SD_ERR_TC_NO_GRID_POINTS, "no geolocation grid points provided");
+  SD_TRY(sd_tc_output_grid(ctx, scene, cfg, info));
+  if (cfg->projector_anchors <= 0)
+    return set_error(ctx, SD_ERR_TC_CONFIG, "SARDINE_TC_PROJECTOR_ANCHORS must be >= 1 (default 256)");
+  if (dem->width < 2 || dem->height < 2 || !(dem->pixel_size > 0.0))
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "DEM grid must be at least 2x2 with positive spacing");
+  if (image->lines == 0 || image->samples == 0)
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "radar image is empty");
+
+  TcDev p{};
+  p.rows = info->rows;
+  p.cols = info->cols;
+  p.lat_north = info->origin_lat_deg;
+  p.lon_west = info->origin_lon_deg;
+  p.sp = cfg->pixel_spacing;
+  p.utm = cfg->crs != SD_CRS_WGS84;
+  if (p.utm) p.proj = make_utm(cfg->utm_zone, cfg->crs == SD_CRS_UTM_SOUTH);
+  p.step_deg = p.utm ? p.sp / 111320.0 : p.sp;  // cardinal_neighbour_step_deg (452-465)
+  p.lines = image->lines;
+  p.samples = image->samples;
+  p.az_start = image->azimuth_start_time_us;
+  p.ati = ati;
+  p.near_range = image->near_slant_range_time_s * SPEED_OF_LIGHT / 2.0;
+  p.rps = image->range_pixel_spacing_m;
+  p.max_iter = cfg->max_newton_iterations < 0 ? 0 : cfg->max_newton_iterations;
+  p.tol = cfg->newton_tolerance_s;
+  p.flatten = cfg->flatten != 0;
+  p.compute_lia = cfg->compute_lia != 0;
+  p.need_geom = p.flatten || p.compute_lia;
+  p.resampling = cfg->resampling;
+  p.nesz_mask = std::isfinite(cfg->noise_floor_margin_db) && image->nesz != nullptr;
+  p.nesz_factor = p.nesz_mask ? std::pow(10.0f, cfg->noise_floor_margin_db / 10.0f) : 0.0f;
+  const uint64_t npx = p.rows * p.cols;
+  cudaStream_t st = ctx->stream;
+
+  // ── inputs ──
+  const void *d_img, *d_nesz = nullptr, *d_dem, *d_geoid = nullptr, *d_svs;
+  SD_TRY(stage_in(ctx, "tc.img", image->data, image->lines * image->samples * sizeof(float), &d_img));
+  if (p.nesz_mask)
+    SD_TRY(stage_in(ctx, "tc.nesz", image->nesz, image->lines * image->samples * sizeof(float), &d_nesz));
+  SD_TRY(stage_in(ctx, "tc.dem", dem->data, dem->width * dem->height * sizeof(float), &d_dem));
+  if (geoid->kind == SD_GEOID_GRID) {
+    if (!geoid->undulations_m) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "geoid grid is null");
+    SD_TRY(stage_in(ctx, "tc.geoid", geoid->undulations_m, 73 * 144 * sizeof(float), &d_geoid));
+  }
+  const uint64_t nsv = scene->n_state_vectors;
+  SD_TRY(stage_in(ctx, "tc.svs", scene->state_vectors, std::max<uint64_t>(nsv, 1) * sizeof(sd_state_vector), &d_svs));
+  double *d_lut_lat;
+  int64_t *d_lut_t;
+  SD_TRY(scratch_t(ctx, "tc.lut_lat", lut_lat.size(), &d_lut_lat));
+  SD_TRY(scratch_t(ctx, "tc.lut_t", lut_t.size(), &d_lut_t));
+  SD_CUDA(ctx, cudaMemcpyAsync(d_lut_lat, lut_lat.data(), lut_lat.size() * 8, cudaMemcpyHostToDevice, st));
+  SD_CUDA(ctx, cudaMemcpyAsync(d_lut_t, lut_t.data(), lut_t.size() * 8, cudaMemcpyHostToDevice, st));
+  p.img = (const float *)d_img;
+  p.nesz = (const float *)d_nesz;
+  p.geoid = (const float *)d_geoid;
+  p.lut_lat = d_lut_lat;
+  p.lut_t = d_lut_t;
+  p.lut_n = (int)lut_lat.size();
+  p.dem.data = (const float *)d_dem;
+  p.dem.width = dem->width;
+  p.dem.height = dem->height;
+  p.dem.origin_y = dem->origin_y;
+  p.dem.origin_x = dem->origin_x;
+  p.dem.pixel_size = dem->pixel_size;
+  p.dem.kind = dem->kind;
+  if (dem->kind == SD_DEM_PROJECTED_UTM) {
+    if (dem->utm_zone < 1 || dem->utm_zone > 60)
+      return set_error(ctx, SD_ERR_TC_DEM, "projected DEM needs a UTM zone in 1..60");
+    p.dem.utm = make_utm(dem->utm_zone, dem->utm_south != 0);
+  }
+  p.orb.svs = (const sd_state_vector *)d_svs;
+  p.orb.n = nsv;
+  p.orb.tab = nullptr;
+  p.orb.tab_t0 = 0;
+  p.orb.tab_n = 0;
+
+  // ── per-row set-up ──
+  int64_t *d_row_guess, *d_knots;
+  double *d_row_flat, *d_ax = nullptr, *d_alon = nullptr, *d_alat = nullptr;
+  unsigned long long *d_trange;
+  SD_TRY(scratch_t(ctx, "tc.row_guess", p.rows, &d_row_guess));
+  SD_TRY(scratch_t(ctx, "tc.row_flat", p.rows, &d_row_flat));
+  SD_TRY(scratch_t(ctx, "tc.knots", p.rows * KNOTS, &d_knots));
+  SD_TRY(scratch_t(ctx, "tc.trange", 2, &d_trange));
+  p.row_guess = d_row_guess;
+  p.row_flat = d_row_flat;
+  p.knot_t = d_knots;
+  p.trange = d_trange;
+  unsigned long long tr_init[2] = {~0ull, 0ull};
+  SD_CUDA(ctx, cudaMemcpyAsync(d_trange, tr_init, sizeof tr_init, cudaMemcpyHostToDevice, st));
+  std::vector<double> ax;
+  if (p.utm) {
+    // project_row anchors (output_crs.rs:383-396); x positions are row-independent
+    const uint64_t n_anchors = std::min<uint64_t>((uint64_t)cfg->projector_anchors, p.cols);
+    const double x_start = p.lon_west + 0.5 * p.sp;
+    const double x_end = x_start + ((double)p.cols - 1.0) * p.sp;
+    const double anchor_dx = (x_end - x_start) / (double)n_anchors;
+    for (uint64_t a = 0; a <= n_anchors; ++a) ax.push_back(x_start + (double)a * anchor_dx);
+    p.n_anchors = (int)n_anchors;
+    p.n_pts = (int)n_anchors + 1;
+    SD_TRY(scratch_t(ctx, "tc.ax", ax.size(), &d_ax));
+    SD_TRY(scratch_t(ctx, "tc.alon", p.rows * p.n_pts, &d_alon));
+    SD_TRY(scratch_t(ctx, "tc.alat", p.rows * p.n_pts, &d_alat));
+    SD_CUDA(ctx, cudaMemcpyAsync(d_ax, ax.data(), ax.size() * 8, cudaMemcpyHostToDevice, st));
+    p.ax = d_ax;
+    p.alon = d_alon;
+    p.alat = d_alat;
+    uint64_t na = p.rows * p.n_pts;
+    k_row_anchors<<<grid_for(na, 128), 128, 0, st>>>(p);
+    SD_LAUNCHED(ctx);
+  }
+  k_row_setup<<<grid_for(p.rows, 128), 128, 0, st>>>(p);
+  SD_LAUNCHED(ctx);
+  k_row_model<<<grid_for(p.rows * KNOTS, 128), 128, 0, st>>>(p);
+  SD_LAUNCHED(ctx);
+  unsigned long long tr[2];
+  SD_CUDA(ctx, cudaMemcpyAsync(tr, d_trange, sizeof tr, cudaMemcpyDeviceToHost, st));
+  SD_TRY(sync(ctx));
+
+  // ── orbit table over the model's time span (+/- 0.5 s), inside the SV window ──
+  if (nsv >= 8 && tr[0] <= tr[1]) {
+    int64_t tmin = (int64_t)(tr[0] ^ 0x8000000000000000ull);
+    int64_t tmax = (int64_t)(tr[1] ^ 0x8000000000000000ull);
+    int64_t t0 = std::max(scene->state_vectors[0].time_us, tmin - 500000);
+    int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us, tmax + 500000);
+    const int64_t max_entries = 96ll * 1000 * 1000;  // 7.7 GB cap
+    if (t1 - t0 + 1 > max_entries) {
+      int64_t mid = (tmin / 2 + tmax / 2);
+      t0 = std::max(t0, mid - max_entries / 2);
+      t1 = std::min(t1, t0 + max_entries - 1);
+    }
+    if (t1 >= t0) {
+      double2 *d_tab;
+      SD_TRY(scratch_t(ctx, "tc.orbit_table", (size_t)(t1 - t0 + 1) * 5, &d_tab));
+      k_orbit_table<<<grid_for((size_t)(t1 - t0 + 1), 128), 128, 0, st>>>(
+          (const sd_state_vector *)d_svs, nsv, t0, t1 - t0 + 1, d_tab);
+      SD_LAUNCHED(ctx);
+      p.orb.tab = d_tab;
+      p.orb.tab_t0 = t0;
+      p.orb.tab_n = t1 - t0 + 1;
+    }
+  }
+
+  // ── per-pixel scratch and outputs ──
+  SD_TRY(scratch_t(ctx, "tc.px", npx, &p.px));
+  SD_TRY(scratch_t(ctx, "tc.py", npx, &p.py));
+  SD_TRY(scratch_t(ctx, "tc.pz", npx, &p.pz));
+  SD_TRY(scratch_t(ctx, "tc.rec", npx, &p.rec));
+  SD_TRY(scratch_t(ctx, "tc.codes", npx, &p.codes));
+  SD_TRY(scratch_t(ctx, "tc.tsol", npx, &p.tsol));
+  SD_TRY(scratch_t(ctx, "tc.stit", npx, &p.stit));
+  void *d_out, *d_cos = nullptr, *d_mask = nullptr;
+  SD_TRY(stage_out(ctx, "tc.out", out_data, npx * sizeof(float), &d_out));
+  if (p.compute_lia) {
+    SD_TRY(stage_out(ctx, "tc.cos", out_cos_lia, npx * sizeof(float), &d_cos));
+    SD_TRY(stage_out(ctx, "tc.mask", out_mask, npx, &d_mask));
+  }
+  p.out = (float *)d_out;
+  p.cos_lia = (float *)d_cos;
+  p.mask = (uint8_t *)d_mask;
+  p.flags = ctx->d_flags;
+  p.counters = ctx->d_counters;
+  SD_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, 64 * sizeof(int), st));
+  SD_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 64 * sizeof(unsigned long long), st));
+
+  // The candidate-set scheme needs tol <= 1 us (then at most three
+  // consecutive microseconds can satisfy |delta| < tol).  Larger tolerances
+  // run every solve in the row walk.
+  const int fast = (p.tol <= 1e-6) ? 1 : 0;
+  const unsigned B = 256;
+  k_geo<<<grid_for(npx, B), B, 0, st>>>(p, fast);
+  SD_LAUNCHED(ctx);
+  if (fast) {
+    k_cand<<<grid_for(npx, B), B, 0, st>>>(p);
+    SD_LAUNCHED(ctx);
+  } else {
+    SD_CUDA(ctx, cudaMemsetAsync(p.codes, 0xFF, npx * sizeof(uint32_t), st));
+  }
+  k_scan<<<grid_for(p.rows, 128), 128, 0, st>>>(p);
+  SD_LAUNCHED(ctx);
+  if (p.resampling == SD_RESAMPLE_BICUBIC) k_out<SD_RESAMPLE_BICUBIC><<<grid_for(npx, B), B, 0, st>>>(p);
+  else if (p.resampling == SD_RESAMPLE_LANCZOS3) k_out<SD_RESAMPLE_LANCZOS3><<<grid_for(npx, B), B, 0, st>>>(p);
+  else k_out<SD_RESAMPLE_BILINEAR><<<grid_for(npx, B), B, 0, st>>>(p);
+  SD_LAUNCHED(ctx);
+
+  int flags[4];
+  unsigned long long cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
+  SD_CUDA(ctx, cudaMemcpyAsync(flags, ctx->d_flags, sizeof flags, cudaMemcpyDeviceToHost, st));
+  SD_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost, st));
+  SD_TRY(sync(ctx));
+  if (flags[0]) {
+    return set_error(ctx, SD_ERR_TC_ORBIT,
+                     "orbit interpolation failed: interpolation time outside orbit window; "
+                     "refusing to extrapolate");
+  }
+  SD_TRY(finish_out(ctx, out_data, d_out, npx * sizeof(float)));
+  if (p.compute_lia) {
+    SD_TRY(finish_out(ctx, out_cos_lia, d_cos, npx * sizeof(float)));
+    SD_TRY(finish_out(ctx, out_mask, d_mask, npx));
+  }
+  info->valid_pixel_count = cnt[0];
+  info->dem_missing_count = cnt[1];
+  info->outside_footprint_count = cnt[2];
+  info->non_converged_count = cnt[3];
+  info->degenerate_geometry_count = cnt[4];
+  info->flat_masked_count = cnt[5];
+  info->noise_masked_count = cnt[6];
+  for (int k = 0; k < SD_NEWTON_ITER_HIST_SIZE; ++k) info->newton_iter_histogram[k] = cnt[kCounters + k];
+  SD_TRY(sync(ctx));
+  return SD_OK;
+}

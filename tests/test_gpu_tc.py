@@ -1,0 +1,157 @@
+"""GPU terrain correction vs the CPU oracle on identical seeded scenes.
+
+Bar (see tests/README in DESIGN): masks, counters and the Newton histogram
+bit-exact; sigma0/gamma0 and cos(LIA) within 1e-4 relative.  A pixel may
+exceed 1e-4 only where the two sides' libm sin/cos differ by an ulp right at
+a microsecond boundary of the Newton step; such flips move the sample by
+4.9e-4 azimuth line (inside the 1e-3 px geolocation bar) and are capped at
+1e-5 of the valid pixels.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import sardine_b200 as sd
+from sardine_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-4
+FLIP_CAP = 1e-5
+
+
+def _rel(a, b):
+    a = a.astype(np.float64)
+    b = b.astype(np.float64)
+    both = np.isfinite(a) & np.isfinite(b)
+    d = np.zeros_like(a)
+    d[both] = np.abs(a[both] - b[both]) / np.maximum(np.abs(b[both]), 1e-30)
+    return d, both
+
+
+def assert_tc_parity(gpu: sd.GeocodedImage, ref: sd.GeocodedImage, compute_lia=True):
+    assert (gpu.rows, gpu.cols) == (ref.rows, ref.cols)
+    for k in ("valid_pixel_count", "dem_missing_count", "outside_footprint_count",
+              "non_converged_count", "degenerate_geometry_count", "flat_masked_count",
+              "noise_masked_count", "total_pixel_count"):
+        assert getattr(gpu, k) == getattr(ref, k), k
+    assert gpu.newton_iter_histogram == ref.newton_iter_histogram
+    assert tuple(gpu.geotransform) == tuple(ref.geotransform)
+    g = np.asarray(gpu.data)
+    r = np.asarray(ref.data)
+    assert np.array_equal(np.isnan(g), np.isnan(r)), "NaN pattern differs"
+    d, both = _rel(g, r)
+    n_bad = int((d > REL_TOL).sum())
+    assert n_bad <= max(1, FLIP_CAP * both.sum()), f"{n_bad} pixels beyond {REL_TOL}, max {d.max()}"
+    if compute_lia:
+        assert np.array_equal(np.asarray(gpu.mask), np.asarray(ref.mask)), "mask differs"
+        gc, rc_ = np.asarray(gpu.cos_lia), np.asarray(ref.cos_lia)
+        assert np.array_equal(np.isnan(gc), np.isnan(rc_))
+        d2, b2 = _rel(gc, rc_)
+        assert int((d2 > REL_TOL).sum()) <= max(1, FLIP_CAP * b2.sum())
+
+
+@pytest.mark.parametrize("resampling,flatten", [
+    (sd.ResamplingKernel.Bilinear, False),
+    (sd.ResamplingKernel.Bicubic, True),
+    (sd.ResamplingKernel.Lanczos3, True),
+])
+def test_config1_shape_parity(ctx, resampling, flatten):
+    sc = synth.config1_scene(seed=11, n_lines=1024, n_samples=2048, dem_n=256,
+                             resampling=resampling, flatten=flatten)
+    ref = oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert ref.valid_pixel_count > 0.5 * ref.total_pixel_count
+    assert_tc_parity(gpu, ref)
+
+
+def test_config1_partial_footprint_and_voids(ctx):
+    """DEM larger than the radar footprint (outside-footprint pixels) with
+    NaN voids (DEM_MISSING and DEM_NEIGHBOUR_MISSING)."""
+    sc = synth.config1_scene(seed=12, n_lines=256, n_samples=512, dem_n=320, flatten=True)
+    dem = np.array(sc.dem.data)
+    dem[40:60, 100:130] = np.nan
+    dem[200, :] = np.nan
+    sc.dem.data = dem
+    ref = oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert ref.outside_footprint_count > 0 and ref.dem_missing_count > 0
+    assert_tc_parity(gpu, ref)
+
+
+def test_nesz_masking_and_nan_seams(ctx):
+    sc = synth.config1_scene(seed=13, n_lines=512, n_samples=1024, dem_n=200)
+    rng = np.random.default_rng(5)
+    img = np.array(sc.merged.data)
+    img[:, 300:310] = np.nan  # merge-seam gap
+    nesz = rng.uniform(0.0, 0.06, size=img.shape).astype(np.float32)
+    sc.merged.data = img
+    sc.merged.nesz = nesz
+    sc.config.noise_floor_margin_db = 0.0
+    ref = oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert ref.noise_masked_count > 0
+    assert_tc_parity(gpu, ref)
+
+
+def test_small_max_iter_non_converged(ctx):
+    sc = synth.config1_scene(seed=14, n_lines=256, n_samples=512, dem_n=96)
+    sc.config.max_newton_iterations = 1
+    ref = oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert ref.non_converged_count > 0
+    assert_tc_parity(gpu, ref)
+
+
+def test_loose_tolerance_generic_path(ctx):
+    sc = synth.config1_scene(seed=15, n_lines=256, n_samples=512, dem_n=96)
+    sc.config.newton_tolerance_s = 2e-4
+    ref = oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert_tc_parity(gpu, ref)
+
+
+def test_orbit_window_error(ctx):
+    sc = synth.config1_scene(seed=16, n_lines=256, n_samples=512, dem_n=64)
+    o = sc.scene.orbit
+    sc.scene.orbit = sd.OrbitData(o.times_us[:9].copy(), o.positions_m[:9].copy(),
+                                  o.velocities_m_s[:9].copy())
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    with pytest.raises(sd.TerrainCorrectionError) as g:
+        sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert g.value.kind == "Orbit" and e.value.code == g.value.code
+
+
+def test_config2_shape_utm_parity(ctx):
+    """UTM output grid, projected DEM, bicubic, gamma0 flattening + LIA."""
+    sc = synth.config2_scene(seed=21, n_bursts=3, lines_per_burst=400, tiff_width=1500,
+                             burst_step=300, swath_overlap=150, out_rows=None, out_cols=None,
+                             lut_lines_step=150)
+    swaths = sc.swaths
+    merged_g = sd.calibrate_deburst_merge(swaths, ctx=ctx)
+    # oracle chain: deburst -> calibrate -> merge
+    inputs = []
+    for s in swaths:
+        deb = oracle.deburst_subswath(s.slc, s.sw, s.bursts)
+        sig = oracle.apply_calibration(deb, s.cal, s.noise, s.bursts[0].first_line)
+        inputs.append(sd.SwathInput(sig, s.sw, s.bursts[0].azimuth_time_us))
+    merged_o, _ = oracle.merge_subswaths(inputs)
+    assert np.array_equal(np.asarray(merged_g.data), merged_o.data, equal_nan=True)
+    assert np.array_equal(np.asarray(merged_g.nesz), merged_o.nesz, equal_nan=True)
+    ref = oracle.terrain_correction(merged_o, sc.scene, sc.dem, sc.grids, sc.config)
+    gpu = sd.terrain_correction(merged_g, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert ref.valid_pixel_count > 0
+    assert_tc_parity(gpu, ref)
+
+
+def test_device_resident_inputs(ctx):
+    import torch
+    sc = synth.config1_scene(seed=17, n_lines=512, n_samples=1024, dem_n=128)
+    ref = oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    sc.merged.data = torch.from_numpy(np.asarray(sc.merged.data)).cuda()
+    sc.dem.data = torch.from_numpy(np.asarray(sc.dem.data)).cuda()
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert gpu.data.is_cuda
+    gpu.data, gpu.cos_lia, gpu.mask = gpu.data.cpu().numpy(), gpu.cos_lia.cpu().numpy(), gpu.mask.cpu().numpy()
+    assert_tc_parity(gpu, ref)
