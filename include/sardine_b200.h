@@ -279,6 +279,14 @@ const char *sd_last_error(const sd_ctx *ctx);
 uint64_t sd_kernel_launches(const sd_ctx *ctx);
 /* The context's CUDA stream (cudaStream_t), for callers that interleave work. */
 void *sd_ctx_stream(sd_ctx *ctx);
+/* Per-kernel timing: when on, every kernel launch is bracketed by CUDA events
+ * on the context's stream and the durations accumulate per kernel name.
+ * Turning it on clears the accumulators. */
+int sd_ctx_set_timing(sd_ctx *ctx, int on);
+/* Accumulated kernel times: names as a newline-separated list (same order as
+ * ms/counts); *n_out = number of distinct kernels. */
+int sd_ctx_kernel_times(sd_ctx *ctx, char *names, uint64_t names_len, double *ms,
+                        uint64_t *counts, uint64_t max_entries, uint64_t *n_out);
 
 /* ── Speckle ──────────────────────────────────────────────────────────────
  * Replaces SpeckleKernel::apply / apply_speckle_filter (speckle.rs:131-180,

@@ -24,6 +24,8 @@ _SIGS = {
     "sd_last_error": (C.c_char_p, [P]),
     "sd_kernel_launches": (C.c_uint64, [P]),
     "sd_ctx_stream": (P, [P]),
+    "sd_ctx_set_timing": (C.c_int, [P, C.c_int]),
+    "sd_ctx_kernel_times": (C.c_int, [P, P, C.c_uint64, P, P, C.c_uint64, P]),
     "sd_speckle": (C.c_int, [P, P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int32, C.c_uint64,
                              C.c_float, C.c_float, P]),
     "sd_compute_overlap_lines": (C.c_int, [P, P, P, C.c_double, C.c_uint64, P]),
@@ -94,6 +96,24 @@ class Context:
     @property
     def stream_ptr(self) -> int:
         return int(lib().sd_ctx_stream(self.handle) or 0)
+
+    def set_timing(self, on: bool) -> None:
+        """Bracket every kernel launch with CUDA events on the context's stream."""
+        lib().sd_ctx_set_timing(self.handle, int(on))
+
+    def kernel_times(self) -> dict:
+        """{kernel name: (total ms, launches)} accumulated since set_timing(True)."""
+        n = C.c_uint64()
+        lib().sd_ctx_kernel_times(self.handle, None, 0, None, None, 0, C.byref(n))
+        m = int(n.value)
+        if m == 0:
+            return {}
+        names = C.create_string_buffer(64 * m + 64)
+        ms = (C.c_double * m)()
+        cnt = (C.c_uint64 * m)()
+        lib().sd_ctx_kernel_times(self.handle, names, len(names), ms, cnt, m, C.byref(n))
+        keys = names.value.decode().split("\n")[:m]
+        return {k: (ms[i], int(cnt[i])) for i, k in enumerate(keys)}
 
     def last_error(self) -> str:
         s = lib().sd_last_error(self.handle)

@@ -374,6 +374,7 @@ int cal_device(sd_ctx *ctx, const std::string &tag, const CalPlan &P, uint64_t c
     uint64_t nv = L.lines.size();
     SD_TRY(scratch_t(ctx, (t + ".tab").c_str(), nv * std::max<uint64_t>(samples, 1), &tab));
     if (samples > 0) {
+      SD_TIMED_BEGIN(ctx, "k_lut_table");
       k_lut_table<<<grid_for(nv * samples, 256), 256, 0, ctx->stream>>>(d, nv, samples, col_offset, tab);
       SD_LAUNCHED(ctx);
     }
@@ -500,6 +501,7 @@ extern "C" int sd_deburst_subswath(sd_ctx *ctx, const int16_t *slc, uint64_t tif
   SD_TRY(stage_out(ctx, "db.out", out, p.lines * p.samples * 4, &d_out));
   SD_TRY(upload(ctx, "db.map", p.line_map, &d_map));
   dim3 grid(grid_for(p.samples, 256), (unsigned)p.lines);
+  SD_TIMED_BEGIN(ctx, "k_deburst_copy");
   k_deburst_copy<<<grid, 256, 0, ctx->stream>>>((const uint32_t *)d_raw, tiff_width, d_map, p.offset, p.lines,
                                                  p.samples, (uint32_t *)d_out);
   SD_LAUNCHED(ctx);
@@ -536,6 +538,7 @@ extern "C" int sd_apply_calibration(sd_ctx *ctx, const int16_t *iq, uint64_t lin
   s.line_map = d_map;
   s.col0 = 0;
   dim3 grid(grid_for(samples, 256), (unsigned)lines);
+  SD_TIMED_BEGIN(ctx, "k_calibrate");
   k_calibrate<<<grid, 256, 0, ctx->stream>>>(s, lines, samples, (float *)d_out, (float *)d_nesz);
   SD_LAUNCHED(ctx);
   SD_TRY(finish_out(ctx, out, d_out, lines * samples * 4));
@@ -580,6 +583,7 @@ extern "C" int sd_merge_subswaths(sd_ctx *ctx, int32_t n, const float *const *si
   SD_TRY(stage_out(ctx, "mg.nesz", out_nesz, L * Cc * 4, &d_nesz));
   if (L > 0 && Cc > 0) {
     dim3 grid(grid_for(Cc, 256), (unsigned)L);
+    SD_TIMED_BEGIN(ctx, "k_merge");
     k_merge<<<grid, 256, 0, ctx->stream>>>(m, L, Cc, (float *)d_out, (float *)d_nesz);
     SD_LAUNCHED(ctx);
   }
@@ -656,6 +660,7 @@ extern "C" int sd_calibrate_deburst_merge(sd_ctx *ctx, int32_t n, const sd_swath
   SD_TRY(stage_out(ctx, "fu.nesz", out_nesz, L * Cc * 4, &d_nesz));
   if (L > 0 && Cc > 0) {
     dim3 grid(grid_for(Cc, 256), (unsigned)L);
+    SD_TIMED_BEGIN(ctx, "k_fused");
     k_fused<<<grid, 256, 0, ctx->stream>>>(m, L, Cc, (float *)d_out, (float *)d_nesz);
     SD_LAUNCHED(ctx);
   }

@@ -27,9 +27,11 @@ int measure(sd_ctx *ctx, int iters, double *tflops) {
   T *d;
   SD_TRY(scratch_t(ctx, "diag.out", 16, &d));
   const int block = 256, grid = sms * 8;
+  SD_TIMED_BEGIN(ctx, "k_fma_chain<T>");
   k_fma_chain<T><<<grid, block, 0, ctx->stream>>>(d, 64, (T)0.999999, (T)1e-7);  // warm-up
   SD_LAUNCHED(ctx);
   SD_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+  SD_TIMED_BEGIN(ctx, "k_fma_chain<T>");
   k_fma_chain<T><<<grid, block, 0, ctx->stream>>>(d, iters, (T)0.999999, (T)1e-7);
   SD_LAUNCHED(ctx);
   SD_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));

@@ -84,7 +84,42 @@ int finish_out(sd_ctx *ctx, void *user, const void *dev, size_t bytes) {
 
 int sync(sd_ctx *ctx) {
   SD_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  timing_collect(ctx);
   return SD_OK;
+}
+
+static thread_local const char *t_pending_name = nullptr;
+
+void timing_begin(sd_ctx *ctx, const char *name) {
+  if (!ctx->timing) return;
+  sd_ctx::KTime k;
+  k.name = name;
+  cudaEventCreate(&k.a);
+  cudaEventCreate(&k.b);
+  cudaEventRecord(k.a, ctx->stream);
+  ctx->pending.push_back(k);
+  t_pending_name = name;
+}
+
+void timing_end(sd_ctx *ctx) {
+  if (!ctx->timing || !t_pending_name || ctx->pending.empty()) return;
+  cudaEventRecord(ctx->pending.back().b, ctx->stream);
+  t_pending_name = nullptr;
+}
+
+void timing_collect(sd_ctx *ctx) {
+  for (auto &k : ctx->pending) {
+    float ms = 0.0f;
+    if (cudaEventSynchronize(k.b) == cudaSuccess && cudaEventElapsedTime(&ms, k.a, k.b) == cudaSuccess) {
+      auto &acc = ctx->ktimes[k.name];
+      acc.first += ms;
+      acc.second += 1;
+    }
+    cudaEventDestroy(k.a);
+    cudaEventDestroy(k.b);
+  }
+  cudaGetLastError();
+  ctx->pending.clear();
 }
 
 }  // namespace sd
@@ -138,5 +173,39 @@ const char *sd_last_error(const sd_ctx *ctx) { return ctx ? ctx->last_error.c_st
 uint64_t sd_kernel_launches(const sd_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
 void *sd_ctx_stream(sd_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int sd_ctx_set_timing(sd_ctx *ctx, int on) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  cudaStreamSynchronize(ctx->stream);
+  sd::timing_collect(ctx);
+  ctx->timing = on != 0;
+  if (on) ctx->ktimes.clear();
+  return SD_OK;
+}
+
+int sd_ctx_kernel_times(sd_ctx *ctx, char *names, uint64_t names_len, double *ms, uint64_t *counts,
+                        uint64_t max_entries, uint64_t *n_out) {
+  if (!ctx || !n_out) return SD_ERR_INVALID_ARGUMENT;
+  cudaStreamSynchronize(ctx->stream);
+  sd::timing_collect(ctx);
+  uint64_t i = 0;
+  std::string all;
+  for (auto &kv : ctx->ktimes) {
+    if (i < max_entries) {
+      if (ms) ms[i] = kv.second.first;
+      if (counts) counts[i] = kv.second.second;
+      all += kv.first;
+      all += '\n';
+    }
+    ++i;
+  }
+  *n_out = i;
+  if (names && names_len > 0) {
+    size_t n = std::min<size_t>(all.size(), names_len - 1);
+    memcpy(names, all.data(), n);
+    names[n] = 0;
+  }
+  return SD_OK;
+}
 
 }  // extern "C"

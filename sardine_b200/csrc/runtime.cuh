@@ -26,6 +26,14 @@ struct sd_ctx {
   std::unordered_map<std::string, Buf> scratch;  // grow-only named device buffers
   std::vector<void *> pinned;                    // grow-only pinned staging buffers
   int *d_flags = nullptr;                        // device-side error words
+  // optional per-kernel timing: events recorded around every launch
+  bool timing = false;
+  struct KTime {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<KTime> pending;
+  std::unordered_map<std::string, std::pair<double, uint64_t>> ktimes;  // ms, launches
   unsigned long long *d_counters = nullptr;      // device-side counters (64 slots)
 };
 
@@ -43,9 +51,13 @@ int set_error(sd_ctx *ctx, int code, const char *fmt, ...);
                              __FILE__, __LINE__);                                        \
   } while (0)
 
+// Bracket a launch with SD_TIMED_BEGIN(ctx, "name") ... SD_LAUNCHED(ctx).
+#define SD_TIMED_BEGIN(ctx, nm) ::sd::timing_begin((ctx), (nm))
+
 #define SD_LAUNCHED(ctx)                                                                  \
   do {                                                                                   \
     (ctx)->launches++;                                                                   \
+    ::sd::timing_end(ctx);                                                               \
     cudaError_t e__ = cudaGetLastError();                                                \
     if (e__ != cudaSuccess)                                                              \
       return ::sd::set_error((ctx), SD_ERR_CUDA, "kernel launch failed: %s (%s:%d)",     \
@@ -79,6 +91,9 @@ int stage_in(sd_ctx *ctx, const char *name, const void *p, size_t bytes, const v
 int stage_out(sd_ctx *ctx, const char *name, void *p, size_t bytes, void **dev);
 int finish_out(sd_ctx *ctx, void *user, const void *dev, size_t bytes);
 int sync(sd_ctx *ctx);
+void timing_begin(sd_ctx *ctx, const char *name);
+void timing_end(sd_ctx *ctx);
+void timing_collect(sd_ctx *ctx);
 
 inline unsigned grid_for(size_t n, unsigned block) {
   size_t g = (n + block - 1) / block;

@@ -234,6 +234,7 @@ int speckle_launch(sd_ctx *ctx, const float *d_in, float *d_out, uint64_t cols, 
   case K:                                                                                    \
     if (smem > 48 * 1024)                                                                    \
       SD_CUDA(ctx, cudaFuncSetAttribute(k_speckle<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    SD_TIMED_BEGIN(ctx, "k_speckle_" #K);                                               \
     k_speckle<K><<<grid, block, smem, st>>>(p);                                             \
     break;
     SD_LAUNCH_SPECKLE(SD_SPECKLE_BOXCAR)

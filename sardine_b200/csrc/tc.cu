@@ -806,11 +806,14 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
     p.alon = d_alon;
     p.alat = d_alat;
     uint64_t na = p.rows * p.n_pts;
+    SD_TIMED_BEGIN(ctx, "k_row_anchors");
     k_row_anchors<<<grid_for(na, 128), 128, 0, st>>>(p);
     SD_LAUNCHED(ctx);
   }
+  SD_TIMED_BEGIN(ctx, "k_row_setup");
   k_row_setup<<<grid_for(p.rows, 128), 128, 0, st>>>(p);
   SD_LAUNCHED(ctx);
+  SD_TIMED_BEGIN(ctx, "k_row_model");
   k_row_model<<<grid_for(p.rows * KNOTS, 128), 128, 0, st>>>(p);
   SD_LAUNCHED(ctx);
   unsigned long long tr[2];
@@ -832,6 +835,7 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
     if (t1 >= t0) {
       double2 *d_tab;
       SD_TRY(scratch_t(ctx, "tc.orbit_table", (size_t)(t1 - t0 + 1) * 5, &d_tab));
+      SD_TIMED_BEGIN(ctx, "k_orbit_table");
       k_orbit_table<<<grid_for((size_t)(t1 - t0 + 1), 128), 128, 0, st>>>(
           (const sd_state_vector *)d_svs, nsv, t0, t1 - t0 + 1, d_tab);
       SD_LAUNCHED(ctx);
@@ -868,19 +872,31 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
   // run every solve in the row walk.
   const int fast = (p.tol <= 1e-6) ? 1 : 0;
   const unsigned B = 256;
+  SD_TIMED_BEGIN(ctx, "k_geo");
   k_geo<<<grid_for(npx, B), B, 0, st>>>(p, fast);
   SD_LAUNCHED(ctx);
   if (fast) {
+    SD_TIMED_BEGIN(ctx, "k_cand");
     k_cand<<<grid_for(npx, B), B, 0, st>>>(p);
     SD_LAUNCHED(ctx);
   } else {
     SD_CUDA(ctx, cudaMemsetAsync(p.codes, 0xFF, npx * sizeof(uint32_t), st));
   }
+  SD_TIMED_BEGIN(ctx, "k_scan");
   k_scan<<<grid_for(p.rows, 128), 128, 0, st>>>(p);
   SD_LAUNCHED(ctx);
-  if (p.resampling == SD_RESAMPLE_BICUBIC) k_out<SD_RESAMPLE_BICUBIC><<<grid_for(npx, B), B, 0, st>>>(p);
-  else if (p.resampling == SD_RESAMPLE_LANCZOS3) k_out<SD_RESAMPLE_LANCZOS3><<<grid_for(npx, B), B, 0, st>>>(p);
-  else k_out<SD_RESAMPLE_BILINEAR><<<grid_for(npx, B), B, 0, st>>>(p);
+  if (p.resampling == SD_RESAMPLE_BICUBIC) {
+    SD_TIMED_BEGIN(ctx, "k_out<BICUBIC>");
+    k_out<SD_RESAMPLE_BICUBIC><<<grid_for(npx, B), B, 0, st>>>(p);
+  }
+  else if (p.resampling == SD_RESAMPLE_LANCZOS3) {
+    SD_TIMED_BEGIN(ctx, "k_out<LANCZOS3>");
+    k_out<SD_RESAMPLE_LANCZOS3><<<grid_for(npx, B), B, 0, st>>>(p);
+  }
+  else {
+    SD_TIMED_BEGIN(ctx, "k_out<BILINEAR>");
+    k_out<SD_RESAMPLE_BILINEAR><<<grid_for(npx, B), B, 0, st>>>(p);
+  }
   SD_LAUNCHED(ctx);
 
   int flags[4];
