@@ -222,7 +222,7 @@ def run_ours(args):
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_k, 4)}
                for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
 
-    e2e = run_e2e(args, sd, sc, ctx, stream, barrier, dist) if args.config == "c2" else None
+    e2e = run_e2e(args, sd, sc, ctx, stream, barrier, dist) if (args.config == "c2" and args.e2e) else None
 
     if rank == 0:
         out = {
@@ -442,6 +442,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c2", "c1"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--ref-rows", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:
