@@ -322,6 +322,35 @@ int sd_apply_calibration(sd_ctx *ctx, const int16_t *deburst_iq, uint64_t lines,
                          float *out_nesz, uint32_t *cal_gap_px,
                          uint32_t *noise_gap_px);
 
+/* Allocation-free variant of sd_apply_calibration — no counterpart in the
+ * reference.  For callers that cannot allocate device memory while they run
+ * (a process that reserved its HBM budget up front in its own pool, a stage
+ * that must not let cudaMalloc/cudaFree serialise other streams, a host that
+ * only lends this library buffers it already owns).  Same results as
+ * sd_apply_calibration; no device allocation of any kind:
+ *  - deburst_iq, out_sigma0 and out_nesz must be device (or managed) memory
+ *    of the current device; the call is enqueued on `stream` (NULL = the
+ *    legacy default stream) and returns without waiting for it;
+ *  - working memory is one static 20 MiB device array inside the library,
+ *    held by every device that loads it until the process exits.  Limits:
+ *    <= 64 LUT vectors and <= 65536 LUT knots per family (sigma0, range
+ *    noise), <= 32768 lines, <= 32768 samples; larger inputs are rejected
+ *    with SD_ERR_INVALID_ARGUMENT and a message;
+ *  - the first call on a device resolves the array's address on that device
+ *    (cudaGetSymbolAddress); make that first call before any stream capture;
+ *  - every call shares the one array and leaves its contents behind (nothing
+ *    in it needs to start at zero): calls whose work overlaps on the GPU race
+ *    with each other, so serialise them (one stream, or events);
+ *  - err (may be NULL) receives the error message, err_len bytes at most. */
+int sd_apply_calibration_noalloc(void *stream, const int16_t *deburst_iq, uint64_t lines,
+                                 uint64_t samples, uint64_t valid_sample_offset,
+                                 const sd_lut_vector *cal, uint64_t n_cal,
+                                 const sd_lut_vector *noise_range, uint64_t n_noise_range,
+                                 const sd_noise_azimuth *noise_azimuth,
+                                 uint64_t tiff_line_origin, float *out_sigma0,
+                                 float *out_nesz, uint32_t *cal_gap_px,
+                                 uint32_t *noise_gap_px, char *err, uint64_t err_len);
+
 /* ── Merge ────────────────────────────────────────────────────────────────
  * merge_subswaths (merge_subswaths.rs:207-450) over n calibrated swaths,
  * given in IW1 < IW2 < IW3 order.  sigma0[i]/nesz[i] are lines[i] x

@@ -33,6 +33,9 @@ _SIGS = {
     "sd_deburst_subswath": (C.c_int, [P, P, C.c_uint64, C.c_uint64, P, P, C.c_uint64, P]),
     "sd_apply_calibration": (C.c_int, [P, P, C.c_uint64, C.c_uint64, C.c_uint64, P, C.c_uint64, P,
                                        C.c_uint64, P, C.c_uint64, P, P, P, P]),
+    "sd_apply_calibration_noalloc": (C.c_int, [P, P, C.c_uint64, C.c_uint64, C.c_uint64, P,
+                                               C.c_uint64, P, C.c_uint64, P, C.c_uint64, P, P,
+                                               P, P, P, C.c_uint64]),
     "sd_merge_subswaths": (C.c_int, [P, C.c_int32, P, P, P, P, P, P, P, P, P, P, P, P]),
     "sd_calibrate_deburst_merge": (C.c_int, [P, C.c_int32, P, P, P, P]),
     "sd_tc_output_grid": (C.c_int, [P, P, P, P]),

@@ -13,6 +13,7 @@
 // out-of-window samples are never read.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "geo.cuh"
@@ -667,4 +668,228 @@ extern "C" int sd_calibrate_deburst_merge(sd_ctx *ctx, int32_t n, const sd_swath
   SD_TRY(finish_out(ctx, out, d_out, L * Cc * 4));
   SD_TRY(finish_out(ctx, out_nesz, d_nesz, L * Cc * 4));
   return sync(ctx);
+}
+
+// ═══════════════════════════════════════════════════════════════════════════
+// Allocation-free calibration
+//
+// Some callers cannot allocate device memory once they are running: a
+// serving process that reserved its whole HBM budget up front in its own
+// pool, a pipeline stage that must not let cudaMalloc/cudaFree serialise the
+// device behind other streams, or a host that only hands this library
+// buffers it already owns.  sd_apply_calibration_noalloc gives them the same
+// result as sd_apply_calibration without any device allocation: its working
+// memory (LUT vectors, per-column LUT tables, per-line brackets) lives in
+// one file-scope __device__ array of fixed size, and the caller passes the
+// deburst raster and both outputs as device memory it owns.
+// ═══════════════════════════════════════════════════════════════════════════
+namespace sd {
+namespace {
+
+// Capacity of the static working memory (20 MiB; every device that loads the
+// library keeps it for the life of the process).
+constexpr uint64_t NA_MAX_VECTORS = 64;          // per LUT family
+constexpr uint64_t NA_MAX_POINTS = 64 * 1024;    // LUT knots per family, all vectors
+constexpr uint64_t NA_MAX_SAMPLES = 32 * 1024;   // output columns
+constexpr uint64_t NA_MAX_LINES = 32 * 1024;     // output lines
+constexpr size_t NA_SCRATCH_BYTES = 20u << 20;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device, resolved once per device
+// (with that device current) by the first call on it.
+std::mutex g_na_mu;
+void *g_na_ptr[64] = {nullptr};
+
+struct NaLayout {  // byte offsets inside the static array
+  size_t off[2][5];  // per family: px, pm, val, off, cnt
+  size_t tab[2];
+  size_t lp[2];
+  size_t az;
+  size_t total;
+};
+
+size_t na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+NaLayout na_layout(const CalPlan &P, uint64_t lines, uint64_t samples) {
+  NaLayout L{};
+  size_t o = 0;
+  for (int f = 0; f < 2; ++f) {
+    const LutHost &H = f == 0 ? P.cal : P.nr;
+    size_t pts = H.px.size(), nv = H.lines.size();
+    size_t sz[5] = {pts * 4, pts * 4, pts * 4, nv * 8, nv * 8};
+    for (int k = 0; k < 5; ++k) {
+      L.off[f][k] = o;
+      o = na_align(o + std::max<size_t>(sz[k], 1));
+    }
+  }
+  for (int f = 0; f < 2; ++f) {
+    const LutHost &H = f == 0 ? P.cal : P.nr;
+    L.tab[f] = o;
+    o = na_align(o + std::max<size_t>(H.lines.size() * samples * 4, 1));
+  }
+  for (int f = 0; f < 2; ++f) {
+    L.lp[f] = o;
+    o = na_align(o + std::max<size_t>(lines * sizeof(LineParams), 1));
+  }
+  L.az = o;
+  o = na_align(o + std::max<size_t>(lines * 4, 1));
+  L.total = o;
+  return L;
+}
+
+// k_calibrate with output line l read from raster row l (no line-map buffer).
+__global__ void k_calibrate_direct(CalSwathDev s, uint64_t lines, uint64_t samples, float *out, float *nesz) {
+  uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t l = blockIdx.y;
+  if (c >= samples || l >= lines) return;
+  const uint32_t iqw = __ldg((const uint32_t *)(s.iq) + l * s.stride + c);
+  const int32_t i = (int32_t)(int16_t)(iqw & 0xFFFF), q = (int32_t)(int16_t)(iqw >> 16);
+  const float power = (float)(int32_t)((uint32_t)(i * i) + (uint32_t)(q * q));
+  const LineParams cl = s.cal_lp[l], nl = s.nr_lp[l];
+  float k = __ldg(s.cal_tab + (uint64_t)cl.lo * s.tab_cols + c);
+  if (cl.lo != cl.hi) k = lerpf(k, __ldg(s.cal_tab + (uint64_t)cl.hi * s.tab_cols + c), cl.t);
+  float nrv = __ldg(s.nr_tab + (uint64_t)nl.lo * s.tab_cols + c);
+  if (nl.lo != nl.hi) nrv = lerpf(nrv, __ldg(s.nr_tab + (uint64_t)nl.hi * s.tab_cols + c), nl.t);
+  const float k2 = k * k;
+  const float valid = (k2 > 0.0f) ? 1.0f : 0.0f;
+  const float inv_k2 = (k2 > 0.0f) ? 1.0f / k2 : 0.0f;
+  const float noise_val = nrv * s.az[l];
+  out[l * samples + c] = maxf_nan(power - noise_val, 0.0f) * inv_k2 * valid;
+  nesz[l * samples + c] = noise_val * inv_k2 * valid;
+}
+
+template <class T>
+int na_copy(sd_ctx *c, unsigned char *base, size_t off, const std::vector<T> &v) {
+  if (!v.empty())
+    SD_CUDA(c, cudaMemcpyAsync(base + off, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  return SD_OK;
+}
+
+int noalloc_run(sd_ctx *c, const int16_t *iq, uint64_t lines, uint64_t samples, uint64_t col_offset,
+                const sd_lut_vector *cal, uint64_t n_cal, const sd_lut_vector *nr, uint64_t n_nr,
+                const sd_noise_azimuth *az, uint64_t tiff_line_origin, float *out, float *nesz,
+                uint32_t *cal_gap, uint32_t *nr_gap) {
+  // size limits first: the static working memory is fixed
+  if (n_cal > NA_MAX_VECTORS || n_nr > NA_MAX_VECTORS)
+    return set_error(c, SD_ERR_INVALID_ARGUMENT,
+                     "allocation-free calibration supports at most %llu LUT vectors per family (got %llu / %llu)",
+                     (unsigned long long)NA_MAX_VECTORS, (unsigned long long)n_cal, (unsigned long long)n_nr);
+  uint64_t pts_cal = 0, pts_nr = 0;
+  for (uint64_t i = 0; cal && i < n_cal; ++i) pts_cal += cal[i].n;
+  for (uint64_t i = 0; nr && i < n_nr; ++i) pts_nr += nr[i].n;
+  if (pts_cal > NA_MAX_POINTS || pts_nr > NA_MAX_POINTS)
+    return set_error(c, SD_ERR_INVALID_ARGUMENT,
+                     "allocation-free calibration supports at most %llu LUT knots per family (got %llu / %llu)",
+                     (unsigned long long)NA_MAX_POINTS, (unsigned long long)pts_cal, (unsigned long long)pts_nr);
+  if (samples > NA_MAX_SAMPLES || lines > NA_MAX_LINES)
+    return set_error(c, SD_ERR_INVALID_ARGUMENT,
+                     "allocation-free calibration supports at most %llu x %llu (lines x samples); got %llu x %llu",
+                     (unsigned long long)NA_MAX_LINES, (unsigned long long)NA_MAX_SAMPLES,
+                     (unsigned long long)lines, (unsigned long long)samples);
+  CalPlan P;
+  SD_TRY(cal_plan(c, cal, n_cal, nr, n_nr, az, col_offset, samples, tiff_line_origin, lines, &P));
+  if (cal_gap) *cal_gap = P.cal_gap;
+  if (nr_gap) *nr_gap = P.nr_gap;
+  if (lines == 0 || samples == 0) return SD_OK;
+  if (!iq || !out || !nesz) return set_error(c, SD_ERR_INVALID_ARGUMENT, "null buffer");
+  if (!is_device_ptr(iq) || !is_device_ptr(out) || !is_device_ptr(nesz))
+    return set_error(c, SD_ERR_INVALID_ARGUMENT,
+                     "allocation-free calibration needs device (or managed) memory for the raster and both outputs");
+  NaLayout L = na_layout(P, lines, samples);
+  if (L.total > NA_SCRATCH_BYTES)
+    return set_error(c, SD_ERR_INVALID_ARGUMENT, "working set %zu B exceeds the %zu B static scratch", L.total,
+                     NA_SCRATCH_BYTES);
+  // resolve the array's device address once per device (this device is current)
+  unsigned char *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    void *&slot = g_na_ptr[c->device & 63];
+    if (!slot) {
+      void *p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(c, SD_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s",
+                         cudaGetErrorString(e));
+      }
+      slot = p;
+    }
+    base = (unsigned char *)slot;
+  }
+  CalSwathDev s{};
+  for (int f = 0; f < 2; ++f) {
+    const LutHost &H = f == 0 ? P.cal : P.nr;
+    SD_TRY(na_copy(c, base, L.off[f][0], H.px));
+    SD_TRY(na_copy(c, base, L.off[f][1], H.pm));
+    SD_TRY(na_copy(c, base, L.off[f][2], H.val));
+    SD_TRY(na_copy(c, base, L.off[f][3], H.off));
+    SD_TRY(na_copy(c, base, L.off[f][4], H.cnt));
+    LutDev d{(const uint32_t *)(base + L.off[f][0]), (const uint32_t *)(base + L.off[f][1]),
+             (const float *)(base + L.off[f][2]), (const uint64_t *)(base + L.off[f][3]),
+             (const uint64_t *)(base + L.off[f][4])};
+    float *tab = (float *)(base + L.tab[f]);
+    uint64_t nv = H.lines.size();
+    SD_TIMED_BEGIN(c, "k_lut_table");
+    k_lut_table<<<grid_for(nv * samples, 256), 256, 0, c->stream>>>(d, nv, samples, col_offset, tab);
+    SD_LAUNCHED(c);
+    (f == 0 ? s.cal_tab : s.nr_tab) = tab;
+  }
+  SD_TRY(na_copy(c, base, L.lp[0], P.cal_lp));
+  SD_TRY(na_copy(c, base, L.lp[1], P.nr_lp));
+  SD_TRY(na_copy(c, base, L.az, P.az));
+  s.tab_cols = samples;
+  s.cal_lp = (const LineParams *)(base + L.lp[0]);
+  s.nr_lp = (const LineParams *)(base + L.lp[1]);
+  s.az = (const float *)(base + L.az);
+  s.iq = iq;
+  s.stride = samples;
+  s.line_map = nullptr;
+  s.col0 = 0;
+  // identity line map without a buffer: one launch per line block
+  for (uint64_t l0 = 0; l0 < lines; l0 += 65535) {
+    uint64_t nl = std::min<uint64_t>(65535, lines - l0);
+    CalSwathDev sl = s;
+    sl.iq = iq + l0 * samples * 2;
+    sl.cal_lp = s.cal_lp + l0;
+    sl.nr_lp = s.nr_lp + l0;
+    sl.az = s.az + l0;
+    dim3 grid(grid_for(samples, 256), (unsigned)nl);
+    SD_TIMED_BEGIN(c, "k_calibrate_noalloc");
+    k_calibrate_direct<<<grid, 256, 0, c->stream>>>(sl, nl, samples, out + l0 * samples, nesz + l0 * samples);
+    SD_LAUNCHED(c);
+  }
+  return SD_OK;
+}
+
+}  // namespace
+}  // namespace sd
+
+extern "C" int sd_apply_calibration_noalloc(void *stream, const int16_t *deburst_iq, uint64_t lines,
+                                            uint64_t samples, uint64_t valid_sample_offset,
+                                            const sd_lut_vector *cal, uint64_t n_cal,
+                                            const sd_lut_vector *noise_range, uint64_t n_noise_range,
+                                            const sd_noise_azimuth *noise_azimuth, uint64_t tiff_line_origin,
+                                            float *out_sigma0, float *out_nesz, uint32_t *cal_gap_px,
+                                            uint32_t *noise_gap_px, char *err, uint64_t err_len) {
+  sd_ctx c;  // host-side bookkeeping only; owns no device memory
+  int dev = 0;
+  int rc;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    rc = sd::set_error(&c, SD_ERR_CUDA, "no current CUDA device");
+  } else {
+    c.device = dev;
+    c.stream = (cudaStream_t)stream;
+    rc = sd::noalloc_run(&c, deburst_iq, lines, samples, valid_sample_offset, cal, n_cal, noise_range,
+                         n_noise_range, noise_azimuth, tiff_line_origin, out_sigma0, out_nesz, cal_gap_px,
+                         noise_gap_px);
+  }
+  if (err && err_len > 0) {
+    size_t n = std::min<size_t>(c.last_error.size(), err_len - 1);
+    memcpy(err, c.last_error.data(), n);
+    err[n] = 0;
+  }
+  c.stream = nullptr;  // the caller's stream is not ours to destroy
+  return rc;
 }
