@@ -190,7 +190,7 @@ def run_ours(args):
     kt = ctx.kernel_times()
     ctx.set_timing(False)
     total_k = sum(v[0] for v in kt.values()) or 1.0
-    tc_names = [k for k in kt if k.startswith(("k_geo", "k_cand", "k_scan", "k_out", "k_row", "k_orbit"))]
+    tc_names = [k for k in kt if k.startswith(("k_main", "k_scan", "k_select", "k_row", "k_orbit"))]
     tc_ms = sum(kt[k][0] for k in tc_names)
     prep_ms = sum(kt[k][0] for k in kt if k.startswith(("k_fused", "k_lut_table")))
     peaks = {}

@@ -199,6 +199,10 @@ typedef struct sd_geocoded_info {
     uint64_t flat_masked_count;
     uint64_t noise_masked_count;
     uint64_t newton_iter_histogram[SD_NEWTON_ITER_HIST_SIZE];
+    /* diagnostics (no reference counterpart): converged pixels whose
+     * azimuth time fell outside the precomputed fixed-point pair, so their
+     * outputs were computed on the row walk's exact path */
+    uint64_t diag_exact_path_pixels;
 } sd_geocoded_info;
 
 /* CalibrationVector / NoiseRangeVector (calibration.rs:38-82): one LUT row. */

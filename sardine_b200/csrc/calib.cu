@@ -169,19 +169,75 @@ struct MergeDev {
 };
 
 // Fused: merged pixel (l, c) <- owning swath's calibrated raster sample.
-__global__ void k_fused(MergeDev m, uint64_t lines, uint64_t cols, float *out, float *nesz) {
-  uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  uint64_t l = blockIdx.y;
-  if (c >= cols || l >= lines) return;
-  float a = NAN, b = NAN;
-  for (int k = 0; k < m.n; ++k) {
-    if (c < m.fr[k].col_end) {
-      if (c >= m.fr[k].vs && c < m.fr[k].ve) calibrate_px(m.sw[k], l, m.fr[k].in_start + (c - m.fr[k].vs), &a, &b);
-      break;
-    }
+// One block per (line, 2048-column chunk): the line's per-swath raster row,
+// LUT brackets and azimuth-noise factor are read once into shared memory;
+// each thread then handles 8 columns 256 apart (coalesced), in 32-bit
+// column arithmetic.
+constexpr int FU_THREADS = 256, FU_PER_THREAD = 8, FU_COLS = FU_THREADS * FU_PER_THREAD;
+
+struct FuLine {
+  const uint32_t *row;
+  float az;
+  LineParams cal, nr;
+  uint32_t col_end, vs, ve, in_start;
+};
+
+__global__ void __launch_bounds__(FU_THREADS) k_fused(MergeDev m, uint64_t lines, uint64_t cols, float *out,
+                                                     float *nesz) {
+  __shared__ FuLine sl[8];
+  const uint64_t chunks = (cols + FU_COLS - 1) / FU_COLS;
+  const uint64_t l = blockIdx.x / chunks;
+  const uint32_t c0 = (uint32_t)((blockIdx.x % chunks) * FU_COLS);
+  if (l >= lines) return;
+  if (threadIdx.x < (unsigned)m.n) {
+    const int k = threadIdx.x;
+    const CalSwathDev &s = m.sw[k];
+    FuLine f;
+    f.row = (const uint32_t *)s.iq + s.line_map[l] * s.stride + s.col0;
+    f.az = s.az[l];
+    f.cal = s.cal_lp[l];
+    f.nr = s.nr_lp[l];
+    f.col_end = (uint32_t)m.fr[k].col_end;
+    f.vs = (uint32_t)m.fr[k].vs;
+    f.ve = (uint32_t)m.fr[k].ve;
+    f.in_start = (uint32_t)m.fr[k].in_start;
+    sl[k] = f;
   }
-  out[l * cols + c] = a;
-  nesz[l * cols + c] = b;
+  __syncthreads();
+  float *orow = out + l * cols;
+  float *nrow = nesz + l * cols;
+#pragma unroll
+  for (int j = 0; j < FU_PER_THREAD; ++j) {
+    const uint32_t c = c0 + (uint32_t)(j * FU_THREADS) + threadIdx.x;
+    if (c >= cols) break;
+    float a = NAN, b = NAN;
+    for (int k = 0; k < m.n; ++k) {
+      const FuLine &f = sl[k];
+      if (c < f.col_end) {
+        if (c >= f.vs && c < f.ve) {
+          const uint32_t cc = f.in_start + (c - f.vs);
+          const CalSwathDev &s = m.sw[k];
+          const uint32_t iqw = __ldg(f.row + cc);
+          const int32_t i = (int32_t)(int16_t)(iqw & 0xFFFF), q = (int32_t)(int16_t)(iqw >> 16);
+          const float power = (float)(int32_t)((uint32_t)(i * i) + (uint32_t)(q * q));
+          float kk = __ldg(s.cal_tab + (uint64_t)f.cal.lo * s.tab_cols + cc);
+          if (f.cal.lo != f.cal.hi) kk = lerpf(kk, __ldg(s.cal_tab + (uint64_t)f.cal.hi * s.tab_cols + cc), f.cal.t);
+          float nr = __ldg(s.nr_tab + (uint64_t)f.nr.lo * s.tab_cols + cc);
+          if (f.nr.lo != f.nr.hi) nr = lerpf(nr, __ldg(s.nr_tab + (uint64_t)f.nr.hi * s.tab_cols + cc), f.nr.t);
+          // apply_cal_row (apply_calibration.rs:288-309)
+          const float k2 = kk * kk;
+          const float valid = (k2 > 0.0f) ? 1.0f : 0.0f;
+          const float inv_k2 = (k2 > 0.0f) ? 1.0f / k2 : 0.0f;
+          const float noise_val = nr * f.az;
+          a = maxf_nan(power - noise_val, 0.0f) * inv_k2 * valid;
+          b = noise_val * inv_k2 * valid;
+        }
+        break;
+      }
+    }
+    orow[c] = a;
+    nrow[c] = b;
+  }
 }
 
 // Plain merge of calibrated swaths.
@@ -660,9 +716,10 @@ extern "C" int sd_calibrate_deburst_merge(sd_ctx *ctx, int32_t n, const sd_swath
   SD_TRY(stage_out(ctx, "fu.out", out, L * Cc * 4, &d_out));
   SD_TRY(stage_out(ctx, "fu.nesz", out_nesz, L * Cc * 4, &d_nesz));
   if (L > 0 && Cc > 0) {
-    dim3 grid(grid_for(Cc, 256), (unsigned)L);
+    const uint64_t nblk = ((Cc + FU_COLS - 1) / FU_COLS) * L;
+    if (nblk > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "merged raster too large");
     SD_TIMED_BEGIN(ctx, "k_fused");
-    k_fused<<<grid, 256, 0, ctx->stream>>>(m, L, Cc, (float *)d_out, (float *)d_nesz);
+    k_fused<<<(unsigned)nblk, FU_THREADS, 0, ctx->stream>>>(m, L, Cc, (float *)d_out, (float *)d_nesz);
     SD_LAUNCHED(ctx);
   }
   SD_TRY(finish_out(ctx, out, d_out, L * Cc * 4));

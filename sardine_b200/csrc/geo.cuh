@@ -190,6 +190,122 @@ SD_HD void utm_xy_to_lonlat(const Utm &u, double x, double y, double *lon_deg, d
   *lon_deg = adjlon(atan2(s, c) + u.lon0) * (180.0 / kPi);
 }
 
+// The forward projection split into its latitude-only and longitude-only
+// parts, so lookups that share a latitude or a longitude share that work.
+// utm_xy_from(u, utm_taup(u, lat), utm_lam(u, lon)) performs exactly the
+// operations of utm_lonlat_to_xy(u, lon, lat).
+SD_HD double utm_taup(const Utm &u, double lat_deg) { return taupf(tan(lat_deg * (kPi / 180.0)), u.e); }
+struct LamSC {
+  double s, c;
+};
+SD_HD LamSC utm_lam(const Utm &u, double lon_deg) {
+  double lam = adjlon(lon_deg * (kPi / 180.0) - u.lon0);
+  return {sin(lam), cos(lam)};
+}
+SD_HD void utm_xy_from(const Utm &u, double taup, LamSC L, double *x, double *y) {
+  double xip = atan2(taup, L.c);
+  double etap = asinh(L.s / hypot(taup, L.c));
+  double sr, si;
+  krueger_sum(u.alp, xip, etap, &sr, &si);
+  *x = 500000.0 + u.k0A * (etap + si);
+  *y = (u.south ? 10000000.0 : 0.0) + u.k0A * (xip + sr);
+}
+
+// Local expansion of the forward projection around one point, for lookups a
+// few metres away (the four cardinal DEM neighbours of an output pixel).
+// With w = psi + i*lam (isometric latitude, longitude) the spherical step is
+// zeta' = gd(w), so d zeta'/dw = cos(zeta') and d2 zeta'/dw2 =
+// -cos(zeta') sin(zeta'); the Krueger series adds d zeta/d zeta' =
+// 1 + sum 2j a_j cos(2j zeta') and d2 zeta/d zeta'2 = -sum 4j^2 a_j sin(2j zeta').
+// A second-order step of |dw| ~ 2e-6 is exact to ~3e-11 m (the third-order
+// term), below the rounding of the projected coordinates themselves.
+struct UtmLocal {
+  double x, y;             // projected point
+  double zw_re, zw_im;     // d zeta / dw
+  double zww_re, zww_im;   // d2 zeta / dw2
+  double dpsi1, dpsi2;     // d psi/d phi, d2 psi/d phi2 (phi in radians)
+};
+
+SD_HD void utm_local(const Utm &u, double lat_deg, double taup, LamSC L, UtmLocal *o) {
+  const double xip = atan2(taup, L.c);
+  const double etap = asinh(L.s / hypot(taup, L.c));
+  // sin/cos of zeta' and of 2 zeta'
+  const double sx = sin(xip), cx = cos(xip);
+  const double ex = exp(etap), emx = 1.0 / ex;
+  const double sh = 0.5 * (ex - emx), ch = 0.5 * (ex + emx);
+  const double s_re = sx * ch, s_im = cx * sh;    // sin(zeta')
+  const double c_re = cx * ch, c_im = -sx * sh;   // cos(zeta')
+  const double s2_re = 2.0 * (s_re * c_re - s_im * c_im), s2_im = 2.0 * (s_re * c_im + s_im * c_re);
+  const double c2_re = c_re * c_re - c_im * c_im - (s_re * s_re - s_im * s_im);
+  const double c2_im = 2.0 * (c_re * c_im - s_re * s_im);
+  // Chebyshev recurrences for sin(2j z) and cos(2j z): S = sum a_j sin(2jz),
+  // D1 = sum 2j a_j cos(2jz), D2 = sum 4j^2 a_j sin(2jz)
+  double ps_re = 0.0, ps_im = 0.0, qs_re = s2_re, qs_im = s2_im;   // sin(0), sin(2z)
+  double pc_re = 1.0, pc_im = 0.0, qc_re = c2_re, qc_im = c2_im;   // cos(0), cos(2z)
+  double S_re = 0.0, S_im = 0.0, D1_re = 0.0, D1_im = 0.0, D2_re = 0.0, D2_im = 0.0;
+  for (int j = 1; j <= 6; ++j) {
+    const double a = u.alp[j];
+    S_re += a * qs_re;
+    S_im += a * qs_im;
+    D1_re += 2.0 * j * a * qc_re;
+    D1_im += 2.0 * j * a * qc_im;
+    D2_re += 4.0 * j * j * a * qs_re;
+    D2_im += 4.0 * j * j * a * qs_im;
+    const double ns_re = 2.0 * (c2_re * qs_re - c2_im * qs_im) - ps_re;
+    const double ns_im = 2.0 * (c2_re * qs_im + c2_im * qs_re) - ps_im;
+    const double nc_re = 2.0 * (c2_re * qc_re - c2_im * qc_im) - pc_re;
+    const double nc_im = 2.0 * (c2_re * qc_im + c2_im * qc_re) - pc_im;
+    ps_re = qs_re; ps_im = qs_im; qs_re = ns_re; qs_im = ns_im;
+    pc_re = qc_re; pc_im = qc_im; qc_re = nc_re; qc_im = nc_im;
+  }
+  o->x = 500000.0 + u.k0A * (etap + S_im);
+  o->y = (u.south ? 10000000.0 : 0.0) + u.k0A * (xip + S_re);
+  // d zeta/dw = (1 + D1) cos z ;  d2 zeta/dw2 = -D2 cos^2 z - (1 + D1) cos z sin z
+  const double g_re = 1.0 + D1_re, g_im = D1_im;
+  o->zw_re = g_re * c_re - g_im * c_im;
+  o->zw_im = g_re * c_im + g_im * c_re;
+  const double cc_re = c_re * c_re - c_im * c_im, cc_im = 2.0 * c_re * c_im;
+  const double cs_re = c_re * s_re - c_im * s_im, cs_im = c_re * s_im + c_im * s_re;
+  o->zww_re = -(D2_re * cc_re - D2_im * cc_im) - (g_re * cs_re - g_im * cs_im);
+  o->zww_im = -(D2_re * cc_im + D2_im * cc_re) - (g_re * cs_im + g_im * cs_re);
+  // isometric latitude derivatives: psi' = (1-e2)/(cos(phi)(1-e2 sin^2 phi))
+  const double phi = lat_deg * (kPi / 180.0);
+  const double sp = sin(phi), cp = cos(phi);
+  const double e2 = 1.0 - u.e2m;
+  const double q = 1.0 - e2 * sp * sp;
+  const double D = cp * q;
+  o->dpsi1 = u.e2m / D;
+  o->dpsi2 = u.e2m * (sp * q + 2.0 * e2 * sp * cp * cp) / (D * D);
+}
+
+// Projected coordinates of a point displaced by (dphi, dlam) radians.
+SD_HD void utm_local_step(const Utm &u, const UtmLocal &l, double dphi, double dlam, double *x, double *y) {
+  const double dw_re = l.dpsi1 * dphi + 0.5 * l.dpsi2 * dphi * dphi;
+  const double dw_im = dlam;
+  const double w2_re = dw_re * dw_re - dw_im * dw_im, w2_im = 2.0 * dw_re * dw_im;
+  const double dz_re = l.zw_re * dw_re - l.zw_im * dw_im + 0.5 * (l.zww_re * w2_re - l.zww_im * w2_im);
+  const double dz_im = l.zw_re * dw_im + l.zw_im * dw_re + 0.5 * (l.zww_re * w2_im + l.zww_im * w2_re);
+  *x = l.x + u.k0A * dz_im;
+  *y = l.y + u.k0A * dz_re;
+}
+
+// sin/cos of a + b from sin/cos of a, for |b| < 1e-4 (series to b^4).
+SD_HD void sincos_add(double sa, double ca, double b, double *s, double *c) {
+  const double b2 = b * b;
+  const double sb = b * (1.0 - b2 * (1.0 / 6.0) * (1.0 - b2 * (1.0 / 20.0)));
+  const double cb = 1.0 - 0.5 * b2 * (1.0 - b2 * (1.0 / 12.0));
+  *s = sa * cb + ca * sb;
+  *c = ca * cb - sa * sb;
+}
+
+// geodetic_to_ecef with sin/cos of latitude and longitude supplied
+// (same operations as geodetic_to_ecef).
+SD_HD V3 ecef_sc(double sin_lat, double cos_lat, double sin_lon, double cos_lon, double h) {
+  double n = WGS84_A / sqrt(1.0 - WGS84_E2 * sin_lat * sin_lat);
+  return {(n + h) * cos_lat * cos_lon, (n + h) * cos_lat * sin_lon, (n * (1.0 - WGS84_E2) + h) * sin_lat};
+}
+SD_HD double deg2rad_ecef(double deg) { return deg * kPi / 180.0; }  // geodesy.rs:39-40
+
 // ── DEM: DemSource::elevation_at for one grid (dem.rs:351-409, 694-723) ────
 struct DemView {
   const float *data;
@@ -198,6 +314,8 @@ struct DemView {
   int32_t kind;
   Utm utm;
 };
+
+SD_HD bool dem_sample(const DemView &d, double row_f, double col_f, float *h);
 
 // returns false for Err(OutOfBounds); *h = NaN for voids.
 SD_HD bool dem_elevation(const DemView &d, double lat_deg, double lon_deg, float *h) {
@@ -212,6 +330,11 @@ SD_HD bool dem_elevation(const DemView &d, double lat_deg, double lon_deg, float
     row_f = (d.origin_y - y) / d.pixel_size;
     col_f = (x - d.origin_x) / d.pixel_size;
   }
+  return dem_sample(d, row_f, col_f, h);
+}
+
+// Glo30Tile::elevation_at from fractional pixel coordinates (dem.rs:351-409).
+SD_HD bool dem_sample(const DemView &d, double row_f, double col_f, float *h) {
   double max_row = (double)(d.height - 1);
   double max_col = (double)(d.width - 1);
   if (row_f < -0.5 || row_f > max_row + 0.5 || col_f < -0.5 || col_f > max_col + 0.5) return false;
@@ -243,6 +366,14 @@ SD_HD bool dem_elevation(const DemView &d, double lat_deg, double lon_deg, float
              (double)v10 * dr * (1.0 - dc) + (double)v11 * dr * dc;
   *h = (float)v;
   return true;
+}
+
+SD_HD bool dem_at_xy(const DemView &d, double x, double y, float *h) {
+  return dem_sample(d, (d.origin_y - y) / d.pixel_size, (x - d.origin_x) / d.pixel_size, h);
+}
+SD_HD bool dem_at_lonlat(const DemView &d, double lon_deg, double lat_deg, float *h) {
+  double lon_norm = lon_deg >= 180.0 ? lon_deg - 360.0 : lon_deg;
+  return dem_sample(d, (d.origin_y - lat_deg) / d.pixel_size, (lon_norm - d.origin_x) / d.pixel_size, h);
 }
 
 // ── geoid (geoid.rs:220-251) ───────────────────────────────────────────────

@@ -40,17 +40,8 @@ namespace sd {
 namespace {
 
 enum : uint8_t { ST_CONV = 0, ST_NONCONV = 1, ST_DEGEN = 2, ST_ORBIT = 3, ST_DEMMISS = 4 };
-enum : uint8_t { RF_DEM_MISSING = 1, RF_HAS_F = 2 };
-constexpr uint8_t CODE_NONE = 0xFF;
 constexpr int KNOTS = 17;
 constexpr int kCounters = 8;  // valid, dem, outside, nonconv, degen, flat, noise, spare
-
-struct Rec {       // 16 B per pixel
-  int64_t base;    // F members are base + k for mask bit k
-  uint8_t mask;
-  uint8_t flags;
-  uint8_t pad[6];
-};
 
 struct OrbitDev {
   const sd_state_vector *svs;
@@ -100,19 +91,6 @@ __device__ ZdRes newton(const OrbitDev &o, V3 P, int64_t seed, int max_iter, dou
   return {ST_NONCONV, t, max_iter};
 }
 
-// True when the reference iteration seeded at t converges there immediately.
-__device__ bool fixed_point(const OrbitDev &o, V3 P, int64_t t, double tol) {
-  OrbitState s;
-  double vsq;
-  if (orbit_at(o, t, &s, &vsq) != ORB_OK) return false;
-  V3 r = sub3(P, s.pos);
-  double f = dot3(r, s.vel);
-  double fp = -vsq + dot3(r, s.acc);
-  if (fabs(fp) < 1.0) return false;
-  double delta = -f / fp;
-  return fabs(delta) < tol;
-}
-
 struct TcDev {
   // output grid
   uint64_t rows, cols;
@@ -146,11 +124,9 @@ struct TcDev {
   int flatten, compute_lia, need_geom, resampling, nesz_mask;
   float nesz_factor;
   // per-pixel scratch
-  double *px, *py, *pz;
-  Rec *rec;
-  uint32_t *codes;
-  int64_t *tsol;
-  uint8_t *stit;
+  struct Rec *rec;
+  uint32_t *cc;
+  uint8_t *sel;
   // outputs
   float *out;
   float *cos_lia;
@@ -299,119 +275,7 @@ __device__ int64_t predicted_time(const TcDev &p, uint64_t r, uint64_t c) {
   return t0 + (int64_t)llrint(f * (double)(t1 - t0));
 }
 
-// ── K3 ─────────────────────────────────────────────────────────────────────
-__global__ void __launch_bounds__(256) k_geo(TcDev p, int fast) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.rows * p.cols) return;
-  uint64_t r = i / p.cols, c = i % p.cols;
-  double lon, lat;
-  pixel_lonlat(p, r, c, &lon, &lat);
-  float hf;
-  Rec rec;
-  rec.base = 0;
-  rec.mask = 0;
-  rec.flags = 0;
-  if (!dem_elevation(p.dem, lat, lon, &hf) || !isfinite(hf)) {
-    rec.flags = RF_DEM_MISSING;
-    p.rec[i] = rec;
-    return;
-  }
-  double h_ell = (double)hf + geoid_undulation(p.geoid, lat, lon);
-  V3 P = geodetic_to_ecef(lat, lon, h_ell);
-  p.px[i] = P.x;
-  p.py[i] = P.y;
-  p.pz[i] = P.z;
-  if (fast) {
-    ZdRes z = newton(p.orb, P, predicted_time(p, r, c), 40, p.tol);
-    if (z.st == ST_CONV) {
-      rec.base = z.t - 1;
-      rec.mask = 2 | (fixed_point(p.orb, P, z.t - 1, p.tol) ? 1 : 0) |
-                 (fixed_point(p.orb, P, z.t + 1, p.tol) ? 4 : 0);
-      rec.flags = RF_HAS_F;
-    }
-  }
-  p.rec[i] = rec;
-}
-
-// ── K4 ─────────────────────────────────────────────────────────────────────
-__global__ void __launch_bounds__(256) k_cand(TcDev p) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= p.rows * p.cols) return;
-  uint64_t c = i % p.cols;
-  uint32_t codes = 0xFFFFFFFFu;
-  Rec me = p.rec[i];
-  if (c > 0 && (me.flags & RF_HAS_F)) {
-    Rec lf = p.rec[i - 1];
-    if (lf.flags & RF_HAS_F) {
-      V3 P = {p.px[i], p.py[i], p.pz[i]};
-      for (int k = 0; k < 3; ++k) {
-        if (!((lf.mask >> k) & 1)) continue;
-        ZdRes z = newton(p.orb, P, lf.base + k, p.max_iter, p.tol);
-        uint32_t code = CODE_NONE;
-        int it = z.it > 15 ? 15 : z.it;
-        if (z.st == ST_CONV) {
-          int64_t d = z.t - me.base;
-          if (d >= 0 && d <= 2 && ((me.mask >> d) & 1)) code = (uint32_t)d | ((uint32_t)it << 4);
-        } else if (z.st == ST_NONCONV || z.st == ST_DEGEN) {
-          code = 3u | ((uint32_t)z.st << 2) | ((uint32_t)it << 4);
-        }
-        codes = (codes & ~(0xFFu << (8 * k))) | (code << (8 * k));
-      }
-    }
-  }
-  p.codes[i] = codes;
-}
-
-// ── K5 ─────────────────────────────────────────────────────────────────────
-__global__ void __launch_bounds__(128) k_scan(TcDev p) {
-  uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= p.rows) return;
-  int64_t s = p.row_guess[r];
-  int64_t prev_base = 0;
-  uint8_t prev_mask = 0;
-  const uint64_t base_i = r * p.cols;
-  for (uint64_t c = 0; c < p.cols; ++c) {
-    const uint64_t i = base_i + c;
-    Rec rec = p.rec[i];
-    if (rec.flags & RF_DEM_MISSING) {
-      p.stit[i] = ST_DEMMISS;
-      prev_mask = 0;
-      continue;
-    }
-    uint32_t code = CODE_NONE;
-    if (prev_mask && (rec.flags & RF_HAS_F)) {
-      int64_t k = s - prev_base;
-      if (k >= 0 && k <= 2 && ((prev_mask >> k) & 1)) code = (p.codes[i] >> (8 * k)) & 0xFFu;
-    }
-    uint8_t st;
-    int it;
-    int64_t t;
-    if (code != CODE_NONE) {
-      it = (int)(code >> 4);
-      if ((code & 3u) != 3u) {
-        st = ST_CONV;
-        t = rec.base + (int64_t)(code & 3u);
-      } else {
-        st = (uint8_t)((code >> 2) & 3u);
-        t = s;
-      }
-    } else {
-      V3 P = {p.px[i], p.py[i], p.pz[i]};
-      ZdRes z = newton(p.orb, P, s, p.max_iter, p.tol);
-      st = z.st;
-      t = z.t;
-      it = z.it > 15 ? 15 : z.it;
-    }
-    p.tsol[i] = t;
-    p.stit[i] = (uint8_t)(st | (it << 4));
-    if (st == ST_CONV) s = t;
-    if (st == ST_ORBIT) atomicOr(&p.flags[0], 1);
-    prev_base = rec.base;
-    prev_mask = (rec.flags & RF_HAS_F) ? rec.mask : 0;
-  }
-}
-
-// ── K6 ─────────────────────────────────────────────────────────────────────
+// ── resampling (terrain_correction.rs:770-983) ───────────────────────────────
 __device__ __forceinline__ float ldf(const float *p, int64_t i) { return __ldg(p + i); }
 
 __device__ float sample_bilinear(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
@@ -485,118 +349,611 @@ __device__ float sample_lanczos(const float *d, uint64_t nl, uint64_t ns, double
 }
 
 template <int KERNEL>
-__global__ void __launch_bounds__(256) k_out(TcDev p) {
+__device__ __forceinline__ float resample(const TcDev &p, double line, double sample) {
+  return KERNEL == SD_RESAMPLE_BICUBIC    ? sample_bicubic(p.img, p.lines, p.samples, line, sample)
+         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos(p.img, p.lines, p.samples, line, sample)
+                                          : sample_bilinear(p.img, p.lines, p.samples, line, sample);
+}
+
+// ── per-pixel geometry ───────────────────────────────────────────────────────
+// Centre of output pixel (r, c): lat/lon, DEM height and target ECEF.  The
+// sines/cosines and projection terms are kept for the neighbour lookups.
+struct PixGeo {
+  double lat, lon;
+  double la, lo;              // radians as geodesy.rs:39-40 converts them
+  double sla, cla, slo, clo;  // their sines and cosines
+  UtmLocal loc;               // UTM DEM: projection of the centre and its local expansion
+  V3 P;
+};
+
+// DEM lookup of the centre (1529-1536), geoid (1545) and target ECEF (1546).
+// Returns false when the DEM has no finite height there.
+__device__ bool pixel_geo(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g) {
+  pixel_lonlat(p, r, c, &g->lon, &g->lat);
+  float hf;
+  bool ok;
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    utm_local(u, g->lat, utm_taup(u, g->lat), utm_lam(u, g->lon), &g->loc);
+    ok = dem_at_xy(p.dem, g->loc.x, g->loc.y, &hf);
+  } else {
+    ok = dem_at_lonlat(p.dem, g->lon, g->lat, &hf);
+  }
+  if (!ok || !isfinite(hf)) return false;
+  double h_ell = (double)hf + geoid_undulation(p.geoid, g->lat, g->lon);
+  g->la = deg2rad_ecef(g->lat);
+  g->lo = deg2rad_ecef(g->lon);
+  g->sla = sin(g->la);
+  g->cla = cos(g->la);
+  g->slo = sin(g->lo);
+  g->clo = cos(g->lo);
+  g->P = ecef_sc(g->sla, g->cla, g->slo, g->clo, h_ell);
+  return true;
+}
+
+// Facet of the four cardinal DEM neighbours (1642-1675): normal and area.
+// The neighbours sit step_deg from the centre, so their projected
+// coordinates come from the centre's local expansion and their sines and
+// cosines from angle addition over the exact argument differences.
+struct Facet {
+  bool ok;
+  V3 normal;
+  double area;
+};
+
+__device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
+  Facet f{};
+  const double sd = p.step_deg;
+  const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
+  float he, hw, hn, hs;
+  bool ok;
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    const double k = kPi / 180.0;
+    double x, y;
+    utm_local_step(u, g.loc, 0.0, (lon_e - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &he);
+    utm_local_step(u, g.loc, 0.0, (lon_w - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hw) && ok;
+    utm_local_step(u, g.loc, (lat_n - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hn) && ok;
+    utm_local_step(u, g.loc, (lat_s - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hs) && ok;
+  } else {
+    ok = dem_at_lonlat(p.dem, lon_e, g.lat, &he);
+    ok = dem_at_lonlat(p.dem, lon_w, g.lat, &hw) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_n, &hn) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_s, &hs) && ok;
+  }
+  f.ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
+  if (!f.ok) return f;
+  double se, ce, sw, cw, sn, cn, ss, cs;
+  sincos_add(g.slo, g.clo, deg2rad_ecef(lon_e) - g.lo, &se, &ce);
+  sincos_add(g.slo, g.clo, deg2rad_ecef(lon_w) - g.lo, &sw, &cw);
+  sincos_add(g.sla, g.cla, deg2rad_ecef(lat_n) - g.la, &sn, &cn);
+  sincos_add(g.sla, g.cla, deg2rad_ecef(lat_s) - g.la, &ss, &cs);
+  V3 pe = ecef_sc(g.sla, g.cla, se, ce, (double)he);
+  V3 pw = ecef_sc(g.sla, g.cla, sw, cw, (double)hw);
+  V3 pn = ecef_sc(sn, cn, g.slo, g.clo, (double)hn);
+  V3 ps = ecef_sc(ss, cs, g.slo, g.clo, (double)hs);
+  f.normal = cross3(sub3(pe, pw), sub3(pn, ps));
+  f.area = norm3(f.normal);
+  return f;
+}
+
+// Output of one pixel for one converged azimuth time (1585-1739): sigma0 /
+// gamma0, cos(LIA), mask code and counter class (0 valid, 2 outside
+// footprint, 5 flat-masked, 6 noise-masked).
+struct CandOut {
+  float data, cos;
+  uint8_t mask, cls;
+};
+
+struct CandPre {  // steps 4-6 of the reference loop for one candidate
+  double line, sample;
+  float sigma0;
+  bool inside;
+};
+
+template <int KERNEL>
+__device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
+  CandPre c;
+  double slant = norm3(sub3(P, S));
+  double dt = (double)(t - p.az_start) / 1e6;
+  c.line = dt / p.ati;
+  c.sample = (slant - p.near_range) / p.rps;
+  c.inside = !(c.line < -0.5 || c.line > ((double)p.lines - 0.5) || c.sample < -0.5 ||
+               c.sample > ((double)p.samples - 0.5));
+  c.sigma0 = c.inside ? resample<KERNEL>(p, c.line, c.sample) : NAN;
+  if (c.sigma0 != c.sigma0) c.inside = false;
+  return c;
+}
+
+__device__ CandOut cand_post(const TcDev &p, const CandPre &c, V3 P, V3 S, const Facet &f, double flat_area) {
+  CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
+  if (!c.inside) return o;
+  float sigma0 = c.sigma0;
+  uint8_t m = SD_MASK_OUTSIDE_FOOTPRINT;
+  float cosv = NAN;
+  if (p.need_geom) {
+    if (!f.ok) {
+      m = SD_MASK_DEM_NEIGHBOUR_MISSING;
+      if (p.flatten) return {NAN, cosv, m, 5};
+    } else {
+      V3 look = normalize3(sub3(S, P));
+      double local_proj = dot3(f.normal, look);
+      if (local_proj <= 0.0 || f.area == 0.0) {
+        m = SD_MASK_SHADOW;
+        if (p.flatten) return {NAN, cosv, m, 5};
+      } else {
+        double cl = clampd(local_proj / f.area, 0.0, 1.0);
+        double w = local_proj / flat_area;
+        cosv = (float)cl;
+        if (w < 0.05 || w > 2.0) {
+          m = w > 2.0 ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING;
+          if (p.flatten) return {NAN, cosv, m, 5};
+        } else if (p.flatten) {
+          sigma0 /= (float)w;
+        }
+      }
+    }
+  }
+  if (p.nesz_mask) {
+    float nz = sample_bilinear(p.nesz, p.lines, p.samples, c.line, c.sample);
+    if (nz == nz) {
+      float thr = nz * p.nesz_factor;
+      if (sigma0 <= thr) return {NAN, cosv, (uint8_t)SD_MASK_NOISE_MASKED, 6};
+    }
+  }
+  return {sigma0, cosv, (uint8_t)SD_MASK_VALID, 0};
+}
+
+// ── per-pixel stores ─────────────────────────────────────────────────────────
+// Rec: the fixed-point pair F = {fb, fb+1} and the pixel's output for each
+// member.  cc: codes (outcome of the reference iteration seeded at each
+// member of the left neighbour's F), F membership and flags.
+struct __align__(16) Rec {
+  int64_t fb;
+  float data[2];
+  float cos[2];
+  uint8_t omask[2];
+  uint8_t ocls[2];
+  uint32_t pad;
+};
+enum : uint32_t { CF_DEMMISS = 1u << 18, CF_HASF = 1u << 19, CF_HASOUT = 1u << 20 };
+// sel byte written by the scan: low 3 bits = outcome, high 4 bits = iterations
+enum : uint8_t { SEL_M0 = 0, SEL_M1 = 1, SEL_DONE = 2, SEL_NONCONV = 3, SEL_DEGEN = 4, SEL_DEMMISS = 5,
+                 SEL_ORBIT = 6 };
+
+struct Ent {  // one orbit-table record
+  double px, py, pz, vx, vy, vz, ax, ay, az, vsq;
+};
+
+__device__ __forceinline__ int ent_at(const OrbitDev &o, int64_t t, Ent *e) {
+  OrbitState s;
+  double vsq;
+  int rc = orbit_at(o, t, &s, &vsq);
+  if (rc != ORB_OK) return rc;
+  *e = {s.pos.x, s.pos.y, s.pos.z, s.vel.x, s.vel.y, s.vel.z, s.acc.x, s.acc.y, s.acc.z, vsq};
+  return ORB_OK;
+}
+
+// One evaluation of the Newton step at a tabulated state (1030-1053).
+// Returns 0 = converged (|delta| < tol), 1 = step, 2 = degenerate.
+__device__ __forceinline__ int zd_eval(V3 P, const Ent &e, double tol, double *delta) {
+  V3 r = {P.x - e.px, P.y - e.py, P.z - e.pz};
+  double f = r.x * e.vx + r.y * e.vy + r.z * e.vz;
+  double fp = -e.vsq + (r.x * e.ax + r.y * e.ay + r.z * e.az);
+  if (fabs(fp) < 1.0) return 2;
+  double d = -f / fp;
+  *delta = d;
+  return fabs(d) < tol ? 0 : 1;
+}
+
+struct Slot {  // shared-memory record exchanged with the right-hand neighbour
+  int64_t fb;
+  int32_t fmask;
+  int32_t pad;
+  Ent e[2];
+};
+
+constexpr int MAIN_THREADS = 128;
+constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
+
+// ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
+template <int KERNEL>
+__global__ void __launch_bounds__(MAIN_THREADS) k_main(TcDev p, int fast) {
+  __shared__ Slot slot[MAIN_THREADS];
+  const int tid = threadIdx.x;
+  const uint64_t blocks_per_row = (p.cols + MAIN_PIX - 1) / MAIN_PIX;
+  const uint64_t r = blockIdx.x / blocks_per_row;
+  const int64_t c = (int64_t)(blockIdx.x % blocks_per_row) * MAIN_PIX + tid - 1;
+  const bool in_row = c >= 0 && c < (int64_t)p.cols;
+  const uint64_t i = r * p.cols + (uint64_t)(c < 0 ? 0 : c);
+  PixGeo g;
+  bool geo_ok = false;
+  int fmask = 0;
+  int64_t fb = 0;
+  Ent e0{}, e1{};
+  // The warp's 32 pixels lie within ~10 ms of azimuth time: all lanes take
+  // their first Newton step from one shared state (one broadcast read), the
+  // landing point is within a few ns of each lane's own root.
+  const uint64_t rr = r < p.rows ? r : p.rows - 1;
+  const uint64_t cq = c < 0 ? 0 : ((uint64_t)c < p.cols ? (uint64_t)c : p.cols - 1);
+  const int64_t uw = __shfl_sync(0xffffffffu, predicted_time(p, rr, cq), 16);
+  Ent ew;
+  const bool ew_ok = fast && ent_at(p.orb, uw, &ew) == ORB_OK;
+  if (in_row && r < p.rows) {
+    geo_ok = pixel_geo(p, r, (uint64_t)c, &g);
+    if (geo_ok && fast) {
+      // reference iteration from the shared state: one converged t*
+      int64_t t = ew_ok ? uw : predicted_time(p, r, (uint64_t)c);
+      Ent e;
+      double d = 0.0;
+      int st = 1;
+      for (int it = 0; it < 40 && st == 1; ++it) {
+        if (it == 0 && ew_ok) e = ew;
+        else if (ent_at(p.orb, t, &e) != ORB_OK) { st = 3; break; }
+        st = zd_eval(g.P, e, p.tol, &d);
+        if (st == 1) t = t + f2i64(d * 1e6);
+      }
+      if (st == 0) {
+        // F = {t : |delta(t)| < tol} lies in {t*-1, t*, t*+1}.  The root sits
+        // at t* + d; delta carries ~1e-13 s of rounding noise (the dot
+        // product cancels terms of ~6e9), so for |d| >= 1e-11 s only
+        // t* + sign(d) can join t*, while for smaller |d| both neighbours are
+        // evaluated.  A three-member F is left to the exact path.
+        Ent ea, eb;
+        double da = 0.0, db = 0.0;
+        const int64_t ta = d > 0.0 ? t + 1 : t - 1;   // the likely member
+        const bool ma = ent_at(p.orb, ta, &ea) == ORB_OK && zd_eval(g.P, ea, p.tol, &da) == 0;
+        bool mb = false;
+        const int64_t tb = d > 0.0 ? t - 1 : t + 1;
+        if (fabs(d) < 1e-11) mb = ent_at(p.orb, tb, &eb) == ORB_OK && zd_eval(g.P, eb, p.tol, &db) == 0;
+        if (!(ma && mb)) {
+          const bool use_b = mb;                      // pair {t*, tb} when only tb joins
+          const int64_t other = use_b ? tb : ta;
+          const Ent &eo = use_b ? eb : ea;
+          const bool om = use_b ? mb : ma;
+          if (other > t) {
+            fb = t; e0 = e; e1 = eo; fmask = 1 | (om ? 2 : 0);
+          } else {
+            fb = other; e0 = eo; e1 = e; fmask = 2 | (om ? 1 : 0);
+          }
+        }
+      }
+    }
+  }
+  slot[tid].fb = fb;
+  slot[tid].fmask = fmask;
+  slot[tid].e[0] = e0;
+  slot[tid].e[1] = e1;
+  __syncthreads();
+  if (tid == 0 || !in_row || r >= p.rows) return;
+
+  uint32_t cc = 0xFFFFu;
+  Rec rec;
+  rec.fb = fb;
+  rec.pad = 0;
+  rec.data[0] = rec.data[1] = NAN;
+  rec.cos[0] = rec.cos[1] = NAN;
+  rec.omask[0] = rec.omask[1] = SD_MASK_OUTSIDE_FOOTPRINT;
+  rec.ocls[0] = rec.ocls[1] = 2;
+  if (!geo_ok) {
+    cc |= CF_DEMMISS;
+  } else if (fmask) {
+    cc |= CF_HASF | ((uint32_t)fmask << 16);
+    // outcome of the reference iteration seeded at each member of the left
+    // neighbour's F (the only seeds the row walk can hand this pixel)
+    const Slot &L = slot[tid - 1];
+    if (c > 0 && L.fmask) {
+      for (int k = 0; k < 2; ++k) {
+        if (!((L.fmask >> k) & 1)) continue;
+        int64_t t = L.fb + k;
+        uint32_t code = 0xFF;
+        for (int it = 0; it < p.max_iter; ++it) {
+          Ent e;
+          bool have = true;
+          if (t == L.fb + k) e = L.e[k];
+          else if (t == fb && (fmask & 1)) e = e0;
+          else if (t == fb + 1 && (fmask & 2)) e = e1;
+          else have = ent_at(p.orb, t, &e) == ORB_OK;
+          if (!have) break;  // orbit error: the walk redoes it
+          double d;
+          int st = zd_eval(g.P, e, p.tol, &d);
+          if (st == 0) {
+            int64_t m = t - fb;
+            if ((m == 0 || m == 1) && ((fmask >> m) & 1)) code = (uint32_t)m | ((uint32_t)min(it + 1, 15) << 4);
+            break;
+          }
+          if (st == 2) {
+            code = 3u | (2u << 2) | ((uint32_t)min(it, 15) << 4);
+            break;
+          }
+          t = t + f2i64(d * 1e6);
+          if (it + 1 == p.max_iter) code = 3u | (1u << 2) | ((uint32_t)min(p.max_iter, 15) << 4);
+        }
+        cc = (cc & ~(0xFFu << (8 * k))) | (code << (8 * k));
+      }
+    }
+    // outputs for both members of F
+    CandPre pre[2];
+    bool need = false;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const Ent &e = k == 0 ? e0 : e1;
+      if ((fmask >> k) & 1) {
+        pre[k] = cand_pre<KERNEL>(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
+        need = need || pre[k].inside;
+      } else {
+        pre[k].inside = false;
+      }
+    }
+    Facet f{};
+    if (need && p.need_geom) f = pixel_facet(p, g);
+    const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const Ent &e = k == 0 ? e0 : e1;
+      if (!((fmask >> k) & 1)) continue;
+      CandOut o = cand_post(p, pre[k], g.P, V3{e.px, e.py, e.pz}, f, flat_area);
+      rec.data[k] = o.data;
+      rec.cos[k] = o.cos;
+      rec.omask[k] = o.mask;
+      rec.ocls[k] = o.cls;
+    }
+    cc |= CF_HASOUT;
+  }
+  p.rec[i] = rec;
+  p.cc[i] = cc;
+}
+
+// ── K4: the row walk ──────────────────────────────────────────────────────
+// The walk's state between two pixels is either an index into the recorded
+// F of the previous pixel (kind 0) or an explicit seed time (kind 1, after a
+// DEM void, a non-converged solve or an exact-path pixel); kind 2 marks an
+// entry that cannot occur.
+struct WState {
+  int kind;
+  int64_t v;
+};
+
+// The reference solve of pixel (r, c) from seed s, for pixels the
+// precomputed records do not cover.  With `write`, it also stores the
+// pixel's outputs when the converged time has none precomputed.
+template <int KERNEL>
+__device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s, uint32_t cc, int64_t fb,
+                              bool write, uint8_t *sel) {
+  const uint64_t i = r * p.cols + c;
+  PixGeo g;
+  if (!pixel_geo(p, r, c, &g)) {
+    *sel = SEL_DEMMISS;
+    return {1, s};
+  }
+  ZdRes z = newton(p.orb, g.P, s, p.max_iter, p.tol);
+  if (z.st == ST_ORBIT) {
+    if (write) atomicOr(&p.flags[0], 1);
+    *sel = SEL_ORBIT;
+    return {1, s};
+  }
+  if (z.st == ST_NONCONV || z.st == ST_DEGEN) {
+    *sel = z.st == ST_NONCONV ? SEL_NONCONV : SEL_DEGEN;
+    return {1, s};
+  }
+  const int it = z.it > 15 ? 15 : z.it;
+  if (cc & CF_HASOUT) {
+    const uint32_t fm = (cc >> 16) & 3u;
+    const int64_t m = z.t - fb;
+    if ((m == 0 || m == 1) && ((fm >> m) & 1)) {
+      *sel = (uint8_t)(m | (it << 4));
+      return {0, m};
+    }
+  }
+  *sel = (uint8_t)(SEL_DONE | (it << 4));
+  if (write) {
+    atomicAdd(&p.flags[1], 1);
+    OrbitState os;
+    double vsq;
+    orbit_at(p.orb, z.t, &os, &vsq);
+    CandPre pre = cand_pre<KERNEL>(p, g.P, os.pos, z.t);
+    Facet f{};
+    if (pre.inside && p.need_geom) f = pixel_facet(p, g);
+    CandOut o = cand_post(p, pre, g.P, os.pos, f, p.need_geom ? p.row_flat[r] : 0.0);
+    p.out[i] = o.data;
+    if (p.compute_lia) {
+      p.cos_lia[i] = o.cos;
+      p.mask[i] = o.mask;
+    }
+    p.rec[i].ocls[0] = o.cls;
+  }
+  return {1, z.t};
+}
+
+// Walk columns [b, e) of row r from state st (terrain_correction.rs:
+// 1443-1580), any pixel kind.  fb is read only where a seed value is needed.
+template <int KERNEL>
+__device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, WState st, bool write) {
+  const uint64_t base = r * p.cols;
+  uint32_t prev_cc = b > 0 ? p.cc[base + b - 1] : CF_DEMMISS;
+  if (st.kind == 0 && !((prev_cc & CF_HASF) && ((prev_cc >> (16 + st.v)) & 1u))) return {2, 0};
+  for (uint64_t c = b; c < e; ++c) {
+    const uint32_t cc = p.cc[base + c];
+    uint8_t sel;
+    if (cc & CF_DEMMISS) {
+      if (st.kind == 0) st = {1, p.rec[base + c - 1].fb + st.v};  // the seed passes through the void
+      sel = SEL_DEMMISS;
+    } else {
+      uint32_t code = 0xFF;
+      if (st.kind == 0 && (prev_cc & CF_HASF) && (cc & CF_HASOUT)) code = (cc >> (8 * st.v)) & 0xFFu;
+      if (code != 0xFF && (code & 3u) != 3u) {
+        st = {0, (int64_t)(code & 3u)};
+        sel = (uint8_t)((code & 3u) | (code & 0xF0u));
+      } else if (code != 0xFF) {
+        st = {1, p.rec[base + c - 1].fb + st.v};  // not converged: seed unchanged
+        sel = (uint8_t)((((code >> 2) & 3u) == 1u ? SEL_NONCONV : SEL_DEGEN) | (code & 0xF0u));
+      } else {
+        const int64_t s = st.kind == 0 ? p.rec[base + c - 1].fb + st.v : st.v;
+        st = exact_pixel<KERNEL>(p, r, c, s, cc, p.rec[base + c].fb, write, &sel);
+      }
+    }
+    if (write) p.sel[base + c] = sel;
+    prev_cc = cc;
+  }
+  return st;
+}
+
+// One warp per row.  Lane 0 resolves the row's first valid pixel from the
+// LUT guess; the remaining columns are cut into 32 segments, each lane maps
+// the two possible entry states (which member of the left F the seed is)
+// through its segment, the maps are composed in lane order (a lane whose
+// entry is an explicit seed walks its segment at that point), and each lane
+// writes its segment from its actual entry.  In the regular case the
+// segments are streamed 32 columns at a time through shared memory with
+// coalesced transposed loads and stores; a segment with any other pixel
+// kind is (re)done by walk_seg.
+constexpr int SCAN_WARPS = 4;
+
+template <int KERNEL>
+__global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(TcDev p) {
+  __shared__ uint32_t sbuf[SCAN_WARPS][32][33];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t(*buf)[33] = sbuf[wid];
+  const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (r >= p.rows) return;  // uniform per warp
+  const uint64_t n = p.cols, base = r * n;
+  const uint32_t *ccr = p.cc + base;
+  uint64_t c0 = n;
+  WState st0{1, 0};
+  if (lane == 0) {
+    uint64_t c = 0;
+    while (c < n && (ccr[c] & CF_DEMMISS)) {
+      p.sel[base + c] = SEL_DEMMISS;
+      ++c;
+    }
+    if (c < n) {
+      st0 = walk_seg<KERNEL>(p, r, c, c + 1, WState{1, p.row_guess[r]}, true);
+      c0 = c + 1;
+    }
+  }
+  c0 = __shfl_sync(0xffffffffu, c0, 0);
+  st0.kind = __shfl_sync(0xffffffffu, st0.kind, 0);
+  st0.v = __shfl_sync(0xffffffffu, st0.v, 0);
+  if (c0 >= n) return;
+  const uint64_t seg = (n - c0 + 31) / 32;
+  const uint64_t b = c0 + (uint64_t)lane * seg;
+  const uint64_t e = min(n, b + seg);
+  const int nchunks = (int)((seg + 31) / 32);
+
+  // phase 1: both entry states through the segment (regular pixels only)
+  int s0 = 0, s1 = 1, bad = 0;
+  if (b < e) {
+    const uint32_t prev = ccr[b - 1];
+    if (!((prev & CF_HASF) && ((prev >> 16) & 1u))) bad |= 1;
+    if (!((prev & CF_HASF) && ((prev >> 17) & 1u))) bad |= 2;
+  }
+  for (int k = 0; k < nchunks; ++k) {
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t bj = c0 + (uint64_t)j * seg, ej = min(n, bj + seg);
+      const uint64_t idx = bj + 32 * (uint64_t)k + lane;
+      buf[j][lane] = idx < ej ? __ldg(ccr + idx) : 0u;
+    }
+    __syncwarp();
+    const int cnt = b + 32 * (uint64_t)k < e ? (int)min((uint64_t)32, e - b - 32 * (uint64_t)k) : 0;
+    for (int t = 0; t < cnt; ++t) {
+      const uint32_t w = buf[lane][t];
+      if ((w & (CF_DEMMISS | CF_HASOUT)) != CF_HASOUT) bad = 3;
+      const uint32_t x0 = (w >> (8 * s0)) & 0xFFu, x1 = (w >> (8 * s1)) & 0xFFu;
+      if (x0 == 0xFFu || (x0 & 3u) == 3u) bad |= 1;
+      if (x1 == 0xFFu || (x1 & 3u) == 3u) bad |= 2;
+      s0 = (int)(x0 & 1u);
+      s1 = (int)(x1 & 1u);
+    }
+    __syncwarp();
+  }
+  WState ex0 = {0, 0}, ex1 = {0, 1};
+  if (b < e) {
+    ex0 = (bad & 1) ? walk_seg<KERNEL>(p, r, b, e, WState{0, 0}, false) : WState{0, s0};
+    ex1 = (bad & 2) ? walk_seg<KERNEL>(p, r, b, e, WState{0, 1}, false) : WState{0, s1};
+  }
+  // phase 2: compose the lanes' maps in order
+  WState st = st0, entry{2, 0};
+  for (int j = 0; j < 32; ++j) {
+    WState nx = st;
+    if (lane == j) {
+      entry = st;
+      if (b < e) {
+        if (st.kind == 0) nx = st.v == 0 ? ex0 : ex1;
+        else nx = walk_seg<KERNEL>(p, r, b, e, st, false);
+      }
+    }
+    st.kind = __shfl_sync(0xffffffffu, nx.kind, j);
+    st.v = __shfl_sync(0xffffffffu, nx.v, j);
+  }
+  // phase 3: write the segments
+  const bool regular = b < e && entry.kind == 0 && !((bad >> entry.v) & 1);
+  int s = regular ? (int)entry.v : 0;
+  uint8_t *selr = p.sel + base;
+  for (int k = 0; k < nchunks; ++k) {
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t bj = c0 + (uint64_t)j * seg, ej = min(n, bj + seg);
+      const uint64_t idx = bj + 32 * (uint64_t)k + lane;
+      buf[j][lane] = idx < ej ? __ldg(ccr + idx) : 0u;
+    }
+    __syncwarp();
+    if (regular) {
+      const int cnt = b + 32 * (uint64_t)k < e ? (int)min((uint64_t)32, e - b - 32 * (uint64_t)k) : 0;
+      for (int t = 0; t < cnt; ++t) {
+        const uint32_t code = (buf[lane][t] >> (8 * s)) & 0xFFu;
+        s = (int)(code & 3u);
+        buf[lane][t] = (uint32_t)(s | (code & 0xF0u));
+      }
+    }
+    __syncwarp();
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t bj = c0 + (uint64_t)j * seg, ej = min(n, bj + seg);
+      const uint64_t idx = bj + 32 * (uint64_t)k + lane;
+      const bool reg_j = __shfl_sync(0xffffffffu, regular, j);
+      if (reg_j && idx < ej) selr[idx] = (uint8_t)buf[j][lane];
+    }
+    __syncwarp();
+  }
+  if (b < e && !regular) walk_seg<KERNEL>(p, r, b, e, entry, true);
+}
+
+// ── K5: final rasters, counters and Newton histogram ────────────────────────
+__global__ void __launch_bounds__(256) k_select(TcDev p) {
   __shared__ unsigned int s_cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
   for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
   __syncthreads();
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < p.rows * p.cols) {
-    uint64_t r = i / p.cols, c = i % p.cols;
-    uint8_t code = p.stit[i];
-    uint8_t st = code & 15;
-    int it = code >> 4;
-    float outv = NAN, cosv = NAN;
-    uint8_t m = SD_MASK_OUTSIDE_FOOTPRINT;
+    const uint8_t sel = p.sel[i];
+    const int code = sel & 7, it = sel >> 4;
     int counter = -1;
-    if (st == ST_DEMMISS) {
-      m = SD_MASK_DEM_MISSING;
-      counter = 1;
-    } else if (st == ST_NONCONV) {
-      m = SD_MASK_NON_CONVERGED;
-      counter = 3;
-    } else if (st == ST_DEGEN) {
-      m = SD_MASK_DEGENERATE_GEOMETRY;
-      counter = 4;
-    } else if (st == ST_CONV) {
+    if (code == SEL_M0 || code == SEL_M1) {
+      const Rec &rc = p.rec[i];
+      counter = rc.ocls[code];
       atomicAdd(&s_cnt[kCounters + it], 1u);
-      const int64_t t = p.tsol[i];
-      OrbitState s;
-      double vsq;
-      orbit_at(p.orb, t, &s, &vsq);
-      V3 P = {p.px[i], p.py[i], p.pz[i]};
-      double slant = norm3(sub3(P, s.pos));
-      double dt = (double)(t - p.az_start) / 1e6;
-      double line = dt / p.ati;
-      double sample = (slant - p.near_range) / p.rps;
-      do {
-        if (line < -0.5 || line > ((double)p.lines - 0.5) || sample < -0.5 ||
-            sample > ((double)p.samples - 0.5)) {
-          counter = 2;
-          break;
-        }
-        float sigma0 = KERNEL == SD_RESAMPLE_BICUBIC   ? sample_bicubic(p.img, p.lines, p.samples, line, sample)
-                       : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos(p.img, p.lines, p.samples, line, sample)
-                                                        : sample_bilinear(p.img, p.lines, p.samples, line, sample);
-        if (sigma0 != sigma0) {
-          counter = 2;
-          break;
-        }
-        if (p.need_geom) {
-          double lon, lat;
-          pixel_lonlat(p, r, c, &lon, &lat);
-          const double sd = p.step_deg;
-          float he, hw, hn, hs;
-          bool ok = dem_elevation(p.dem, lat, lon + sd, &he);
-          ok = dem_elevation(p.dem, lat, lon - sd, &hw) && ok;
-          ok = dem_elevation(p.dem, lat + sd, lon, &hn) && ok;
-          ok = dem_elevation(p.dem, lat - sd, lon, &hs) && ok;
-          ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
-          if (!ok) {
-            m = SD_MASK_DEM_NEIGHBOUR_MISSING;
-            if (p.flatten) {
-              counter = 5;
-              break;
-            }
-          } else {
-            double w = 0.0, cl = 0.0;
-            int g = terrain_geometry(lat, lon, (double)he, (double)hw, (double)hn, (double)hs, s.pos,
-                                     P, sd, p.row_flat[r], &w, &cl);
-            if (g == GEOM_VALID) {
-              cosv = (float)cl;
-              if (p.flatten) sigma0 /= (float)w;
-            } else if (g == GEOM_FORESHORTENING || g == GEOM_LAYOVER) {
-              cosv = (float)cl;
-              m = g == GEOM_LAYOVER ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING;
-              if (p.flatten) {
-                counter = 5;
-                break;
-              }
-            } else {
-              m = SD_MASK_SHADOW;
-              if (p.flatten) {
-                counter = 5;
-                break;
-              }
-            }
-          }
-        }
-        if (p.nesz_mask) {
-          float nz = sample_bilinear(p.nesz, p.lines, p.samples, line, sample);
-          if (nz == nz) {
-            float thr = nz * p.nesz_factor;
-            if (sigma0 <= thr) {
-              m = SD_MASK_NOISE_MASKED;
-              counter = 6;
-              break;
-            }
-          }
-        }
-        outv = sigma0;
-        m = SD_MASK_VALID;
-        counter = 0;
-      } while (0);
-      if (counter == 2) {
-        m = SD_MASK_OUTSIDE_FOOTPRINT;
-        cosv = NAN;
+      p.out[i] = rc.data[code];
+      if (p.compute_lia) {
+        p.cos_lia[i] = rc.cos[code];
+        p.mask[i] = rc.omask[code];
       }
-      if (counter == 5 && !p.compute_lia) cosv = NAN;
+    } else if (code == SEL_DONE) {
+      counter = p.rec[i].ocls[0];
+      atomicAdd(&s_cnt[kCounters + it], 1u);
+    } else if (code != SEL_ORBIT) {
+      uint8_t m = code == SEL_NONCONV ? SD_MASK_NON_CONVERGED
+                  : code == SEL_DEGEN ? SD_MASK_DEGENERATE_GEOMETRY
+                                      : SD_MASK_DEM_MISSING;
+      counter = code == SEL_NONCONV ? 3 : (code == SEL_DEGEN ? 4 : 1);
+      p.out[i] = NAN;
+      if (p.compute_lia) {
+        p.cos_lia[i] = NAN;
+        p.mask[i] = m;
+      }
     }
     if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
-    p.out[i] = outv;
-    if (p.compute_lia) {
-      p.cos_lia[i] = cosv;
-      p.mask[i] = m;
-    }
   }
   __syncthreads();
   for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
@@ -820,19 +1177,22 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
   SD_CUDA(ctx, cudaMemcpyAsync(tr, d_trange, sizeof tr, cudaMemcpyDeviceToHost, st));
   SD_TRY(sync(ctx));
 
-  // ── orbit table over the model's time span (+/- 0.5 s), inside the SV window ──
+  // ── orbit table over the row models' time span, inside the SV window ──
   if (nsv >= 8 && tr[0] <= tr[1]) {
     int64_t tmin = (int64_t)(tr[0] ^ 0x8000000000000000ull);
     int64_t tmax = (int64_t)(tr[1] ^ 0x8000000000000000ull);
-    int64_t t0 = std::max(scene->state_vectors[0].time_us, tmin - 500000);
-    int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us, tmax + 500000);
+    // +-0.1 s covers the height and interpolation spread of pixel roots
+    // around the row models; iterates outside the table are evaluated directly.
+    int64_t t0 = std::max(scene->state_vectors[0].time_us, tmin - 100000);
+    int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us, tmax + 100000);
     const int64_t max_entries = 96ll * 1000 * 1000;  // 7.7 GB cap
     if (t1 - t0 + 1 > max_entries) {
       int64_t mid = (tmin / 2 + tmax / 2);
       t0 = std::max(t0, mid - max_entries / 2);
       t1 = std::min(t1, t0 + max_entries - 1);
     }
-    if (t1 >= t0) {
+    // a table larger than the grid costs more to build than it saves
+    if (t1 >= t0 && (uint64_t)(t1 - t0 + 1) <= npx) {
       double2 *d_tab;
       SD_TRY(scratch_t(ctx, "tc.orbit_table", (size_t)(t1 - t0 + 1) * 5, &d_tab));
       SD_TIMED_BEGIN(ctx, "k_orbit_table");
@@ -846,13 +1206,9 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
   }
 
   // ── per-pixel scratch and outputs ──
-  SD_TRY(scratch_t(ctx, "tc.px", npx, &p.px));
-  SD_TRY(scratch_t(ctx, "tc.py", npx, &p.py));
-  SD_TRY(scratch_t(ctx, "tc.pz", npx, &p.pz));
   SD_TRY(scratch_t(ctx, "tc.rec", npx, &p.rec));
-  SD_TRY(scratch_t(ctx, "tc.codes", npx, &p.codes));
-  SD_TRY(scratch_t(ctx, "tc.tsol", npx, &p.tsol));
-  SD_TRY(scratch_t(ctx, "tc.stit", npx, &p.stit));
+  SD_TRY(scratch_t(ctx, "tc.cc", npx, &p.cc));
+  SD_TRY(scratch_t(ctx, "tc.sel", npx, &p.sel));
   void *d_out, *d_cos = nullptr, *d_mask = nullptr;
   SD_TRY(stage_out(ctx, "tc.out", out_data, npx * sizeof(float), &d_out));
   if (p.compute_lia) {
@@ -869,37 +1225,33 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
 
   // The candidate-set scheme needs tol <= 1 us (then at most three
   // consecutive microseconds can satisfy |delta| < tol).  Larger tolerances
-  // run every solve in the row walk.
+  // leave every pixel to the row walk's exact path.
   const int fast = (p.tol <= 1e-6) ? 1 : 0;
-  const unsigned B = 256;
-  SD_TIMED_BEGIN(ctx, "k_geo");
-  k_geo<<<grid_for(npx, B), B, 0, st>>>(p, fast);
-  SD_LAUNCHED(ctx);
-  if (fast) {
-    SD_TIMED_BEGIN(ctx, "k_cand");
-    k_cand<<<grid_for(npx, B), B, 0, st>>>(p);
-    SD_LAUNCHED(ctx);
-  } else {
-    SD_CUDA(ctx, cudaMemsetAsync(p.codes, 0xFF, npx * sizeof(uint32_t), st));
+  const uint64_t bpr = (p.cols + MAIN_PIX - 1) / MAIN_PIX;
+  if (bpr * p.rows > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "output grid too large");
+  const unsigned main_grid = (unsigned)(bpr * p.rows);
+  const unsigned scan_grid = grid_for(p.rows * 32, SCAN_WARPS * 32);
+  switch (p.resampling) {
+#define SD_TC_LAUNCH(K, NAME)                                                    \
+  case K:                                                                        \
+    SD_TIMED_BEGIN(ctx, "k_main<" NAME ">");                                     \
+    k_main<K><<<main_grid, MAIN_THREADS, 0, st>>>(p, fast);                      \
+    SD_LAUNCHED(ctx);                                                            \
+    SD_TIMED_BEGIN(ctx, "k_scan");                                               \
+    k_scan<K><<<scan_grid, SCAN_WARPS * 32, 0, st>>>(p);                                     \
+    SD_LAUNCHED(ctx);                                                            \
+    break;
+    SD_TC_LAUNCH(SD_RESAMPLE_BICUBIC, "BICUBIC")
+    SD_TC_LAUNCH(SD_RESAMPLE_LANCZOS3, "LANCZOS3")
+    default:
+    SD_TC_LAUNCH(SD_RESAMPLE_BILINEAR, "BILINEAR")
+#undef SD_TC_LAUNCH
   }
-  SD_TIMED_BEGIN(ctx, "k_scan");
-  k_scan<<<grid_for(p.rows, 128), 128, 0, st>>>(p);
-  SD_LAUNCHED(ctx);
-  if (p.resampling == SD_RESAMPLE_BICUBIC) {
-    SD_TIMED_BEGIN(ctx, "k_out<BICUBIC>");
-    k_out<SD_RESAMPLE_BICUBIC><<<grid_for(npx, B), B, 0, st>>>(p);
-  }
-  else if (p.resampling == SD_RESAMPLE_LANCZOS3) {
-    SD_TIMED_BEGIN(ctx, "k_out<LANCZOS3>");
-    k_out<SD_RESAMPLE_LANCZOS3><<<grid_for(npx, B), B, 0, st>>>(p);
-  }
-  else {
-    SD_TIMED_BEGIN(ctx, "k_out<BILINEAR>");
-    k_out<SD_RESAMPLE_BILINEAR><<<grid_for(npx, B), B, 0, st>>>(p);
-  }
+  SD_TIMED_BEGIN(ctx, "k_select");
+  k_select<<<grid_for(npx, 256), 256, 0, st>>>(p);
   SD_LAUNCHED(ctx);
 
-  int flags[4];
+  int flags[64];
   unsigned long long cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
   SD_CUDA(ctx, cudaMemcpyAsync(flags, ctx->d_flags, sizeof flags, cudaMemcpyDeviceToHost, st));
   SD_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost, st));
@@ -922,6 +1274,7 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
   info->flat_masked_count = cnt[5];
   info->noise_masked_count = cnt[6];
   for (int k = 0; k < SD_NEWTON_ITER_HIST_SIZE; ++k) info->newton_iter_histogram[k] = cnt[kCounters + k];
+  info->diag_exact_path_pixels = (uint64_t)flags[1];
   SD_TRY(sync(ctx));
   return SD_OK;
 }

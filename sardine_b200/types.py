@@ -402,6 +402,7 @@ class GeocodedImage:
     cos_lia: Any
     mask: Any
     newton_iter_histogram: List[int]
+    diag_exact_path_pixels: int = 0  # converged pixels computed on the row walk's exact path
 
     def valid_fraction(self) -> float:
         return self.valid_pixel_count / self.total_pixel_count
@@ -421,7 +422,8 @@ class GeocodedImage:
             flat_masked_count=int(info.flat_masked_count),
             noise_masked_count=int(info.noise_masked_count),
             geotransform=tuple(info.geotransform), crs=crs, cos_lia=cos_lia, mask=mask,
-            newton_iter_histogram=[int(x) for x in info.newton_iter_histogram])
+            newton_iter_histogram=[int(x) for x in info.newton_iter_histogram],
+            diag_exact_path_pixels=int(info.diag_exact_path_pixels))
 
 
 # ── speckle ────────────────────────────────────────────────────────────────
