@@ -562,7 +562,7 @@ constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
 
 // ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
 template <int KERNEL>
-__global__ void __launch_bounds__(MAIN_THREADS) k_main(TcDev p, int fast) {
+__global__ void __launch_bounds__(MAIN_THREADS, 4) k_main(TcDev p, int fast) {
   __shared__ Slot slot[MAIN_THREADS];
   const int tid = threadIdx.x;
   const uint64_t blocks_per_row = (p.cols + MAIN_PIX - 1) / MAIN_PIX;
