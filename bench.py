@@ -110,8 +110,13 @@ class ClockSampler:
 
 def make_workload(cfg: str, device: str, seed: int):
     from sardine_b200 import synth
+    import sardine_b200 as sd
     if cfg == "c1":
         return synth.config1_scene(seed=seed, device=device)
+    if cfg == "c3":
+        sc = synth.config2_scene(seed=seed, device=device, resampling=sd.ResamplingKernel.Lanczos3)
+        sc.config.precision = sd.Precision.SPLIT
+        return sc
     return synth.config2_scene(seed=seed, device=device)
 
 
@@ -155,6 +160,9 @@ def run_ours(args):
             return m, r
         workload = ("config2: full IW scene 3x9x1500x21000 CInt16 -> cal+deburst+merge -> TC "
                     "25000x20000 UTM 10 m, bicubic, gamma0 flatten, LIA+mask, FP64")
+        if args.config == "c3":
+            workload = ("config3: config2 inputs, lanczos3, split precision (FP64 orbit/Newton/slant "
+                        "range, FP32 resampling/facet/flattening), gamma0 flatten, LIA+mask")
 
     def barrier():
         if dist is not None:
@@ -222,7 +230,8 @@ def run_ours(args):
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_k, 4)}
                for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
 
-    e2e = run_e2e(args, sd, sc, ctx, stream, barrier, dist) if (args.config == "c2" and args.e2e) else None
+    e2e = run_e2e(args, sd, sc, ctx, stream, barrier, dist) if (args.config in ("c2", "c3") and args.e2e) else None
+    accuracy = split_accuracy(sd, sc, ctx, stream) if args.config == "c3" else None
 
     if rank == 0:
         out = {
@@ -237,6 +246,8 @@ def run_ours(args):
             "gpu_launches": gpu_launches, "clocks": clk.summary(),
             "e2e": e2e,
         }
+        if accuracy is not None:
+            out["accuracy_vs_fp64"] = accuracy
         if args.cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline(args, sc, res, merged_px)
         print(json.dumps(out), flush=True)
@@ -244,6 +255,34 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     ctx.close()
+
+
+def split_accuracy(sd, sc, ctx, stream):
+    """Split-precision result against the FP64 GPU path on the full scene
+    (the FP64 path is checked against the oracle by the test suite), plus
+    the FP64 path's own step time on the same inputs."""
+    import copy
+    import torch
+    m = sd.calibrate_deburst_merge(sc.swaths, ctx=ctx)
+    split = sd.terrain_correction(m, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx, return_times=True)
+    cfg64 = copy.copy(sc.config)
+    cfg64.precision = sd.Precision.FP64
+    sd.terrain_correction(m, sc.scene, sc.dem, sc.grids, cfg64, ctx=ctx)  # warm
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ref = sd.terrain_correction(m, sc.scene, sc.dem, sc.grids, cfg64, ctx=ctx, return_times=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    from sardine_b200.accuracy import compare_geocoded
+    rep = compare_geocoded(split, ref, split.azimuth_time_us, ref.azimuth_time_us,
+                           sc.scene.sub_swaths[0].azimuth_time_interval_s)
+    rep["fp64_tc_ms"] = e0.elapsed_time(e1)
+    rep["fp64_tc_px_per_s"] = ref.total_pixel_count / (rep["fp64_tc_ms"] / 1e3)
+    rep["counters_equal"] = (split.newton_iter_histogram == ref.newton_iter_histogram and
+                             split.valid_pixel_count == ref.valid_pixel_count and
+                             split.flat_masked_count == ref.flat_masked_count)
+    return rep
 
 
 def ctypes_fp64_peak(ctx):
@@ -440,7 +479,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--ref-rows", type=int, default=16)

@@ -382,14 +382,28 @@ int sd_tc_output_grid(sd_ctx *ctx, const sd_scene *scene, const sd_tc_config *cf
                       sd_geocoded_info *info);
 /* terrain_correction (terrain_correction.rs:1245-1836).  out_data is
  * rows x cols f32; out_cos_lia / out_mask are filled when cfg->compute_lia
- * (otherwise they may be NULL).  In SD_PRECISION_SPLIT mode, out_err (may be
- * NULL) receives per-pixel geolocation error estimates in pixels. */
+ * (otherwise they may be NULL).  cfg->precision selects the FP64 path
+ * (reference arithmetic) or the split-precision path (SD_PRECISION_SPLIT:
+ * same converged azimuth times, mask and counters; FP32 resampling,
+ * facet, LIA and flattening). */
 int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image,
                           const sd_scene *scene, const sd_dem *dem,
                           const sd_geoid *geoid, const sd_geo_grid_point *grid,
                           uint64_t n_grid, const sd_tc_config *cfg,
                           float *out_data, float *out_cos_lia, uint8_t *out_mask,
                           sd_geocoded_info *info);
+/* sd_terrain_correction plus the converged zero-Doppler azimuth time of
+ * every output pixel in integer microseconds (INT64_MIN where the solve did
+ * not converge, the DEM has no height or the orbit refused the time), for
+ * measuring geolocation against another implementation.  No counterpart in
+ * the reference (its per-pixel time is internal to the loop at
+ * terrain_correction.rs:1513-1740). */
+int sd_terrain_correction_with_times(sd_ctx *ctx, const sd_radar_image *image,
+                                     const sd_scene *scene, const sd_dem *dem,
+                                     const sd_geoid *geoid, const sd_geo_grid_point *grid,
+                                     uint64_t n_grid, const sd_tc_config *cfg,
+                                     float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                                     int64_t *out_azimuth_time_us, sd_geocoded_info *info);
 
 /* ── Diagnostics ──────────────────────────────────────────────────────────
  * Runs an FP64 FMA-chain kernel for about `iters` dependent FMAs per thread

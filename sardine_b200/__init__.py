@@ -33,7 +33,7 @@ from . import types as T
 from ._lib import Context, default_context, lib
 from .types import (BoundingBox, BurstEntry, CalibrationVector, DeburstArray, DemGrid,
                     GeocodedImage, GeoidModel, GeolocationGridPoint, MergedSigma0, NoiseAzimuthVector,
-                    NoiseRangeVector, OrbitData, OutputCrs, ResamplingKernel, SceneMetadata,
+                    NoiseRangeVector, OrbitData, OutputCrs, Precision, ResamplingKernel, SceneMetadata,
                     Sigma0Array, SpeckleFilter, SubSwathMetadata, SwathCalibration, SwathInput,
                     SwathNoise, TerrainCorrectionConfig)
 
@@ -118,9 +118,9 @@ def _is_torch_cuda(a) -> bool:
 def _empty_like_kind(ref, shape, dtype: str):
     if _is_torch_cuda(ref):
         import torch
-        tdt = {"f4": torch.float32, "u1": torch.uint8, "i2": torch.int16}[dtype]
+        tdt = {"f4": torch.float32, "u1": torch.uint8, "i2": torch.int16, "i8": torch.int64}[dtype]
         return torch.empty(shape, dtype=tdt, device=ref.device)
-    return np.empty(shape, dtype={"f4": np.float32, "u1": np.uint8, "i2": np.int16}[dtype])
+    return np.empty(shape, dtype={"f4": np.float32, "u1": np.uint8, "i2": np.int16, "i8": np.int64}[dtype])
 
 
 def _prep(a, dtype):
@@ -166,12 +166,14 @@ def tc_output_grid(scene: SceneMetadata, config: TerrainCorrectionConfig,
 
 def terrain_correction(merged: MergedSigma0, scene: SceneMetadata, dem: DemGrid, grids,
                        config: TerrainCorrectionConfig, ctx: Optional[Context] = None,
-                       out=None) -> GeocodedImage:
+                       out=None, return_times: bool = False) -> GeocodedImage:
     """terrain_correction (terrain_correction.rs:1245-1836) on the GPU.
 
     `grids` is a sequence of (sub-swath id, geolocation points); the LUT uses
     IW2's points, else the first sub-swath's.  `out` may supply preallocated
-    (data, cos_lia, mask) buffers of the output-grid shape."""
+    (data, cos_lia, mask) buffers of the output-grid shape.  With
+    `return_times`, the result also carries the converged zero-Doppler time of
+    every pixel (`azimuth_time_us`, int64 microseconds, INT64_MIN where none)."""
     ctx = _ctx(ctx)
     keep = T._Keep()
     merged_data = _prep(merged.data, np.float32)
@@ -199,11 +201,19 @@ def terrain_correction(merged: MergedSigma0, scene: SceneMetadata, dem: DemGrid,
         data = _empty_like_kind(merged_data, (rows, cols), "f4")
         cos = _empty_like_kind(merged_data, (rows, cols), "f4") if config.compute_lia else None
         mask = _empty_like_kind(merged_data, (rows, cols), "u1") if config.compute_lia else None
-    rc = lib().sd_terrain_correction(ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo),
-                                     g, len(pts), C.byref(cfg), T.ptr(data), T.ptr(cos), T.ptr(mask),
-                                     C.byref(info))
+    times = _empty_like_kind(merged_data, (rows, cols), "i8") if return_times else None
+    if return_times:
+        rc = lib().sd_terrain_correction_with_times(
+            ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo), g, len(pts), C.byref(cfg),
+            T.ptr(data), T.ptr(cos), T.ptr(mask), T.ptr(times), C.byref(info))
+    else:
+        rc = lib().sd_terrain_correction(ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo),
+                                         g, len(pts), C.byref(cfg), T.ptr(data), T.ptr(cos), T.ptr(mask),
+                                         C.byref(info))
     _check(ctx, rc, TerrainCorrectionError)
-    return GeocodedImage.from_info(info, config.crs, data, cos, mask)
+    res = GeocodedImage.from_info(info, config.crs, data, cos, mask)
+    res.azimuth_time_us = times
+    return res
 
 
 # ── deburst / calibration / merge ──────────────────────────────────────────

@@ -40,6 +40,7 @@ _SIGS = {
     "sd_calibrate_deburst_merge": (C.c_int, [P, C.c_int32, P, P, P, P]),
     "sd_tc_output_grid": (C.c_int, [P, P, P, P]),
     "sd_terrain_correction": (C.c_int, [P, P, P, P, P, P, C.c_uint64, P, P, P, P, P]),
+    "sd_terrain_correction_with_times": (C.c_int, [P, P, P, P, P, P, C.c_uint64, P, P, P, P, P, P]),
     "sd_measure_fp64_peak": (C.c_int, [P, C.c_int32, P]),
     "sd_measure_fp32_peak": (C.c_int, [P, C.c_int32, P]),
 }

@@ -131,6 +131,7 @@ struct TcDev {
   float *out;
   float *cos_lia;
   uint8_t *mask;
+  int64_t *az_time;  // optional: converged azimuth time per pixel (INT64_MIN if none)
   int *flags;
   unsigned long long *counters;
   unsigned long long *trange;  // [0] = min, [1] = max (biased by 2^63)
@@ -323,35 +324,154 @@ __device__ float sample_bicubic(const float *d, uint64_t nl, uint64_t ns, double
   return (float)acc;
 }
 
-__device__ float sample_lanczos(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+// ── split precision (SD_PRECISION_SPLIT) ─────────────────────────────────────
+// Everything that decides an integer outcome stays FP64: the orbit table,
+// every Newton residual (so the microsecond chain, the converged times and
+// the Newton histogram are those of the FP64 path), the target ECEF, the
+// slant range, the image coordinates and the footprint test.  Resampling
+// weights and sums, the NESZ sample, the facet normal (built from chords
+// between the cardinal neighbours in a frame local to the pixel, never from
+// absolute ECEF coordinates), cos(LIA) and the flattening weight run in FP32.
+// A mask decision FP32 cannot settle (flattening weight within 1e-4
+// relative of 0.05 or 2.0, local projection within 1e-4 of the facet area
+// from zero, sigma0 within 1e-5 relative of the NESZ threshold) is redone
+// with the FP64 candidate, so the mask equals the FP64 path's.
+// The build compiles with --fmad=false (the FP64 path must not contract);
+// the FP32 code contracts explicitly with fmaf.
+
+__device__ __forceinline__ float keys_weight_f(float t) {  // keys_weight, Horner form
+  t = fabsf(t);
+  if (t < 1.f) return fmaf(fmaf(1.5f, t, -2.5f), t * t, 1.f);
+  if (t < 2.f) return fmaf(fmaf(fmaf(-0.5f, t, 2.5f), t, -4.f), t, 2.f);
+  return 0.f;
+}
+
+// Lanczos-3 weights (terrain_correction.rs:938-952) of the taps li = -2..3
+// at x = f - li.  sin(pi x) = (-1)^li sin(pi f) and sin(pi x/3) =
+// sin(pi f/3) cos(pi li/3) - cos(pi f/3) sin(pi li/3), so the six weights
+// take one sinpi and one sincospi.
+template <typename T>
+__device__ __forceinline__ void lanczos6(T f, T w[6]);
+
+template <>
+__device__ __forceinline__ void lanczos6<float>(float f, float w[6]) {
+  const float s1 = sinpif(f);
+  float s3, c3;
+  sincospif(f * (1.f / 3.f), &s3, &c3);
+  const float h = 0.866025403784438647f;  // sin(pi/3)
+  const float cl[6] = {-0.5f, 0.5f, 1.f, 0.5f, -0.5f, -1.f};
+  const float sl[6] = {-h, -h, 0.f, h, h, 0.f};
+  const float k = (float)(3.0 / (kPi * kPi));
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const int li = j - 2;
+    const float x = f - (float)li;
+    const float ax = fabsf(x);
+    const float s = (li & 1) ? -s1 : s1;
+    w[j] = ax < 1e-10f ? 1.f : (ax < 3.f ? k * s * (s3 * cl[j] - c3 * sl[j]) / (x * x) : 0.f);
+  }
+}
+
+template <>
+__device__ __forceinline__ void lanczos6<double>(double f, double w[6]) {
+  const double s1 = sinpi(f);
+  double s3, c3;
+  sincospi(f * (1.0 / 3.0), &s3, &c3);
+  const double h = 0.86602540378443864676;
+  const double cl[6] = {-0.5, 0.5, 1.0, 0.5, -0.5, -1.0};
+  const double sl[6] = {-h, -h, 0.0, h, h, 0.0};
+  const double k = 3.0 / (kPi * kPi);
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const int li = j - 2;
+    const double x = f - (double)li;
+    const double ax = fabs(x);
+    const double s = (li & 1) ? -s1 : s1;
+    w[j] = ax < 1e-10 ? 1.0 : (ax < 3.0 ? k * s * (s3 * cl[j] - c3 * sl[j]) / (x * x) : 0.0);
+  }
+}
+
+__device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+  int64_t max_line = nl == 0 ? 0 : (int64_t)nl - 1;
+  int64_t max_sample = ns == 0 ? 0 : (int64_t)ns - 1;
+  int64_t l0 = clampi(f2i64(floor(line)), 0, max_line);
+  int64_t l1 = l0 + 1 < max_line ? l0 + 1 : max_line;
+  int64_t s0 = clampi(f2i64(floor(sample)), 0, max_sample);
+  int64_t s1 = s0 + 1 < max_sample ? s0 + 1 : max_sample;
+  const float dl = (float)(line - (double)l0), ds = (float)(sample - (double)s0);
+  float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
+  float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
+  if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
+  const float top = fmaf(v01 - v00, ds, v00);
+  const float bot = fmaf(v11 - v10, ds, v10);
+  return fmaf(bot - top, dl, top);
+}
+
+__device__ float sample_bicubic_f(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
-  double ws[6];
+  const float dl = (float)(line - (double)lf), ds = (float)(sample - (double)sf);
+  float ws[4];
+  int64_t cols[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ws[k] = keys_weight_f((float)(k - 1) - ds);
+    cols[k] = clampi(sf + k - 1, 0, max_s);
+  }
+  float acc = 0.f;
+#pragma unroll
+  for (int li = -1; li <= 2; ++li) {
+    int64_t row = clampi(lf + li, 0, max_l);
+    const float wl = keys_weight_f((float)li - dl);
+    float racc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) return NAN;
+      racc = fmaf(v, ws[k], racc);
+    }
+    acc = fmaf(racc, wl, acc);
+  }
+  return acc;
+}
+
+template <typename T>
+__device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
+  T wl[6], ws[6];
+  lanczos6<T>((T)(line - (double)lf), wl);
+  lanczos6<T>((T)(sample - (double)sf), ws);
   int64_t cols[6];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) {
-    ws[k] = lanczos_weight(sample - (double)(sf + k - 2));
-    cols[k] = clampi(sf + k - 2, 0, max_s);
-  }
-  double acc = 0.0;
+  for (int k = 0; k < 6; ++k) cols[k] = clampi(sf + k - 2, 0, max_s);
+  T acc = 0;
 #pragma unroll
-  for (int li = -2; li <= 3; ++li) {
-    int64_t row = clampi(lf + li, 0, max_l);
-    double wl = lanczos_weight(line - (double)(lf + li));
+  for (int j = 0; j < 6; ++j) {
+    int64_t row = clampi(lf + j - 2, 0, max_l);
+    T racc = 0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
       float v = ldf(d, row * (int64_t)ns + cols[k]);
       if (v != v) return NAN;
-      acc += (double)v * wl * ws[k];
+      racc += (T)v * ws[k];
     }
+    acc += racc * wl[j];
   }
   return (float)acc;
 }
 
 template <int KERNEL>
+__device__ __forceinline__ float resample_f(const TcDev &p, double line, double sample) {
+  return KERNEL == SD_RESAMPLE_BICUBIC    ? sample_bicubic_f(p.img, p.lines, p.samples, line, sample)
+         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos_t<float>(p.img, p.lines, p.samples, line, sample)
+                                          : sample_bilinear_f(p.img, p.lines, p.samples, line, sample);
+}
+
+template <int KERNEL>
 __device__ __forceinline__ float resample(const TcDev &p, double line, double sample) {
   return KERNEL == SD_RESAMPLE_BICUBIC    ? sample_bicubic(p.img, p.lines, p.samples, line, sample)
-         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos(p.img, p.lines, p.samples, line, sample)
+         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos_t<double>(p.img, p.lines, p.samples, line, sample)
                                           : sample_bilinear(p.img, p.lines, p.samples, line, sample);
 }
 
@@ -455,7 +575,7 @@ struct CandPre {  // steps 4-6 of the reference loop for one candidate
   bool inside;
 };
 
-template <int KERNEL>
+template <int KERNEL, bool SPLIT>
 __device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
   CandPre c;
   double slant = norm3(sub3(P, S));
@@ -464,7 +584,8 @@ __device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
   c.sample = (slant - p.near_range) / p.rps;
   c.inside = !(c.line < -0.5 || c.line > ((double)p.lines - 0.5) || c.sample < -0.5 ||
                c.sample > ((double)p.samples - 0.5));
-  c.sigma0 = c.inside ? resample<KERNEL>(p, c.line, c.sample) : NAN;
+  if (c.inside) c.sigma0 = SPLIT ? resample_f<KERNEL>(p, c.line, c.sample) : resample<KERNEL>(p, c.line, c.sample);
+  else c.sigma0 = NAN;
   if (c.sigma0 != c.sigma0) c.inside = false;
   return c;
 }
@@ -506,6 +627,132 @@ __device__ CandOut cand_post(const TcDev &p, const CandPre &c, V3 P, V3 S, const
     }
   }
   return {sigma0, cosv, (uint8_t)SD_MASK_VALID, 0};
+}
+
+// Facet in FP32: the east-west and north-south chords between the cardinal
+// neighbours, expanded about the centre (latitude phi, longitude lam,
+// prime-vertical radius N(phi)) to first order in the angular steps a, b, c,
+// d (~1.6e-6 rad); the dropped terms are below 1e-7 m on chords of ~20 m.
+//   E-W: cos(phi) (cos(lam) dh - sin(lam) q, sin(lam) dh + cos(lam) q),
+//        sin(phi) dh,  dh = he - hw, q = (N + he) a + (N + hw) b
+//   N-S: (cos(lam) An, sin(lam) An, Zn) with
+//        An = cos(phi) (hn - hs + N'(c + d)) - sin(phi) ((N + hn) c + (N + hs) d)
+//        Zn = sin(phi) (hn - hs + B'(c + d)) + cos(phi) ((B + hn) c + (B + hs) d)
+//        B = N (1 - e^2), N' = dN/dphi = N e^2 sin cos / (1 - e^2 sin^2).
+struct FacetF {
+  bool ok;
+  float nx, ny, nz, area;
+};
+
+__device__ FacetF pixel_facet_f(const TcDev &p, const PixGeo &g) {
+  FacetF f{};
+  const double sd = p.step_deg;
+  const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
+  float he, hw, hn, hs;
+  bool ok;
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    const double k = kPi / 180.0;
+    double x, y;
+    utm_local_step(u, g.loc, 0.0, (lon_e - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &he);
+    utm_local_step(u, g.loc, 0.0, (lon_w - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hw) && ok;
+    utm_local_step(u, g.loc, (lat_n - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hn) && ok;
+    utm_local_step(u, g.loc, (lat_s - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hs) && ok;
+  } else {
+    ok = dem_at_lonlat(p.dem, lon_e, g.lat, &he);
+    ok = dem_at_lonlat(p.dem, lon_w, g.lat, &hw) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_n, &hn) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_s, &hs) && ok;
+  }
+  f.ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
+  if (!f.ok) return f;
+  const float a = (float)(deg2rad_ecef(lon_e) - g.lo), b = (float)(g.lo - deg2rad_ecef(lon_w));
+  const float c = (float)(deg2rad_ecef(lat_n) - g.la), d = (float)(g.la - deg2rad_ecef(lat_s));
+  const float sp = (float)g.sla, cp = (float)g.cla, sl = (float)g.slo, cl = (float)g.clo;
+  const float e2 = (float)WGS84_E2;
+  const float den = 1.f - e2 * sp * sp;
+  const float N = (float)WGS84_A * rsqrtf(den);
+  const float dN = N * e2 * sp * cp / den;
+  const float B = N * (1.f - e2), dB = dN * (1.f - e2);
+  const float dh = he - hw;
+  const float q = fmaf(N + he, a, (N + hw) * b);
+  const float ex = cp * (cl * dh - sl * q), ey = cp * (sl * dh + cl * q), ez = sp * dh;
+  const float dv = hn - hs;
+  const float An = cp * fmaf(dN, c + d, dv) - sp * fmaf(N + hn, c, (N + hs) * d);
+  const float nx = cl * An, ny = sl * An;
+  const float nz = sp * fmaf(dB, c + d, dv) + cp * fmaf(B + hn, c, (B + hs) * d);
+  f.nx = ey * nz - ez * ny;
+  f.ny = ez * nx - ex * nz;
+  f.nz = ex * ny - ey * nx;
+  f.area = sqrtf(f.nx * f.nx + f.ny * f.ny + f.nz * f.nz);
+  return f;
+}
+
+// cand_post in split precision; *redo is set when a mask decision falls
+// inside the FP32 error margin and the FP64 candidate must decide.
+__device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g, V3 S, const FacetF &f,
+                               float flat_area, bool *redo) {
+  CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
+  *redo = false;
+  if (!c.inside) return o;
+  float sigma0 = c.sigma0;
+  float cosv = NAN;
+  if (p.need_geom) {
+    if (!f.ok) {
+      if (p.flatten) return {NAN, cosv, (uint8_t)SD_MASK_DEM_NEIGHBOUR_MISSING, 5};
+    } else {
+      const float lx = (float)(S.x - g.P.x), ly = (float)(S.y - g.P.y), lz = (float)(S.z - g.P.z);
+      const float il = rsqrtf(lx * lx + ly * ly + lz * lz);
+      const float lp = (f.nx * lx + f.ny * ly + f.nz * lz) * il;
+      if (fabsf(lp) <= 1e-4f * f.area) { *redo = true; return o; }
+      if (lp <= 0.f || f.area == 0.f) {
+        if (p.flatten) return {NAN, cosv, (uint8_t)SD_MASK_SHADOW, 5};
+      } else {
+        const float w = lp / flat_area;
+        if (fabsf(w - 0.05f) <= 5e-6f || fabsf(w - 2.0f) <= 2e-4f) { *redo = true; return o; }
+        cosv = fminf(fmaxf(lp / f.area, 0.f), 1.f);
+        if (w < 0.05f || w > 2.0f) {
+          if (p.flatten) return {NAN, cosv, (uint8_t)(w > 2.0f ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING), 5};
+        } else if (p.flatten) {
+          sigma0 /= w;
+        }
+      }
+    }
+  }
+  if (p.nesz_mask) {
+    float nz = sample_bilinear_f(p.nesz, p.lines, p.samples, c.line, c.sample);
+    if (nz == nz) {
+      float thr = nz * p.nesz_factor;
+      if (fabsf(sigma0 - thr) <= 1e-5f * fabsf(thr)) { *redo = true; return o; }
+      if (sigma0 <= thr) return {NAN, cosv, (uint8_t)SD_MASK_NOISE_MASKED, 6};
+    }
+  }
+  return {sigma0, cosv, (uint8_t)SD_MASK_VALID, 0};
+}
+
+// One candidate's output from scratch (exact-path pixels, and split-precision
+// candidates whose mask FP32 cannot settle).
+template <int KERNEL>
+__device__ CandOut cand_fp64(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area) {
+  CandPre pre = cand_pre<KERNEL, false>(p, g.P, S, t);
+  Facet f{};
+  if (pre.inside && p.need_geom) f = pixel_facet(p, g);
+  return cand_post(p, pre, g.P, S, f, flat_area);
+}
+
+template <int KERNEL, bool SPLIT>
+__device__ CandOut cand_full(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area) {
+  if (!SPLIT) return cand_fp64<KERNEL>(p, g, S, t, flat_area);
+  CandPre pre = cand_pre<KERNEL, true>(p, g.P, S, t);
+  FacetF f{};
+  if (pre.inside && p.need_geom) f = pixel_facet_f(p, g);
+  bool redo;
+  CandOut o = cand_post_f(p, pre, g, S, f, (float)flat_area, &redo);
+  return redo ? cand_fp64<KERNEL>(p, g, S, t, flat_area) : o;
 }
 
 // ── per-pixel stores ─────────────────────────────────────────────────────────
@@ -561,7 +808,7 @@ constexpr int MAIN_THREADS = 128;
 constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
 
 // ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
-template <int KERNEL>
+template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(MAIN_THREADS, 4) k_main(TcDev p, int fast) {
   __shared__ Slot slot[MAIN_THREADS];
   const int tid = threadIdx.x;
@@ -683,24 +930,42 @@ __global__ void __launch_bounds__(MAIN_THREADS, 4) k_main(TcDev p, int fast) {
     for (int k = 0; k < 2; ++k) {
       const Ent &e = k == 0 ? e0 : e1;
       if ((fmask >> k) & 1) {
-        pre[k] = cand_pre<KERNEL>(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
+        pre[k] = cand_pre<KERNEL, SPLIT>(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
         need = need || pre[k].inside;
       } else {
         pre[k].inside = false;
       }
     }
-    Facet f{};
-    if (need && p.need_geom) f = pixel_facet(p, g);
     const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+    if constexpr (SPLIT) {
+      FacetF f{};
+      if (need && p.need_geom) f = pixel_facet_f(p, g);
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const Ent &e = k == 0 ? e0 : e1;
-      if (!((fmask >> k) & 1)) continue;
-      CandOut o = cand_post(p, pre[k], g.P, V3{e.px, e.py, e.pz}, f, flat_area);
-      rec.data[k] = o.data;
-      rec.cos[k] = o.cos;
-      rec.omask[k] = o.mask;
-      rec.ocls[k] = o.cls;
+      for (int k = 0; k < 2; ++k) {
+        const Ent &e = k == 0 ? e0 : e1;
+        if (!((fmask >> k) & 1)) continue;
+        const V3 S{e.px, e.py, e.pz};
+        bool redo;
+        CandOut o = cand_post_f(p, pre[k], g, S, f, (float)flat_area, &redo);
+        if (redo) o = cand_fp64<KERNEL>(p, g, S, fb + k, flat_area);
+        rec.data[k] = o.data;
+        rec.cos[k] = o.cos;
+        rec.omask[k] = o.mask;
+        rec.ocls[k] = o.cls;
+      }
+    } else {
+      Facet f{};
+      if (need && p.need_geom) f = pixel_facet(p, g);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const Ent &e = k == 0 ? e0 : e1;
+        if (!((fmask >> k) & 1)) continue;
+        CandOut o = cand_post(p, pre[k], g.P, V3{e.px, e.py, e.pz}, f, flat_area);
+        rec.data[k] = o.data;
+        rec.cos[k] = o.cos;
+        rec.omask[k] = o.mask;
+        rec.ocls[k] = o.cls;
+      }
     }
     cc |= CF_HASOUT;
   }
@@ -721,7 +986,7 @@ struct WState {
 // The reference solve of pixel (r, c) from seed s, for pixels the
 // precomputed records do not cover.  With `write`, it also stores the
 // pixel's outputs when the converged time has none precomputed.
-template <int KERNEL>
+template <int KERNEL, bool SPLIT>
 __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s, uint32_t cc, int64_t fb,
                               bool write, uint8_t *sel) {
   const uint64_t i = r * p.cols + c;
@@ -755,15 +1020,13 @@ __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s,
     OrbitState os;
     double vsq;
     orbit_at(p.orb, z.t, &os, &vsq);
-    CandPre pre = cand_pre<KERNEL>(p, g.P, os.pos, z.t);
-    Facet f{};
-    if (pre.inside && p.need_geom) f = pixel_facet(p, g);
-    CandOut o = cand_post(p, pre, g.P, os.pos, f, p.need_geom ? p.row_flat[r] : 0.0);
+    CandOut o = cand_full<KERNEL, SPLIT>(p, g, os.pos, z.t, p.need_geom ? p.row_flat[r] : 0.0);
     p.out[i] = o.data;
     if (p.compute_lia) {
       p.cos_lia[i] = o.cos;
       p.mask[i] = o.mask;
     }
+    if (p.az_time) p.az_time[i] = z.t;
     p.rec[i].ocls[0] = o.cls;
   }
   return {1, z.t};
@@ -771,7 +1034,7 @@ __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s,
 
 // Walk columns [b, e) of row r from state st (terrain_correction.rs:
 // 1443-1580), any pixel kind.  fb is read only where a seed value is needed.
-template <int KERNEL>
+template <int KERNEL, bool SPLIT>
 __device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, WState st, bool write) {
   const uint64_t base = r * p.cols;
   uint32_t prev_cc = b > 0 ? p.cc[base + b - 1] : CF_DEMMISS;
@@ -793,7 +1056,7 @@ __device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, W
         sel = (uint8_t)((((code >> 2) & 3u) == 1u ? SEL_NONCONV : SEL_DEGEN) | (code & 0xF0u));
       } else {
         const int64_t s = st.kind == 0 ? p.rec[base + c - 1].fb + st.v : st.v;
-        st = exact_pixel<KERNEL>(p, r, c, s, cc, p.rec[base + c].fb, write, &sel);
+        st = exact_pixel<KERNEL, SPLIT>(p, r, c, s, cc, p.rec[base + c].fb, write, &sel);
       }
     }
     if (write) p.sel[base + c] = sel;
@@ -813,7 +1076,7 @@ __device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, W
 // kind is (re)done by walk_seg.
 constexpr int SCAN_WARPS = 4;
 
-template <int KERNEL>
+template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(TcDev p) {
   __shared__ uint32_t sbuf[SCAN_WARPS][32][33];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -831,7 +1094,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(TcDev p) {
       ++c;
     }
     if (c < n) {
-      st0 = walk_seg<KERNEL>(p, r, c, c + 1, WState{1, p.row_guess[r]}, true);
+      st0 = walk_seg<KERNEL, SPLIT>(p, r, c, c + 1, WState{1, p.row_guess[r]}, true);
       c0 = c + 1;
     }
   }
@@ -872,8 +1135,8 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(TcDev p) {
   }
   WState ex0 = {0, 0}, ex1 = {0, 1};
   if (b < e) {
-    ex0 = (bad & 1) ? walk_seg<KERNEL>(p, r, b, e, WState{0, 0}, false) : WState{0, s0};
-    ex1 = (bad & 2) ? walk_seg<KERNEL>(p, r, b, e, WState{0, 1}, false) : WState{0, s1};
+    ex0 = (bad & 1) ? walk_seg<KERNEL, SPLIT>(p, r, b, e, WState{0, 0}, false) : WState{0, s0};
+    ex1 = (bad & 2) ? walk_seg<KERNEL, SPLIT>(p, r, b, e, WState{0, 1}, false) : WState{0, s1};
   }
   // phase 2: compose the lanes' maps in order
   WState st = st0, entry{2, 0};
@@ -883,7 +1146,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(TcDev p) {
       entry = st;
       if (b < e) {
         if (st.kind == 0) nx = st.v == 0 ? ex0 : ex1;
-        else nx = walk_seg<KERNEL>(p, r, b, e, st, false);
+        else nx = walk_seg<KERNEL, SPLIT>(p, r, b, e, st, false);
       }
     }
     st.kind = __shfl_sync(0xffffffffu, nx.kind, j);
@@ -917,7 +1180,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(TcDev p) {
     }
     __syncwarp();
   }
-  if (b < e && !regular) walk_seg<KERNEL>(p, r, b, e, entry, true);
+  if (b < e && !regular) walk_seg<KERNEL, SPLIT>(p, r, b, e, entry, true);
 }
 
 // ── K5: final rasters, counters and Newton histogram ────────────────────────
@@ -939,6 +1202,7 @@ __global__ void __launch_bounds__(256) k_select(TcDev p) {
         p.cos_lia[i] = rc.cos[code];
         p.mask[i] = rc.omask[code];
       }
+      if (p.az_time) p.az_time[i] = rc.fb + code;
     } else if (code == SEL_DONE) {
       counter = p.rec[i].ocls[0];
       atomicAdd(&s_cnt[kCounters + it], 1u);
@@ -947,6 +1211,7 @@ __global__ void __launch_bounds__(256) k_select(TcDev p) {
                   : code == SEL_DEGEN ? SD_MASK_DEGENERATE_GEOMETRY
                                       : SD_MASK_DEM_MISSING;
       counter = code == SEL_NONCONV ? 3 : (code == SEL_DEGEN ? 4 : 1);
+      if (p.az_time) p.az_time[i] = INT64_MIN;
       p.out[i] = NAN;
       if (p.compute_lia) {
         p.cos_lia[i] = NAN;
@@ -1024,11 +1289,10 @@ extern "C" int sd_tc_output_grid(sd_ctx *ctx, const sd_scene *scene, const sd_tc
   return rc;
 }
 
-extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene,
-                                     const sd_dem *dem, const sd_geoid *geoid,
-                                     const sd_geo_grid_point *grid, uint64_t n_grid,
-                                     const sd_tc_config *cfg, float *out_data, float *out_cos_lia,
-                                     uint8_t *out_mask, sd_geocoded_info *info) {
+static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene, const sd_dem *dem,
+                  const sd_geoid *geoid, const sd_geo_grid_point *grid, uint64_t n_grid,
+                  const sd_tc_config *cfg, float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                  int64_t *out_times, sd_geocoded_info *info) {
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!image || !scene || !dem || !geoid || !cfg || !info || !out_data)
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null argument");
@@ -1058,6 +1322,8 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
   SD_TRY(sd_tc_output_grid(ctx, scene, cfg, info));
   if (cfg->projector_anchors <= 0)
     return set_error(ctx, SD_ERR_TC_CONFIG, "SARDINE_TC_PROJECTOR_ANCHORS must be >= 1 (default 256)");
+  if (cfg->precision != SD_PRECISION_FP64 && cfg->precision != SD_PRECISION_SPLIT)
+    return set_error(ctx, SD_ERR_TC_CONFIG, "unknown precision mode %d", cfg->precision);
   if (dem->width < 2 || dem->height < 2 || !(dem->pixel_size > 0.0))
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "DEM grid must be at least 2x2 with positive spacing");
   if (image->lines == 0 || image->samples == 0)
@@ -1215,9 +1481,12 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
     SD_TRY(stage_out(ctx, "tc.cos", out_cos_lia, npx * sizeof(float), &d_cos));
     SD_TRY(stage_out(ctx, "tc.mask", out_mask, npx, &d_mask));
   }
+  void *d_times = nullptr;
+  if (out_times) SD_TRY(stage_out(ctx, "tc.times", out_times, npx * sizeof(int64_t), &d_times));
   p.out = (float *)d_out;
   p.cos_lia = (float *)d_cos;
   p.mask = (uint8_t *)d_mask;
+  p.az_time = (int64_t *)d_times;
   p.flags = ctx->d_flags;
   p.counters = ctx->d_counters;
   SD_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, 64 * sizeof(int), st));
@@ -1231,22 +1500,27 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
   if (bpr * p.rows > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "output grid too large");
   const unsigned main_grid = (unsigned)(bpr * p.rows);
   const unsigned scan_grid = grid_for(p.rows * 32, SCAN_WARPS * 32);
-  switch (p.resampling) {
-#define SD_TC_LAUNCH(K, NAME)                                                    \
-  case K:                                                                        \
+  const bool split = cfg->precision == SD_PRECISION_SPLIT;
+#define SD_TC_LAUNCH(K, S, NAME)                                                 \
+  do {                                                                           \
     SD_TIMED_BEGIN(ctx, "k_main<" NAME ">");                                     \
-    k_main<K><<<main_grid, MAIN_THREADS, 0, st>>>(p, fast);                      \
+    k_main<K, S><<<main_grid, MAIN_THREADS, 0, st>>>(p, fast);                   \
     SD_LAUNCHED(ctx);                                                            \
     SD_TIMED_BEGIN(ctx, "k_scan");                                               \
-    k_scan<K><<<scan_grid, SCAN_WARPS * 32, 0, st>>>(p);                                     \
+    k_scan<K, S><<<scan_grid, SCAN_WARPS * 32, 0, st>>>(p);                      \
     SD_LAUNCHED(ctx);                                                            \
-    break;
-    SD_TC_LAUNCH(SD_RESAMPLE_BICUBIC, "BICUBIC")
-    SD_TC_LAUNCH(SD_RESAMPLE_LANCZOS3, "LANCZOS3")
-    default:
-    SD_TC_LAUNCH(SD_RESAMPLE_BILINEAR, "BILINEAR")
-#undef SD_TC_LAUNCH
+  } while (0)
+  if (p.resampling == SD_RESAMPLE_BICUBIC) {
+    if (split) SD_TC_LAUNCH(SD_RESAMPLE_BICUBIC, true, "BICUBIC,SPLIT");
+    else SD_TC_LAUNCH(SD_RESAMPLE_BICUBIC, false, "BICUBIC");
+  } else if (p.resampling == SD_RESAMPLE_LANCZOS3) {
+    if (split) SD_TC_LAUNCH(SD_RESAMPLE_LANCZOS3, true, "LANCZOS3,SPLIT");
+    else SD_TC_LAUNCH(SD_RESAMPLE_LANCZOS3, false, "LANCZOS3");
+  } else {
+    if (split) SD_TC_LAUNCH(SD_RESAMPLE_BILINEAR, true, "BILINEAR,SPLIT");
+    else SD_TC_LAUNCH(SD_RESAMPLE_BILINEAR, false, "BILINEAR");
   }
+#undef SD_TC_LAUNCH
   SD_TIMED_BEGIN(ctx, "k_select");
   k_select<<<grid_for(npx, 256), 256, 0, st>>>(p);
   SD_LAUNCHED(ctx);
@@ -1266,6 +1540,7 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
     SD_TRY(finish_out(ctx, out_cos_lia, d_cos, npx * sizeof(float)));
     SD_TRY(finish_out(ctx, out_mask, d_mask, npx));
   }
+  if (out_times) SD_TRY(finish_out(ctx, out_times, d_times, npx * sizeof(int64_t)));
   info->valid_pixel_count = cnt[0];
   info->dem_missing_count = cnt[1];
   info->outside_footprint_count = cnt[2];
@@ -1277,4 +1552,25 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
   info->diag_exact_path_pixels = (uint64_t)flags[1];
   SD_TRY(sync(ctx));
   return SD_OK;
+}
+
+extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene,
+                                     const sd_dem *dem, const sd_geoid *geoid,
+                                     const sd_geo_grid_point *grid, uint64_t n_grid,
+                                     const sd_tc_config *cfg, float *out_data, float *out_cos_lia,
+                                     uint8_t *out_mask, sd_geocoded_info *info) {
+  return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, out_data, out_cos_lia, out_mask, nullptr,
+                info);
+}
+
+extern "C" int sd_terrain_correction_with_times(sd_ctx *ctx, const sd_radar_image *image,
+                                                const sd_scene *scene, const sd_dem *dem,
+                                                const sd_geoid *geoid, const sd_geo_grid_point *grid,
+                                                uint64_t n_grid, const sd_tc_config *cfg, float *out_data,
+                                                float *out_cos_lia, uint8_t *out_mask,
+                                                int64_t *out_azimuth_time_us, sd_geocoded_info *info) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!out_azimuth_time_us) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null time buffer");
+  return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, out_data, out_cos_lia, out_mask,
+                out_azimuth_time_us, info);
 }

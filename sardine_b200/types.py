@@ -350,6 +350,15 @@ class GeoidModel:
         return _abi.Geoid(_abi.GEOID_GRID, 0, g.ctypes.data)
 
 
+class Precision:
+    """Terrain-correction arithmetic: FP64 reproduces the reference; SPLIT
+    keeps the FP64 orbit, Newton residuals and slant range (same converged
+    times, mask and counters) and runs resampling, facet, LIA and flattening
+    in FP32."""
+    FP64 = _abi.PRECISION_FP64
+    SPLIT = _abi.PRECISION_SPLIT
+
+
 @dataclass
 class TerrainCorrectionConfig:
     """terrain_correction.rs:100-236; TerrainCorrectionConfig::new defaults."""
@@ -403,6 +412,7 @@ class GeocodedImage:
     mask: Any
     newton_iter_histogram: List[int]
     diag_exact_path_pixels: int = 0  # converged pixels computed on the row walk's exact path
+    azimuth_time_us: Any = None      # converged zero-Doppler time per pixel (INT64_MIN: none)
 
     def valid_fraction(self) -> float:
         return self.valid_pixel_count / self.total_pixel_count
