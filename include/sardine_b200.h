@@ -405,6 +405,64 @@ int sd_terrain_correction_with_times(sd_ctx *ctx, const sd_radar_image *image,
                                      float *out_data, float *out_cos_lia, uint8_t *out_mask,
                                      int64_t *out_azimuth_time_us, sd_geocoded_info *info);
 
+/* ── Device-resident scenes and batched tiles ──────────────────────────────
+ * No single counterpart in the reference: its terrain_correction
+ * (terrain_correction.rs:1245-1836) geocodes one scene onto one grid per call.
+ * Here a scene is uploaded once and any number of output tiles (windows of
+ * any size, over any resident scene) are geocoded per batch, each tile
+ * exactly as terrain_correction would geocode that tile's own grid (its rows
+ * seeded from the LUT, its own per-row flat area and UTM anchors). */
+typedef struct sd_scene_dev sd_scene_dev;
+
+/* Keeps the radar image (and NESZ), DEM, geoid, state vectors, the
+ * azimuth-time LUT of `grid` and an FP64 orbit table over the image's azimuth
+ * span in device memory.  Host buffers are copied; device buffers are
+ * borrowed (keep them alive until sd_scene_destroy).  Errors as
+ * sd_terrain_correction's argument checks. */
+int sd_scene_create(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene,
+                    const sd_dem *dem, const sd_geoid *geoid, const sd_geo_grid_point *grid,
+                    uint64_t n_grid, sd_scene_dev **out);
+/* Device bytes the scene owns (copies and orbit table). */
+uint64_t sd_scene_device_bytes(const sd_scene_dev *scene);
+/* Frees the scene; no batch that reads it may be in flight. */
+void sd_scene_destroy(sd_scene_dev *scene);
+
+typedef struct {
+    sd_scene_dev *scene;
+    sd_tc_config cfg;           /* pixel_spacing, crs and utm_zone give the tile's CRS */
+    double origin_x;            /* west edge: longitude (deg) or UTM easting (m) */
+    double origin_y;            /* north edge: latitude (deg) or UTM northing (m) */
+    uint64_t rows, cols;
+    int32_t speckle;            /* -1: none, else SD_SPECKLE_* applied after geocoding */
+    int32_t speckle_window;     /* odd, 3..15 (Refined Lee: 7) */
+    float enl, damping;
+    /* rows x cols outputs, device or host memory (host: pinned for overlap).
+     * With a speckle filter the tile is geocoded with a halo of half a
+     * window on every side and filtered before cropping, so the result
+     * equals the filter applied to the larger raster, then cropped. */
+    float *out_data;
+    float *out_cos_lia;         /* required when cfg.compute_lia */
+    uint8_t *out_mask;          /* required when cfg.compute_lia */
+} sd_tile;
+
+/* Enqueues the batch on the context's stream and returns; tiles may mix
+ * scenes, sizes, resampling kernels, precisions and filters.  One batch per
+ * context is in flight at a time (SD_ERR_BUSY otherwise). */
+int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n);
+/* SD_OK when the batch in flight has finished (or none is), SD_ERR_BUSY if not. */
+int sd_tc_tiles_poll(sd_ctx *ctx);
+/* Waits for the batch and fills infos[0..n) (counters, histogram, grid). */
+int sd_tc_tiles_finish(sd_ctx *ctx, sd_geocoded_info *infos, uint64_t n);
+/* sd_tc_tiles_launch + sd_tc_tiles_finish. */
+int sd_tc_tiles(sd_ctx *ctx, const sd_tile *tiles, uint64_t n, sd_geocoded_info *infos);
+/* Replay the tile stages as CUDA graphs of persistent kernels (captured on
+ * first use per variant; work tables keep fixed addresses up to 1024 tiles). */
+int sd_ctx_set_graphs(sd_ctx *ctx, int enable);
+/* Allocates the context's tile scratch up front: an arena of
+ * `tile_arena_bytes` plus the work tables of a 1024-tile batch, so batches
+ * that fit it run without device allocations. */
+int sd_ctx_reserve(sd_ctx *ctx, uint64_t tile_arena_bytes);
+
 /* ── Diagnostics ──────────────────────────────────────────────────────────
  * Runs an FP64 FMA-chain kernel for about `iters` dependent FMAs per thread
  * over the whole device and returns the achieved FP64 TFLOP/s. */

@@ -60,6 +60,8 @@ def _declare(L):
         "orc_guess_azimuth_time": (i64, [P, u64, d]),
         "orc_tc_output_grid": (C.c_int, [P, P, P]),
         "orc_terrain_correction": (C.c_int, [P, P, P, P, P, u64, P, u64, u64, P, P, P, P, P, P]),
+        "orc_terrain_correction_grid": (C.c_int, [P, P, P, P, P, u64, P, C.c_double, C.c_double, u64,
+                                                  u64, P, P, P, P, P]),
         "orc_compute_overlap_lines": (C.c_int, [P, P, d, u64, P]),
         "orc_deburst_plan": (C.c_int, [P, P, u64, u64, P, P, P, P, P]),
         "orc_deburst_subswath": (C.c_int, [P, u64, u64, P, P, u64, P]),
@@ -238,6 +240,36 @@ def terrain_correction(merged: T.MergedSigma0, scene: T.SceneMetadata, dem: T.De
     out = T.GeocodedImage.from_info(info, config.crs, data, cos, mask)
     if return_times:
         return out, t_us, iters
+    return out
+
+
+def terrain_correction_grid(merged: T.MergedSigma0, scene: T.SceneMetadata, dem: T.DemGrid, grids,
+                            config: T.TerrainCorrectionConfig, origin_x: float, origin_y: float,
+                            rows: int, cols: int, anchors: int = 256, return_times: bool = False):
+    """terrain_correction onto an explicit output grid: west edge origin_x,
+    north edge origin_y (config CRS units), rows x cols at the config spacing."""
+    keep = T._Keep()
+    img = merged.to_c()
+    sc = T.scene_to_c(scene, keep)
+    d = dem.to_c()
+    geo = config.geoid.to_c(keep)
+    pts = T.pick_lut_grid(grids)
+    g = T.grid_to_c(pts)
+    cfg = config.to_c(anchors)
+    info = _abi.GeocodedInfo()
+    data = np.empty((rows, cols), np.float32)
+    cos = np.empty((rows, cols), np.float32) if config.compute_lia else None
+    mask = np.empty((rows, cols), np.uint8) if config.compute_lia else None
+    t_us = np.empty((rows, cols), np.int64) if return_times else None
+    rc = lib().orc_terrain_correction_grid(
+        C.byref(img), C.byref(sc), C.byref(d), C.byref(geo), g, len(pts), C.byref(cfg),
+        float(origin_x), float(origin_y), rows, cols, data.ctypes.data,
+        cos.ctypes.data if cos is not None else None, mask.ctypes.data if mask is not None else None,
+        t_us.ctypes.data if t_us is not None else None, C.byref(info))
+    _check(rc, "terrain_correction_grid")
+    out = T.GeocodedImage.from_info(info, config.crs, data, cos, mask)
+    if return_times:
+        return out, t_us
     return out
 
 

@@ -743,11 +743,11 @@ int orc_tc_output_grid(const sd_scene *scene, const sd_tc_config *cfg, sd_geocod
 // band an exact sub-problem, which the CPU baseline uses as its sample.
 // out_t_us / out_iters (optional) receive the converged azimuth time and the
 // Newton iteration count per pixel (INT64_MIN / 0 where no solve converged).
-int orc_terrain_correction(const sd_radar_image *img, const sd_scene *scene, const sd_dem *dem_in,
-                           const sd_geoid *geoid, const sd_geo_grid_point *grid, uint64_t n_grid,
-                           const sd_tc_config *cfg, uint64_t row_begin, uint64_t row_end,
-                           float *out_data, float *out_cos_lia, uint8_t *out_mask,
-                           int64_t *out_t_us, uint8_t *out_iters, sd_geocoded_info *info) {
+static int tc_impl(const sd_radar_image *img, const sd_scene *scene, const sd_dem *dem_in,
+                   const sd_geoid *geoid, const sd_geo_grid_point *grid, uint64_t n_grid,
+                   const sd_tc_config *cfg, const double *forced_grid, uint64_t row_begin,
+                   uint64_t row_end, float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                   int64_t *out_t_us, uint8_t *out_iters, sd_geocoded_info *info) {
   if (n_grid == 0) return SD_ERR_TC_NO_GRID_POINTS;
   if (!(cfg->pixel_spacing > 0.0)) return SD_ERR_TC_CONFIG;
   if (scene->n_sub_swaths <= 0) return SD_ERR_TC_NO_SUBSWATHS;
@@ -757,7 +757,25 @@ int orc_terrain_correction(const sd_radar_image *img, const sd_scene *scene, con
   const double rps = img->range_pixel_spacing_m;
   auto lut = build_azimuth_time_lut(grid, n_grid);
   if (lut.empty()) return SD_ERR_TC_NO_GRID_POINTS;
-  int rc = orc_tc_output_grid(scene, cfg, info);
+  int rc = SD_OK;
+  if (forced_grid) {
+    // an explicit grid {west edge, north edge, rows, cols}: the output grid
+    // terrain_correction derives from a bounding box that snaps to it
+    std::memset(info, 0, sizeof *info);
+    info->origin_lon_deg = forced_grid[0];
+    info->origin_lat_deg = forced_grid[1];
+    info->rows = (uint64_t)forced_grid[2];
+    info->cols = (uint64_t)forced_grid[3];
+    info->pixel_spacing = cfg->pixel_spacing;
+    info->geotransform[0] = forced_grid[0];
+    info->geotransform[1] = cfg->pixel_spacing;
+    info->geotransform[3] = forced_grid[1];
+    info->geotransform[5] = -cfg->pixel_spacing;
+    info->total_pixel_count = info->rows * info->cols;
+    if (info->rows == 0 || info->cols == 0) return SD_ERR_TC_CONFIG;
+  } else {
+    rc = orc_tc_output_grid(scene, cfg, info);
+  }
   if (rc != SD_OK) return rc;
   if (cfg->projector_anchors <= 0) return SD_ERR_TC_CONFIG;
   const bool utm = cfg->crs != SD_CRS_WGS84;
@@ -918,6 +936,27 @@ int orc_terrain_correction(const sd_radar_image *img, const sd_scene *scene, con
   info->noise_masked_count = c_noise;
   std::memcpy(info->newton_iter_histogram, hist, sizeof(hist));
   return SD_OK;
+}
+
+int orc_terrain_correction(const sd_radar_image *img, const sd_scene *scene, const sd_dem *dem_in,
+                           const sd_geoid *geoid, const sd_geo_grid_point *grid, uint64_t n_grid,
+                           const sd_tc_config *cfg, uint64_t row_begin, uint64_t row_end,
+                           float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                           int64_t *out_t_us, uint8_t *out_iters, sd_geocoded_info *info) {
+  return tc_impl(img, scene, dem_in, geoid, grid, n_grid, cfg, nullptr, row_begin, row_end, out_data,
+                 out_cos_lia, out_mask, out_t_us, out_iters, info);
+}
+
+// terrain_correction on an explicit output grid (west edge, north edge,
+// rows, cols in the config's CRS) instead of the grid of the scene's bbox.
+int orc_terrain_correction_grid(const sd_radar_image *img, const sd_scene *scene, const sd_dem *dem_in,
+                                const sd_geoid *geoid, const sd_geo_grid_point *grid, uint64_t n_grid,
+                                const sd_tc_config *cfg, double origin_x, double origin_y, uint64_t rows,
+                                uint64_t cols, float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                                int64_t *out_t_us, sd_geocoded_info *info) {
+  const double g[4] = {origin_x, origin_y, (double)rows, (double)cols};
+  return tc_impl(img, scene, dem_in, geoid, grid, n_grid, cfg, g, 0, 0, out_data, out_cos_lia, out_mask,
+                 out_t_us, nullptr, info);
 }
 
 // ── deburst (deburst.rs:172-344) ─────────────────────────────────────────

@@ -147,3 +147,11 @@ class MergedInfo(C.Structure):
                 ("azimuth_start_time_us", C.c_int64), ("n_swaths", C.c_int32), ("_pad", C.c_int32),
                 ("swath_out_offset", C.c_int64 * 8), ("swath_seam", C.c_uint64 * 8),
                 ("swath_lines", C.c_uint64 * 8), ("swath_valid_offset", C.c_uint64 * 8)]
+
+
+class Tile(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("cfg", TcConfig), ("origin_x", C.c_double),
+                ("origin_y", C.c_double), ("rows", C.c_uint64), ("cols", C.c_uint64),
+                ("speckle", C.c_int32), ("speckle_window", C.c_int32), ("enl", C.c_float),
+                ("damping", C.c_float), ("out_data", C.c_void_p), ("out_cos_lia", C.c_void_p),
+                ("out_mask", C.c_void_p)]

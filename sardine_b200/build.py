@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libsardine_b200.so")
-SOURCES = ["runtime.cu", "tc.cu", "speckle.cu", "calib.cu", "diag.cu"]
+SOURCES = ["runtime.cu", "tc.cu", "tc_tiles.cu", "speckle.cu", "calib.cu", "diag.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -32,13 +32,30 @@ def build(verbose: bool = False, force: bool = False) -> str:
         t_out = os.path.getmtime(OUT)
         if all(os.path.getmtime(d) <= t_out for d in deps):
             return OUT
-    cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", OUT + ".tmp"] + srcs
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    # every translation unit compiles in its own nvcc process, then one link
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    objs = [os.path.join(objdir, os.path.basename(s)[:-3] + ".o") for s in srcs]
+    cflags = [f for f in FLAGS if f not in ("-shared", "-lcudart")]
+    procs = []
+    for src, obj in zip(srcs, objs):
+        cmd = [NVCC] + cflags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src]
+        procs.append(subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    failed = False
+    for pr in procs:
+        out, err = pr.communicate()
+        if pr.returncode != 0:
+            failed = True
+            sys.stderr.write(out + err)
+        elif verbose:
+            sys.stderr.write(err)
+    if failed:
+        raise RuntimeError("nvcc failed building libsardine_b200.so")
+    link = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT + ".tmp"] + objs + ["-lcudart"]
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libsardine_b200.so")
-    if verbose:
-        sys.stderr.write(res.stderr)
+        raise RuntimeError("nvcc failed linking libsardine_b200.so")
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

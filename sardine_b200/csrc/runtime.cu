@@ -162,6 +162,10 @@ void sd_ctx_destroy(sd_ctx *ctx) {
   for (void *p : ctx->pinned) cudaFreeHost(p);
   if (ctx->d_flags) cudaFree(ctx->d_flags);
   if (ctx->d_counters) cudaFree(ctx->d_counters);
+  for (auto &kv : ctx->graph_exec) cudaGraphExecDestroy(kv.second.exec);
+  if (ctx->tiles_done) cudaEventDestroy(ctx->tiles_done);
+  if (ctx->h_tile_counters) cudaFreeHost(ctx->h_tile_counters);
+  if (ctx->h_tile_flags) cudaFreeHost(ctx->h_tile_flags);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

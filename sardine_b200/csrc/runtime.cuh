@@ -35,6 +35,21 @@ struct sd_ctx {
   std::vector<KTime> pending;
   std::unordered_map<std::string, std::pair<double, uint64_t>> ktimes;  // ms, launches
   unsigned long long *d_counters = nullptr;      // device-side counters (64 slots)
+  // batched tiles (sd_tc_tiles_*): the last launch's results land here
+  cudaEvent_t tiles_done = nullptr;
+  unsigned long long *h_tile_counters = nullptr;  // pinned, tile_cap x 32
+  int *h_tile_flags = nullptr;                    // pinned, tile_cap x 4
+  uint64_t tile_cap = 0, tile_n = 0;
+  std::vector<sd_geocoded_info> tile_info;
+  bool tiles_pending = false;
+  // CUDA graphs of the tile stages (persistent kernels over fixed work tables)
+  bool graphs = false;
+  struct GraphRec {
+    cudaGraphExec_t exec;
+    const void *tag;    // address of the work table the graph reads
+    uint64_t launches;  // kernels per replay
+  };
+  std::unordered_map<int, GraphRec> graph_exec;
 };
 
 namespace sd {
@@ -97,6 +112,20 @@ void timing_collect(sd_ctx *ctx);
 
 inline unsigned grid_for(size_t n, unsigned block) {
   size_t g = (n + block - 1) / block;
+  return (unsigned)(g == 0 ? 1 : g);
+}
+
+// Grid of a persistent kernel: the CTAs the current device keeps resident
+// at once (occupancy x SMs), or fewer when there are fewer work blocks.
+template <class K>
+unsigned persistent_grid(K kernel, int threads, size_t smem, uint64_t blocks) {
+  int dev = 0, sms = 1, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1)
+    occ = 1;
+  uint64_t g = (uint64_t)occ * (uint64_t)(sms < 1 ? 1 : sms);
+  if (blocks < g) g = blocks;
   return (unsigned)(g == 0 ? 1 : g);
 }
 

@@ -11,6 +11,7 @@
 
 #include "geo.cuh"
 #include "runtime.cuh"
+#include "tiles.cuh"
 
 namespace sd {
 namespace {
@@ -67,6 +68,111 @@ struct SpParams {
 
 __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
 
+struct SpCoef {
+  float enl, damping, cv_n_sq, cv_max_sq;
+};
+
+// One output pixel of filter KIND from the staged window: `tile` holds the
+// footprint with row stride tw, the pixel sits at (lx, ly), h = half window.
+template <int KIND>
+__device__ float speckle_px(const float *tile, int tw, int lx, int ly, int h, const SpCoef &p) {
+  const float centre = tile[ly * tw + lx];
+  float o = NAN;
+  if (!finitef(centre)) return o;
+  if (KIND == SD_SPECKLE_REFINED_LEE) {
+    float best_cv = INFINITY, best_mean = centre, best_var = 0.0f;
+    for (int d = 0; d < 8; ++d) {
+      double sum = 0.0, sum_sq = 0.0;
+      int n = 0;
+      const int nt = c_rl.n[d];
+      for (int k = 0; k < nt; ++k) {
+        float v = tile[(ly + c_rl.dy[d][k]) * tw + lx + c_rl.dx[d][k]];
+        if (!finitef(v)) continue;
+        double vd = (double)v;
+        sum += vd;
+        sum_sq += vd * vd;
+        ++n;
+      }
+      if (n == 0) continue;
+      double md = sum / (double)n;
+      double vard = maxd_nan(sum_sq / (double)n - md * md, 0.0);
+      float mean = (float)md, var = (float)vard;
+      if (!(mean > 0.0f)) continue;
+      float cv = var / (mean * mean);
+      if (cv < best_cv) {
+        best_cv = cv;
+        best_mean = mean;
+        best_var = var;
+      }
+    }
+    if (!isfinite(best_cv)) {
+      o = centre;
+    } else {
+      float noise_var = best_mean * best_mean * p.cv_n_sq;
+      float signal_var = maxf_nan(best_var - noise_var, 0.0f);
+      float denom = signal_var + noise_var;
+      float k = denom > 0.0f ? signal_var / denom : 0.0f;
+      o = best_mean + k * (centre - best_mean);
+    }
+    return o;
+  }
+  double sum = 0.0, sum_sq = 0.0;
+  int n = 0;
+  for (int dy = -h; dy <= h; ++dy) {
+    const float *row = tile + (ly + dy) * tw + lx;
+    for (int dx = -h; dx <= h; ++dx) {
+      float v = row[dx];
+      if (!finitef(v)) continue;
+      double vd = (double)v;
+      sum += vd;
+      sum_sq += vd * vd;
+      ++n;
+    }
+  }
+  if (n == 0) return o;
+  double md = sum / (double)n;
+  double vard = maxd_nan(sum_sq / (double)n - md * md, 0.0);
+  float mean = (float)md, var = (float)vard;
+  if (KIND == SD_SPECKLE_BOXCAR) {
+    o = mean;
+  } else if (KIND == SD_SPECKLE_LEE) {
+    float noise_var = mean * mean * p.cv_n_sq;
+    float signal_var = maxf_nan(var - noise_var, 0.0f);
+    float denom = signal_var + noise_var;
+    float k = denom > 0.0f ? signal_var / denom : 0.0f;
+    o = mean + k * (centre - mean);
+  } else if (KIND == SD_SPECKLE_FROST) {
+    float cv_sq = mean > 0.0f ? var / (mean * mean) : 0.0f;
+    float alpha = p.damping * cv_sq;
+    double wsum = 0.0, vwsum = 0.0;
+    for (int dy = -h; dy <= h; ++dy) {
+      const float *row = tile + (ly + dy) * tw + lx;
+      for (int dx = -h; dx <= h; ++dx) {
+        float v = row[dx];
+        if (!finitef(v)) continue;
+        float dd = (float)(abs(dy) + abs(dx));
+        double w = (double)expf(-alpha * dd);
+        wsum += w;
+        vwsum += w * (double)v;
+      }
+    }
+    if (wsum > 0.0) o = (float)(vwsum / wsum);
+  } else {  // Gamma-MAP (speckle.rs:348-411)
+    float cv_sq = mean > 0.0f ? var / (mean * mean) : 0.0f;
+    if (cv_sq <= p.cv_n_sq) {
+      o = mean;
+    } else if (cv_sq >= p.cv_max_sq) {
+      o = centre;
+    } else {
+      float alpha = (1.0f + p.cv_n_sq) / (cv_sq - p.cv_n_sq);
+      float b = (alpha - p.enl - 1.0f) * mean;
+      float disc = b * b + 4.0f * alpha * p.enl * mean * centre;
+      o = disc >= 0.0f ? ((p.enl - alpha + 1.0f) * mean + sqrtf(disc)) / (2.0f * p.enl) : mean;
+    }
+  }
+  return o;
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
   extern __shared__ float tile[];
@@ -83,109 +189,100 @@ __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
   __syncthreads();
   const int64_t c = (int64_t)blockIdx.x * TX + threadIdx.x, r = (int64_t)blockIdx.y * TY + threadIdx.y;
   if (c >= p.cols || r >= p.rows) return;
-  const int lx = threadIdx.x + h, ly = threadIdx.y + h;
-  const float centre = tile[ly * tw + lx];
-  float o = NAN;
-  if (finitef(centre)) {
-    if (KIND == SD_SPECKLE_REFINED_LEE) {
-      float best_cv = INFINITY, best_mean = centre, best_var = 0.0f;
-      for (int d = 0; d < 8; ++d) {
-        double sum = 0.0, sum_sq = 0.0;
-        int n = 0;
-        const int nt = c_rl.n[d];
-        for (int k = 0; k < nt; ++k) {
-          float v = tile[(ly + c_rl.dy[d][k]) * tw + lx + c_rl.dx[d][k]];
-          if (!finitef(v)) continue;
-          double vd = (double)v;
-          sum += vd;
-          sum_sq += vd * vd;
-          ++n;
-        }
-        if (n == 0) continue;
-        double md = sum / (double)n;
-        double vard = maxd_nan(sum_sq / (double)n - md * md, 0.0);
-        float mean = (float)md, var = (float)vard;
-        if (!(mean > 0.0f)) continue;
-        float cv = var / (mean * mean);
-        if (cv < best_cv) {
-          best_cv = cv;
-          best_mean = mean;
-          best_var = var;
-        }
+  const SpCoef cf{p.enl, p.damping, p.cv_n_sq, p.cv_max_sq};
+  p.out[r * p.cols + c] = speckle_px<KIND>(tile, tw, threadIdx.x + h, threadIdx.y + h, h, cf);
+}
+
+// ── batched form: many tiles, each a halo'd geocoded raster ──────────────────
+// Item = one TX x TY block of one tile's output.  The block stages its
+// window from the tile's halo'd raster (cells outside it are NaN, which the
+// filters skip like out-of-image cells), filters the data plane with the
+// tile's kind (or copies it when kind < 0) and crops cos(LIA) and the mask.
+__global__ void __launch_bounds__(TX *TY) k_speckle_tiles(const SpWork *__restrict__ wp) {
+  __shared__ float tile[(TX + 2 * SP_MAX_HALF) * (TY + 2 * SP_MAX_HALF)];
+  const SpWork w = *wp;
+  const uint64_t total = w.pre[w.n_jobs];
+  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    int lo = 0, hi = w.n_jobs;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (w.pre[mid] <= item) lo = mid;
+      else hi = mid;
+    }
+    const SpJob &jb = w.jobs[lo];
+    const uint64_t li = item - w.pre[lo];
+    const int64_t bx = (int64_t)(jb.cols + TX - 1) / TX;
+    const int64_t tr = (int64_t)li / bx, tc = (int64_t)li % bx;
+    const int h = jb.kind >= 0 ? jb.half : 0;
+    const int tw = TX + 2 * h, th = TY + 2 * h;
+    const int64_t in_cols = jb.cols + 2 * jb.halo, in_rows = jb.rows + 2 * jb.halo;
+    // output (r, c) is input (r + halo, c + halo)
+    const int64_t c0 = tc * TX + jb.halo - h, r0 = tr * TY + jb.halo - h;
+    __syncthreads();
+    for (int k = threadIdx.y * TX + threadIdx.x; k < tw * th; k += TX * TY) {
+      const int ty = k / tw, tx = k % tw;
+      const int64_t rr = r0 + ty, cc = c0 + tx;
+      float v = NAN;
+      if (rr >= 0 && cc >= 0 && rr < in_rows && cc < in_cols) v = __ldg(jb.in + rr * in_cols + cc);
+      tile[k] = v;
+    }
+    __syncthreads();
+    const int64_t c = tc * TX + threadIdx.x, r = tr * TY + threadIdx.y;
+    if (c < jb.cols && r < jb.rows) {
+      const SpCoef cf{jb.enl, jb.damping, jb.cv_n_sq, jb.cv_max_sq};
+      const int lx = threadIdx.x + h, ly = threadIdx.y + h;
+      float o;
+      switch (jb.kind) {
+        case SD_SPECKLE_BOXCAR: o = speckle_px<SD_SPECKLE_BOXCAR>(tile, tw, lx, ly, h, cf); break;
+        case SD_SPECKLE_LEE: o = speckle_px<SD_SPECKLE_LEE>(tile, tw, lx, ly, h, cf); break;
+        case SD_SPECKLE_FROST: o = speckle_px<SD_SPECKLE_FROST>(tile, tw, lx, ly, h, cf); break;
+        case SD_SPECKLE_GAMMA_MAP: o = speckle_px<SD_SPECKLE_GAMMA_MAP>(tile, tw, lx, ly, h, cf); break;
+        case SD_SPECKLE_REFINED_LEE: o = speckle_px<SD_SPECKLE_REFINED_LEE>(tile, tw, lx, ly, h, cf); break;
+        default: o = tile[ly * tw + lx];
       }
-      if (!isfinite(best_cv)) {
-        o = centre;
-      } else {
-        float noise_var = best_mean * best_mean * p.cv_n_sq;
-        float signal_var = maxf_nan(best_var - noise_var, 0.0f);
-        float denom = signal_var + noise_var;
-        float k = denom > 0.0f ? signal_var / denom : 0.0f;
-        o = best_mean + k * (centre - best_mean);
-      }
-    } else {
-      double sum = 0.0, sum_sq = 0.0;
-      int n = 0;
-      for (int dy = -h; dy <= h; ++dy) {
-        const float *row = tile + (ly + dy) * tw + lx;
-        for (int dx = -h; dx <= h; ++dx) {
-          float v = row[dx];
-          if (!finitef(v)) continue;
-          double vd = (double)v;
-          sum += vd;
-          sum_sq += vd * vd;
-          ++n;
-        }
-      }
-      if (n > 0) {
-        double md = sum / (double)n;
-        double vard = maxd_nan(sum_sq / (double)n - md * md, 0.0);
-        float mean = (float)md, var = (float)vard;
-        if (KIND == SD_SPECKLE_BOXCAR) {
-          o = mean;
-        } else if (KIND == SD_SPECKLE_LEE) {
-          float noise_var = mean * mean * p.cv_n_sq;
-          float signal_var = maxf_nan(var - noise_var, 0.0f);
-          float denom = signal_var + noise_var;
-          float k = denom > 0.0f ? signal_var / denom : 0.0f;
-          o = mean + k * (centre - mean);
-        } else if (KIND == SD_SPECKLE_FROST) {
-          float cv_sq = mean > 0.0f ? var / (mean * mean) : 0.0f;
-          float alpha = p.damping * cv_sq;
-          double wsum = 0.0, vwsum = 0.0;
-          for (int dy = -h; dy <= h; ++dy) {
-            const float *row = tile + (ly + dy) * tw + lx;
-            for (int dx = -h; dx <= h; ++dx) {
-              float v = row[dx];
-              if (!finitef(v)) continue;
-              float dd = (float)(abs(dy) + abs(dx));
-              double w = (double)expf(-alpha * dd);
-              wsum += w;
-              vwsum += w * (double)v;
-            }
-          }
-          if (wsum > 0.0) o = (float)(vwsum / wsum);
-        } else {  // Gamma-MAP (speckle.rs:348-411)
-          float cv_sq = mean > 0.0f ? var / (mean * mean) : 0.0f;
-          if (cv_sq <= p.cv_n_sq) {
-            o = mean;
-          } else if (cv_sq >= p.cv_max_sq) {
-            o = centre;
-          } else {
-            float alpha = (1.0f + p.cv_n_sq) / (cv_sq - p.cv_n_sq);
-            float b = (alpha - p.enl - 1.0f) * mean;
-            float disc = b * b + 4.0f * alpha * p.enl * mean * centre;
-            o = disc >= 0.0f ? ((p.enl - alpha + 1.0f) * mean + sqrtf(disc)) / (2.0f * p.enl) : mean;
-          }
-        }
-      }
+      const int64_t oi = r * jb.cols + c, ii = (r + jb.halo) * in_cols + (c + jb.halo);
+      jb.out[oi] = o;
+      if (jb.cos_out) jb.cos_out[oi] = __ldg(jb.cos_in + ii);
+      if (jb.mask_out) jb.mask_out[oi] = __ldg(jb.mask_in + ii);
     }
   }
-  p.out[r * p.cols + c] = o;
 }
 
 bool g_masks_uploaded[64] = {false};
 
 }  // namespace
+
+int speckle_masks(sd_ctx *ctx) {
+  if (!g_masks_uploaded[ctx->device & 63]) {
+    RlMasks m = make_masks();
+    SD_CUDA(ctx, cudaMemcpyToSymbol(c_rl, &m, sizeof m));
+    g_masks_uploaded[ctx->device & 63] = true;
+  }
+  return SD_OK;
+}
+
+void speckle_coefs(int kind, uint64_t window, float enl, float damping, SpJob *j) {
+  const uint64_t win = kind == SD_SPECKLE_REFINED_LEE ? 7 : window;
+  j->kind = kind;
+  j->half = kind >= 0 ? (int)(win / 2) : 0;
+  j->enl = enl;
+  j->damping = damping;
+  j->cv_n_sq = kind >= 0 ? 1.0f / enl : 0.0f;
+  j->cv_max_sq = j->cv_n_sq < 1.0f ? 2.0f * j->cv_n_sq / (1.0f - j->cv_n_sq) : INFINITY;
+}
+
+int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool full_grid) {
+  SD_TRY(speckle_masks(ctx));
+  const unsigned g = persistent_grid(k_speckle_tiles, TX * TY, 0, full_grid ? ~0ull : total);
+  SD_TIMED_BEGIN(ctx, "k_speckle_tiles");
+  k_speckle_tiles<<<g, dim3(TX, TY), 0, ctx->stream>>>(d_work);
+  SD_LAUNCHED(ctx);
+  return SD_OK;
+}
+
+uint64_t speckle_tile_items(const SpJob &j) {
+  return (uint64_t)((j.cols + TX - 1) / TX) * (uint64_t)((j.rows + TY - 1) / TY);
+}
 
 // Validation in the reference's order (speckle.rs:137-178).
 int speckle_validate(uint64_t len, uint64_t cols, uint64_t rows, int kind, uint64_t window, float enl,
@@ -206,11 +303,7 @@ int speckle_validate(uint64_t len, uint64_t cols, uint64_t rows, int kind, uint6
 int speckle_launch(sd_ctx *ctx, const float *d_in, float *d_out, uint64_t cols, uint64_t rows,
                    int kind, uint64_t window, float enl, float damping, cudaStream_t st) {
   if (cols == 0 || rows == 0) return SD_OK;
-  if (!g_masks_uploaded[ctx->device & 63]) {
-    RlMasks m = make_masks();
-    SD_CUDA(ctx, cudaMemcpyToSymbol(c_rl, &m, sizeof m));
-    g_masks_uploaded[ctx->device & 63] = true;
-  }
+  SD_TRY(speckle_masks(ctx));
   uint64_t win = kind == SD_SPECKLE_REFINED_LEE ? 7 : window;
   SpParams p;
   p.in = d_in;

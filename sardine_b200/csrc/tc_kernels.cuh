@@ -1,0 +1,1542 @@
+// tc_kernels.cuh — device code of the backward Range-Doppler terrain
+// correction (terrain_correction.rs:1245-1836) and the host helpers that lay
+// out work tables and launch its stages.  Included by tc.cu (one scene per
+// call) and tc_tiles.cu (batches of tiles over resident scenes).
+//
+// The reference walks each output row column by column: the Newton
+// zero-Doppler solve of column c starts from the converged azimuth time of
+// the previous converged column (1443, 1580), moves in whole microseconds
+// truncated toward zero (1067) and stops BEFORE applying a sub-tolerance
+// step (1045-1065).  The converged time therefore depends on the seed, and a
+// 1 us difference moves the sample by ~5e-4 azimuth line.  The stages
+// reproduce that chain exactly while keeping the work data-parallel:
+//
+//  k_orbit_table   FP64 Lagrange state (pos, vel, acc, |v|^2) at every
+//                  microsecond of the span a scene needs (80 B each), so a
+//                  Newton iteration is one table read instead of an
+//                  8-point Lagrange evaluation with 64 divisions.
+//  k_row_*         per-row set-up: UTM anchors (output_crs.rs:364-417),
+//                  latitude seed, LUT guess, flat-cell area, and a coarse
+//                  azimuth-time model (17 knots per row).
+//  k_main          per pixel: DEM, geoid, target ECEF; the reference
+//                  iteration from the model time gives one converged time
+//                  t*; the set F = {t : |delta(t)| < tol} of possible
+//                  converged times (a pair {fb, fb+1}); the outcome of the
+//                  reference iteration from every member of the left
+//                  neighbour's F (the only seeds the chain can hand it); and
+//                  the outputs (resampling, Small-2011 geometry, mask, NESZ)
+//                  for both members of F.
+//  k_scan          per row: a warp walks the columns composing the per-pixel
+//                  outcome maps, selects each pixel's member of F, and runs
+//                  the reference iteration in place for any seed outside the
+//                  precomputed set.
+//  k_select        per pixel: final rasters, counters and Newton histogram.
+#pragma once
+#include <algorithm>
+#include <limits>
+#include <memory>
+
+#include "tiles.cuh"
+
+#include "geo.cuh"
+#include "runtime.cuh"
+
+namespace sd {
+namespace {
+
+enum : uint8_t { ST_CONV = 0, ST_NONCONV = 1, ST_DEGEN = 2, ST_ORBIT = 3, ST_DEMMISS = 4 };
+constexpr int KNOTS = 17;
+constexpr int kCounters = 8;  // valid, dem, outside, nonconv, degen, flat, noise, spare
+
+struct OrbitDev {
+  const sd_state_vector *svs;
+  uint64_t n;
+  const double2 *tab;  // 5 double2 per microsecond
+  int64_t tab_t0;
+  int64_t tab_n;
+};
+
+__device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
+  int64_t i = t - o.tab_t0;
+  if (i >= 0 && i < o.tab_n) {
+    const double2 *e = o.tab + 5 * i;
+    double2 a = __ldg(e), b = __ldg(e + 1), c = __ldg(e + 2), d = __ldg(e + 3), f = __ldg(e + 4);
+    s->pos = {a.x, a.y, b.x};
+    s->vel = {b.y, c.x, c.y};
+    s->acc = {d.x, d.y, f.x};
+    *vsq = f.y;
+    return ORB_OK;
+  }
+  int rc = orbit_eval(o.svs, o.n, t, s);
+  if (rc == ORB_OK) *vsq = dot3(s->vel, s->vel);
+  return rc;
+}
+
+struct ZdRes {
+  uint8_t st;
+  int64_t t;
+  int it;
+};
+
+// solve_zero_doppler (terrain_correction.rs:1010-1073), bit-exact.
+__device__ ZdRes newton(const OrbitDev &o, V3 P, int64_t seed, int max_iter, double tol) {
+  int64_t t = seed;
+  for (int i = 0; i < max_iter; ++i) {
+    OrbitState s;
+    double vsq;
+    if (orbit_at(o, t, &s, &vsq) != ORB_OK) return {ST_ORBIT, t, i};
+    V3 r = sub3(P, s.pos);
+    double f = dot3(r, s.vel);
+    double fp = -vsq + dot3(r, s.acc);
+    if (fabs(fp) < 1.0) return {ST_DEGEN, t, i};
+    double delta = -f / fp;
+    if (fabs(delta) < tol) return {ST_CONV, t, i + 1};
+    t = t + f2i64(delta * 1e6);
+  }
+  return {ST_NONCONV, t, max_iter};
+}
+
+struct TcDev {
+  // output grid
+  uint64_t rows, cols;
+  double lat_north, lon_west, sp, step_deg;
+  int utm;
+  Utm proj;
+  // anchors (UTM)
+  const double *ax;   // n_pts
+  const double *alon; // rows * n_pts
+  const double *alat;
+  int n_anchors, n_pts;
+  // LUT
+  const double *lut_lat;
+  const int64_t *lut_t;
+  int lut_n;
+  // rows
+  int64_t *row_guess;
+  double *row_flat;
+  int64_t *knot_t;
+  // scene
+  OrbitDev orb;
+  DemView dem;
+  const float *geoid;
+  const float *img;
+  const float *nesz;
+  uint64_t lines, samples;
+  int64_t az_start;
+  double ati, near_range, rps;
+  int max_iter;
+  double tol;
+  int flatten, compute_lia, need_geom, resampling, nesz_mask;
+  float nesz_factor;
+  // per-pixel scratch
+  struct Rec *rec;
+  uint32_t *cc;
+  uint8_t *sel;
+  // outputs
+  float *out;
+  float *cos_lia;
+  uint8_t *mask;
+  int64_t *az_time;  // optional: converged azimuth time per pixel (INT64_MIN if none)
+  int *flags;
+  unsigned long long *counters;
+  unsigned long long *trange;  // [0] = min, [1] = max (biased by 2^63), or null
+  uint64_t bpr;                // k_main work items per row
+  int fast;                    // tolerance allows the fixed-point-pair scheme
+  int pad_;
+};
+
+// ── work table ──────────────────────────────────────────────────────────────
+// Every kernel below is one launch over a table of jobs (a whole scene, or
+// many tiles of many scenes): for each stage, pre[stage][j] is the exclusive
+// prefix sum of the stage's work items over jobs 0..j-1.  Kernels are
+// persistent (grid sized to the device's resident CTAs) and stride over the
+// items; a CUDA graph of the stages therefore does not depend on the batch.
+enum { WK_ANCH = 0, WK_ROWS = 1, WK_KNOT = 2, WK_MAIN = 3, WK_SCAN = 4, WK_SEL = 5, kWk = 6 };
+constexpr int SEL_THREADS = 256;
+
+struct TcWork {
+  int n_jobs;
+  int pad;
+  const TcDev *jobs;
+  const uint64_t *pre;  // kWk x (n_jobs + 1)
+};
+
+__device__ __forceinline__ const uint64_t *stage_pre(const TcWork &w, int stage) {
+  return w.pre + (size_t)stage * (size_t)(w.n_jobs + 1);
+}
+
+// last job j with pre[j] <= item (jobs without items in the stage are skipped)
+__device__ __forceinline__ int find_job(const uint64_t *pre, int n_jobs, uint64_t item) {
+  int lo = 0, hi = n_jobs;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(pre + mid) <= item) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Copies a job record into shared memory with the calling threads.
+__device__ __forceinline__ void load_job(unsigned char *dst, const TcDev *src, int lane, int nthreads) {
+  static_assert(sizeof(TcDev) % 8 == 0, "TcDev size");
+  const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+  unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+  for (int k = lane; k < (int)(sizeof(TcDev) / 8); k += nthreads) d[k] = __ldg(s + k);
+}
+
+__device__ __forceinline__ double row_y(const TcDev &p, uint64_t r) {
+  return p.lat_north - ((double)r + 0.5) * p.sp;
+}
+
+// Output pixel centre in lon/lat: direct for WGS84, project_row anchors for
+// UTM (output_crs.rs:383-415).
+__device__ void pixel_lonlat(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat) {
+  if (!p.utm) {
+    *lon = p.lon_west + ((double)c + 0.5) * p.sp;
+    *lat = row_y(p, r);
+    return;
+  }
+  const double x_start = p.lon_west + 0.5 * p.sp;
+  const double x = x_start + (double)c * p.sp;
+  const int na = p.n_anchors;
+  // segment: smallest s with s == na-1 or x <= ax[s+1]
+  double anchor_dx = p.ax[1] - p.ax[0];
+  int g = 0;
+  if (anchor_dx > 0.0) {
+    double q = floor((x - x_start) / anchor_dx);
+    g = q < 0.0 ? 0 : (q > (double)(na - 1) ? na - 1 : (int)q);
+  }
+  while (g > 0 && x <= p.ax[g]) g--;
+  while (g + 1 < na && x > p.ax[g + 1]) g++;
+  const double x0 = p.ax[g], x1 = p.ax[g + 1];
+  const double *lo = p.alon + r * p.n_pts, *la = p.alat + r * p.n_pts;
+  double t = (x1 == x0) ? 0.0 : (x - x0) / (x1 - x0);
+  *lon = lo[g] + t * (lo[g + 1] - lo[g]);
+  *lat = la[g] + t * (la[g + 1] - la[g]);
+}
+
+// guess_azimuth_time (terrain_correction.rs:1107-1137)
+__device__ int64_t guess_time(const TcDev &p, double lat) {
+  if (p.lut_n == 1) return p.lut_t[0];
+  int lo = 0, hi = p.lut_n;
+  while (lo < hi) {
+    int mid = lo + (hi - lo) / 2;
+    double v = p.lut_lat[mid];
+    if (v < lat) lo = mid + 1;
+    else if (v > lat) hi = mid;
+    else return p.lut_t[mid];
+  }
+  if (lo == 0) return p.lut_t[0];
+  if (lo >= p.lut_n) return p.lut_t[p.lut_n - 1];
+  double frac = (lat - p.lut_lat[lo - 1]) / (p.lut_lat[lo] - p.lut_lat[lo - 1]);
+  double dt_us = (double)(p.lut_t[lo] - p.lut_t[lo - 1]);
+  return p.lut_t[lo - 1] + f2i64(frac * dt_us);
+}
+
+// ── K1 ─────────────────────────────────────────────────────────────────────
+__global__ void k_orbit_table(const sd_state_vector *svs, uint64_t n, int64_t t0, int64_t cnt,
+                              double2 *tab) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  OrbitState s;
+  orbit_eval(svs, n, t0 + i, &s);  // range is inside the state-vector window
+  double2 *e = tab + 5 * i;
+  e[0] = make_double2(s.pos.x, s.pos.y);
+  e[1] = make_double2(s.pos.z, s.vel.x);
+  e[2] = make_double2(s.vel.y, s.vel.z);
+  e[3] = make_double2(s.acc.x, s.acc.y);
+  e[4] = make_double2(s.acc.z, dot3(s.vel, s.vel));
+}
+
+// ── K2 ─────────────────────────────────────────────────────────────────────
+#define SD_FOR_ITEMS(STAGE)                                                                  \
+  const TcWork w = *wp;                                                                      \
+  const uint64_t *pre = stage_pre(w, STAGE);                                                 \
+  const uint64_t total = pre[w.n_jobs];                                                      \
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;              \
+       i += (uint64_t)gridDim.x * blockDim.x)
+
+__global__ void k_row_anchors(const TcWork *__restrict__ wp) {
+  SD_FOR_ITEMS(WK_ANCH) {
+    const int j = find_job(pre, w.n_jobs, i);
+    const TcDev &p = w.jobs[j];
+    const uint64_t li = i - pre[j];
+    const uint64_t r = li / p.n_pts, a = li % p.n_pts;
+    double lon, lat;
+    utm_xy_to_lonlat(p.proj, p.ax[a], row_y(p, r), &lon, &lat);
+    ((double *)p.alon)[li] = lon;
+    ((double *)p.alat)[li] = lat;
+  }
+}
+
+__global__ void k_row_setup(const TcWork *__restrict__ wp) {
+  SD_FOR_ITEMS(WK_ROWS) {
+    const int j = find_job(pre, w.n_jobs, i);
+    const TcDev &p = w.jobs[j];
+    const uint64_t r = i - pre[j];
+    if (r == 0) {  // the job's counters and flags start at zero
+      for (int k = 0; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; ++k) p.counters[k] = 0;
+      p.flags[0] = 0;
+      p.flags[1] = 0;
+    }
+    const double y = row_y(p, r);
+    double lat_seed = y;
+    if (p.utm) {
+      double mid_x = p.lon_west + ((double)p.cols / 2.0) * p.sp;
+      double lo;
+      utm_xy_to_lonlat(p.proj, mid_x, y, &lo, &lat_seed);
+    }
+    p.row_guess[r] = guess_time(p, lat_seed);
+    if (p.need_geom) {
+      double ref_lon;
+      if (p.utm) {
+        double la;
+        pixel_lonlat(p, r, p.cols / 2, &ref_lon, &la);
+      } else {
+        ref_lon = p.lon_west + ((double)p.cols / 2.0) * p.sp;
+      }
+      p.row_flat[r] = flat_cell_area(lat_seed, ref_lon, p.step_deg);
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t knot_col(const TcDev &p, int j) {
+  return p.cols <= 1 ? 0 : (uint64_t)j * (p.cols - 1) / (KNOTS - 1);
+}
+
+// Coarse azimuth-time model: the reference iteration at KNOTS columns per
+// row with the geoid surface (h = 0 orthometric).  Only a seed predictor.
+__global__ void k_row_model(const TcWork *__restrict__ wp) {
+  SD_FOR_ITEMS(WK_KNOT) {
+    const int jb = find_job(pre, w.n_jobs, i);
+    const TcDev &p = w.jobs[jb];
+    const uint64_t li = i - pre[jb];
+    const uint64_t r = li / KNOTS;
+    const int j = (int)(li % KNOTS);
+    const uint64_t c = knot_col(p, j);
+    double lon, lat;
+    pixel_lonlat(p, r, c, &lon, &lat);
+    V3 P = geodetic_to_ecef(lat, lon, geoid_undulation(p.geoid, lat, lon));
+    ZdRes z = newton(p.orb, P, p.row_guess[r], 40, 1e-6);
+    if (z.st == ST_CONV) {
+      p.knot_t[li] = z.t;
+      if (p.trange) {
+        unsigned long long b = (unsigned long long)z.t ^ 0x8000000000000000ull;
+        atomicMin(&p.trange[0], b);
+        atomicMax(&p.trange[1], b);
+      }
+    } else {
+      p.knot_t[li] = INT64_MIN;
+    }
+  }
+}
+
+__device__ int64_t predicted_time(const TcDev &p, uint64_t r, uint64_t c) {
+  const int64_t *k = p.knot_t + r * KNOTS;
+  if (p.cols <= 1) return k[0] != INT64_MIN ? k[0] : p.row_guess[r];
+  int j = (int)((c * (KNOTS - 1)) / (p.cols - 1));
+  if (j >= KNOTS - 1) j = KNOTS - 2;
+  uint64_t c0 = knot_col(p, j), c1 = knot_col(p, j + 1);
+  int64_t t0 = k[j], t1 = k[j + 1];
+  if (t0 == INT64_MIN && t1 == INT64_MIN) return p.row_guess[r];
+  if (t0 == INT64_MIN) return t1;
+  if (t1 == INT64_MIN || c1 == c0) return t0;
+  double f = (double)(c - c0) / (double)(c1 - c0);
+  return t0 + (int64_t)llrint(f * (double)(t1 - t0));
+}
+
+// ── resampling (terrain_correction.rs:770-983) ───────────────────────────────
+__device__ __forceinline__ float ldf(const float *p, int64_t i) { return __ldg(p + i); }
+
+__device__ float sample_bilinear(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+  int64_t max_line = nl == 0 ? 0 : (int64_t)nl - 1;
+  int64_t max_sample = ns == 0 ? 0 : (int64_t)ns - 1;
+  int64_t l0 = clampi(f2i64(floor(line)), 0, max_line);
+  int64_t l1 = l0 + 1 < max_line ? l0 + 1 : max_line;
+  int64_t s0 = clampi(f2i64(floor(sample)), 0, max_sample);
+  int64_t s1 = s0 + 1 < max_sample ? s0 + 1 : max_sample;
+  double dl = line - (double)l0;
+  double ds = sample - (double)s0;
+  float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
+  float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
+  if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
+  double w00 = (1.0 - dl) * (1.0 - ds);
+  double w01 = (1.0 - dl) * ds;
+  double w10 = dl * (1.0 - ds);
+  double w11 = dl * ds;
+  return (float)((double)v00 * w00 + (double)v01 * w01 + (double)v10 * w10 + (double)v11 * w11);
+}
+
+__device__ float sample_bicubic(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
+  double dl = line - (double)lf, ds = sample - (double)sf;
+  double ws[4];
+  int64_t cols[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ws[k] = keys_weight((double)(k - 1) - ds);
+    cols[k] = clampi(sf + k - 1, 0, max_s);
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int li = -1; li <= 2; ++li) {
+    int64_t row = clampi(lf + li, 0, max_l);
+    double wl = keys_weight((double)li - dl);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) return NAN;
+      acc += (double)v * wl * ws[k];
+    }
+  }
+  return (float)acc;
+}
+
+// ── split precision (SD_PRECISION_SPLIT) ─────────────────────────────────────
+// Everything that decides an integer outcome stays FP64: the orbit table,
+// every Newton residual (so the microsecond chain, the converged times and
+// the Newton histogram are those of the FP64 path), the target ECEF, the
+// slant range, the image coordinates and the footprint test.  Resampling
+// weights and sums, the NESZ sample, the facet normal (built from chords
+// between the cardinal neighbours in a frame local to the pixel, never from
+// absolute ECEF coordinates), cos(LIA) and the flattening weight run in FP32.
+// A mask decision FP32 cannot settle (flattening weight within 1e-4
+// relative of 0.05 or 2.0, local projection within 1e-4 of the facet area
+// from zero, sigma0 within 1e-5 relative of the NESZ threshold) is redone
+// with the FP64 candidate, so the mask equals the FP64 path's.
+// The build compiles with --fmad=false (the FP64 path must not contract);
+// the FP32 code contracts explicitly with fmaf.
+
+__device__ __forceinline__ float keys_weight_f(float t) {  // keys_weight, Horner form
+  t = fabsf(t);
+  if (t < 1.f) return fmaf(fmaf(1.5f, t, -2.5f), t * t, 1.f);
+  if (t < 2.f) return fmaf(fmaf(fmaf(-0.5f, t, 2.5f), t, -4.f), t, 2.f);
+  return 0.f;
+}
+
+// Lanczos-3 weights (terrain_correction.rs:938-952) of the taps li = -2..3
+// at x = f - li.  sin(pi x) = (-1)^li sin(pi f) and sin(pi x/3) =
+// sin(pi f/3) cos(pi li/3) - cos(pi f/3) sin(pi li/3), so the six weights
+// take one sinpi and one sincospi (plus one sinpi for the tap li = 1).
+template <typename T>
+__device__ __forceinline__ void lanczos6(T f, T w[6]);
+
+template <>
+__device__ __forceinline__ void lanczos6<float>(float f, float w[6]) {
+  const float s1 = sinpif(f);
+  float s3, c3;
+  sincospif(f * (1.f / 3.f), &s3, &c3);
+  const float h = 0.866025403784438647f;  // sin(pi/3)
+  const float cl[6] = {-0.5f, 0.5f, 1.f, 0.5f, -0.5f, -1.f};
+  const float sl[6] = {-h, -h, 0.f, h, h, 0.f};
+  const float k = (float)(3.0 / (kPi * kPi));
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const int li = j - 2;
+    const float x = f - (float)li;
+    const float ax = fabsf(x);
+    const float s = (li & 1) ? -s1 : s1;
+    // tap li = 1: the angle-addition form cancels as f -> 1 (where this tap
+    // carries the weight), so its sine is taken directly
+    const float s3l = li == 1 ? sinpif((f - 1.f) * (1.f / 3.f)) : s3 * cl[j] - c3 * sl[j];
+    w[j] = ax < 1e-10f ? 1.f : (ax < 3.f ? k * s * s3l / (x * x) : 0.f);
+  }
+}
+
+template <>
+__device__ __forceinline__ void lanczos6<double>(double f, double w[6]) {
+  const double s1 = sinpi(f);
+  double s3, c3;
+  sincospi(f * (1.0 / 3.0), &s3, &c3);
+  const double h = 0.86602540378443864676;
+  const double cl[6] = {-0.5, 0.5, 1.0, 0.5, -0.5, -1.0};
+  const double sl[6] = {-h, -h, 0.0, h, h, 0.0};
+  const double k = 3.0 / (kPi * kPi);
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const int li = j - 2;
+    const double x = f - (double)li;
+    const double ax = fabs(x);
+    const double s = (li & 1) ? -s1 : s1;
+    const double s3l = li == 1 ? sinpi((f - 1.0) * (1.0 / 3.0)) : s3 * cl[j] - c3 * sl[j];
+    w[j] = ax < 1e-10 ? 1.0 : (ax < 3.0 ? k * s * s3l / (x * x) : 0.0);
+  }
+}
+
+// The FP32 samplers also form the magnitude sum A = sum |v w|: the FP32
+// rounding error of the result is a few ulps of A, so where |result| <
+// A / kCancel (negative lobes or extrapolation cancelling) the FP64 sampler
+// redoes the pixel and the result keeps its 1e-4 relative bound.
+constexpr float kCancel = 16.f;
+
+__device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, double line, double sample,
+                                   bool *redo) {
+  int64_t max_line = nl == 0 ? 0 : (int64_t)nl - 1;
+  int64_t max_sample = ns == 0 ? 0 : (int64_t)ns - 1;
+  int64_t l0 = clampi(f2i64(floor(line)), 0, max_line);
+  int64_t l1 = l0 + 1 < max_line ? l0 + 1 : max_line;
+  int64_t s0 = clampi(f2i64(floor(sample)), 0, max_sample);
+  int64_t s1 = s0 + 1 < max_sample ? s0 + 1 : max_sample;
+  const float dl = (float)(line - (double)l0), ds = (float)(sample - (double)s0);
+  float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
+  float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
+  if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
+  const float top = fmaf(v01 - v00, ds, v00);
+  const float bot = fmaf(v11 - v10, ds, v10);
+  const float r = fmaf(bot - top, dl, top);
+  // the weights leave [0, 1] only where the clamped index extrapolates
+  // (line or sample in [-0.5, 0)); the magnitude sum is checked there
+  if (dl < 0.f || ds < 0.f) {
+    const float a = (fabsf(v00) * fabsf(1.f - ds) + fabsf(v01) * fabsf(ds)) * fabsf(1.f - dl) +
+                    (fabsf(v10) * fabsf(1.f - ds) + fabsf(v11) * fabsf(ds)) * fabsf(dl);
+    if (a > kCancel * fabsf(r)) *redo = true;
+  }
+  return r;
+}
+
+__device__ float sample_bicubic_f(const float *d, uint64_t nl, uint64_t ns, double line, double sample,
+                                  bool *redo) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
+  const float dl = (float)(line - (double)lf), ds = (float)(sample - (double)sf);
+  float ws[4];
+  int64_t cols[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ws[k] = keys_weight_f((float)(k - 1) - ds);
+    cols[k] = clampi(sf + k - 1, 0, max_s);
+  }
+  float acc = 0.f, aacc = 0.f;
+#pragma unroll
+  for (int li = -1; li <= 2; ++li) {
+    int64_t row = clampi(lf + li, 0, max_l);
+    const float wl = keys_weight_f((float)li - dl);
+    float racc = 0.f, rabs = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) return NAN;
+      racc = fmaf(v, ws[k], racc);
+      rabs = fmaf(fabsf(v), fabsf(ws[k]), rabs);
+    }
+    acc = fmaf(racc, wl, acc);
+    aacc = fmaf(rabs, fabsf(wl), aacc);
+  }
+  if (aacc > kCancel * fabsf(acc)) *redo = true;
+  return acc;
+}
+
+template <typename T>
+__device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, double line, double sample,
+                                  bool *redo) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
+  T wl[6], ws[6];
+  lanczos6<T>((T)(line - (double)lf), wl);
+  lanczos6<T>((T)(sample - (double)sf), ws);
+  int64_t cols[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) cols[k] = clampi(sf + k - 2, 0, max_s);
+  T acc = 0, aacc = 0;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    int64_t row = clampi(lf + j - 2, 0, max_l);
+    T racc = 0, rabs = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) return NAN;
+      racc += (T)v * ws[k];
+      if (redo) rabs += fabs((T)v * ws[k]);
+    }
+    acc += racc * wl[j];
+    if (redo) aacc += rabs * fabs(wl[j]);
+  }
+  if (redo && aacc > (T)kCancel * fabs(acc)) *redo = true;
+  return (float)acc;
+}
+
+// KDYN: the resampling kernel is read from the job record (batches whose
+// tiles mix kernels); 0..2 fix it at compile time.
+constexpr int KDYN = 3;
+
+template <int KERNEL>
+__device__ __forceinline__ float resample_f(const TcDev &p, double line, double sample, bool *redo) {
+  if (KERNEL == KDYN) {
+    switch (p.resampling) {
+      case SD_RESAMPLE_BICUBIC: return sample_bicubic_f(p.img, p.lines, p.samples, line, sample, redo);
+      case SD_RESAMPLE_LANCZOS3: return sample_lanczos_t<float>(p.img, p.lines, p.samples, line, sample, redo);
+      default: return sample_bilinear_f(p.img, p.lines, p.samples, line, sample, redo);
+    }
+  }
+  return KERNEL == SD_RESAMPLE_BICUBIC    ? sample_bicubic_f(p.img, p.lines, p.samples, line, sample, redo)
+         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos_t<float>(p.img, p.lines, p.samples, line, sample, redo)
+                                          : sample_bilinear_f(p.img, p.lines, p.samples, line, sample, redo);
+}
+
+template <int KERNEL>
+__device__ __forceinline__ float resample(const TcDev &p, double line, double sample) {
+  if (KERNEL == KDYN) {
+    switch (p.resampling) {
+      case SD_RESAMPLE_BICUBIC: return sample_bicubic(p.img, p.lines, p.samples, line, sample);
+      case SD_RESAMPLE_LANCZOS3: return sample_lanczos_t<double>(p.img, p.lines, p.samples, line, sample, nullptr);
+      default: return sample_bilinear(p.img, p.lines, p.samples, line, sample);
+    }
+  }
+  return KERNEL == SD_RESAMPLE_BICUBIC    ? sample_bicubic(p.img, p.lines, p.samples, line, sample)
+         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos_t<double>(p.img, p.lines, p.samples, line, sample, nullptr)
+                                          : sample_bilinear(p.img, p.lines, p.samples, line, sample);
+}
+
+// ── per-pixel geometry ───────────────────────────────────────────────────────
+// Centre of output pixel (r, c): lat/lon, DEM height and target ECEF.  The
+// sines/cosines and projection terms are kept for the neighbour lookups.
+struct PixGeo {
+  double lat, lon;
+  double la, lo;              // radians as geodesy.rs:39-40 converts them
+  double sla, cla, slo, clo;  // their sines and cosines
+  UtmLocal loc;               // UTM DEM: projection of the centre and its local expansion
+  V3 P;
+};
+
+// DEM lookup of the centre (1529-1536), geoid (1545) and target ECEF (1546).
+// Returns false when the DEM has no finite height there.
+__device__ bool pixel_geo(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g) {
+  pixel_lonlat(p, r, c, &g->lon, &g->lat);
+  float hf;
+  bool ok;
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    utm_local(u, g->lat, utm_taup(u, g->lat), utm_lam(u, g->lon), &g->loc);
+    ok = dem_at_xy(p.dem, g->loc.x, g->loc.y, &hf);
+  } else {
+    ok = dem_at_lonlat(p.dem, g->lon, g->lat, &hf);
+  }
+  if (!ok || !isfinite(hf)) return false;
+  double h_ell = (double)hf + geoid_undulation(p.geoid, g->lat, g->lon);
+  g->la = deg2rad_ecef(g->lat);
+  g->lo = deg2rad_ecef(g->lon);
+  g->sla = sin(g->la);
+  g->cla = cos(g->la);
+  g->slo = sin(g->lo);
+  g->clo = cos(g->lo);
+  g->P = ecef_sc(g->sla, g->cla, g->slo, g->clo, h_ell);
+  return true;
+}
+
+// Facet of the four cardinal DEM neighbours (1642-1675): normal and area.
+// The neighbours sit step_deg from the centre, so their projected
+// coordinates come from the centre's local expansion and their sines and
+// cosines from angle addition over the exact argument differences.
+struct Facet {
+  bool ok;
+  V3 normal;
+  double area;
+};
+
+__device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
+  Facet f{};
+  const double sd = p.step_deg;
+  const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
+  float he, hw, hn, hs;
+  bool ok;
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    const double k = kPi / 180.0;
+    double x, y;
+    utm_local_step(u, g.loc, 0.0, (lon_e - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &he);
+    utm_local_step(u, g.loc, 0.0, (lon_w - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hw) && ok;
+    utm_local_step(u, g.loc, (lat_n - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hn) && ok;
+    utm_local_step(u, g.loc, (lat_s - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hs) && ok;
+  } else {
+    ok = dem_at_lonlat(p.dem, lon_e, g.lat, &he);
+    ok = dem_at_lonlat(p.dem, lon_w, g.lat, &hw) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_n, &hn) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_s, &hs) && ok;
+  }
+  f.ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
+  if (!f.ok) return f;
+  double se, ce, sw, cw, sn, cn, ss, cs;
+  sincos_add(g.slo, g.clo, deg2rad_ecef(lon_e) - g.lo, &se, &ce);
+  sincos_add(g.slo, g.clo, deg2rad_ecef(lon_w) - g.lo, &sw, &cw);
+  sincos_add(g.sla, g.cla, deg2rad_ecef(lat_n) - g.la, &sn, &cn);
+  sincos_add(g.sla, g.cla, deg2rad_ecef(lat_s) - g.la, &ss, &cs);
+  V3 pe = ecef_sc(g.sla, g.cla, se, ce, (double)he);
+  V3 pw = ecef_sc(g.sla, g.cla, sw, cw, (double)hw);
+  V3 pn = ecef_sc(sn, cn, g.slo, g.clo, (double)hn);
+  V3 ps = ecef_sc(ss, cs, g.slo, g.clo, (double)hs);
+  f.normal = cross3(sub3(pe, pw), sub3(pn, ps));
+  f.area = norm3(f.normal);
+  return f;
+}
+
+// Output of one pixel for one converged azimuth time (1585-1739): sigma0 /
+// gamma0, cos(LIA), mask code and counter class (0 valid, 2 outside
+// footprint, 5 flat-masked, 6 noise-masked).
+struct CandOut {
+  float data, cos;
+  uint8_t mask, cls;
+};
+
+struct CandPre {  // steps 4-6 of the reference loop for one candidate
+  double line, sample;
+  float sigma0;
+  bool inside;
+};
+
+template <int KERNEL, bool SPLIT>
+__device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
+  CandPre c;
+  double slant = norm3(sub3(P, S));
+  double dt = (double)(t - p.az_start) / 1e6;
+  c.line = dt / p.ati;
+  c.sample = (slant - p.near_range) / p.rps;
+  c.inside = !(c.line < -0.5 || c.line > ((double)p.lines - 0.5) || c.sample < -0.5 ||
+               c.sample > ((double)p.samples - 0.5));
+  if (c.inside) {
+    bool redo = false;
+    if (SPLIT) c.sigma0 = resample_f<KERNEL>(p, c.line, c.sample, &redo);
+    if (!SPLIT || redo) c.sigma0 = resample<KERNEL>(p, c.line, c.sample);
+  } else {
+    c.sigma0 = NAN;
+  }
+  if (c.sigma0 != c.sigma0) c.inside = false;
+  return c;
+}
+
+__device__ CandOut cand_post(const TcDev &p, const CandPre &c, V3 P, V3 S, const Facet &f, double flat_area) {
+  CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
+  if (!c.inside) return o;
+  float sigma0 = c.sigma0;
+  uint8_t m = SD_MASK_OUTSIDE_FOOTPRINT;
+  float cosv = NAN;
+  if (p.need_geom) {
+    if (!f.ok) {
+      m = SD_MASK_DEM_NEIGHBOUR_MISSING;
+      if (p.flatten) return {NAN, cosv, m, 5};
+    } else {
+      V3 look = normalize3(sub3(S, P));
+      double local_proj = dot3(f.normal, look);
+      if (local_proj <= 0.0 || f.area == 0.0) {
+        m = SD_MASK_SHADOW;
+        if (p.flatten) return {NAN, cosv, m, 5};
+      } else {
+        double cl = clampd(local_proj / f.area, 0.0, 1.0);
+        double w = local_proj / flat_area;
+        cosv = (float)cl;
+        if (w < 0.05 || w > 2.0) {
+          m = w > 2.0 ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING;
+          if (p.flatten) return {NAN, cosv, m, 5};
+        } else if (p.flatten) {
+          sigma0 /= (float)w;
+        }
+      }
+    }
+  }
+  if (p.nesz_mask) {
+    float nz = sample_bilinear(p.nesz, p.lines, p.samples, c.line, c.sample);
+    if (nz == nz) {
+      float thr = nz * p.nesz_factor;
+      if (sigma0 <= thr) return {NAN, cosv, (uint8_t)SD_MASK_NOISE_MASKED, 6};
+    }
+  }
+  return {sigma0, cosv, (uint8_t)SD_MASK_VALID, 0};
+}
+
+// Facet in FP32: the east-west and north-south chords between the cardinal
+// neighbours, expanded about the centre (latitude phi, longitude lam,
+// prime-vertical radius N(phi)) to first order in the angular steps a, b, c,
+// d (~1.6e-6 rad); the dropped terms are below 1e-7 m on chords of ~20 m.
+//   E-W: cos(phi) (cos(lam) dh - sin(lam) q, sin(lam) dh + cos(lam) q),
+//        sin(phi) dh,  dh = he - hw, q = (N + he) a + (N + hw) b
+//   N-S: (cos(lam) An, sin(lam) An, Zn) with
+//        An = cos(phi) (hn - hs + N'(c + d)) - sin(phi) ((N + hn) c + (N + hs) d)
+//        Zn = sin(phi) (hn - hs + B'(c + d)) + cos(phi) ((B + hn) c + (B + hs) d)
+//        B = N (1 - e^2), N' = dN/dphi = N e^2 sin cos / (1 - e^2 sin^2).
+struct FacetF {
+  bool ok;
+  float nx, ny, nz, area;
+};
+
+__device__ FacetF pixel_facet_f(const TcDev &p, const PixGeo &g) {
+  FacetF f{};
+  const double sd = p.step_deg;
+  const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
+  float he, hw, hn, hs;
+  bool ok;
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    const double k = kPi / 180.0;
+    double x, y;
+    utm_local_step(u, g.loc, 0.0, (lon_e - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &he);
+    utm_local_step(u, g.loc, 0.0, (lon_w - g.lon) * k, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hw) && ok;
+    utm_local_step(u, g.loc, (lat_n - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hn) && ok;
+    utm_local_step(u, g.loc, (lat_s - g.lat) * k, 0.0, &x, &y);
+    ok = dem_at_xy(p.dem, x, y, &hs) && ok;
+  } else {
+    ok = dem_at_lonlat(p.dem, lon_e, g.lat, &he);
+    ok = dem_at_lonlat(p.dem, lon_w, g.lat, &hw) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_n, &hn) && ok;
+    ok = dem_at_lonlat(p.dem, g.lon, lat_s, &hs) && ok;
+  }
+  f.ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
+  if (!f.ok) return f;
+  const float a = (float)(deg2rad_ecef(lon_e) - g.lo), b = (float)(g.lo - deg2rad_ecef(lon_w));
+  const float c = (float)(deg2rad_ecef(lat_n) - g.la), d = (float)(g.la - deg2rad_ecef(lat_s));
+  const float sp = (float)g.sla, cp = (float)g.cla, sl = (float)g.slo, cl = (float)g.clo;
+  const float e2 = (float)WGS84_E2;
+  const float den = 1.f - e2 * sp * sp;
+  const float N = (float)WGS84_A * rsqrtf(den);
+  const float dN = N * e2 * sp * cp / den;
+  const float B = N * (1.f - e2), dB = dN * (1.f - e2);
+  const float dh = he - hw;
+  const float q = fmaf(N + he, a, (N + hw) * b);
+  const float ex = cp * (cl * dh - sl * q), ey = cp * (sl * dh + cl * q), ez = sp * dh;
+  const float dv = hn - hs;
+  const float An = cp * fmaf(dN, c + d, dv) - sp * fmaf(N + hn, c, (N + hs) * d);
+  const float nx = cl * An, ny = sl * An;
+  const float nz = sp * fmaf(dB, c + d, dv) + cp * fmaf(B + hn, c, (B + hs) * d);
+  f.nx = ey * nz - ez * ny;
+  f.ny = ez * nx - ex * nz;
+  f.nz = ex * ny - ey * nx;
+  f.area = sqrtf(f.nx * f.nx + f.ny * f.ny + f.nz * f.nz);
+  return f;
+}
+
+// cand_post in split precision; *redo is set when a mask decision falls
+// inside the FP32 error margin and the FP64 candidate must decide.
+__device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g, V3 S, const FacetF &f,
+                               float flat_area, bool *redo) {
+  CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
+  *redo = false;
+  if (!c.inside) return o;
+  float sigma0 = c.sigma0;
+  float cosv = NAN;
+  if (p.need_geom) {
+    if (!f.ok) {
+      if (p.flatten) return {NAN, cosv, (uint8_t)SD_MASK_DEM_NEIGHBOUR_MISSING, 5};
+    } else {
+      const float lx = (float)(S.x - g.P.x), ly = (float)(S.y - g.P.y), lz = (float)(S.z - g.P.z);
+      const float il = rsqrtf(lx * lx + ly * ly + lz * lz);
+      const float lp = (f.nx * lx + f.ny * ly + f.nz * lz) * il;
+      if (fabsf(lp) <= 1e-4f * f.area) { *redo = true; return o; }
+      if (lp <= 0.f || f.area == 0.f) {
+        if (p.flatten) return {NAN, cosv, (uint8_t)SD_MASK_SHADOW, 5};
+      } else {
+        const float w = lp / flat_area;
+        if (fabsf(w - 0.05f) <= 5e-6f || fabsf(w - 2.0f) <= 2e-4f) { *redo = true; return o; }
+        cosv = fminf(fmaxf(lp / f.area, 0.f), 1.f);
+        if (w < 0.05f || w > 2.0f) {
+          if (p.flatten) return {NAN, cosv, (uint8_t)(w > 2.0f ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING), 5};
+        } else if (p.flatten) {
+          sigma0 /= w;
+        }
+      }
+    }
+  }
+  if (p.nesz_mask) {
+    bool nz_redo = false;
+    float nz = sample_bilinear_f(p.nesz, p.lines, p.samples, c.line, c.sample, &nz_redo);
+    if (nz == nz) {
+      float thr = nz * p.nesz_factor;
+      if (nz_redo || fabsf(sigma0 - thr) <= 1e-5f * fabsf(thr)) { *redo = true; return o; }
+      if (sigma0 <= thr) return {NAN, cosv, (uint8_t)SD_MASK_NOISE_MASKED, 6};
+    }
+  }
+  return {sigma0, cosv, (uint8_t)SD_MASK_VALID, 0};
+}
+
+// One candidate's output from scratch (exact-path pixels, and split-precision
+// candidates whose mask FP32 cannot settle).
+template <int KERNEL>
+__device__ CandOut cand_fp64(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area) {
+  CandPre pre = cand_pre<KERNEL, false>(p, g.P, S, t);
+  Facet f{};
+  if (pre.inside && p.need_geom) f = pixel_facet(p, g);
+  return cand_post(p, pre, g.P, S, f, flat_area);
+}
+
+template <int KERNEL, bool SPLIT>
+__device__ CandOut cand_full(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area) {
+  if (!SPLIT) return cand_fp64<KERNEL>(p, g, S, t, flat_area);
+  CandPre pre = cand_pre<KERNEL, true>(p, g.P, S, t);
+  FacetF f{};
+  if (pre.inside && p.need_geom) f = pixel_facet_f(p, g);
+  bool redo;
+  CandOut o = cand_post_f(p, pre, g, S, f, (float)flat_area, &redo);
+  return redo ? cand_fp64<KERNEL>(p, g, S, t, flat_area) : o;
+}
+
+// ── per-pixel stores ─────────────────────────────────────────────────────────
+// Rec: the fixed-point pair F = {fb, fb+1} and the pixel's output for each
+// member.  cc: codes (outcome of the reference iteration seeded at each
+// member of the left neighbour's F), F membership and flags.
+struct __align__(16) Rec {
+  int64_t fb;
+  float data[2];
+  float cos[2];
+  uint8_t omask[2];
+  uint8_t ocls[2];
+  uint32_t pad;
+};
+enum : uint32_t { CF_DEMMISS = 1u << 18, CF_HASF = 1u << 19, CF_HASOUT = 1u << 20 };
+// sel byte written by the scan: low 3 bits = outcome, high 4 bits = iterations
+enum : uint8_t { SEL_M0 = 0, SEL_M1 = 1, SEL_DONE = 2, SEL_NONCONV = 3, SEL_DEGEN = 4, SEL_DEMMISS = 5,
+                 SEL_ORBIT = 6 };
+
+struct Ent {  // one orbit-table record
+  double px, py, pz, vx, vy, vz, ax, ay, az, vsq;
+};
+
+__device__ __forceinline__ int ent_at(const OrbitDev &o, int64_t t, Ent *e) {
+  OrbitState s;
+  double vsq;
+  int rc = orbit_at(o, t, &s, &vsq);
+  if (rc != ORB_OK) return rc;
+  *e = {s.pos.x, s.pos.y, s.pos.z, s.vel.x, s.vel.y, s.vel.z, s.acc.x, s.acc.y, s.acc.z, vsq};
+  return ORB_OK;
+}
+
+// One evaluation of the Newton step at a tabulated state (1030-1053).
+// Returns 0 = converged (|delta| < tol), 1 = step, 2 = degenerate.
+__device__ __forceinline__ int zd_eval(V3 P, const Ent &e, double tol, double *delta) {
+  V3 r = {P.x - e.px, P.y - e.py, P.z - e.pz};
+  double f = r.x * e.vx + r.y * e.vy + r.z * e.vz;
+  double fp = -e.vsq + (r.x * e.ax + r.y * e.ay + r.z * e.az);
+  if (fabs(fp) < 1.0) return 2;
+  double d = -f / fp;
+  *delta = d;
+  return fabs(d) < tol ? 0 : 1;
+}
+
+struct Slot {  // shared-memory record exchanged with the right-hand neighbour
+  int64_t fb;
+  int32_t fmask;
+  int32_t pad;
+  Ent e[2];
+};
+
+constexpr int MAIN_THREADS = 128;
+constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
+
+// ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
+// One k_main work item: MAIN_PIX pixels of row r starting at chunk * MAIN_PIX
+// (plus the left neighbour on thread 0).  Every thread of the block calls it.
+template <int KERNEL, bool SPLIT>
+__device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t chunk, Slot *slot) {
+  const int tid = threadIdx.x;
+  const int fast = p.fast;
+  const int64_t c = (int64_t)chunk * MAIN_PIX + tid - 1;
+  const bool in_row = c >= 0 && c < (int64_t)p.cols;
+  const uint64_t i = r * p.cols + (uint64_t)(c < 0 ? 0 : c);
+  PixGeo g;
+  bool geo_ok = false;
+  int fmask = 0;
+  int64_t fb = 0;
+  Ent e0{}, e1{};
+  // The warp's 32 pixels lie within ~10 ms of azimuth time: all lanes take
+  // their first Newton step from one shared state (one broadcast read), the
+  // landing point is within a few ns of each lane's own root.
+  const uint64_t rr = r < p.rows ? r : p.rows - 1;
+  const uint64_t cq = c < 0 ? 0 : ((uint64_t)c < p.cols ? (uint64_t)c : p.cols - 1);
+  const int64_t uw = __shfl_sync(0xffffffffu, predicted_time(p, rr, cq), 16);
+  Ent ew;
+  const bool ew_ok = fast && ent_at(p.orb, uw, &ew) == ORB_OK;
+  if (in_row && r < p.rows) {
+    geo_ok = pixel_geo(p, r, (uint64_t)c, &g);
+    if (geo_ok && fast) {
+      // reference iteration from the shared state: one converged t*
+      int64_t t = ew_ok ? uw : predicted_time(p, r, (uint64_t)c);
+      Ent e;
+      double d = 0.0;
+      int st = 1;
+      for (int it = 0; it < 40 && st == 1; ++it) {
+        if (it == 0 && ew_ok) e = ew;
+        else if (ent_at(p.orb, t, &e) != ORB_OK) { st = 3; break; }
+        st = zd_eval(g.P, e, p.tol, &d);
+        if (st == 1) t = t + f2i64(d * 1e6);
+      }
+      if (st == 0) {
+        // F = {t : |delta(t)| < tol} lies in {t*-1, t*, t*+1}.  The root sits
+        // at t* + d; delta carries ~1e-13 s of rounding noise (the dot
+        // product cancels terms of ~6e9), so for |d| >= 1e-11 s only
+        // t* + sign(d) can join t*, while for smaller |d| both neighbours are
+        // evaluated.  A three-member F is left to the exact path.
+        Ent ea, eb;
+        double da = 0.0, db = 0.0;
+        const int64_t ta = d > 0.0 ? t + 1 : t - 1;   // the likely member
+        const bool ma = ent_at(p.orb, ta, &ea) == ORB_OK && zd_eval(g.P, ea, p.tol, &da) == 0;
+        bool mb = false;
+        const int64_t tb = d > 0.0 ? t - 1 : t + 1;
+        if (fabs(d) < 1e-11) mb = ent_at(p.orb, tb, &eb) == ORB_OK && zd_eval(g.P, eb, p.tol, &db) == 0;
+        if (!(ma && mb)) {
+          const bool use_b = mb;                      // pair {t*, tb} when only tb joins
+          const int64_t other = use_b ? tb : ta;
+          const Ent &eo = use_b ? eb : ea;
+          const bool om = use_b ? mb : ma;
+          if (other > t) {
+            fb = t; e0 = e; e1 = eo; fmask = 1 | (om ? 2 : 0);
+          } else {
+            fb = other; e0 = eo; e1 = e; fmask = 2 | (om ? 1 : 0);
+          }
+        }
+      }
+    }
+  }
+  slot[tid].fb = fb;
+  slot[tid].fmask = fmask;
+  slot[tid].e[0] = e0;
+  slot[tid].e[1] = e1;
+  __syncthreads();
+  if (tid == 0 || !in_row || r >= p.rows) return;
+
+  uint32_t cc = 0xFFFFu;
+  Rec rec;
+  rec.fb = fb;
+  rec.pad = 0;
+  rec.data[0] = rec.data[1] = NAN;
+  rec.cos[0] = rec.cos[1] = NAN;
+  rec.omask[0] = rec.omask[1] = SD_MASK_OUTSIDE_FOOTPRINT;
+  rec.ocls[0] = rec.ocls[1] = 2;
+  if (!geo_ok) {
+    cc |= CF_DEMMISS;
+  } else if (fmask) {
+    cc |= CF_HASF | ((uint32_t)fmask << 16);
+    // outcome of the reference iteration seeded at each member of the left
+    // neighbour's F (the only seeds the row walk can hand this pixel)
+    const Slot &L = slot[tid - 1];
+    if (c > 0 && L.fmask) {
+      for (int k = 0; k < 2; ++k) {
+        if (!((L.fmask >> k) & 1)) continue;
+        int64_t t = L.fb + k;
+        uint32_t code = 0xFF;
+        for (int it = 0; it < p.max_iter; ++it) {
+          Ent e;
+          bool have = true;
+          if (t == L.fb + k) e = L.e[k];
+          else if (t == fb && (fmask & 1)) e = e0;
+          else if (t == fb + 1 && (fmask & 2)) e = e1;
+          else have = ent_at(p.orb, t, &e) == ORB_OK;
+          if (!have) break;  // orbit error: the walk redoes it
+          double d;
+          int st = zd_eval(g.P, e, p.tol, &d);
+          if (st == 0) {
+            int64_t m = t - fb;
+            if ((m == 0 || m == 1) && ((fmask >> m) & 1)) code = (uint32_t)m | ((uint32_t)min(it + 1, 15) << 4);
+            break;
+          }
+          if (st == 2) {
+            code = 3u | (2u << 2) | ((uint32_t)min(it, 15) << 4);
+            break;
+          }
+          t = t + f2i64(d * 1e6);
+          if (it + 1 == p.max_iter) code = 3u | (1u << 2) | ((uint32_t)min(p.max_iter, 15) << 4);
+        }
+        cc = (cc & ~(0xFFu << (8 * k))) | (code << (8 * k));
+      }
+    }
+    // outputs for both members of F
+    CandPre pre[2];
+    bool need = false;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const Ent &e = k == 0 ? e0 : e1;
+      if ((fmask >> k) & 1) {
+        pre[k] = cand_pre<KERNEL, SPLIT>(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
+        need = need || pre[k].inside;
+      } else {
+        pre[k].inside = false;
+      }
+    }
+    const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+    if constexpr (SPLIT) {
+      FacetF f{};
+      if (need && p.need_geom) f = pixel_facet_f(p, g);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const Ent &e = k == 0 ? e0 : e1;
+        if (!((fmask >> k) & 1)) continue;
+        const V3 S{e.px, e.py, e.pz};
+        bool redo;
+        CandOut o = cand_post_f(p, pre[k], g, S, f, (float)flat_area, &redo);
+        if (redo) o = cand_fp64<KERNEL>(p, g, S, fb + k, flat_area);
+        rec.data[k] = o.data;
+        rec.cos[k] = o.cos;
+        rec.omask[k] = o.mask;
+        rec.ocls[k] = o.cls;
+      }
+    } else {
+      Facet f{};
+      if (need && p.need_geom) f = pixel_facet(p, g);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const Ent &e = k == 0 ? e0 : e1;
+        if (!((fmask >> k) & 1)) continue;
+        CandOut o = cand_post(p, pre[k], g.P, V3{e.px, e.py, e.pz}, f, flat_area);
+        rec.data[k] = o.data;
+        rec.cos[k] = o.cos;
+        rec.omask[k] = o.mask;
+        rec.ocls[k] = o.cls;
+      }
+    }
+    cc |= CF_HASOUT;
+  }
+  p.rec[i] = rec;
+  p.cc[i] = cc;
+}
+
+// Single job: the job record is a kernel parameter (constant-bank operands)
+// and the grid covers its rows x bpr items.
+template <int KERNEL, bool SPLIT>
+__global__ void __launch_bounds__(MAIN_THREADS, 4) k_main(TcDev p) {
+  __shared__ Slot slot[MAIN_THREADS];
+  main_item<KERNEL, SPLIT>(p, blockIdx.x / p.bpr, blockIdx.x % p.bpr, slot);
+}
+
+// Tile batches: persistent CTAs over the work table; the current job's
+// record is staged in shared memory.
+template <int KERNEL, bool SPLIT>
+__global__ void __launch_bounds__(MAIN_THREADS, 4) k_main_batch(const TcWork *__restrict__ wp) {
+  __shared__ Slot slot[MAIN_THREADS];
+  __shared__ __align__(16) unsigned char s_job[sizeof(TcDev)];
+  __shared__ int s_j;
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_MAIN);
+  const uint64_t total = pre[w.n_jobs];
+  const TcDev &p = *reinterpret_cast<const TcDev *>(s_job);
+  const int tid = threadIdx.x;
+  int cur = -1;
+  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    __syncthreads();  // the previous item is done with slot[] and the job record
+    if (tid == 0) s_j = find_job(pre, w.n_jobs, item);
+    __syncthreads();
+    const int jb = s_j;
+    if (jb != cur) {
+      load_job(s_job, w.jobs + jb, tid, MAIN_THREADS);
+      __syncthreads();
+      cur = jb;
+    }
+    const uint64_t li = item - pre[jb];
+    main_item<KERNEL, SPLIT>(p, li / p.bpr, li % p.bpr, slot);
+  }
+}
+
+// ── K4: the row walk ──────────────────────────────────────────────────────
+// The walk's state between two pixels is either an index into the recorded
+// F of the previous pixel (kind 0) or an explicit seed time (kind 1, after a
+// DEM void, a non-converged solve or an exact-path pixel); kind 2 marks an
+// entry that cannot occur.
+struct WState {
+  int kind;
+  int64_t v;
+};
+
+// The reference solve of pixel (r, c) from seed s, for pixels the
+// precomputed records do not cover.  With `write`, it also stores the
+// pixel's outputs when the converged time has none precomputed.
+template <int KERNEL, bool SPLIT>
+__device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s, uint32_t cc, int64_t fb,
+                              bool write, uint8_t *sel) {
+  const uint64_t i = r * p.cols + c;
+  PixGeo g;
+  if (!pixel_geo(p, r, c, &g)) {
+    *sel = SEL_DEMMISS;
+    return {1, s};
+  }
+  ZdRes z = newton(p.orb, g.P, s, p.max_iter, p.tol);
+  if (z.st == ST_ORBIT) {
+    if (write) atomicOr(&p.flags[0], 1);
+    *sel = SEL_ORBIT;
+    return {1, s};
+  }
+  if (z.st == ST_NONCONV || z.st == ST_DEGEN) {
+    *sel = z.st == ST_NONCONV ? SEL_NONCONV : SEL_DEGEN;
+    return {1, s};
+  }
+  const int it = z.it > 15 ? 15 : z.it;
+  if (cc & CF_HASOUT) {
+    const uint32_t fm = (cc >> 16) & 3u;
+    const int64_t m = z.t - fb;
+    if ((m == 0 || m == 1) && ((fm >> m) & 1)) {
+      *sel = (uint8_t)(m | (it << 4));
+      return {0, m};
+    }
+  }
+  *sel = (uint8_t)(SEL_DONE | (it << 4));
+  if (write) {
+    atomicAdd(&p.flags[1], 1);
+    OrbitState os;
+    double vsq;
+    orbit_at(p.orb, z.t, &os, &vsq);
+    CandOut o = cand_full<KERNEL, SPLIT>(p, g, os.pos, z.t, p.need_geom ? p.row_flat[r] : 0.0);
+    p.out[i] = o.data;
+    if (p.compute_lia) {
+      p.cos_lia[i] = o.cos;
+      p.mask[i] = o.mask;
+    }
+    if (p.az_time) p.az_time[i] = z.t;
+    p.rec[i].ocls[0] = o.cls;
+  }
+  return {1, z.t};
+}
+
+// Walk columns [b, e) of row r from state st (terrain_correction.rs:
+// 1443-1580), any pixel kind.  fb is read only where a seed value is needed.
+template <int KERNEL, bool SPLIT>
+__device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, WState st, bool write) {
+  const uint64_t base = r * p.cols;
+  uint32_t prev_cc = b > 0 ? p.cc[base + b - 1] : CF_DEMMISS;
+  if (st.kind == 0 && !((prev_cc & CF_HASF) && ((prev_cc >> (16 + st.v)) & 1u))) return {2, 0};
+  for (uint64_t c = b; c < e; ++c) {
+    const uint32_t cc = p.cc[base + c];
+    uint8_t sel;
+    if (cc & CF_DEMMISS) {
+      if (st.kind == 0) st = {1, p.rec[base + c - 1].fb + st.v};  // the seed passes through the void
+      sel = SEL_DEMMISS;
+    } else {
+      uint32_t code = 0xFF;
+      if (st.kind == 0 && (prev_cc & CF_HASF) && (cc & CF_HASOUT)) code = (cc >> (8 * st.v)) & 0xFFu;
+      if (code != 0xFF && (code & 3u) != 3u) {
+        st = {0, (int64_t)(code & 3u)};
+        sel = (uint8_t)((code & 3u) | (code & 0xF0u));
+      } else if (code != 0xFF) {
+        st = {1, p.rec[base + c - 1].fb + st.v};  // not converged: seed unchanged
+        sel = (uint8_t)((((code >> 2) & 3u) == 1u ? SEL_NONCONV : SEL_DEGEN) | (code & 0xF0u));
+      } else {
+        const int64_t s = st.kind == 0 ? p.rec[base + c - 1].fb + st.v : st.v;
+        st = exact_pixel<KERNEL, SPLIT>(p, r, c, s, cc, p.rec[base + c].fb, write, &sel);
+      }
+    }
+    if (write) p.sel[base + c] = sel;
+    prev_cc = cc;
+  }
+  return st;
+}
+
+// One warp per row.  Lane 0 resolves the row's first valid pixel from the
+// LUT guess; the remaining columns are cut into 32 segments, each lane maps
+// the two possible entry states (which member of the left F the seed is)
+// through its segment, the maps are composed in lane order (a lane whose
+// entry is an explicit seed walks its segment at that point), and each lane
+// writes its segment from its actual entry.  In the regular case the
+// segments are streamed 32 columns at a time through shared memory with
+// coalesced transposed loads and stores; a segment with any other pixel
+// kind is (re)done by walk_seg.
+constexpr int SCAN_WARPS = 4;
+
+template <int KERNEL, bool SPLIT>
+__global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restrict__ wp) {
+  __shared__ uint32_t sbuf[SCAN_WARPS][32][33];
+  __shared__ __align__(16) unsigned char s_job[SCAN_WARPS][sizeof(TcDev)];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t(*buf)[33] = sbuf[wid];
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_SCAN);
+  const uint64_t total = pre[w.n_jobs];
+  const TcDev &p = *reinterpret_cast<const TcDev *>(s_job[wid]);
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  int cur = -1;
+  for (uint64_t item = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < total;
+       item += nwarps) {  // one output row per warp and item
+  const int jb = find_job(pre, w.n_jobs, item);
+  __syncwarp();
+  if (jb != cur) {
+    load_job(s_job[wid], w.jobs + jb, lane, 32);
+    __syncwarp();
+    cur = jb;
+  }
+  const uint64_t r = item - pre[jb];
+  const uint64_t n = p.cols, base = r * n;
+  const uint32_t *ccr = p.cc + base;
+  uint64_t c0 = n;
+  WState st0{1, 0};
+  if (lane == 0) {
+    uint64_t c = 0;
+    while (c < n && (ccr[c] & CF_DEMMISS)) {
+      p.sel[base + c] = SEL_DEMMISS;
+      ++c;
+    }
+    if (c < n) {
+      st0 = walk_seg<KERNEL, SPLIT>(p, r, c, c + 1, WState{1, p.row_guess[r]}, true);
+      c0 = c + 1;
+    }
+  }
+  c0 = __shfl_sync(0xffffffffu, c0, 0);
+  st0.kind = __shfl_sync(0xffffffffu, st0.kind, 0);
+  st0.v = __shfl_sync(0xffffffffu, st0.v, 0);
+  if (c0 >= n) continue;
+  const uint64_t seg = (n - c0 + 31) / 32;
+  const uint64_t b = c0 + (uint64_t)lane * seg;
+  const uint64_t e = min(n, b + seg);
+  const int nchunks = (int)((seg + 31) / 32);
+
+  // phase 1: both entry states through the segment (regular pixels only)
+  int s0 = 0, s1 = 1, bad = 0;
+  if (b < e) {
+    const uint32_t prev = ccr[b - 1];
+    if (!((prev & CF_HASF) && ((prev >> 16) & 1u))) bad |= 1;
+    if (!((prev & CF_HASF) && ((prev >> 17) & 1u))) bad |= 2;
+  }
+  for (int k = 0; k < nchunks; ++k) {
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t bj = c0 + (uint64_t)j * seg, ej = min(n, bj + seg);
+      const uint64_t idx = bj + 32 * (uint64_t)k + lane;
+      buf[j][lane] = idx < ej ? __ldg(ccr + idx) : 0u;
+    }
+    __syncwarp();
+    const int cnt = b + 32 * (uint64_t)k < e ? (int)min((uint64_t)32, e - b - 32 * (uint64_t)k) : 0;
+    for (int t = 0; t < cnt; ++t) {
+      const uint32_t w = buf[lane][t];
+      if ((w & (CF_DEMMISS | CF_HASOUT)) != CF_HASOUT) bad = 3;
+      const uint32_t x0 = (w >> (8 * s0)) & 0xFFu, x1 = (w >> (8 * s1)) & 0xFFu;
+      if (x0 == 0xFFu || (x0 & 3u) == 3u) bad |= 1;
+      if (x1 == 0xFFu || (x1 & 3u) == 3u) bad |= 2;
+      s0 = (int)(x0 & 1u);
+      s1 = (int)(x1 & 1u);
+    }
+    __syncwarp();
+  }
+  WState ex0 = {0, 0}, ex1 = {0, 1};
+  if (b < e) {
+    ex0 = (bad & 1) ? walk_seg<KERNEL, SPLIT>(p, r, b, e, WState{0, 0}, false) : WState{0, s0};
+    ex1 = (bad & 2) ? walk_seg<KERNEL, SPLIT>(p, r, b, e, WState{0, 1}, false) : WState{0, s1};
+  }
+  // phase 2: compose the lanes' maps in order
+  WState st = st0, entry{2, 0};
+  for (int j = 0; j < 32; ++j) {
+    WState nx = st;
+    if (lane == j) {
+      entry = st;
+      if (b < e) {
+        if (st.kind == 0) nx = st.v == 0 ? ex0 : ex1;
+        else nx = walk_seg<KERNEL, SPLIT>(p, r, b, e, st, false);
+      }
+    }
+    st.kind = __shfl_sync(0xffffffffu, nx.kind, j);
+    st.v = __shfl_sync(0xffffffffu, nx.v, j);
+  }
+  // phase 3: write the segments
+  const bool regular = b < e && entry.kind == 0 && !((bad >> entry.v) & 1);
+  int s = regular ? (int)entry.v : 0;
+  uint8_t *selr = p.sel + base;
+  for (int k = 0; k < nchunks; ++k) {
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t bj = c0 + (uint64_t)j * seg, ej = min(n, bj + seg);
+      const uint64_t idx = bj + 32 * (uint64_t)k + lane;
+      buf[j][lane] = idx < ej ? __ldg(ccr + idx) : 0u;
+    }
+    __syncwarp();
+    if (regular) {
+      const int cnt = b + 32 * (uint64_t)k < e ? (int)min((uint64_t)32, e - b - 32 * (uint64_t)k) : 0;
+      for (int t = 0; t < cnt; ++t) {
+        const uint32_t code = (buf[lane][t] >> (8 * s)) & 0xFFu;
+        s = (int)(code & 3u);
+        buf[lane][t] = (uint32_t)(s | (code & 0xF0u));
+      }
+    }
+    __syncwarp();
+    for (int j = 0; j < 32; ++j) {
+      const uint64_t bj = c0 + (uint64_t)j * seg, ej = min(n, bj + seg);
+      const uint64_t idx = bj + 32 * (uint64_t)k + lane;
+      const bool reg_j = __shfl_sync(0xffffffffu, regular, j);
+      if (reg_j && idx < ej) selr[idx] = (uint8_t)buf[j][lane];
+    }
+    __syncwarp();
+  }
+  if (b < e && !regular) walk_seg<KERNEL, SPLIT>(p, r, b, e, entry, true);
+  }
+}
+
+// ── K5: final rasters, counters and Newton histogram ────────────────────────
+__global__ void __launch_bounds__(SEL_THREADS) k_select(const TcWork *__restrict__ wp) {
+  __shared__ unsigned int s_cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_SEL);
+  const uint64_t total = pre[w.n_jobs];
+  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    const int jb = find_job(pre, w.n_jobs, item);
+    const TcDev &p = w.jobs[jb];
+    __syncthreads();  // the previous item's flush is done
+    for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
+    __syncthreads();
+    const uint64_t npx = p.rows * p.cols;
+    const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
+    if (i < npx) {
+      const uint8_t sel = p.sel[i];
+      const int code = sel & 7, it = sel >> 4;
+      int counter = -1;
+      if (code == SEL_M0 || code == SEL_M1) {
+        const Rec &rc = p.rec[i];
+        counter = rc.ocls[code];
+        atomicAdd(&s_cnt[kCounters + it], 1u);
+        p.out[i] = rc.data[code];
+        if (p.compute_lia) {
+          p.cos_lia[i] = rc.cos[code];
+          p.mask[i] = rc.omask[code];
+        }
+        if (p.az_time) p.az_time[i] = rc.fb + code;
+      } else if (code == SEL_DONE) {
+        counter = p.rec[i].ocls[0];
+        atomicAdd(&s_cnt[kCounters + it], 1u);
+      } else if (code != SEL_ORBIT) {
+        uint8_t m = code == SEL_NONCONV ? SD_MASK_NON_CONVERGED
+                    : code == SEL_DEGEN ? SD_MASK_DEGENERATE_GEOMETRY
+                                        : SD_MASK_DEM_MISSING;
+        counter = code == SEL_NONCONV ? 3 : (code == SEL_DEGEN ? 4 : 1);
+        if (p.az_time) p.az_time[i] = INT64_MIN;
+        p.out[i] = NAN;
+        if (p.compute_lia) {
+          p.cos_lia[i] = NAN;
+          p.mask[i] = m;
+        }
+      }
+      if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
+      if (s_cnt[k]) atomicAdd(&p.counters[k], (unsigned long long)s_cnt[k]);
+  }
+}
+
+}  // namespace
+}  // namespace sd
+
+namespace sd {
+namespace {
+
+// ── work tables and stage launches (host) ───────────────────────────────────
+struct TcWorkHost {
+  uint64_t totals[kWk];
+  TcDev *d_jobs;  // device address of the job records
+};
+
+size_t al16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+size_t work_bytes(int n) {
+  return al16(sizeof(TcWork)) + al16((size_t)n * sizeof(TcDev)) + (size_t)kWk * (size_t)(n + 1) * 8;
+}
+
+uint64_t stage_items(int stage, const TcDev &p) {
+  switch (stage) {
+    case WK_ANCH: return p.utm ? p.rows * (uint64_t)p.n_pts : 0;
+    case WK_ROWS: return p.rows;
+    case WK_KNOT: return p.rows * KNOTS;
+    case WK_MAIN: return p.rows * p.bpr;
+    case WK_SCAN: return p.rows;
+    default: return (p.rows * p.cols + SEL_THREADS - 1) / SEL_THREADS;
+  }
+}
+
+// Lays out the table for `n` jobs in host memory `h`, addressed for the
+// device copy at `d`: TcWork | TcDev[n] | pre[kWk][n + 1].
+void work_layout(const TcDev *jobs, int n, unsigned char *h, unsigned char *d, TcWorkHost *wk) {
+  const size_t o_jobs = al16(sizeof(TcWork));
+  const size_t o_pre = o_jobs + al16((size_t)n * sizeof(TcDev));
+  TcWork w{};
+  w.n_jobs = n;
+  w.jobs = reinterpret_cast<const TcDev *>(d + o_jobs);
+  w.pre = reinterpret_cast<const uint64_t *>(d + o_pre);
+  std::memcpy(h, &w, sizeof w);
+  std::memcpy(h + o_jobs, jobs, (size_t)n * sizeof(TcDev));
+  uint64_t *pre = reinterpret_cast<uint64_t *>(h + o_pre);
+  for (int st = 0; st < kWk; ++st) {
+    uint64_t acc = 0;
+    for (int j = 0; j < n; ++j) {
+      pre[st * (n + 1) + j] = acc;
+      acc += stage_items(st, jobs[j]);
+    }
+    pre[st * (n + 1) + n] = acc;
+    wk->totals[st] = acc;
+  }
+  wk->d_jobs = reinterpret_cast<TcDev *>(d + o_jobs);
+}
+
+int work_upload(sd_ctx *ctx, const char *name, const TcDev *jobs, int n, TcWorkHost *wk, TcWork **d_work) {
+  const size_t bytes = work_bytes(n);
+  void *d = nullptr;
+  SD_TRY(scratch(ctx, name, bytes, &d));
+  std::vector<unsigned char> h(bytes);
+  work_layout(jobs, n, h.data(), (unsigned char *)d, wk);
+  // pageable source: the copy is staged before the call returns
+  SD_CUDA(ctx, cudaMemcpyAsync(d, h.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+  *d_work = (TcWork *)d;
+  return SD_OK;
+}
+
+// work blocks of `items` items, `per` per block (~0 = a full resident grid)
+uint64_t blocks_for(uint64_t items, unsigned per) { return items == ~0ull ? ~0ull : grid_for(items, per); }
+
+int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
+  cudaStream_t st = ctx->stream;
+  if (totals[WK_ANCH]) {
+    SD_TIMED_BEGIN(ctx, "k_row_anchors");
+    k_row_anchors<<<persistent_grid(k_row_anchors, 128, 0, blocks_for(totals[WK_ANCH], 128)), 128, 0, st>>>(d_work);
+    SD_LAUNCHED(ctx);
+  }
+  SD_TIMED_BEGIN(ctx, "k_row_setup");
+  k_row_setup<<<persistent_grid(k_row_setup, 128, 0, blocks_for(totals[WK_ROWS], 128)), 128, 0, st>>>(d_work);
+  SD_LAUNCHED(ctx);
+  SD_TIMED_BEGIN(ctx, "k_row_model");
+  k_row_model<<<persistent_grid(k_row_model, 128, 0, blocks_for(totals[WK_KNOT], 128)), 128, 0, st>>>(d_work);
+  SD_LAUNCHED(ctx);
+  return SD_OK;
+}
+
+// job: the single job's record (parameter form of k_main), or null for the
+// persistent work-table form.
+template <int K, bool S>
+int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const char *name,
+                    const TcDev *job) {
+  cudaStream_t st = ctx->stream;
+  SD_TIMED_BEGIN(ctx, name);
+  if (job) {
+    if (totals[WK_MAIN] > 0x7FFFFFFFull)
+      return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "output grid too large");
+    k_main<K, S><<<(unsigned)std::max<uint64_t>(totals[WK_MAIN], 1), MAIN_THREADS, 0, st>>>(*job);
+  } else {
+    k_main_batch<K, S><<<persistent_grid(k_main_batch<K, S>, MAIN_THREADS, 0, totals[WK_MAIN]), MAIN_THREADS, 0,
+                         st>>>(d_work);
+  }
+  SD_LAUNCHED(ctx);
+  SD_TIMED_BEGIN(ctx, "k_scan");
+  k_scan<K, S><<<persistent_grid(k_scan<K, S>, SCAN_WARPS * 32, 0, blocks_for(totals[WK_SCAN], SCAN_WARPS)),
+                 SCAN_WARPS * 32, 0, st>>>(d_work);
+  SD_LAUNCHED(ctx);
+  SD_TIMED_BEGIN(ctx, "k_select");
+  k_select<<<persistent_grid(k_select, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
+  SD_LAUNCHED(ctx);
+  return SD_OK;
+}
+
+// FP64 Lagrange state at every microsecond of [t0, t1] into scratch `name`
+// (capped at 96 M entries, 7.7 GB, centred on [tmin, tmax]).
+int build_orbit_table(sd_ctx *ctx, const char *name, const sd_state_vector *d_svs, uint64_t nsv, int64_t t0,
+                      int64_t t1, int64_t tmin, int64_t tmax, OrbitDev *orb) {
+  const int64_t max_entries = 96ll * 1000 * 1000;
+  if (t1 - t0 + 1 > max_entries) {
+    const int64_t mid = (tmin / 2 + tmax / 2);
+    t0 = std::max(t0, mid - max_entries / 2);
+    t1 = std::min(t1, t0 + max_entries - 1);
+  }
+  if (t1 < t0) return SD_OK;
+  double2 *d_tab;
+  SD_TRY(scratch_t(ctx, name, (size_t)(t1 - t0 + 1) * 5, &d_tab));
+  SD_TIMED_BEGIN(ctx, "k_orbit_table");
+  k_orbit_table<<<grid_for((size_t)(t1 - t0 + 1), 128), 128, 0, ctx->stream>>>(d_svs, nsv, t0, t1 - t0 + 1, d_tab);
+  SD_LAUNCHED(ctx);
+  orb->tab = d_tab;
+  orb->tab_t0 = t0;
+  orb->tab_n = t1 - t0 + 1;
+  return SD_OK;
+}
+
+}  // namespace
+}  // namespace sd

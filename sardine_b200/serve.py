@@ -1,0 +1,173 @@
+"""Served geocoding: a device-resident request loop with continuous batching.
+
+Scenes stay resident in HBM (`tiles.ResidentScene`).  Tile requests arrive
+at any time; each scheduler step
+
+  1. collects every slot whose batch has finished (its requests complete,
+     their scratch leaves the HBM budget),
+  2. admits queued requests, oldest first, into a batch for a free slot while
+     the batch fits the slot's share of the HBM budget and `max_batch`,
+  3. launches that batch asynchronously (one persistent launch per stage,
+     replayed from a CUDA graph).
+
+A slot is a context (CUDA stream + reserved scratch arena); with two or more
+slots, a batch admitted while another is on the GPU runs concurrently with
+it.  Requests never wait for a batch boundary longer than one in-flight
+batch per slot.  A request's result does not depend on the batch it lands in
+(each tile is an independent job of the launch).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Callable, Deque, List, Optional
+
+from ._lib import Context, lib
+from .tiles import TileBatch, TileRequest
+
+
+@dataclass
+class Ticket:
+    """One submitted request and, once done, its result and timings."""
+    request: TileRequest
+    t_submit: float
+    t_launch: float = 0.0
+    t_done: float = 0.0
+    result: object = None
+    error: Optional[BaseException] = None
+
+    @property
+    def latency_s(self) -> float:
+        return self.t_done - self.t_submit
+
+    @property
+    def done(self) -> bool:
+        return self.t_done > 0.0
+
+
+class _Slot:
+    def __init__(self, device: int, arena_bytes: int, graphs: bool):
+        self.ctx = Context(device)
+        self.capacity = arena_bytes
+        lib().sd_ctx_set_graphs(self.ctx.handle, int(graphs))
+        if arena_bytes:
+            rc = lib().sd_ctx_reserve(self.ctx.handle, C.c_uint64(arena_bytes))
+            if rc != 0:
+                raise MemoryError(self.ctx.last_error())
+        self.batch: Optional[TileBatch] = None
+        self.tickets: List[Ticket] = []
+        self.bytes = 0
+
+    def launch(self, requests):
+        return TileBatch(self.ctx, requests).launch()
+
+    def close(self):
+        self.ctx.close()
+
+
+class GeocodingServer:
+    """Continuous-batching request loop over resident scenes on one GPU.
+
+    hbm_budget: device bytes the in-flight batches may hold for tile scratch
+    (split evenly over `slots`; each slot reserves its share up front, so the
+    loop itself never allocates device memory for scratch).
+    """
+
+    def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, slots: int = 2,
+                 max_batch: int = 64, graphs: bool = True,
+                 clock: Callable[[], float] = time.perf_counter, slot_factory=None):
+        if slots < 1:
+            raise ValueError("slots must be >= 1")
+        self.clock = clock
+        self.max_batch = max_batch
+        make = slot_factory or (lambda cap: _Slot(device, cap, graphs))
+        self.slots = [make(hbm_budget // slots) for _ in range(slots)]
+        self.queue: Deque[Ticket] = deque()
+        self.completed: List[Ticket] = []
+
+    # ── client side ──
+    def submit(self, req: TileRequest) -> Ticket:
+        t = Ticket(req, self.clock())
+        if req.device_bytes() > self.slots[0].capacity:
+            t.error = MemoryError(f"tile needs {req.device_bytes()} B, above a slot's "
+                                  f"{self.slots[0].capacity} B share of the HBM budget")
+            t.t_done = t.t_submit
+            self.completed.append(t)
+            return t
+        self.queue.append(t)
+        return t
+
+    # ── scheduler ──
+    def step(self) -> int:
+        """One scheduler pass; returns the number of requests that completed."""
+        n_done = 0
+        for s in self.slots:
+            if s.batch is not None and s.batch.done():
+                n_done += self._collect(s)
+        for s in self.slots:
+            if s.batch is None and self.queue:
+                self._admit(s)
+        return n_done
+
+    def _collect(self, s: _Slot) -> int:
+        now = None
+        try:
+            results = s.batch.finish()
+            now = self.clock()
+            for t, r in zip(s.tickets, results):
+                t.result = r
+                t.t_done = now
+        except Exception as e:  # the whole batch failed: report it on every ticket
+            now = self.clock()
+            for t in s.tickets:
+                t.error = e
+                t.t_done = now
+        self.completed.extend(s.tickets)
+        n = len(s.tickets)
+        s.batch, s.tickets, s.bytes = None, [], 0
+        return n
+
+    def _admit(self, s: _Slot) -> None:
+        take: List[Ticket] = []
+        used = 0
+        while self.queue and len(take) < self.max_batch:
+            need = self.queue[0].request.device_bytes()
+            if used + need > s.capacity:
+                break
+            used += need
+            take.append(self.queue.popleft())
+        if not take:
+            return
+        now = self.clock()
+        for t in take:
+            t.t_launch = now
+        s.tickets, s.bytes = take, used
+        s.batch = s.launch([t.request for t in take])
+
+    def busy(self) -> bool:
+        return bool(self.queue) or any(s.batch is not None for s in self.slots)
+
+    def drain(self) -> None:
+        while self.busy():
+            self.step()
+
+    def close(self) -> None:
+        self.drain()
+        for s in self.slots:
+            s.close()
+
+
+def latency_summary(tickets: List[Ticket]) -> dict:
+    import numpy as np
+    ok = [t for t in tickets if t.error is None and t.done]
+    if not ok:
+        return {"completed": 0}
+    lat = np.array([t.latency_s for t in ok]) * 1e3
+    px = sum(t.request.rows * t.request.cols for t in ok)
+    t0 = min(t.t_submit for t in ok)
+    t1 = max(t.t_done for t in ok)
+    return {"completed": len(ok), "failed": len(tickets) - len(ok), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "px": int(px), "span_s": t1 - t0, "px_per_s": px / max(t1 - t0, 1e-9)}
