@@ -399,6 +399,372 @@ def cpu_baseline(args, sc, res_gpu, merged_px, threads=None, budget_s=12.0):
     return out
 
 
+# ── config 4: batched multi-scene tiles ─────────────────────────────────────
+def _c4_setup(sd, ctx, dev, rank, n_scenes=8, n_tiles=64, precision=None):
+    import copy
+    import torch
+    from sardine_b200 import synth, tiles
+    precision = sd.Precision.SPLIT if precision is None else precision
+    scenes = []
+    for k in range(n_scenes):
+        sc, slc, cal, noise = synth.config4_scene(100 + k + 1000 * rank, device=dev)
+        L, S = slc.shape[0], slc.shape[1]
+        deb = sd.DeburstArray(slc, L, S, 0)
+        sig = torch.empty((L, S), dtype=torch.float32, device=dev)
+        nesz = torch.empty((L, S), dtype=torch.float32, device=dev)
+        sd.apply_calibration(deb, cal, noise, 0, ctx=ctx, out=(sig, nesz))
+        m = sc.merged
+        merged = sd.MergedSigma0(sig, L, S, m.near_slant_range_time_s, m.range_pixel_spacing_s,
+                                 m.range_pixel_spacing_m, 0, 0, nesz, m.azimuth_start_time_us)
+        rs = tiles.ResidentScene(merged, sc.scene, sc.dem, sc.grids, sc.config.geoid, ctx)
+        cfg = copy.copy(sc.config)
+        cfg.pixel_spacing_deg = sc.config.pixel_spacing_deg / 4.0   # output spacing = posting / 4
+        info = sd.tc_output_grid(sc.scene, cfg, ctx=ctx)
+        scenes.append(dict(sc=sc, deb=deb, cal=cal, noise=noise, sig=sig, nesz=nesz, rs=rs, cfg=cfg,
+                           info=info))
+    rng = np.random.default_rng(4 + rank)
+    specs = synth.random_tiles(rng, [(int(s["info"].rows), int(s["info"].cols)) for s in scenes],
+                               n_tiles, 256, 4096)
+    reqs = []
+    for t in specs:
+        s = scenes[t["scene"]]
+        cfg = copy.copy(s["cfg"])
+        cfg.resampling = t["kernel"]
+        cfg.precision = precision
+        sp = cfg.pixel_spacing_deg
+        reqs.append(tiles.TileRequest(s["rs"], cfg, s["info"].origin_lon_deg + t["c0"] * sp,
+                                      s["info"].origin_lat_deg - t["r0"] * sp, t["rows"], t["cols"],
+                                      t["speckle"]))
+    return scenes, reqs
+
+
+def run_c4(args):
+    import torch
+    import sardine_b200 as sd
+    from sardine_b200 import autotune, tiles
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = _init_dist(world)
+    ctx = sd.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
+    dev = f"cuda:{local}"
+    scenes, reqs = _c4_setup(sd, ctx, dev, rank)
+    outputs = [tiles._alloc_outputs(r, dev) for r in reqs]
+    tune = autotune.tune(ctx, reqs)
+    tiles.set_graphs(ctx, True)
+    px_step = sum(r.rows * r.cols for r in reqs)
+
+    def step():
+        for s in scenes:  # calibrate every scene's SLC into its resident sigma0
+            sd.apply_calibration(s["deb"], s["cal"], s["noise"], 0, ctx=ctx, out=(s["sig"], s["nesz"]))
+        return tiles.TileBatch(ctx, reqs, outputs).launch().finish()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        res = step()
+    barrier()
+    l0 = ctx.launches
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        barrier()
+        evs[0].record(stream)
+        for i in range(args.steps):
+            res = step()
+            evs[i + 1].record(stream)
+        barrier()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    ms = sum(step_ms)
+    gpu_launches = ctx.launches - l0
+    ms = _max_over_ranks(dist, ms)
+    value = world * px_step * args.steps / (ms / 1e3)
+    ctx.set_timing(True)
+    step()
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    total_k = sum(v[0] for v in kt.values()) or 1.0
+    hist = np.sum([r.newton_iter_histogram for r in res], axis=0)
+    n_it = n_iter_mean(hist)
+    tc_ms = sum(v[0] for k, v in kt.items() if k.startswith(("k_main", "k_scan", "k_select", "k_row")))
+    fp64 = ctypes_fp64_peak(ctx)
+    tc_tf = TC_FLOPS(n_it) * px_step / (tc_ms / 1e3) / 1e12 if tc_ms else None
+    sp_ms = kt.get("k_speckle_tiles", (0.0, 0))[0]
+    hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    sp_gbs = 9.0 * px_step / (sp_ms / 1e3) / 1e9 if sp_ms else None
+    roofline = {"bound": "fp64", "kernel": "tile geocoding (k_main_batch+k_scan+k_select+k_row*)",
+                "achieved": tc_tf, "peak": fp64, "unit": "TFLOP/s",
+                "frac": tc_tf / fp64 if (tc_tf and fp64) else None, "traffic": None,
+                "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
+                "speckle_stage": {"kernel": "k_speckle_tiles", "bound": "hbm", "achieved": sp_gbs,
+                                  "peak": hbm, "unit": "GB/s", "frac": sp_gbs / hbm if sp_gbs else None,
+                                  "bytes_per_px": 9.0, "ms": sp_ms}}
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_k, 4)}
+               for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
+    if rank == 0:
+        sizes = [r.rows for r in reqs]
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (split)",
+            "data": "synthetic (seeded config-1-shape scenes, CInt16 SLC + LUTs)",
+            "config": {"workload": ("config4: 8 scenes (4096x8192 CInt16, distinct orbits) calibrated on "
+                                    "the device each step, 64 tiles 256^2-4096^2 log-uniform at posting/4, "
+                                    "mixed bilinear/bicubic/lanczos3, split precision, Refined Lee 7x7 or "
+                                    "Gamma-MAP 5x5 (ENL 4.4) after a halo, one persistent launch per stage "
+                                    "replayed from a CUDA graph"),
+                       "tiles": len(reqs), "tile_px": px_step, "tile_side_min": min(sizes),
+                       "tile_side_max": max(sizes), "autotune": tune,
+                       "l2": "inputs larger than L2 (SLC 8 x 128 MB, sigma0 8 x 128 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99)),
+                           "what": "batch latency (all 64 tiles complete together)"},
+            "roofline": roofline, "kernels": kernels, "gpu_launches": gpu_launches, "clocks": clk.summary(),
+            "e2e": None,
+        }
+        if args.cpu_baseline and world == 1:
+            out["cpu_baseline"] = _tiles_cpu_baseline(scenes, reqs)
+        print(json.dumps(out), flush=True)
+    _finish_dist(dist)
+    ctx.close()
+
+
+def _tiles_cpu_baseline(scenes, reqs, budget_s=12.0):
+    """The oracle (C++ restatement) on the host cores: geocode + speckle of
+    the smallest tiles of the batch until ~budget_s of work."""
+    import oracle
+    import sardine_b200 as sd
+    threads = os.cpu_count()
+    oracle.set_threads(threads)
+    by_req = sorted(range(len(reqs)), key=lambda i: reqs[i].rows * reqs[i].cols)
+    host = {}
+    px, t = 0, 0.0
+    done = 0
+    for i in by_req:
+        r = reqs[i]
+        s = next(x for x in scenes if x["rs"] is r.scene)
+        key = id(s)
+        if key not in host:
+            m, sc = s["sc"].merged, s["sc"]
+            merged = sd.MergedSigma0(s["sig"].cpu().numpy(), m.lines, m.samples, m.near_slant_range_time_s,
+                                     m.range_pixel_spacing_s, m.range_pixel_spacing_m, 0, 0,
+                                     s["nesz"].cpu().numpy(), m.azimuth_start_time_us)
+            dem = sd.DemGrid(sc.dem.data.cpu().numpy() if hasattr(sc.dem.data, "cpu") else sc.dem.data,
+                             sc.dem.origin_y, sc.dem.origin_x, sc.dem.pixel_size, sc.dem.kind,
+                             sc.dem.utm_zone, sc.dem.utm_south)
+            host[key] = (merged, dem, sc)
+        merged, dem, sc = host[key]
+        h = r.halo()
+        spd = r.config.pixel_spacing_deg
+        t0 = time.perf_counter()
+        g = oracle.terrain_correction_grid(merged, sc.scene, dem, sc.grids, r.config, r.origin_x - h * spd,
+                                           r.origin_y + h * spd, r.rows + 2 * h, r.cols + 2 * h)
+        if r.speckle is not None:
+            oracle.apply_speckle_filter(g.data, r.cols + 2 * h, r.rows + 2 * h, r.speckle)
+        t += time.perf_counter() - t0
+        px += r.rows * r.cols
+        done += 1
+        if t > budget_s:
+            break
+    return {"value": px / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle geocode+speckle of the {done} smallest of {len(reqs)} tiles ({px} px, {t:.1f} s)"}
+
+
+# ── config 5: served geocoding ──────────────────────────────────────────────
+def _c5_setup(sd, ctx, dev, rank, n_scenes):
+    import torch
+    from sardine_b200 import synth, tiles
+    scenes = []
+    for k in range(n_scenes):
+        sc = synth.config2_scene(seed=200 + k + 1000 * rank, device=dev)
+        m = sd.calibrate_deburst_merge(sc.swaths, ctx=ctx)
+        sc.swaths = None  # the SLC leaves HBM; the merged sigma0 + NESZ stay resident
+        rs = tiles.ResidentScene(m, sc.scene, sc.dem, sc.grids, sc.config.geoid, ctx)
+        info = sd.tc_output_grid(sc.scene, sc.config, ctx=ctx)
+        scenes.append(dict(sc=sc, merged=m, rs=rs, cfg=sc.config, info=info))
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return scenes
+
+
+def _c5_requests(sd, scenes, rng, n, precision):
+    import copy
+    from sardine_b200 import synth, tiles
+    specs = synth.random_tiles(rng, [(int(s["info"].rows), int(s["info"].cols)) for s in scenes], n, 256, 2048,
+                               speckles=(None, "refined_lee", "gamma_map"))
+    reqs = []
+    for t in specs:
+        s = scenes[t["scene"]]
+        cfg = copy.copy(s["cfg"])
+        cfg.resampling = t["kernel"]
+        cfg.precision = precision
+        sp = cfg.pixel_spacing_deg
+        reqs.append(tiles.TileRequest(s["rs"], cfg, s["info"].origin_lon_deg + t["c0"] * sp,
+                                      s["info"].origin_lat_deg - t["r0"] * sp, t["rows"], t["cols"],
+                                      t["speckle"]))
+    return reqs
+
+
+def _serve(server, reqs, arrivals, clock=time.perf_counter):
+    """Feeds requests at their arrival offsets (s) and runs the loop dry."""
+    t0 = clock()
+    tickets = []
+    i = 0
+    while i < len(reqs) or server.busy():
+        now = clock() - t0
+        while i < len(reqs) and arrivals[i] <= now:
+            tickets.append(server.submit(reqs[i]))
+            i += 1
+        server.step()
+    return tickets
+
+
+def run_c5(args):
+    import torch
+    import sardine_b200 as sd
+    from sardine_b200 import autotune, tiles
+    from sardine_b200.serve import GeocodingServer, latency_summary
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = _init_dist(world)
+    ctx = sd.Context(local)
+    dev = f"cuda:{local}"
+    scenes = _c5_setup(sd, ctx, dev, rank, args.scenes)
+    rng = np.random.default_rng(5 + rank)
+    burst = args.burst
+    rate = args.rate
+    budget = args.budget_gb << 30
+    server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=64, graphs=True)
+    sample = _c5_requests(sd, scenes, rng, 64, sd.Precision.SPLIT)
+    for s in server.slots:
+        autotune.tune(s.ctx, sample[:32])
+    # warm-up bursts (graph capture, allocator), then the timed stream
+    for _ in range(args.warmup):
+        reqs = _c5_requests(sd, scenes, rng, burst // 4, sd.Precision.SPLIT)
+        _serve(server, reqs, np.cumsum(rng.exponential(1.0 / rate, len(reqs))))
+    n = burst * args.steps
+    reqs = _c5_requests(sd, scenes, rng, n, sd.Precision.SPLIT)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    l0 = sum(s.ctx.launches for s in server.slots)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record()
+        tickets = _serve(server, reqs, arrivals)
+        torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = _max_over_ranks(dist, e0.elapsed_time(e1))
+    summ = latency_summary(tickets)
+    gpu_launches = sum(s.ctx.launches for s in server.slots) - l0
+    value = world * summ["px"] / (ms / 1e3)
+    # plain per-request FP64 path on the same GPU: one tile per launch, no graphs
+    base = GeocodingServer(local, hbm_budget=4 << 30, slots=1, max_batch=1, graphs=False)
+    nb = max(64, n // 2)
+    breqs = _c5_requests(sd, scenes, np.random.default_rng(55 + rank), nb, sd.Precision.FP64)
+    barr = np.cumsum(np.random.default_rng(56).exponential(1.0 / rate, nb))
+    _serve(base, breqs[:8], barr[:8])
+    bsum = latency_summary(_serve(base, breqs, barr))
+    # split accuracy: the same tiles through the FP64 path
+    acc = _split_vs_fp64(sd, tiles, server.slots[0].ctx, scenes, rng)
+    base.close()
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (split)",
+            "data": "synthetic (seeded config-2-shape IW scenes resident in HBM)",
+            "config": {"workload": (f"config5: {args.scenes} config-2-shape scenes resident (merged sigma0+NESZ, "
+                                    f"DEM, orbit table); Poisson tile requests at {rate} req/s, sides "
+                                    "256-2048 log-uniform, random scene/bbox/resampler/speckle, split precision, "
+                                    "continuous batching over 2 slots, HBM-budget admission"),
+                       "requests": n, "burst_per_step": burst, "rate_req_s": rate,
+                       "hbm_budget_gb": args.budget_gb,
+                       "scene_device_gb": round(sum(s["rs"].device_bytes for s in scenes) / 2**30, 2),
+                       "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": summ["p50_ms"], "p99": summ["p99_ms"], "mean": summ["mean_ms"],
+                           "what": "request submit -> results on the device"},
+            "served": summ,
+            "per_request_fp64": bsum,
+            "accuracy_split_vs_fp64": acc,
+            "gpu_launches": gpu_launches, "clocks": clk.summary(), "e2e": None,
+        }
+        print(json.dumps(out), flush=True)
+    server.close()
+    _finish_dist(dist)
+
+
+def _split_vs_fp64(sd, tiles, ctx, scenes, rng, n=8):
+    """Split-precision tiles against the same tiles through the FP64 path:
+    geocoded values (before any speckle filter: the filters' regime and
+    direction choices amplify 1e-7 input differences into flips, counted
+    separately), mask, Newton histogram."""
+    import copy
+    from sardine_b200.accuracy import compare_geocoded
+    reqs = _c5_requests(sd, scenes, rng, n, sd.Precision.SPLIT)
+    filtered = [r for r in reqs if r.speckle is not None]
+    r64, raw = [], []
+    for r in reqs:
+        q = copy.copy(r)
+        q.speckle = None
+        raw.append(q)
+        q64 = copy.copy(q)
+        q64.config = copy.copy(r.config)
+        q64.config.precision = sd.Precision.FP64
+        r64.append(q64)
+    a = tiles.tc_tiles(raw, ctx)
+    b = tiles.tc_tiles(r64, ctx)
+    worst = {}
+    if filtered:
+        f64 = []
+        for r in filtered:
+            q = copy.copy(r)
+            q.config = copy.copy(r.config)
+            q.config.precision = sd.Precision.FP64
+            f64.append(q)
+        fa, fb = tiles.tc_tiles(filtered, ctx), tiles.tc_tiles(f64, ctx)
+        flips = sum(compare_geocoded(x, y)["sigma_rel_over_1e-4_px"] for x, y in zip(fa, fb))
+        worst["speckled_px_over_1e-4"] = int(flips)
+        worst["speckled_px"] = int(sum(r.rows * r.cols for r in filtered))
+    for x, y in zip(a, b):
+        rep = compare_geocoded(x, y)
+        for k, v in rep.items():
+            if isinstance(v, bool):
+                worst[k] = worst.get(k, True) and v
+            elif isinstance(v, (int, float)):
+                worst[k] = max(worst.get(k, 0), v)
+        worst["hist_equal"] = worst.get("hist_equal", True) and x.newton_iter_histogram == y.newton_iter_histogram
+    worst["tiles"] = n
+    worst["what"] = "geocoded sigma0/gamma0 before speckle; times equal by construction (histogram, mask)"
+    return worst
+
+
+def _init_dist(world):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def _max_over_ranks(dist, ms):
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _finish_dist(dist):
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_reference(args):
     """Reference arm: the reference is Rust and cannot be built here, so the
     oracle port (its C++ restatement) is timed on the host cores, each step a
@@ -479,7 +845,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c4", "c5"])
+    ap.add_argument("--rate", type=float, default=2000.0, help="config5 request rate (req/s)")
+    ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
+    ap.add_argument("--scenes", type=int, default=8, help="config5 resident scenes")
+    ap.add_argument("--budget-gb", dest="budget_gb", type=int, default=16, help="config5 HBM budget")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--ref-rows", type=int, default=16)
@@ -488,6 +858,10 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "c4":
+        run_c4(args)
+    elif args.config == "c5":
+        run_c5(args)
     else:
         run_ours(args)
 

@@ -392,6 +392,19 @@ int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image,
                           uint64_t n_grid, const sd_tc_config *cfg,
                           float *out_data, float *out_cos_lia, uint8_t *out_mask,
                           sd_geocoded_info *info);
+/* Rows [row_begin, row_end) of sd_terrain_correction's output grid
+ * (row_end 0 = to the last row): the outputs hold (row_end - row_begin) x
+ * cols pixels, the counters cover the band, and the band's values equal
+ * those rows of the whole-grid call (each output row's solve chain starts
+ * from its own LUT seed, terrain_correction.rs:1443).  This is how one
+ * scene shards over GPUs by output rows without any exchange. */
+int sd_terrain_correction_rows(sd_ctx *ctx, const sd_radar_image *image,
+                               const sd_scene *scene, const sd_dem *dem,
+                               const sd_geoid *geoid, const sd_geo_grid_point *grid,
+                               uint64_t n_grid, const sd_tc_config *cfg,
+                               uint64_t row_begin, uint64_t row_end,
+                               float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                               sd_geocoded_info *info);
 /* sd_terrain_correction plus the converged zero-Doppler azimuth time of
  * every output pixel in integer microseconds (INT64_MIN where the solve did
  * not converge, the DEM has no height or the orbit refused the time), for
@@ -462,6 +475,12 @@ int sd_ctx_set_graphs(sd_ctx *ctx, int enable);
  * `tile_arena_bytes` plus the work tables of a 1024-tile batch, so batches
  * that fit it run without device allocations. */
 int sd_ctx_reserve(sd_ctx *ctx, uint64_t tile_arena_bytes);
+/* Launch shapes of the tile stages: the speckle/crop block (tx x ty
+ * threads, tx >= 8, tx*ty <= 1024 and a multiple of 32; default 32 x 8) and
+ * the CTAs per SM of the persistent geocoding kernel (0 = as many as fit).
+ * Results do not depend on them; sardine_b200.autotune picks them. */
+int sd_ctx_set_tile_shape(sd_ctx *ctx, int32_t speckle_tx, int32_t speckle_ty,
+                          int32_t main_ctas_per_sm);
 
 /* ── Diagnostics ──────────────────────────────────────────────────────────
  * Runs an FP64 FMA-chain kernel for about `iters` dependent FMAs per thread

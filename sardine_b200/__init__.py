@@ -166,14 +166,16 @@ def tc_output_grid(scene: SceneMetadata, config: TerrainCorrectionConfig,
 
 def terrain_correction(merged: MergedSigma0, scene: SceneMetadata, dem: DemGrid, grids,
                        config: TerrainCorrectionConfig, ctx: Optional[Context] = None,
-                       out=None, return_times: bool = False) -> GeocodedImage:
+                       out=None, return_times: bool = False, row_range=None) -> GeocodedImage:
     """terrain_correction (terrain_correction.rs:1245-1836) on the GPU.
 
     `grids` is a sequence of (sub-swath id, geolocation points); the LUT uses
     IW2's points, else the first sub-swath's.  `out` may supply preallocated
     (data, cos_lia, mask) buffers of the output-grid shape.  With
     `return_times`, the result also carries the converged zero-Doppler time of
-    every pixel (`azimuth_time_us`, int64 microseconds, INT64_MIN where none)."""
+    every pixel (`azimuth_time_us`, int64 microseconds, INT64_MIN where none).
+    `row_range=(r0, r1)` geocodes only those output rows (a row band: equal to
+    the same rows of the whole grid; how one scene shards over GPUs)."""
     ctx = _ctx(ctx)
     keep = T._Keep()
     merged_data = _prep(merged.data, np.float32)
@@ -195,6 +197,9 @@ def terrain_correction(merged: MergedSigma0, scene: SceneMetadata, dem: DemGrid,
         _check(ctx, lib().sd_tc_output_grid(ctx.handle, C.byref(sc), C.byref(cfg), C.byref(info)),
                TerrainCorrectionError)
     rows, cols = int(info.rows), int(info.cols)
+    if row_range is not None:
+        r0, r1 = int(row_range[0]), int(row_range[1] or rows)
+        rows = max(0, min(r1, rows) - r0)
     if out is not None:
         data, cos, mask = out
     else:
@@ -202,7 +207,13 @@ def terrain_correction(merged: MergedSigma0, scene: SceneMetadata, dem: DemGrid,
         cos = _empty_like_kind(merged_data, (rows, cols), "f4") if config.compute_lia else None
         mask = _empty_like_kind(merged_data, (rows, cols), "u1") if config.compute_lia else None
     times = _empty_like_kind(merged_data, (rows, cols), "i8") if return_times else None
-    if return_times:
+    if row_range is not None:
+        if return_times:
+            raise ValueError("row_range and return_times are exclusive")
+        rc = lib().sd_terrain_correction_rows(ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo),
+                                              g, len(pts), C.byref(cfg), r0, r1, T.ptr(data), T.ptr(cos),
+                                              T.ptr(mask), C.byref(info))
+    elif return_times:
         rc = lib().sd_terrain_correction_with_times(
             ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo), g, len(pts), C.byref(cfg),
             T.ptr(data), T.ptr(cos), T.ptr(mask), T.ptr(times), C.byref(info))
@@ -247,16 +258,20 @@ def deburst_subswath(slc_iq, sw: SubSwathMetadata, bursts: Sequence[BurstEntry],
 
 
 def apply_calibration(deburst: DeburstArray, cal: SwathCalibration, noise: SwathNoise,
-                      tiff_line_origin: int, ctx: Optional[Context] = None) -> Sigma0Array:
-    """apply_calibration (apply_calibration.rs:374-572)."""
+                      tiff_line_origin: int, ctx: Optional[Context] = None, out=None) -> Sigma0Array:
+    """apply_calibration (apply_calibration.rs:374-572).  `out` may supply
+    preallocated (sigma0, nesz) buffers of shape (lines, samples)."""
     ctx = _ctx(ctx)
     keep = T._Keep()
     cv = T.lut_vectors_to_c(cal.vectors, keep, "sigma_nought")
     nv = T.lut_vectors_to_c(noise.range_vectors, keep, "noise_range_lut")
     na = T.noise_azimuth_to_c(noise, keep)
     iq = _prep(deburst.data, np.int16)
-    out = _empty_like_kind(iq, (deburst.lines, deburst.samples), "f4")
-    nesz = _empty_like_kind(iq, (deburst.lines, deburst.samples), "f4")
+    if out is not None:
+        out, nesz = out
+    else:
+        out = _empty_like_kind(iq, (deburst.lines, deburst.samples), "f4")
+        nesz = _empty_like_kind(iq, (deburst.lines, deburst.samples), "f4")
     cg, ng = C.c_uint32(), C.c_uint32()
     rc = lib().sd_apply_calibration(ctx.handle, T.ptr(iq), deburst.lines, deburst.samples,
                                     deburst.valid_sample_offset, cv, len(cal.vectors), nv,

@@ -42,6 +42,9 @@ struct sd_ctx {
   uint64_t tile_cap = 0, tile_n = 0;
   std::vector<sd_geocoded_info> tile_info;
   bool tiles_pending = false;
+  // launch shapes of the tile stages (set by the tile autotuner)
+  int sp_tx = 32, sp_ty = 8;  // speckle/crop block
+  int main_cps = 0;           // k_main_batch CTAs per SM (0: as many as fit)
   // CUDA graphs of the tile stages (persistent kernels over fixed work tables)
   bool graphs = false;
   struct GraphRec {

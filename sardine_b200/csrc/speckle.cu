@@ -194,13 +194,16 @@ __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
 }
 
 // ── batched form: many tiles, each a halo'd geocoded raster ──────────────────
-// Item = one TX x TY block of one tile's output.  The block stages its
-// window from the tile's halo'd raster (cells outside it are NaN, which the
-// filters skip like out-of-image cells), filters the data plane with the
-// tile's kind (or copies it when kind < 0) and crops cos(LIA) and the mask.
-__global__ void __launch_bounds__(TX *TY) k_speckle_tiles(const SpWork *__restrict__ wp) {
-  __shared__ float tile[(TX + 2 * SP_MAX_HALF) * (TY + 2 * SP_MAX_HALF)];
+// Item = one tx x ty block (the launch's block shape, chosen by the tile
+// autotuner) of one tile's output.  The block stages its window from the
+// tile's halo'd raster (cells outside it are NaN, which the filters skip like
+// out-of-image cells), filters the data plane with the tile's kind (or
+// copies it when kind < 0) and crops cos(LIA) and the mask.
+__global__ void __launch_bounds__(1024) k_speckle_tiles(const SpWork *__restrict__ wp) {
+  extern __shared__ float tile[];
   const SpWork w = *wp;
+  const int bx = (int)blockDim.x, by = (int)blockDim.y, nt = bx * by;
+  const int tid = threadIdx.y * bx + threadIdx.x;
   const uint64_t total = w.pre[w.n_jobs];
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
     int lo = 0, hi = w.n_jobs;
@@ -211,15 +214,15 @@ __global__ void __launch_bounds__(TX *TY) k_speckle_tiles(const SpWork *__restri
     }
     const SpJob &jb = w.jobs[lo];
     const uint64_t li = item - w.pre[lo];
-    const int64_t bx = (int64_t)(jb.cols + TX - 1) / TX;
-    const int64_t tr = (int64_t)li / bx, tc = (int64_t)li % bx;
+    const int64_t nbx = (jb.cols + bx - 1) / bx;
+    const int64_t tr = (int64_t)li / nbx, tc = (int64_t)li % nbx;
     const int h = jb.kind >= 0 ? jb.half : 0;
-    const int tw = TX + 2 * h, th = TY + 2 * h;
+    const int tw = bx + 2 * h, th = by + 2 * h;
     const int64_t in_cols = jb.cols + 2 * jb.halo, in_rows = jb.rows + 2 * jb.halo;
     // output (r, c) is input (r + halo, c + halo)
-    const int64_t c0 = tc * TX + jb.halo - h, r0 = tr * TY + jb.halo - h;
+    const int64_t c0 = tc * bx + jb.halo - h, r0 = tr * by + jb.halo - h;
     __syncthreads();
-    for (int k = threadIdx.y * TX + threadIdx.x; k < tw * th; k += TX * TY) {
+    for (int k = tid; k < tw * th; k += nt) {
       const int ty = k / tw, tx = k % tw;
       const int64_t rr = r0 + ty, cc = c0 + tx;
       float v = NAN;
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(TX *TY) k_speckle_tiles(const SpWork *__restri
       tile[k] = v;
     }
     __syncthreads();
-    const int64_t c = tc * TX + threadIdx.x, r = tr * TY + threadIdx.y;
+    const int64_t c = tc * bx + threadIdx.x, r = tr * by + threadIdx.y;
     if (c < jb.cols && r < jb.rows) {
       const SpCoef cf{jb.enl, jb.damping, jb.cv_n_sq, jb.cv_max_sq};
       const int lx = threadIdx.x + h, ly = threadIdx.y + h;
@@ -271,17 +274,22 @@ void speckle_coefs(int kind, uint64_t window, float enl, float damping, SpJob *j
   j->cv_max_sq = j->cv_n_sq < 1.0f ? 2.0f * j->cv_n_sq / (1.0f - j->cv_n_sq) : INFINITY;
 }
 
-int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool full_grid) {
+bool speckle_shape_ok(int tx, int ty) {
+  return tx >= 8 && ty >= 1 && tx <= 256 && tx * ty <= 1024 && (tx * ty) % 32 == 0;
+}
+
+int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool full_grid, int tx, int ty) {
   SD_TRY(speckle_masks(ctx));
-  const unsigned g = persistent_grid(k_speckle_tiles, TX * TY, 0, full_grid ? ~0ull : total);
+  const size_t smem = (size_t)(tx + 2 * SP_MAX_HALF) * (ty + 2 * SP_MAX_HALF) * sizeof(float);
+  const unsigned g = persistent_grid(k_speckle_tiles, tx * ty, smem, full_grid ? ~0ull : total);
   SD_TIMED_BEGIN(ctx, "k_speckle_tiles");
-  k_speckle_tiles<<<g, dim3(TX, TY), 0, ctx->stream>>>(d_work);
+  k_speckle_tiles<<<g, dim3(tx, ty), smem, ctx->stream>>>(d_work);
   SD_LAUNCHED(ctx);
   return SD_OK;
 }
 
-uint64_t speckle_tile_items(const SpJob &j) {
-  return (uint64_t)((j.cols + TX - 1) / TX) * (uint64_t)((j.rows + TY - 1) / TY);
+uint64_t speckle_tile_items(const SpJob &j, int tx, int ty) {
+  return (uint64_t)((j.cols + tx - 1) / tx) * (uint64_t)((j.rows + ty - 1) / ty);
 }
 
 // Validation in the reference's order (speckle.rs:137-178).

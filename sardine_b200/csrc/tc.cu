@@ -89,8 +89,8 @@ int launch_pixels_single(sd_ctx *ctx, const TcWork *d_work, const uint64_t *tota
 
 static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene, const sd_dem *dem,
                   const sd_geoid *geoid, const sd_geo_grid_point *grid, uint64_t n_grid,
-                  const sd_tc_config *cfg, float *out_data, float *out_cos_lia, uint8_t *out_mask,
-                  int64_t *out_times, sd_geocoded_info *info) {
+                  const sd_tc_config *cfg, uint64_t row_begin, uint64_t row_end, float *out_data,
+                  float *out_cos_lia, uint8_t *out_mask, int64_t *out_times, sd_geocoded_info *info) {
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!image || !scene || !dem || !geoid || !cfg || !info || !out_data)
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null argument");
@@ -128,7 +128,12 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "radar image is empty");
 
   TcDev p{};
-  p.rows = info->rows;
+  if (row_end == 0 || row_end > info->rows) row_end = info->rows;
+  if (row_begin >= row_end)
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "empty row band [%llu, %llu)",
+                     (unsigned long long)row_begin, (unsigned long long)row_end);
+  p.rows = row_end - row_begin;
+  p.row0 = row_begin;
   p.cols = info->cols;
   p.lat_north = info->origin_lat_deg;
   p.lon_west = info->origin_lon_deg;
@@ -313,8 +318,8 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
                                      const sd_geo_grid_point *grid, uint64_t n_grid,
                                      const sd_tc_config *cfg, float *out_data, float *out_cos_lia,
                                      uint8_t *out_mask, sd_geocoded_info *info) {
-  return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, out_data, out_cos_lia, out_mask, nullptr,
-                info);
+  return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, 0, 0, out_data, out_cos_lia, out_mask,
+                nullptr, info);
 }
 
 extern "C" int sd_terrain_correction_with_times(sd_ctx *ctx, const sd_radar_image *image,
@@ -325,6 +330,16 @@ extern "C" int sd_terrain_correction_with_times(sd_ctx *ctx, const sd_radar_imag
                                                 int64_t *out_azimuth_time_us, sd_geocoded_info *info) {
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!out_azimuth_time_us) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null time buffer");
-  return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, out_data, out_cos_lia, out_mask,
+  return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, 0, 0, out_data, out_cos_lia, out_mask,
                 out_azimuth_time_us, info);
+}
+
+extern "C" int sd_terrain_correction_rows(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene,
+                                          const sd_dem *dem, const sd_geoid *geoid,
+                                          const sd_geo_grid_point *grid, uint64_t n_grid,
+                                          const sd_tc_config *cfg, uint64_t row_begin, uint64_t row_end,
+                                          float *out_data, float *out_cos_lia, uint8_t *out_mask,
+                                          sd_geocoded_info *info) {
+  return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, row_begin, row_end, out_data, out_cos_lia,
+                out_mask, nullptr, info);
 }

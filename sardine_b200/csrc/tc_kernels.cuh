@@ -143,6 +143,7 @@ struct TcDev {
   uint64_t bpr;                // k_main work items per row
   int fast;                    // tolerance allows the fixed-point-pair scheme
   int pad_;
+  uint64_t row0;               // grid row of the job's first row (row bands)
 };
 
 // ── work table ──────────────────────────────────────────────────────────────
@@ -185,7 +186,7 @@ __device__ __forceinline__ void load_job(unsigned char *dst, const TcDev *src, i
 }
 
 __device__ __forceinline__ double row_y(const TcDev &p, uint64_t r) {
-  return p.lat_north - ((double)r + 0.5) * p.sp;
+  return p.lat_north - ((double)(r + p.row0) + 0.5) * p.sp;
 }
 
 // Output pixel centre in lon/lat: direct for WGS84, project_row anchors for
@@ -1502,8 +1503,14 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
       return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "output grid too large");
     k_main<K, S><<<(unsigned)std::max<uint64_t>(totals[WK_MAIN], 1), MAIN_THREADS, 0, st>>>(*job);
   } else {
-    k_main_batch<K, S><<<persistent_grid(k_main_batch<K, S>, MAIN_THREADS, 0, totals[WK_MAIN]), MAIN_THREADS, 0,
-                         st>>>(d_work);
+    unsigned g = persistent_grid(k_main_batch<K, S>, MAIN_THREADS, 0, totals[WK_MAIN]);
+    if (ctx->main_cps > 0) {
+      int dev = 0, sms = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      g = std::min<unsigned>(g, (unsigned)(ctx->main_cps * sms));
+    }
+    k_main_batch<K, S><<<g, MAIN_THREADS, 0, st>>>(d_work);
   }
   SD_LAUNCHED(ctx);
   SD_TIMED_BEGIN(ctx, "k_scan");

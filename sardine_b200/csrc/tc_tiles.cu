@@ -475,7 +475,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     const bool split = g == 1;
     if (use_graph) {
       static const uint64_t kFull[kWk] = {~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull};
-      SD_TRY(run_graph(ctx, g, d_work, [&]() -> int {
+      SD_TRY(run_graph(ctx, g + 2 * ctx->main_cps, d_work, [&]() -> int {
         SD_TRY(launch_rows(ctx, d_work, kFull));
         return launch_pixels_batch(ctx, d_work, kFull, split);
       }));
@@ -493,8 +493,11 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     unsigned char *d_sw = nullptr;
     SD_TRY(scratch_t(ctx, "tiles.spwork", bytes, &d_sw));
     std::vector<unsigned char> h(o_pre + (m + 1) * 8);
+    const int tx = ctx->sp_tx, ty = ctx->sp_ty;
     SpWork w{};
     w.n_jobs = (int)m;
+    w.tx = tx;
+    w.ty = ty;
     w.jobs = (const SpJob *)(d_sw + o_jobs);
     w.pre = (const uint64_t *)(d_sw + o_pre);
     std::memcpy(h.data(), &w, sizeof w);
@@ -502,17 +505,17 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     uint64_t *pre = (uint64_t *)(h.data() + o_pre), acc = 0;
     for (size_t j = 0; j < m; ++j) {
       pre[j] = acc;
-      acc += speckle_tile_items(spj[j]);
+      acc += speckle_tile_items(spj[j], tx, ty);
     }
     pre[m] = acc;
     SD_CUDA(ctx, cudaMemcpyAsync(d_sw, h.data(), h.size(), cudaMemcpyHostToDevice, st));
     if (use_graph && m < 1024) {
       SD_TRY(speckle_masks(ctx));
-      SD_TRY(run_graph(ctx, 64, d_sw, [&]() -> int {
-        return speckle_tiles_launch(ctx, (const SpWork *)d_sw, acc, true);
+      SD_TRY(run_graph(ctx, 1 << 20 | tx << 10 | ty, d_sw, [&]() -> int {
+        return speckle_tiles_launch(ctx, (const SpWork *)d_sw, acc, true, tx, ty);
       }));
     } else {
-      SD_TRY(speckle_tiles_launch(ctx, (const SpWork *)d_sw, acc, false));
+      SD_TRY(speckle_tiles_launch(ctx, (const SpWork *)d_sw, acc, false, tx, ty));
     }
   }
   // ── results to the caller's host buffers, counters to pinned memory ──
@@ -608,5 +611,19 @@ extern "C" int sd_ctx_reserve(sd_ctx *ctx, uint64_t tile_arena_bytes) {
   SD_TRY(scratch(ctx, "tiles.counters", 1024 * 32 * 8, &p));
   SD_TRY(scratch(ctx, "tiles.flags", 1024 * 4 * 4, &p));
   SD_TRY(scratch(ctx, "tiles.ax", 1024 * 257 * 8, &p));
+  return SD_OK;
+}
+
+extern "C" int sd_ctx_set_tile_shape(sd_ctx *ctx, int32_t speckle_tx, int32_t speckle_ty,
+                                     int32_t main_ctas_per_sm) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!speckle_shape_ok(speckle_tx, speckle_ty))
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "speckle block %dx%d: need tx >= 8, tx*ty <= 1024, tx*ty %% 32 == 0",
+                     speckle_tx, speckle_ty);
+  if (main_ctas_per_sm < 0 || main_ctas_per_sm > 64)
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "main_ctas_per_sm must be 0..64");
+  ctx->sp_tx = speckle_tx;
+  ctx->sp_ty = speckle_ty;
+  ctx->main_cps = main_ctas_per_sm;
   return SD_OK;
 }

@@ -27,16 +27,18 @@ struct SpJob {
 
 struct SpWork {
   int n_jobs;
+  int tx, ty;  // block shape (= blockDim) the item prefix was computed for
   int pad;
   const SpJob *jobs;
-  const uint64_t *pre;  // n_jobs + 1: exclusive prefix of TX x TY blocks
+  const uint64_t *pre;  // n_jobs + 1: exclusive prefix of tx x ty blocks
 };
 
 int speckle_masks(sd_ctx *ctx);
 int speckle_validate(uint64_t len, uint64_t cols, uint64_t rows, int kind, uint64_t window, float enl,
                      float damping);
 void speckle_coefs(int kind, uint64_t window, float enl, float damping, SpJob *j);
-uint64_t speckle_tile_items(const SpJob &j);
-int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool full_grid);
+uint64_t speckle_tile_items(const SpJob &j, int tx, int ty);
+int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool full_grid, int tx, int ty);
+bool speckle_shape_ok(int tx, int ty);
 
 }  // namespace sd

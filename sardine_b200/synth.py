@@ -424,3 +424,42 @@ def _inv_guess(x, y, zone):
 
 def _inv_guess_lat(x, y, zone):
     return y / 111_320.0
+
+
+# ── batched tiles (config 4) and served requests (config 5) ────────────────
+def config4_scene(seed: int, n_lines: int = 4096, n_samples: int = 8192, dem_n: int = 1024,
+                  device: Optional[str] = None):
+    """A config-1-shape scene whose radar image starts as CInt16 SLC with
+    sigma0/noise LUTs (calibrated on the device every step): returns the
+    TcScene, the (lines, samples, 2) int16 raster and (cal, noise)."""
+    sc = config1_scene(seed=seed, n_lines=n_lines, n_samples=n_samples, dem_n=dem_n, flatten=True,
+                       device=device)
+    rng = np.random.default_rng(seed + 7919)
+    slc = slc_raster(rng, n_lines, n_samples, 60.0, device)
+    cal, noise = _luts(rng, "IW1", n_lines, n_samples, int(round(1.0 / ATI)))
+    return sc, slc, cal, noise
+
+
+def random_tiles(rng: np.random.Generator, grids, n: int, side_min: int, side_max: int,
+                 kernels=(0, 1, 2), speckles=("refined_lee", "gamma_map"), enl: float = 4.4):
+    """n tile specs over `grids` (per scene: (rows, cols)): side log-uniform
+    in [side_min, side_max] (clipped to the grid), uniform scene, origin,
+    resampling kernel and speckle filter.  Returns dicts of
+    scene, r0, c0, rows, cols, kernel, speckle."""
+    out = []
+    for _ in range(n):
+        k = int(rng.integers(0, len(grids)))
+        gr, gc = grids[k]
+        side = int(round(side_min * (side_max / side_min) ** rng.uniform()))
+        rows, cols = min(side, gr), min(side, gc)
+        r0 = int(rng.integers(0, gr - rows + 1))
+        c0 = int(rng.integers(0, gc - cols + 1))
+        sp = speckles[int(rng.integers(0, len(speckles)))] if speckles else None
+        filt = None
+        if sp == "refined_lee":
+            filt = T.SpeckleFilter.RefinedLee(enl)
+        elif sp == "gamma_map":
+            filt = T.SpeckleFilter.GammaMap(5, enl)
+        out.append({"scene": k, "r0": r0, "c0": c0, "rows": rows, "cols": cols,
+                    "kernel": int(kernels[int(rng.integers(0, len(kernels)))]), "speckle": filt})
+    return out

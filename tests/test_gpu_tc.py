@@ -155,3 +155,17 @@ def test_device_resident_inputs(ctx):
     assert gpu.data.is_cuda
     gpu.data, gpu.cos_lia, gpu.mask = gpu.data.cpu().numpy(), gpu.cos_lia.cpu().numpy(), gpu.mask.cpu().numpy()
     assert_tc_parity(gpu, ref)
+
+
+def test_row_bands_equal_whole_grid(ctx):
+    """Row bands (the multi-GPU decomposition of one scene) reproduce the
+    whole grid's rows exactly and their counters add up."""
+    sc = synth.config1_scene(seed=18, n_lines=512, n_samples=1024, dem_n=128, flatten=True)
+    whole = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    bands = [(0, 37), (37, 200), (200, 0)]
+    parts = [sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx, row_range=b)
+             for b in bands]
+    assert np.array_equal(np.concatenate([p.data for p in parts]), whole.data, equal_nan=True)
+    assert np.array_equal(np.concatenate([p.mask for p in parts]), whole.mask)
+    assert sum(p.valid_pixel_count for p in parts) == whole.valid_pixel_count
+    assert list(np.sum([p.newton_iter_histogram for p in parts], axis=0)) == whole.newton_iter_histogram
