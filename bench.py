@@ -108,16 +108,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(cfg: str, device: str, seed: int):
+# reduced IW shape for profiler captures (a few GB on the device, inputs
+# still larger than L2): 3 sub-swaths x 3 bursts x 1500 x 10000 -> 2000 x 12000
+SMALL_IW = dict(n_bursts=3, lines_per_burst=1500, tiff_width=10000, swath_overlap=1000,
+                out_rows=2000, out_cols=12000)
+
+
+def make_workload(cfg: str, device: str, seed: int, small: bool = False):
     from sardine_b200 import synth
     import sardine_b200 as sd
+    kw = SMALL_IW if small else {}
     if cfg == "c1":
         return synth.config1_scene(seed=seed, device=device)
     if cfg == "c3":
-        sc = synth.config2_scene(seed=seed, device=device, resampling=sd.ResamplingKernel.Lanczos3)
+        sc = synth.config2_scene(seed=seed, device=device, resampling=sd.ResamplingKernel.Lanczos3, **kw)
         sc.config.precision = sd.Precision.SPLIT
         return sc
-    return synth.config2_scene(seed=seed, device=device)
+    return synth.config2_scene(seed=seed, device=device, **kw)
 
 
 def n_iter_mean(hist):
@@ -137,7 +144,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     ctx = sd.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr, device=torch.device("cuda", local))
-    sc = make_workload(args.config, f"cuda:{local}", seed=2 + 1000 * rank)
+    sc = make_workload(args.config, f"cuda:{local}", seed=2 + 1000 * rank, small=args.small)
 
     if args.config == "c1":
         def step():
@@ -163,6 +170,9 @@ def run_ours(args):
         if args.config == "c3":
             workload = ("config3: config2 inputs, lanczos3, split precision (FP64 orbit/Newton/slant "
                         "range, FP32 resampling/facet/flattening), gamma0 flatten, LIA+mask")
+
+    if args.small:
+        workload = "REDUCED SHAPE (profiler capture, not a bench number): " + workload + f" {SMALL_IW}"
 
     def barrier():
         if dist is not None:
@@ -853,6 +863,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--ref-rows", type=int, default=16)
+    ap.add_argument("--small", action="store_true",
+                    help="reduced IW shape (profiler captures); not a bench number")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

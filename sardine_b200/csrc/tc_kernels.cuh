@@ -483,16 +483,15 @@ __device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, dou
   float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
   float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
   if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
-  const float top = fmaf(v01 - v00, ds, v00);
-  const float bot = fmaf(v11 - v10, ds, v10);
-  const float r = fmaf(bot - top, dl, top);
-  // the weights leave [0, 1] only where the clamped index extrapolates
-  // (line or sample in [-0.5, 0)); the magnitude sum is checked there
-  if (dl < 0.f || ds < 0.f) {
-    const float a = (fabsf(v00) * fabsf(1.f - ds) + fabsf(v01) * fabsf(ds)) * fabsf(1.f - dl) +
-                    (fabsf(v10) * fabsf(1.f - ds) + fabsf(v11) * fabsf(ds)) * fabsf(dl);
-    if (a > kCancel * fabsf(r)) *redo = true;
-  }
+  // explicit weights, as the reference forms them: with non-negative
+  // weights and samples every term is non-negative and the sum keeps its
+  // relative accuracy even near zero (the lerp form a + t(b - a) does not)
+  const float w00 = (1.f - dl) * (1.f - ds), w01 = (1.f - dl) * ds;
+  const float w10 = dl * (1.f - ds), w11 = dl * ds;
+  const float r = fmaf(v00, w00, fmaf(v01, w01, fmaf(v10, w10, v11 * w11)));
+  const float a = fmaf(fabsf(v00), fabsf(w00), fmaf(fabsf(v01), fabsf(w01),
+                       fmaf(fabsf(v10), fabsf(w10), fabsf(v11) * fabsf(w11))));
+  if (a > kCancel * fabsf(r)) *redo = true;
   return r;
 }
 

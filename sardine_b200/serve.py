@@ -47,21 +47,47 @@ class Ticket:
         return self.t_done > 0.0
 
 
+def output_bytes(req: TileRequest) -> int:
+    """Device bytes of a tile's results (f32 data, f32 cos(LIA), u8 mask),
+    each plane 256 B aligned."""
+    n = req.rows * req.cols
+    al = lambda x: (x + 255) // 256 * 256
+    return al(4 * n) + (al(4 * n) + al(n) if req.config.compute_lia else 0)
+
+
 class _Slot:
-    def __init__(self, device: int, arena_bytes: int, graphs: bool):
+    """A context (stream) with its scratch arena reserved up front and a
+    result arena the batch's outputs are carved from."""
+
+    def __init__(self, device: int, arena_bytes: int, graphs: bool, out_bytes: int):
+        import torch
         self.ctx = Context(device)
         self.capacity = arena_bytes
+        self.out_capacity = out_bytes
         lib().sd_ctx_set_graphs(self.ctx.handle, int(graphs))
         if arena_bytes:
             rc = lib().sd_ctx_reserve(self.ctx.handle, C.c_uint64(arena_bytes))
             if rc != 0:
                 raise MemoryError(self.ctx.last_error())
+        self.out_arena = torch.empty(out_bytes, dtype=torch.uint8, device=f"cuda:{device}")
         self.batch: Optional[TileBatch] = None
         self.tickets: List[Ticket] = []
         self.bytes = 0
 
     def launch(self, requests):
-        return TileBatch(self.ctx, requests).launch()
+        import torch
+        outs, off = [], 0
+        for r in requests:
+            n = r.rows * r.cols
+            views = []
+            for k, (dt, esz) in enumerate(((torch.float32, 4), (torch.float32, 4), (torch.uint8, 1))):
+                if k > 0 and not r.config.compute_lia:
+                    views.append(None)
+                    continue
+                views.append(self.out_arena[off:off + esz * n].view(dt).view(r.rows, r.cols))
+                off += (esz * n + 255) // 256 * 256
+            outs.append(tuple(views))
+        return TileBatch(self.ctx, requests, outs).launch()
 
     def close(self):
         self.ctx.close()
@@ -77,20 +103,31 @@ class GeocodingServer:
 
     def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, slots: int = 2,
                  max_batch: int = 64, graphs: bool = True,
-                 clock: Callable[[], float] = time.perf_counter, slot_factory=None):
+                 clock: Callable[[], float] = time.perf_counter, slot_factory=None,
+                 on_done: Optional[Callable[[Ticket], None]] = None, keep_results: bool = False):
+        """hbm_budget covers each slot's scratch arena (4/5 of its share) and
+        result arena (1/5).  Results live in the slot's result arena until
+        that slot's next batch: `on_done(ticket)` runs as each request
+        completes (copy out what must outlive it); unless keep_results, the
+        completed ticket keeps only counters and timings."""
         if slots < 1:
             raise ValueError("slots must be >= 1")
         self.clock = clock
         self.max_batch = max_batch
-        make = slot_factory or (lambda cap: _Slot(device, cap, graphs))
-        self.slots = [make(hbm_budget // slots) for _ in range(slots)]
+        self.on_done = on_done
+        self.keep_results = keep_results
+        share = hbm_budget // slots
+        make = slot_factory or (lambda cap: _Slot(device, cap * 4 // 5, graphs, cap // 5))
+        self.slots = [make(share) for _ in range(slots)]
         self.queue: Deque[Ticket] = deque()
         self.completed: List[Ticket] = []
 
     # ── client side ──
     def submit(self, req: TileRequest) -> Ticket:
         t = Ticket(req, self.clock())
-        if req.device_bytes() > self.slots[0].capacity:
+        out_cap = getattr(self.slots[0], "out_capacity", None)
+        if req.device_bytes() > self.slots[0].capacity or \
+                (out_cap is not None and output_bytes(req) > out_cap):
             t.error = MemoryError(f"tile needs {req.device_bytes()} B, above a slot's "
                                   f"{self.slots[0].capacity} B share of the HBM budget")
             t.t_done = t.t_submit
@@ -119,6 +156,10 @@ class GeocodingServer:
             for t, r in zip(s.tickets, results):
                 t.result = r
                 t.t_done = now
+                if self.on_done is not None:
+                    self.on_done(t)
+                if not self.keep_results and hasattr(r, "data"):
+                    r.data = r.cos_lia = r.mask = None
         except Exception as e:  # the whole batch failed: report it on every ticket
             now = self.clock()
             for t in s.tickets:
@@ -131,12 +172,15 @@ class GeocodingServer:
 
     def _admit(self, s: _Slot) -> None:
         take: List[Ticket] = []
-        used = 0
+        used = used_out = 0
+        out_cap = getattr(s, "out_capacity", float("inf"))
         while self.queue and len(take) < self.max_batch:
             need = self.queue[0].request.device_bytes()
-            if used + need > s.capacity:
+            need_out = output_bytes(self.queue[0].request) if out_cap != float("inf") else 0
+            if used + need > s.capacity or used_out + need_out > out_cap:
                 break
             used += need
+            used_out += need_out
             take.append(self.queue.popleft())
         if not take:
             return

@@ -110,3 +110,22 @@ def test_bad_precision_mode(ctx):
     with pytest.raises(sd.TerrainCorrectionError) as e:
         sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
     assert e.value.kind == "Config"
+
+
+@pytest.mark.parametrize("resampling", [sd.ResamplingKernel.Bilinear, sd.ResamplingKernel.Bicubic,
+                                        sd.ResamplingKernel.Lanczos3])
+def test_split_zero_clipped_sigma0(ctx, resampling):
+    """Calibrated sigma0 is clipped at zero by the noise subtraction: values
+    interpolated between zeros and non-zeros must keep 1e-4 relative."""
+    sc = synth.config1_scene(seed=37, n_lines=1024, n_samples=2048, dem_n=256, resampling=resampling,
+                             flatten=True)
+    img = np.array(sc.merged.data)
+    rng = np.random.default_rng(9)
+    img[rng.uniform(size=img.shape) < 0.35] = 0.0
+    sc.merged.data = img
+    ref, ref_t, _ = oracle.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config,
+                                              return_times=True)
+    sc.config.precision = SPLIT
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx,
+                                return_times=True)
+    _check(gpu, ref, ref_t, sc.scene.sub_swaths[0].azimuth_time_interval_s)
