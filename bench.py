@@ -259,7 +259,16 @@ def run_ours(args):
         if accuracy is not None:
             out["accuracy_vs_fp64"] = accuracy
         if args.cpu_baseline and world == 1:
-            out["cpu_baseline"] = cpu_baseline(args, sc, res, merged_px)
+            def gpu_band(b0, b1):
+                m = sd.calibrate_deburst_merge(sc.swaths, ctx=ctx) if merged_px else sc.merged
+                g = sd.terrain_correction(m, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx,
+                                          row_range=(b0, b1), return_times=True)
+                for k in ("data", "cos_lia", "mask", "azimuth_time_us"):
+                    v = getattr(g, k)
+                    if v is not None and hasattr(v, "cpu"):
+                        setattr(g, k, v.cpu().numpy())
+                return g
+            out["cpu_baseline"] = cpu_baseline(args, sc, res, merged_px, gpu_band=gpu_band)
         print(json.dumps(out), flush=True)
     if dist is not None:
         dist.barrier()
@@ -359,7 +368,7 @@ def run_e2e(args, sd, sc, ctx, stream, barrier, dist):
             "api": "sardine_b200.calibrate_deburst_merge + terrain_correction, pinned host buffers"}
 
 
-def cpu_baseline(args, sc, res_gpu, merged_px, threads=None, budget_s=12.0):
+def cpu_baseline(args, sc, res_gpu, merged_px, threads=None, budget_s=12.0, gpu_band=None):
     """The oracle (C++ restatement of the reference) on the host cores over a
     bounded sample of the same workload: the full fused prep is timed at full
     size; the terrain correction on a band of output rows."""
@@ -398,7 +407,8 @@ def cpu_baseline(args, sc, res_gpu, merged_px, threads=None, budget_s=12.0):
     t_probe = (time.perf_counter() - t0) / 4
     band = int(max(4, min(rows - r0, budget_s / max(t_probe, 1e-4))))
     t0 = time.perf_counter()
-    oracle.terrain_correction(merged, sc.scene, dem_h, sc.grids, sc.config, row_begin=r0, row_end=r0 + band)
+    ref, ref_t, _ = oracle.terrain_correction(merged, sc.scene, dem_h, sc.grids, sc.config, row_begin=r0,
+                                              row_end=r0 + band, return_times=True)
     t_band = time.perf_counter() - t0
     t_tc_full = t_band / band * rows
     value = res_gpu.total_pixel_count / (t_prep + t_tc_full)
@@ -406,6 +416,17 @@ def cpu_baseline(args, sc, res_gpu, merged_px, threads=None, budget_s=12.0):
                 "sample": (f"full-size fused prep ({merged_px} merged px) + terrain correction on "
                            f"{band} of {rows} output rows (rows {r0}..{r0 + band}); value = output px / "
                            f"(prep time + per-row TC time x rows)")})
+    if gpu_band is not None:
+        # the GPU product path on the same rows of the full-size scene, against the oracle
+        from sardine_b200.accuracy import compare_geocoded
+        g = gpu_band(r0, r0 + band)
+        rep = compare_geocoded(g, ref, g.azimuth_time_us, ref_t,
+                               sc.scene.sub_swaths[0].azimuth_time_interval_s)
+        rep["rows"] = [r0, r0 + band]
+        rep["counters_equal"] = (g.valid_pixel_count == ref.valid_pixel_count and
+                                 g.newton_iter_histogram == ref.newton_iter_histogram and
+                                 g.flat_masked_count == ref.flat_masked_count)
+        out["parity_vs_oracle"] = rep
     return out
 
 

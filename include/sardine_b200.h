@@ -397,14 +397,16 @@ int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image,
  * cols pixels, the counters cover the band, and the band's values equal
  * those rows of the whole-grid call (each output row's solve chain starts
  * from its own LUT seed, terrain_correction.rs:1443).  This is how one
- * scene shards over GPUs by output rows without any exchange. */
+ * scene shards over GPUs by output rows without any exchange.
+ * out_azimuth_time_us (may be NULL) receives the per-pixel converged times
+ * as in sd_terrain_correction_with_times. */
 int sd_terrain_correction_rows(sd_ctx *ctx, const sd_radar_image *image,
                                const sd_scene *scene, const sd_dem *dem,
                                const sd_geoid *geoid, const sd_geo_grid_point *grid,
                                uint64_t n_grid, const sd_tc_config *cfg,
                                uint64_t row_begin, uint64_t row_end,
                                float *out_data, float *out_cos_lia, uint8_t *out_mask,
-                               sd_geocoded_info *info);
+                               int64_t *out_azimuth_time_us, sd_geocoded_info *info);
 /* sd_terrain_correction plus the converged zero-Doppler azimuth time of
  * every output pixel in integer microseconds (INT64_MIN where the solve did
  * not converge, the DEM has no height or the orbit refused the time), for
@@ -477,10 +479,19 @@ int sd_ctx_set_graphs(sd_ctx *ctx, int enable);
 int sd_ctx_reserve(sd_ctx *ctx, uint64_t tile_arena_bytes);
 /* Launch shapes of the tile stages: the speckle/crop block (tx x ty
  * threads, tx >= 8, tx*ty <= 1024 and a multiple of 32; default 32 x 8) and
- * the CTAs per SM of the persistent geocoding kernel (0 = as many as fit).
- * Results do not depend on them; sardine_b200.autotune picks them. */
+ * the geocoding kernel: CTAs per SM of its persistent form (0 = as many as
+ * fit), or -1 for one launch per tile with the job in parameter space over
+ * four forked streams.  Results do not depend on them;
+ * sardine_b200.autotune picks them. */
 int sd_ctx_set_tile_shape(sd_ctx *ctx, int32_t speckle_tx, int32_t speckle_ty,
                           int32_t main_ctas_per_sm);
+
+/* interpolate_orbit_and_accel (orbit.rs:498-596) at m integer-microsecond
+ * times, as the terrain correction evaluates it on the GPU: out holds
+ * m x {pos xyz, vel xyz, acc xyz}.  SD_ERR_TC_ORBIT when a time is outside
+ * the state vectors' span or fewer than 8 vectors are given. */
+int sd_orbit_states(sd_ctx *ctx, const sd_state_vector *svs, uint64_t n, const int64_t *t_us,
+                    uint64_t m, double *out);
 
 /* ── Diagnostics ──────────────────────────────────────────────────────────
  * Runs an FP64 FMA-chain kernel for about `iters` dependent FMAs per thread

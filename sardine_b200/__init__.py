@@ -208,11 +208,9 @@ def terrain_correction(merged: MergedSigma0, scene: SceneMetadata, dem: DemGrid,
         mask = _empty_like_kind(merged_data, (rows, cols), "u1") if config.compute_lia else None
     times = _empty_like_kind(merged_data, (rows, cols), "i8") if return_times else None
     if row_range is not None:
-        if return_times:
-            raise ValueError("row_range and return_times are exclusive")
         rc = lib().sd_terrain_correction_rows(ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo),
                                               g, len(pts), C.byref(cfg), r0, r1, T.ptr(data), T.ptr(cos),
-                                              T.ptr(mask), C.byref(info))
+                                              T.ptr(mask), T.ptr(times), C.byref(info))
     elif return_times:
         rc = lib().sd_terrain_correction_with_times(
             ctx.handle, C.byref(img), C.byref(sc), C.byref(d), C.byref(geo), g, len(pts), C.byref(cfg),

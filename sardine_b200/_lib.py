@@ -42,7 +42,7 @@ _SIGS = {
     "sd_terrain_correction": (C.c_int, [P, P, P, P, P, P, C.c_uint64, P, P, P, P, P]),
     "sd_terrain_correction_with_times": (C.c_int, [P, P, P, P, P, P, C.c_uint64, P, P, P, P, P, P]),
     "sd_terrain_correction_rows": (C.c_int, [P, P, P, P, P, P, C.c_uint64, P, C.c_uint64, C.c_uint64,
-                                             P, P, P, P]),
+                                             P, P, P, P, P]),
     "sd_scene_create": (C.c_int, [P, P, P, P, P, P, C.c_uint64, P]),
     "sd_scene_device_bytes": (C.c_uint64, [P]),
     "sd_scene_destroy": (None, [P]),
@@ -53,6 +53,7 @@ _SIGS = {
     "sd_ctx_set_graphs": (C.c_int, [P, C.c_int]),
     "sd_ctx_reserve": (C.c_int, [P, C.c_uint64]),
     "sd_ctx_set_tile_shape": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32]),
+    "sd_orbit_states": (C.c_int, [P, P, C.c_uint64, P, C.c_uint64, P]),
     "sd_measure_fp64_peak": (C.c_int, [P, C.c_int32, P]),
     "sd_measure_fp32_peak": (C.c_int, [P, C.c_int32, P]),
 }

@@ -18,7 +18,9 @@ from ._lib import Context, lib
 from .tiles import TileRequest, tc_tiles
 
 SPECKLE_SHAPES: List[Tuple[int, int]] = [(32, 8), (32, 4), (64, 4), (32, 16), (16, 16), (128, 2)]
-MAIN_CTAS_PER_SM: List[int] = [0, 3, 2]
+# 0: persistent over all tiles, as many CTAs as fit; 3, 2: fewer per SM;
+# -1: one parameter-form launch per tile over four streams
+MAIN_CTAS_PER_SM: List[int] = [0, 3, -1]
 DEFAULT = {"speckle": [32, 8], "main_cps": 0}
 
 
@@ -85,7 +87,7 @@ def tune(ctx: Context, requests: Sequence[TileRequest], repeats: int = 2,
     for cps in MAIN_CTAS_PER_SM:
         apply(ctx, {"speckle": best["speckle"], "main_cps": cps})
         tc_tiles(requests, ctx)
-        ms = min(_stage_ms(ctx, requests, ("k_main_batch", "k_scan")) for _ in range(repeats))
+        ms = min(_stage_ms(ctx, requests, ("k_main", "k_scan")) for _ in range(repeats))
         scores[f"main_cps {cps}"] = ms
         if best_ms is None or ms < best_ms:
             best_ms, best["main_cps"] = ms, cps

@@ -37,8 +37,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(objdir, exist_ok=True)
     objs = [os.path.join(objdir, os.path.basename(s)[:-3] + ".o") for s in srcs]
     cflags = [f for f in FLAGS if f not in ("-shared", "-lcudart")]
+    headers = [d for d in deps if not d.endswith(".cu")]
+    t_hdr = max(os.path.getmtime(h) for h in headers)
     procs = []
     for src, obj in zip(srcs, objs):
+        # a translation unit recompiles when it or any header is newer than its object
+        if (not force and os.path.exists(obj)
+                and os.path.getmtime(obj) >= max(os.path.getmtime(src), t_hdr)):
+            continue
         cmd = [NVCC] + cflags + (["-Xptxas", "-v"] if verbose else []) + ["-c", "-o", obj, src]
         procs.append(subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
     failed = False

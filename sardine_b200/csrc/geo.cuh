@@ -454,6 +454,89 @@ SD_HD int orbit_eval(const sd_state_vector *svs, uint64_t n, int64_t t, OrbitSta
   return ORB_OK;
 }
 
+// ── orbit as window polynomials ─────────────────────────────────────────────
+// Inside one 8-point window (fixed by the "last state vector at or before t"
+// rule, orbit.rs:530-535) the reference's position and velocity are degree-7
+// polynomials in time (Lagrange interpolants of the window's positions and
+// velocities) and its acceleration is the derivative of the velocity
+// polynomial (orbit.rs:553-593: sum of L_k' v_k).  OrbPoly keeps their
+// monomial coefficients about the window's fourth node, so a state is 60
+// FMAs (Horner) instead of the Lagrange weights' divisions, and a scene's
+// orbit is a few KB instead of a per-microsecond table.  The coefficients are
+// formed in long double on the host; the states differ from the direct
+// Lagrange sums by rounding only (~1e-9 m on 7e6 m).  At a time equal to a
+// state-vector time the reference drops that node's 1/(t - t_j) term, which
+// makes its acceleration differ from the derivative there; orbit_poly_eval
+// then evaluates the reference formula directly.
+struct OrbPoly {
+  int64_t tc;       // time of the window's fourth node (us): x = (t - tc) / 1e6
+  double c[9][8];   // pos xyz, vel xyz, acc xyz: coefficient of x^m at [.][m]
+};
+
+inline void orbit_poly_build(const sd_state_vector *svs, uint64_t n, OrbPoly *out) {
+  for (uint64_t s = 0; s + 8 <= n; ++s) {
+    OrbPoly &w = out[s];
+    w.tc = svs[s + 3].time_us;
+    long double x[8];
+    for (int j = 0; j < 8; ++j) x[j] = (long double)(svs[s + j].time_us - w.tc) / 1e6L;
+    long double cp[6][8] = {};
+    for (int k = 0; k < 8; ++k) {
+      long double poly[8] = {1.0L, 0, 0, 0, 0, 0, 0, 0};
+      long double den = 1.0L;
+      int deg = 0;
+      for (int j = 0; j < 8; ++j) {
+        if (j == k) continue;
+        for (int m = deg + 1; m >= 1; --m) poly[m] = poly[m - 1] - x[j] * poly[m];
+        poly[0] = -x[j] * poly[0];
+        ++deg;
+        den *= x[k] - x[j];
+      }
+      const sd_state_vector &sv = svs[s + k];
+      for (int m = 0; m < 8; ++m) {
+        const long double b = poly[m] / den;
+        for (int d = 0; d < 3; ++d) {
+          cp[d][m] += b * (long double)sv.position_m[d];
+          cp[3 + d][m] += b * (long double)sv.velocity_m_s[d];
+        }
+      }
+    }
+    for (int d = 0; d < 6; ++d)
+      for (int m = 0; m < 8; ++m) w.c[d][m] = (double)cp[d][m];
+    for (int d = 0; d < 3; ++d) {
+      for (int m = 0; m < 7; ++m) w.c[6 + d][m] = (double)((long double)(m + 1) * cp[3 + d][m + 1]);
+      w.c[6 + d][7] = 0.0;
+    }
+  }
+}
+
+SD_HD double horner8(const double *c, double x) {
+  double r = c[7];
+  for (int m = 6; m >= 0; --m) r = fma(r, x, c[m]);
+  return r;
+}
+
+// State at integer microsecond t from the window polynomials (orbit.rs:498-596
+// semantics: window choice, refusal outside the state-vector span).
+SD_HD int orbit_poly_eval(const sd_state_vector *svs, uint64_t n, const OrbPoly *win, int64_t t,
+                          OrbitState *o) {
+  if (n < 8) return ORB_INSUFFICIENT;
+  if (t < svs[0].time_us || t > svs[n - 1].time_us) return ORB_OUTSIDE;
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) / 2;
+    if (svs[mid].time_us <= t) lo = mid + 1; else hi = mid;
+  }
+  const uint64_t centre = lo - 1;
+  if (svs[centre].time_us == t) return orbit_eval(svs, n, t, o);
+  const uint64_t start = centre < 4 ? 0 : (centre + 4 >= n ? n - 8 : centre - 3);
+  const OrbPoly &w = win[start];
+  const double x = (double)(t - w.tc) / 1e6;
+  o->pos = {horner8(w.c[0], x), horner8(w.c[1], x), horner8(w.c[2], x)};
+  o->vel = {horner8(w.c[3], x), horner8(w.c[4], x), horner8(w.c[5], x)};
+  o->acc = {horner8(w.c[6], x), horner8(w.c[7], x), horner8(w.c[8], x)};
+  return ORB_OK;
+}
+
 // One Newton step of solve_zero_doppler (terrain_correction.rs:1030-1067).
 // Returns 0 = converged (|delta| < tol), 1 = step (t advanced), 2 = degenerate.
 SD_HD int zd_step(V3 target, const OrbitState &s, double tol, double *delta_out) {

@@ -164,6 +164,11 @@ void sd_ctx_destroy(sd_ctx *ctx) {
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   for (auto &kv : ctx->graph_exec) cudaGraphExecDestroy(kv.second.exec);
   if (ctx->tiles_done) cudaEventDestroy(ctx->tiles_done);
+  for (int k = 0; k < 4; ++k) {
+    if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
+    if (ctx->ev_join[k]) cudaEventDestroy(ctx->ev_join[k]);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->h_tile_counters) cudaFreeHost(ctx->h_tile_counters);
   if (ctx->h_tile_flags) cudaFreeHost(ctx->h_tile_flags);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);

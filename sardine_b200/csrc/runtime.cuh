@@ -44,7 +44,10 @@ struct sd_ctx {
   bool tiles_pending = false;
   // launch shapes of the tile stages (set by the tile autotuner)
   int sp_tx = 32, sp_ty = 8;  // speckle/crop block
-  int main_cps = 0;           // k_main_batch CTAs per SM (0: as many as fit)
+  int main_cps = 0;           // k_main_batch CTAs per SM (0: as many as fit; -1: per-tile
+                              // parameter launches over the side streams)
+  cudaStream_t side[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[4] = {nullptr, nullptr, nullptr, nullptr};
   // CUDA graphs of the tile stages (persistent kernels over fixed work tables)
   bool graphs = false;
   struct GraphRec {

@@ -85,6 +85,30 @@ int launch_pixels_single(sd_ctx *ctx, const TcWork *d_work, const uint64_t *tota
 }
 
 }  // namespace
+
+int launch_main_param(sd_ctx *ctx, const void *job, cudaStream_t st) {
+  const TcDev &p = *static_cast<const TcDev *>(job);
+  const uint64_t items = p.rows * p.bpr;
+  if (items == 0) return SD_OK;
+  if (items > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "tile too large");
+  const unsigned g = (unsigned)items;
+#define SD_MAIN_PARAM(K)                                                              \
+  if (p.split) k_main<K, true><<<g, MAIN_THREADS, 0, st>>>(p);                         \
+  else k_main<K, false><<<g, MAIN_THREADS, 0, st>>>(p);
+  if (p.resampling == SD_RESAMPLE_BICUBIC) {
+    SD_MAIN_PARAM(SD_RESAMPLE_BICUBIC)
+  } else if (p.resampling == SD_RESAMPLE_LANCZOS3) {
+    SD_MAIN_PARAM(SD_RESAMPLE_LANCZOS3)
+  } else {
+    SD_MAIN_PARAM(SD_RESAMPLE_BILINEAR)
+  }
+#undef SD_MAIN_PARAM
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(ctx, SD_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  return SD_OK;
+}
+
 }  // namespace sd
 
 static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene, const sd_dem *dem,
@@ -196,24 +220,19 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   }
   p.orb.svs = (const sd_state_vector *)d_svs;
   p.orb.n = nsv;
-  p.orb.tab = nullptr;
-  p.orb.tab_t0 = 0;
-  p.orb.tab_n = 0;
+  p.orb.poly = nullptr;
+  SD_TRY(upload_orbit_poly(ctx, "tc.orbit_poly", scene->state_vectors, nsv, &p.orb));
 
   // ── per-row scratch, per-pixel scratch and outputs ──
   int64_t *d_row_guess, *d_knots;
   double *d_row_flat, *d_ax = nullptr, *d_alon = nullptr, *d_alat = nullptr;
-  unsigned long long *d_trange;
   SD_TRY(scratch_t(ctx, "tc.row_guess", p.rows, &d_row_guess));
   SD_TRY(scratch_t(ctx, "tc.row_flat", p.rows, &d_row_flat));
   SD_TRY(scratch_t(ctx, "tc.knots", p.rows * KNOTS, &d_knots));
-  SD_TRY(scratch_t(ctx, "tc.trange", 2, &d_trange));
   p.row_guess = d_row_guess;
   p.row_flat = d_row_flat;
   p.knot_t = d_knots;
-  p.trange = d_trange;
-  unsigned long long tr_init[2] = {~0ull, 0ull};
-  SD_CUDA(ctx, cudaMemcpyAsync(d_trange, tr_init, sizeof tr_init, cudaMemcpyHostToDevice, st));
+  p.trange = nullptr;
   std::vector<double> ax;
   if (p.utm) {
     // project_row anchors (output_crs.rs:383-396); x positions are row-independent
@@ -256,32 +275,13 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   // leave every pixel to the row walk's exact path.
   p.fast = (p.tol <= 1e-6) ? 1 : 0;
   p.bpr = (p.cols + MAIN_PIX - 1) / MAIN_PIX;
+  p.split = cfg->precision == SD_PRECISION_SPLIT;
 
   // ── one-job work table ──
   TcWorkHost wk;
   TcWork *d_work = nullptr;
   SD_TRY(work_upload(ctx, "tc.work", &p, 1, &wk, &d_work));
   SD_TRY(launch_rows(ctx, d_work, wk.totals));
-  unsigned long long tr[2];
-  SD_CUDA(ctx, cudaMemcpyAsync(tr, d_trange, sizeof tr, cudaMemcpyDeviceToHost, st));
-  SD_TRY(sync(ctx));
-
-  // ── orbit table over the row models' time span, inside the SV window ──
-  if (nsv >= 8 && tr[0] <= tr[1]) {
-    int64_t tmin = (int64_t)(tr[0] ^ 0x8000000000000000ull);
-    int64_t tmax = (int64_t)(tr[1] ^ 0x8000000000000000ull);
-    // +-0.1 s covers the height and interpolation spread of pixel roots
-    // around the row models; iterates outside the table are evaluated directly.
-    int64_t t0 = std::max(scene->state_vectors[0].time_us, tmin - 100000);
-    int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us, tmax + 100000);
-    // a table larger than the grid costs more to build than it saves
-    if (t1 >= t0 && (uint64_t)(t1 - t0 + 1) <= npx) {
-      SD_TRY(build_orbit_table(ctx, "tc.orbit_table", (const sd_state_vector *)d_svs, nsv, t0, t1, tmin, tmax,
-                               &p.orb));
-      // the job record on the device carries the table
-      SD_CUDA(ctx, cudaMemcpyAsync((void *)wk.d_jobs, &p, sizeof(TcDev), cudaMemcpyHostToDevice, st));
-    }
-  }
   const bool split = cfg->precision == SD_PRECISION_SPLIT;
   SD_TRY(launch_pixels_single(ctx, d_work, wk.totals, p.resampling, split, &p));
   int flags[64];
@@ -339,7 +339,54 @@ extern "C" int sd_terrain_correction_rows(sd_ctx *ctx, const sd_radar_image *ima
                                           const sd_geo_grid_point *grid, uint64_t n_grid,
                                           const sd_tc_config *cfg, uint64_t row_begin, uint64_t row_end,
                                           float *out_data, float *out_cos_lia, uint8_t *out_mask,
-                                          sd_geocoded_info *info) {
+                                          int64_t *out_azimuth_time_us, sd_geocoded_info *info) {
   return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, row_begin, row_end, out_data, out_cos_lia,
-                out_mask, nullptr, info);
+                out_mask, out_azimuth_time_us, info);
+}
+
+namespace sd {
+namespace {
+__global__ void k_orbit_states(OrbitDev o, const int64_t *t, uint64_t m, double *out, int *flag) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  OrbitState s;
+  double vsq;
+  if (orbit_at(o, t[i], &s, &vsq) != ORB_OK) {
+    atomicOr(flag, 1);
+    return;
+  }
+  double *r = out + 9 * i;
+  r[0] = s.pos.x, r[1] = s.pos.y, r[2] = s.pos.z;
+  r[3] = s.vel.x, r[4] = s.vel.y, r[5] = s.vel.z;
+  r[6] = s.acc.x, r[7] = s.acc.y, r[8] = s.acc.z;
+}
+}  // namespace
+}  // namespace sd
+
+extern "C" int sd_orbit_states(sd_ctx *ctx, const sd_state_vector *svs, uint64_t n, const int64_t *t_us,
+                               uint64_t m, double *out) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!svs || (m && (!t_us || !out))) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null argument");
+  if (m == 0) return SD_OK;
+  SD_CUDA(ctx, cudaSetDevice(ctx->device));
+  const void *d_svs, *d_t;
+  void *d_out;
+  SD_TRY(stage_in(ctx, "orb.svs", svs, n * sizeof(sd_state_vector), &d_svs));
+  SD_TRY(stage_in(ctx, "orb.t", t_us, m * sizeof(int64_t), &d_t));
+  SD_TRY(stage_out(ctx, "orb.out", out, m * 9 * sizeof(double), &d_out));
+  OrbitDev o{(const sd_state_vector *)d_svs, n, nullptr};
+  SD_TRY(upload_orbit_poly(ctx, "orb.poly", svs, n, &o));
+  SD_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, sizeof(int), ctx->stream));
+  SD_TIMED_BEGIN(ctx, "k_orbit_states");
+  k_orbit_states<<<grid_for(m, 128), 128, 0, ctx->stream>>>(o, (const int64_t *)d_t, m, (double *)d_out,
+                                                            ctx->d_flags);
+  SD_LAUNCHED(ctx);
+  int flag = 0;
+  SD_CUDA(ctx, cudaMemcpyAsync(&flag, ctx->d_flags, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  SD_TRY(finish_out(ctx, out, d_out, m * 9 * sizeof(double)));
+  SD_TRY(sync(ctx));
+  if (flag)
+    return set_error(ctx, SD_ERR_TC_ORBIT,
+                     "orbit interpolation failed: interpolation time outside orbit window; refusing to extrapolate");
+  return SD_OK;
 }

@@ -11,10 +11,9 @@
 // 1 us difference moves the sample by ~5e-4 azimuth line.  The stages
 // reproduce that chain exactly while keeping the work data-parallel:
 //
-//  k_orbit_table   FP64 Lagrange state (pos, vel, acc, |v|^2) at every
-//                  microsecond of the span a scene needs (80 B each), so a
-//                  Newton iteration is one table read instead of an
-//                  8-point Lagrange evaluation with 64 divisions.
+//  (orbit)         the 8-point Lagrange orbit as window polynomials
+//                  (geo.cuh: OrbPoly), so a Newton iteration evaluates 60
+//                  FMAs instead of the Lagrange weights' divisions.
 //  k_row_*         per-row set-up: UTM anchors (output_crs.rs:364-417),
 //                  latitude seed, LUT guess, flat-cell area, and a coarse
 //                  azimuth-time model (17 knots per row).
@@ -51,23 +50,11 @@ constexpr int kCounters = 8;  // valid, dem, outside, nonconv, degen, flat, nois
 struct OrbitDev {
   const sd_state_vector *svs;
   uint64_t n;
-  const double2 *tab;  // 5 double2 per microsecond
-  int64_t tab_t0;
-  int64_t tab_n;
+  const OrbPoly *poly;  // n - 7 window polynomials (null: direct Lagrange sums)
 };
 
 __device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
-  int64_t i = t - o.tab_t0;
-  if (i >= 0 && i < o.tab_n) {
-    const double2 *e = o.tab + 5 * i;
-    double2 a = __ldg(e), b = __ldg(e + 1), c = __ldg(e + 2), d = __ldg(e + 3), f = __ldg(e + 4);
-    s->pos = {a.x, a.y, b.x};
-    s->vel = {b.y, c.x, c.y};
-    s->acc = {d.x, d.y, f.x};
-    *vsq = f.y;
-    return ORB_OK;
-  }
-  int rc = orbit_eval(o.svs, o.n, t, s);
+  const int rc = o.poly ? orbit_poly_eval(o.svs, o.n, o.poly, t, s) : orbit_eval(o.svs, o.n, t, s);
   if (rc == ORB_OK) *vsq = dot3(s->vel, s->vel);
   return rc;
 }
@@ -142,7 +129,7 @@ struct TcDev {
   unsigned long long *trange;  // [0] = min, [1] = max (biased by 2^63), or null
   uint64_t bpr;                // k_main work items per row
   int fast;                    // tolerance allows the fixed-point-pair scheme
-  int pad_;
+  int split;                   // SD_PRECISION_SPLIT
   uint64_t row0;               // grid row of the job's first row (row bands)
 };
 
@@ -235,19 +222,6 @@ __device__ int64_t guess_time(const TcDev &p, double lat) {
 }
 
 // ── K1 ─────────────────────────────────────────────────────────────────────
-__global__ void k_orbit_table(const sd_state_vector *svs, uint64_t n, int64_t t0, int64_t cnt,
-                              double2 *tab) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= cnt) return;
-  OrbitState s;
-  orbit_eval(svs, n, t0 + i, &s);  // range is inside the state-vector window
-  double2 *e = tab + 5 * i;
-  e[0] = make_double2(s.pos.x, s.pos.y);
-  e[1] = make_double2(s.pos.z, s.vel.x);
-  e[2] = make_double2(s.vel.y, s.vel.z);
-  e[3] = make_double2(s.acc.x, s.acc.y);
-  e[4] = make_double2(s.acc.z, dot3(s.vel, s.vel));
-}
 
 // ── K2 ─────────────────────────────────────────────────────────────────────
 #define SD_FOR_ITEMS(STAGE)                                                                  \
@@ -1494,8 +1468,9 @@ int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
 // persistent work-table form.
 template <int K, bool S>
 int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const char *name,
-                    const TcDev *job) {
+                    const TcDev *job, bool with_main = true) {
   cudaStream_t st = ctx->stream;
+  if (with_main) {
   SD_TIMED_BEGIN(ctx, name);
   if (job) {
     if (totals[WK_MAIN] > 0x7FFFFFFFull)
@@ -1512,6 +1487,7 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
     k_main_batch<K, S><<<g, MAIN_THREADS, 0, st>>>(d_work);
   }
   SD_LAUNCHED(ctx);
+  }
   SD_TIMED_BEGIN(ctx, "k_scan");
   k_scan<K, S><<<persistent_grid(k_scan<K, S>, SCAN_WARPS * 32, 0, blocks_for(totals[WK_SCAN], SCAN_WARPS)),
                  SCAN_WARPS * 32, 0, st>>>(d_work);
@@ -1522,25 +1498,16 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
   return SD_OK;
 }
 
-// FP64 Lagrange state at every microsecond of [t0, t1] into scratch `name`
-// (capped at 96 M entries, 7.7 GB, centred on [tmin, tmax]).
-int build_orbit_table(sd_ctx *ctx, const char *name, const sd_state_vector *d_svs, uint64_t nsv, int64_t t0,
-                      int64_t t1, int64_t tmin, int64_t tmax, OrbitDev *orb) {
-  const int64_t max_entries = 96ll * 1000 * 1000;
-  if (t1 - t0 + 1 > max_entries) {
-    const int64_t mid = (tmin / 2 + tmax / 2);
-    t0 = std::max(t0, mid - max_entries / 2);
-    t1 = std::min(t1, t0 + max_entries - 1);
-  }
-  if (t1 < t0) return SD_OK;
-  double2 *d_tab;
-  SD_TRY(scratch_t(ctx, name, (size_t)(t1 - t0 + 1) * 5, &d_tab));
-  SD_TIMED_BEGIN(ctx, "k_orbit_table");
-  k_orbit_table<<<grid_for((size_t)(t1 - t0 + 1), 128), 128, 0, ctx->stream>>>(d_svs, nsv, t0, t1 - t0 + 1, d_tab);
-  SD_LAUNCHED(ctx);
-  orb->tab = d_tab;
-  orb->tab_t0 = t0;
-  orb->tab_n = t1 - t0 + 1;
+// Window polynomials of the orbit (orbit_poly_build) in scratch `name`.
+int upload_orbit_poly(sd_ctx *ctx, const char *name, const sd_state_vector *svs, uint64_t nsv,
+                      OrbitDev *orb) {
+  if (nsv < 8) return SD_OK;  // the solve reports the reference's orbit error
+  std::vector<OrbPoly> w(nsv - 7);
+  orbit_poly_build(svs, nsv, w.data());
+  OrbPoly *d = nullptr;
+  SD_TRY(scratch_t(ctx, name, w.size(), &d));
+  SD_CUDA(ctx, cudaMemcpyAsync(d, w.data(), w.size() * sizeof(OrbPoly), cudaMemcpyHostToDevice, ctx->stream));
+  orb->poly = d;
   return SD_OK;
 }
 

@@ -12,10 +12,45 @@ namespace sd {
 namespace {
 
 // Tile batches: the persistent work-table kernels; the resampler is read
-// per job.
-int launch_pixels_batch(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, bool split) {
-  return split ? launch_pixels_t<KDYN, true>(ctx, d_work, totals, "k_main_batch<SPLIT>", nullptr)
-               : launch_pixels_t<KDYN, false>(ctx, d_work, totals, "k_main_batch", nullptr);
+// per job.  with_main false: k_scan and k_select only (k_main ran per tile).
+int launch_pixels_batch(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, bool split,
+                        bool with_main = true) {
+  return split ? launch_pixels_t<KDYN, true>(ctx, d_work, totals, "k_main_batch<SPLIT>", nullptr, with_main)
+               : launch_pixels_t<KDYN, false>(ctx, d_work, totals, "k_main_batch", nullptr, with_main);
+}
+
+// k_main per tile in its parameter form (job record in the kernel's
+// parameter space rather than in shared memory), the tiles spread largest
+// first over four side streams forked from and joined back to the
+// context's stream so that small tiles overlap.
+int fork_main_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs) {
+  for (int k = 0; k < 4; ++k) {
+    if (!ctx->side[k]) SD_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
+    if (!ctx->ev_join[k]) SD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_join[k], cudaEventDisableTiming));
+  }
+  if (!ctx->ev_fork) SD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  const int ns = (int)std::min<size_t>(4, jobs.size());
+  SD_TIMED_BEGIN(ctx, "k_main (per tile)");
+  SD_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+  for (int k = 0; k < ns; ++k) SD_CUDA(ctx, cudaStreamWaitEvent(ctx->side[k], ctx->ev_fork, 0));
+  std::vector<size_t> order(jobs.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+  std::sort(order.begin(), order.end(),
+            [&](size_t a, size_t b) { return jobs[a].rows * jobs[a].cols > jobs[b].rows * jobs[b].cols; });
+  uint64_t load[4] = {0, 0, 0, 0};
+  for (size_t i : order) {
+    int k = 0;
+    for (int q = 1; q < ns; ++q)
+      if (load[q] < load[k]) k = q;
+    SD_TRY(launch_main_param(ctx, &jobs[i], ctx->side[k]));
+    load[k] += jobs[i].rows * jobs[i].cols;
+  }
+  for (int k = 0; k < ns; ++k) {
+    SD_CUDA(ctx, cudaEventRecord(ctx->ev_join[k], ctx->side[k]));
+    SD_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_join[k], 0));
+  }
+  ::sd::timing_end(ctx);
+  return SD_OK;
 }
 
 }  // namespace
@@ -201,30 +236,12 @@ extern "C" int sd_scene_create(sd_ctx *ctx, const sd_radar_image *image, const s
   s->rps = image->range_pixel_spacing_m;
   s->orb.svs = s->svs;
   s->orb.n = nsv;
-  // orbit table over the image's azimuth span +-0.2 s, inside the SV window
+  // the orbit as window polynomials (a few KB), copied with the scene
   if (nsv >= 8) {
-    int64_t t0 = std::max(scene->state_vectors[0].time_us, s->az_start - 200000);
-    int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us,
-                          s->az_start + (int64_t)std::llround((double)s->lines * ati * 1e6) + 200000);
-    const int64_t max_entries = 96ll * 1000 * 1000;
-    if (t1 - t0 + 1 > max_entries) t1 = t0 + max_entries - 1;
-    if (t1 >= t0) {
-      const size_t n = (size_t)(t1 - t0 + 1);
-      void *tab = nullptr;
-      cudaError_t e = cudaMalloc(&tab, n * 5 * sizeof(double2));
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(ctx, SD_ERR_OUT_OF_MEMORY, "scene orbit table: cudaMalloc failed");
-      }
-      s->owned.push_back(tab);
-      s->bytes += n * 5 * sizeof(double2);
-      SD_TIMED_BEGIN(ctx, "k_orbit_table");
-      k_orbit_table<<<grid_for(n, 128), 128, 0, ctx->stream>>>(s->svs, nsv, t0, (int64_t)n, (double2 *)tab);
-      SD_LAUNCHED(ctx);
-      s->orb.tab = (const double2 *)tab;
-      s->orb.tab_t0 = t0;
-      s->orb.tab_n = (int64_t)n;
-    }
+    std::vector<OrbPoly> w(nsv - 7);
+    orbit_poly_build(scene->state_vectors, nsv, w.data());
+    SD_TRY(scene_copy(ctx, s.get(), w.data(), w.size() * sizeof(OrbPoly), &d));
+    s->orb.poly = (const OrbPoly *)d;
   }
   SD_TRY(sync(ctx));
   *out = s.release();
@@ -441,6 +458,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     p.flags = d_flg + 4 * i;
     p.trange = nullptr;
     const int g = tiles[i].cfg.precision == SD_PRECISION_SPLIT ? 1 : 0;
+    p.split = g;
     grp[g].push_back(p);
     if (pl.crop) {
       SpJob j = pl.sp;
@@ -473,7 +491,11 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     }
     SD_TRY(work_upload(ctx, wname, grp[g].data(), (int)grp[g].size(), &wk, &d_work));
     const bool split = g == 1;
-    if (use_graph) {
+    if (ctx->main_cps < 0) {  // per-tile parameter launches of k_main
+      SD_TRY(launch_rows(ctx, d_work, wk.totals));
+      SD_TRY(fork_main_per_tile(ctx, grp[g]));
+      SD_TRY(launch_pixels_batch(ctx, d_work, wk.totals, split, false));
+    } else if (use_graph) {
       static const uint64_t kFull[kWk] = {~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull};
       SD_TRY(run_graph(ctx, g + 2 * ctx->main_cps, d_work, [&]() -> int {
         SD_TRY(launch_rows(ctx, d_work, kFull));
@@ -620,8 +642,8 @@ extern "C" int sd_ctx_set_tile_shape(sd_ctx *ctx, int32_t speckle_tx, int32_t sp
   if (!speckle_shape_ok(speckle_tx, speckle_ty))
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "speckle block %dx%d: need tx >= 8, tx*ty <= 1024, tx*ty %% 32 == 0",
                      speckle_tx, speckle_ty);
-  if (main_ctas_per_sm < 0 || main_ctas_per_sm > 64)
-    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "main_ctas_per_sm must be 0..64");
+  if (main_ctas_per_sm < -1 || main_ctas_per_sm > 64)
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "main_ctas_per_sm must be -1..64");
   ctx->sp_tx = speckle_tx;
   ctx->sp_ty = speckle_ty;
   ctx->main_cps = main_ctas_per_sm;

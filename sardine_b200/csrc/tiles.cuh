@@ -34,6 +34,9 @@ struct SpWork {
 };
 
 int speckle_masks(sd_ctx *ctx);
+// k_main in its parameter form for one terrain-correction job record (the
+// TcDev layout of tc_kernels.cuh), on stream st.
+int launch_main_param(sd_ctx *ctx, const void *job, cudaStream_t st);
 int speckle_validate(uint64_t len, uint64_t cols, uint64_t rows, int kind, uint64_t window, float enl,
                      float damping);
 void speckle_coefs(int kind, uint64_t window, float enl, float damping, SpJob *j);

@@ -170,3 +170,26 @@ def test_row_bands_equal_whole_grid(ctx):
     assert np.array_equal(np.concatenate([p.mask for p in parts]), whole.mask)
     assert sum(p.valid_pixel_count for p in parts) == whole.valid_pixel_count
     assert list(np.sum([p.newton_iter_histogram for p in parts], axis=0)) == whole.newton_iter_histogram
+
+
+def test_orbit_window_polynomials_match_lagrange(ctx):
+    """The GPU orbit (window polynomials) against the oracle's 8-point
+    Lagrange at random microseconds and at the state-vector times themselves
+    (where the reference's acceleration formula drops a term)."""
+    import ctypes as C
+    sc = synth.config1_scene(seed=19, n_lines=256, n_samples=512, dem_n=64)
+    orb = sc.scene.orbit
+    t = np.asarray(orb.times_us, np.int64)
+    rng = np.random.default_rng(3)
+    times = np.concatenate([rng.integers(t[0], t[-1] + 1, 4000), t, t[1:-1] - 1, t[1:-1] + 1]).astype(np.int64)
+    out = np.empty((len(times), 9), np.float64)
+    svs = orb.to_c()
+    rc = sd.lib().sd_orbit_states(ctx.handle, svs, len(t), times.ctypes.data, len(times), out.ctypes.data)
+    assert rc == 0, ctx.last_error()
+    ref = np.array([np.concatenate(oracle.interpolate_orbit_and_accel(orb, int(x))[1:]) for x in times])
+    assert np.abs(out[:, 0:3] - ref[:, 0:3]).max() < 1e-7        # m, of ~7e6 m
+    assert np.abs(out[:, 3:6] - ref[:, 3:6]).max() < 1e-9        # m/s
+    assert np.abs(out[:, 6:9] - ref[:, 6:9]).max() < 1e-9        # m/s^2
+    bad = np.array([t[-1] + 1], np.int64)
+    rc = sd.lib().sd_orbit_states(ctx.handle, svs, len(t), bad.ctypes.data, 1, out.ctypes.data)
+    assert rc == 10

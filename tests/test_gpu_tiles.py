@@ -163,3 +163,26 @@ def test_tiles_async_and_errors(ctx):
         tiles.tc_tiles([bad], ctx)
     assert e.value.kind == "Config"
     rs.close()
+
+
+def test_tiles_launch_shapes_do_not_change_results(ctx):
+    """Every launch shape the autotuner may pick (speckle block, persistent
+    CTAs per SM, per-tile parameter launches) gives bit-identical tiles."""
+    from sardine_b200 import autotune
+    sc, rs, g = _scene(ctx, 59)
+    reqs = [_req(sc, rs, g, 0, 0, 60, 80, K.Bicubic, speckle=sd.SpeckleFilter.GammaMap(5, 4.4)),
+            _req(sc, rs, g, 70, 10, 33, 120, K.Lanczos3, precision=sd.Precision.SPLIT),
+            _req(sc, rs, g, 11, 12, 90, 45, K.Bilinear, speckle=sd.SpeckleFilter.RefinedLee(4.4))]
+    base = [_host(r) for r in tiles.tc_tiles(reqs, ctx)]
+    try:
+        for shape in ([64, 4], [16, 16], [128, 2]):
+            for cps in (0, 2, -1):
+                autotune.apply(ctx, {"speckle": shape, "main_cps": cps})
+                got = [_host(r) for r in tiles.tc_tiles(reqs, ctx)]
+                for x, y in zip(base, got):
+                    assert np.array_equal(x.data, y.data, equal_nan=True), (shape, cps)
+                    assert np.array_equal(x.mask, y.mask)
+                    assert x.newton_iter_histogram == y.newton_iter_histogram
+    finally:
+        autotune.apply(ctx, autotune.DEFAULT)
+    rs.close()
