@@ -664,41 +664,79 @@ def run_c5(args):
     dev = f"cuda:{local}"
     scenes = _c5_setup(sd, ctx, dev, rank, args.scenes)
     rng = np.random.default_rng(5 + rank)
-    burst = args.burst
-    rate = args.rate
+    rates = [float(r) for r in args.rates.split(",")]
     budget = args.budget_gb << 30
     server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=64, graphs=True)
     sample = _c5_requests(sd, scenes, rng, 64, sd.Precision.SPLIT)
+    tune = None
     for s in server.slots:
-        autotune.tune(s.ctx, sample[:32])
-    # warm-up bursts (graph capture, allocator), then the timed stream
-    for _ in range(args.warmup):
-        reqs = _c5_requests(sd, scenes, rng, burst // 4, sd.Precision.SPLIT)
-        _serve(server, reqs, np.cumsum(rng.exponential(1.0 / rate, len(reqs))))
-    n = burst * args.steps
+        tune = autotune.tune(s.ctx, sample[:32])
+    for _ in range(args.warmup):  # graph capture, allocator, autotuned shapes in place
+        reqs = _c5_requests(sd, scenes, rng, args.burst // 4, sd.Precision.SPLIT)
+        _serve(server, reqs, np.cumsum(rng.exponential(1.0 / rates[-1], len(reqs))))
+    by_rate = {}
+    value = ms = None
+    gpu_launches = 0
+    clk_summary = None
+    for rate in rates:
+        n = args.burst * args.steps if rate == rates[-1] else int(max(64, min(args.burst * args.steps, rate * 3)))
+        reqs = _c5_requests(sd, scenes, rng, n, sd.Precision.SPLIT)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        l0 = sum(s.ctx.launches for s in server.slots)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            torch.cuda.synchronize()
+            e0.record()
+            tickets = _serve(server, reqs, arrivals)
+            torch.cuda.synchronize()
+            e1.record()
+            torch.cuda.synchronize()
+        summ = latency_summary(tickets)
+        summ["rate_req_s"] = rate
+        summ["requests"] = n
+        by_rate[str(int(rate))] = summ
+        if rate == rates[-1]:
+            ms = _max_over_ranks(dist, e0.elapsed_time(e1))
+            value = world * summ["px"] / (ms / 1e3)
+            gpu_launches = sum(s.ctx.launches for s in server.slots) - l0
+            clk_summary = clk.summary()
+            head = summ
+    # end to end: the headline stream again, each result copied to host memory
+    # as it completes (the D2H is inside the latency)
+    host_buf = torch.empty(3 * 2048 * 2048 * 4 + 4096, dtype=torch.uint8, pin_memory=True)
+    d2h = [0]
+
+    def to_host(t):
+        off = 0
+        for plane in (t.result.data, t.result.cos_lia, t.result.mask):
+            if plane is None:
+                continue
+            nb = plane.numel() * plane.element_size()
+            host_buf[off:off + nb].copy_(plane.reshape(-1).view(torch.uint8))
+            off += nb
+        d2h[0] += off
+    e2e_server = GeocodingServer(local, hbm_budget=budget // 2, slots=2, max_batch=64, graphs=True,
+                                 on_done=to_host)
+    for s in e2e_server.slots:
+        autotune.apply(s.ctx, tune)
+    n = args.burst * args.steps
     reqs = _c5_requests(sd, scenes, rng, n, sd.Precision.SPLIT)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
-    l0 = sum(s.ctx.launches for s in server.slots)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        torch.cuda.synchronize()
-        e0.record()
-        tickets = _serve(server, reqs, arrivals)
-        torch.cuda.synchronize()
-        e1.record()
-        torch.cuda.synchronize()
-    ms = _max_over_ranks(dist, e0.elapsed_time(e1))
-    summ = latency_summary(tickets)
-    gpu_launches = sum(s.ctx.launches for s in server.slots) - l0
-    value = world * summ["px"] / (ms / 1e3)
+    arrivals = np.cumsum(rng.exponential(1.0 / rates[-1], n))
+    _serve(e2e_server, reqs[:16], arrivals[:16])
+    d2h[0] = 0
+    t0 = time.perf_counter()
+    et = _serve(e2e_server, reqs, arrivals)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    esum = latency_summary(et)
+    e2e_server.close()
     # plain per-request FP64 path on the same GPU: one tile per launch, no graphs
     base = GeocodingServer(local, hbm_budget=4 << 30, slots=1, max_batch=1, graphs=False)
-    nb = max(64, n // 2)
+    nb = max(64, args.burst * args.steps // 2)
     breqs = _c5_requests(sd, scenes, np.random.default_rng(55 + rank), nb, sd.Precision.FP64)
-    barr = np.cumsum(np.random.default_rng(56).exponential(1.0 / rate, nb))
+    barr = np.cumsum(np.random.default_rng(56).exponential(1.0 / rates[-1], nb))
     _serve(base, breqs[:8], barr[:8])
     bsum = latency_summary(_serve(base, breqs, barr))
-    # split accuracy: the same tiles through the FP64 path
     acc = _split_vs_fp64(sd, tiles, server.slots[0].ctx, scenes, rng)
     base.close()
     if rank == 0:
@@ -708,19 +746,24 @@ def run_c5(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (split)",
             "data": "synthetic (seeded config-2-shape IW scenes resident in HBM)",
             "config": {"workload": (f"config5: {args.scenes} config-2-shape scenes resident (merged sigma0+NESZ, "
-                                    f"DEM, orbit table); Poisson tile requests at {rate} req/s, sides "
-                                    "256-2048 log-uniform, random scene/bbox/resampler/speckle, split precision, "
-                                    "continuous batching over 2 slots, HBM-budget admission"),
-                       "requests": n, "burst_per_step": burst, "rate_req_s": rate,
-                       "hbm_budget_gb": args.budget_gb,
+                                    "DEM, orbit table); Poisson tile requests, sides 256-2048 log-uniform, "
+                                    "random scene/bbox/resampler/speckle, split precision, continuous batching "
+                                    "over 2 slots, HBM-budget admission; value at the highest rate"),
+                       "rates_req_s": rates, "burst_per_step": args.burst,
+                       "hbm_budget_gb": args.budget_gb, "autotune": tune,
                        "scene_device_gb": round(sum(s["rs"].device_bytes for s in scenes) / 2**30, 2),
                        "parallelism": f"replicas x{world}"},
-            "latency_ms": {"p50": summ["p50_ms"], "p99": summ["p99_ms"], "mean": summ["mean_ms"],
-                           "what": "request submit -> results on the device"},
-            "served": summ,
+            "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"], "mean": head["mean_ms"],
+                           "what": f"request submit -> results on the device, at {rates[-1]:.0f} req/s"},
+            "served_by_rate": by_rate,
             "per_request_fp64": bsum,
             "accuracy_split_vs_fp64": acc,
-            "gpu_launches": gpu_launches, "clocks": clk.summary(), "e2e": None,
+            "gpu_launches": gpu_launches, "clocks": clk_summary,
+            "e2e": {"value": world * esum["px"] / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": int(d2h[0] / max(1, args.steps)),
+                    "p50_ms": esum["p50_ms"], "p99_ms": esum["p99_ms"],
+                    "api": "GeocodingServer with every result copied to pinned host memory on completion "
+                           "(scenes resident; request inputs are descriptors only)"},
         }
         print(json.dumps(out), flush=True)
     server.close()
@@ -877,7 +920,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c4", "c5"])
-    ap.add_argument("--rate", type=float, default=2000.0, help="config5 request rate (req/s)")
+    ap.add_argument("--rates", default="100,500,2000", help="config5 request rates (req/s); value at the last")
     ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
     ap.add_argument("--scenes", type=int, default=8, help="config5 resident scenes")
     ap.add_argument("--budget-gb", dest="budget_gb", type=int, default=16, help="config5 HBM budget")

@@ -41,6 +41,14 @@ def compare_geocoded(test, ref, t_test=None, t_ref=None, ati_s: float = 1.0) -> 
         db = np.abs(10.0 * np.log10(x[pos] / y[pos])) if pos.any() else np.zeros(1)
         rep["sigma_rel_err_max"] = float(rel.max())
         rep["sigma_rel_over_1e-4_px"] = int((rel > 1e-4).sum())
+        # relative to max(|ref|, floor): a value interpolated to nearly zero
+        # between non-zero samples is ill-conditioned (any sub-ulp change of
+        # the image coordinates moves it by more than 1e-4 of itself); the
+        # floor, 1 % of the median |ref|, is a noise-floor-level magnitude
+        pos_b = np.abs(y[y != 0])
+        floor = 0.01 * float(np.median(pos_b)) if pos_b.size else 0.0
+        rep["sigma_floor"] = floor
+        rep["sigma_floor_over_1e-4_px"] = int((np.abs(x - y) > 1e-4 * np.maximum(np.abs(y), floor)).sum())
         rep["sigma_rel_err_p99"] = float(np.quantile(rel, 0.99))
         rep["sigma_rel_err_mean"] = float(rel.mean())
         rep["sigma_db_err_max"] = float(db.max())
@@ -51,6 +59,8 @@ def compare_geocoded(test, ref, t_test=None, t_ref=None, ati_s: float = 1.0) -> 
                   "sigma_db_err_max", "sigma_db_err_p99", "sigma_db_err_mean"):
             rep[k] = 0.0
         rep["sigma_rel_over_1e-4_px"] = 0
+        rep["sigma_floor_over_1e-4_px"] = 0
+        rep["sigma_floor"] = 0.0
     if test.mask is not None and ref.mask is not None:
         rep["mask_equal"] = bool(np.array_equal(_np(test.mask), _np(ref.mask)))
         ca = _np(test.cos_lia).astype(np.float64)
@@ -83,6 +93,11 @@ def _compare_torch(test, ref, t_test, t_ref, ati_s):
     rel = (x - y).abs() / y.abs().clamp_min(1e-30)
     rep["sigma_rel_err_max"] = float(rel.max()) if rel.numel() else 0.0
     rep["sigma_rel_over_1e-4_px"] = int((rel > 1e-4).sum())
+    nz = y.abs()[y != 0]
+    floor = 0.01 * float(nz[torch.randint(0, max(1, nz.numel()), (min(nz.numel(), 1 << 22),),
+                                          device=nz.device)].median()) if nz.numel() else 0.0
+    rep["sigma_floor"] = floor
+    rep["sigma_floor_over_1e-4_px"] = int(((x - y).abs() > 1e-4 * y.abs().clamp_min(floor)).sum())
     rep["sigma_rel_err_mean"] = float(rel.mean()) if rel.numel() else 0.0
     g = torch.Generator(device=rel.device).manual_seed(0)
     sub = rel[torch.randint(0, max(1, rel.numel()), (min(rel.numel(), 1 << 22),), device=rel.device,

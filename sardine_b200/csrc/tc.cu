@@ -220,6 +220,9 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   }
   p.orb.svs = (const sd_state_vector *)d_svs;
   p.orb.n = nsv;
+  p.orb.tab = nullptr;
+  p.orb.tab_t0 = 0;
+  p.orb.tab_n = 0;
   p.orb.poly = nullptr;
   SD_TRY(upload_orbit_poly(ctx, "tc.orbit_poly", scene->state_vectors, nsv, &p.orb));
 
@@ -229,10 +232,14 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   SD_TRY(scratch_t(ctx, "tc.row_guess", p.rows, &d_row_guess));
   SD_TRY(scratch_t(ctx, "tc.row_flat", p.rows, &d_row_flat));
   SD_TRY(scratch_t(ctx, "tc.knots", p.rows * KNOTS, &d_knots));
+  unsigned long long *d_trange;
+  SD_TRY(scratch_t(ctx, "tc.trange", 2, &d_trange));
   p.row_guess = d_row_guess;
   p.row_flat = d_row_flat;
   p.knot_t = d_knots;
-  p.trange = nullptr;
+  p.trange = d_trange;
+  unsigned long long tr_init[2] = {~0ull, 0ull};
+  SD_CUDA(ctx, cudaMemcpyAsync(d_trange, tr_init, sizeof tr_init, cudaMemcpyHostToDevice, st));
   std::vector<double> ax;
   if (p.utm) {
     // project_row anchors (output_crs.rs:383-396); x positions are row-independent
@@ -282,6 +289,26 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   TcWork *d_work = nullptr;
   SD_TRY(work_upload(ctx, "tc.work", &p, 1, &wk, &d_work));
   SD_TRY(launch_rows(ctx, d_work, wk.totals));
+  unsigned long long tr[2];
+  SD_CUDA(ctx, cudaMemcpyAsync(tr, d_trange, sizeof tr, cudaMemcpyDeviceToHost, st));
+  SD_TRY(sync(ctx));
+
+  // ── orbit table over the row models' time span, inside the SV window ──
+  if (nsv >= 8 && tr[0] <= tr[1]) {
+    int64_t tmin = (int64_t)(tr[0] ^ 0x8000000000000000ull);
+    int64_t tmax = (int64_t)(tr[1] ^ 0x8000000000000000ull);
+    // +-0.1 s covers the height and interpolation spread of pixel roots
+    // around the row models; iterates outside the table are evaluated directly.
+    int64_t t0 = std::max(scene->state_vectors[0].time_us, tmin - 100000);
+    int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us, tmax + 100000);
+    // a table larger than the grid costs more to build than it saves
+    if (t1 >= t0 && (uint64_t)(t1 - t0 + 1) <= npx) {
+      SD_TRY(build_orbit_table(ctx, "tc.orbit_table", (const sd_state_vector *)d_svs, nsv, t0, t1, tmin, tmax,
+                               &p.orb));
+      // the job record on the device carries the table
+      SD_CUDA(ctx, cudaMemcpyAsync((void *)wk.d_jobs, &p, sizeof(TcDev), cudaMemcpyHostToDevice, st));
+    }
+  }
   const bool split = cfg->precision == SD_PRECISION_SPLIT;
   SD_TRY(launch_pixels_single(ctx, d_work, wk.totals, p.resampling, split, &p));
   int flags[64];
@@ -374,7 +401,9 @@ extern "C" int sd_orbit_states(sd_ctx *ctx, const sd_state_vector *svs, uint64_t
   SD_TRY(stage_in(ctx, "orb.svs", svs, n * sizeof(sd_state_vector), &d_svs));
   SD_TRY(stage_in(ctx, "orb.t", t_us, m * sizeof(int64_t), &d_t));
   SD_TRY(stage_out(ctx, "orb.out", out, m * 9 * sizeof(double), &d_out));
-  OrbitDev o{(const sd_state_vector *)d_svs, n, nullptr};
+  OrbitDev o{};
+  o.svs = (const sd_state_vector *)d_svs;
+  o.n = n;
   SD_TRY(upload_orbit_poly(ctx, "orb.poly", svs, n, &o));
   SD_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, sizeof(int), ctx->stream));
   SD_TIMED_BEGIN(ctx, "k_orbit_states");

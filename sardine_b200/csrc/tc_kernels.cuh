@@ -11,9 +11,11 @@
 // 1 us difference moves the sample by ~5e-4 azimuth line.  The stages
 // reproduce that chain exactly while keeping the work data-parallel:
 //
-//  (orbit)         the 8-point Lagrange orbit as window polynomials
-//                  (geo.cuh: OrbPoly), so a Newton iteration evaluates 60
-//                  FMAs instead of the Lagrange weights' divisions.
+//  k_orbit_table   FP64 Lagrange state (pos, vel, acc, |v|^2) at every
+//                  microsecond of the span a scene needs (80 B each), so a
+//                  Newton iteration is one table read instead of an 8-point
+//                  Lagrange evaluation with 56 divisions; outside the table
+//                  the window polynomials (geo.cuh: OrbPoly) stand in.
 //  k_row_*         per-row set-up: UTM anchors (output_crs.rs:364-417),
 //                  latitude seed, LUT guess, flat-cell area, and a coarse
 //                  azimuth-time model (17 knots per row).
@@ -50,10 +52,26 @@ constexpr int kCounters = 8;  // valid, dem, outside, nonconv, degen, flat, nois
 struct OrbitDev {
   const sd_state_vector *svs;
   uint64_t n;
-  const OrbPoly *poly;  // n - 7 window polynomials (null: direct Lagrange sums)
+  const double2 *tab;   // 5 double2 per microsecond: pos, vel, acc, |v|^2
+  int64_t tab_t0;
+  int64_t tab_n;
+  const OrbPoly *poly;  // n - 7 window polynomials for times outside the table
 };
 
+// State at integer microsecond t: the table (the reference's Lagrange sums,
+// evaluated once per microsecond) inside its span, the window polynomials
+// outside it, the Lagrange sums directly when neither exists.
 __device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
+  const int64_t i = t - o.tab_t0;
+  if (i >= 0 && i < o.tab_n) {
+    const double2 *e = o.tab + 5 * i;
+    double2 a = __ldg(e), b = __ldg(e + 1), c = __ldg(e + 2), d = __ldg(e + 3), f = __ldg(e + 4);
+    s->pos = {a.x, a.y, b.x};
+    s->vel = {b.y, c.x, c.y};
+    s->acc = {d.x, d.y, f.x};
+    *vsq = f.y;
+    return ORB_OK;
+  }
   const int rc = o.poly ? orbit_poly_eval(o.svs, o.n, o.poly, t, s) : orbit_eval(o.svs, o.n, t, s);
   if (rc == ORB_OK) *vsq = dot3(s->vel, s->vel);
   return rc;
@@ -224,6 +242,21 @@ __device__ int64_t guess_time(const TcDev &p, double lat) {
 // ── K1 ─────────────────────────────────────────────────────────────────────
 
 // ── K2 ─────────────────────────────────────────────────────────────────────
+// ── orbit table ──────────────────────────────────────────────────────────────
+__global__ void k_orbit_table(const sd_state_vector *svs, uint64_t n, int64_t t0, int64_t cnt,
+                              double2 *tab) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnt) return;
+  OrbitState s;
+  orbit_eval(svs, n, t0 + i, &s);  // range is inside the state-vector window
+  double2 *e = tab + 5 * i;
+  e[0] = make_double2(s.pos.x, s.pos.y);
+  e[1] = make_double2(s.pos.z, s.vel.x);
+  e[2] = make_double2(s.vel.y, s.vel.z);
+  e[3] = make_double2(s.acc.x, s.acc.y);
+  e[4] = make_double2(s.acc.z, dot3(s.vel, s.vel));
+}
+
 #define SD_FOR_ITEMS(STAGE)                                                                  \
   const TcWork w = *wp;                                                                      \
   const uint64_t *pre = stage_pre(w, STAGE);                                                 \
@@ -383,17 +416,23 @@ __device__ float sample_bicubic(const float *d, uint64_t nl, uint64_t ns, double
 // The build compiles with --fmad=false (the FP64 path must not contract);
 // the FP32 code contracts explicitly with fmaf.
 
-__device__ __forceinline__ float keys_weight_f(float t) {  // keys_weight, Horner form
-  t = fabsf(t);
-  if (t < 1.f) return fmaf(fmaf(1.5f, t, -2.5f), t * t, 1.f);
-  if (t < 2.f) return fmaf(fmaf(fmaf(-0.5f, t, 2.5f), t, -4.f), t, 2.f);
-  return 0.f;
+// keys_weight (a = -0.5) of the taps -1, 0, 1, 2 at offsets k - f, in
+// factored form: 1.5u^3 - 2.5u^2 + 1 = (1 - u)(1 + u - 1.5u^2) on [0, 1) and
+// -0.5u^3 + 2.5u^2 - 4u + 2 = -0.5(u - 1)(u - 2)^2 on [1, 2).  Expanded, the
+// cubics cancel near their roots and a small weight loses its leading
+// digits; factored, every weight keeps its relative accuracy.
+__device__ __forceinline__ void keys4_f(float f, float w[4]) {
+  const float g = 1.f - f;
+  w[0] = -0.5f * f * g * g;
+  w[1] = g * fmaf(-1.5f * f, f, 1.f + f);
+  w[2] = f * fmaf(-1.5f * g, g, 1.f + g);
+  w[3] = -0.5f * g * f * f;
 }
 
 // Lanczos-3 weights (terrain_correction.rs:938-952) of the taps li = -2..3
 // at x = f - li.  sin(pi x) = (-1)^li sin(pi f) and sin(pi x/3) =
 // sin(pi f/3) cos(pi li/3) - cos(pi f/3) sin(pi li/3), so the six weights
-// take one sinpi and one sincospi (plus one sinpi for the tap li = 1).
+// take two sinpi and one sincospi.
 template <typename T>
 __device__ __forceinline__ void lanczos6(T f, T w[6]);
 
@@ -402,6 +441,7 @@ __device__ __forceinline__ void lanczos6<float>(float f, float w[6]) {
   const float s1 = sinpif(f);
   float s3, c3;
   sincospif(f * (1.f / 3.f), &s3, &c3);
+  const float q = sinpif((1.f - f) * (1.f / 3.f));
   const float h = 0.866025403784438647f;  // sin(pi/3)
   const float cl[6] = {-0.5f, 0.5f, 1.f, 0.5f, -0.5f, -1.f};
   const float sl[6] = {-h, -h, 0.f, h, h, 0.f};
@@ -412,9 +452,9 @@ __device__ __forceinline__ void lanczos6<float>(float f, float w[6]) {
     const float x = f - (float)li;
     const float ax = fabsf(x);
     const float s = (li & 1) ? -s1 : s1;
-    // tap li = 1: the angle-addition form cancels as f -> 1 (where this tap
-    // carries the weight), so its sine is taken directly
-    const float s3l = li == 1 ? sinpif((f - 1.f) * (1.f / 3.f)) : s3 * cl[j] - c3 * sl[j];
+    // taps li = -2 and 1: the angle-addition form cancels as f -> 1, so
+    // their sines are taken directly, sin(pi(f+2)/3) = -sin(pi(f-1)/3) = q
+    const float s3l = li == 1 ? -q : (li == -2 ? q : s3 * cl[j] - c3 * sl[j]);
     w[j] = ax < 1e-10f ? 1.f : (ax < 3.f ? k * s * s3l / (x * x) : 0.f);
   }
 }
@@ -424,6 +464,7 @@ __device__ __forceinline__ void lanczos6<double>(double f, double w[6]) {
   const double s1 = sinpi(f);
   double s3, c3;
   sincospi(f * (1.0 / 3.0), &s3, &c3);
+  const double q = sinpi((1.0 - f) * (1.0 / 3.0));
   const double h = 0.86602540378443864676;
   const double cl[6] = {-0.5, 0.5, 1.0, 0.5, -0.5, -1.0};
   const double sl[6] = {-h, -h, 0.0, h, h, 0.0};
@@ -434,7 +475,7 @@ __device__ __forceinline__ void lanczos6<double>(double f, double w[6]) {
     const double x = f - (double)li;
     const double ax = fabs(x);
     const double s = (li & 1) ? -s1 : s1;
-    const double s3l = li == 1 ? sinpi((f - 1.0) * (1.0 / 3.0)) : s3 * cl[j] - c3 * sl[j];
+    const double s3l = li == 1 ? -q : (li == -2 ? q : s3 * cl[j] - c3 * sl[j]);
     w[j] = ax < 1e-10 ? 1.0 : (ax < 3.0 ? k * s * s3l / (x * x) : 0.0);
   }
 }
@@ -474,18 +515,17 @@ __device__ float sample_bicubic_f(const float *d, uint64_t nl, uint64_t ns, doub
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
   const float dl = (float)(line - (double)lf), ds = (float)(sample - (double)sf);
-  float ws[4];
+  float ws[4], wls[4];
+  keys4_f(ds, ws);
+  keys4_f(dl, wls);
   int64_t cols[4];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    ws[k] = keys_weight_f((float)(k - 1) - ds);
-    cols[k] = clampi(sf + k - 1, 0, max_s);
-  }
+  for (int k = 0; k < 4; ++k) cols[k] = clampi(sf + k - 1, 0, max_s);
   float acc = 0.f, aacc = 0.f;
 #pragma unroll
   for (int li = -1; li <= 2; ++li) {
     int64_t row = clampi(lf + li, 0, max_l);
-    const float wl = keys_weight_f((float)li - dl);
+    const float wl = wls[li + 1];
     float racc = 0.f, rabs = 0.f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -1495,6 +1535,28 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
   SD_TIMED_BEGIN(ctx, "k_select");
   k_select<<<persistent_grid(k_select, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
   SD_LAUNCHED(ctx);
+  return SD_OK;
+}
+
+// FP64 Lagrange state at every microsecond of [t0, t1] into scratch `name`
+// (capped at 96 M entries, 7.7 GB, centred on [tmin, tmax]).
+int build_orbit_table(sd_ctx *ctx, const char *name, const sd_state_vector *d_svs, uint64_t nsv, int64_t t0,
+                      int64_t t1, int64_t tmin, int64_t tmax, OrbitDev *orb) {
+  const int64_t max_entries = 96ll * 1000 * 1000;
+  if (t1 - t0 + 1 > max_entries) {
+    const int64_t mid = (tmin / 2 + tmax / 2);
+    t0 = std::max(t0, mid - max_entries / 2);
+    t1 = std::min(t1, t0 + max_entries - 1);
+  }
+  if (t1 < t0) return SD_OK;
+  double2 *d_tab;
+  SD_TRY(scratch_t(ctx, name, (size_t)(t1 - t0 + 1) * 5, &d_tab));
+  SD_TIMED_BEGIN(ctx, "k_orbit_table");
+  k_orbit_table<<<grid_for((size_t)(t1 - t0 + 1), 128), 128, 0, ctx->stream>>>(d_svs, nsv, t0, t1 - t0 + 1, d_tab);
+  SD_LAUNCHED(ctx);
+  orb->tab = d_tab;
+  orb->tab_t0 = t0;
+  orb->tab_n = t1 - t0 + 1;
   return SD_OK;
 }
 

@@ -236,12 +236,37 @@ extern "C" int sd_scene_create(sd_ctx *ctx, const sd_radar_image *image, const s
   s->rps = image->range_pixel_spacing_m;
   s->orb.svs = s->svs;
   s->orb.n = nsv;
-  // the orbit as window polynomials (a few KB), copied with the scene
+  // the orbit as window polynomials (a few KB; used outside the table)
   if (nsv >= 8) {
     std::vector<OrbPoly> w(nsv - 7);
     orbit_poly_build(scene->state_vectors, nsv, w.data());
     SD_TRY(scene_copy(ctx, s.get(), w.data(), w.size() * sizeof(OrbPoly), &d));
     s->orb.poly = (const OrbPoly *)d;
+  }
+  // orbit table over the image's azimuth span +-0.2 s, inside the SV window
+  if (nsv >= 8) {
+    int64_t t0 = std::max(scene->state_vectors[0].time_us, s->az_start - 200000);
+    int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us,
+                          s->az_start + (int64_t)std::llround((double)s->lines * ati * 1e6) + 200000);
+    const int64_t max_entries = 96ll * 1000 * 1000;
+    if (t1 - t0 + 1 > max_entries) t1 = t0 + max_entries - 1;
+    if (t1 >= t0) {
+      const size_t n = (size_t)(t1 - t0 + 1);
+      void *tab = nullptr;
+      cudaError_t e = cudaMalloc(&tab, n * 5 * sizeof(double2));
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(ctx, SD_ERR_OUT_OF_MEMORY, "scene orbit table: cudaMalloc failed");
+      }
+      s->owned.push_back(tab);
+      s->bytes += n * 5 * sizeof(double2);
+      SD_TIMED_BEGIN(ctx, "k_orbit_table");
+      k_orbit_table<<<grid_for(n, 128), 128, 0, ctx->stream>>>(s->svs, nsv, t0, (int64_t)n, (double2 *)tab);
+      SD_LAUNCHED(ctx);
+      s->orb.tab = (const double2 *)tab;
+      s->orb.tab_t0 = t0;
+      s->orb.tab_n = (int64_t)n;
+    }
   }
   SD_TRY(sync(ctx));
   *out = s.release();

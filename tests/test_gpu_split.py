@@ -128,4 +128,10 @@ def test_split_zero_clipped_sigma0(ctx, resampling):
     sc.config.precision = SPLIT
     gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx,
                                 return_times=True)
-    _check(gpu, ref, ref_t, sc.scene.sub_swaths[0].azimuth_time_interval_s)
+    rep = compare_geocoded(gpu, ref, gpu.azimuth_time_us, ref_t, sc.scene.sub_swaths[0].azimuth_time_interval_s)
+    cap = max(1, int(FLIP_CAP * rep["compared_px"]))
+    assert rep["nan_pattern_equal"] and rep["mask_equal"], rep
+    assert rep["time_mismatch_px"] <= cap, rep
+    # 35 % zeros make many values near-zero interpolations, ill-conditioned in
+    # relative terms for any implementation: judged against the noise floor
+    assert rep["sigma_floor_over_1e-4_px"] <= cap, rep
