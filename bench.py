@@ -1,22 +1,30 @@
 #!/usr/bin/env python
-"""Benchmark: geocoded pixels per second of the full Sentinel-1 IW pipeline.
+"""Benchmark: geocoded pixels per second of SARdine's hot path on one B200.
 
-Workload (one step): 3 sub-swaths x 9 bursts x 1500 lines x 21000 samples of
-CInt16 SLC -> sigma0 calibration with NESZ, TOPS midpoint deburst and IW
-merge (one fused pass) -> backward Range-Doppler terrain correction onto a
-25000 x 20000 UTM 10 m grid with a 10 m projected DEM (fBm 0-3000 m),
-bicubic resampling, gamma0 flattening, LIA and shadow/layover mask, FP64
-geometry.  Inputs are seeded synthetic data of that shape (no real S1 data
-exists here).  All inputs exceed the 126 MB L2 (SLC 3.4 GB, DEM 2 GB).
+Default workload (config 5, served geocoding): 8 Sentinel-1 IW scenes of
+config-2 shape (3 sub-swaths x 9 bursts x 1500 x 21000 CInt16, calibrated,
+debursted and merged on the device, then resident in HBM with their 10 m UTM
+DEM and orbit) receive Poisson streams of tile requests (sides 256-2048
+log-uniform, random scene, bounding box, resampler and speckle filter, split
+precision) at 100, 500 and 2000 req/s.  A continuous-batching loop admits
+them by HBM budget into two overlapping slots.  `value` = geocoded output
+pixels per second of device time at the highest rate; p50/p99 request
+latency per rate; the plain per-request FP64 path on the same GPU beside it.
+
+Other workloads: --config c2 (one full IW scene per step: fused
+calibration+deburst+merge then terrain correction onto 25000 x 20000 UTM
+10 m, bicubic, flatten, LIA, FP64), c3 (c2 with lanczos3 in split
+precision), c4 (64 uneven tiles over 8 config-1-shape scenes per step,
+one persistent launch per stage replayed from a CUDA graph), c1 (plain
+terrain correction of the config-1 scene).  Inputs are seeded synthetic
+data of those shapes (no real S1 data exists here) and exceed the 126 MB L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config c2|c1]
+                    [--config c5|c2|c3|c4|c1]
 
-Prints one JSON line (rank 0).  `value` = output-grid pixels of all ranks /
-max-over-ranks device time of the K timed steps, inputs resident in HBM.
-`e2e` = the same metric through the public API with pinned host buffers,
-host<->device copies inside the timed region.  Under torchrun (N > 1) every
-rank processes its own scene (weak scaling, no data-path collective).
+Prints one JSON line (rank 0).  Under torchrun (N > 1) every rank serves
+its own scenes / processes its own scene (weak scaling, no data-path
+collective); times are the max over ranks.
 """
 from __future__ import annotations
 
@@ -562,6 +570,36 @@ def run_c4(args):
     ctx.close()
 
 
+def _tile_roofline(sd, tiles, ctx, reqs):
+    """Per-stage CUDA-event times of one batch of `reqs` on `ctx` (timing
+    replaces graph replay for that batch): the geocoding stage against the
+    measured FP64 peak, the speckle/crop stage against measured HBM."""
+    ctx.set_timing(True)
+    res = tiles.tc_tiles(reqs, ctx)
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    px = sum(r.rows * r.cols for r in reqs)
+    hist = np.sum([r.newton_iter_histogram for r in res], axis=0)
+    n_it = n_iter_mean(hist)
+    tc_ms = sum(v[0] for k, v in kt.items() if k.startswith(("k_main", "k_scan", "k_select", "k_row")))
+    sp_ms = kt.get("k_speckle_tiles", (0.0, 0))[0]
+    fp64 = ctypes_fp64_peak(ctx)
+    hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    tf = TC_FLOPS(n_it) * px / (tc_ms / 1e3) / 1e12 if tc_ms else None
+    gbs = 9.0 * px / (sp_ms / 1e3) / 1e9 if sp_ms else None
+    total = sum(v[0] for v in kt.values()) or 1.0
+    roof = {"bound": "fp64", "kernel": "tile geocoding (" + "+".join(sorted(k for k in kt if k.startswith(("k_main", "k_scan", "k_select", "k_row")))) + ")",
+            "achieved": tf, "peak": fp64, "unit": "TFLOP/s", "frac": tf / fp64 if (tf and fp64) else None,
+            "traffic": None, "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
+            "batch": f"{len(reqs)} tiles, {px} px",
+            "speckle_stage": {"kernel": "k_speckle_tiles", "bound": "hbm", "achieved": gbs, "peak": hbm,
+                              "unit": "GB/s", "frac": gbs / hbm if gbs else None, "bytes_per_px": 9.0,
+                              "ms": sp_ms}}
+    kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total, 4)}
+               for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
+    return roof, kernels
+
+
 def _tiles_cpu_baseline(scenes, reqs, budget_s=12.0):
     """The oracle (C++ restatement) on the host cores: geocode + speckle of
     the smallest tiles of the batch until ~budget_s of work."""
@@ -570,6 +608,9 @@ def _tiles_cpu_baseline(scenes, reqs, budget_s=12.0):
     threads = os.cpu_count()
     oracle.set_threads(threads)
     by_req = sorted(range(len(reqs)), key=lambda i: reqs[i].rows * reqs[i].cols)
+    # tiles of one scene only (a host copy of a config-2-shape scene is 6 GB)
+    first = reqs[by_req[0]].scene
+    by_req = [i for i in by_req if reqs[i].scene is first]
     host = {}
     px, t = 0, 0.0
     done = 0
@@ -578,10 +619,13 @@ def _tiles_cpu_baseline(scenes, reqs, budget_s=12.0):
         s = next(x for x in scenes if x["rs"] is r.scene)
         key = id(s)
         if key not in host:
-            m, sc = s["sc"].merged, s["sc"]
-            merged = sd.MergedSigma0(s["sig"].cpu().numpy(), m.lines, m.samples, m.near_slant_range_time_s,
+            sc = s["sc"]
+            m = s.get("merged") or sc.merged
+            sig = s["sig"] if "sig" in s else m.data
+            nz = s["nesz"] if "nesz" in s else m.nesz
+            merged = sd.MergedSigma0(sig.cpu().numpy(), m.lines, m.samples, m.near_slant_range_time_s,
                                      m.range_pixel_spacing_s, m.range_pixel_spacing_m, 0, 0,
-                                     s["nesz"].cpu().numpy(), m.azimuth_start_time_us)
+                                     nz.cpu().numpy() if nz is not None else None, m.azimuth_start_time_us)
             dem = sd.DemGrid(sc.dem.data.cpu().numpy() if hasattr(sc.dem.data, "cpu") else sc.dem.data,
                              sc.dem.origin_y, sc.dem.origin_x, sc.dem.pixel_size, sc.dem.kind,
                              sc.dem.utm_zone, sc.dem.utm_south)
@@ -600,7 +644,8 @@ def _tiles_cpu_baseline(scenes, reqs, budget_s=12.0):
         if t > budget_s:
             break
     return {"value": px / t, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"oracle geocode+speckle of the {done} smallest of {len(reqs)} tiles ({px} px, {t:.1f} s)"}
+            "sample": (f"oracle geocode+speckle of the {done} smallest tiles of one scene among {len(reqs)} "
+                       f"requests ({px} px, {t:.1f} s)")}
 
 
 # ── config 5: served geocoding ──────────────────────────────────────────────
@@ -739,6 +784,8 @@ def run_c5(args):
     bsum = latency_summary(_serve(base, breqs, barr))
     acc = _split_vs_fp64(sd, tiles, server.slots[0].ctx, scenes, rng)
     base.close()
+    roofline, kernels = _tile_roofline(sd, tiles, server.slots[0].ctx, sample)
+    cpu = _tiles_cpu_baseline(scenes, sample) if (args.cpu_baseline and world == 1) else None
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -758,6 +805,7 @@ def run_c5(args):
             "served_by_rate": by_rate,
             "per_request_fp64": bsum,
             "accuracy_split_vs_fp64": acc,
+            "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
             "gpu_launches": gpu_launches, "clocks": clk_summary,
             "e2e": {"value": world * esum["px"] / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(d2h[0] / max(1, args.steps)),
@@ -839,6 +887,75 @@ def _finish_dist(dist):
         dist.destroy_process_group()
 
 
+def run_reference_tiles(args):
+    """Reference arm for config 5: the oracle port geocodes (and filters) a
+    bounded sample of the same request stream per step, on the host cores,
+    from one config-2-shape scene it prepared itself (deburst, calibration,
+    merge on the CPU)."""
+    import oracle
+    import sardine_b200 as sd
+    from sardine_b200 import synth, tiles
+    threads = os.cpu_count()
+    oracle.set_threads(threads)
+    dev = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            dev = "cuda"
+    except Exception:
+        pass
+    sc = synth.config2_scene(seed=200, device=dev)   # synthetic inputs only
+    swaths_h = [type(s)(s.id, s.slc.cpu().numpy() if dev else s.slc, s.sw, s.bursts, s.cal, s.noise)
+                for s in sc.swaths]
+    sc.swaths = None
+    inputs = []
+    for s in swaths_h:
+        deb = oracle.deburst_subswath(s.slc, s.sw, s.bursts)
+        sig = oracle.apply_calibration(deb, s.cal, s.noise, s.bursts[0].first_line)
+        inputs.append(sd.SwathInput(sig, s.sw, s.bursts[0].azimuth_time_us))
+    merged = oracle.merge_subswaths(inputs)[0]
+    del inputs, swaths_h
+    dem = sd.DemGrid(sc.dem.data.cpu().numpy() if dev else sc.dem.data, sc.dem.origin_y, sc.dem.origin_x,
+                     sc.dem.pixel_size, sc.dem.kind, sc.dem.utm_zone, sc.dem.utm_south)
+    rc, g = oracle.tc_output_grid(sc.scene, sc.config)
+    fake = type("S", (), {})()  # request geometry only; the oracle reads the host scene
+    scenes = [{"rs": fake, "cfg": sc.config, "info": g}]
+    rng = np.random.default_rng(5)
+    per_step, px_all, t_all = [], 0, 0.0
+    for i in range(args.warmup + args.steps):
+        reqs = _c5_requests(sd, scenes, rng, 16, sd.Precision.FP64)
+        reqs = sorted(reqs, key=lambda r: r.rows * r.cols)[:4]   # bounded sample per step
+        px, t = 0, 0.0
+        for r in reqs:
+            h = r.halo()
+            t0 = time.perf_counter()
+            out = oracle.terrain_correction_grid(merged, sc.scene, dem, sc.grids, r.config,
+                                                 r.origin_x - h * r.config.pixel_spacing_deg,
+                                                 r.origin_y + h * r.config.pixel_spacing_deg,
+                                                 r.rows + 2 * h, r.cols + 2 * h)
+            if r.speckle is not None:
+                oracle.apply_speckle_filter(out.data, r.cols + 2 * h, r.rows + 2 * h, r.speckle)
+            t += time.perf_counter() - t0
+            px += r.rows * r.cols
+        if i >= args.warmup:
+            per_step.append(t)
+            px_all += px
+            t_all += t
+    value = px_all / t_all
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(per_step)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded config-2-shape IW scene)", "config": {"workload": args.config},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": (f"oracle port, {threads} threads: geocode + speckle of the 4 smallest of 16 "
+                                    "random tile requests per step from one resident scene")},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference (Rust) unbuildable here: no cargo/rustc and crates not vendored; "
+                "the C++ oracle port stands in",
+    }), flush=True)
+
+
 def run_reference(args):
     """Reference arm: the reference is Rust and cannot be built here, so the
     oracle port (its C++ restatement) is timed on the host cores, each step a
@@ -846,6 +963,8 @@ def run_reference(args):
     rank, world, _ = _rank_env()
     if rank != 0:
         return
+    if args.config in ("c4", "c5"):
+        return run_reference_tiles(args)
     import oracle
     import sardine_b200 as sd
     from sardine_b200 import synth
@@ -919,7 +1038,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c3", "c4", "c5"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4"])
     ap.add_argument("--rates", default="100,500,2000", help="config5 request rates (req/s); value at the last")
     ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
     ap.add_argument("--scenes", type=int, default=8, help="config5 resident scenes")
