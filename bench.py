@@ -785,7 +785,10 @@ def run_c5(args):
     acc = _split_vs_fp64(sd, tiles, server.slots[0].ctx, scenes, rng)
     base.close()
     roofline, kernels = _tile_roofline(sd, tiles, server.slots[0].ctx, sample)
-    cpu = _tiles_cpu_baseline(scenes, sample) if (args.cpu_baseline and world == 1) else None
+    cpu = None
+    if args.cpu_baseline and world == 1:  # tiles of one scene (one 6 GB host copy)
+        cpu = _tiles_cpu_baseline(scenes, _c5_requests(sd, scenes[:1], np.random.default_rng(57), 96,
+                                                       sd.Precision.FP64))
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

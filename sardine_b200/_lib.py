@@ -12,7 +12,9 @@ import threading
 from . import _abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libsardine_b200.so")
+# SARDINE_B200_LIB selects another build of the same library (a variant
+# compiled with different switches); the default is the in-tree build
+LIB_PATH = os.environ.get("SARDINE_B200_LIB", os.path.join(_HERE, "libsardine_b200.so"))
 _lib = None
 _lock = threading.Lock()
 

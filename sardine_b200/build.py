@@ -24,7 +24,21 @@ FLAGS = [
 ]
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
+def build(verbose: bool = False, force: bool = False, extra_flags=(), out: str = None) -> str:
+    """Compiles the library (incrementally); `extra_flags` and `out` build a
+    variant (e.g. -D switches) into another file with its own objects."""
+    global OUT
+    if out is not None:
+        saved = OUT
+        OUT = out
+        try:
+            return _build(verbose, force, list(extra_flags), os.path.join(os.path.dirname(out), "_build"))
+        finally:
+            OUT = saved
+    return _build(verbose, force, list(extra_flags), os.path.join(HERE, "_build"))
+
+
+def _build(verbose: bool, force: bool, extra_flags, objdir: str) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     deps.append(os.path.join(HERE, "..", "include", "sardine_b200.h"))
@@ -33,10 +47,9 @@ def build(verbose: bool = False, force: bool = False) -> str:
         if all(os.path.getmtime(d) <= t_out for d in deps):
             return OUT
     # every translation unit compiles in its own nvcc process, then one link
-    objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = [os.path.join(objdir, os.path.basename(s)[:-3] + ".o") for s in srcs]
-    cflags = [f for f in FLAGS if f not in ("-shared", "-lcudart")]
+    cflags = [f for f in FLAGS if f not in ("-shared", "-lcudart")] + extra_flags
     headers = [d for d in deps if not d.endswith(".cu")]
     t_hdr = max(os.path.getmtime(h) for h in headers)
     procs = []

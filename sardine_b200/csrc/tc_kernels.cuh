@@ -39,6 +39,10 @@
 
 #include "tiles.cuh"
 
+#ifndef SD_FACET_ABSOLUTE
+#define SD_FACET_ABSOLUTE 0
+#endif
+
 #include "geo.cuh"
 #include "runtime.cuh"
 
@@ -675,6 +679,8 @@ __device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
   }
   f.ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
   if (!f.ok) return f;
+#if SD_FACET_ABSOLUTE
+  // the reference's form: four absolute ECEF points, then their differences
   double se, ce, sw, cw, sn, cn, ss, cs;
   sincos_add(g.slo, g.clo, deg2rad_ecef(lon_e) - g.lo, &se, &ce);
   sincos_add(g.slo, g.clo, deg2rad_ecef(lon_w) - g.lo, &sw, &cw);
@@ -685,6 +691,33 @@ __device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
   V3 pn = ecef_sc(sn, cn, g.slo, g.clo, (double)hn);
   V3 ps = ecef_sc(ss, cs, g.slo, g.clo, (double)hs);
   f.normal = cross3(sub3(pe, pw), sub3(pn, ps));
+#else
+  // The same two chords pe - pw and pn - ps, expanded about the centre in
+  // the angular steps a, b (east, west) and c, d (north, south), ~1.6e-6
+  // rad, through second order (the third-order terms are ~1e-11 m on ~20 m
+  // chords).  The reference subtracts absolute ECEF coordinates of ~6.4e6 m,
+  // which already costs it ~3e-11 of relative precision, so the two forms
+  // agree to the reference's own rounding; this one needs no square root or
+  // division per neighbour.
+  const double a = deg2rad_ecef(lon_e) - g.lo, b = g.lo - deg2rad_ecef(lon_w);
+  const double c = deg2rad_ecef(lat_n) - g.la, d = g.la - deg2rad_ecef(lat_s);
+  const double sp = g.sla, cp = g.cla, sl = g.slo, cl = g.clo;
+  const double den = 1.0 - WGS84_E2 * sp * sp;
+  const double N = WGS84_A / sqrt(den);
+  const double dN = N * WGS84_E2 * sp * cp / den;
+  const double B = N * (1.0 - WGS84_E2), dB = dN * (1.0 - WGS84_E2);
+  const double Hn = (double)hn, Hs = (double)hs, He = (double)he, Hw = (double)hw;
+  // east-west: (N + h) cos(phi) (cos, sin)(lam +- step), (B + h) sin(phi)
+  const double dh = He - Hw;
+  const double q = (N + He) * a + (N + Hw) * b;
+  const double r2 = 0.5 * ((N + He) * a * a - (N + Hw) * b * b);
+  const V3 e = {cp * (cl * dh - sl * q - cl * r2), cp * (sl * dh + cl * q - sl * r2), sp * dh};
+  // north-south: G(phi) = N cos(phi), Z(phi) = B sin(phi) and the heights
+  const double dv = Hn - Hs, h2 = 0.5 * (Hn * c * c - Hs * d * d);
+  const double An = cp * (dv + dN * (c + d)) - sp * ((N + Hn) * c + (N + Hs) * d) - cp * h2;
+  const double Zn = sp * (dv + dB * (c + d)) + cp * ((B + Hn) * c + (B + Hs) * d) - sp * h2;
+  f.normal = cross3(e, V3{cl * An, sl * An, Zn});
+#endif
   f.area = norm3(f.normal);
   return f;
 }
@@ -938,7 +971,13 @@ struct Slot {  // shared-memory record exchanged with the right-hand neighbour
   Ent e[2];
 };
 
-constexpr int MAIN_THREADS = 128;
+#ifndef SD_MAIN_THREADS
+#define SD_MAIN_THREADS 128
+#endif
+#ifndef SD_MAIN_MINB
+#define SD_MAIN_MINB 4  // blocks per SM the register budget is cut for
+#endif
+constexpr int MAIN_THREADS = SD_MAIN_THREADS;
 constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
 
 // ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
@@ -1110,7 +1149,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
 // Single job: the job record is a kernel parameter (constant-bank operands)
 // and the grid covers its rows x bpr items.
 template <int KERNEL, bool SPLIT>
-__global__ void __launch_bounds__(MAIN_THREADS, 4) k_main(TcDev p) {
+__global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main(TcDev p) {
   __shared__ Slot slot[MAIN_THREADS];
   main_item<KERNEL, SPLIT>(p, blockIdx.x / p.bpr, blockIdx.x % p.bpr, slot);
 }
@@ -1118,7 +1157,7 @@ __global__ void __launch_bounds__(MAIN_THREADS, 4) k_main(TcDev p) {
 // Tile batches: persistent CTAs over the work table; the current job's
 // record is staged in shared memory.
 template <int KERNEL, bool SPLIT>
-__global__ void __launch_bounds__(MAIN_THREADS, 4) k_main_batch(const TcWork *__restrict__ wp) {
+__global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const TcWork *__restrict__ wp) {
   __shared__ Slot slot[MAIN_THREADS];
   __shared__ __align__(16) unsigned char s_job[sizeof(TcDev)];
   __shared__ int s_j;
