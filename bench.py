@@ -742,7 +742,7 @@ def run_c5(args):
         by_rate[str(int(rate))] = summ
         if rate == rates[-1]:
             ms = _max_over_ranks(dist, e0.elapsed_time(e1))
-            value = world * summ["px"] / (ms / 1e3)
+            value = _sum_over_ranks(dist, summ["px"]) / (ms / 1e3)
             gpu_launches = sum(s.ctx.launches for s in server.slots) - l0
             clk_summary = clk.summary()
             head = summ
@@ -774,6 +774,8 @@ def run_c5(args):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     esum = latency_summary(et)
+    e2e_s = _max_over_ranks(dist, e2e_s)
+    e2e_px = _sum_over_ranks(dist, esum["px"])
     e2e_server.close()
     # plain per-request FP64 path on the same GPU: one tile per launch, no graphs
     base = GeocodingServer(local, hbm_budget=4 << 30, slots=1, max_batch=1, graphs=False)
@@ -810,7 +812,7 @@ def run_c5(args):
             "accuracy_split_vs_fp64": acc,
             "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
             "gpu_launches": gpu_launches, "clocks": clk_summary,
-            "e2e": {"value": world * esum["px"] / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
+            "e2e": {"value": e2e_px / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(d2h[0] / max(1, args.steps)),
                     "p50_ms": esum["p50_ms"], "p99_ms": esum["p99_ms"],
                     "api": "GeocodingServer with every result copied to pinned host memory on completion "
@@ -881,6 +883,15 @@ def _max_over_ranks(dist, ms):
     import torch
     t = torch.tensor([ms], device="cuda")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _sum_over_ranks(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 

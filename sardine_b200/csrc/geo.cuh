@@ -311,6 +311,7 @@ struct DemView {
   const float *data;
   uint64_t width, height;
   double origin_y, origin_x, pixel_size;
+  double inv_ps;  // 1 / pixel_size: fractional indices by multiplication (within an ulp of the quotient)
   int32_t kind;
   Utm utm;
 };
@@ -368,12 +369,15 @@ SD_HD bool dem_sample(const DemView &d, double row_f, double col_f, float *h) {
   return true;
 }
 
+// The reference divides by the pixel size; the product with its reciprocal
+// differs by at most an ulp of the fractional index (1e-16 px), far below
+// anything the bilinear weights or the floor can resolve.
 SD_HD bool dem_at_xy(const DemView &d, double x, double y, float *h) {
-  return dem_sample(d, (d.origin_y - y) / d.pixel_size, (x - d.origin_x) / d.pixel_size, h);
+  return dem_sample(d, (d.origin_y - y) * d.inv_ps, (x - d.origin_x) * d.inv_ps, h);
 }
 SD_HD bool dem_at_lonlat(const DemView &d, double lon_deg, double lat_deg, float *h) {
   double lon_norm = lon_deg >= 180.0 ? lon_deg - 360.0 : lon_deg;
-  return dem_sample(d, (d.origin_y - lat_deg) / d.pixel_size, (lon_norm - d.origin_x) / d.pixel_size, h);
+  return dem_sample(d, (d.origin_y - lat_deg) * d.inv_ps, (lon_norm - d.origin_x) * d.inv_ps, h);
 }
 
 // ── geoid (geoid.rs:220-251) ───────────────────────────────────────────────

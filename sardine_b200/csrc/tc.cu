@@ -212,6 +212,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   p.dem.origin_y = dem->origin_y;
   p.dem.origin_x = dem->origin_x;
   p.dem.pixel_size = dem->pixel_size;
+  p.dem.inv_ps = 1.0 / dem->pixel_size;
   p.dem.kind = dem->kind;
   if (dem->kind == SD_DEM_PROJECTED_UTM) {
     if (dem->utm_zone < 1 || dem->utm_zone > 60)

@@ -972,10 +972,10 @@ struct Slot {  // shared-memory record exchanged with the right-hand neighbour
 };
 
 #ifndef SD_MAIN_THREADS
-#define SD_MAIN_THREADS 128
+#define SD_MAIN_THREADS 256  // 255 pixels + the left neighbour per block
 #endif
 #ifndef SD_MAIN_MINB
-#define SD_MAIN_MINB 4  // blocks per SM the register budget is cut for
+#define SD_MAIN_MINB 2  // blocks per SM the register budget is cut for (128 regs)
 #endif
 constexpr int MAIN_THREADS = SD_MAIN_THREADS;
 constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
@@ -1072,11 +1072,16 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         int64_t t = L.fb + k;
         uint32_t code = 0xFF;
         for (int it = 0; it < p.max_iter; ++it) {
+          // a member of this pixel's F converges by definition (|delta| < tol
+          // was evaluated there with the same state and arithmetic)
+          const int64_t mf = t - fb;
+          if ((mf == 0 || mf == 1) && ((fmask >> mf) & 1)) {
+            code = (uint32_t)mf | ((uint32_t)min(it + 1, 15) << 4);
+            break;
+          }
           Ent e;
           bool have = true;
           if (t == L.fb + k) e = L.e[k];
-          else if (t == fb && (fmask & 1)) e = e0;
-          else if (t == fb + 1 && (fmask & 2)) e = e1;
           else have = ent_at(p.orb, t, &e) == ORB_OK;
           if (!have) break;  // orbit error: the walk redoes it
           double d;

@@ -213,6 +213,7 @@ extern "C" int sd_scene_create(sd_ctx *ctx, const sd_radar_image *image, const s
   s->dem.origin_y = dem->origin_y;
   s->dem.origin_x = dem->origin_x;
   s->dem.pixel_size = dem->pixel_size;
+  s->dem.inv_ps = 1.0 / dem->pixel_size;
   s->dem.kind = dem->kind;
   if (dem->kind == SD_DEM_PROJECTED_UTM) s->dem.utm = make_utm(dem->utm_zone, dem->utm_south != 0);
   if (geoid->kind == SD_GEOID_GRID) {
