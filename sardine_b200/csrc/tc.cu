@@ -259,6 +259,12 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
     p.alon = d_alon;
     p.alat = d_alat;
   }
+  float *d_hc;
+  float4 *d_hnb;
+  SD_TRY(scratch_t(ctx, "tc.hc", npx, &d_hc));
+  SD_TRY(scratch_t(ctx, "tc.hnb", npx, &d_hnb));
+  p.hc = d_hc;
+  p.hnb = d_hnb;
   SD_TRY(scratch_t(ctx, "tc.rec", npx, &p.rec));
   SD_TRY(scratch_t(ctx, "tc.cc", npx, &p.cc));
   SD_TRY(scratch_t(ctx, "tc.sel", npx, &p.sel));

@@ -153,6 +153,8 @@ struct TcDev {
   int fast;                    // tolerance allows the fixed-point-pair scheme
   int split;                   // SD_PRECISION_SPLIT
   uint64_t row0;               // grid row of the job's first row (row bands)
+  const float *hc;             // per pixel: DEM height of the centre (NaN: none), from k_heights
+  const float4 *hnb;           // per pixel: heights of the E, W, N, S neighbours (NaN: facet missing)
 };
 
 // ── work table ──────────────────────────────────────────────────────────────
@@ -620,18 +622,23 @@ struct PixGeo {
 
 // DEM lookup of the centre (1529-1536), geoid (1545) and target ECEF (1546).
 // Returns false when the DEM has no finite height there.
-__device__ bool pixel_geo(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g) {
+// Centre of the pixel: lon/lat, the UTM local expansion for a projected DEM,
+// and the DEM height; false when there is no finite height.
+__device__ bool pixel_height(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g, float *hf) {
   pixel_lonlat(p, r, c, &g->lon, &g->lat);
-  float hf;
   bool ok;
   if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
     const Utm &u = p.dem.utm;
     utm_local(u, g->lat, utm_taup(u, g->lat), utm_lam(u, g->lon), &g->loc);
-    ok = dem_at_xy(p.dem, g->loc.x, g->loc.y, &hf);
+    ok = dem_at_xy(p.dem, g->loc.x, g->loc.y, hf);
   } else {
-    ok = dem_at_lonlat(p.dem, g->lon, g->lat, &hf);
+    ok = dem_at_lonlat(p.dem, g->lon, g->lat, hf);
   }
-  if (!ok || !isfinite(hf)) return false;
+  return ok && isfinite(*hf);
+}
+
+// Geoid, sines and cosines and the target ECEF from the centre height.
+__device__ __forceinline__ void pixel_ecef(const TcDev &p, PixGeo *g, float hf) {
   double h_ell = (double)hf + geoid_undulation(p.geoid, g->lat, g->lon);
   g->la = deg2rad_ecef(g->lat);
   g->lo = deg2rad_ecef(g->lon);
@@ -640,6 +647,12 @@ __device__ bool pixel_geo(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g) {
   g->slo = sin(g->lo);
   g->clo = cos(g->lo);
   g->P = ecef_sc(g->sla, g->cla, g->slo, g->clo, h_ell);
+}
+
+__device__ bool pixel_geo(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g) {
+  float hf;
+  if (!pixel_height(p, r, c, g, &hf)) return false;
+  pixel_ecef(p, g, hf);
   return true;
 }
 
@@ -653,8 +666,9 @@ struct Facet {
   double area;
 };
 
-__device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
-  Facet f{};
+// Heights of the east, west, north and south neighbours (1642-1675: DEM
+// heights without the geoid); false when any lies outside the DEM or on a void.
+__device__ bool facet_heights(const TcDev &p, const PixGeo &g, float h[4]) {
   const double sd = p.step_deg;
   const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
   float he, hw, hn, hs;
@@ -677,8 +691,17 @@ __device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
     ok = dem_at_lonlat(p.dem, g.lon, lat_n, &hn) && ok;
     ok = dem_at_lonlat(p.dem, g.lon, lat_s, &hs) && ok;
   }
-  f.ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
-  if (!f.ok) return f;
+  h[0] = he, h[1] = hw, h[2] = hn, h[3] = hs;
+  return ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
+}
+
+// Normal and area of the facet from the four neighbour heights.
+__device__ Facet facet_from(const TcDev &p, const PixGeo &g, const float h[4]) {
+  Facet f{};
+  f.ok = true;
+  const float he = h[0], hw = h[1], hn = h[2], hs = h[3];
+  const double sd = p.step_deg;
+  const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
 #if SD_FACET_ABSOLUTE
   // the reference's form: four absolute ECEF points, then their differences
   double se, ce, sw, cw, sn, cn, ss, cs;
@@ -720,6 +743,12 @@ __device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
 #endif
   f.area = norm3(f.normal);
   return f;
+}
+
+__device__ Facet pixel_facet(const TcDev &p, const PixGeo &g) {
+  float h[4];
+  if (!facet_heights(p, g, h)) return Facet{};
+  return facet_from(p, g, h);
 }
 
 // Output of one pixel for one converged azimuth time (1585-1739): sigma0 /
@@ -810,32 +839,12 @@ struct FacetF {
   float nx, ny, nz, area;
 };
 
-__device__ FacetF pixel_facet_f(const TcDev &p, const PixGeo &g) {
+__device__ FacetF facetf_from(const TcDev &p, const PixGeo &g, const float h[4]) {
   FacetF f{};
+  f.ok = true;
+  const float he = h[0], hw = h[1], hn = h[2], hs = h[3];
   const double sd = p.step_deg;
   const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
-  float he, hw, hn, hs;
-  bool ok;
-  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
-    const Utm &u = p.dem.utm;
-    const double k = kPi / 180.0;
-    double x, y;
-    utm_local_step(u, g.loc, 0.0, (lon_e - g.lon) * k, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &he);
-    utm_local_step(u, g.loc, 0.0, (lon_w - g.lon) * k, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &hw) && ok;
-    utm_local_step(u, g.loc, (lat_n - g.lat) * k, 0.0, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &hn) && ok;
-    utm_local_step(u, g.loc, (lat_s - g.lat) * k, 0.0, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &hs) && ok;
-  } else {
-    ok = dem_at_lonlat(p.dem, lon_e, g.lat, &he);
-    ok = dem_at_lonlat(p.dem, lon_w, g.lat, &hw) && ok;
-    ok = dem_at_lonlat(p.dem, g.lon, lat_n, &hn) && ok;
-    ok = dem_at_lonlat(p.dem, g.lon, lat_s, &hs) && ok;
-  }
-  f.ok = ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
-  if (!f.ok) return f;
   const float a = (float)(deg2rad_ecef(lon_e) - g.lo), b = (float)(g.lo - deg2rad_ecef(lon_w));
   const float c = (float)(deg2rad_ecef(lat_n) - g.la), d = (float)(g.la - deg2rad_ecef(lat_s));
   const float sp = (float)g.sla, cp = (float)g.cla, sl = (float)g.slo, cl = (float)g.clo;
@@ -856,6 +865,12 @@ __device__ FacetF pixel_facet_f(const TcDev &p, const PixGeo &g) {
   f.nz = ex * ny - ey * nx;
   f.area = sqrtf(f.nx * f.nx + f.ny * f.ny + f.nz * f.nz);
   return f;
+}
+
+__device__ FacetF pixel_facet_f(const TcDev &p, const PixGeo &g) {
+  float h[4];
+  if (!facet_heights(p, g, h)) return FacetF{};
+  return facetf_from(p, g, h);
 }
 
 // cand_post in split precision; *redo is set when a mask decision falls
@@ -903,23 +918,32 @@ __device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g
 
 // One candidate's output from scratch (exact-path pixels, and split-precision
 // candidates whose mask FP32 cannot settle).
+// h4: the neighbour heights when already known (NaN when the facet is
+// missing), else null to look them up.
+__device__ __forceinline__ bool heights_ok(const float *h4) {
+  return isfinite(h4[0]) && isfinite(h4[1]) && isfinite(h4[2]) && isfinite(h4[3]);
+}
+
 template <int KERNEL>
-__device__ CandOut cand_fp64(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area) {
+__device__ CandOut cand_fp64(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area,
+                             const float *h4) {
   CandPre pre = cand_pre<KERNEL, false>(p, g.P, S, t);
   Facet f{};
-  if (pre.inside && p.need_geom) f = pixel_facet(p, g);
+  if (pre.inside && p.need_geom) f = h4 ? (heights_ok(h4) ? facet_from(p, g, h4) : Facet{}) : pixel_facet(p, g);
   return cand_post(p, pre, g.P, S, f, flat_area);
 }
 
 template <int KERNEL, bool SPLIT>
-__device__ CandOut cand_full(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area) {
-  if (!SPLIT) return cand_fp64<KERNEL>(p, g, S, t, flat_area);
+__device__ CandOut cand_full(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area,
+                             const float *h4) {
+  if (!SPLIT) return cand_fp64<KERNEL>(p, g, S, t, flat_area, h4);
   CandPre pre = cand_pre<KERNEL, true>(p, g.P, S, t);
   FacetF f{};
-  if (pre.inside && p.need_geom) f = pixel_facet_f(p, g);
+  if (pre.inside && p.need_geom)
+    f = h4 ? (heights_ok(h4) ? facetf_from(p, g, h4) : FacetF{}) : pixel_facet_f(p, g);
   bool redo;
   CandOut o = cand_post_f(p, pre, g, S, f, (float)flat_area, &redo);
-  return redo ? cand_fp64<KERNEL>(p, g, S, t, flat_area) : o;
+  return redo ? cand_fp64<KERNEL>(p, g, S, t, flat_area, h4) : o;
 }
 
 // ── per-pixel stores ─────────────────────────────────────────────────────────
@@ -981,6 +1005,37 @@ constexpr int MAIN_THREADS = SD_MAIN_THREADS;
 constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
 
 // ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
+// ── k_heights: the DEM side of every pixel ahead of k_main ─────────────────
+// Per pixel: the centre height (DEM lookup of 1529-1536, NaN where the DEM
+// has none) and, where the facet is needed, the four neighbour heights
+// (NaN when any is missing).  These are the latency-bound gathers and
+// projections; done here at low register pressure they overlap well, and
+// k_main reads 20 B per pixel instead.
+__global__ void __launch_bounds__(SEL_THREADS) k_heights(const TcWork *__restrict__ wp) {
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_SEL);
+  const uint64_t total = pre[w.n_jobs];
+  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    const int jb = find_job(pre, w.n_jobs, item);
+    const TcDev &p = w.jobs[jb];
+    if (!p.hc) continue;
+    const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
+    if (i >= p.rows * p.cols) continue;
+    const uint64_t r = i / p.cols, c = i % p.cols;
+    PixGeo g;
+    float hf;
+    const bool ok = pixel_height(p, r, c, &g, &hf);
+    float h[4] = {NAN, NAN, NAN, NAN};
+    if (ok && p.need_geom) {
+      g.lo = deg2rad_ecef(g.lon);
+      g.la = deg2rad_ecef(g.lat);
+      if (!facet_heights(p, g, h)) h[0] = h[1] = h[2] = h[3] = NAN;
+    }
+    ((float *)p.hc)[i] = ok ? hf : NAN;
+    ((float4 *)p.hnb)[i] = make_float4(h[0], h[1], h[2], h[3]);
+  }
+}
+
 // One k_main work item: MAIN_PIX pixels of row r starting at chunk * MAIN_PIX
 // (plus the left neighbour on thread 0).  Every thread of the block calls it.
 template <int KERNEL, bool SPLIT>
@@ -1003,8 +1058,16 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   const int64_t uw = __shfl_sync(0xffffffffu, predicted_time(p, rr, cq), 16);
   Ent ew;
   const bool ew_ok = fast && ent_at(p.orb, uw, &ew) == ORB_OK;
+  float h4[4] = {NAN, NAN, NAN, NAN};
   if (in_row && r < p.rows) {
-    geo_ok = pixel_geo(p, r, (uint64_t)c, &g);
+    if (p.hc) {  // heights from k_heights
+      pixel_lonlat(p, r, (uint64_t)c, &g.lon, &g.lat);
+      const float hf = __ldg(p.hc + i);
+      geo_ok = isfinite(hf);
+      if (geo_ok) pixel_ecef(p, &g, hf);
+    } else {
+      geo_ok = pixel_geo(p, r, (uint64_t)c, &g);
+    }
     if (geo_ok && fast) {
       // reference iteration from the shared state: one converged t*
       int64_t t = ew_ok ? uw : predicted_time(p, r, (uint64_t)c);
@@ -1117,7 +1180,15 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
     const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
     if constexpr (SPLIT) {
       FacetF f{};
-      if (need && p.need_geom) f = pixel_facet_f(p, g);
+      if (need && p.need_geom) {
+        if (p.hnb) {
+          const float4 q4 = __ldg(p.hnb + i);
+          h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
+          if (heights_ok(h4)) f = facetf_from(p, g, h4);
+        } else if (facet_heights(p, g, h4)) {
+          f = facetf_from(p, g, h4);
+        }
+      }
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const Ent &e = k == 0 ? e0 : e1;
@@ -1125,7 +1196,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         const V3 S{e.px, e.py, e.pz};
         bool redo;
         CandOut o = cand_post_f(p, pre[k], g, S, f, (float)flat_area, &redo);
-        if (redo) o = cand_fp64<KERNEL>(p, g, S, fb + k, flat_area);
+        if (redo) o = cand_fp64<KERNEL>(p, g, S, fb + k, flat_area, h4);
         rec.data[k] = o.data;
         rec.cos[k] = o.cos;
         rec.omask[k] = o.mask;
@@ -1133,7 +1204,15 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
       }
     } else {
       Facet f{};
-      if (need && p.need_geom) f = pixel_facet(p, g);
+      if (need && p.need_geom) {
+        if (p.hnb) {
+          const float4 q4 = __ldg(p.hnb + i);
+          h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
+          if (heights_ok(h4)) f = facet_from(p, g, h4);
+        } else {
+          f = pixel_facet(p, g);
+        }
+      }
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const Ent &e = k == 0 ? e0 : e1;
@@ -1234,7 +1313,7 @@ __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s,
     OrbitState os;
     double vsq;
     orbit_at(p.orb, z.t, &os, &vsq);
-    CandOut o = cand_full<KERNEL, SPLIT>(p, g, os.pos, z.t, p.need_geom ? p.row_flat[r] : 0.0);
+    CandOut o = cand_full<KERNEL, SPLIT>(p, g, os.pos, z.t, p.need_geom ? p.row_flat[r] : 0.0, nullptr);
     p.out[i] = o.data;
     if (p.compute_lia) {
       p.cos_lia[i] = o.cos;
@@ -1544,6 +1623,9 @@ int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
   SD_LAUNCHED(ctx);
   SD_TIMED_BEGIN(ctx, "k_row_model");
   k_row_model<<<persistent_grid(k_row_model, 128, 0, blocks_for(totals[WK_KNOT], 128)), 128, 0, st>>>(d_work);
+  SD_LAUNCHED(ctx);
+  SD_TIMED_BEGIN(ctx, "k_heights");
+  k_heights<<<persistent_grid(k_heights, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
   SD_LAUNCHED(ctx);
   return SD_OK;
 }

@@ -397,7 +397,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     return o;
   };
   struct Offs {
-    size_t guess, flat, knots, alon, alat, rec, cc, sel, hout[3], fin[3];
+    size_t guess, flat, knots, alon, alat, hc, hnb, rec, cc, sel, hout[3], fin[3];
   };
   std::vector<Offs> of(n);
   size_t ax_total = 0;
@@ -414,6 +414,8 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
       o.alat = take(p.rows * p.n_pts * 8);
       ax_total += p.n_pts;
     }
+    o.hc = take(npx * sizeof(float));
+    o.hnb = take(npx * sizeof(float4));
     o.rec = take(npx * sizeof(Rec));
     o.cc = take(npx * 4);
     o.sel = take(npx);
@@ -466,6 +468,8 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
       p.alon = (const double *)(arena + o.alon);
       p.alat = (const double *)(arena + o.alat);
     }
+    p.hc = (const float *)(arena + o.hc);
+    p.hnb = (const float4 *)(arena + o.hnb);
     p.rec = (Rec *)(arena + o.rec);
     p.cc = (uint32_t *)(arena + o.cc);
     p.sel = (uint8_t *)(arena + o.sel);

@@ -101,14 +101,14 @@ class TileRequest:
 
     def device_bytes(self) -> int:
         """Device scratch this tile needs inside a batch (admission budget):
-        per-pixel records (32 B), codes (4 B), selection (1 B) and halo'd
-        outputs (9 B) over the halo'd grid, plus per-row state and the final
-        rasters when they are staged."""
+        per-pixel heights (20 B), records (32 B), codes (4 B), selection (1 B)
+        and halo'd outputs (9 B) over the halo'd grid, plus per-row state and
+        the final rasters when they are staged."""
         h = self.halo()
         r, c = self.rows + 2 * h, self.cols + 2 * h
         anchors = min(256, c) + 1 if self.config.crs.kind != _abi.CRS_WGS84 else 0
         per_row = 8 + 8 + 17 * 8 + 16 * anchors
-        return r * c * (32 + 4 + 1 + 9) + r * per_row + self.rows * self.cols * 9 + 4096
+        return r * c * (20 + 32 + 4 + 1 + 9) + r * per_row + self.rows * self.cols * 9 + 8192
 
 
 def _tile_to_c(req: TileRequest, outs, anchors: int) -> _abi.Tile:
