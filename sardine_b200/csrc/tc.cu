@@ -258,6 +258,11 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
     p.ax = d_ax;
     p.alon = d_alon;
     p.alat = d_alat;
+    if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+      UtmLocal *d_aloc;
+      SD_TRY(scratch_t(ctx, "tc.aloc", p.rows * p.n_pts, &d_aloc));
+      p.aloc = d_aloc;
+    }
   }
   float *d_hc;
   float4 *d_hnb;

@@ -115,6 +115,7 @@ struct TcDev {
   const double *ax;   // n_pts
   const double *alon; // rows * n_pts
   const double *alat;
+  const UtmLocal *aloc; // rows * n_pts: DEM projection (UTM DEM) at every anchor, or null
   int n_anchors, n_pts;
   // LUT
   const double *lut_lat;
@@ -202,7 +203,21 @@ __device__ __forceinline__ double row_y(const TcDev &p, uint64_t r) {
 
 // Output pixel centre in lon/lat: direct for WGS84, project_row anchors for
 // UTM (output_crs.rs:383-415).
+// Pixel centre as in pixel_lonlat, plus the anchor segment g and the
+// position t in it (UTM grids only).
+__device__ void pixel_seg(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat, int *gs,
+                          double *ts);
+
 __device__ void pixel_lonlat(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat) {
+  int g;
+  double t;
+  pixel_seg(p, r, c, lon, lat, &g, &t);
+}
+
+__device__ void pixel_seg(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat, int *gs,
+                          double *ts) {
+  *gs = 0;
+  *ts = 0.0;
   if (!p.utm) {
     *lon = p.lon_west + ((double)c + 0.5) * p.sp;
     *lat = row_y(p, r);
@@ -225,6 +240,40 @@ __device__ void pixel_lonlat(const TcDev &p, uint64_t r, uint64_t c, double *lon
   double t = (x1 == x0) ? 0.0 : (x - x0) / (x1 - x0);
   *lon = lo[g] + t * (lo[g + 1] - lo[g]);
   *lat = la[g] + t * (la[g + 1] - la[g]);
+  *gs = g;
+  *ts = t;
+}
+
+// DEM-side projection of a pixel centre from its row's anchors (UTM grid on
+// a UTM DEM).  The centre is the linear interpolation of anchors g, g+1 in
+// lon/lat, so its projected position is a smooth function of t over the
+// ~1 km segment: a cubic Hermite through the anchors' projected points and
+// their derivatives along the segment (d/dt = dzeta/dw . (psi' dphi + i
+// dlam)) reproduces the exact projection to ~1e-11 m.  The local-expansion
+// terms used for the cardinal neighbours move by ~1e-4 relative over a
+// segment and are interpolated linearly (effect ~3e-8 m on a 10 m step).
+__device__ void dem_local_from_anchors(const TcDev &p, uint64_t r, int g, double t, UtmLocal *o) {
+  const UtmLocal &A = p.aloc[r * p.n_pts + g], &B = p.aloc[r * p.n_pts + g + 1];
+  const double *lo = p.alon + r * p.n_pts, *la = p.alat + r * p.n_pts;
+  const double k = kPi / 180.0;
+  const double dphi = (la[g + 1] - la[g]) * k, dlam = (lo[g + 1] - lo[g]) * k;
+  const double k0A = p.dem.utm.k0A;
+  // derivatives along the segment at both ends
+  const double aw = A.dpsi1 * dphi, bw = B.dpsi1 * dphi;
+  const double ax_ = k0A * (A.zw_re * dlam + A.zw_im * aw), ay_ = k0A * (A.zw_re * aw - A.zw_im * dlam);
+  const double bx_ = k0A * (B.zw_re * dlam + B.zw_im * bw), by_ = k0A * (B.zw_re * bw - B.zw_im * dlam);
+  const double t2 = t * t, t3 = t2 * t;
+  const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
+  const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+  o->x = h00 * A.x + h10 * ax_ + h01 * B.x + h11 * bx_;
+  o->y = h00 * A.y + h10 * ay_ + h01 * B.y + h11 * by_;
+  const double u = 1.0 - t;
+  o->zw_re = u * A.zw_re + t * B.zw_re;
+  o->zw_im = u * A.zw_im + t * B.zw_im;
+  o->zww_re = u * A.zww_re + t * B.zww_re;
+  o->zww_im = u * A.zww_im + t * B.zww_im;
+  o->dpsi1 = u * A.dpsi1 + t * B.dpsi1;
+  o->dpsi2 = u * A.dpsi2 + t * B.dpsi2;
 }
 
 // guess_azimuth_time (terrain_correction.rs:1107-1137)
@@ -280,6 +329,10 @@ __global__ void k_row_anchors(const TcWork *__restrict__ wp) {
     utm_xy_to_lonlat(p.proj, p.ax[a], row_y(p, r), &lon, &lat);
     ((double *)p.alon)[li] = lon;
     ((double *)p.alat)[li] = lat;
+    if (p.aloc) {
+      const Utm &u = p.dem.utm;
+      utm_local(u, lat, utm_taup(u, lat), utm_lam(u, lon), (UtmLocal *)p.aloc + li);
+    }
   }
 }
 
@@ -625,11 +678,14 @@ struct PixGeo {
 // Centre of the pixel: lon/lat, the UTM local expansion for a projected DEM,
 // and the DEM height; false when there is no finite height.
 __device__ bool pixel_height(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g, float *hf) {
-  pixel_lonlat(p, r, c, &g->lon, &g->lat);
+  int seg;
+  double t;
+  pixel_seg(p, r, c, &g->lon, &g->lat, &seg, &t);
   bool ok;
   if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
     const Utm &u = p.dem.utm;
-    utm_local(u, g->lat, utm_taup(u, g->lat), utm_lam(u, g->lon), &g->loc);
+    if (p.aloc) dem_local_from_anchors(p, r, seg, t, &g->loc);
+    else utm_local(u, g->lat, utm_taup(u, g->lat), utm_lam(u, g->lon), &g->loc);
     ok = dem_at_xy(p.dem, g->loc.x, g->loc.y, hf);
   } else {
     ok = dem_at_lonlat(p.dem, g->lon, g->lat, hf);
@@ -1011,7 +1067,7 @@ constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
 // (NaN when any is missing).  These are the latency-bound gathers and
 // projections; done here at low register pressure they overlap well, and
 // k_main reads 20 B per pixel instead.
-__global__ void __launch_bounds__(SEL_THREADS) k_heights(const TcWork *__restrict__ wp) {
+__global__ void __launch_bounds__(SEL_THREADS, 4) k_heights(const TcWork *__restrict__ wp) {
   const TcWork w = *wp;
   const uint64_t *pre = stage_pre(w, WK_SEL);
   const uint64_t total = pre[w.n_jobs];

@@ -397,7 +397,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     return o;
   };
   struct Offs {
-    size_t guess, flat, knots, alon, alat, hc, hnb, rec, cc, sel, hout[3], fin[3];
+    size_t guess, flat, knots, alon, alat, aloc, hc, hnb, rec, cc, sel, hout[3], fin[3];
   };
   std::vector<Offs> of(n);
   size_t ax_total = 0;
@@ -408,10 +408,11 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     o.guess = take(p.rows * 8);
     o.flat = take(p.rows * 8);
     o.knots = take(p.rows * KNOTS * 8);
-    o.alon = o.alat = 0;
+    o.alon = o.alat = o.aloc = SIZE_MAX;
     if (p.utm) {
       o.alon = take(p.rows * p.n_pts * 8);
       o.alat = take(p.rows * p.n_pts * 8);
+      if (p.dem.kind == SD_DEM_PROJECTED_UTM) o.aloc = take(p.rows * p.n_pts * sizeof(UtmLocal));
       ax_total += p.n_pts;
     }
     o.hc = take(npx * sizeof(float));
@@ -467,6 +468,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
       for (int a = 0; a <= p.n_anchors; ++a) ax_h.push_back(x_start + (double)a * anchor_dx);
       p.alon = (const double *)(arena + o.alon);
       p.alat = (const double *)(arena + o.alat);
+      p.aloc = o.aloc != SIZE_MAX ? (const UtmLocal *)(arena + o.aloc) : nullptr;
     }
     p.hc = (const float *)(arena + o.hc);
     p.hnb = (const float4 *)(arena + o.hnb);

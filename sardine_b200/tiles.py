@@ -107,7 +107,7 @@ class TileRequest:
         h = self.halo()
         r, c = self.rows + 2 * h, self.cols + 2 * h
         anchors = min(256, c) + 1 if self.config.crs.kind != _abi.CRS_WGS84 else 0
-        per_row = 8 + 8 + 17 * 8 + 16 * anchors
+        per_row = 8 + 8 + 17 * 8 + (16 + 64) * anchors
         return r * c * (20 + 32 + 4 + 1 + 9) + r * per_row + self.rows * self.cols * 9 + 8192
 
 
