@@ -630,6 +630,139 @@ __device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, doub
   return (float)acc;
 }
 
+// ── both members of F at once ─────────────────────────────────────────────────
+// The two members' image coordinates differ by 1 us of azimuth time (~5e-4
+// line) and nanometres of slant range, so they almost always share their tap
+// window: one pass over the window then feeds both sums, each in the order
+// of its single-candidate sampler.  They return false (nothing done) when
+// the windows differ.
+__device__ bool sample_bicubic_pair(const float *d, uint64_t nl, uint64_t ns, const double *line,
+                                    const double *sample, float *out) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
+  if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
+  double ws0[4], ws1[4];
+  int64_t cols[4];
+  const double ds0 = sample[0] - (double)sf, ds1 = sample[1] - (double)sf;
+  const double dl0 = line[0] - (double)lf, dl1 = line[1] - (double)lf;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ws0[k] = keys_weight((double)(k - 1) - ds0);
+    ws1[k] = keys_weight((double)(k - 1) - ds1);
+    cols[k] = clampi(sf + k - 1, 0, max_s);
+  }
+  double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll
+  for (int li = -1; li <= 2; ++li) {
+    const int64_t row = clampi(lf + li, 0, max_l);
+    const double wl0 = keys_weight((double)li - dl0), wl1 = keys_weight((double)li - dl1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) {
+        out[0] = out[1] = NAN;
+        return true;
+      }
+      acc0 += (double)v * wl0 * ws0[k];
+      acc1 += (double)v * wl1 * ws1[k];
+    }
+  }
+  out[0] = (float)acc0;
+  out[1] = (float)acc1;
+  return true;
+}
+
+__device__ bool sample_bicubic_pair_f(const float *d, uint64_t nl, uint64_t ns, const double *line,
+                                      const double *sample, float *out, bool *redo) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
+  if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
+  float ws0[4], ws1[4], wl0[4], wl1[4];
+  keys4_f((float)(sample[0] - (double)sf), ws0);
+  keys4_f((float)(sample[1] - (double)sf), ws1);
+  keys4_f((float)(line[0] - (double)lf), wl0);
+  keys4_f((float)(line[1] - (double)lf), wl1);
+  int64_t cols[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) cols[k] = clampi(sf + k - 1, 0, max_s);
+  float acc0 = 0.f, acc1 = 0.f, aac0 = 0.f, aac1 = 0.f;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int64_t row = clampi(lf + j - 1, 0, max_l);
+    float r0 = 0.f, r1 = 0.f, a0 = 0.f, a1 = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) {
+        out[0] = out[1] = NAN;
+        return true;
+      }
+      r0 = fmaf(v, ws0[k], r0);
+      r1 = fmaf(v, ws1[k], r1);
+      a0 = fmaf(fabsf(v), fabsf(ws0[k]), a0);
+      a1 = fmaf(fabsf(v), fabsf(ws1[k]), a1);
+    }
+    acc0 = fmaf(r0, wl0[j], acc0);
+    acc1 = fmaf(r1, wl1[j], acc1);
+    aac0 = fmaf(a0, fabsf(wl0[j]), aac0);
+    aac1 = fmaf(a1, fabsf(wl1[j]), aac1);
+  }
+  out[0] = acc0;
+  out[1] = acc1;
+  redo[0] = aac0 > kCancel * fabsf(acc0);
+  redo[1] = aac1 > kCancel * fabsf(acc1);
+  return true;
+}
+
+template <typename T>
+__device__ bool sample_lanczos_pair(const float *d, uint64_t nl, uint64_t ns, const double *line,
+                                    const double *sample, float *out, bool *redo) {
+  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
+  const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
+  if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
+  T wl0[6], ws0[6], wl1[6], ws1[6];
+  lanczos6<T>((T)(line[0] - (double)lf), wl0);
+  lanczos6<T>((T)(sample[0] - (double)sf), ws0);
+  lanczos6<T>((T)(line[1] - (double)lf), wl1);
+  lanczos6<T>((T)(sample[1] - (double)sf), ws1);
+  int64_t cols[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) cols[k] = clampi(sf + k - 2, 0, max_s);
+  T acc0 = 0, acc1 = 0, aac0 = 0, aac1 = 0;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    const int64_t row = clampi(lf + j - 2, 0, max_l);
+    T r0 = 0, r1 = 0, a0 = 0, a1 = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const float v = ldf(d, row * (int64_t)ns + cols[k]);
+      if (v != v) {
+        out[0] = out[1] = NAN;
+        return true;
+      }
+      r0 += (T)v * ws0[k];
+      r1 += (T)v * ws1[k];
+      if (redo) {
+        a0 += fabs((T)v * ws0[k]);
+        a1 += fabs((T)v * ws1[k]);
+      }
+    }
+    acc0 += r0 * wl0[j];
+    acc1 += r1 * wl1[j];
+    if (redo) {
+      aac0 += a0 * fabs(wl0[j]);
+      aac1 += a1 * fabs(wl1[j]);
+    }
+  }
+  out[0] = (float)acc0;
+  out[1] = (float)acc1;
+  if (redo) {
+    redo[0] = aac0 > (T)kCancel * fabs(acc0);
+    redo[1] = aac1 > (T)kCancel * fabs(acc1);
+  }
+  return true;
+}
+
 // KDYN: the resampling kernel is read from the job record (batches whose
 // tiles mix kernels); 0..2 fix it at compile time.
 constexpr int KDYN = 3;
@@ -821,8 +954,8 @@ struct CandPre {  // steps 4-6 of the reference loop for one candidate
   bool inside;
 };
 
-template <int KERNEL, bool SPLIT>
-__device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
+// Slant range, image coordinates and the footprint test (745-760).
+__device__ __forceinline__ CandPre cand_geom(const TcDev &p, V3 P, V3 S, int64_t t) {
   CandPre c;
   double slant = norm3(sub3(P, S));
   double dt = (double)(t - p.az_start) / 1e6;
@@ -830,6 +963,48 @@ __device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
   c.sample = (slant - p.near_range) / p.rps;
   c.inside = !(c.line < -0.5 || c.line > ((double)p.lines - 0.5) || c.sample < -0.5 ||
                c.sample > ((double)p.samples - 0.5));
+  c.sigma0 = NAN;
+  return c;
+}
+
+// Resamples both members of F (pre[k] from cand_geom), sharing the tap window
+// when they can; members the pair samplers do not cover go one by one.
+template <int KERNEL, bool SPLIT>
+__device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask) {
+  const int kind = KERNEL == KDYN ? p.resampling : KERNEL;
+  bool done = false;
+  if (fmask == 3 && pre[0].inside && pre[1].inside && kind != SD_RESAMPLE_BILINEAR) {
+    const double line[2] = {pre[0].line, pre[1].line}, sample[2] = {pre[0].sample, pre[1].sample};
+    float out[2];
+    bool redo[2] = {false, false};
+    if (kind == SD_RESAMPLE_BICUBIC)
+      done = SPLIT ? sample_bicubic_pair_f(p.img, p.lines, p.samples, line, sample, out, redo)
+                   : sample_bicubic_pair(p.img, p.lines, p.samples, line, sample, out);
+    else
+      done = SPLIT ? sample_lanczos_pair<float>(p.img, p.lines, p.samples, line, sample, out, redo)
+                   : sample_lanczos_pair<double>(p.img, p.lines, p.samples, line, sample, out, nullptr);
+    if (done) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        pre[k].sigma0 = (SPLIT && redo[k]) ? resample<KERNEL>(p, pre[k].line, pre[k].sample) : out[k];
+        if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
+      }
+    }
+  }
+  if (done) return;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    if (!((fmask >> k) & 1) || !pre[k].inside) continue;
+    bool redo = false;
+    if (SPLIT) pre[k].sigma0 = resample_f<KERNEL>(p, pre[k].line, pre[k].sample, &redo);
+    if (!SPLIT || redo) pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
+    if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
+  }
+}
+
+template <int KERNEL, bool SPLIT>
+__device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
+  CandPre c = cand_geom(p, P, S, t);
   if (c.inside) {
     bool redo = false;
     if (SPLIT) c.sigma0 = resample_f<KERNEL>(p, c.line, c.sample, &redo);
@@ -1227,12 +1402,13 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
     for (int k = 0; k < 2; ++k) {
       const Ent &e = k == 0 ? e0 : e1;
       if ((fmask >> k) & 1) {
-        pre[k] = cand_pre<KERNEL, SPLIT>(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
-        need = need || pre[k].inside;
+        pre[k] = cand_geom(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
       } else {
         pre[k].inside = false;
       }
     }
+    resample_members<KERNEL, SPLIT>(p, pre, fmask);
+    need = pre[0].inside || pre[1].inside;
     const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
     if constexpr (SPLIT) {
       FacetF f{};
