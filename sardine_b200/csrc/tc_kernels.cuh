@@ -969,8 +969,11 @@ __device__ __forceinline__ CandPre cand_geom(const TcDev &p, V3 P, V3 S, int64_t
 
 // Resamples both members of F (pre[k] from cand_geom), sharing the tap window
 // when they can; members the pair samplers do not cover go one by one.
+// defer (split only): a value FP32 cannot settle is left for k_redo and
+// *defer set, instead of resampling it in FP64 here (a few lanes taking the
+// FP64 path would hold their whole warp).
 template <int KERNEL, bool SPLIT>
-__device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask) {
+__device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask, bool *defer) {
   const int kind = KERNEL == KDYN ? p.resampling : KERNEL;
   bool done = false;
   if (fmask == 3 && pre[0].inside && pre[1].inside && kind != SD_RESAMPLE_BILINEAR) {
@@ -986,7 +989,11 @@ __device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask) {
     if (done) {
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
-        pre[k].sigma0 = (SPLIT && redo[k]) ? resample<KERNEL>(p, pre[k].line, pre[k].sample) : out[k];
+        pre[k].sigma0 = out[k];
+        if (SPLIT && redo[k]) {
+          if (defer) *defer = true;
+          else pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
+        }
         if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
       }
     }
@@ -997,7 +1004,8 @@ __device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask) {
     if (!((fmask >> k) & 1) || !pre[k].inside) continue;
     bool redo = false;
     if (SPLIT) pre[k].sigma0 = resample_f<KERNEL>(p, pre[k].line, pre[k].sample, &redo);
-    if (!SPLIT || redo) pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
+    if (SPLIT && redo && defer) *defer = true;
+    else if (!SPLIT || redo) pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
     if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
   }
 }
@@ -1189,7 +1197,8 @@ struct __align__(16) Rec {
   uint8_t ocls[2];
   uint32_t pad;
 };
-enum : uint32_t { CF_DEMMISS = 1u << 18, CF_HASF = 1u << 19, CF_HASOUT = 1u << 20 };
+enum : uint32_t { CF_DEMMISS = 1u << 18, CF_HASF = 1u << 19, CF_HASOUT = 1u << 20,
+                  CF_REDO = 1u << 21 /* split: outputs to be redone in FP64 (k_redo) */ };
 // sel byte written by the scan: low 3 bits = outcome, high 4 bits = iterations
 enum : uint8_t { SEL_M0 = 0, SEL_M1 = 1, SEL_DONE = 2, SEL_NONCONV = 3, SEL_DEGEN = 4, SEL_DEMMISS = 5,
                  SEL_ORBIT = 6 };
@@ -1407,7 +1416,8 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         pre[k].inside = false;
       }
     }
-    resample_members<KERNEL, SPLIT>(p, pre, fmask);
+    bool defer = false;
+    resample_members<KERNEL, SPLIT>(p, pre, fmask, SPLIT ? &defer : nullptr);
     need = pre[0].inside || pre[1].inside;
     const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
     if constexpr (SPLIT) {
@@ -1428,7 +1438,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         const V3 S{e.px, e.py, e.pz};
         bool redo;
         CandOut o = cand_post_f(p, pre[k], g, S, f, (float)flat_area, &redo);
-        if (redo) o = cand_fp64<KERNEL>(p, g, S, fb + k, flat_area, h4);
+        defer = defer || redo;
         rec.data[k] = o.data;
         rec.cos[k] = o.cos;
         rec.omask[k] = o.mask;
@@ -1457,6 +1467,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
       }
     }
     cc |= CF_HASOUT;
+    if (defer) cc |= CF_REDO;
   }
   p.rec[i] = rec;
   p.cc[i] = cc;
@@ -1495,6 +1506,53 @@ __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const
     }
     const uint64_t li = item - pre[jb];
     main_item<KERNEL, SPLIT>(p, li / p.bpr, li % p.bpr, slot);
+  }
+}
+
+// ── k_redo (split precision): FP64 outputs for the flagged pixels ──────────
+// Pixels whose FP32 result fell inside its error margin (near-cancelling
+// resampling, or a mask decision at a threshold) get both members of F
+// recomputed with the FP64 candidate here, outside k_main's warps.
+template <int KERNEL>
+__global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__ wp) {
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_SEL);
+  const uint64_t total = pre[w.n_jobs];
+  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    const int jb = find_job(pre, w.n_jobs, item);
+    const TcDev &p = w.jobs[jb];
+    const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
+    if (i >= p.rows * p.cols) continue;
+    const uint32_t cc = p.cc[i];
+    if (!(cc & CF_REDO)) continue;
+    const uint64_t r = i / p.cols, c = i % p.cols;
+    PixGeo g;
+    float h4[4] = {NAN, NAN, NAN, NAN};
+    const float *hp = nullptr;
+    if (p.hc) {
+      pixel_lonlat(p, r, c, &g.lon, &g.lat);
+      pixel_ecef(p, &g, p.hc[i]);
+      const float4 q4 = p.hnb[i];
+      h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
+      hp = h4;
+    } else if (!pixel_geo(p, r, c, &g)) {
+      continue;
+    }
+    Rec rec = p.rec[i];
+    const int fmask = (int)((cc >> 16) & 3u);
+    const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+    for (int k = 0; k < 2; ++k) {
+      if (!((fmask >> k) & 1)) continue;
+      OrbitState os;
+      double vsq;
+      if (orbit_at(p.orb, rec.fb + k, &os, &vsq) != ORB_OK) continue;
+      const CandOut o = cand_fp64<KERNEL>(p, g, os.pos, rec.fb + k, flat_area, hp);
+      rec.data[k] = o.data;
+      rec.cos[k] = o.cos;
+      rec.omask[k] = o.mask;
+      rec.ocls[k] = o.cls;
+    }
+    p.rec[i] = rec;
   }
 }
 
@@ -1885,6 +1943,11 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
     k_main_batch<K, S><<<g, MAIN_THREADS, 0, st>>>(d_work);
   }
   SD_LAUNCHED(ctx);
+  }
+  if (S) {
+    SD_TIMED_BEGIN(ctx, "k_redo");
+    k_redo<K><<<persistent_grid(k_redo<K>, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
+    SD_LAUNCHED(ctx);
   }
   SD_TIMED_BEGIN(ctx, "k_scan");
   k_scan<K, S><<<persistent_grid(k_scan<K, S>, SCAN_WARPS * 32, 0, blocks_for(totals[WK_SCAN], SCAN_WARPS)),
