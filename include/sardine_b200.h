@@ -203,6 +203,9 @@ typedef struct sd_geocoded_info {
      * azimuth time fell outside the precomputed fixed-point pair, so their
      * outputs were computed on the row walk's exact path */
     uint64_t diag_exact_path_pixels;
+    /* diagnostic (split precision): pixels whose FP32 outputs fell inside
+     * their error margin and were recomputed in FP64 */
+    uint64_t diag_fp64_redo_pixels;
 } sd_geocoded_info;
 
 /* CalibrationVector / NoiseRangeVector (calibration.rs:38-82): one LUT row. */

@@ -348,6 +348,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   info->noise_masked_count = cnt[6];
   for (int k = 0; k < SD_NEWTON_ITER_HIST_SIZE; ++k) info->newton_iter_histogram[k] = cnt[kCounters + k];
   info->diag_exact_path_pixels = (uint64_t)flags[1];
+  info->diag_fp64_redo_pixels = (uint64_t)flags[2];
   SD_TRY(sync(ctx));
   return SD_OK;
 }

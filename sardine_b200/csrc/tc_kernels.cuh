@@ -345,6 +345,7 @@ __global__ void k_row_setup(const TcWork *__restrict__ wp) {
       for (int k = 0; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; ++k) p.counters[k] = 0;
       p.flags[0] = 0;
       p.flags[1] = 0;
+      p.flags[2] = 0;
     }
     const double y = row_y(p, r);
     double lat_seed = y;
@@ -1276,10 +1277,100 @@ __global__ void __launch_bounds__(SEL_THREADS, 4) k_heights(const TcWork *__rest
   }
 }
 
+// ── the orbit around a warp's shared time ────────────────────────────────────
+// A warp's 32 pixels converge within ~±5 ms of its shared time uw.  Inside
+// one Lagrange window the reference's position and velocity are degree-7
+// polynomials in time, so their Taylor expansions about uw reproduce them;
+// to third order the remainder is < 1e-14 m and 1e-17 m/s over 20 ms.  The
+// expansion starts from the table entry at uw (the reference's own sums) and
+// takes its higher derivatives from the window polynomials, so a lane's
+// states cost ~30 FMAs from shared memory instead of 80 B orbit-table reads
+// at scattered microseconds (the table entries of neighbouring pixels lie
+// ~250 us apart).  Times outside uw's window, at a state-vector time (where
+// the reference's acceleration drops a term) or more than 20 ms from uw read
+// the table.
+struct OrbTaylor {
+  double p0[3], v0[3], a0[3];  // table state at uw
+  double dp[3], p2[3], p3[3];  // position: d/dt, d2/dt2 / 2, d3/dt3 / 6
+  double v2[3], v3[3];         // velocity: d2/dt2 / 2, d3/dt3 / 6
+  int64_t uw, lo, hi;          // valid for lo < t < hi (uw's window), |t - uw| <= 20 ms
+  int ok, pad;
+};
+
+// Lanes 0-2 of the warp fill coordinate `lane` of T; lane 0 the bounds.
+__device__ __forceinline__ void orb_taylor_build(const OrbitDev &o, int64_t uw, const Ent &ew, bool ew_ok,
+                                                 int lane, OrbTaylor *T) {
+  if (lane > 2) return;
+  bool ok = ew_ok && o.poly && o.n >= 8;
+  uint64_t centre = 0;
+  if (ok) {
+    uint64_t lo = 0, hi = o.n;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) / 2;
+      if (o.svs[mid].time_us <= uw) lo = mid + 1; else hi = mid;
+    }
+    centre = lo - 1;
+    ok = centre + 1 < o.n && o.svs[centre].time_us != uw;
+  }
+  if (lane == 0) {
+    T->ok = ok;
+    T->uw = uw;
+    T->lo = ok ? o.svs[centre].time_us : 0;
+    T->hi = ok ? o.svs[centre + 1].time_us : 0;
+  }
+  if (!ok) return;
+  const uint64_t start = centre < 4 ? 0 : (centre + 4 >= o.n ? o.n - 8 : centre - 3);
+  const OrbPoly &w = o.poly[start];
+  const double x = (double)(uw - w.tc) / 1e6;
+  const int d = lane;
+  double b[8], v[8];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    b[m] = w.c[d][m];
+    v[m] = w.c[3 + d][m];
+  }
+  // Taylor shift by repeated synthetic division: after pass k, b[k] = p^(k)(x)/k!
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int j = 6; j >= k; --j) {
+      b[j] = fma(x, b[j + 1], b[j]);
+      v[j] = fma(x, v[j + 1], v[j]);
+    }
+  const double pe[3] = {ew.px, ew.py, ew.pz}, ve[3] = {ew.vx, ew.vy, ew.vz}, ae[3] = {ew.ax, ew.ay, ew.az};
+  T->p0[d] = pe[d];
+  T->v0[d] = ve[d];
+  T->a0[d] = ae[d];
+  T->dp[d] = b[1];
+  T->p2[d] = b[2];
+  T->p3[d] = b[3];
+  T->v2[d] = v[2];
+  T->v3[d] = v[3];
+}
+
+// State at t from the warp's expansion, or from the table.
+__device__ __forceinline__ int ent_lane(const OrbitDev &o, const OrbTaylor &T, int64_t t, Ent *e) {
+  const int64_t dt = t - T.uw;
+  if (T.ok && t > T.lo && t < T.hi && dt <= 20000 && dt >= -20000) {
+    const double h = (double)dt * 1e-6;
+    double P[3], V[3], A[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      P[d] = fma(h, fma(h, fma(h, T.p3[d], T.p2[d]), T.dp[d]), T.p0[d]);
+      V[d] = fma(h, fma(h, fma(h, T.v3[d], T.v2[d]), T.a0[d]), T.v0[d]);
+      A[d] = fma(h, fma(h, 3.0 * T.v3[d], 2.0 * T.v2[d]), T.a0[d]);
+    }
+    *e = {P[0], P[1], P[2], V[0], V[1], V[2], A[0], A[1], A[2], V[0] * V[0] + V[1] * V[1] + V[2] * V[2]};
+    return ORB_OK;
+  }
+  return ent_at(o, t, e);
+}
+
 // One k_main work item: MAIN_PIX pixels of row r starting at chunk * MAIN_PIX
 // (plus the left neighbour on thread 0).  Every thread of the block calls it.
 template <int KERNEL, bool SPLIT>
-__device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t chunk, Slot *slot) {
+__device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t chunk, Slot *slot,
+                                          OrbTaylor *tw) {
   const int tid = threadIdx.x;
   const int fast = p.fast;
   const int64_t c = (int64_t)chunk * MAIN_PIX + tid - 1;
@@ -1298,6 +1389,9 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   const int64_t uw = __shfl_sync(0xffffffffu, predicted_time(p, rr, cq), 16);
   Ent ew;
   const bool ew_ok = fast && ent_at(p.orb, uw, &ew) == ORB_OK;
+  OrbTaylor &T = tw[tid >> 5];
+  orb_taylor_build(p.orb, uw, ew, ew_ok, tid & 31, &T);
+  __syncwarp();
   float h4[4] = {NAN, NAN, NAN, NAN};
   if (in_row && r < p.rows) {
     if (p.hc) {  // heights from k_heights
@@ -1316,7 +1410,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
       int st = 1;
       for (int it = 0; it < 40 && st == 1; ++it) {
         if (it == 0 && ew_ok) e = ew;
-        else if (ent_at(p.orb, t, &e) != ORB_OK) { st = 3; break; }
+        else if (ent_lane(p.orb, T, t, &e) != ORB_OK) { st = 3; break; }
         st = zd_eval(g.P, e, p.tol, &d);
         if (st == 1) t = t + f2i64(d * 1e6);
       }
@@ -1329,10 +1423,10 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         Ent ea, eb;
         double da = 0.0, db = 0.0;
         const int64_t ta = d > 0.0 ? t + 1 : t - 1;   // the likely member
-        const bool ma = ent_at(p.orb, ta, &ea) == ORB_OK && zd_eval(g.P, ea, p.tol, &da) == 0;
+        const bool ma = ent_lane(p.orb, T, ta, &ea) == ORB_OK && zd_eval(g.P, ea, p.tol, &da) == 0;
         bool mb = false;
         const int64_t tb = d > 0.0 ? t - 1 : t + 1;
-        if (fabs(d) < 1e-11) mb = ent_at(p.orb, tb, &eb) == ORB_OK && zd_eval(g.P, eb, p.tol, &db) == 0;
+        if (fabs(d) < 1e-11) mb = ent_lane(p.orb, T, tb, &eb) == ORB_OK && zd_eval(g.P, eb, p.tol, &db) == 0;
         if (!(ma && mb)) {
           const bool use_b = mb;                      // pair {t*, tb} when only tb joins
           const int64_t other = use_b ? tb : ta;
@@ -1385,7 +1479,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
           Ent e;
           bool have = true;
           if (t == L.fb + k) e = L.e[k];
-          else have = ent_at(p.orb, t, &e) == ORB_OK;
+          else have = ent_lane(p.orb, T, t, &e) == ORB_OK;
           if (!have) break;  // orbit error: the walk redoes it
           double d;
           int st = zd_eval(g.P, e, p.tol, &d);
@@ -1478,7 +1572,8 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
 template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main(TcDev p) {
   __shared__ Slot slot[MAIN_THREADS];
-  main_item<KERNEL, SPLIT>(p, blockIdx.x / p.bpr, blockIdx.x % p.bpr, slot);
+  __shared__ OrbTaylor tw[MAIN_THREADS / 32];
+  main_item<KERNEL, SPLIT>(p, blockIdx.x / p.bpr, blockIdx.x % p.bpr, slot, tw);
 }
 
 // Tile batches: persistent CTAs over the work table; the current job's
@@ -1487,6 +1582,7 @@ template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const TcWork *__restrict__ wp) {
   __shared__ Slot slot[MAIN_THREADS];
   __shared__ __align__(16) unsigned char s_job[sizeof(TcDev)];
+  __shared__ OrbTaylor tw[MAIN_THREADS / 32];
   __shared__ int s_j;
   const TcWork w = *wp;
   const uint64_t *pre = stage_pre(w, WK_MAIN);
@@ -1505,7 +1601,7 @@ __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const
       cur = jb;
     }
     const uint64_t li = item - pre[jb];
-    main_item<KERNEL, SPLIT>(p, li / p.bpr, li % p.bpr, slot);
+    main_item<KERNEL, SPLIT>(p, li / p.bpr, li % p.bpr, slot, tw);
   }
 }
 
@@ -1541,6 +1637,7 @@ __global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__
     Rec rec = p.rec[i];
     const int fmask = (int)((cc >> 16) & 3u);
     const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+    atomicAdd(&p.flags[2], 1);
     for (int k = 0; k < 2; ++k) {
       if (!((fmask >> k) & 1)) continue;
       OrbitState os;

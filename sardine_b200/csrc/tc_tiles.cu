@@ -631,6 +631,7 @@ extern "C" int sd_tc_tiles_finish(sd_ctx *ctx, sd_geocoded_info *infos, uint64_t
     f.noise_masked_count = c[6];
     for (int k = 0; k < SD_NEWTON_ITER_HIST_SIZE; ++k) f.newton_iter_histogram[k] = c[kCounters + k];
     f.diag_exact_path_pixels = (uint64_t)ctx->h_tile_flags[4 * i + 1];
+    f.diag_fp64_redo_pixels = (uint64_t)ctx->h_tile_flags[4 * i + 2];
     if (ctx->h_tile_flags[4 * i] && orbit_bad < 0) orbit_bad = (int)i;
     infos[i] = f;
   }

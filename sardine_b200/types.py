@@ -412,6 +412,7 @@ class GeocodedImage:
     mask: Any
     newton_iter_histogram: List[int]
     diag_exact_path_pixels: int = 0  # converged pixels computed on the row walk's exact path
+    diag_fp64_redo_pixels: int = 0   # split precision: pixels recomputed in FP64
     azimuth_time_us: Any = None      # converged zero-Doppler time per pixel (INT64_MIN: none)
 
     def valid_fraction(self) -> float:
@@ -433,7 +434,8 @@ class GeocodedImage:
             noise_masked_count=int(info.noise_masked_count),
             geotransform=tuple(info.geotransform), crs=crs, cos_lia=cos_lia, mask=mask,
             newton_iter_histogram=[int(x) for x in info.newton_iter_histogram],
-            diag_exact_path_pixels=int(info.diag_exact_path_pixels))
+            diag_exact_path_pixels=int(info.diag_exact_path_pixels),
+            diag_fp64_redo_pixels=int(info.diag_fp64_redo_pixels))
 
 
 # ── speckle ────────────────────────────────────────────────────────────────
