@@ -206,6 +206,9 @@ typedef struct sd_geocoded_info {
     /* diagnostic (split precision): pixels whose FP32 outputs fell inside
      * their error margin and were recomputed in FP64 */
     uint64_t diag_fp64_redo_pixels;
+    /* diagnostic (split precision): candidates whose FP32 resampling sum
+     * cancelled beyond its error bound and was re-sampled in FP64 */
+    uint64_t diag_fp64_resampled;
 } sd_geocoded_info;
 
 /* CalibrationVector / NoiseRangeVector (calibration.rs:38-82): one LUT row. */

@@ -98,7 +98,8 @@ class GeocodedInfo(C.Structure):
                 ("degenerate_geometry_count", C.c_uint64), ("flat_masked_count", C.c_uint64),
                 ("noise_masked_count", C.c_uint64),
                 ("newton_iter_histogram", C.c_uint64 * SD_NEWTON_ITER_HIST_SIZE),
-                ("diag_exact_path_pixels", C.c_uint64), ("diag_fp64_redo_pixels", C.c_uint64)]
+                ("diag_exact_path_pixels", C.c_uint64), ("diag_fp64_redo_pixels", C.c_uint64),
+                ("diag_fp64_resampled", C.c_uint64)]
 
     COUNTERS = ("total_pixel_count", "valid_pixel_count", "dem_missing_count",
                 "outside_footprint_count", "non_converged_count", "degenerate_geometry_count",

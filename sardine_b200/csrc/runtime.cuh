@@ -38,7 +38,7 @@ struct sd_ctx {
   // batched tiles (sd_tc_tiles_*): the last launch's results land here
   cudaEvent_t tiles_done = nullptr;
   unsigned long long *h_tile_counters = nullptr;  // pinned, tile_cap x 32
-  int *h_tile_flags = nullptr;                    // pinned, tile_cap x 4
+  int *h_tile_flags = nullptr;                    // pinned, tile_cap x 8
   uint64_t tile_cap = 0, tile_n = 0;
   std::vector<sd_geocoded_info> tile_info;
   bool tiles_pending = false;

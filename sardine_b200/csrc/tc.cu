@@ -295,6 +295,10 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   p.fast = (p.tol <= 1e-6) ? 1 : 0;
   p.bpr = (p.cols + MAIN_PIX - 1) / MAIN_PIX;
   p.split = cfg->precision == SD_PRECISION_SPLIT;
+  if (p.split) {  // FP64 re-sample queue of every k_main item
+    SD_TRY(scratch_t(ctx, "tc.rs_cnt", p.rows * p.bpr, &p.rs_cnt));
+    SD_TRY(scratch_t(ctx, "tc.rs_ent", p.rows * p.bpr * RS_CAP, &p.rs_ent));
+  }
 
   // ── one-job work table ──
   TcWorkHost wk;
@@ -349,6 +353,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   for (int k = 0; k < SD_NEWTON_ITER_HIST_SIZE; ++k) info->newton_iter_histogram[k] = cnt[kCounters + k];
   info->diag_exact_path_pixels = (uint64_t)flags[1];
   info->diag_fp64_redo_pixels = (uint64_t)flags[2];
+  info->diag_fp64_resampled = (uint64_t)flags[4];
   SD_TRY(sync(ctx));
   return SD_OK;
 }

@@ -156,6 +156,8 @@ struct TcDev {
   uint64_t row0;               // grid row of the job's first row (row bands)
   const float *hc;             // per pixel: DEM height of the centre (NaN: none), from k_heights
   const float4 *hnb;           // per pixel: heights of the E, W, N, S neighbours (NaN: facet missing)
+  uint32_t *rs_cnt;            // split: per k_main item, FP64 re-samples queued (may exceed RS_CAP)
+  struct RsEnt *rs_ent;        // split: per k_main item, RS_CAP queued re-samples
 };
 
 // ── work table ──────────────────────────────────────────────────────────────
@@ -164,8 +166,9 @@ struct TcDev {
 // prefix sum of the stage's work items over jobs 0..j-1.  Kernels are
 // persistent (grid sized to the device's resident CTAs) and stride over the
 // items; a CUDA graph of the stages therefore does not depend on the batch.
-enum { WK_ANCH = 0, WK_ROWS = 1, WK_KNOT = 2, WK_MAIN = 3, WK_SCAN = 4, WK_SEL = 5, kWk = 6 };
+enum { WK_ANCH = 0, WK_ROWS = 1, WK_KNOT = 2, WK_MAIN = 3, WK_SCAN = 4, WK_SEL = 5, WK_REDO = 6, kWk = 7 };
 constexpr int SEL_THREADS = 256;
+constexpr int REDO_CHUNK = SEL_THREADS * 32;  // pixels one k_redo block compacts
 
 struct TcWork {
   int n_jobs;
@@ -343,10 +346,10 @@ __global__ void k_row_setup(const TcWork *__restrict__ wp) {
     const uint64_t r = i - pre[j];
     if (r == 0) {  // the job's counters and flags start at zero
       for (int k = 0; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; ++k) p.counters[k] = 0;
-      p.flags[0] = 0;
-      p.flags[1] = 0;
-      p.flags[2] = 0;
+      for (int k = 0; k < 5; ++k) p.flags[k] = 0;
     }
+    if (p.rs_cnt)
+      for (uint64_t b = 0; b < p.bpr; ++b) p.rs_cnt[r * p.bpr + b] = 0;
     const double y = row_y(p, r);
     double lat_seed = y;
     if (p.utm) {
@@ -540,14 +543,29 @@ __device__ __forceinline__ void lanczos6<double>(double f, double w[6]) {
   }
 }
 
-// The FP32 samplers also form the magnitude sum A = sum |v w|: the FP32
-// rounding error of the result is a few ulps of A, so where |result| <
-// A / kCancel (negative lobes or extrapolation cancelling) the FP64 sampler
-// redoes the pixel and the result keeps its 1e-4 relative bound.
-constexpr float kCancel = 16.f;
+// The FP32 samplers also return the magnitude sum A = sum |v w|.  Their
+// error is at most kSampErr * A: two nested fma chains of <= 6 terms
+// (12 u of A) plus the FP32 weights' own rounding (a few ulps each, 2e-6 for
+// a weight product).  The bound travels with the value (CandPre::serr) to
+// the mask decisions, so an inexact sum (negative lobes cancelling) costs an
+// FP64 re-sample only where it can change the output: a valid pixel whose
+// bound exceeds kSampRel of its value, or a noise-floor test within it.
+constexpr float kSampErr = 4e-6f;
+constexpr float kSampRel = 5e-5f;
+
+// cand_post_f outcomes: settled; the whole candidate again in FP64 (a mask
+// decision within its FP32 margin: k_redo); only the value in FP64 (the
+// image coordinates and flattening weight are queued for k_resample).
+enum { RD_NONE = 0, RD_FULL = 1, RD_SAMPLE = 2 };
+struct RsEnt {
+  double line, sample;  // FP64 image coordinates of the candidate
+  float wdiv;           // flattening weight the value is divided by (1: none)
+  uint32_t meta;        // thread of the k_main item (1..255) | member << 8
+};
+constexpr int RS_CAP = 64;  // queued re-samples per k_main item (beyond: k_redo)
 
 __device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, double line, double sample,
-                                   bool *redo) {
+                                   float *amag) {
   int64_t max_line = nl == 0 ? 0 : (int64_t)nl - 1;
   int64_t max_sample = ns == 0 ? 0 : (int64_t)ns - 1;
   int64_t l0 = clampi(f2i64(floor(line)), 0, max_line);
@@ -566,12 +584,12 @@ __device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, dou
   const float r = fmaf(v00, w00, fmaf(v01, w01, fmaf(v10, w10, v11 * w11)));
   const float a = fmaf(fabsf(v00), fabsf(w00), fmaf(fabsf(v01), fabsf(w01),
                        fmaf(fabsf(v10), fabsf(w10), fabsf(v11) * fabsf(w11))));
-  if (a > kCancel * fabsf(r)) *redo = true;
+  *amag = a;
   return r;
 }
 
 __device__ float sample_bicubic_f(const float *d, uint64_t nl, uint64_t ns, double line, double sample,
-                                  bool *redo) {
+                                  float *amag) {
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
   const float dl = (float)(line - (double)lf), ds = (float)(sample - (double)sf);
@@ -597,13 +615,13 @@ __device__ float sample_bicubic_f(const float *d, uint64_t nl, uint64_t ns, doub
     acc = fmaf(racc, wl, acc);
     aacc = fmaf(rabs, fabsf(wl), aacc);
   }
-  if (aacc > kCancel * fabsf(acc)) *redo = true;
+  *amag = aacc;
   return acc;
 }
 
 template <typename T>
 __device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, double line, double sample,
-                                  bool *redo) {
+                                  float *amag) {
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
   T wl[6], ws[6];
@@ -622,12 +640,12 @@ __device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, doub
       float v = ldf(d, row * (int64_t)ns + cols[k]);
       if (v != v) return NAN;
       racc += (T)v * ws[k];
-      if (redo) rabs += fabs((T)v * ws[k]);
+      if (amag) rabs += fabs((T)v * ws[k]);
     }
     acc += racc * wl[j];
-    if (redo) aacc += rabs * fabs(wl[j]);
+    if (amag) aacc += rabs * fabs(wl[j]);
   }
-  if (redo && aacc > (T)kCancel * fabs(acc)) *redo = true;
+  if (amag) *amag = (float)aacc;
   return (float)acc;
 }
 
@@ -674,7 +692,7 @@ __device__ bool sample_bicubic_pair(const float *d, uint64_t nl, uint64_t ns, co
 }
 
 __device__ bool sample_bicubic_pair_f(const float *d, uint64_t nl, uint64_t ns, const double *line,
-                                      const double *sample, float *out, bool *redo) {
+                                      const double *sample, float *out, float *amag) {
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
   if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
@@ -710,14 +728,14 @@ __device__ bool sample_bicubic_pair_f(const float *d, uint64_t nl, uint64_t ns, 
   }
   out[0] = acc0;
   out[1] = acc1;
-  redo[0] = aac0 > kCancel * fabsf(acc0);
-  redo[1] = aac1 > kCancel * fabsf(acc1);
+  amag[0] = aac0;
+  amag[1] = aac1;
   return true;
 }
 
 template <typename T>
 __device__ bool sample_lanczos_pair(const float *d, uint64_t nl, uint64_t ns, const double *line,
-                                    const double *sample, float *out, bool *redo) {
+                                    const double *sample, float *out, float *amag) {
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
   if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
@@ -743,23 +761,23 @@ __device__ bool sample_lanczos_pair(const float *d, uint64_t nl, uint64_t ns, co
       }
       r0 += (T)v * ws0[k];
       r1 += (T)v * ws1[k];
-      if (redo) {
+      if (amag) {
         a0 += fabs((T)v * ws0[k]);
         a1 += fabs((T)v * ws1[k]);
       }
     }
     acc0 += r0 * wl0[j];
     acc1 += r1 * wl1[j];
-    if (redo) {
+    if (amag) {
       aac0 += a0 * fabs(wl0[j]);
       aac1 += a1 * fabs(wl1[j]);
     }
   }
   out[0] = (float)acc0;
   out[1] = (float)acc1;
-  if (redo) {
-    redo[0] = aac0 > (T)kCancel * fabs(acc0);
-    redo[1] = aac1 > (T)kCancel * fabs(acc1);
+  if (amag) {
+    amag[0] = (float)aac0;
+    amag[1] = (float)aac1;
   }
   return true;
 }
@@ -769,17 +787,17 @@ __device__ bool sample_lanczos_pair(const float *d, uint64_t nl, uint64_t ns, co
 constexpr int KDYN = 3;
 
 template <int KERNEL>
-__device__ __forceinline__ float resample_f(const TcDev &p, double line, double sample, bool *redo) {
+__device__ __forceinline__ float resample_f(const TcDev &p, double line, double sample, float *amag) {
   if (KERNEL == KDYN) {
     switch (p.resampling) {
-      case SD_RESAMPLE_BICUBIC: return sample_bicubic_f(p.img, p.lines, p.samples, line, sample, redo);
-      case SD_RESAMPLE_LANCZOS3: return sample_lanczos_t<float>(p.img, p.lines, p.samples, line, sample, redo);
-      default: return sample_bilinear_f(p.img, p.lines, p.samples, line, sample, redo);
+      case SD_RESAMPLE_BICUBIC: return sample_bicubic_f(p.img, p.lines, p.samples, line, sample, amag);
+      case SD_RESAMPLE_LANCZOS3: return sample_lanczos_t<float>(p.img, p.lines, p.samples, line, sample, amag);
+      default: return sample_bilinear_f(p.img, p.lines, p.samples, line, sample, amag);
     }
   }
-  return KERNEL == SD_RESAMPLE_BICUBIC    ? sample_bicubic_f(p.img, p.lines, p.samples, line, sample, redo)
-         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos_t<float>(p.img, p.lines, p.samples, line, sample, redo)
-                                          : sample_bilinear_f(p.img, p.lines, p.samples, line, sample, redo);
+  return KERNEL == SD_RESAMPLE_BICUBIC    ? sample_bicubic_f(p.img, p.lines, p.samples, line, sample, amag)
+         : KERNEL == SD_RESAMPLE_LANCZOS3 ? sample_lanczos_t<float>(p.img, p.lines, p.samples, line, sample, amag)
+                                          : sample_bilinear_f(p.img, p.lines, p.samples, line, sample, amag);
 }
 
 template <int KERNEL>
@@ -952,6 +970,7 @@ struct CandOut {
 struct CandPre {  // steps 4-6 of the reference loop for one candidate
   double line, sample;
   float sigma0;
+  float serr;  // bound on |sigma0 - FP64 value| (0 when sampled in FP64)
   bool inside;
 };
 
@@ -965,36 +984,33 @@ __device__ __forceinline__ CandPre cand_geom(const TcDev &p, V3 P, V3 S, int64_t
   c.inside = !(c.line < -0.5 || c.line > ((double)p.lines - 0.5) || c.sample < -0.5 ||
                c.sample > ((double)p.samples - 0.5));
   c.sigma0 = NAN;
+  c.serr = 0.f;
   return c;
 }
 
 // Resamples both members of F (pre[k] from cand_geom), sharing the tap window
 // when they can; members the pair samplers do not cover go one by one.
-// defer (split only): a value FP32 cannot settle is left for k_redo and
-// *defer set, instead of resampling it in FP64 here (a few lanes taking the
-// FP64 path would hold their whole warp).
+// Split precision samples in FP32 and leaves the error bound in serr for
+// cand_post_f to judge (a few lanes taking an FP64 path here would hold
+// their whole warp).
 template <int KERNEL, bool SPLIT>
-__device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask, bool *defer) {
+__device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask) {
   const int kind = KERNEL == KDYN ? p.resampling : KERNEL;
   bool done = false;
   if (fmask == 3 && pre[0].inside && pre[1].inside && kind != SD_RESAMPLE_BILINEAR) {
     const double line[2] = {pre[0].line, pre[1].line}, sample[2] = {pre[0].sample, pre[1].sample};
-    float out[2];
-    bool redo[2] = {false, false};
+    float out[2], amag[2] = {0.f, 0.f};
     if (kind == SD_RESAMPLE_BICUBIC)
-      done = SPLIT ? sample_bicubic_pair_f(p.img, p.lines, p.samples, line, sample, out, redo)
+      done = SPLIT ? sample_bicubic_pair_f(p.img, p.lines, p.samples, line, sample, out, amag)
                    : sample_bicubic_pair(p.img, p.lines, p.samples, line, sample, out);
     else
-      done = SPLIT ? sample_lanczos_pair<float>(p.img, p.lines, p.samples, line, sample, out, redo)
+      done = SPLIT ? sample_lanczos_pair<float>(p.img, p.lines, p.samples, line, sample, out, amag)
                    : sample_lanczos_pair<double>(p.img, p.lines, p.samples, line, sample, out, nullptr);
     if (done) {
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         pre[k].sigma0 = out[k];
-        if (SPLIT && redo[k]) {
-          if (defer) *defer = true;
-          else pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
-        }
+        if (SPLIT) pre[k].serr = kSampErr * amag[k];
         if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
       }
     }
@@ -1003,10 +1019,13 @@ __device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask, bool
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
     if (!((fmask >> k) & 1) || !pre[k].inside) continue;
-    bool redo = false;
-    if (SPLIT) pre[k].sigma0 = resample_f<KERNEL>(p, pre[k].line, pre[k].sample, &redo);
-    if (SPLIT && redo && defer) *defer = true;
-    else if (!SPLIT || redo) pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
+    if (SPLIT) {
+      float amag = 0.f;
+      pre[k].sigma0 = resample_f<KERNEL>(p, pre[k].line, pre[k].sample, &amag);
+      pre[k].serr = kSampErr * amag;
+    } else {
+      pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
+    }
     if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
   }
 }
@@ -1015,9 +1034,13 @@ template <int KERNEL, bool SPLIT>
 __device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
   CandPre c = cand_geom(p, P, S, t);
   if (c.inside) {
-    bool redo = false;
-    if (SPLIT) c.sigma0 = resample_f<KERNEL>(p, c.line, c.sample, &redo);
-    if (!SPLIT || redo) c.sigma0 = resample<KERNEL>(p, c.line, c.sample);
+    if (SPLIT) {
+      float amag = 0.f;
+      c.sigma0 = resample_f<KERNEL>(p, c.line, c.sample, &amag);
+      c.serr = kSampErr * amag;
+    } else {
+      c.sigma0 = resample<KERNEL>(p, c.line, c.sample);
+    }
   } else {
     c.sigma0 = NAN;
   }
@@ -1116,11 +1139,11 @@ __device__ FacetF pixel_facet_f(const TcDev &p, const PixGeo &g) {
 // cand_post in split precision; *redo is set when a mask decision falls
 // inside the FP32 error margin and the FP64 candidate must decide.
 __device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g, V3 S, const FacetF &f,
-                               float flat_area, bool *redo) {
+                               float flat_area, int *redo, float *wdiv) {
   CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
-  *redo = false;
+  *redo = RD_NONE;
   if (!c.inside) return o;
-  float sigma0 = c.sigma0;
+  float sigma0 = c.sigma0, serr = c.serr, wd = 1.f;
   float cosv = NAN;
   if (p.need_geom) {
     if (!f.ok) {
@@ -1129,29 +1152,43 @@ __device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g
       const float lx = (float)(S.x - g.P.x), ly = (float)(S.y - g.P.y), lz = (float)(S.z - g.P.z);
       const float il = rsqrtf(lx * lx + ly * ly + lz * lz);
       const float lp = (f.nx * lx + f.ny * ly + f.nz * lz) * il;
-      if (fabsf(lp) <= 1e-4f * f.area) { *redo = true; return o; }
+      if (fabsf(lp) <= 1e-4f * f.area) { *redo = RD_FULL; return o; }
       if (lp <= 0.f || f.area == 0.f) {
         if (p.flatten) return {NAN, cosv, (uint8_t)SD_MASK_SHADOW, 5};
       } else {
         const float w = lp / flat_area;
-        if (fabsf(w - 0.05f) <= 5e-6f || fabsf(w - 2.0f) <= 2e-4f) { *redo = true; return o; }
+        if (fabsf(w - 0.05f) <= 5e-6f || fabsf(w - 2.0f) <= 2e-4f) { *redo = RD_FULL; return o; }
         cosv = fminf(fmaxf(lp / f.area, 0.f), 1.f);
         if (w < 0.05f || w > 2.0f) {
           if (p.flatten) return {NAN, cosv, (uint8_t)(w > 2.0f ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING), 5};
         } else if (p.flatten) {
           sigma0 /= w;
+          serr /= w;
+          wd = w;
         }
       }
     }
   }
+  const bool sample_ok = serr <= kSampRel * fabsf(sigma0);
   if (p.nesz_mask) {
-    bool nz_redo = false;
-    float nz = sample_bilinear_f(p.nesz, p.lines, p.samples, c.line, c.sample, &nz_redo);
+    // NESZ is non-negative, so its bilinear sum is accurate to a few ulps
+    float nz_mag;
+    float nz = sample_bilinear_f(p.nesz, p.lines, p.samples, c.line, c.sample, &nz_mag);
     if (nz == nz) {
       float thr = nz * p.nesz_factor;
-      if (nz_redo || fabsf(sigma0 - thr) <= 1e-5f * fabsf(thr)) { *redo = true; return o; }
-      if (sigma0 <= thr) return {NAN, cosv, (uint8_t)SD_MASK_NOISE_MASKED, 6};
+      if (fabsf(sigma0 - thr) > serr + 1e-5f * (fabsf(thr) + nz_mag * fabsf(p.nesz_factor))) {
+        if (sigma0 <= thr) return {NAN, cosv, (uint8_t)SD_MASK_NOISE_MASKED, 6};
+      } else if (sample_ok) {
+        *redo = RD_FULL;  // the threshold test itself is marginal
+        return o;
+      }
     }
+  }
+  if (!sample_ok) {  // geometry settled; the value (and a NESZ test) wait for the FP64 re-sample
+    *redo = RD_SAMPLE;
+    *wdiv = wd;
+    o.cos = cosv;
+    return o;
   }
   return {sigma0, cosv, (uint8_t)SD_MASK_VALID, 0};
 }
@@ -1181,9 +1218,10 @@ __device__ CandOut cand_full(const TcDev &p, const PixGeo &g, V3 S, int64_t t, d
   FacetF f{};
   if (pre.inside && p.need_geom)
     f = h4 ? (heights_ok(h4) ? facetf_from(p, g, h4) : FacetF{}) : pixel_facet_f(p, g);
-  bool redo;
-  CandOut o = cand_post_f(p, pre, g, S, f, (float)flat_area, &redo);
-  return redo ? cand_fp64<KERNEL>(p, g, S, t, flat_area, h4) : o;
+  int redo;
+  float wd;
+  CandOut o = cand_post_f(p, pre, g, S, f, (float)flat_area, &redo, &wd);
+  return redo != RD_NONE ? cand_fp64<KERNEL>(p, g, S, t, flat_area, h4) : o;
 }
 
 // ── per-pixel stores ─────────────────────────────────────────────────────────
@@ -1244,6 +1282,7 @@ struct Slot {  // shared-memory record exchanged with the right-hand neighbour
 #endif
 constexpr int MAIN_THREADS = SD_MAIN_THREADS;
 constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
+static_assert(MAIN_THREADS <= 256, "RsEnt::meta holds the k_main thread in 8 bits");
 
 // ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
 // ── k_heights: the DEM side of every pixel ahead of k_main ─────────────────
@@ -1511,7 +1550,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
       }
     }
     bool defer = false;
-    resample_members<KERNEL, SPLIT>(p, pre, fmask, SPLIT ? &defer : nullptr);
+    resample_members<KERNEL, SPLIT>(p, pre, fmask);
     need = pre[0].inside || pre[1].inside;
     const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
     if constexpr (SPLIT) {
@@ -1530,9 +1569,18 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         const Ent &e = k == 0 ? e0 : e1;
         if (!((fmask >> k) & 1)) continue;
         const V3 S{e.px, e.py, e.pz};
-        bool redo;
-        CandOut o = cand_post_f(p, pre[k], g, S, f, (float)flat_area, &redo);
-        defer = defer || redo;
+        int redo;
+        float wd;
+        CandOut o = cand_post_f(p, pre[k], g, S, f, (float)flat_area, &redo, &wd);
+        if (redo == RD_SAMPLE) {  // queue the FP64 re-sample in this item's slots
+          const uint64_t item = r * p.bpr + chunk;
+          const uint32_t q = atomicAdd(p.rs_cnt + item, 1u);
+          if (q < (uint32_t)RS_CAP)
+            p.rs_ent[item * RS_CAP + q] = RsEnt{pre[k].line, pre[k].sample, wd, (uint32_t)tid | ((uint32_t)k << 8)};
+          else
+            redo = RD_FULL;
+        }
+        defer = defer || redo == RD_FULL;
         rec.data[k] = o.data;
         rec.cos[k] = o.cos;
         rec.omask[k] = o.mask;
@@ -1561,7 +1609,10 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
       }
     }
     cc |= CF_HASOUT;
-    if (defer) cc |= CF_REDO;
+    if (defer) {
+      cc |= CF_REDO;
+      atomicAdd(&p.flags[3], 1);
+    }
   }
   p.rec[i] = rec;
   p.cc[i] = cc;
@@ -1605,51 +1656,129 @@ __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const
   }
 }
 
+// ── k_resample (split precision): FP64 values of the queued candidates ────────
+// k_main queues a candidate (RD_SAMPLE) whose geometry, masks and flattening
+// weight FP32 settled but whose resampling sum cancelled past its error
+// bound.  One warp per k_main item, one lane per queued candidate: the FP64
+// sampler, the flattening division and the NESZ test of cand_post; a NESZ
+// test within its margin sends the pixel to k_redo instead.
+template <int KERNEL>
+__global__ void __launch_bounds__(SEL_THREADS) k_resample(const TcWork *__restrict__ wp) {
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_MAIN);
+  const uint64_t total = pre[w.n_jobs];
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (SEL_THREADS / 32);
+  for (uint64_t item = (uint64_t)blockIdx.x * (SEL_THREADS / 32) + (threadIdx.x >> 5); item < total;
+       item += nwarps) {
+    const int jb = find_job(pre, w.n_jobs, item);
+    const TcDev &p = w.jobs[jb];
+    if (!p.rs_cnt) continue;
+    const uint64_t li = item - pre[jb];
+    const uint32_t n = min(p.rs_cnt[li], (uint32_t)RS_CAP);
+    if (n == 0) continue;
+    const uint64_t r = li / p.bpr, chunk = li % p.bpr;
+    for (uint32_t q = lane; q < n; q += 32) {
+      const RsEnt e = p.rs_ent[li * RS_CAP + q];
+      const uint64_t c = chunk * MAIN_PIX + (e.meta & 0xFFu) - 1;
+      const int k = (int)(e.meta >> 8);
+      const uint64_t i = r * p.cols + c;
+      Rec &rec = p.rec[i];
+      float sigma0 = resample<KERNEL>(p, e.line, e.sample);
+      if (sigma0 != sigma0) {
+        rec.data[k] = NAN;
+        rec.cos[k] = NAN;
+        rec.omask[k] = SD_MASK_OUTSIDE_FOOTPRINT;
+        rec.ocls[k] = 2;
+        continue;
+      }
+      sigma0 /= e.wdiv;
+      uint8_t m = SD_MASK_VALID, cls = 0;
+      if (p.nesz_mask) {
+        const float nz = sample_bilinear(p.nesz, p.lines, p.samples, e.line, e.sample);
+        if (nz == nz) {
+          const float thr = nz * p.nesz_factor;
+          if (fabsf(sigma0 - thr) <= 1e-5f * fabsf(thr)) {
+            atomicOr(p.cc + i, (uint32_t)CF_REDO);
+            atomicAdd(&p.flags[3], 1);
+            continue;
+          }
+          if (sigma0 <= thr) {
+            sigma0 = NAN;
+            m = SD_MASK_NOISE_MASKED;
+            cls = 6;
+          }
+        }
+      }
+      rec.data[k] = sigma0;
+      rec.omask[k] = m;
+      rec.ocls[k] = cls;
+    }
+    if (lane == 0) atomicAdd(&p.flags[4], (int)n);
+  }
+}
+
 // ── k_redo (split precision): FP64 outputs for the flagged pixels ──────────
-// Pixels whose FP32 result fell inside its error margin (near-cancelling
-// resampling, or a mask decision at a threshold) get both members of F
-// recomputed with the FP64 candidate here, outside k_main's warps.
+// Pixels with a mask decision inside its FP32 margin (or more queued
+// re-samples than their item holds) get both members of F recomputed with
+// the FP64 candidate here, outside k_main's warps; flags[3] counts them.
 template <int KERNEL>
 __global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__ wp) {
+  // flagged pixels are sparse: each block first compacts the flagged pixels
+  // of a REDO_CHUNK into shared memory, then runs them densely
+  __shared__ uint16_t list[REDO_CHUNK];
+  __shared__ int n_list;
   const TcWork w = *wp;
-  const uint64_t *pre = stage_pre(w, WK_SEL);
+  const uint64_t *pre = stage_pre(w, WK_REDO);
   const uint64_t total = pre[w.n_jobs];
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
     const int jb = find_job(pre, w.n_jobs, item);
     const TcDev &p = w.jobs[jb];
-    const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
-    if (i >= p.rows * p.cols) continue;
-    const uint32_t cc = p.cc[i];
-    if (!(cc & CF_REDO)) continue;
-    const uint64_t r = i / p.cols, c = i % p.cols;
-    PixGeo g;
-    float h4[4] = {NAN, NAN, NAN, NAN};
-    const float *hp = nullptr;
-    if (p.hc) {
-      pixel_lonlat(p, r, c, &g.lon, &g.lat);
-      pixel_ecef(p, &g, p.hc[i]);
-      const float4 q4 = p.hnb[i];
-      h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
-      hp = h4;
-    } else if (!pixel_geo(p, r, c, &g)) {
-      continue;
+    if (p.flags[3] == 0) continue;  // nothing flagged in this job (uniform over the block)
+    const uint64_t npx = p.rows * p.cols;
+    const uint64_t base = (item - pre[jb]) * REDO_CHUNK;
+    __syncthreads();  // the previous item is done with the list
+    if (threadIdx.x == 0) n_list = 0;
+    __syncthreads();
+    for (int k = 0; k < REDO_CHUNK / SEL_THREADS; ++k) {
+      const uint64_t i = base + (uint64_t)k * SEL_THREADS + threadIdx.x;
+      if (i < npx && (p.cc[i] & CF_REDO)) list[atomicAdd(&n_list, 1)] = (uint16_t)(i - base);
     }
-    Rec rec = p.rec[i];
-    const int fmask = (int)((cc >> 16) & 3u);
-    const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
-    atomicAdd(&p.flags[2], 1);
-    for (int k = 0; k < 2; ++k) {
-      if (!((fmask >> k) & 1)) continue;
-      OrbitState os;
-      double vsq;
-      if (orbit_at(p.orb, rec.fb + k, &os, &vsq) != ORB_OK) continue;
-      const CandOut o = cand_fp64<KERNEL>(p, g, os.pos, rec.fb + k, flat_area, hp);
-      rec.data[k] = o.data;
-      rec.cos[k] = o.cos;
-      rec.omask[k] = o.mask;
-      rec.ocls[k] = o.cls;
+    __syncthreads();
+    const int n = n_list;
+    if (n > 0 && threadIdx.x == 0) atomicAdd(&p.flags[2], n);
+    for (int q = threadIdx.x; q < n; q += SEL_THREADS) {
+      const uint64_t i = base + list[q];
+      const uint32_t cc = p.cc[i];
+      const uint64_t r = i / p.cols, c = i % p.cols;
+      PixGeo g;
+      float h4[4] = {NAN, NAN, NAN, NAN};
+      const float *hp = nullptr;
+      if (p.hc) {
+        pixel_lonlat(p, r, c, &g.lon, &g.lat);
+        pixel_ecef(p, &g, p.hc[i]);
+        const float4 q4 = p.hnb[i];
+        h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
+        hp = h4;
+      } else if (!pixel_geo(p, r, c, &g)) {
+        continue;
+      }
+      Rec rec = p.rec[i];
+      const int fmask = (int)((cc >> 16) & 3u);
+      const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+      for (int k = 0; k < 2; ++k) {
+        if (!((fmask >> k) & 1)) continue;
+        OrbitState os;
+        double vsq;
+        if (orbit_at(p.orb, rec.fb + k, &os, &vsq) != ORB_OK) continue;
+        const CandOut o = cand_fp64<KERNEL>(p, g, os.pos, rec.fb + k, flat_area, hp);
+        rec.data[k] = o.data;
+        rec.cos[k] = o.cos;
+        rec.omask[k] = o.mask;
+        rec.ocls[k] = o.cls;
+      }
+      p.rec[i] = rec;
     }
-    p.rec[i] = rec;
   }
 }
 
@@ -1955,6 +2084,7 @@ uint64_t stage_items(int stage, const TcDev &p) {
     case WK_KNOT: return p.rows * KNOTS;
     case WK_MAIN: return p.rows * p.bpr;
     case WK_SCAN: return p.rows;
+    case WK_REDO: return (p.rows * p.cols + REDO_CHUNK - 1) / REDO_CHUNK;
     default: return (p.rows * p.cols + SEL_THREADS - 1) / SEL_THREADS;
   }
 }
@@ -2042,8 +2172,12 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
   SD_LAUNCHED(ctx);
   }
   if (S) {
+    SD_TIMED_BEGIN(ctx, "k_resample");
+    k_resample<K><<<persistent_grid(k_resample<K>, SEL_THREADS, 0, blocks_for(totals[WK_MAIN], SEL_THREADS / 32)),
+                    SEL_THREADS, 0, st>>>(d_work);
+    SD_LAUNCHED(ctx);
     SD_TIMED_BEGIN(ctx, "k_redo");
-    k_redo<K><<<persistent_grid(k_redo<K>, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
+    k_redo<K><<<persistent_grid(k_redo<K>, SEL_THREADS, 0, totals[WK_REDO]), SEL_THREADS, 0, st>>>(d_work);
     SD_LAUNCHED(ctx);
   }
   SD_TIMED_BEGIN(ctx, "k_scan");

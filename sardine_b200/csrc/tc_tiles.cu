@@ -397,7 +397,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     return o;
   };
   struct Offs {
-    size_t guess, flat, knots, alon, alat, aloc, hc, hnb, rec, cc, sel, hout[3], fin[3];
+    size_t guess, flat, knots, alon, alat, aloc, hc, hnb, rec, cc, sel, rscnt, rsent, hout[3], fin[3];
   };
   std::vector<Offs> of(n);
   size_t ax_total = 0;
@@ -420,6 +420,11 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     o.rec = take(npx * sizeof(Rec));
     o.cc = take(npx * 4);
     o.sel = take(npx);
+    o.rscnt = o.rsent = SIZE_MAX;
+    if (tiles[i].cfg.precision == SD_PRECISION_SPLIT) {
+      o.rscnt = take(p.rows * p.bpr * 4);
+      o.rsent = take(p.rows * p.bpr * RS_CAP * sizeof(RsEnt));
+    }
     for (int k = 0; k < 3; ++k) {
       o.hout[k] = o.fin[k] = SIZE_MAX;
       const size_t esz = k == 2 ? 1 : 4;
@@ -435,7 +440,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
   unsigned long long *d_cnt = nullptr;
   int *d_flg = nullptr;
   SD_TRY(scratch_t(ctx, "tiles.counters", n * 32, &d_cnt));
-  SD_TRY(scratch_t(ctx, "tiles.flags", n * 4, &d_flg));
+  SD_TRY(scratch_t(ctx, "tiles.flags", n * 8, &d_flg));
   if (ctx->tile_cap < n) {
     if (ctx->h_tile_counters) cudaFreeHost(ctx->h_tile_counters);
     if (ctx->h_tile_flags) cudaFreeHost(ctx->h_tile_flags);
@@ -443,7 +448,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     ctx->h_tile_flags = nullptr;
     ctx->tile_cap = 0;
     SD_CUDA(ctx, cudaHostAlloc((void **)&ctx->h_tile_counters, n * 32 * 8, cudaHostAllocDefault));
-    SD_CUDA(ctx, cudaHostAlloc((void **)&ctx->h_tile_flags, n * 4 * 4, cudaHostAllocDefault));
+    SD_CUDA(ctx, cudaHostAlloc((void **)&ctx->h_tile_flags, n * 8 * 4, cudaHostAllocDefault));
     ctx->tile_cap = n;
   }
   if (!ctx->tiles_done) SD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->tiles_done, cudaEventDisableTiming));
@@ -475,6 +480,8 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     p.rec = (Rec *)(arena + o.rec);
     p.cc = (uint32_t *)(arena + o.cc);
     p.sel = (uint8_t *)(arena + o.sel);
+    p.rs_cnt = o.rscnt != SIZE_MAX ? (uint32_t *)(arena + o.rscnt) : nullptr;
+    p.rs_ent = o.rsent != SIZE_MAX ? (RsEnt *)(arena + o.rsent) : nullptr;
     for (int k = 0; k < 3; ++k) {
       if (pl.final_bytes[k] == 0) continue;
       pl.dev_final[k] = o.fin[k] != SIZE_MAX ? (void *)(arena + o.fin[k]) : pl.user[k];
@@ -487,7 +494,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     p.mask = (uint8_t *)tc_out[2];
     p.az_time = nullptr;
     p.counters = d_cnt + 32 * i;
-    p.flags = d_flg + 4 * i;
+    p.flags = d_flg + 8 * i;
     p.trange = nullptr;
     const int g = tiles[i].cfg.precision == SD_PRECISION_SPLIT ? 1 : 0;
     p.split = g;
@@ -528,7 +535,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
       SD_TRY(fork_main_per_tile(ctx, grp[g]));
       SD_TRY(launch_pixels_batch(ctx, d_work, wk.totals, split, false));
     } else if (use_graph) {
-      static const uint64_t kFull[kWk] = {~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull};
+      static const uint64_t kFull[kWk] = {~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull};
       SD_TRY(run_graph(ctx, g + 2 * ctx->main_cps, d_work, [&]() -> int {
         SD_TRY(launch_rows(ctx, d_work, kFull));
         return launch_pixels_batch(ctx, d_work, kFull, split);
@@ -579,7 +586,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
         SD_CUDA(ctx, cudaMemcpyAsync(plans[i].user[k], plans[i].dev_final[k], plans[i].final_bytes[k],
                                      cudaMemcpyDeviceToHost, st));
   SD_CUDA(ctx, cudaMemcpyAsync(ctx->h_tile_counters, d_cnt, n * 32 * 8, cudaMemcpyDeviceToHost, st));
-  SD_CUDA(ctx, cudaMemcpyAsync(ctx->h_tile_flags, d_flg, n * 4 * 4, cudaMemcpyDeviceToHost, st));
+  SD_CUDA(ctx, cudaMemcpyAsync(ctx->h_tile_flags, d_flg, n * 8 * 4, cudaMemcpyDeviceToHost, st));
   SD_CUDA(ctx, cudaEventRecord(ctx->tiles_done, st));
   ctx->tile_info.assign(n, sd_geocoded_info{});
   for (uint64_t i = 0; i < n; ++i) {
@@ -630,9 +637,10 @@ extern "C" int sd_tc_tiles_finish(sd_ctx *ctx, sd_geocoded_info *infos, uint64_t
     f.flat_masked_count = c[5];
     f.noise_masked_count = c[6];
     for (int k = 0; k < SD_NEWTON_ITER_HIST_SIZE; ++k) f.newton_iter_histogram[k] = c[kCounters + k];
-    f.diag_exact_path_pixels = (uint64_t)ctx->h_tile_flags[4 * i + 1];
-    f.diag_fp64_redo_pixels = (uint64_t)ctx->h_tile_flags[4 * i + 2];
-    if (ctx->h_tile_flags[4 * i] && orbit_bad < 0) orbit_bad = (int)i;
+    f.diag_exact_path_pixels = (uint64_t)ctx->h_tile_flags[8 * i + 1];
+    f.diag_fp64_redo_pixels = (uint64_t)ctx->h_tile_flags[8 * i + 2];
+    f.diag_fp64_resampled = (uint64_t)ctx->h_tile_flags[8 * i + 4];
+    if (ctx->h_tile_flags[8 * i] && orbit_bad < 0) orbit_bad = (int)i;
     infos[i] = f;
   }
   if (orbit_bad >= 0)
@@ -664,7 +672,7 @@ extern "C" int sd_ctx_reserve(sd_ctx *ctx, uint64_t tile_arena_bytes) {
   SD_TRY(scratch(ctx, "tiles.work1", work_bytes(1024), &p));
   SD_TRY(scratch(ctx, "tiles.spwork", 64 + al256(1024 * sizeof(SpJob)) + 1025 * 8, &p));
   SD_TRY(scratch(ctx, "tiles.counters", 1024 * 32 * 8, &p));
-  SD_TRY(scratch(ctx, "tiles.flags", 1024 * 4 * 4, &p));
+  SD_TRY(scratch(ctx, "tiles.flags", 1024 * 8 * 4, &p));
   SD_TRY(scratch(ctx, "tiles.ax", 1024 * 257 * 8, &p));
   return SD_OK;
 }

@@ -108,7 +108,12 @@ class TileRequest:
         r, c = self.rows + 2 * h, self.cols + 2 * h
         anchors = min(256, c) + 1 if self.config.crs.kind != _abi.CRS_WGS84 else 0
         per_row = 8 + 8 + 17 * 8 + (16 + 64) * anchors
-        return r * c * (20 + 32 + 4 + 1 + 9) + r * per_row + self.rows * self.cols * 9 + 8192
+        extra = 0
+        if self.config.precision == T.Precision.SPLIT:
+            # FP64 re-sample queue: per k_main item (255 px) a count and 64 x 24 B
+            per_row += -(-c // 255) * (4 + 64 * 24)
+            extra = 512
+        return r * c * (20 + 32 + 4 + 1 + 9) + r * per_row + self.rows * self.cols * 9 + 8192 + extra
 
 
 def _tile_to_c(req: TileRequest, outs, anchors: int) -> _abi.Tile:

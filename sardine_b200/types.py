@@ -413,6 +413,7 @@ class GeocodedImage:
     newton_iter_histogram: List[int]
     diag_exact_path_pixels: int = 0  # converged pixels computed on the row walk's exact path
     diag_fp64_redo_pixels: int = 0   # split precision: pixels recomputed in FP64
+    diag_fp64_resampled: int = 0     # split precision: candidates re-sampled in FP64
     azimuth_time_us: Any = None      # converged zero-Doppler time per pixel (INT64_MIN: none)
 
     def valid_fraction(self) -> float:
@@ -435,7 +436,8 @@ class GeocodedImage:
             geotransform=tuple(info.geotransform), crs=crs, cos_lia=cos_lia, mask=mask,
             newton_iter_histogram=[int(x) for x in info.newton_iter_histogram],
             diag_exact_path_pixels=int(info.diag_exact_path_pixels),
-            diag_fp64_redo_pixels=int(info.diag_fp64_redo_pixels))
+            diag_fp64_redo_pixels=int(info.diag_fp64_redo_pixels),
+            diag_fp64_resampled=int(info.diag_fp64_resampled))
 
 
 # ── speckle ────────────────────────────────────────────────────────────────
