@@ -1237,7 +1237,8 @@ struct __align__(16) Rec {
   uint32_t pad;
 };
 enum : uint32_t { CF_DEMMISS = 1u << 18, CF_HASF = 1u << 19, CF_HASOUT = 1u << 20,
-                  CF_REDO = 1u << 21 /* split: outputs to be redone in FP64 (k_redo) */ };
+                  CF_REDO = 1u << 21 /* split: outputs to be redone in FP64 (k_redo) */,
+                  CF_OUT0 = 1u << 22 /* bits 22-23: members whose outputs Rec holds */ };
 // sel byte written by the scan: low 3 bits = outcome, high 4 bits = iterations
 enum : uint8_t { SEL_M0 = 0, SEL_M1 = 1, SEL_DONE = 2, SEL_NONCONV = 3, SEL_DEGEN = 4, SEL_DEMMISS = 5,
                  SEL_ORBIT = 6 };
@@ -1537,20 +1538,35 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         cc = (cc & ~(0xFFu << (8 * k))) | (code << (8 * k));
       }
     }
-    // outputs for both members of F
+    // Outputs only for the members the row walk can select through the codes
+    // (the left neighbour's F members that converge here); both at a row
+    // start, after a void or when no code converges.  A walk from an
+    // explicit seed that lands on a member without outputs computes it
+    // there (exact_pixel).
+    int outm = fmask;
+    if (c > 0 && L.fmask) {
+      int reach = 0;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const uint32_t code = (cc >> (8 * k)) & 0xFFu;
+        if (((L.fmask >> k) & 1) && code != 0xFFu && (code & 3u) < 2u) reach |= 1 << (code & 1u);
+      }
+      if (reach & fmask) outm = reach & fmask;
+    }
+    cc |= (uint32_t)outm * CF_OUT0;
     CandPre pre[2];
     bool need = false;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const Ent &e = k == 0 ? e0 : e1;
-      if ((fmask >> k) & 1) {
+      if ((outm >> k) & 1) {
         pre[k] = cand_geom(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
       } else {
         pre[k].inside = false;
       }
     }
     bool defer = false;
-    resample_members<KERNEL, SPLIT>(p, pre, fmask);
+    resample_members<KERNEL, SPLIT>(p, pre, outm);
     need = pre[0].inside || pre[1].inside;
     const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
     if constexpr (SPLIT) {
@@ -1567,7 +1583,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const Ent &e = k == 0 ? e0 : e1;
-        if (!((fmask >> k) & 1)) continue;
+        if (!((outm >> k) & 1)) continue;
         const V3 S{e.px, e.py, e.pz};
         int redo;
         float wd;
@@ -1600,7 +1616,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         const Ent &e = k == 0 ? e0 : e1;
-        if (!((fmask >> k) & 1)) continue;
+        if (!((outm >> k) & 1)) continue;
         CandOut o = cand_post(p, pre[k], g.P, V3{e.px, e.py, e.pz}, f, flat_area);
         rec.data[k] = o.data;
         rec.cos[k] = o.cos;
@@ -1764,10 +1780,10 @@ __global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__
         continue;
       }
       Rec rec = p.rec[i];
-      const int fmask = (int)((cc >> 16) & 3u);
+      const int outm = (int)((cc >> 22) & 3u);  // members k_main gave outputs
       const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
       for (int k = 0; k < 2; ++k) {
-        if (!((fmask >> k) & 1)) continue;
+        if (!((outm >> k) & 1)) continue;
         OrbitState os;
         double vsq;
         if (orbit_at(p.orb, rec.fb + k, &os, &vsq) != ORB_OK) continue;
@@ -1819,6 +1835,17 @@ __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s,
     const uint32_t fm = (cc >> 16) & 3u;
     const int64_t m = z.t - fb;
     if ((m == 0 || m == 1) && ((fm >> m) & 1)) {
+      if (write && !((cc >> (22 + m)) & 1u)) {  // k_main left this member's outputs out
+        OrbitState os;
+        double vsq;
+        orbit_at(p.orb, z.t, &os, &vsq);
+        const CandOut o = cand_full<KERNEL, SPLIT>(p, g, os.pos, z.t, p.need_geom ? p.row_flat[r] : 0.0, nullptr);
+        Rec &rc = p.rec[i];
+        rc.data[m] = o.data;
+        rc.cos[m] = o.cos;
+        rc.omask[m] = o.mask;
+        rc.ocls[m] = o.cls;
+      }
       *sel = (uint8_t)(m | (it << 4));
       return {0, m};
     }
