@@ -6,10 +6,11 @@ config-2 shape (3 sub-swaths x 9 bursts x 1500 x 21000 CInt16, calibrated,
 debursted and merged on the device, then resident in HBM with their 10 m UTM
 DEM and orbit) receive Poisson streams of tile requests (sides 256-2048
 log-uniform, random scene, bounding box, resampler and speckle filter, split
-precision) at 100, 500 and 2000 req/s.  A continuous-batching loop admits
-them by HBM budget into two overlapping slots.  `value` = geocoded output
-pixels per second of device time at the highest rate; p50/p99 request
-latency per rate; the plain per-request FP64 path on the same GPU beside it.
+precision) at 100, 500 and 2000 req/s, then all queued at once ('max').  A
+continuous-batching loop admits them by HBM budget into two overlapping
+slots.  `value` = geocoded output pixels per second of device time with every
+request queued at once (the saturated throughput); p50/p99 request latency
+per Poisson rate; the plain per-request FP64 path on the same GPU beside it.
 
 Other workloads: --config c2 (one full IW scene per step: fused
 calibration+deburst+merge then terrain correction onto 25000 x 20000 UTM
@@ -30,6 +31,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -683,6 +685,18 @@ def _c5_requests(sd, scenes, rng, n, precision):
     return reqs
 
 
+def _arrivals(rng, rate, n):
+    """Poisson arrival offsets (s) at `rate` req/s; rate inf ('max') queues
+    every request at once, which measures the saturated throughput."""
+    if math.isinf(rate):
+        return np.zeros(n)
+    return np.cumsum(rng.exponential(1.0 / rate, n))
+
+
+def _rate_key(rate):
+    return "max" if math.isinf(rate) else str(int(rate))
+
+
 def _serve(server, reqs, arrivals, clock=time.perf_counter):
     """Feeds requests at their arrival offsets (s) and runs the loop dry."""
     t0 = clock()
@@ -709,7 +723,7 @@ def run_c5(args):
     dev = f"cuda:{local}"
     scenes = _c5_setup(sd, ctx, dev, rank, args.scenes)
     rng = np.random.default_rng(5 + rank)
-    rates = [float(r) for r in args.rates.split(",")]
+    rates = [math.inf if r.strip() == "max" else float(r) for r in args.rates.split(",")]
     budget = args.budget_gb << 30
     server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=64, graphs=True)
     sample = _c5_requests(sd, scenes, rng, 64, sd.Precision.SPLIT)
@@ -718,15 +732,17 @@ def run_c5(args):
         tune = autotune.tune(s.ctx, sample[:32])
     for _ in range(args.warmup):  # graph capture, allocator, autotuned shapes in place
         reqs = _c5_requests(sd, scenes, rng, args.burst // 4, sd.Precision.SPLIT)
-        _serve(server, reqs, np.cumsum(rng.exponential(1.0 / rates[-1], len(reqs))))
+        _serve(server, reqs, _arrivals(rng, rates[-1], len(reqs)))
     by_rate = {}
+    lat = None
     value = ms = None
     gpu_launches = 0
     clk_summary = None
     for rate in rates:
-        n = args.burst * args.steps if rate == rates[-1] else int(max(64, min(args.burst * args.steps, rate * 3)))
+        n = (args.burst * args.steps if rate == rates[-1] or math.isinf(rate)
+             else int(max(64, min(args.burst * args.steps, rate * 3))))
         reqs = _c5_requests(sd, scenes, rng, n, sd.Precision.SPLIT)
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        arrivals = _arrivals(rng, rate, n)
         l0 = sum(s.ctx.launches for s in server.slots)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(local) as clk:
@@ -737,15 +753,16 @@ def run_c5(args):
             e1.record()
             torch.cuda.synchronize()
         summ = latency_summary(tickets)
-        summ["rate_req_s"] = rate
+        summ["rate_req_s"] = _rate_key(rate)
         summ["requests"] = n
-        by_rate[str(int(rate))] = summ
+        by_rate[_rate_key(rate)] = summ
+        if not math.isinf(rate):
+            lat = (rate, summ)
         if rate == rates[-1]:
             ms = _max_over_ranks(dist, e0.elapsed_time(e1))
             value = _sum_over_ranks(dist, summ["px"]) / (ms / 1e3)
             gpu_launches = sum(s.ctx.launches for s in server.slots) - l0
             clk_summary = clk.summary()
-            head = summ
     # end to end: the headline stream again, each result copied to host memory
     # as it completes (the D2H is inside the latency)
     host_buf = torch.empty(3 * 2048 * 2048 * 4 + 4096, dtype=torch.uint8, pin_memory=True)
@@ -766,7 +783,7 @@ def run_c5(args):
         autotune.apply(s.ctx, tune)
     n = args.burst * args.steps
     reqs = _c5_requests(sd, scenes, rng, n, sd.Precision.SPLIT)
-    arrivals = np.cumsum(rng.exponential(1.0 / rates[-1], n))
+    arrivals = _arrivals(rng, rates[-1], n)
     _serve(e2e_server, reqs[:16], arrivals[:16])
     d2h[0] = 0
     t0 = time.perf_counter()
@@ -781,7 +798,7 @@ def run_c5(args):
     base = GeocodingServer(local, hbm_budget=4 << 30, slots=1, max_batch=1, graphs=False)
     nb = max(64, args.burst * args.steps // 2)
     breqs = _c5_requests(sd, scenes, np.random.default_rng(55 + rank), nb, sd.Precision.FP64)
-    barr = np.cumsum(np.random.default_rng(56).exponential(1.0 / rates[-1], nb))
+    barr = _arrivals(np.random.default_rng(56), rates[-1], nb)
     _serve(base, breqs[:8], barr[:8])
     bsum = latency_summary(_serve(base, breqs, barr))
     acc = _split_vs_fp64(sd, tiles, server.slots[0].ctx, scenes, rng)
@@ -800,13 +817,15 @@ def run_c5(args):
             "config": {"workload": (f"config5: {args.scenes} config-2-shape scenes resident (merged sigma0+NESZ, "
                                     "DEM, orbit table); Poisson tile requests, sides 256-2048 log-uniform, "
                                     "random scene/bbox/resampler/speckle, split precision, continuous batching "
-                                    "over 2 slots, HBM-budget admission; value at the highest rate"),
-                       "rates_req_s": rates, "burst_per_step": args.burst,
+                                    "over 2 slots, HBM-budget admission; value at the last rate ('max': "
+                                    "every request queued at once = saturated throughput)"),
+                       "rates_req_s": [_rate_key(r) for r in rates], "burst_per_step": args.burst,
                        "hbm_budget_gb": args.budget_gb, "autotune": tune,
                        "scene_device_gb": round(sum(s["rs"].device_bytes for s in scenes) / 2**30, 2),
                        "parallelism": f"replicas x{world}"},
-            "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"], "mean": head["mean_ms"],
-                           "what": f"request submit -> results on the device, at {rates[-1]:.0f} req/s"},
+            "latency_ms": ({"p50": lat[1]["p50_ms"], "p99": lat[1]["p99_ms"], "mean": lat[1]["mean_ms"],
+                            "what": f"request submit -> results on the device, at {lat[0]:.0f} req/s (Poisson)"}
+                           if lat else None),
             "served_by_rate": by_rate,
             "per_request_fp64": bsum,
             "accuracy_split_vs_fp64": acc,
@@ -1053,7 +1072,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4"])
-    ap.add_argument("--rates", default="100,500,2000", help="config5 request rates (req/s); value at the last")
+    ap.add_argument("--rates", default="100,500,2000,max",
+                    help="config5 request rates (req/s; 'max' queues every request at once); value at the last")
     ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
     ap.add_argument("--scenes", type=int, default=8, help="config5 resident scenes")
     ap.add_argument("--budget-gb", dest="budget_gb", type=int, default=16, help="config5 HBM budget")

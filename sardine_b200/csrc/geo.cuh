@@ -384,7 +384,8 @@ SD_HD bool dem_at_lonlat(const DemView &d, double lon_deg, double lat_deg, float
 SD_HD double geoid_undulation(const float *g, double lat_deg, double lon_deg) {
   if (g == nullptr) return 0.0;
   const uint64_t NLAT = 73, NLON = 144;
-  double lon = fmod(lon_deg, 360.0);
+  // fmod(x, 360) is x itself for |x| < 360 (exactly, sign included)
+  double lon = (lon_deg < 360.0 && lon_deg > -360.0) ? lon_deg : fmod(lon_deg, 360.0);
   if (lon < 0.0) lon += 360.0;
   double row_f = (90.0 - clampd(lat_deg, -90.0, 90.0)) / 2.5;
   double col_f = lon / 2.5;
