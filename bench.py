@@ -54,6 +54,8 @@ UNIT = "px/s"
 #    + 90 (target ECEF, slant range, image coordinates) + 150 (4 neighbour
 #    ECEF + facet normal + flattening/LIA), N_it = mean Newton iterations.
 PREP_BYTES_PER_PX = 12.0
+# every kernel of the terrain-correction stage (the FP64 roofline's time)
+TC_STAGE = ("k_main", "k_heights", "k_resample", "k_redo", "k_scan", "k_select", "k_row")
 TC_FLOPS = lambda n_it: n_it * 430.0 + 90.0 + 150.0
 
 
@@ -218,7 +220,7 @@ def run_ours(args):
     kt = ctx.kernel_times()
     ctx.set_timing(False)
     total_k = sum(v[0] for v in kt.values()) or 1.0
-    tc_names = [k for k in kt if k.startswith(("k_main", "k_scan", "k_select", "k_row", "k_orbit"))]
+    tc_names = [k for k in kt if k.startswith(TC_STAGE + ("k_orbit",))]
     tc_ms = sum(kt[k][0] for k in tc_names)
     prep_ms = sum(kt[k][0] for k in kt if k.startswith(("k_fused", "k_lut_table")))
     peaks = {}
@@ -529,13 +531,13 @@ def run_c4(args):
     total_k = sum(v[0] for v in kt.values()) or 1.0
     hist = np.sum([r.newton_iter_histogram for r in res], axis=0)
     n_it = n_iter_mean(hist)
-    tc_ms = sum(v[0] for k, v in kt.items() if k.startswith(("k_main", "k_scan", "k_select", "k_row")))
+    tc_ms = sum(v[0] for k, v in kt.items() if k.startswith(TC_STAGE))
     fp64 = ctypes_fp64_peak(ctx)
     tc_tf = TC_FLOPS(n_it) * px_step / (tc_ms / 1e3) / 1e12 if tc_ms else None
     sp_ms = kt.get("k_speckle_tiles", (0.0, 0))[0]
     hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
     sp_gbs = 9.0 * px_step / (sp_ms / 1e3) / 1e9 if sp_ms else None
-    roofline = {"bound": "fp64", "kernel": "tile geocoding (k_main_batch+k_scan+k_select+k_row*)",
+    roofline = {"bound": "fp64", "kernel": "tile geocoding (" + "+".join(sorted(k for k in kt if k.startswith(TC_STAGE))) + ")",
                 "achieved": tc_tf, "peak": fp64, "unit": "TFLOP/s",
                 "frac": tc_tf / fp64 if (tc_tf and fp64) else None, "traffic": None,
                 "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
@@ -583,14 +585,14 @@ def _tile_roofline(sd, tiles, ctx, reqs):
     px = sum(r.rows * r.cols for r in reqs)
     hist = np.sum([r.newton_iter_histogram for r in res], axis=0)
     n_it = n_iter_mean(hist)
-    tc_ms = sum(v[0] for k, v in kt.items() if k.startswith(("k_main", "k_scan", "k_select", "k_row")))
+    tc_ms = sum(v[0] for k, v in kt.items() if k.startswith(TC_STAGE))
     sp_ms = kt.get("k_speckle_tiles", (0.0, 0))[0]
     fp64 = ctypes_fp64_peak(ctx)
     hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
     tf = TC_FLOPS(n_it) * px / (tc_ms / 1e3) / 1e12 if tc_ms else None
     gbs = 9.0 * px / (sp_ms / 1e3) / 1e9 if sp_ms else None
     total = sum(v[0] for v in kt.values()) or 1.0
-    roof = {"bound": "fp64", "kernel": "tile geocoding (" + "+".join(sorted(k for k in kt if k.startswith(("k_main", "k_scan", "k_select", "k_row")))) + ")",
+    roof = {"bound": "fp64", "kernel": "tile geocoding (" + "+".join(sorted(k for k in kt if k.startswith(TC_STAGE))) + ")",
             "achieved": tf, "peak": fp64, "unit": "TFLOP/s", "frac": tf / fp64 if (tf and fp64) else None,
             "traffic": None, "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
             "batch": f"{len(reqs)} tiles, {px} px",
@@ -887,6 +889,118 @@ def _split_vs_fp64(sd, tiles, ctx, scenes, rng, n=8):
     return worst
 
 
+def _hbm_peak():
+    """Measured HBM copy bandwidth (GB/s), else the fallback figure."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    except Exception:
+        return 6650.0
+
+
+def run_export(args):
+    """The output stage of the reference pipeline (run.rs:394-450):
+    to_db_inplace + compute_db_stats, then write_cog_with_crs (512-px tiles)
+    of a geocoded raster on the config-2 output grid (25000 x 20000 UTM 10 m),
+    resident on the device.  value = output pixels per second of device time
+    of the stage's kernels; e2e = the two public calls end to end, file
+    written to local disk included."""
+    import torch
+    import sardine_b200 as sd
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = _init_dist(world)
+    ctx = sd.Context(local)
+    dev = f"cuda:{local}"
+    rows, cols = (2000, 12000) if args.small else (20000, 25000)
+    n = rows * cols
+    g = torch.Generator(device=dev).manual_seed(7 + rank)
+    src = torch.empty(n, device=dev).exponential_(20.0, generator=g)  # mean 0.05, as calibrated sigma0
+    src[torch.rand(n, device=dev, generator=g) < 0.1] = float("nan")
+    src[torch.rand(n, device=dev, generator=g) < 0.05] = 0.0
+    work = torch.empty_like(src)
+    gt = [500000.0, 10.0, 0.0, 5_200_000.0, 0.0, -10.0]
+    crs = sd.OutputCrs.utm_north(32)
+    path = f"/tmp/sardine_b200_export_r{rank}.tif"
+    ts = 512
+
+    def step():
+        c, st = sd.to_db_inplace(work, 0.0, ctx=ctx, stats=True)
+        sd.write_cog_with_crs(path, work, cols, rows, gt, crs, ts, ctx=ctx)
+        return c, st
+
+    for _ in range(args.warmup):
+        work.copy_(src)
+        step()
+    ctx.set_timing(True)
+    wall = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            work.copy_(src)
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+            t0 = time.perf_counter()
+            counts, stats = step()
+            wall += time.perf_counter() - t0
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    names = ("k_to_db", "k_db_sample", "k_downsample_2x", "k_tile_pack")
+    dev_ms = sum(kt[k][0] for k in names if k in kt) / args.steps
+    dev_ms = _max_over_ranks(dist, dev_ms)
+    wall = _max_over_ranks(dist, wall)
+    # algorithmic bytes per step and kernel
+    lv, c, r = [], (cols + 1) // 2, (rows + 1) // 2
+    while True:
+        lv.append((c, r))
+        if not (c > ts or r > ts):
+            break
+        c, r = (c + 1) // 2, (r + 1) // 2
+    ds_bytes = 4 * (cols * rows + sum(a * b for a, b in lv[:-1])) + 4 * sum(a * b for a, b in lv)
+    tiles = lambda a, b: -(-a // ts) * -(-b // ts)
+    pack_bytes = sum(4 * a * b + 4 * tiles(a, b) * ts * ts for a, b in lv + [(cols, rows)])
+    alg = {"k_to_db": 8 * n, "k_db_sample": 4 * n, "k_downsample_2x": ds_bytes, "k_tile_pack": pack_bytes}
+    per_k = {k: {"ms": round(kt[k][0] / args.steps, 3), "launches": kt[k][1] // args.steps,
+                 "gbs": round(alg[k] / (kt[k][0] / args.steps / 1e3) / 1e9, 1)} for k in names if k in kt}
+    dom = max(per_k, key=lambda k: per_k[k]["ms"])
+    peak = _hbm_peak()
+    roof = {"bound": "hbm", "kernel": dom, "achieved": per_k[dom]["gbs"], "peak": peak, "unit": "GB/s",
+            "frac": per_k[dom]["gbs"] / peak, "traffic": None,
+            "bytes_per_step": alg[dom], "stage_gbs": round(sum(alg.values()) / (dev_ms / 1e3) / 1e9, 1)}
+    file_bytes = os.path.getsize(path)
+    cpu = None
+    if args.cpu_baseline and world == 1 and rank == 0:
+        import oracle
+        band = min(rows, 1000)
+        sample = src[: band * cols].cpu().numpy().copy()
+        t0 = time.perf_counter()
+        oracle.to_db_inplace(sample, 0.0)
+        oracle.db_stats(sample)
+        oracle.write_cog(path + ".cpu", sample, cols, band, gt, crs, ts)
+        cpu_s = (time.perf_counter() - t0) * rows / band
+        os.remove(path + ".cpu")
+        cpu = {"value": n / cpu_s, "unit": "px/s", "cores": 1, "kind": "port",
+               "sample": f"oracle to_db + stats + COG writer on {band} of {rows} rows, scaled to all rows"}
+    os.remove(path)
+    if rank == 0:
+        out = {
+            "metric": "output px/s", "value": world * n / (dev_ms / 1e3), "unit": "px/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 sums)",
+            "data": "synthetic (seeded exponential sigma0 with NaN and zero pixels)",
+            "config": {"workload": f"export: to_db + dB stats + COG (tile {ts}) of a {rows}x{cols} geocoded raster"
+                                   + (" (REDUCED SHAPE)" if args.small else ""),
+                       "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+            "kernels": per_k, "roofline": roof, "counts": list(counts), "db_stats": list(stats),
+            "cpu_baseline": cpu, "gpu_launches": sum(v["launches"] for v in per_k.values()),
+            "clocks": clk.summary(),
+            "e2e": {"value": world * n / (wall / args.steps), "unit": "px/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": file_bytes, "file_bytes": file_bytes,
+                    "api": "sardine_b200.to_db_inplace + write_cog_with_crs, file on local disk"},
+        }
+        print(json.dumps(out), flush=True)
+    _finish_dist(dist)
+
+
 def _init_dist(world):
     if world <= 1:
         return None
@@ -1071,7 +1185,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4", "export"])
     ap.add_argument("--rates", default="100,500,2000,max",
                     help="config5 request rates (req/s; 'max' queues every request at once); value at the last")
     ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
@@ -1091,6 +1205,8 @@ def main():
         run_c4(args)
     elif args.config == "c5":
         run_c5(args)
+    elif args.config == "export":
+        run_export(args)
     else:
         run_ours(args)
 

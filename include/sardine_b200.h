@@ -70,7 +70,12 @@ typedef enum sd_status {
     /* MergeError (merge_subswaths.rs:62-81) */
     SD_ERR_MERGE_EMPTY_INPUTS = 50,
     SD_ERR_MERGE_INCONSISTENT_PIXEL_SPACING = 51,
-    SD_ERR_MERGE_EMPTY_SWATH = 52
+    SD_ERR_MERGE_EMPTY_SWATH = 52,
+    /* ExportError (export.rs:25-40) */
+    SD_ERR_EXPORT_IO = 60,
+    SD_ERR_EXPORT_INVALID_NOISE_FLOOR = 61,
+    SD_ERR_EXPORT_INVALID_GEOTRANSFORM = 62,
+    SD_ERR_EXPORT_INVALID_TILE_SIZE = 63
 } sd_status;
 
 /* ── Enumerations mirroring the reference's enums ─────────────────────── */
@@ -498,6 +503,35 @@ int sd_ctx_set_tile_shape(sd_ctx *ctx, int32_t speckle_tx, int32_t speckle_ty,
  * the state vectors' span or fewer than 8 vectors are given. */
 int sd_orbit_states(sd_ctx *ctx, const sd_state_vector *svs, uint64_t n, const int64_t *t_us,
                     uint64_t m, double *out);
+
+/* ── Output: dB conversion and Cloud-Optimised GeoTIFF ───────────────────
+ * to_db_inplace (export.rs:59-99) on data[0..n) in place (host or device
+ * memory): NaN stays NaN; v <= noise_floor_linear (and any v <= 0) becomes
+ * NaN and is counted as noise-masked; every other value becomes
+ * 10 log10(v) (f32).  counts (may be NULL) receives {converted,
+ * noise_masked}.  stats (may be NULL) receives compute_db_stats
+ * (run.rs:63-97) of the converted raster: {min, max, mean, median} of the
+ * finite values, the mean from an f64 sum, the median of every
+ * max(n_finite / 100000, 1)-th finite value; NaN when none is finite.
+ * SD_ERR_EXPORT_INVALID_NOISE_FLOOR when noise_floor_linear < 0. */
+int sd_to_db(sd_ctx *ctx, float *data, uint64_t n, float noise_floor_linear, uint64_t *counts,
+             float *stats);
+
+/* downsample_2x (export.rs:362-392): dst ((cols+1)/2 x (rows+1)/2) holds the
+ * f64 mean of the non-NaN pixels of each 2x2 patch of src, NaN when all
+ * are NaN.  The overview step of sd_write_cog. */
+int sd_downsample_2x(sd_ctx *ctx, const float *src, uint64_t cols, uint64_t rows, float *dst);
+
+/* write_cog_with_crs (export.rs:329-355, writer 417-760): a single-band
+ * Float32 COG of data (rows x cols, host or device) at `path`: overview
+ * levels by downsample_2x down to one tile, IFDs coarsest first, 17 tags
+ * each, GeoKeys of crs (SD_CRS_*, utm_zone 1..60 for UTM), tiles of
+ * tile_size^2 padded with NaN, BigTIFF when rows*cols*4 exceeds 4 GiB.
+ * Overviews and tiles are built on the device; the host writes the file.
+ * Errors: SD_ERR_EXPORT_INVALID_GEOTRANSFORM, SD_ERR_EXPORT_INVALID_TILE_SIZE
+ * (a power of two in [64, 4096]), SD_ERR_EXPORT_IO. */
+int sd_write_cog(sd_ctx *ctx, const char *path, const float *data, uint64_t cols, uint64_t rows,
+                 const double *geotransform, int32_t crs, int32_t utm_zone, uint32_t tile_size);
 
 /* ── Diagnostics ──────────────────────────────────────────────────────────
  * Runs an FP64 FMA-chain kernel for about `iters` dependent FMAs per thread

@@ -69,6 +69,10 @@ def _declare(L):
         "orc_merge_plan": (C.c_int, [i32, P, P, P, P, P, P]),
         "orc_merge_subswaths": (C.c_int, [i32, P, P, P, P, P, P, P, P, P, P, P, P]),
         "orc_speckle": (C.c_int, [P, u64, u64, u64, C.c_int, u64, f, f, P]),
+        "orc_to_db_inplace": (C.c_int, [P, u64, f, P, P]),
+        "orc_db_stats": (None, [P, u64, P]),
+        "orc_downsample_2x": (None, [P, u64, u64, P]),
+        "orc_write_cog": (C.c_int, [C.c_char_p, P, u64, u64, P, C.c_int, C.c_int, C.c_uint32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -351,3 +355,40 @@ def apply_speckle_filter(data: np.ndarray, cols: int, rows: int, flt: T.SpeckleF
                            flt.damping, out.ctypes.data)
     _check(rc, "apply_speckle_filter")
     return out
+
+
+# ── output path (oracle/export_oracle.cpp) ───────────────────────────────────
+def to_db_inplace(data: np.ndarray, noise_floor_linear: float):
+    """to_db_inplace (export.rs:59-99) on a contiguous float32 array:
+    returns (converted, noise_masked); raises for a negative floor."""
+    assert data.dtype == np.float32 and data.flags.c_contiguous
+    cv, nm = C.c_uint64(), C.c_uint64()
+    rc = lib().orc_to_db_inplace(data.ctypes.data, data.size, float(noise_floor_linear), C.byref(cv),
+                                 C.byref(nm))
+    _check(rc, "to_db_inplace")
+    return int(cv.value), int(nm.value)
+
+
+def db_stats(data: np.ndarray):
+    """compute_db_stats (run.rs:63-97): (min, max, mean, median)."""
+    data = np.ascontiguousarray(data, dtype=np.float32).reshape(-1)
+    out = (C.c_float * 4)()
+    lib().orc_db_stats(data.ctypes.data, data.size, out)
+    return tuple(float(x) for x in out)
+
+
+def downsample_2x(src: np.ndarray, cols: int, rows: int) -> np.ndarray:
+    """downsample_2x (export.rs:362-392)."""
+    src = np.ascontiguousarray(src, dtype=np.float32).reshape(-1)
+    out = np.empty(((rows + 1) // 2, (cols + 1) // 2), np.float32)
+    lib().orc_downsample_2x(src.ctypes.data, cols, rows, out.ctypes.data)
+    return out
+
+
+def write_cog(path: str, data: np.ndarray, cols: int, rows: int, geotransform, crs: T.OutputCrs,
+              tile_size: int = 512) -> int:
+    """write_cog_with_crs (export.rs:329-760); returns the status code."""
+    data = np.ascontiguousarray(data, dtype=np.float32).reshape(-1)
+    gt = (C.c_double * 6)(*[float(x) for x in geotransform])
+    return int(lib().orc_write_cog(os.fsencode(path), data.ctypes.data, cols, rows, gt, int(crs.kind),
+                                   int(crs.zone), int(tile_size)))

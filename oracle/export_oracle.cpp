@@ -1,0 +1,296 @@
+// CPU oracle for the output path: dB conversion, dB statistics, overview
+// downsampling and the Cloud-Optimised GeoTIFF writer.
+//
+// TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline): a plain
+// sequential restatement of the reference's arithmetic and file layout,
+// never linked into the product library.
+//
+//   to_db_inplace          sardine/src/export.rs:59-99
+//   compute_db_stats       sardine/src/run.rs:63-97
+//   downsample_2x          sardine/src/export.rs:362-392
+//   write_cog_with_crs     sardine/src/export.rs:329-355
+//   write_cog_raw_inner    sardine/src/export.rs:417-760
+//   geo_key_directory      sardine/src/output_crs.rs:265-287
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "../include/sardine_b200.h"
+
+namespace {
+
+// GeoKeyDirectoryTag payload (output_crs.rs:265-287).
+std::vector<uint16_t> geo_keys(int crs, int zone) {
+  if (crs == SD_CRS_WGS84) return {1, 1, 0, 3, 1024, 0, 1, 2, 1025, 0, 1, 1, 2048, 0, 1, 4326};
+  const uint16_t epsg = (uint16_t)((crs == SD_CRS_UTM_SOUTH ? 32700 : 32600) + zone);
+  return {1, 1, 0, 4, 1024, 0, 1, 1, 1025, 0, 1, 1, 3072, 0, 1, epsg, 3076, 0, 1, 9001};
+}
+
+// export.rs:362-392: each destination pixel is the f64 mean of the non-NaN,
+// in-range pixels of its 2x2 source patch (row-major order), NaN when none.
+std::vector<float> downsample(const std::vector<float> &src, uint64_t c, uint64_t r, uint64_t *dc,
+                              uint64_t *dr) {
+  const uint64_t oc = (c + 1) / 2, orows = (r + 1) / 2;
+  std::vector<float> dst(oc * orows, NAN);
+  for (uint64_t y = 0; y < orows; ++y)
+    for (uint64_t x = 0; x < oc; ++x) {
+      double sum = 0.0;
+      uint32_t cnt = 0;
+      for (uint64_t a = 0; a < 2; ++a)
+        for (uint64_t b = 0; b < 2; ++b) {
+          const uint64_t sy = 2 * y + a, sx = 2 * x + b;
+          if (sy < r && sx < c) {
+            const float v = src[sy * c + sx];
+            if (!std::isnan(v)) {
+              sum += (double)v;
+              cnt += 1;
+            }
+          }
+        }
+      if (cnt > 0) dst[y * oc + x] = (float)(sum / (double)cnt);
+    }
+  *dc = oc;
+  *dr = orows;
+  return dst;
+}
+
+struct Out {
+  FILE *f;
+  bool ok = true;
+  void bytes(const void *p, size_t n) {
+    if (ok && fwrite(p, 1, n, f) != n) ok = false;
+  }
+  void u16(uint16_t v) { bytes(&v, 2); }
+  void u32(uint32_t v) { bytes(&v, 4); }
+  void u64(uint64_t v) { bytes(&v, 8); }
+  void f64(double v) { bytes(&v, 8); }
+};
+
+}  // namespace
+
+extern "C" {
+
+// to_db_inplace: NaN kept; v <= floor -> NaN (noise-masked); else 10 log10 v.
+int orc_to_db_inplace(float *data, uint64_t n, float noise_floor_linear, uint64_t *converted,
+                      uint64_t *masked) {
+  if (noise_floor_linear < 0.0f) return SD_ERR_EXPORT_INVALID_NOISE_FLOOR;
+  uint64_t cv = 0, nm = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const float v = data[i];
+    if (std::isnan(v)) continue;
+    if (v <= noise_floor_linear) {
+      data[i] = NAN;
+      ++nm;
+    } else {
+      data[i] = 10.0f * std::log10(v);
+      ++cv;
+    }
+  }
+  *converted = cv;
+  *masked = nm;
+  return SD_OK;
+}
+
+// compute_db_stats: min, max, f64 mean of the finite values, and the median
+// of every stride-th finite value (stride = max(n_finite / 100000, 1)).
+void orc_db_stats(const float *data, uint64_t n, float *out) {
+  float mn = INFINITY, mx = -INFINITY;
+  double sum = 0.0;
+  uint64_t cnt = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const float v = data[i];
+    if (!std::isfinite(v)) continue;
+    if (v < mn) mn = v;
+    if (v > mx) mx = v;
+    sum += (double)v;
+    ++cnt;
+  }
+  if (cnt == 0) {
+    out[0] = out[1] = out[2] = out[3] = NAN;
+    return;
+  }
+  const uint64_t stride = std::max<uint64_t>(cnt / 100000, 1);
+  std::vector<float> sample;
+  uint64_t k = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const float v = data[i];
+    if (!std::isfinite(v)) continue;
+    if (k % stride == 0) sample.push_back(v);
+    ++k;
+  }
+  std::sort(sample.begin(), sample.end());
+  out[0] = mn;
+  out[1] = mx;
+  out[2] = (float)(sum / (double)cnt);
+  out[3] = sample[sample.size() / 2];
+}
+
+void orc_downsample_2x(const float *src, uint64_t cols, uint64_t rows, float *dst) {
+  std::vector<float> s(src, src + cols * rows);
+  uint64_t dc, dr;
+  std::vector<float> d = downsample(s, cols, rows, &dc, &dr);
+  std::memcpy(dst, d.data(), d.size() * sizeof(float));
+}
+
+// write_cog_with_crs / write_cog_raw_inner.
+int orc_write_cog(const char *path, const float *data, uint64_t cols, uint64_t rows, const double *gt,
+                  int crs, int zone, uint32_t tile_size) {
+  const double pw = gt[1], ph = -gt[5];
+  if (!std::isfinite(pw) || pw <= 0.0 || !std::isfinite(ph) || ph <= 0.0) return SD_ERR_EXPORT_INVALID_GEOTRANSFORM;
+  if (tile_size < 64 || tile_size > 4096 || (tile_size & (tile_size - 1)) != 0) return SD_ERR_EXPORT_INVALID_TILE_SIZE;
+  const std::vector<uint16_t> keys = geo_keys(crs, zone);
+  const uint64_t ts = tile_size;
+
+  // overview pyramid: finest first, then reversed (coarsest first)
+  struct Level {
+    std::vector<float> d;
+    uint64_t c, r;
+  };
+  std::vector<Level> ov;
+  {
+    std::vector<float> full(data, data + cols * rows);
+    uint64_t c, r;
+    std::vector<float> cur = downsample(full, cols, rows, &c, &r);
+    while (c > ts || r > ts) {
+      ov.push_back({cur, c, r});
+      uint64_t c2, r2;
+      std::vector<float> nxt = downsample(cur, c, r, &c2, &r2);
+      cur = std::move(nxt);
+      c = c2;
+      r = r2;
+    }
+    ov.push_back({cur, c, r});
+  }
+  std::reverse(ov.begin(), ov.end());
+
+  const bool big = rows * cols * 4ull > 0xFFFFFFFFull;
+  auto grid = [&](uint64_t c, uint64_t r) { return ((c + ts - 1) / ts) * ((r + ts - 1) / ts); };
+  const uint64_t entries = 17;
+  const uint64_t ifd_bytes = big ? 8 + entries * 20 + 8 : 2 + entries * 12 + 4;
+  const uint64_t arr_entry = big ? 8 : 4;
+  uint64_t off = big ? 16 : 8;
+
+  std::vector<std::pair<uint64_t, uint64_t>> dims;
+  for (const Level &l : ov) dims.push_back({l.c, l.r});
+  dims.push_back({cols, rows});
+  std::vector<uint64_t> ifd_off, toff_off, tbc_off, ntiles;
+  for (auto &cr : dims) {
+    ifd_off.push_back(off);
+    off += ifd_bytes;
+    const uint64_t nt = grid(cr.first, cr.second);
+    toff_off.push_back(off);
+    off += nt * arr_entry;
+    tbc_off.push_back(off);
+    off += nt * arr_entry;
+    ntiles.push_back(nt);
+  }
+  const uint64_t scale_off = off;
+  off += 24;
+  const uint64_t tie_off = off;
+  off += 48;
+  const uint64_t keys_off = off;
+  off += keys.size() * 2;
+  const uint64_t tile_bytes = ts * ts * 4;
+  std::vector<uint64_t> data_start;
+  for (uint64_t nt : ntiles) {
+    data_start.push_back(off);
+    off += nt * tile_bytes;
+  }
+
+  Out o{std::fopen(path, "wb")};
+  if (!o.f) return SD_ERR_EXPORT_IO;
+  o.bytes("II", 2);
+  if (big) {
+    o.u16(43);
+    o.u16(8);
+    o.u16(0);
+    o.u64(ifd_off[0]);
+  } else {
+    o.u16(42);
+    o.u32((uint32_t)ifd_off[0]);
+  }
+  const size_t n_ifd = dims.size();
+  for (size_t k = 0; k < n_ifd; ++k) {
+    const uint64_t c = dims[k].first, r = dims[k].second, nt = ntiles[k];
+    const uint64_t next = k + 1 < n_ifd ? ifd_off[k + 1] : 0;
+    auto e = [&](uint16_t tag, uint16_t typ, uint64_t count, uint64_t val) {
+      o.u16(tag);
+      o.u16(typ);
+      if (big) {
+        o.u64(count);
+        o.u64(val);
+      } else {
+        o.u32((uint32_t)count);
+        o.u32((uint32_t)val);
+      }
+    };
+    if (big) o.u64(entries);
+    else o.u16((uint16_t)entries);
+    e(256, 4, 1, c);
+    e(257, 4, 1, r);
+    e(258, 3, 1, 32);
+    e(259, 3, 1, 1);
+    e(262, 3, 1, 1);
+    e(277, 3, 1, 1);
+    if (big) {
+      e(282, 5, 1, (1ull << 32) | 72ull);
+      e(283, 5, 1, (1ull << 32) | 72ull);
+    } else {
+      e(282, 4, 1, 72);
+      e(283, 4, 1, 72);
+    }
+    e(296, 3, 1, 1);
+    e(322, 4, 1, ts);
+    e(323, 4, 1, ts);
+    e(324, big ? 16 : 4, nt, toff_off[k]);
+    e(325, big ? 16 : 4, nt, tbc_off[k]);
+    e(339, 3, 1, 3);
+    e(33550, 12, 3, scale_off);
+    e(33922, 12, 6, tie_off);
+    e(34735, 3, keys.size(), keys_off);
+    if (big) o.u64(next);
+    else o.u32((uint32_t)next);
+    for (uint64_t t = 0; t < nt; ++t) {
+      if (big) o.u64(data_start[k] + t * tile_bytes);
+      else o.u32((uint32_t)(data_start[k] + t * tile_bytes));
+    }
+    for (uint64_t t = 0; t < nt; ++t) {
+      if (big) o.u64(tile_bytes);
+      else o.u32((uint32_t)tile_bytes);
+    }
+  }
+  o.f64(gt[1]);
+  o.f64(-gt[5]);
+  o.f64(0.0);
+  o.f64(0.0);
+  o.f64(0.0);
+  o.f64(0.0);
+  o.f64(gt[0]);
+  o.f64(gt[3]);
+  o.f64(0.0);
+  for (uint16_t k : keys) o.u16(k);
+
+  std::vector<float> tile(ts * ts);
+  for (size_t k = 0; k < n_ifd; ++k) {
+    const float *src = k + 1 < n_ifd ? ov[k].d.data() : data;
+    const uint64_t c = dims[k].first, r = dims[k].second;
+    const uint64_t nx = (c + ts - 1) / ts, ny = (r + ts - 1) / ts;
+    for (uint64_t ty = 0; ty < ny; ++ty)
+      for (uint64_t tx = 0; tx < nx; ++tx) {
+        std::fill(tile.begin(), tile.end(), NAN);
+        const uint64_t r0 = ty * ts, c0 = tx * ts;
+        const uint64_t r1 = std::min(r0 + ts, r), c1 = std::min(c0 + ts, c);
+        for (uint64_t y = r0; y < r1; ++y)
+          std::memcpy(&tile[(y - r0) * ts], src + y * c + c0, (c1 - c0) * sizeof(float));
+        o.bytes(tile.data(), tile_bytes);
+      }
+  }
+  const bool ok = o.ok;
+  if (std::fclose(o.f) != 0 || !ok) return SD_ERR_EXPORT_IO;
+  return SD_OK;
+}
+
+}  // extern "C"

@@ -42,7 +42,7 @@ __all__ = [
     "merge_subswaths", "calibrate_deburst_merge", "apply_speckle_filter", "SpeckleKernel",
     "GpuSpeckleKernel", "SardineError", "TerrainCorrectionError", "SpeckleError",
     "CalibrationError", "DeburstError", "MergeError", "Context", "default_context",
-    "tc_output_grid",
+    "tc_output_grid", "to_db_inplace", "write_cog_with_crs", "downsample_2x", "ExportError",
 ] + [n for n in dir(T) if n[:1].isupper()]
 
 
@@ -74,6 +74,10 @@ class MergeError(SardineError):
     """merge_subswaths.rs:62-81"""
 
 
+class ExportError(SardineError):
+    """export.rs:25-40"""
+
+
 _KINDS = {
     _abi.SD_ERR_TC_ORBIT: (TerrainCorrectionError, "Orbit"),
     _abi.SD_ERR_TC_DEM: (TerrainCorrectionError, "Dem"),
@@ -97,6 +101,10 @@ _KINDS = {
     _abi.SD_ERR_MERGE_EMPTY_INPUTS: (MergeError, "EmptyInputs"),
     _abi.SD_ERR_MERGE_INCONSISTENT_PIXEL_SPACING: (MergeError, "InconsistentPixelSpacing"),
     _abi.SD_ERR_MERGE_EMPTY_SWATH: (MergeError, "EmptySwath"),
+    _abi.SD_ERR_EXPORT_IO: (ExportError, "Io"),
+    _abi.SD_ERR_EXPORT_INVALID_NOISE_FLOOR: (ExportError, "InvalidNoiseFloor"),
+    _abi.SD_ERR_EXPORT_INVALID_GEOTRANSFORM: (ExportError, "InvalidGeotransform"),
+    _abi.SD_ERR_EXPORT_INVALID_TILE_SIZE: (ExportError, "InvalidTileSize"),
 }
 
 
@@ -397,3 +405,47 @@ def apply_speckle_step(data, cols: int, rows: int, kernel: Optional[SpeckleKerne
     if kernel is None:
         return data
     return kernel.apply(data, cols, rows)
+
+
+# ── output: dB conversion and Cloud-Optimised GeoTIFF ─────────────────────
+def to_db_inplace(data, noise_floor_linear: float, ctx: Optional[Context] = None,
+                  stats: bool = False):
+    """to_db_inplace (export.rs:59-99) on the buffer itself (numpy or torch,
+    host or device): returns (converted, noise_masked), and with stats=True
+    also compute_db_stats (run.rs:63-97) of the result: (min, max, mean,
+    median) of the finite dB values."""
+    ctx = _ctx(ctx)
+    if isinstance(data, np.ndarray) and (data.dtype != np.float32 or not data.flags.c_contiguous):
+        raise TypeError("to_db_inplace works in place: pass a contiguous float32 array")
+    if not isinstance(data, np.ndarray) and not data.is_contiguous():
+        raise TypeError("to_db_inplace works in place: pass a contiguous float32 tensor")
+    counts = (C.c_uint64 * 2)()
+    st = (C.c_float * 4)()
+    rc = lib().sd_to_db(ctx.handle, T.ptr(data), T.numel(data), float(noise_floor_linear), counts,
+                        st if stats else None)
+    _check(ctx, rc, ExportError)
+    out = (int(counts[0]), int(counts[1]))
+    return (out, tuple(float(x) for x in st)) if stats else out
+
+
+def downsample_2x(src, cols: int, rows: int, ctx: Optional[Context] = None):
+    """downsample_2x (export.rs:362-392): ((rows+1)//2, (cols+1)//2) raster
+    of 2x2 NaN-skipping f64 means."""
+    ctx = _ctx(ctx)
+    src = _prep(src, np.float32)
+    out = _empty_like_kind(src, ((rows + 1) // 2, (cols + 1) // 2), "f4")
+    rc = lib().sd_downsample_2x(ctx.handle, T.ptr(src), cols, rows, T.ptr(out))
+    _check(ctx, rc, ExportError)
+    return out
+
+
+def write_cog_with_crs(path: str, data, cols: int, rows: int, geotransform, crs: OutputCrs,
+                       tile_size: int = 512, ctx: Optional[Context] = None) -> None:
+    """write_cog_with_crs (export.rs:329-355): single-band Float32 COG with
+    overviews; data host or device."""
+    ctx = _ctx(ctx)
+    data = _prep(data, np.float32)
+    gt = (C.c_double * 6)(*[float(x) for x in geotransform])
+    rc = lib().sd_write_cog(ctx.handle, os.fsencode(path), T.ptr(data), cols, rows, gt, int(crs.kind),
+                            int(getattr(crs, "zone", 0) or 0), int(tile_size))
+    _check(ctx, rc, ExportError)

@@ -39,6 +39,10 @@ SD_ERR_DEBURST_IMPLAUSIBLE_OVERLAP = 45
 SD_ERR_MERGE_EMPTY_INPUTS = 50
 SD_ERR_MERGE_INCONSISTENT_PIXEL_SPACING = 51
 SD_ERR_MERGE_EMPTY_SWATH = 52
+SD_ERR_EXPORT_IO = 60
+SD_ERR_EXPORT_INVALID_NOISE_FLOOR = 61
+SD_ERR_EXPORT_INVALID_GEOTRANSFORM = 62
+SD_ERR_EXPORT_INVALID_TILE_SIZE = 63
 
 RESAMPLE_BILINEAR, RESAMPLE_BICUBIC, RESAMPLE_LANCZOS3 = 0, 1, 2
 CRS_WGS84, CRS_UTM_NORTH, CRS_UTM_SOUTH = 0, 1, 2

@@ -56,6 +56,9 @@ _SIGS = {
     "sd_ctx_reserve": (C.c_int, [P, C.c_uint64]),
     "sd_ctx_set_tile_shape": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32]),
     "sd_orbit_states": (C.c_int, [P, P, C.c_uint64, P, C.c_uint64, P]),
+    "sd_to_db": (C.c_int, [P, P, C.c_uint64, C.c_float, P, P]),
+    "sd_downsample_2x": (C.c_int, [P, P, C.c_uint64, C.c_uint64, P]),
+    "sd_write_cog": (C.c_int, [P, C.c_char_p, P, C.c_uint64, C.c_uint64, P, C.c_int32, C.c_int32, C.c_uint32]),
     "sd_measure_fp64_peak": (C.c_int, [P, C.c_int32, P]),
     "sd_measure_fp32_peak": (C.c_int, [P, C.c_int32, P]),
 }
