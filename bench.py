@@ -889,6 +889,109 @@ def _split_vs_fp64(sd, tiles, ctx, scenes, rng, n=8):
     return worst
 
 
+def _write_slc_tiff(path, iq):
+    """A Sentinel-1-style measurement TIFF of iq ((lines, samples, 2) int16):
+    one IFD, LONG strip offsets, one contiguous row per strip."""
+    import struct
+    h, w = iq.shape[:2]
+    tags = [(256, 4, w), (257, 4, h), (258, 3, 32), (259, 3, 1), (273, 4, None), (277, 3, 1), (278, 4, 1),
+            (339, 3, 5)]
+    table_at = 8 + 2 + 12 * len(tags) + 4
+    data_at = table_at + 4 * h
+    head = bytearray(b"II" + struct.pack("<HIH", 42, 8, len(tags)))
+    for tag, typ, val in tags:
+        if tag == 273:
+            head += struct.pack("<HHII", 273, 4, h, table_at)
+        elif typ == 3:
+            head += struct.pack("<HHIHH", tag, typ, 1, val, 0)
+        else:
+            head += struct.pack("<HHII", tag, typ, 1, val)
+    head += struct.pack("<I", 0)
+    head += (data_at + np.arange(h, dtype=np.uint64) * (w * 4)).astype("<u4").tobytes()
+    with open(path, "wb") as f:
+        f.write(bytes(head))
+        np.ascontiguousarray(iq, dtype="<i2").tofile(f)
+
+
+def run_ingest(args):
+    """SLC ingest feeding the fused calibrate+deburst+merge: the three
+    sub-swath measurement TIFFs of a config-2 scene (3 x 13,500 x 21,000
+    CInt16, 3.4 GB, on the box's local disk, in its page cache after the
+    warm-up) are read through SlcReader straight into device buffers, then
+    calibrated, debursted and merged.  value = merged pixels per second of
+    the whole step; the read alone is reported in GB/s."""
+    import torch
+    import sardine_b200 as sd
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = _init_dist(world)
+    ctx = sd.Context(local)
+    dev = f"cuda:{local}"
+    sc = make_workload("c2", dev, seed=2 + 1000 * rank, small=args.small)
+    paths, bufs = [], []
+    for k, s in enumerate(sc.swaths):
+        p = f"/tmp/sardine_b200_slc_r{rank}_{k}.tiff"
+        _write_slc_tiff(p, s.slc.cpu().numpy())
+        paths.append(p)
+        bufs.append(torch.empty_like(s.slc))
+    swaths = [type(s)(s.id, b, s.sw, s.bursts, s.cal, s.noise) for s, b in zip(sc.swaths, bufs)]
+    m0 = sd.calibrate_deburst_merge(sc.swaths, ctx=ctx)
+    mbuf = (m0.data, m0.nesz)
+    slc_bytes = sum(b.numel() * 2 for b in bufs)
+
+    readers = [sd.SlcReader.open(p, ctx=ctx) for p in paths]  # open once, as a pipeline run does
+
+    def read_all():
+        for r, b in zip(readers, bufs):
+            r.read_burst_raw(0, r.height, out=b)
+
+    for _ in range(args.warmup):
+        read_all()
+        sd.calibrate_deburst_merge(swaths, ctx=ctx, out=mbuf)
+    t_read = t_step = 0.0
+    l0 = ctx.launches
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+            t0 = time.perf_counter()
+            read_all()
+            t1 = time.perf_counter()
+            m = sd.calibrate_deburst_merge(swaths, ctx=ctx, out=mbuf)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            t_read += t1 - t0
+            t_step += t2 - t0
+    t_read = _max_over_ranks(dist, t_read) / args.steps
+    t_step = _max_over_ranks(dist, t_step) / args.steps
+    ok = bool(torch.equal(m.data, m0.data))
+    merged_px = int(m.lines) * int(m.samples)
+    for r in readers:
+        r.close()
+    for p in paths:
+        os.remove(p)
+    if rank == 0:
+        out = {
+            "metric": "merged px/s from measurement TIFFs", "value": world * merged_px / t_step, "unit": "px/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16 -> f32",
+            "data": "synthetic config-2 SLC written as measurement TIFFs",
+            "config": {"workload": "ingest: 3 sub-swath TIFFs -> SlcReader into device buffers -> fused "
+                                   "calibrate+deburst+merge" + (" (REDUCED SHAPE)" if args.small else ""),
+                       "slc_bytes": slc_bytes, "merged_px": merged_px, "parallelism": f"replicas x{world}"},
+            "read_gbs": slc_bytes / t_read / 1e9, "read_ms": t_read * 1e3,
+            "merged_equal_to_device_input": ok, "clocks": clk.summary(),
+            "gpu_launches": (ctx.launches - l0) // args.steps,
+            "e2e": {"value": world * merged_px / t_step, "unit": "px/s", "h2d_bytes_per_step": slc_bytes,
+                    "d2h_bytes_per_step": 0,
+                    "api": "sardine_b200.SlcReader.read_burst_raw (device out) + calibrate_deburst_merge"},
+            "cpu_baseline": None,
+        }
+        print(json.dumps(out), flush=True)
+    _finish_dist(dist)
+
+
 def _hbm_peak():
     """Measured HBM copy bandwidth (GB/s), else the fallback figure."""
     try:
@@ -1185,7 +1288,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4", "export"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4", "export", "ingest"])
     ap.add_argument("--rates", default="100,500,2000,max",
                     help="config5 request rates (req/s; 'max' queues every request at once); value at the last")
     ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
@@ -1207,6 +1310,8 @@ def main():
         run_c5(args)
     elif args.config == "export":
         run_export(args)
+    elif args.config == "ingest":
+        run_ingest(args)
     else:
         run_ours(args)
 

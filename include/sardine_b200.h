@@ -75,7 +75,15 @@ typedef enum sd_status {
     SD_ERR_EXPORT_IO = 60,
     SD_ERR_EXPORT_INVALID_NOISE_FLOOR = 61,
     SD_ERR_EXPORT_INVALID_GEOTRANSFORM = 62,
-    SD_ERR_EXPORT_INVALID_TILE_SIZE = 63
+    SD_ERR_EXPORT_INVALID_TILE_SIZE = 63,
+    /* SlcReadError (slc_reader.rs:66-98; the multi-slice variants are out of scope) */
+    SD_ERR_SLC_IO = 70,
+    SD_ERR_SLC_NOT_TIFF = 71,
+    SD_ERR_SLC_BIGTIFF = 72,
+    SD_ERR_SLC_MISSING_TAG = 73,
+    SD_ERR_SLC_UNSUPPORTED_FORMAT = 74,
+    SD_ERR_SLC_NON_CONTIGUOUS_STRIPS = 75,
+    SD_ERR_SLC_LINE_OUT_OF_BOUNDS = 76
 } sd_status;
 
 /* ── Enumerations mirroring the reference's enums ─────────────────────── */
@@ -503,6 +511,27 @@ int sd_ctx_set_tile_shape(sd_ctx *ctx, int32_t speckle_tx, int32_t speckle_ty,
  * the state vectors' span or fewer than 8 vectors are given. */
 int sd_orbit_states(sd_ctx *ctx, const sd_state_vector *svs, uint64_t n, const int64_t *t_us,
                     uint64_t m, double *out);
+
+/* ── SLC ingest ───────────────────────────────────────────────────────────
+ * SlcReader (slc_reader.rs:485-598) over a Sentinel-1 measurement TIFF:
+ * classic TIFF, CInt16 (SampleFormat 5, 32 bits), uncompressed, one row per
+ * strip, contiguous strips (the checks of parse_ifd, 268-465, in its
+ * order and with its errors, SD_ERR_SLC_*).  sd_slc_open keeps the file
+ * open until sd_slc_close; sd_slc_dims gives width, height and byte order. */
+typedef struct sd_slc_reader sd_slc_reader;
+int sd_slc_open(sd_ctx *ctx, const char *path, sd_slc_reader **out);
+int sd_slc_dims(const sd_slc_reader *reader, uint32_t *width, uint32_t *height, int32_t *little_endian);
+void sd_slc_close(sd_slc_reader *reader);
+/* read_burst_raw (532-583): line_count rows from first_line as [I, Q]
+ * int16 pairs (line_count x width x 2), in host byte order.  out may be
+ * host or device memory.  Into device memory, four threads read 32 MB
+ * chunks in parallel into pinned buffers the reader keeps (256 MB, freed
+ * by sd_slc_close) while earlier chunks are copied on the context's
+ * stream.  One read at a time per reader (it is `&mut self` in the
+ * reference).  Rows past the image give SD_ERR_SLC_LINE_OUT_OF_BOUNDS,
+ * failed reads SD_ERR_SLC_IO. */
+int sd_slc_read_burst_raw(sd_ctx *ctx, sd_slc_reader *reader, uint64_t first_line, uint64_t line_count,
+                          int16_t *out);
 
 /* ── Output: dB conversion and Cloud-Optimised GeoTIFF ───────────────────
  * to_db_inplace (export.rs:59-99) on data[0..n) in place (host or device

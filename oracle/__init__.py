@@ -73,6 +73,7 @@ def _declare(L):
         "orc_db_stats": (None, [P, u64, P]),
         "orc_downsample_2x": (None, [P, u64, u64, P]),
         "orc_write_cog": (C.c_int, [C.c_char_p, P, u64, u64, P, C.c_int, C.c_int, C.c_uint32]),
+        "orc_slc_read": (C.c_int, [C.c_char_p, u64, u64, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -392,3 +393,15 @@ def write_cog(path: str, data: np.ndarray, cols: int, rows: int, geotransform, c
     gt = (C.c_double * 6)(*[float(x) for x in geotransform])
     return int(lib().orc_write_cog(os.fsencode(path), data.ctypes.data, cols, rows, gt, int(crs.kind),
                                    int(crs.zone), int(tile_size)))
+
+
+def slc_read(path: str, first_line: int = 0, line_count: int = 0, read: bool = True):
+    """SlcReader::open + read_burst_raw (slc_reader.rs:268-583): returns
+    (status, width, height, rows as int16 [line_count, width, 2] or None)."""
+    w, h = C.c_uint32(), C.c_uint32()
+    rc = lib().orc_slc_read(os.fsencode(path), 0, 0, None, C.byref(w), C.byref(h))
+    if rc != 0 or not read:
+        return rc, int(w.value), int(h.value), None
+    out = np.empty((line_count, w.value, 2), np.int16)
+    rc = lib().orc_slc_read(os.fsencode(path), first_line, line_count, out.ctypes.data, None, None)
+    return rc, int(w.value), int(h.value), (out if rc == 0 else None)

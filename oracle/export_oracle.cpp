@@ -1,5 +1,6 @@
-// CPU oracle for the output path: dB conversion, dB statistics, overview
-// downsampling and the Cloud-Optimised GeoTIFF writer.
+// CPU oracle for the pipeline's file ends: the SLC measurement TIFF reader,
+// dB conversion, dB statistics, overview downsampling and the
+// Cloud-Optimised GeoTIFF writer.
 //
 // TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline): a plain
 // sequential restatement of the reference's arithmetic and file layout,
@@ -11,6 +12,7 @@
 //   write_cog_with_crs     sardine/src/export.rs:329-355
 //   write_cog_raw_inner    sardine/src/export.rs:417-760
 //   geo_key_directory      sardine/src/output_crs.rs:265-287
+//   SlcReader              sardine/src/slc_reader.rs:268-583
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -294,3 +296,101 @@ int orc_write_cog(const char *path, const float *data, uint64_t cols, uint64_t r
 }
 
 }  // extern "C"
+
+// ── SLC measurement TIFF reader (slc_reader.rs:268-583) ─────────────────────
+// parse_ifd's checks in its order, then read_burst_raw of [first, first+n)
+// rows into out (n * width * 2 int16, host byte order).  width/height are
+// filled once the IFD is accepted; out may be null to only open the file.
+namespace {
+uint16_t o_rd16(const unsigned char *b, bool le) {
+  return le ? (uint16_t)(b[0] | (b[1] << 8)) : (uint16_t)(b[1] | (b[0] << 8));
+}
+uint32_t o_rd32(const unsigned char *b, bool le) {
+  uint32_t v = 0;
+  for (int k = 0; k < 4; ++k) v |= (uint32_t)b[le ? k : 3 - k] << (8 * k);
+  return v;
+}
+bool o_read(FILE *f, uint64_t off, void *dst, size_t n) {
+  return std::fseek(f, (long)off, SEEK_SET) == 0 && std::fread(dst, 1, n, f) == n;
+}
+}  // namespace
+
+extern "C" int orc_slc_read(const char *path, uint64_t first, uint64_t n, int16_t *out, uint32_t *width_out,
+                            uint32_t *height_out) {
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return SD_ERR_SLC_IO;
+  struct C {
+    FILE *f;
+    ~C() { std::fclose(f); }
+  } closer{f};
+  unsigned char h[8];
+  if (!o_read(f, 0, h, 8)) return SD_ERR_SLC_IO;
+  bool le;
+  if (h[0] == 'I' && h[1] == 'I') le = true;
+  else if (h[0] == 'M' && h[1] == 'M') le = false;
+  else return SD_ERR_SLC_NOT_TIFF;
+  const uint16_t magic = o_rd16(h + 2, le);
+  if (magic == 43) return SD_ERR_SLC_BIGTIFF;
+  if (magic != 42) return SD_ERR_SLC_NOT_TIFF;
+  const uint64_t ifd = o_rd32(h + 4, le);
+  unsigned char nb[2];
+  if (!o_read(f, ifd, nb, 2)) return SD_ERR_SLC_IO;
+  const size_t ne = o_rd16(nb, le);
+  std::vector<unsigned char> e(ne * 12);
+  if (ne && !o_read(f, ifd + 2, e.data(), e.size())) return SD_ERR_SLC_IO;
+  long width = -1, height = -1, bps = -1, comp = -1, rps = -1, spp = -1, sfmt = -1;
+  bool so = false;
+  uint16_t so_type = 0;
+  uint32_t so_count = 0, so_val = 0;
+  for (size_t k = 0; k < ne; ++k) {
+    const unsigned char *p = &e[12 * k];
+    const uint16_t tag = o_rd16(p, le), typ = o_rd16(p + 2, le);
+    const uint32_t cnt = o_rd32(p + 4, le);
+    long v = typ == 3 ? (long)o_rd16(p + 8, le) : (typ == 4 ? (long)o_rd32(p + 8, le) : -1);
+    switch (tag) {
+      case 256: width = v; break;
+      case 257: height = v; break;
+      case 258: bps = v; break;
+      case 259: comp = v; break;
+      case 278: rps = v; break;
+      case 277: spp = v; break;
+      case 339: sfmt = v; break;
+      case 273:
+        so = true;
+        so_type = typ;
+        so_count = cnt;
+        so_val = o_rd32(p + 8, le);
+        break;
+      default: break;
+    }
+  }
+  if (width < 0 || height < 0 || bps < 0 || comp < 0 || rps < 0 || sfmt < 0 || !so) return SD_ERR_SLC_MISSING_TAG;
+  if (spp < 0) spp = 1;
+  if ((uint16_t)comp != 1 || (uint16_t)sfmt != 5 || (uint16_t)bps != 32 || rps != 1 || (uint16_t)spp != 1 ||
+      so_count != (uint32_t)height || height == 0)
+    return SD_ERR_SLC_UNSUPPORTED_FORMAT;
+  const uint64_t row = (uint64_t)width * 4;
+  uint64_t base = so_val, last = so_val;
+  if (so_count > 1) {
+    if (so_type != 3 && so_type != 4) return SD_ERR_SLC_UNSUPPORTED_FORMAT;
+    const size_t each = so_type == 3 ? 2 : 4;
+    unsigned char b[4];
+    if (!o_read(f, so_val, b, each)) return SD_ERR_SLC_IO;
+    base = each == 2 ? o_rd16(b, le) : o_rd32(b, le);
+    if (!o_read(f, so_val + (uint64_t)(so_count - 1) * each, b, each)) return SD_ERR_SLC_IO;
+    last = each == 2 ? o_rd16(b, le) : o_rd32(b, le);
+  }
+  if (last != base + (uint64_t)(height - 1) * row) return SD_ERR_SLC_NON_CONTIGUOUS_STRIPS;
+  if (width_out) *width_out = (uint32_t)width;
+  if (height_out) *height_out = (uint32_t)height;
+  if (!out) return SD_OK;
+  if (first > (uint64_t)height || n > (uint64_t)height - first) return SD_ERR_SLC_LINE_OUT_OF_BOUNDS;
+  if (n == 0) return SD_OK;
+  if (!o_read(f, base + first * row, out, n * row)) return SD_ERR_SLC_IO;
+  if (!le)
+    for (uint64_t i = 0; i < n * (uint64_t)width * 2; ++i) {
+      const uint16_t u = (uint16_t)out[i];
+      out[i] = (int16_t)(uint16_t)((u >> 8) | (u << 8));
+    }
+  return SD_OK;
+}

@@ -43,6 +43,7 @@ __all__ = [
     "GpuSpeckleKernel", "SardineError", "TerrainCorrectionError", "SpeckleError",
     "CalibrationError", "DeburstError", "MergeError", "Context", "default_context",
     "tc_output_grid", "to_db_inplace", "write_cog_with_crs", "downsample_2x", "ExportError",
+    "SlcReader", "SlcReadError",
 ] + [n for n in dir(T) if n[:1].isupper()]
 
 
@@ -78,6 +79,10 @@ class ExportError(SardineError):
     """export.rs:25-40"""
 
 
+class SlcReadError(SardineError):
+    """slc_reader.rs:66-98"""
+
+
 _KINDS = {
     _abi.SD_ERR_TC_ORBIT: (TerrainCorrectionError, "Orbit"),
     _abi.SD_ERR_TC_DEM: (TerrainCorrectionError, "Dem"),
@@ -105,6 +110,13 @@ _KINDS = {
     _abi.SD_ERR_EXPORT_INVALID_NOISE_FLOOR: (ExportError, "InvalidNoiseFloor"),
     _abi.SD_ERR_EXPORT_INVALID_GEOTRANSFORM: (ExportError, "InvalidGeotransform"),
     _abi.SD_ERR_EXPORT_INVALID_TILE_SIZE: (ExportError, "InvalidTileSize"),
+    _abi.SD_ERR_SLC_IO: (SlcReadError, "Io"),
+    _abi.SD_ERR_SLC_NOT_TIFF: (SlcReadError, "NotTiff"),
+    _abi.SD_ERR_SLC_BIGTIFF: (SlcReadError, "BigTiff"),
+    _abi.SD_ERR_SLC_MISSING_TAG: (SlcReadError, "MissingTag"),
+    _abi.SD_ERR_SLC_UNSUPPORTED_FORMAT: (SlcReadError, "UnsupportedFormat"),
+    _abi.SD_ERR_SLC_NON_CONTIGUOUS_STRIPS: (SlcReadError, "NonContiguousStrips"),
+    _abi.SD_ERR_SLC_LINE_OUT_OF_BOUNDS: (SlcReadError, "LineOutOfBounds"),
 }
 
 
@@ -449,3 +461,55 @@ def write_cog_with_crs(path: str, data, cols: int, rows: int, geotransform, crs:
     rc = lib().sd_write_cog(ctx.handle, os.fsencode(path), T.ptr(data), cols, rows, gt, int(crs.kind),
                             int(getattr(crs, "zone", 0) or 0), int(tile_size))
     _check(ctx, rc, ExportError)
+
+
+# ── SLC ingest ─────────────────────────────────────────────────────────────
+class SlcReader:
+    """SlcReader (slc_reader.rs:485-598) over a Sentinel-1 measurement TIFF;
+    reads bursts into host arrays or straight into device tensors."""
+
+    def __init__(self, path: str, ctx: Optional[Context] = None):
+        self.ctx = _ctx(ctx)
+        self._h = C.c_void_p()
+        rc = lib().sd_slc_open(self.ctx.handle, os.fsencode(path), C.byref(self._h))
+        _check(self.ctx, rc, SlcReadError)
+        w, h, le = C.c_uint32(), C.c_uint32(), C.c_int32()
+        lib().sd_slc_dims(self._h, C.byref(w), C.byref(h), C.byref(le))
+        self.width, self.height, self.little_endian = int(w.value), int(h.value), bool(le.value)
+
+    @classmethod
+    def open(cls, path: str, ctx: Optional[Context] = None) -> "SlcReader":
+        return cls(path, ctx)
+
+    def read_burst_raw(self, first_line: int, line_count: int, out=None):
+        """line_count rows from first_line as int16 [line_count, width, 2]
+        ([I, Q] per pixel).  `out` (numpy, or a CUDA tensor the rows are
+        streamed into) is filled and returned; by default a numpy array."""
+        if out is None:
+            out = np.empty((line_count, self.width, 2), np.int16)
+        if T.numel(out) != line_count * self.width * 2:
+            raise ValueError("out must hold line_count x width x 2 int16")
+        rc = lib().sd_slc_read_burst_raw(self.ctx.handle, self._h, int(first_line), int(line_count), T.ptr(out))
+        _check(self.ctx, rc, SlcReadError)
+        return out
+
+    def read_burst_complex(self, first_line: int, line_count: int):
+        """read_burst_complex (585-598): the same rows as float32 [.., 2]."""
+        return self.read_burst_raw(first_line, line_count).astype(np.float32)
+
+    def close(self):
+        if self._h:
+            lib().sd_slc_close(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

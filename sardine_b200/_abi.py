@@ -43,6 +43,13 @@ SD_ERR_EXPORT_IO = 60
 SD_ERR_EXPORT_INVALID_NOISE_FLOOR = 61
 SD_ERR_EXPORT_INVALID_GEOTRANSFORM = 62
 SD_ERR_EXPORT_INVALID_TILE_SIZE = 63
+SD_ERR_SLC_IO = 70
+SD_ERR_SLC_NOT_TIFF = 71
+SD_ERR_SLC_BIGTIFF = 72
+SD_ERR_SLC_MISSING_TAG = 73
+SD_ERR_SLC_UNSUPPORTED_FORMAT = 74
+SD_ERR_SLC_NON_CONTIGUOUS_STRIPS = 75
+SD_ERR_SLC_LINE_OUT_OF_BOUNDS = 76
 
 RESAMPLE_BILINEAR, RESAMPLE_BICUBIC, RESAMPLE_LANCZOS3 = 0, 1, 2
 CRS_WGS84, CRS_UTM_NORTH, CRS_UTM_SOUTH = 0, 1, 2
