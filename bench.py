@@ -967,6 +967,20 @@ def run_ingest(args):
     t_step = _max_over_ranks(dist, t_step) / args.steps
     ok = bool(torch.equal(m.data, m0.data))
     merged_px = int(m.lines) * int(m.samples)
+    # pre-TC multilook of the merged image (4 range looks), HBM-bound
+    ml = None
+    if rank == 0:
+        for _ in range(2):
+            sd.apply_multilook(m, 4, 1, 2.055556e-3, ctx=ctx)
+        ctx.set_timing(True)
+        for _ in range(3):
+            mo = sd.apply_multilook(m, 4, 1, 2.055556e-3, ctx=ctx)
+        kt = ctx.kernel_times()
+        ctx.set_timing(False)
+        ml_ms = kt["k_multilook"][0] / 3
+        ml_bytes = 8 * merged_px + 8 * int(mo.lines) * int(mo.samples)
+        ml = {"looks": "4x1", "ms": ml_ms, "gbs": ml_bytes / (ml_ms / 1e3) / 1e9,
+              "frac_of_hbm": ml_bytes / (ml_ms / 1e3) / 1e9 / _hbm_peak(), "bytes": ml_bytes}
     for r in readers:
         r.close()
     for p in paths:
@@ -981,7 +995,7 @@ def run_ingest(args):
                                    "calibrate+deburst+merge" + (" (REDUCED SHAPE)" if args.small else ""),
                        "slc_bytes": slc_bytes, "merged_px": merged_px, "parallelism": f"replicas x{world}"},
             "read_gbs": slc_bytes / t_read / 1e9, "read_ms": t_read * 1e3,
-            "merged_equal_to_device_input": ok, "clocks": clk.summary(),
+            "merged_equal_to_device_input": ok, "multilook": ml, "clocks": clk.summary(),
             "gpu_launches": (ctx.launches - l0) // args.steps,
             "e2e": {"value": world * merged_px / t_step, "unit": "px/s", "h2d_bytes_per_step": slc_bytes,
                     "d2h_bytes_per_step": 0,

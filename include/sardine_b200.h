@@ -533,6 +533,19 @@ void sd_slc_close(sd_slc_reader *reader);
 int sd_slc_read_burst_raw(sd_ctx *ctx, sd_slc_reader *reader, uint64_t first_line, uint64_t line_count,
                           int16_t *out);
 
+/* ── Pre-TC multilook ─────────────────────────────────────────────────────
+ * The boxcar of apply_multilook (scene_prep.rs:1060-1160) over a merged
+ * image (lines x samples, host or device): out_data/out_nesz
+ * ((lines / azimuth_looks) x (samples / range_looks)) hold the f64 mean of
+ * the non-NaN sigma0 of each azimuth_looks x range_looks block and of the
+ * NESZ at those same pixels, NaN when all are NaN.  nesz may be NULL (then
+ * out_nesz is ignored).  The geometry update (spacing x range_looks, near
+ * range + (R-1)/2 spacings, azimuth start + (A-1)/2 ATI) is the caller's;
+ * sardine_b200.apply_multilook does both.  Factors of 0, or larger than
+ * the image, give SD_ERR_INVALID_ARGUMENT with the reference's message. */
+int sd_multilook(sd_ctx *ctx, const float *data, const float *nesz, uint64_t lines, uint64_t samples,
+                 uint32_t range_looks, uint32_t azimuth_looks, float *out_data, float *out_nesz);
+
 /* ── Output: dB conversion and Cloud-Optimised GeoTIFF ───────────────────
  * to_db_inplace (export.rs:59-99) on data[0..n) in place (host or device
  * memory): NaN stays NaN; v <= noise_floor_linear (and any v <= 0) becomes

@@ -74,6 +74,7 @@ def _declare(L):
         "orc_downsample_2x": (None, [P, u64, u64, P]),
         "orc_write_cog": (C.c_int, [C.c_char_p, P, u64, u64, P, C.c_int, C.c_int, C.c_uint32]),
         "orc_slc_read": (C.c_int, [C.c_char_p, u64, u64, P, P, P]),
+        "orc_multilook": (C.c_int, [P, P, u64, u64, C.c_uint32, C.c_uint32, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -405,3 +406,15 @@ def slc_read(path: str, first_line: int = 0, line_count: int = 0, read: bool = T
     out = np.empty((line_count, w.value, 2), np.int16)
     rc = lib().orc_slc_read(os.fsencode(path), first_line, line_count, out.ctypes.data, None, None)
     return rc, int(w.value), int(h.value), (out if rc == 0 else None)
+
+
+def multilook(data: np.ndarray, nesz: np.ndarray, lines: int, samples: int, range_looks: int, azimuth_looks: int):
+    """The boxcar of apply_multilook (scene_prep.rs:1060-1160): (status, data, nesz)."""
+    d = np.ascontiguousarray(data, dtype=np.float32).reshape(-1)
+    n = np.ascontiguousarray(nesz, dtype=np.float32).reshape(-1)
+    ol, os_ = (lines // azimuth_looks if azimuth_looks else 0), (samples // range_looks if range_looks else 0)
+    od = np.empty((max(ol, 1), max(os_, 1)), np.float32)
+    on = np.empty_like(od)
+    rc = lib().orc_multilook(d.ctypes.data, n.ctypes.data, lines, samples, range_looks, azimuth_looks,
+                             od.ctypes.data, on.ctypes.data)
+    return rc, (od if rc == 0 else None), (on if rc == 0 else None)

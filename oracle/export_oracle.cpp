@@ -13,6 +13,7 @@
 //   write_cog_raw_inner    sardine/src/export.rs:417-760
 //   geo_key_directory      sardine/src/output_crs.rs:265-287
 //   SlcReader              sardine/src/slc_reader.rs:268-583
+//   apply_multilook        sardine/src/scene_prep.rs:1060-1160
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -391,6 +392,31 @@ extern "C" int orc_slc_read(const char *path, uint64_t first, uint64_t n, int16_
     for (uint64_t i = 0; i < n * (uint64_t)width * 2; ++i) {
       const uint16_t u = (uint16_t)out[i];
       out[i] = (int16_t)(uint16_t)((u >> 8) | (u << 8));
+    }
+  return SD_OK;
+}
+
+// ── pre-TC multilook (scene_prep.rs:1060-1160, the boxcar part) ────────────
+extern "C" int orc_multilook(const float *d, const float *nz, uint64_t lines, uint64_t samples, uint32_t rl,
+                             uint32_t al, float *od, float *onz) {
+  if (rl == 0 || al == 0) return SD_ERR_INVALID_ARGUMENT;
+  const uint64_t ol = lines / al, os = samples / rl;
+  if (ol == 0 || os == 0) return SD_ERR_INVALID_ARGUMENT;
+  for (uint64_t y = 0; y < ol; ++y)
+    for (uint64_t x = 0; x < os; ++x) {
+      double s = 0.0, sn = 0.0;
+      uint32_t c = 0;
+      for (uint32_t a = 0; a < al; ++a)
+        for (uint32_t r = 0; r < rl; ++r) {
+          const uint64_t k = (y * al + a) * samples + x * rl + r;
+          if (!std::isnan(d[k])) {
+            s += (double)d[k];
+            sn += (double)nz[k];
+            ++c;
+          }
+        }
+      od[y * os + x] = c ? (float)(s / (double)c) : NAN;
+      onz[y * os + x] = c ? (float)(sn / (double)c) : NAN;
     }
   return SD_OK;
 }

@@ -43,7 +43,7 @@ __all__ = [
     "GpuSpeckleKernel", "SardineError", "TerrainCorrectionError", "SpeckleError",
     "CalibrationError", "DeburstError", "MergeError", "Context", "default_context",
     "tc_output_grid", "to_db_inplace", "write_cog_with_crs", "downsample_2x", "ExportError",
-    "SlcReader", "SlcReadError",
+    "SlcReader", "SlcReadError", "apply_multilook",
 ] + [n for n in dir(T) if n[:1].isupper()]
 
 
@@ -513,3 +513,34 @@ class SlcReader:
             self.close()
         except Exception:
             pass
+
+
+# ── pre-TC multilook ───────────────────────────────────────────────────────
+def apply_multilook(merged: MergedSigma0, range_looks: int, azimuth_looks: int,
+                    azimuth_time_interval_s: float, ctx: Optional[Context] = None) -> MergedSigma0:
+    """apply_multilook (scene_prep.rs:1060-1160): the boxcar on the device and
+    the reference's geometry update.  R = A = 1 returns the input itself."""
+    if range_looks == 1 and azimuth_looks == 1:
+        return merged
+    ctx = _ctx(ctx)
+    if range_looks >= 1 and azimuth_looks > 1 and not (
+            np.isfinite(azimuth_time_interval_s) and azimuth_time_interval_s > 0.0):
+        raise SardineError(_abi.SD_ERR_INVALID_ARGUMENT, "InvalidArgument",
+                           f"azimuth_time_interval_s must be > 0 when azimuth_looks > 1 "
+                           f"(got {azimuth_time_interval_s})")
+    ol = merged.lines // azimuth_looks if azimuth_looks else 0
+    os_ = merged.samples // range_looks if range_looks else 0
+    data = _prep(merged.data, np.float32)
+    nesz = _prep(merged.nesz, np.float32)
+    out = _empty_like_kind(data, (max(ol, 1), max(os_, 1)), "f4")
+    onz = _empty_like_kind(data, (max(ol, 1), max(os_, 1)), "f4")
+    rc = lib().sd_multilook(ctx.handle, T.ptr(data), T.ptr(nesz), merged.lines, merged.samples,
+                            int(range_looks), int(azimuth_looks), T.ptr(out), T.ptr(onz))
+    _check(ctx, rc)
+    az0 = int(merged.azimuth_start_time_us)
+    if azimuth_looks > 1:  # (A-1)/2 lines forward, truncated to whole microseconds (as i64)
+        az0 += int((azimuth_looks - 1) / 2.0 * azimuth_time_interval_s * 1e6)
+    return MergedSigma0(out, ol, os_,
+                        merged.near_slant_range_time_s + (range_looks - 1) / 2.0 * merged.range_pixel_spacing_s,
+                        merged.range_pixel_spacing_s * range_looks, merged.range_pixel_spacing_m * range_looks,
+                        merged.cal_lut_extrapolation_gap_px, merged.noise_lut_extrapolation_gap_px, onz, az0)
