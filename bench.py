@@ -981,6 +981,25 @@ def run_ingest(args):
         ml_bytes = 8 * merged_px + 8 * int(mo.lines) * int(mo.samples)
         ml = {"looks": "4x1", "ms": ml_ms, "gbs": ml_bytes / (ml_ms / 1e3) / 1e9,
               "frac_of_hbm": ml_bytes / (ml_ms / 1e3) / 1e9 / _hbm_peak(), "bytes": ml_bytes}
+        # ground range at 10 m (synthetic incidence grids of three overlapping sub-swaths, 30-46 deg)
+        from sardine_b200.types import GeolocationGridPoint as GP
+        S = int(m.samples)
+        grids = []
+        for k, (c0, c1) in enumerate([(0, 0.40 * S), (0.33 * S, 0.72 * S), (0.66 * S, S - 1)]):
+            pts = [GP(0, 0.0, 0.0, m.near_slant_range_time_s + (c0 + (c1 - c0) * i / 20) * m.range_pixel_spacing_s,
+                      line, 30.0 + 16.0 * (c0 + (c1 - c0) * i / 20) / S) for line in (0, 5000, 10000) for i in range(21)]
+            grids.append((f"IW{k + 1}", pts))
+        for _ in range(2):
+            sd.to_ground_range(m, grids, 10.0, 13.9, ctx=ctx)
+        ctx.set_timing(True)
+        for _ in range(3):
+            g = sd.to_ground_range(m, grids, 10.0, 13.9, ctx=ctx)
+        kt = ctx.kernel_times()
+        ctx.set_timing(False)
+        g_ms = kt["k_grd"][0] / 3
+        g_bytes = 4 * merged_px + 4 * g.lines * g.samples  # input read once (neighbouring columns share taps)
+        ml["grd"] = {"target_m": 10.0, "out": [g.lines, g.samples], "ms": g_ms,
+                     "gbs": g_bytes / (g_ms / 1e3) / 1e9, "frac_of_hbm": g_bytes / (g_ms / 1e3) / 1e9 / _hbm_peak()}
     for r in readers:
         r.close()
     for p in paths:

@@ -83,7 +83,13 @@ typedef enum sd_status {
     SD_ERR_SLC_MISSING_TAG = 73,
     SD_ERR_SLC_UNSUPPORTED_FORMAT = 74,
     SD_ERR_SLC_NON_CONTIGUOUS_STRIPS = 75,
-    SD_ERR_SLC_LINE_OUT_OF_BOUNDS = 76
+    SD_ERR_SLC_LINE_OUT_OF_BOUNDS = 76,
+    /* GroundRangeError (ground_range.rs:42-57) */
+    SD_ERR_GRD_NO_GRID_POINTS = 80,
+    SD_ERR_GRD_EMPTY_IMAGE = 81,
+    SD_ERR_GRD_INVALID_SPACING = 82,
+    SD_ERR_GRD_INVALID_AZIMUTH_SPACING = 83,
+    SD_ERR_GRD_INTERPOLATION_FAILED = 84
 } sd_status;
 
 /* ── Enumerations mirroring the reference's enums ─────────────────────── */
@@ -545,6 +551,37 @@ int sd_slc_read_burst_raw(sd_ctx *ctx, sd_slc_reader *reader, uint64_t first_lin
  * the image, give SD_ERR_INVALID_ARGUMENT with the reference's message. */
 int sd_multilook(sd_ctx *ctx, const float *data, const float *nesz, uint64_t lines, uint64_t samples,
                  uint32_t range_looks, uint32_t azimuth_looks, float *out_data, float *out_nesz);
+
+/* ── Ground range (GRD) ───────────────────────────────────────────────────
+ * to_ground_range (ground_range.rs:303-427) of a merged slant-range image
+ * (lines x samples, host or device): the incidence-angle profile from each
+ * sub-swath's mid-azimuth geolocation row, ground spacing = slant spacing /
+ * sin(incidence), output columns every target_spacing_m of cumulative
+ * ground range (linear f32 interpolation between slant columns), then the
+ * f64 mean of round(target / azimuth_pixel_spacing_m) lines (NaN skipped).
+ * Call with out == NULL to only fill *info (the output dimensions). */
+typedef struct sd_grd_grid_point {   /* GeolocationGridPoint fields read here (types.rs:171) */
+    uint32_t line;
+    uint32_t pad;
+    double slant_range_time_s;
+    double incidence_angle_deg;
+} sd_grd_grid_point;
+typedef struct sd_grd_swath_grid {   /* one (SubSwathId, Vec<GeolocationGridPoint>) */
+    int32_t swath_id;                 /* 1..3 for IW1..IW3 (messages only) */
+    int32_t pad;
+    const sd_grd_grid_point *points;
+    uint64_t n_points;
+} sd_grd_swath_grid;
+typedef struct sd_grd_info {         /* GroundRangeImage (ground_range.rs:60-85) minus data */
+    uint64_t lines, samples;
+    double range_pixel_spacing_m, azimuth_pixel_spacing_m;
+    uint64_t range_looks, azimuth_looks;
+} sd_grd_info;
+int sd_to_ground_range(sd_ctx *ctx, const float *data, uint64_t lines, uint64_t samples,
+                       double near_slant_range_time_s, double range_pixel_spacing_s,
+                       double range_pixel_spacing_m, const sd_grd_swath_grid *grids, int32_t n_grids,
+                       double target_spacing_m, double azimuth_pixel_spacing_m, float *out,
+                       sd_grd_info *info);
 
 /* ── Output: dB conversion and Cloud-Optimised GeoTIFF ───────────────────
  * to_db_inplace (export.rs:59-99) on data[0..n) in place (host or device

@@ -75,6 +75,7 @@ def _declare(L):
         "orc_write_cog": (C.c_int, [C.c_char_p, P, u64, u64, P, C.c_int, C.c_int, C.c_uint32]),
         "orc_slc_read": (C.c_int, [C.c_char_p, u64, u64, P, P, P]),
         "orc_multilook": (C.c_int, [P, P, u64, u64, C.c_uint32, C.c_uint32, P, P]),
+        "orc_to_ground_range": (C.c_int, [P, u64, u64, d, d, d, P, C.c_int32, d, d, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -418,3 +419,21 @@ def multilook(data: np.ndarray, nesz: np.ndarray, lines: int, samples: int, rang
     rc = lib().orc_multilook(d.ctypes.data, n.ctypes.data, lines, samples, range_looks, azimuth_looks,
                              od.ctypes.data, on.ctypes.data)
     return rc, (od if rc == 0 else None), (on if rc == 0 else None)
+
+
+def to_ground_range(merged: T.MergedSigma0, grids, target_spacing_m: float, azimuth_pixel_spacing_m: float):
+    """to_ground_range (ground_range.rs:303-427): (status, GroundRangeImage or None)."""
+    from sardine_b200 import _grd_grids
+    d = np.ascontiguousarray(merged.data, dtype=np.float32).reshape(-1)
+    arr, keep = _grd_grids(grids)
+    info = _abi.GrdInfo()
+    args = (merged.lines, merged.samples, float(merged.near_slant_range_time_s), float(merged.range_pixel_spacing_s),
+            float(merged.range_pixel_spacing_m), arr, len(grids), float(target_spacing_m),
+            float(azimuth_pixel_spacing_m))
+    rc = lib().orc_to_ground_range(d.ctypes.data, *args, None, C.byref(info))
+    if rc != 0:
+        return rc, None
+    out = np.empty((int(info.lines), int(info.samples)), np.float32)
+    rc = lib().orc_to_ground_range(d.ctypes.data, *args, out.ctypes.data if out.size else None, C.byref(info))
+    return rc, T.GroundRangeImage(out, int(info.lines), int(info.samples), info.range_pixel_spacing_m,
+                                  info.azimuth_pixel_spacing_m, int(info.range_looks), int(info.azimuth_looks))

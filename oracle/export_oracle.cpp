@@ -14,6 +14,7 @@
 //   geo_key_directory      sardine/src/output_crs.rs:265-287
 //   SlcReader              sardine/src/slc_reader.rs:268-583
 //   apply_multilook        sardine/src/scene_prep.rs:1060-1160
+//   to_ground_range        sardine/src/ground_range.rs:148-485
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -417,6 +418,178 @@ extern "C" int orc_multilook(const float *d, const float *nz, uint64_t lines, ui
         }
       od[y * os + x] = c ? (float)(s / (double)c) : NAN;
       onz[y * os + x] = c ? (float)(sn / (double)c) : NAN;
+    }
+  return SD_OK;
+}
+
+// ── ground range (ground_range.rs:148-485) ──────────────────────────────────
+// The reference's structure: per-swath range interpolators at the
+// mid-azimuth grid row, the per-column incidence profile, cumulative ground
+// range, the column mapping, the full projected image, then the azimuth
+// multilook.
+namespace {
+struct ORange {
+  std::vector<double> t, a;
+  double lo, hi;
+  bool eval(double st, double *out) const {  // RangeInterpolator::interpolate
+    if (st < lo || st > hi) return false;
+    size_t b = 0, e = t.size();            // binary search: first index with t >= st
+    while (b < e) {
+      const size_t m = (b + e) / 2;
+      if (t[m] < st) b = m + 1;
+      else e = m;
+    }
+    if (b < t.size() && t[b] == st) {
+      *out = a[b];
+      return true;
+    }
+    if (b == 0) {
+      *out = a[0];
+      return true;
+    }
+    if (b >= t.size()) {
+      *out = a[t.size() - 1];
+      return true;
+    }
+    const double f = (st - t[b - 1]) / (t[b] - t[b - 1]);
+    *out = a[b - 1] + f * (a[b] - a[b - 1]);
+    return true;
+  }
+};
+}  // namespace
+
+extern "C" int orc_to_ground_range(const float *data, uint64_t lines, uint64_t samples, double near_t, double rps_s,
+                                   double rps_m, const sd_grd_swath_grid *grids, int32_t n_grids, double target,
+                                   double az_spacing, float *out, sd_grd_info *info) {
+  if (lines == 0 || samples == 0) return SD_ERR_GRD_EMPTY_IMAGE;
+  if (target <= 0.0) return SD_ERR_GRD_INVALID_SPACING;
+  if (!std::isfinite(az_spacing) || az_spacing <= 0.0) return SD_ERR_GRD_INVALID_AZIMUTH_SPACING;
+  std::vector<ORange> rs;
+  for (int32_t g = 0; g < n_grids; ++g) {
+    if (grids[g].n_points == 0) return SD_ERR_GRD_NO_GRID_POINTS;
+    std::vector<uint32_t> ls;
+    for (uint64_t k = 0; k < grids[g].n_points; ++k) ls.push_back(grids[g].points[k].line);
+    std::sort(ls.begin(), ls.end());
+    ls.erase(std::unique(ls.begin(), ls.end()), ls.end());
+    const uint32_t mid = ls[ls.size() / 2];
+    std::vector<std::pair<double, double>> v;
+    for (uint64_t k = 0; k < grids[g].n_points; ++k)
+      if (grids[g].points[k].line == mid)
+        v.push_back({grids[g].points[k].slant_range_time_s, grids[g].points[k].incidence_angle_deg});
+    std::stable_sort(v.begin(), v.end(), [](const std::pair<double, double> &x, const std::pair<double, double> &y) {
+      return x.first < y.first;
+    });
+    ORange r;
+    for (auto &q : v) {
+      r.t.push_back(q.first);
+      r.a.push_back(q.second);
+    }
+    r.lo = r.t.front();
+    r.hi = r.t.back();
+    rs.push_back(r);
+  }
+  std::stable_sort(rs.begin(), rs.end(), [](const ORange &x, const ORange &y) { return x.lo < y.lo; });
+  std::vector<double> ang(samples);
+  for (uint64_t c = 0; c < samples; ++c) {
+    const double st = near_t + (double)c * rps_s;
+    bool got = false;
+    double best = 0.0, bd = 0.0;
+    for (const ORange &r : rs) {
+      double a;
+      if (r.eval(st, &a)) {
+        const double d = std::fabs(st - (r.lo + r.hi) / 2.0);
+        if (!got || d < bd) {
+          got = true;
+          bd = d;
+          best = a;
+        }
+      }
+    }
+    if (!got) {
+      const ORange *nr = nullptr;
+      double nd = 0.0;
+      for (const ORange &r : rs) {
+        const double d = st < r.lo ? r.lo - st : st - r.hi;
+        if (!nr || d < nd) {
+          nr = &r;
+          nd = d;
+        }
+      }
+      if (!nr || !(nd < (nr->hi - nr->lo) * 0.01) || !nr->eval(std::min(std::max(st, nr->lo), nr->hi), &best))
+        return SD_ERR_GRD_INTERPOLATION_FAILED;
+    }
+    ang[c] = best * (M_PI / 180.0);
+  }
+  std::vector<double> gsp(samples), cum;
+  for (uint64_t c = 0; c < samples; ++c) gsp[c] = rps_m / std::sin(ang[c]);
+  double acc = 0.0;
+  cum.push_back(0.0);
+  for (uint64_t c = 1; c < samples; ++c) {
+    acc += (gsp[c - 1] + gsp[c]) / 2.0;
+    cum.push_back(acc);
+  }
+  const uint64_t os = (uint64_t)std::floor(cum.back() / target);
+  if (os == 0) return SD_ERR_GRD_INVALID_SPACING;
+  const uint64_t al = (uint64_t)std::max(std::round(target / az_spacing), 1.0);
+  const uint64_t ol = lines / al;
+  info->lines = ol;
+  info->samples = os;
+  info->range_pixel_spacing_m = target;
+  info->azimuth_pixel_spacing_m = az_spacing * (double)al;
+  info->range_looks = 1;
+  info->azimuth_looks = al;
+  if (!out) return SD_OK;
+  // mapping: (left, right, frac); left == right means Exact
+  std::vector<uint64_t> ml(os), mr(os);
+  std::vector<double> mf(os, 0.0);
+  uint64_t start = 0;
+  for (uint64_t j = 0; j < os; ++j) {
+    const double tg = (double)j * target;
+    uint64_t b = start, e = samples;
+    while (b < e) {
+      const uint64_t m = (b + e) / 2;
+      if (cum[m] < tg) b = m + 1;
+      else e = m;
+    }
+    if (b < samples && cum[b] == tg) {
+      ml[j] = mr[j] = b;
+      start = b;
+    } else if (b == 0) {
+      ml[j] = mr[j] = 0;
+    } else if (b >= samples) {
+      ml[j] = mr[j] = samples - 1;
+    } else {
+      ml[j] = b - 1;
+      mr[j] = b;
+      mf[j] = (tg - cum[b - 1]) / (cum[b] - cum[b - 1]);
+      start = b - 1;
+    }
+  }
+  std::vector<float> proj(lines * os, NAN);
+  for (uint64_t l = 0; l < lines; ++l)
+    for (uint64_t j = 0; j < os; ++j) {
+      const float *row = data + l * samples;
+      float v;
+      if (ml[j] == mr[j]) {
+        v = row[ml[j]];
+      } else {
+        const float v0 = row[ml[j]], v1 = row[mr[j]];
+        v = (std::isnan(v0) || std::isnan(v1)) ? NAN : v0 + (v1 - v0) * (float)mf[j];
+      }
+      proj[l * os + j] = v;
+    }
+  for (uint64_t o = 0; o < ol; ++o)
+    for (uint64_t j = 0; j < os; ++j) {
+      double s = 0.0;
+      uint32_t c = 0;
+      for (uint64_t l = o * al; l < o * al + al; ++l) {
+        const float v = proj[l * os + j];
+        if (!std::isnan(v)) {
+          s += (double)v;
+          ++c;
+        }
+      }
+      out[o * os + j] = c ? (float)(s / (double)c) : NAN;
     }
   return SD_OK;
 }

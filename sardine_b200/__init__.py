@@ -43,7 +43,7 @@ __all__ = [
     "GpuSpeckleKernel", "SardineError", "TerrainCorrectionError", "SpeckleError",
     "CalibrationError", "DeburstError", "MergeError", "Context", "default_context",
     "tc_output_grid", "to_db_inplace", "write_cog_with_crs", "downsample_2x", "ExportError",
-    "SlcReader", "SlcReadError", "apply_multilook",
+    "SlcReader", "SlcReadError", "apply_multilook", "to_ground_range", "GroundRangeError",
 ] + [n for n in dir(T) if n[:1].isupper()]
 
 
@@ -83,6 +83,10 @@ class SlcReadError(SardineError):
     """slc_reader.rs:66-98"""
 
 
+class GroundRangeError(SardineError):
+    """ground_range.rs:42-57"""
+
+
 _KINDS = {
     _abi.SD_ERR_TC_ORBIT: (TerrainCorrectionError, "Orbit"),
     _abi.SD_ERR_TC_DEM: (TerrainCorrectionError, "Dem"),
@@ -117,6 +121,11 @@ _KINDS = {
     _abi.SD_ERR_SLC_UNSUPPORTED_FORMAT: (SlcReadError, "UnsupportedFormat"),
     _abi.SD_ERR_SLC_NON_CONTIGUOUS_STRIPS: (SlcReadError, "NonContiguousStrips"),
     _abi.SD_ERR_SLC_LINE_OUT_OF_BOUNDS: (SlcReadError, "LineOutOfBounds"),
+    _abi.SD_ERR_GRD_NO_GRID_POINTS: (GroundRangeError, "NoGridPoints"),
+    _abi.SD_ERR_GRD_EMPTY_IMAGE: (GroundRangeError, "EmptyImage"),
+    _abi.SD_ERR_GRD_INVALID_SPACING: (GroundRangeError, "InvalidSpacing"),
+    _abi.SD_ERR_GRD_INVALID_AZIMUTH_SPACING: (GroundRangeError, "InvalidAzimuthSpacing"),
+    _abi.SD_ERR_GRD_INTERPOLATION_FAILED: (GroundRangeError, "InterpolationFailed"),
 }
 
 
@@ -544,3 +553,43 @@ def apply_multilook(merged: MergedSigma0, range_looks: int, azimuth_looks: int,
                         merged.near_slant_range_time_s + (range_looks - 1) / 2.0 * merged.range_pixel_spacing_s,
                         merged.range_pixel_spacing_s * range_looks, merged.range_pixel_spacing_m * range_looks,
                         merged.cal_lut_extrapolation_gap_px, merged.noise_lut_extrapolation_gap_px, onz, az0)
+
+
+# ── ground range ───────────────────────────────────────────────────────────
+def _grd_grids(grids):
+    keep, arr = [], (_abi.GrdSwathGrid * max(1, len(grids)))()
+    for k, (sid, pts) in enumerate(grids):
+        p = (_abi.GrdGridPoint * max(1, len(pts)))()
+        for i, g in enumerate(pts):
+            p[i].line = int(g.line)
+            p[i].slant_range_time_s = float(g.slant_range_time_s)
+            p[i].incidence_angle_deg = float(g.incidence_angle_deg)
+        keep.append(p)
+        arr[k].swath_id = int(str(sid)[-1]) if str(sid)[-1:].isdigit() else 0
+        arr[k].points = C.cast(p, C.c_void_p)
+        arr[k].n_points = len(pts)
+    return arr, keep
+
+
+def to_ground_range(merged: MergedSigma0, grids, target_spacing_m: float, azimuth_pixel_spacing_m: float,
+                    ctx: Optional[Context] = None) -> T.GroundRangeImage:
+    """to_ground_range (ground_range.rs:303-427): slant range -> ground range
+    at target_spacing_m, then the azimuth looks; `grids` as for
+    terrain_correction, with each point's line, slant_range_time_s and
+    incidence_angle_deg."""
+    ctx = _ctx(ctx)
+    data = _prep(merged.data, np.float32)
+    arr, keep = _grd_grids(grids)
+    info = _abi.GrdInfo()
+    args = (merged.lines, merged.samples, float(merged.near_slant_range_time_s),
+            float(merged.range_pixel_spacing_s), float(merged.range_pixel_spacing_m), arr, len(grids),
+            float(target_spacing_m), float(azimuth_pixel_spacing_m))
+    rc = lib().sd_to_ground_range(ctx.handle, T.ptr(data), *args, None, C.byref(info))
+    _check(ctx, rc, GroundRangeError)
+    out = _empty_like_kind(data, (max(int(info.lines), 1), int(info.samples)), "f4")
+    if info.lines:
+        rc = lib().sd_to_ground_range(ctx.handle, T.ptr(data), *args, T.ptr(out), C.byref(info))
+        _check(ctx, rc, GroundRangeError)
+    return T.GroundRangeImage(out[: int(info.lines)], int(info.lines), int(info.samples),
+                              info.range_pixel_spacing_m, info.azimuth_pixel_spacing_m, int(info.range_looks),
+                              int(info.azimuth_looks))

@@ -50,6 +50,11 @@ SD_ERR_SLC_MISSING_TAG = 73
 SD_ERR_SLC_UNSUPPORTED_FORMAT = 74
 SD_ERR_SLC_NON_CONTIGUOUS_STRIPS = 75
 SD_ERR_SLC_LINE_OUT_OF_BOUNDS = 76
+SD_ERR_GRD_NO_GRID_POINTS = 80
+SD_ERR_GRD_EMPTY_IMAGE = 81
+SD_ERR_GRD_INVALID_SPACING = 82
+SD_ERR_GRD_INVALID_AZIMUTH_SPACING = 83
+SD_ERR_GRD_INTERPOLATION_FAILED = 84
 
 RESAMPLE_BILINEAR, RESAMPLE_BICUBIC, RESAMPLE_LANCZOS3 = 0, 1, 2
 CRS_WGS84, CRS_UTM_NORTH, CRS_UTM_SOUTH = 0, 1, 2
@@ -90,6 +95,21 @@ class Geoid(C.Structure):
 
 class GeoGridPoint(C.Structure):
     _fields_ = [("azimuth_time_us", C.c_int64), ("latitude_deg", C.c_double)]
+
+
+class GrdGridPoint(C.Structure):
+    _fields_ = [("line", C.c_uint32), ("pad", C.c_uint32), ("slant_range_time_s", C.c_double),
+                ("incidence_angle_deg", C.c_double)]
+
+
+class GrdSwathGrid(C.Structure):
+    _fields_ = [("swath_id", C.c_int32), ("pad", C.c_int32), ("points", C.c_void_p), ("n_points", C.c_uint64)]
+
+
+class GrdInfo(C.Structure):
+    _fields_ = [("lines", C.c_uint64), ("samples", C.c_uint64), ("range_pixel_spacing_m", C.c_double),
+                ("azimuth_pixel_spacing_m", C.c_double), ("range_looks", C.c_uint64),
+                ("azimuth_looks", C.c_uint64)]
 
 
 class TcConfig(C.Structure):

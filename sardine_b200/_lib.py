@@ -61,6 +61,8 @@ _SIGS = {
     "sd_slc_dims": (C.c_int, [P, P, P, P]),
     "sd_slc_close": (None, [P]),
     "sd_multilook": (C.c_int, [P, P, P, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, P, P]),
+    "sd_to_ground_range": (C.c_int, [P, P, C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double, P,
+                                     C.c_int32, C.c_double, C.c_double, P, P]),
     "sd_slc_read_burst_raw": (C.c_int, [P, P, C.c_uint64, C.c_uint64, P]),
     "sd_downsample_2x": (C.c_int, [P, P, C.c_uint64, C.c_uint64, P]),
     "sd_write_cog": (C.c_int, [P, C.c_char_p, P, C.c_uint64, C.c_uint64, P, C.c_int32, C.c_int32, C.c_uint32]),

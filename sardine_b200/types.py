@@ -169,6 +169,20 @@ class GeolocationGridPoint:
     latitude_deg: float
     longitude_deg: float = 0.0
     slant_range_time_s: float = 0.0
+    line: int = 0                    # read by the ground-range projection
+    incidence_angle_deg: float = 0.0
+
+
+@dataclass
+class GroundRangeImage:
+    """ground_range.rs:60-85."""
+    data: Any
+    lines: int
+    samples: int
+    range_pixel_spacing_m: float
+    azimuth_pixel_spacing_m: float
+    range_looks: int
+    azimuth_looks: int
 
 
 def grid_to_c(points: Sequence[GeolocationGridPoint]) -> C.Array:
