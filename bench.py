@@ -1000,6 +1000,37 @@ def run_ingest(args):
         g_bytes = 4 * merged_px + 4 * g.lines * g.samples  # input read once (neighbouring columns share taps)
         ml["grd"] = {"target_m": 10.0, "out": [g.lines, g.samples], "ms": g_ms,
                      "gbs": g_bytes / (g_ms / 1e3) / 1e9, "frac_of_hbm": g_bytes / (g_ms / 1e3) / 1e9 / _hbm_peak()}
+        # TOPS deramping of the first sub-swath as read (CInt16 -> complex f32), nine DC estimates
+        # 2.758 s apart with quadratic range terms, line 0 0.8 s before the first
+        from sardine_b200.types import DcEstimate, DeburstArray
+        sw0 = sc.swaths[0].sw
+        est = [DcEstimate(800_000 + int(2.758e6 * k), sw0.slant_range_time_s + 1e-6 * (k % 3),
+                          [-40.0 + 10.0 * k, 3.0e4 - 7.0e3 * k, -5.0e6 + 1.3e6 * k]) for k in range(9)]
+        sw_dc = type(sw0)(**{**sw0.__dict__, "dc_estimates": est})
+        db = DeburstArray(bufs[0], int(bufs[0].shape[0]), int(bufs[0].shape[1]), 0)
+        for _ in range(2):
+            sd.deramp_subswath(db, sw_dc, 0, ctx=ctx)
+        ctx.set_timing(True)
+        for _ in range(3):
+            dr = sd.deramp_subswath(db, sw_dc, 0, ctx=ctx)
+        kt = ctx.kernel_times()
+        ctx.set_timing(False)
+        d_ms = kt["k_deramp"][0] / 3
+        d_px = db.lines * db.samples
+        d_bytes = 12 * d_px  # 4 B CInt16 in, 8 B complex f32 out
+        del dr
+        ml["deramp"] = {"in": [db.lines, db.samples], "ms": d_ms, "gpx_s": d_px / (d_ms / 1e3) / 1e9,
+                        "gbs": d_bytes / (d_ms / 1e3) / 1e9,
+                        "frac_of_hbm": d_bytes / (d_ms / 1e3) / 1e9 / _hbm_peak()}
+        # the oracle's sequential deramp on the first 64 lines, one host thread
+        import oracle
+        n_cpu = min(64, db.lines)
+        db_cpu = DeburstArray(bufs[0][:n_cpu].cpu().numpy(), n_cpu, db.samples, 0)
+        t_c = time.perf_counter()
+        oracle.deramp_subswath(db_cpu, sw_dc, 0)
+        t_c = time.perf_counter() - t_c
+        ml["deramp"]["cpu_baseline"] = {"value": n_cpu * db.samples / t_c, "unit": "px/s", "cores": 1,
+                                        "kind": "port", "sample": f"{n_cpu} lines x {db.samples} samples"}
     for r in readers:
         r.close()
     for p in paths:

@@ -89,7 +89,10 @@ typedef enum sd_status {
     SD_ERR_GRD_EMPTY_IMAGE = 81,
     SD_ERR_GRD_INVALID_SPACING = 82,
     SD_ERR_GRD_INVALID_AZIMUTH_SPACING = 83,
-    SD_ERR_GRD_INTERPOLATION_FAILED = 84
+    SD_ERR_GRD_INTERPOLATION_FAILED = 84,
+    /* InsarError (insar/error.rs:7-33) */
+    SD_ERR_INSAR_NO_DC_ESTIMATES = 90,
+    SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC = 91
 } sd_status;
 
 /* ── Enumerations mirroring the reference's enums ─────────────────────── */
@@ -582,6 +585,29 @@ int sd_to_ground_range(sd_ctx *ctx, const float *data, uint64_t lines, uint64_t 
                        double range_pixel_spacing_m, const sd_grd_swath_grid *grids, int32_t n_grids,
                        double target_spacing_m, double azimuth_pixel_spacing_m, float *out,
                        sd_grd_info *info);
+
+/* ── TOPS deramping (InSAR) ───────────────────────────────────────────────
+ * deramp_subswath (insar/deramp.rs:114-210) of a debursted sub-swath iq
+ * (lines x samples CInt16 pairs, host or device): out (lines x samples
+ * complex f32 pairs, same kind of memory) = iq * exp(-j phi), phi =
+ * 2 pi f_DC(tau) t_az, tau = slant_range_time_s + (c + valid_sample_offset)
+ * * 2 range_pixel_spacing_m / c, t_az = l * azimuth_time_interval_s and
+ * f_DC = a0 + a1 (tau - t0) + a2 (tau - t0)^2 with (a0, a1, a2, t0)
+ * interpolated linearly in azimuth time between the two estimates around
+ * the line (interp_dc_poly, deramp.rs:227-276; first/last estimate outside
+ * them).  burst_start_us is the azimuth time of line 0; swath_id (1..3 for
+ * IW1..IW3) only names the swath in messages.
+ * Errors: SD_ERR_INSAR_NO_DC_ESTIMATES, SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC
+ * (a line more than 2 s before the first estimate). */
+typedef struct sd_dc_estimate {      /* DcEstimate (types.rs:206-213) */
+    int64_t azimuth_time_us;         /* UTC, microseconds (any fixed epoch shared with burst_start_us) */
+    double t0_s;
+    double data_dc_poly[3];
+} sd_dc_estimate;
+int sd_deramp_subswath(sd_ctx *ctx, const int16_t *iq, uint64_t lines, uint64_t samples,
+                       uint64_t valid_sample_offset, double slant_range_time_s, double range_pixel_spacing_m,
+                       double azimuth_time_interval_s, const sd_dc_estimate *estimates, uint64_t n_estimates,
+                       int64_t burst_start_us, int32_t swath_id, float *out);
 
 /* ── Output: dB conversion and Cloud-Optimised GeoTIFF ───────────────────
  * to_db_inplace (export.rs:59-99) on data[0..n) in place (host or device

@@ -76,6 +76,7 @@ def _declare(L):
         "orc_slc_read": (C.c_int, [C.c_char_p, u64, u64, P, P, P]),
         "orc_multilook": (C.c_int, [P, P, u64, u64, C.c_uint32, C.c_uint32, P, P]),
         "orc_to_ground_range": (C.c_int, [P, u64, u64, d, d, d, P, C.c_int32, d, d, P, P]),
+        "orc_deramp": (C.c_int, [P, u64, u64, u64, d, d, d, P, u64, i64, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -437,3 +438,22 @@ def to_ground_range(merged: T.MergedSigma0, grids, target_spacing_m: float, azim
     rc = lib().orc_to_ground_range(d.ctypes.data, *args, out.ctypes.data if out.size else None, C.byref(info))
     return rc, T.GroundRangeImage(out, int(info.lines), int(info.samples), info.range_pixel_spacing_m,
                                   info.azimuth_pixel_spacing_m, int(info.range_looks), int(info.azimuth_looks))
+
+
+def deramp_subswath(deburst: T.DeburstArray, swath: T.SubSwathMetadata, burst_start_us: int):
+    """deramp_subswath (insar/deramp.rs:114-210): (status, Deramped or None);
+    for AzimuthTimeBeforeDcEstimates the status comes with the failing line's
+    relative time in Deramped.data."""
+    from sardine_b200 import _dc_to_c
+    est = list(swath.dc_estimates or [])
+    iq = np.ascontiguousarray(deburst.data, dtype=np.int16).reshape(-1)
+    lines, samples = int(deburst.lines), int(deburst.samples)
+    out = np.empty((lines, samples, 2), np.float32)
+    bad = C.c_double(0.0)
+    rc = lib().orc_deramp(iq.ctypes.data, lines, samples, int(deburst.valid_sample_offset),
+                          float(swath.slant_range_time_s), float(swath.range_pixel_spacing_m),
+                          float(swath.azimuth_time_interval_s), _dc_to_c(est), len(est), int(burst_start_us),
+                          out.ctypes.data, C.byref(bad))
+    if rc != 0:
+        return rc, (bad.value if rc == _abi.SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC else None)
+    return rc, T.Deramped(out, lines, samples, int(deburst.valid_sample_offset))

@@ -15,6 +15,7 @@
 //   SlcReader              sardine/src/slc_reader.rs:268-583
 //   apply_multilook        sardine/src/scene_prep.rs:1060-1160
 //   to_ground_range        sardine/src/ground_range.rs:148-485
+//   deramp_subswath        sardine/src/insar/deramp.rs:114-276
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -591,5 +592,73 @@ extern "C" int orc_to_ground_range(const float *data, uint64_t lines, uint64_t s
       }
       out[o * os + j] = c ? (float)(s / (double)c) : NAN;
     }
+  return SD_OK;
+}
+
+// deramp_subswath (insar/deramp.rs:114-210) with interp_dc_poly (227-276):
+// the column times, the per-line interpolated polynomials, then one
+// sequential pass over the pixels with the C library's sin and cos.
+namespace {
+int orc_interp_dc(const sd_dc_estimate *e, const std::vector<double> &et, double t, double q[4], double *bad_t) {
+  const size_t n = et.size();
+  const sd_dc_estimate *pick = nullptr;
+  if (t < et[0]) {
+    if (et[0] - t > 2.0) {
+      *bad_t = t;
+      return SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC;
+    }
+    pick = &e[0];
+  } else if (t >= et[n - 1]) {
+    pick = &e[n - 1];
+  }
+  if (pick) {
+    q[0] = pick->data_dc_poly[0];
+    q[1] = pick->data_dc_poly[1];
+    q[2] = pick->data_dc_poly[2];
+    q[3] = pick->t0_s;
+    return SD_OK;
+  }
+  size_t k = n - 2;
+  for (size_t j = 0; j + 1 < n; ++j)
+    if (t >= et[j] && t < et[j + 1]) {
+      k = j;
+      break;
+    }
+  const double a = (t - et[k]) / (et[k + 1] - et[k]);
+  for (int j = 0; j < 3; ++j) q[j] = e[k].data_dc_poly[j] + (e[k + 1].data_dc_poly[j] - e[k].data_dc_poly[j]) * a;
+  q[3] = e[k].t0_s + (e[k + 1].t0_s - e[k].t0_s) * a;
+  return SD_OK;
+}
+}  // namespace
+
+extern "C" int orc_deramp(const int16_t *iq, uint64_t lines, uint64_t samples, uint64_t col_off, double near_tau,
+                          double rps_m, double ati, const sd_dc_estimate *est, uint64_t n_est, int64_t start_us,
+                          float *out, double *bad_t) {
+  if (n_est == 0) return SD_ERR_INSAR_NO_DC_ESTIMATES;
+  const double dtau = 2.0 * rps_m / 299792458.0;
+  std::vector<double> tau(samples);
+  for (uint64_t c = 0; c < samples; ++c) tau[c] = near_tau + (double)(c + col_off) * dtau;
+  std::vector<double> et(n_est);
+  for (uint64_t k = 0; k < n_est; ++k) et[k] = (double)(est[k].azimuth_time_us - start_us) / 1e6;
+  std::vector<double> poly(4 * lines);
+  for (uint64_t l = 0; l < lines; ++l) {
+    const int rc = orc_interp_dc(est, et, (double)l * ati, &poly[4 * l], bad_t);
+    if (rc) return rc;
+  }
+  const double two_pi = 6.283185307179586;
+  for (uint64_t l = 0; l < lines; ++l) {
+    const double *q = &poly[4 * l];
+    const double t_az = (double)l * ati;
+    for (uint64_t c = 0; c < samples; ++c) {
+      const double dt = tau[c] - q[3];
+      const double f_dc = q[0] + q[1] * dt + q[2] * dt * dt;
+      const double phi = two_pi * f_dc * t_az;
+      const double sp = std::sin(phi), cp = std::cos(phi);
+      const uint64_t i = l * samples + c;
+      const double iv = iq[2 * i], qv = iq[2 * i + 1];
+      out[2 * i] = (float)(iv * cp + qv * sp);
+      out[2 * i + 1] = (float)(qv * cp - iv * sp);
+    }
+  }
   return SD_OK;
 }

@@ -31,8 +31,8 @@ import numpy as np
 from . import _abi
 from . import types as T
 from ._lib import Context, default_context, lib
-from .types import (BoundingBox, BurstEntry, CalibrationVector, DeburstArray, DemGrid,
-                    GeocodedImage, GeoidModel, GeolocationGridPoint, MergedSigma0, NoiseAzimuthVector,
+from .types import (BoundingBox, BurstEntry, CalibrationVector, DcEstimate, DeburstArray, Deramped, DemGrid,
+                    GeocodedImage, GroundRangeImage, GeoidModel, GeolocationGridPoint, MergedSigma0, NoiseAzimuthVector,
                     NoiseRangeVector, OrbitData, OutputCrs, Precision, ResamplingKernel, SceneMetadata,
                     Sigma0Array, SpeckleFilter, SubSwathMetadata, SwathCalibration, SwathInput,
                     SwathNoise, TerrainCorrectionConfig)
@@ -44,7 +44,8 @@ __all__ = [
     "CalibrationError", "DeburstError", "MergeError", "Context", "default_context",
     "tc_output_grid", "to_db_inplace", "write_cog_with_crs", "downsample_2x", "ExportError",
     "SlcReader", "SlcReadError", "apply_multilook", "to_ground_range", "GroundRangeError",
-] + [n for n in dir(T) if n[:1].isupper()]
+    "deramp_subswath", "InsarError",
+] + [n for n in dir(T) if n[:1].isupper() and getattr(getattr(T, n), "__module__", "") == T.__name__]
 
 
 # ── errors (one class per reference error enum; .kind = variant name) ──────
@@ -81,6 +82,10 @@ class ExportError(SardineError):
 
 class SlcReadError(SardineError):
     """slc_reader.rs:66-98"""
+
+
+class InsarError(SardineError):
+    """insar/error.rs:7-80"""
 
 
 class GroundRangeError(SardineError):
@@ -126,6 +131,8 @@ _KINDS = {
     _abi.SD_ERR_GRD_INVALID_SPACING: (GroundRangeError, "InvalidSpacing"),
     _abi.SD_ERR_GRD_INVALID_AZIMUTH_SPACING: (GroundRangeError, "InvalidAzimuthSpacing"),
     _abi.SD_ERR_GRD_INTERPOLATION_FAILED: (GroundRangeError, "InterpolationFailed"),
+    _abi.SD_ERR_INSAR_NO_DC_ESTIMATES: (InsarError, "NoDcEstimates"),
+    _abi.SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC: (InsarError, "AzimuthTimeBeforeDcEstimates"),
 }
 
 
@@ -593,3 +600,34 @@ def to_ground_range(merged: MergedSigma0, grids, target_spacing_m: float, azimut
     return T.GroundRangeImage(out[: int(info.lines)], int(info.lines), int(info.samples),
                               info.range_pixel_spacing_m, info.azimuth_pixel_spacing_m, int(info.range_looks),
                               int(info.azimuth_looks))
+
+
+# ── InSAR: TOPS deramping ──────────────────────────────────────────────────
+def _dc_to_c(estimates):
+    arr = (_abi.DcEstimateC * max(1, len(estimates)))()
+    for k, e in enumerate(estimates):
+        arr[k].azimuth_time_us = int(e.azimuth_time_us)
+        arr[k].t0_s = float(e.t0_s)
+        for j in range(3):
+            arr[k].data_dc_poly[j] = float(e.data_dc_poly[j])
+    return arr
+
+
+def deramp_subswath(deburst: DeburstArray, swath: SubSwathMetadata, burst_start_us: int,
+                    ctx: Optional[Context] = None) -> T.Deramped:
+    """deramp_subswath (insar/deramp.rs:114-210): every CInt16 sample of the
+    debursted sub-swath times exp(-j 2 pi f_DC(tau_c) t_az(l)), as complex
+    f32 (lines, samples, 2) in the input's kind of memory.  burst_start_us is
+    the UTC azimuth time (microseconds) of the first line."""
+    ctx = _ctx(ctx)
+    est = list(swath.dc_estimates or [])
+    iq = _prep(deburst.data, np.int16)
+    lines, samples = int(deburst.lines), int(deburst.samples)
+    out = _empty_like_kind(iq, (lines, samples, 2), "f4")
+    sid = int(str(swath.id)[-1]) if str(swath.id)[-1:].isdigit() else 0
+    rc = lib().sd_deramp_subswath(ctx.handle, T.ptr(iq), lines, samples, int(deburst.valid_sample_offset),
+                                  float(swath.slant_range_time_s), float(swath.range_pixel_spacing_m),
+                                  float(swath.azimuth_time_interval_s), _dc_to_c(est), len(est),
+                                  int(burst_start_us), sid, T.ptr(out))
+    _check(ctx, rc, InsarError)
+    return T.Deramped(out, lines, samples, int(deburst.valid_sample_offset))

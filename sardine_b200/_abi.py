@@ -55,6 +55,8 @@ SD_ERR_GRD_EMPTY_IMAGE = 81
 SD_ERR_GRD_INVALID_SPACING = 82
 SD_ERR_GRD_INVALID_AZIMUTH_SPACING = 83
 SD_ERR_GRD_INTERPOLATION_FAILED = 84
+SD_ERR_INSAR_NO_DC_ESTIMATES = 90
+SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC = 91
 
 RESAMPLE_BILINEAR, RESAMPLE_BICUBIC, RESAMPLE_LANCZOS3 = 0, 1, 2
 CRS_WGS84, CRS_UTM_NORTH, CRS_UTM_SOUTH = 0, 1, 2
@@ -110,6 +112,10 @@ class GrdInfo(C.Structure):
     _fields_ = [("lines", C.c_uint64), ("samples", C.c_uint64), ("range_pixel_spacing_m", C.c_double),
                 ("azimuth_pixel_spacing_m", C.c_double), ("range_looks", C.c_uint64),
                 ("azimuth_looks", C.c_uint64)]
+
+
+class DcEstimateC(C.Structure):
+    _fields_ = [("azimuth_time_us", C.c_int64), ("t0_s", C.c_double), ("data_dc_poly", C.c_double * 3)]
 
 
 class TcConfig(C.Structure):

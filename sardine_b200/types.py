@@ -124,6 +124,7 @@ class SubSwathMetadata:
     azimuth_time_interval_s: float
     range_pixel_spacing_m: float
     slant_range_time_s: float
+    dc_estimates: list = None  # [DcEstimate]; deramp_subswath needs them
 
     def to_c(self) -> _abi.SubSwath:
         return _abi.SubSwath(self.burst_count, self.lines_per_burst, self.azimuth_time_interval_s,
@@ -171,6 +172,24 @@ class GeolocationGridPoint:
     slant_range_time_s: float = 0.0
     line: int = 0                    # read by the ground-range projection
     incidence_angle_deg: float = 0.0
+
+
+@dataclass
+class DcEstimate:
+    """types.rs:206-213: a Doppler-centroid polynomial f_DC(tau) = a0 + a1 (tau - t0)
+    + a2 (tau - t0)^2 valid around azimuth_time_us (UTC microseconds)."""
+    azimuth_time_us: int
+    t0_s: float
+    data_dc_poly: Sequence[float]
+
+
+@dataclass
+class Deramped:
+    """insar/deramp.rs:73-84.  data: (lines, samples, 2) float32 [I, Q]."""
+    data: Any
+    lines: int
+    samples: int
+    valid_sample_offset: int
 
 
 @dataclass
