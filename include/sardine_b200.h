@@ -92,7 +92,9 @@ typedef enum sd_status {
     SD_ERR_GRD_INTERPOLATION_FAILED = 84,
     /* InsarError (insar/error.rs:7-33) */
     SD_ERR_INSAR_NO_DC_ESTIMATES = 90,
-    SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC = 91
+    SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC = 91,
+    SD_ERR_INSAR_INVALID_WINDOW_SIZE = 92,
+    SD_ERR_INSAR_ORBIT = 93
 } sd_status;
 
 /* ── Enumerations mirroring the reference's enums ─────────────────────── */
@@ -608,6 +610,34 @@ int sd_deramp_subswath(sd_ctx *ctx, const int16_t *iq, uint64_t lines, uint64_t 
                        uint64_t valid_sample_offset, double slant_range_time_s, double range_pixel_spacing_m,
                        double azimuth_time_interval_s, const sd_dc_estimate *estimates, uint64_t n_estimates,
                        int64_t burst_start_us, int32_t swath_id, float *out);
+
+/* resample_secondary (insar/coreg.rs:230-264): out (lines x samples complex
+ * f32) at reference pixel (l, c) is the bilinear sample (coreg.rs:428-456;
+ * f32 weights, zero outside) of sec (sec_lines x sec_samples complex f32) at
+ * (l + P_az(l, c), c + P_rg(l, c)), P(l, c) = p0 + p1 l + p2 c + p3 l^2 +
+ * p4 l c + p5 c^2 (CoregPoly, coreg.rs:73-90).  Host or device memory. */
+int sd_resample_secondary(sd_ctx *ctx, const float *sec, uint64_t sec_lines, uint64_t sec_samples,
+                          uint64_t lines, uint64_t samples, const double *az_poly, const double *rg_poly,
+                          float *out);
+
+/* form_interferogram (insar/interferogram.rs:165-398) of a co-registered
+ * pair ref, sec (lines x samples complex f32, host or device): per pixel the
+ * flat-earth phase (4 pi / wavelength) (R_ref - R_sec) of the point on the
+ * WGS84 ellipsoid at the reference range in the zero-Doppler plane of the
+ * reference state at line time ref_first_us + trunc(l * ATI * 1e6) us
+ * (ecef_from_slant_range_doppler, coreg.rs:280-362; 0 where it does not
+ * converge), igram = ref conj(sec) exp(+j phi_flat), then over the window of
+ * rows l -+ az_looks/2 and columns c -+ rg_looks/2 (clamped to the image)
+ * coherence = min(|sum igram| / sqrt(sum |ref|^2 sum |sec|^2), 1) (0 when the
+ * powers sum to 0) and, when phase != NULL, phase = atan2 of the summed
+ * igram.  Errors: SD_ERR_INSAR_INVALID_WINDOW_SIZE (a zero window),
+ * SD_ERR_INSAR_ORBIT (a line time outside either orbit). */
+int sd_form_interferogram(sd_ctx *ctx, const float *ref, const float *sec, uint64_t lines, uint64_t samples,
+                          uint64_t valid_sample_offset, double slant_range_time_s, double range_pixel_spacing_m,
+                          double azimuth_time_interval_s, const sd_state_vector *ref_orbit, uint64_t n_ref,
+                          int64_t ref_first_us, const sd_state_vector *sec_orbit, uint64_t n_sec,
+                          double wavelength_m, uint32_t az_looks, uint32_t rg_looks, float *coherence,
+                          float *phase);
 
 /* ── Output: dB conversion and Cloud-Optimised GeoTIFF ───────────────────
  * to_db_inplace (export.rs:59-99) on data[0..n) in place (host or device

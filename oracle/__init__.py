@@ -77,6 +77,10 @@ def _declare(L):
         "orc_multilook": (C.c_int, [P, P, u64, u64, C.c_uint32, C.c_uint32, P, P]),
         "orc_to_ground_range": (C.c_int, [P, u64, u64, d, d, d, P, C.c_int32, d, d, P, P]),
         "orc_deramp": (C.c_int, [P, u64, u64, u64, d, d, d, P, u64, i64, P, P]),
+        "orc_resample_secondary": (C.c_int, [P, u64, u64, u64, u64, P, P, P]),
+        "orc_ecef_from_slant_range_doppler": (C.c_int, [P, P, d, u64, d, P]),
+        "orc_form_interferogram": (C.c_int, [P, P, u64, u64, u64, d, d, d, P, u64, i64, P, u64, d, u64, u64, P,
+                                             P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -457,3 +461,45 @@ def deramp_subswath(deburst: T.DeburstArray, swath: T.SubSwathMetadata, burst_st
     if rc != 0:
         return rc, (bad.value if rc == _abi.SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC else None)
     return rc, T.Deramped(out, lines, samples, int(deburst.valid_sample_offset))
+
+
+def resample_secondary(ref_lines: int, ref_samples: int, poly: T.CoregPoly, secondary: T.Deramped):
+    """resample_secondary (insar/coreg.rs:230-264): Deramped."""
+    sec = np.ascontiguousarray(secondary.data, dtype=np.float32).reshape(-1)
+    out = np.empty((int(ref_lines), int(ref_samples), 2), np.float32)
+    az = (C.c_double * 6)(*[float(v) for v in poly.az])
+    rg = (C.c_double * 6)(*[float(v) for v in poly.rg])
+    _check(lib().orc_resample_secondary(sec.ctypes.data, int(secondary.lines), int(secondary.samples),
+                                        int(ref_lines), int(ref_samples), az, rg, out.ctypes.data),
+           "resample_secondary")
+    return T.Deramped(out, int(ref_lines), int(ref_samples), int(secondary.valid_sample_offset))
+
+
+def ecef_from_slant_range_doppler(sat_pos, sat_vel, range_m: float, max_iter: int, tol_m: float):
+    """ecef_from_slant_range_doppler (insar/coreg.rs:280-362): the point, or None."""
+    out = (C.c_double * 3)()
+    rc = lib().orc_ecef_from_slant_range_doppler((C.c_double * 3)(*sat_pos), (C.c_double * 3)(*sat_vel),
+                                                 float(range_m), int(max_iter), float(tol_m), out)
+    return None if rc else (out[0], out[1], out[2])
+
+
+def form_interferogram(coreg: T.Coregistered, ref_swath: T.SubSwathMetadata, ref_orbit: T.OrbitData,
+                       ref_first_us: int, sec_orbit: T.OrbitData, wavelength_m: float,
+                       cfg: T.InterferogramConfig = None):
+    """form_interferogram (insar/interferogram.rs:165-398): (status, Interferogram or None)."""
+    cfg = cfg or T.InterferogramConfig()
+    r, s_ = coreg.ref_data, coreg.secondary_resampled
+    ref = np.ascontiguousarray(r.data, dtype=np.float32).reshape(-1)
+    sec = np.ascontiguousarray(s_.data, dtype=np.float32).reshape(-1)
+    lines, samples = int(r.lines), int(r.samples)
+    coh = np.empty((lines, samples), np.float32)
+    ph = np.empty((lines, samples), np.float32) if cfg.compute_phase else None
+    rc = lib().orc_form_interferogram(ref.ctypes.data, sec.ctypes.data, lines, samples, int(r.valid_sample_offset),
+                                      float(ref_swath.slant_range_time_s), float(ref_swath.range_pixel_spacing_m),
+                                      float(ref_swath.azimuth_time_interval_s), ref_orbit.to_c(),
+                                      len(ref_orbit.times_us), int(ref_first_us), sec_orbit.to_c(),
+                                      len(sec_orbit.times_us), float(wavelength_m), int(cfg.az_looks),
+                                      int(cfg.rg_looks), coh.ctypes.data, None if ph is None else ph.ctypes.data)
+    if rc:
+        return rc, None
+    return rc, T.Interferogram(coh, ph, lines, samples, int(cfg.az_looks), int(cfg.rg_looks))

@@ -16,6 +16,9 @@
 //   apply_multilook        sardine/src/scene_prep.rs:1060-1160
 //   to_ground_range        sardine/src/ground_range.rs:148-485
 //   deramp_subswath        sardine/src/insar/deramp.rs:114-276
+//   resample_secondary     sardine/src/insar/coreg.rs:230-264, 428-466
+//   ecef_from_slant_range_doppler  sardine/src/insar/coreg.rs:280-362
+//   form_interferogram     sardine/src/insar/interferogram.rs:165-398
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -658,6 +661,144 @@ extern "C" int orc_deramp(const int16_t *iq, uint64_t lines, uint64_t samples, u
       const double iv = iq[2 * i], qv = iq[2 * i + 1];
       out[2 * i] = (float)(iv * cp + qv * sp);
       out[2 * i + 1] = (float)(qv * cp - iv * sp);
+    }
+  }
+  return SD_OK;
+}
+
+// ── InSAR: co-registration resampling and interferogram ──────────────────
+extern "C" int orc_interpolate_orbit_and_accel(const sd_state_vector *svs, uint64_t n, int64_t t, double *pos,
+                                               double *vel, double *acc);
+
+namespace {
+// eval_poly6 (coreg.rs:462-464)
+double orc_poly6(const double *p, double l, double c) {
+  return p[0] + p[1] * l + p[2] * c + p[3] * l * l + p[4] * l * c + p[5] * c * c;
+}
+
+// bilinear (coreg.rs:428-456); `l as usize` of NaN is 0 in Rust
+void orc_bilinear(const float *sec, uint64_t lines, uint64_t samples, double l, double c, float *o) {
+  o[0] = o[1] = 0.0f;
+  if (l < 0.0 || c < 0.0) return;
+  const double lf = std::floor(l), cf = std::floor(c);
+  // `as usize`: NaN -> 0; indices at or past the end only need to fail the bounds test below
+  const uint64_t l0 = lf == lf ? (lf < (double)lines ? (uint64_t)lf : lines) : 0;
+  const uint64_t c0 = cf == cf ? (cf < (double)samples ? (uint64_t)cf : samples) : 0;
+  const uint64_t l1 = l0 + 1, c1 = c0 + 1;
+  if (l1 >= lines || c1 >= samples) return;
+  const float wl = (float)(l - (double)l0), wc = (float)(c - (double)c0);
+  auto lerp = [](float a, float b, float t) { return a + (b - a) * t; };
+  for (int k = 0; k < 2; ++k) {
+    const float p00 = sec[2 * (l0 * samples + c0) + k], p01 = sec[2 * (l0 * samples + c1) + k];
+    const float p10 = sec[2 * (l1 * samples + c0) + k], p11 = sec[2 * (l1 * samples + c1) + k];
+    o[k] = lerp(lerp(p00, p01, wc), lerp(p10, p11, wc), wl);
+  }
+}
+}  // namespace
+
+extern "C" int orc_resample_secondary(const float *sec, uint64_t sec_lines, uint64_t sec_samples, uint64_t lines,
+                                      uint64_t samples, const double *az, const double *rg, float *out) {
+  for (uint64_t l = 0; l < lines; ++l)
+    for (uint64_t c = 0; c < samples; ++c) {
+      const double lf = (double)l, cf = (double)c;
+      const double ls = lf + orc_poly6(az, lf, cf), cs = cf + orc_poly6(rg, lf, cf);
+      orc_bilinear(sec, sec_lines, sec_samples, ls, cs, out + 2 * (l * samples + c));
+    }
+  return SD_OK;
+}
+
+// ecef_from_slant_range_doppler (coreg.rs:280-362): 0 and the point, or 1.
+extern "C" int orc_ecef_from_slant_range_doppler(const double *sat_pos, const double *sat_vel, double range_m,
+                                                 uint64_t max_iter, double tol_m, double *out) {
+  const double px = sat_pos[0], py = sat_pos[1], pz = sat_pos[2];
+  const double vx = sat_vel[0], vy = sat_vel[1], vz = sat_vel[2];
+  const double r = range_m, a = 6378137.0, b = 6356752.314245;
+  const double sat_r = std::sqrt(px * px + py * py + pz * pz);
+  const double scale = a / sat_r;
+  double tx = px * scale, ty = py * scale, tz = pz * scale * (b / a);
+  for (uint64_t it = 0; it < max_iter; ++it) {
+    const double dx = tx - px, dy = ty - py, dz = tz - pz;
+    const double f1 = dx * vx + dy * vy + dz * vz;
+    const double f2 = dx * dx + dy * dy + dz * dz - r * r;
+    const double f3 = tx * tx / (a * a) + ty * ty / (a * a) + tz * tz / (b * b) - 1.0;
+    const double j00 = vx, j01 = vy, j02 = vz;
+    const double j10 = 2.0 * dx, j11 = 2.0 * dy, j12 = 2.0 * dz;
+    const double j20 = 2.0 * tx / (a * a), j21 = 2.0 * ty / (a * a), j22 = 2.0 * tz / (b * b);
+    const double det = j00 * (j11 * j22 - j12 * j21) - j01 * (j10 * j22 - j12 * j20) + j02 * (j10 * j21 - j11 * j20);
+    if (std::fabs(det) < 1e-20) return 1;
+    const double dxt = (f1 * (j11 * j22 - j12 * j21) - j01 * (f2 * j22 - j12 * f3) + j02 * (f2 * j21 - j11 * f3)) / det;
+    const double dyt = (j00 * (f2 * j22 - j12 * f3) - f1 * (j10 * j22 - j12 * j20) + j02 * (j10 * f3 - f2 * j20)) / det;
+    const double dzt = (j00 * (j11 * f3 - f2 * j21) - j01 * (j10 * f3 - f2 * j20) + f1 * (j10 * j21 - j11 * j20)) / det;
+    tx -= dxt;
+    ty -= dyt;
+    tz -= dzt;
+    if (std::sqrt(dxt * dxt + dyt * dyt + dzt * dzt) < tol_m) {
+      out[0] = tx, out[1] = ty, out[2] = tz;
+      return 0;
+    }
+  }
+  return 1;
+}
+
+// form_interferogram (interferogram.rs:165-398), its three loops in turn.
+extern "C" int orc_form_interferogram(const float *ref, const float *sec, uint64_t lines, uint64_t samples,
+                                      uint64_t col_off, double srt, double rps_m, double ati,
+                                      const sd_state_vector *ref_svs, uint64_t n_ref, int64_t first_us,
+                                      const sd_state_vector *sec_svs, uint64_t n_sec, double wavelength_m,
+                                      uint64_t az_looks, uint64_t rg_looks, float *coh, float *phase) {
+  if (az_looks == 0 || rg_looks == 0) return SD_ERR_INSAR_INVALID_WINDOW_SIZE;
+  const uint64_t n = lines * samples;
+  const double c_light = 299792458.0;
+  const double dtau = 2.0 * rps_m / c_light, off = (double)col_off;
+  const double k = 6.283185307179586 / wavelength_m;
+  std::vector<float> fe(n);
+  for (uint64_t l = 0; l < lines; ++l) {
+    const int64_t t = first_us + (int64_t)((double)l * ati * 1e6);
+    double pr[3], vr[3], ps[3], vs[3], acc[3];
+    if (orc_interpolate_orbit_and_accel(ref_svs, n_ref, t, pr, vr, acc) != 0) return SD_ERR_INSAR_ORBIT;
+    if (orc_interpolate_orbit_and_accel(sec_svs, n_sec, t, ps, vs, acc) != 0) return SD_ERR_INSAR_ORBIT;
+    for (uint64_t c = 0; c < samples; ++c) {
+      const double tau = srt + ((double)c + off) * dtau;
+      const double r_ref = tau * c_light / 2.0;
+      double p[3];
+      if (orc_ecef_from_slant_range_doppler(pr, vr, r_ref, 10, 1.0, p) != 0) {
+        fe[l * samples + c] = 0.0f;
+        continue;
+      }
+      const double dx = ps[0] - p[0], dy = ps[1] - p[1], dz = ps[2] - p[2];
+      const double r_sec = std::sqrt(dx * dx + dy * dy + dz * dz);
+      fe[l * samples + c] = (float)(k * 2.0 * (r_ref - r_sec));
+    }
+  }
+  std::vector<float> ig_re(n), ig_im(n), rp(n), sp(n);
+  for (uint64_t i = 0; i < n; ++i) {
+    const float ri = ref[2 * i], rq = ref[2 * i + 1], si = sec[2 * i], sq = sec[2 * i + 1];
+    const double phi = (double)fe[i];
+    const double sn = std::sin(phi), cs = std::cos(phi);
+    const double re = (double)si * cs + (double)sq * sn;
+    const double im = (double)si * sn - (double)sq * cs;
+    ig_re[i] = (float)((double)ri * re - (double)rq * im);
+    ig_im[i] = (float)((double)ri * im + (double)rq * re);
+    rp[i] = ri * ri + rq * rq;
+    sp[i] = si * si + sq * sq;
+  }
+  const uint64_t ah = az_looks / 2, rh = rg_looks / 2;
+  for (uint64_t l = 0; l < lines; ++l) {
+    const uint64_t l0 = l > ah ? l - ah : 0, l1 = std::min(l + ah + 1, lines);
+    for (uint64_t c = 0; c < samples; ++c) {
+      const uint64_t c0 = c > rh ? c - rh : 0, c1 = std::min(c + rh + 1, samples);
+      double sre = 0.0, sim = 0.0, srp = 0.0, ssp = 0.0;
+      for (uint64_t wl = l0; wl < l1; ++wl)
+        for (uint64_t wc = c0; wc < c1; ++wc) {
+          const uint64_t w = wl * samples + wc;
+          sre += (double)ig_re[w];
+          sim += (double)ig_im[w];
+          srp += (double)rp[w];
+          ssp += (double)sp[w];
+        }
+      const double den = std::sqrt(srp * ssp);
+      coh[l * samples + c] = den > 0.0 ? (float)std::fmin(std::sqrt(sre * sre + sim * sim) / den, 1.0) : 0.0f;
+      if (phase) phase[l * samples + c] = (float)std::atan2(sim, sre);
     }
   }
   return SD_OK;

@@ -31,8 +31,8 @@ import numpy as np
 from . import _abi
 from . import types as T
 from ._lib import Context, default_context, lib
-from .types import (BoundingBox, BurstEntry, CalibrationVector, DcEstimate, DeburstArray, Deramped, DemGrid,
-                    GeocodedImage, GroundRangeImage, GeoidModel, GeolocationGridPoint, MergedSigma0, NoiseAzimuthVector,
+from .types import (BoundingBox, BurstEntry, CalibrationVector, CoregPoly, Coregistered, DcEstimate, DeburstArray, Deramped, DemGrid,
+                    GeocodedImage, GroundRangeImage, Interferogram, InterferogramConfig, GeoidModel, GeolocationGridPoint, MergedSigma0, NoiseAzimuthVector,
                     NoiseRangeVector, OrbitData, OutputCrs, Precision, ResamplingKernel, SceneMetadata,
                     Sigma0Array, SpeckleFilter, SubSwathMetadata, SwathCalibration, SwathInput,
                     SwathNoise, TerrainCorrectionConfig)
@@ -44,7 +44,7 @@ __all__ = [
     "CalibrationError", "DeburstError", "MergeError", "Context", "default_context",
     "tc_output_grid", "to_db_inplace", "write_cog_with_crs", "downsample_2x", "ExportError",
     "SlcReader", "SlcReadError", "apply_multilook", "to_ground_range", "GroundRangeError",
-    "deramp_subswath", "InsarError",
+    "deramp_subswath", "InsarError", "resample_secondary", "form_interferogram",
 ] + [n for n in dir(T) if n[:1].isupper() and getattr(getattr(T, n), "__module__", "") == T.__name__]
 
 
@@ -133,6 +133,8 @@ _KINDS = {
     _abi.SD_ERR_GRD_INTERPOLATION_FAILED: (GroundRangeError, "InterpolationFailed"),
     _abi.SD_ERR_INSAR_NO_DC_ESTIMATES: (InsarError, "NoDcEstimates"),
     _abi.SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC: (InsarError, "AzimuthTimeBeforeDcEstimates"),
+    _abi.SD_ERR_INSAR_INVALID_WINDOW_SIZE: (InsarError, "InvalidWindowSize"),
+    _abi.SD_ERR_INSAR_ORBIT: (InsarError, "Orbit"),
 }
 
 
@@ -631,3 +633,46 @@ def deramp_subswath(deburst: DeburstArray, swath: SubSwathMetadata, burst_start_
                                   int(burst_start_us), sid, T.ptr(out))
     _check(ctx, rc, InsarError)
     return T.Deramped(out, lines, samples, int(deburst.valid_sample_offset))
+
+
+# ── InSAR: co-registration resampling, interferogram and coherence ─────────
+def resample_secondary(ref_lines: int, ref_samples: int, poly: T.CoregPoly, secondary: T.Deramped,
+                       ctx: Optional[Context] = None) -> T.Deramped:
+    """resample_secondary (insar/coreg.rs:230-264): the secondary sampled
+    bilinearly at each reference pixel moved by the offset polynomials;
+    zero outside the secondary."""
+    ctx = _ctx(ctx)
+    sec = _prep(secondary.data, np.float32)
+    out = _empty_like_kind(sec, (int(ref_lines), int(ref_samples), 2), "f4")
+    az = (C.c_double * 6)(*[float(v) for v in poly.az])
+    rg = (C.c_double * 6)(*[float(v) for v in poly.rg])
+    rc = lib().sd_resample_secondary(ctx.handle, T.ptr(sec), int(secondary.lines), int(secondary.samples),
+                                     int(ref_lines), int(ref_samples), az, rg, T.ptr(out))
+    _check(ctx, rc, InsarError)
+    return T.Deramped(out, int(ref_lines), int(ref_samples), int(secondary.valid_sample_offset))
+
+
+def form_interferogram(coreg: T.Coregistered, ref_swath: SubSwathMetadata, ref_orbit: OrbitData,
+                       ref_first_us: int, sec_orbit: OrbitData, wavelength_m: float,
+                       cfg: Optional[T.InterferogramConfig] = None,
+                       ctx: Optional[Context] = None) -> T.Interferogram:
+    """form_interferogram (insar/interferogram.rs:165-398): flat-earth phase,
+    cross-product and windowed coherence (and the wrapped phase when
+    cfg.compute_phase) in the reference's slant-range geometry."""
+    ctx = _ctx(ctx)
+    cfg = cfg or T.InterferogramConfig()
+    r, s_ = coreg.ref_data, coreg.secondary_resampled
+    ref = _prep(r.data, np.float32)
+    sec = _prep(s_.data, np.float32)
+    lines, samples = int(r.lines), int(r.samples)
+    coh = _empty_like_kind(ref, (lines, samples), "f4")
+    ph = _empty_like_kind(ref, (lines, samples), "f4") if cfg.compute_phase else None
+    ro, so = ref_orbit.to_c(), sec_orbit.to_c()
+    rc = lib().sd_form_interferogram(ctx.handle, T.ptr(ref), T.ptr(sec), lines, samples,
+                                     int(r.valid_sample_offset), float(ref_swath.slant_range_time_s),
+                                     float(ref_swath.range_pixel_spacing_m),
+                                     float(ref_swath.azimuth_time_interval_s), ro, len(ref_orbit.times_us),
+                                     int(ref_first_us), so, len(sec_orbit.times_us), float(wavelength_m),
+                                     int(cfg.az_looks), int(cfg.rg_looks), T.ptr(coh), T.ptr(ph))
+    _check(ctx, rc, InsarError)
+    return T.Interferogram(coh, ph, lines, samples, int(cfg.az_looks), int(cfg.rg_looks))

@@ -57,6 +57,8 @@ SD_ERR_GRD_INVALID_AZIMUTH_SPACING = 83
 SD_ERR_GRD_INTERPOLATION_FAILED = 84
 SD_ERR_INSAR_NO_DC_ESTIMATES = 90
 SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC = 91
+SD_ERR_INSAR_INVALID_WINDOW_SIZE = 92
+SD_ERR_INSAR_ORBIT = 93
 
 RESAMPLE_BILINEAR, RESAMPLE_BICUBIC, RESAMPLE_LANCZOS3 = 0, 1, 2
 CRS_WGS84, CRS_UTM_NORTH, CRS_UTM_SOUTH = 0, 1, 2

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libsardine_b200.so")
-SOURCES = ["runtime.cu", "tc.cu", "tc_tiles.cu", "speckle.cu", "calib.cu", "diag.cu", "export.cu", "slc.cu", "multilook.cu", "grd.cu", "deramp.cu"]
+SOURCES = ["runtime.cu", "tc.cu", "tc_tiles.cu", "speckle.cu", "calib.cu", "diag.cu", "export.cu", "slc.cu", "multilook.cu", "grd.cu", "deramp.cu", "insar.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -1,0 +1,282 @@
+// InSAR after deramping: co-registration resampling of the secondary
+// (resample_secondary, insar/coreg.rs:230-264) and interferogram formation
+// with coherence (form_interferogram, insar/interferogram.rs:165-398).
+//
+// k_coreg_resample: one thread per reference pixel; the degree-2 offset
+//   polynomials in f64 and the f32 bilinear gather of coreg.rs:428-456.
+// k_igram: one thread per pixel; the flat-earth point by the 3x3 Newton
+//   solve of ecef_from_slant_range_doppler (coreg.rs:280-362) from the
+//   line's reference state, the secondary range, the f32 flat-earth phase,
+//   its FP64 sincos and the cross-product.  It writes {Re, Im, |ref|^2,
+//   |sec|^2} as one float4 a pixel; the satellite states per line come from
+//   the host (orbit_eval, the reference's Lagrange interpolation).
+// k_coherence: the boxcar sums in f64, each output in the reference's
+//   order (window rows ascending, columns ascending within a row), so the
+//   sums equal a sequential evaluation bit for bit.  A thread owns R
+//   outputs of one column on consecutive rows; every window pixel it loads
+//   is added to each of its outputs whose window holds that row, which
+//   keeps each output's order and shares the load and the f32->f64
+//   conversions.  The block's window rows and columns are staged in
+//   shared memory when they fit.
+#include <cmath>
+#include <vector>
+
+#include "geo.cuh"
+#include "runtime.cuh"
+
+namespace sd {
+namespace {
+
+constexpr double kC = 299792458.0;
+constexpr double kA = 6378137.0, kB = 6356752.314245;  // WGS84 (interferogram.rs / coreg.rs)
+constexpr int kCohThreads = 128;
+constexpr int kCohRows = 4;
+
+__device__ __forceinline__ double poly6(const double *p, double l, double c) {
+  return p[0] + p[1] * l + p[2] * c + p[3] * l * l + p[4] * l * c + p[5] * c * c;
+}
+
+struct Poly12 {
+  double az[6], rg[6];
+};
+
+__global__ void k_coreg_resample(const float2 *__restrict__ sec, uint64_t sl, uint64_t ss, uint64_t lines,
+                                 uint32_t samples, Poly12 p, float2 *__restrict__ out) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= samples) return;
+  const double cf = (double)c;
+  for (uint64_t l = blockIdx.y; l < lines; l += gridDim.y) {
+    const double lf = (double)l;
+    const double ls = lf + poly6(p.az, lf, cf), cs = cf + poly6(p.rg, lf, cf);
+    float2 o = make_float2(0.0f, 0.0f);
+    if (!(ls < 0.0 || cs < 0.0)) {
+      const double lfl = floor(ls), cfl = floor(cs);
+      // `as usize`: NaN -> 0; indices at or past the end only need to fail the bounds test
+      const uint64_t l0 = lfl == lfl ? (lfl < (double)sl ? (uint64_t)lfl : sl) : 0;
+      const uint64_t c0 = cfl == cfl ? (cfl < (double)ss ? (uint64_t)cfl : ss) : 0;
+      if (l0 + 1 < sl && c0 + 1 < ss) {
+        const float wl = (float)(ls - (double)l0), wc = (float)(cs - (double)c0);
+        const float2 p00 = __ldg(sec + l0 * ss + c0), p01 = __ldg(sec + l0 * ss + c0 + 1);
+        const float2 p10 = __ldg(sec + (l0 + 1) * ss + c0), p11 = __ldg(sec + (l0 + 1) * ss + c0 + 1);
+        const float i0 = p00.x + (p01.x - p00.x) * wc, i1 = p10.x + (p11.x - p10.x) * wc;
+        const float q0 = p00.y + (p01.y - p00.y) * wc, q1 = p10.y + (p11.y - p10.y) * wc;
+        o = make_float2(i0 + (i1 - i0) * wl, q0 + (q1 - q0) * wl);
+      }
+    }
+    out[l * samples + c] = o;
+  }
+}
+
+// ecef_from_slant_range_doppler (coreg.rs:280-362) with max_iter 10, tol 1 m.
+__device__ bool flat_point(const double *sp, const double *sv, double r, double *t) {
+  const double px = sp[0], py = sp[1], pz = sp[2], vx = sv[0], vy = sv[1], vz = sv[2];
+  const double a = kA, b = kB;
+  const double sat_r = sqrt(px * px + py * py + pz * pz);
+  const double scale = a / sat_r;
+  double tx = px * scale, ty = py * scale, tz = pz * scale * (b / a);
+  for (int it = 0; it < 10; ++it) {
+    const double dx = tx - px, dy = ty - py, dz = tz - pz;
+    const double f1 = dx * vx + dy * vy + dz * vz;
+    const double f2 = dx * dx + dy * dy + dz * dz - r * r;
+    const double f3 = tx * tx / (a * a) + ty * ty / (a * a) + tz * tz / (b * b) - 1.0;
+    const double j00 = vx, j01 = vy, j02 = vz;
+    const double j10 = 2.0 * dx, j11 = 2.0 * dy, j12 = 2.0 * dz;
+    const double j20 = 2.0 * tx / (a * a), j21 = 2.0 * ty / (a * a), j22 = 2.0 * tz / (b * b);
+    const double det = j00 * (j11 * j22 - j12 * j21) - j01 * (j10 * j22 - j12 * j20) + j02 * (j10 * j21 - j11 * j20);
+    if (fabs(det) < 1e-20) return false;
+    const double dxt = (f1 * (j11 * j22 - j12 * j21) - j01 * (f2 * j22 - j12 * f3) + j02 * (f2 * j21 - j11 * f3)) / det;
+    const double dyt = (j00 * (f2 * j22 - j12 * f3) - f1 * (j10 * j22 - j12 * j20) + j02 * (j10 * f3 - f2 * j20)) / det;
+    const double dzt = (j00 * (j11 * f3 - f2 * j21) - j01 * (j10 * f3 - f2 * j20) + f1 * (j10 * j21 - j11 * j20)) / det;
+    tx -= dxt;
+    ty -= dyt;
+    tz -= dzt;
+    if (sqrt(dxt * dxt + dyt * dyt + dzt * dzt) < 1.0) {
+      t[0] = tx, t[1] = ty, t[2] = tz;
+      return true;
+    }
+  }
+  return false;
+}
+
+__global__ void k_igram(const float2 *__restrict__ ref, const float2 *__restrict__ sec,
+                        const double *__restrict__ st, uint64_t lines, uint32_t samples, double srt, double dtau,
+                        double col_off, double k, float4 *__restrict__ out) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= samples) return;
+  const double tau = srt + ((double)c + col_off) * dtau;
+  const double r_ref = tau * kC / 2.0;
+  for (uint64_t l = blockIdx.y; l < lines; l += gridDim.y) {
+    double s[9];  // reference position, velocity; secondary position
+#pragma unroll
+    for (int j = 0; j < 9; ++j) s[j] = __ldg(st + 9 * l + j);
+    double p[3];
+    float fe = 0.0f;  // a point that does not converge keeps a zero flat-earth phase
+    if (flat_point(s, s + 3, r_ref, p)) {
+      const double dx = s[6] - p[0], dy = s[7] - p[1], dz = s[8] - p[2];
+      const double r_sec = sqrt(dx * dx + dy * dy + dz * dz);
+      fe = (float)(k * 2.0 * (r_ref - r_sec));
+    }
+    const uint64_t i = l * samples + c;
+    const float2 rv = __ldg(ref + i), sv = __ldg(sec + i);
+    double sn, cs;
+    sincos((double)fe, &sn, &cs);
+    const double re = (double)sv.x * cs + (double)sv.y * sn;
+    const double im = (double)sv.x * sn - (double)sv.y * cs;
+    out[i] = make_float4((float)((double)rv.x * re - (double)rv.y * im), (float)((double)rv.x * im + (double)rv.y * re),
+                         rv.x * rv.x + rv.y * rv.y, sv.x * sv.x + sv.y * sv.y);
+  }
+}
+
+template <int R, bool SMEM>
+__global__ void __launch_bounds__(kCohThreads) k_coherence(const float4 *__restrict__ ig, int64_t lines,
+                                                           int64_t samples, int64_t ah, int64_t rh,
+                                                           float *__restrict__ coh, float *__restrict__ phase) {
+  extern __shared__ float4 tile[];
+  const int64_t cb = (int64_t)blockIdx.x * kCohThreads;
+  const int64_t c = cb + threadIdx.x;
+  const int64_t tcols = kCohThreads + 2 * rh, trows = R + 2 * ah;
+  for (int64_t lb = (int64_t)blockIdx.y * R; lb < lines; lb += (int64_t)gridDim.y * R) {
+    if (SMEM) {
+      __syncthreads();  // the previous group's reads are done
+      for (int64_t e = threadIdx.x; e < trows * tcols; e += kCohThreads) {
+        const int64_t tr = e / tcols, tc = e - tr * tcols;
+        const int64_t gl = lb - ah + tr, gc = cb - rh + tc;
+        tile[e] = (gl >= 0 && gl < lines && gc >= 0 && gc < samples) ? __ldg(ig + gl * samples + gc)
+                                                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      __syncthreads();
+    }
+    if (c >= samples) continue;
+    const int64_t c0 = c > rh ? c - rh : 0, c1 = c + rh + 1 < samples ? c + rh + 1 : samples;
+    const int64_t wlo = lb > ah ? lb - ah : 0;
+    const int64_t whi = lb + R + ah < lines ? lb + R + ah : lines;
+    double acc[R][4];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = 0.0;
+    for (int64_t wl = wlo; wl < whi; ++wl) {
+      const int64_t rlo = wl - lb - ah, rhi = wl - lb + ah;  // outputs lb + r with |wl - (lb + r)| <= ah
+      // the window row: in the tile its columns start at cb - rh
+      const float4 *row = SMEM ? tile + (wl - lb + ah) * tcols : ig + wl * samples;
+      const int64_t xo = SMEM ? cb - rh : 0;
+      for (int64_t x = c0; x < c1; ++x) {
+        const float4 v = SMEM ? row[x - xo] : __ldg(row + x);
+        const double d0 = v.x, d1 = v.y, d2 = v.z, d3 = v.w;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          if (r >= rlo && r <= rhi) {
+            acc[r][0] += d0;
+            acc[r][1] += d1;
+            acc[r][2] += d2;
+            acc[r][3] += d3;
+          }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t l = lb + r;
+      if (l >= lines) break;
+      const double den = sqrt(acc[r][2] * acc[r][3]);
+      coh[l * samples + c] =
+          den > 0.0 ? (float)fmin(sqrt(acc[r][0] * acc[r][0] + acc[r][1] * acc[r][1]) / den, 1.0) : 0.0f;
+      if (phase) phase[l * samples + c] = (float)atan2(acc[r][1], acc[r][0]);
+    }
+  }
+}
+
+}  // namespace
+}  // namespace sd
+
+using namespace sd;
+
+extern "C" int sd_resample_secondary(sd_ctx *ctx, const float *sec, uint64_t sec_lines, uint64_t sec_samples,
+                                     uint64_t lines, uint64_t samples, const double *az_poly, const double *rg_poly,
+                                     float *out) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!az_poly || !rg_poly) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null polynomial");
+  if (samples > 0xffffffffull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "too many samples per line");
+  if (lines == 0 || samples == 0) return SD_OK;
+  if (!out || (!sec && sec_lines * sec_samples)) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null buffer");
+  SD_CUDA(ctx, cudaSetDevice(ctx->device));
+  Poly12 p;
+  for (int j = 0; j < 6; ++j) p.az[j] = az_poly[j], p.rg[j] = rg_poly[j];
+  const void *din = nullptr;
+  void *dout;
+  if (sec_lines * sec_samples) SD_TRY(stage_in(ctx, "co.sec", sec, sec_lines * sec_samples * 8, &din));
+  SD_TRY(stage_out(ctx, "co.out", out, lines * samples * 8, &dout));
+  const dim3 grid((unsigned)((samples + 255) / 256), (unsigned)(lines < 65535 ? lines : 65535));
+  SD_TIMED_BEGIN(ctx, "k_coreg_resample");
+  k_coreg_resample<<<grid, 256, 0, ctx->stream>>>((const float2 *)din, sec_lines, sec_samples, lines,
+                                                  (uint32_t)samples, p, (float2 *)dout);
+  SD_LAUNCHED(ctx);
+  SD_TRY(finish_out(ctx, out, dout, lines * samples * 8));
+  return sync(ctx);
+}
+
+extern "C" int sd_form_interferogram(sd_ctx *ctx, const float *ref, const float *sec, uint64_t lines,
+                                     uint64_t samples, uint64_t valid_sample_offset, double slant_range_time_s,
+                                     double range_pixel_spacing_m, double azimuth_time_interval_s,
+                                     const sd_state_vector *ref_orbit, uint64_t n_ref, int64_t ref_first_us,
+                                     const sd_state_vector *sec_orbit, uint64_t n_sec, double wavelength_m,
+                                     uint32_t az_looks, uint32_t rg_looks, float *coherence, float *phase) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (az_looks == 0 || rg_looks == 0)
+    return set_error(ctx, SD_ERR_INSAR_INVALID_WINDOW_SIZE,
+                     "coherence estimation window size must be > 0, got az=%u rg=%u", az_looks, rg_looks);
+  if (samples > 0x7fffffffull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "too many samples per line");
+  if (!ref_orbit || !sec_orbit) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null orbit");
+  // the satellite states of every line (interferogram.rs:206-212), on the host
+  std::vector<double> st(9 * lines);
+  for (uint64_t l = 0; l < lines; ++l) {
+    const int64_t t = ref_first_us + (int64_t)((double)l * azimuth_time_interval_s * 1e6);
+    OrbitState a, b;
+    const int ra = orbit_eval(ref_orbit, n_ref, t, &a), rb = ra ? ra : orbit_eval(sec_orbit, n_sec, t, &b);
+    if (ra || rb)
+      return set_error(ctx, SD_ERR_INSAR_ORBIT, "orbit interpolation error: %s",
+                       (ra ? ra : rb) == ORB_INSUFFICIENT ? "insufficient state vectors for interpolation"
+                                                          : "interpolation time outside orbit window");
+    double *q = st.data() + 9 * l;
+    q[0] = a.pos.x, q[1] = a.pos.y, q[2] = a.pos.z, q[3] = a.vel.x, q[4] = a.vel.y, q[5] = a.vel.z;
+    q[6] = b.pos.x, q[7] = b.pos.y, q[8] = b.pos.z;
+  }
+  if (lines == 0 || samples == 0) return SD_OK;
+  if (!ref || !sec || !coherence) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null buffer");
+  SD_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const uint64_t n = lines * samples;
+  const void *dref, *dsec;
+  void *dcoh, *dph = nullptr;
+  double *dst;
+  float4 *dig;
+  SD_TRY(stage_in(ctx, "ig.ref", ref, n * 8, &dref));
+  SD_TRY(stage_in(ctx, "ig.sec", sec, n * 8, &dsec));
+  SD_TRY(stage_out(ctx, "ig.coh", coherence, n * 4, &dcoh));
+  if (phase) SD_TRY(stage_out(ctx, "ig.phase", phase, n * 4, &dph));
+  SD_TRY(scratch_t(ctx, "ig.states", 9 * lines, &dst));
+  SD_TRY(scratch_t(ctx, "ig.buf", n, &dig));
+  SD_CUDA(ctx, cudaMemcpyAsync(dst, st.data(), lines * 72, cudaMemcpyHostToDevice, s));
+  const double dtau = 2.0 * range_pixel_spacing_m / kC;
+  const double k = 6.283185307179586 / wavelength_m;
+  const dim3 g1((unsigned)((samples + 127) / 128), (unsigned)(lines < 65535 ? lines : 65535));
+  SD_TIMED_BEGIN(ctx, "k_igram");
+  k_igram<<<g1, 128, 0, s>>>((const float2 *)dref, (const float2 *)dsec, dst, lines, (uint32_t)samples,
+                             slant_range_time_s, dtau, (double)valid_sample_offset, k, dig);
+  SD_LAUNCHED(ctx);
+  const int64_t ah = az_looks / 2, rh = rg_looks / 2;
+  const size_t smem = (size_t)(kCohRows + 2 * ah) * (size_t)(kCohThreads + 2 * rh) * sizeof(float4);
+  const uint64_t groups = (lines + kCohRows - 1) / kCohRows;
+  const dim3 g2((unsigned)((samples + kCohThreads - 1) / kCohThreads), (unsigned)(groups < 65535 ? groups : 65535));
+  SD_TIMED_BEGIN(ctx, "k_coherence");
+  if (smem <= 96 * 1024) {
+    SD_CUDA(ctx, cudaFuncSetAttribute(k_coherence<kCohRows, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    k_coherence<kCohRows, true><<<g2, kCohThreads, smem, s>>>(dig, (int64_t)lines, (int64_t)samples, ah, rh,
+                                                             (float *)dcoh, (float *)dph);
+  } else {
+    k_coherence<kCohRows, false><<<g2, kCohThreads, 0, s>>>(dig, (int64_t)lines, (int64_t)samples, ah, rh,
+                                                           (float *)dcoh, (float *)dph);
+  }
+  SD_LAUNCHED(ctx);
+  SD_TRY(finish_out(ctx, coherence, dcoh, n * 4));
+  if (phase) SD_TRY(finish_out(ctx, phase, dph, n * 4));
+  return sync(ctx);  // the host state table lives until here
+}

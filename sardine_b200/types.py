@@ -193,6 +193,39 @@ class Deramped:
 
 
 @dataclass
+class CoregPoly:
+    """insar/coreg.rs:73-90: offsets (dl, dc) = p0 + p1 l + p2 c + p3 l^2 + p4 l c + p5 c^2."""
+    az: Sequence[float]
+    rg: Sequence[float]
+
+
+@dataclass
+class Coregistered:
+    """insar/coreg.rs:93-98: reference and resampled secondary, both Deramped."""
+    ref_data: Any
+    secondary_resampled: Any
+
+
+@dataclass
+class InterferogramConfig:
+    """insar/interferogram.rs:123-150 (defaults 10 x 40, no phase)."""
+    az_looks: int = 10
+    rg_looks: int = 40
+    compute_phase: bool = False
+
+
+@dataclass
+class Interferogram:
+    """insar/interferogram.rs:100-117.  phase is None unless requested."""
+    coherence: Any
+    phase: Any
+    lines: int
+    samples: int
+    az_looks: int
+    rg_looks: int
+
+
+@dataclass
 class GroundRangeImage:
     """ground_range.rs:60-85."""
     data: Any
