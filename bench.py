@@ -1056,6 +1056,144 @@ def run_ingest(args):
     _finish_dist(dist)
 
 
+def _insar_orbit(baseline=(0.0, 0.0, 0.0), t0_us=0):
+    """A circular, 98-degree inclined orbit 700 km up, 15 state vectors 10 s
+    apart from t0 - 20 s; `baseline` shifts every position (a secondary pass)."""
+    import math
+    from sardine_b200.types import OrbitData
+    r = 6_378_137.0 + 700_000.0
+    w = math.sqrt(3.986004418e14 / r ** 3)
+    e1, e2 = np.array([1.0, 0.0, 0.0]), np.array([0.0, math.cos(math.radians(98.0)), math.sin(math.radians(98.0))])
+    t = [-20.0 + 10.0 * i for i in range(15)]
+    ps = [r * (math.cos(0.7 + w * x) * e1 + math.sin(0.7 + w * x) * e2) + np.array(baseline) for x in t]
+    vs = [r * w * (-math.sin(0.7 + w * x) * e1 + math.cos(0.7 + w * x) * e2) for x in t]
+    return OrbitData(np.array([t0_us + int(x * 1e6) for x in t], np.int64), np.array(ps), np.array(vs))
+
+
+def run_insar(args):
+    """The InSAR chain of one IW sub-swath pair after deburst (insar/deramp.rs,
+    coreg.rs, interferogram.rs): deramp both CInt16 sub-swaths, resample the
+    secondary through the degree-2 offset polynomials, then the flat-earth
+    phase, cross-product and 10 x 40 coherence (the reference's defaults).
+    13,500 x 21,000 pixels (one config-2 sub-swath).  value = reference-grid
+    pixels per second of device time of the chain's kernels, inputs resident;
+    e2e = the same four public calls from pinned host CInt16 buffers with the
+    coherence read back to host memory."""
+    import torch
+    import sardine_b200 as sd
+    from sardine_b200.types import (CoregPoly, Coregistered, DcEstimate, DeburstArray, InterferogramConfig,
+                                    SubSwathMetadata)
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    dist = _init_dist(world)
+    ctx = sd.Context(local)
+    dev = f"cuda:{local}"
+    lines, samples = (1500, 21000) if args.small else (13500, 21000)
+    g = torch.Generator(device=dev).manual_seed(11 + rank)
+    ref_iq = torch.randint(-120, 121, (lines, samples, 2), device=dev, dtype=torch.int16, generator=g)
+    noise = torch.randint(-40, 41, (lines, samples, 2), device=dev, dtype=torch.int16, generator=g)
+    sec_iq = torch.roll(ref_iq, shifts=(1, 2), dims=(0, 1)) + noise  # offset by ~(1, 2) px
+    ati, rps, srt, wl = 2.055556e-3, 2.329562, 5.35e-3, 0.05546576
+    est = [DcEstimate(800_000 + int(2.758e6 * k), srt + 1e-6 * (k % 3),
+                      [-40.0 + 10.0 * k, 3.0e4 - 7.0e3 * k, -5.0e6 + 1.3e6 * k]) for k in range(6)]
+    sw = SubSwathMetadata("IW1", 9, 1500, samples, ati, rps, srt, est)
+    ro, so = _insar_orbit(), _insar_orbit((110.0, -60.0, 150.0))
+    poly = CoregPoly([1.03, 1e-6, -2e-7, 0.0, 0.0, 0.0], [1.98, 0.0, 3e-6, 0.0, 0.0, 1e-10])
+    cfg = InterferogramConfig()
+
+    def chain(r_iq, s_iq, host_out=False):
+        rd = sd.deramp_subswath(DeburstArray(r_iq, lines, samples, 0), sw, 0, ctx=ctx)
+        sdr = sd.deramp_subswath(DeburstArray(s_iq, lines, samples, 0), sw, 0, ctx=ctx)
+        rs = sd.resample_secondary(lines, samples, poly, sdr, ctx=ctx)
+        return sd.form_interferogram(Coregistered(rd, rs), sw, ro, 0, so, wl, cfg, ctx=ctx)
+
+    for _ in range(args.warmup):
+        chain(ref_iq, sec_iq)
+    names = ("k_deramp", "k_coreg_resample", "k_igram", "k_coherence")
+    ctx.set_timing(True)
+    l0 = ctx.launches
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+            ig = chain(ref_iq, sec_iq)
+    launches = (ctx.launches - l0) // args.steps
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    n = lines * samples
+    dev_ms = _max_over_ranks(dist, sum(kt[k][0] for k in names if k in kt) / args.steps)
+    # algorithmic bytes per launch: CInt16 in + complex f32 out; 4 corners in + out; ref + sec in + float4
+    # out; the float4 plane in once + coherence out
+    alg = {"k_deramp": 12 * n, "k_coreg_resample": 16 * n, "k_igram": 32 * n, "k_coherence": 20 * n}
+    per_k = {k: {"ms": round(kt[k][0] / args.steps, 3), "launches": kt[k][1] // args.steps,
+                 "gbs": round(alg[k] * (kt[k][1] // args.steps) / (kt[k][0] / args.steps / 1e3) / 1e9, 1)}
+             for k in names if k in kt}
+    # coherence: 4 sums of (2 az/2 + 1)(2 rg/2 + 1) f64 adds per pixel, the reference's order
+    win = (2 * (cfg.az_looks // 2) + 1) * (2 * (cfg.rg_looks // 2) + 1)
+    coh_ms = kt["k_coherence"][0] / args.steps
+    fp64 = ctypes_fp64_peak(ctx)
+    coh_tflops = 4 * win * n / (coh_ms / 1e3) / 1e12
+    add_peak = fp64 / 2 if fp64 else None  # an f64 add takes the issue slot of an FMA (2 FLOPs)
+    roof = {"bound": "fp64", "kernel": "k_coherence", "achieved": coh_tflops, "peak": add_peak,
+            "unit": "T f64 adds/s", "frac": coh_tflops / add_peak if add_peak else None, "traffic": None,
+            "adds_per_step": 4 * win * n,
+            "peak_source": "measured FP64 FMA chain (sd_measure_fp64_peak) / 2: the f64 add issue rate"}
+    mean_coh = float(ig.coherence.float().mean())
+    # e2e: pinned host CInt16 in, coherence out to pinned host memory
+    e2e = None
+    if args.e2e:
+        hr = ref_iq.cpu().pin_memory()
+        hs = sec_iq.cpu().pin_memory()
+        hc = torch.empty((lines, samples), dtype=torch.float32).pin_memory()
+        t_e = 0.0
+        for i in range(args.steps + 1):
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+            t0 = time.perf_counter()
+            r_d = hr.to(dev, non_blocking=True)
+            s_d = hs.to(dev, non_blocking=True)
+            out = chain(r_d, s_d)
+            hc.copy_(out.coherence, non_blocking=True)
+            torch.cuda.synchronize()
+            if i:
+                t_e += time.perf_counter() - t0
+        t_e = _max_over_ranks(dist, t_e / args.steps)
+        e2e = {"value": world * n / t_e, "unit": "px/s", "ms_per_step": t_e * 1e3,
+               "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 4 * n,
+               "api": "sardine_b200.deramp_subswath x2 + resample_secondary + form_interferogram"}
+    cpu = None
+    if args.cpu_baseline and world == 1 and rank == 0:
+        import oracle
+        band = 24
+        r_np, s_np = ref_iq[:band].cpu().numpy(), sec_iq[:band].cpu().numpy()
+        t0 = time.perf_counter()
+        _, rd = oracle.deramp_subswath(DeburstArray(r_np, band, samples, 0), sw, 0)
+        _, sdr = oracle.deramp_subswath(DeburstArray(s_np, band, samples, 0), sw, 0)
+        rs = oracle.resample_secondary(band, samples, poly, sdr)
+        oracle.form_interferogram(Coregistered(rd, rs), sw, ro, 0, so, wl, cfg)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": band * samples / cpu_s, "unit": "px/s", "cores": 1, "kind": "port",
+               "sample": f"oracle chain on the first {band} lines (coherence at the band's edge rows included)"}
+    if rank == 0:
+        out = {
+            "metric": "interferogram px/s", "value": world * n / (dev_ms / 1e3), "unit": "px/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (f32 storage)",
+            "data": "synthetic (seeded CInt16 pair, secondary offset by ~(1, 2) px plus noise; inclined "
+                    "circular orbits 700 km up with a 200 m baseline)",
+            "config": {"workload": f"insar: deramp x2 + resample_secondary + form_interferogram "
+                                   f"({cfg.az_looks}x{cfg.rg_looks} coherence) of {lines}x{samples}"
+                                   + (" (REDUCED SHAPE)" if args.small else ""),
+                       "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+            "kernels": per_k, "roofline": roof, "mean_coherence": mean_coh, "cpu_baseline": cpu,
+            "gpu_launches": launches, "e2e": e2e, "clocks": clk.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    _finish_dist(dist)
+
+
 def _hbm_peak():
     """Measured HBM copy bandwidth (GB/s), else the fallback figure."""
     try:
@@ -1352,7 +1490,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4", "export", "ingest"])
+    ap.add_argument("--config", default="c5", choices=["c5", "c2", "c1", "c3", "c4", "export", "ingest", "insar"])
     ap.add_argument("--rates", default="100,500,2000,max",
                     help="config5 request rates (req/s; 'max' queues every request at once); value at the last")
     ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
@@ -1376,6 +1514,8 @@ def main():
         run_export(args)
     elif args.config == "ingest":
         run_ingest(args)
+    elif args.config == "insar":
+        run_insar(args)
     else:
         run_ours(args)
 
