@@ -1152,8 +1152,8 @@ def run_insar(args):
             if dist is not None:
                 dist.barrier()
             t0 = time.perf_counter()
-            r_d = hr.to(dev, non_blocking=True)
-            s_d = hs.to(dev, non_blocking=True)
+            r_d = hr.to(dev)  # blocking: the library's calls run on their own stream
+            s_d = hs.to(dev)
             out = chain(r_d, s_d)
             hc.copy_(out.coherence, non_blocking=True)
             torch.cuda.synchronize()
