@@ -255,7 +255,7 @@ def test_gpu_flat_earth_phase_matches_oracle(ctx):
     co = Coregistered(_deramped(lines, samples, (1.0, 0.0)), _deramped(lines, samples, (1.0, 0.0)))
     cfg = InterferogramConfig(1, 1, True)
     rc, want = oracle.form_interferogram(co, sw, ro, T0_US, so, 0.05546576, cfg)
-    assert rc == 0 and np.ptp(want.phase) > 6.0 and 0.2 < np.mean(want.phase == 0.0) < 0.9  # fringes wrap
+    assert rc == 0 and np.ptp(want.phase) > 6.0 and 0.1 < np.mean(want.phase == 0.0) < 0.9  # fringes wrap
     got = sd.form_interferogram(co, sw, ro, T0_US, so, 0.05546576, cfg, ctx=ctx)
     _close(got.phase, want.phase, rtol=0.0, atol=2e-6)
     _close(got.coherence, want.coherence, rtol=1.2e-7)
