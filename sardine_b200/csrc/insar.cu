@@ -15,9 +15,11 @@
 //   sums equal a sequential evaluation bit for bit.  A thread owns R
 //   outputs of one column on consecutive rows; every window pixel it loads
 //   is added to each of its outputs whose window holds that row, which
-//   keeps each output's order and shares the load and the f32->f64
-//   conversions.  The block's window rows and columns are staged in
-//   shared memory when they fit.
+//   keeps each output's order and shares the load.  Each window row runs
+//   an add loop compiled for its exact range of outputs, so no add is
+//   issued under a false predicate.  The block's window rows and columns
+//   are staged in shared memory when they fit in 96 KB (otherwise the loads
+//   go through L1).
 #include <cmath>
 #include <vector>
 
@@ -30,7 +32,7 @@ namespace {
 constexpr double kC = 299792458.0;
 constexpr double kA = 6378137.0, kB = 6356752.314245;  // WGS84 (interferogram.rs / coreg.rs)
 constexpr int kCohThreads = 128;
-constexpr int kCohRows = 4;
+constexpr int kCohRows = 8;
 
 __device__ __forceinline__ double poly6(const double *p, double l, double c) {
   return p[0] + p[1] * l + p[2] * c + p[3] * l * l + p[4] * l * c + p[5] * c * c;
@@ -127,18 +129,50 @@ __global__ void k_igram(const float2 *__restrict__ ref, const float2 *__restrict
   }
 }
 
+// window pixels of one window row added to outputs LO..HI of the thread;
+// `row` is the tile row (its columns start at xo) or the image row (xo 0)
+template <int R, int LO, int HI, bool SMEM>
+__device__ __forceinline__ void coh_row(double (&acc)[R][4], const float4 *row, int64_t c0, int64_t c1,
+                                        int64_t xo) {
+  for (int64_t x = c0; x < c1; ++x) {
+    const float4 v = SMEM ? row[x - xo] : __ldg(row + x);
+    const double d0 = v.x, d1 = v.y, d2 = v.z, d3 = v.w;
+#pragma unroll
+    for (int r = LO; r <= HI; ++r) {
+      acc[r][0] += d0;
+      acc[r][1] += d1;
+      acc[r][2] += d2;
+      acc[r][3] += d3;
+    }
+  }
+}
+
+// calls coh_row<LO, HI> for the runtime range [lo, hi] (0 <= lo <= hi < R)
+template <int R, bool SMEM, int LO = 0, int HI = 0>
+__device__ __forceinline__ void coh_dispatch(int lo, int hi, double (&acc)[R][4], const float4 *row, int64_t c0,
+                                             int64_t c1, int64_t xo) {
+  if (lo == LO && hi == HI) {
+    coh_row<R, LO, HI, SMEM>(acc, row, c0, c1, xo);
+    return;
+  }
+  if constexpr (HI + 1 < R)
+    coh_dispatch<R, SMEM, LO, HI + 1>(lo, hi, acc, row, c0, c1, xo);
+  else if constexpr (LO + 1 < R)
+    coh_dispatch<R, SMEM, LO + 1, LO + 1>(lo, hi, acc, row, c0, c1, xo);
+}
+
 template <int R, bool SMEM>
 __global__ void __launch_bounds__(kCohThreads) k_coherence(const float4 *__restrict__ ig, int64_t lines,
                                                            int64_t samples, int64_t ah, int64_t rh,
                                                            float *__restrict__ coh, float *__restrict__ phase) {
-  extern __shared__ float4 tile[];
+  extern __shared__ float4 tile[];  // trows x tcols window pixels {Re, Im, |ref|^2, |sec|^2}
   const int64_t cb = (int64_t)blockIdx.x * kCohThreads;
   const int64_t c = cb + threadIdx.x;
-  const int64_t tcols = kCohThreads + 2 * rh, trows = R + 2 * ah;
+  const int64_t tcols = kCohThreads + 2 * rh, trows = R + 2 * ah, ps = trows * tcols;
   for (int64_t lb = (int64_t)blockIdx.y * R; lb < lines; lb += (int64_t)gridDim.y * R) {
     if (SMEM) {
       __syncthreads();  // the previous group's reads are done
-      for (int64_t e = threadIdx.x; e < trows * tcols; e += kCohThreads) {
+      for (int64_t e = threadIdx.x; e < ps; e += kCohThreads) {
         const int64_t tr = e / tcols, tc = e - tr * tcols;
         const int64_t gl = lb - ah + tr, gc = cb - rh + tc;
         tile[e] = (gl >= 0 && gl < lines && gc >= 0 && gc < samples) ? __ldg(ig + gl * samples + gc)
@@ -154,22 +188,12 @@ __global__ void __launch_bounds__(kCohThreads) k_coherence(const float4 *__restr
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[r][0] = acc[r][1] = acc[r][2] = acc[r][3] = 0.0;
     for (int64_t wl = wlo; wl < whi; ++wl) {
-      const int64_t rlo = wl - lb - ah, rhi = wl - lb + ah;  // outputs lb + r with |wl - (lb + r)| <= ah
-      // the window row: in the tile its columns start at cb - rh
-      const float4 *row = SMEM ? tile + (wl - lb + ah) * tcols : ig + wl * samples;
-      const int64_t xo = SMEM ? cb - rh : 0;
-      for (int64_t x = c0; x < c1; ++x) {
-        const float4 v = SMEM ? row[x - xo] : __ldg(row + x);
-        const double d0 = v.x, d1 = v.y, d2 = v.z, d3 = v.w;
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-          if (r >= rlo && r <= rhi) {
-            acc[r][0] += d0;
-            acc[r][1] += d1;
-            acc[r][2] += d2;
-            acc[r][3] += d3;
-          }
-      }
+      // outputs lb + r whose window holds row wl: |wl - (lb + r)| <= ah, a range [lo, hi] with lo <= hi
+      const int64_t d = wl - lb;
+      const int lo = (int)(d - ah > 0 ? d - ah : 0), hi = (int)(d + ah < R - 1 ? d + ah : R - 1);
+      // in the tile the window row's columns start at cb - rh
+      coh_dispatch<R, SMEM>(lo, hi, acc, SMEM ? tile + (d + ah) * tcols : ig + wl * samples, c0, c1,
+                            SMEM ? cb - rh : 0);
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
