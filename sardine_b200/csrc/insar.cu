@@ -15,8 +15,9 @@
 //   sums equal a sequential evaluation bit for bit.  A thread owns R
 //   outputs of one column on consecutive rows; every window pixel it loads
 //   is added to each of its outputs whose window holds that row, which
-//   keeps each output's order and shares the load.  Each window row runs
-//   an add loop compiled for its exact range of outputs, so no add is
+//   keeps each output's order and shares the load.  A window row feeding
+//   outputs 0..k or k..R-1 (every row, once the half window is at least
+//   (R - 1) / 2) runs an add loop compiled for that range, so no add is
 //   issued under a false predicate.  The block's window rows and columns
 //   are staged in shared memory when they fit in 96 KB (otherwise the loads
 //   go through L1).
@@ -100,7 +101,7 @@ __device__ bool flat_point(const double *sp, const double *sv, double r, double 
   return false;
 }
 
-__global__ void k_igram(const float2 *__restrict__ ref, const float2 *__restrict__ sec,
+__global__ void __launch_bounds__(128, 7) k_igram(const float2 *__restrict__ ref, const float2 *__restrict__ sec,
                         const double *__restrict__ st, uint64_t lines, uint32_t samples, double srt, double dtau,
                         double col_off, double k, float4 *__restrict__ out) {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -147,18 +148,53 @@ __device__ __forceinline__ void coh_row(double (&acc)[R][4], const float4 *row, 
   }
 }
 
-// calls coh_row<LO, HI> for the runtime range [lo, hi] (0 <= lo <= hi < R)
-template <int R, bool SMEM, int LO = 0, int HI = 0>
+// window pixels of one window row added to outputs lo..hi (runtime range, predicated adds)
+template <int R, bool SMEM>
+__device__ __forceinline__ void coh_row_any(int lo, int hi, double (&acc)[R][4], const float4 *row, int64_t c0,
+                                            int64_t c1, int64_t xo) {
+  for (int64_t x = c0; x < c1; ++x) {
+    const float4 v = SMEM ? row[x - xo] : __ldg(row + x);
+    const double d0 = v.x, d1 = v.y, d2 = v.z, d3 = v.w;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (r >= lo && r <= hi) {
+        acc[r][0] += d0;
+        acc[r][1] += d1;
+        acc[r][2] += d2;
+        acc[r][3] += d3;
+      }
+  }
+}
+
+// outputs 0..hi: coh_row<0, K> for K == hi
+template <int R, bool SMEM, int K = 0>
+__device__ __forceinline__ void coh_prefix(int hi, double (&acc)[R][4], const float4 *row, int64_t c0, int64_t c1,
+                                           int64_t xo) {
+  if (hi == K) return coh_row<R, 0, K, SMEM>(acc, row, c0, c1, xo);
+  if constexpr (K + 1 < R) coh_prefix<R, SMEM, K + 1>(hi, acc, row, c0, c1, xo);
+}
+
+// outputs lo..R-1: coh_row<K, R - 1> for K == lo
+template <int R, bool SMEM, int K = 1>
+__device__ __forceinline__ void coh_suffix(int lo, double (&acc)[R][4], const float4 *row, int64_t c0, int64_t c1,
+                                           int64_t xo) {
+  if (lo == K) return coh_row<R, K, R - 1, SMEM>(acc, row, c0, c1, xo);
+  if constexpr (K + 1 < R) coh_suffix<R, SMEM, K + 1>(lo, acc, row, c0, c1, xo);
+}
+
+// the window row's outputs [lo, hi] (0 <= lo <= hi < R).  When the half
+// window is at least (R - 1) / 2 every range holds output 0 or output R - 1,
+// and those ranges have loops of their own (2R - 1 of them); ranges inside
+// (small windows only) take the predicated loop.
+template <int R, bool SMEM>
 __device__ __forceinline__ void coh_dispatch(int lo, int hi, double (&acc)[R][4], const float4 *row, int64_t c0,
                                              int64_t c1, int64_t xo) {
-  if (lo == LO && hi == HI) {
-    coh_row<R, LO, HI, SMEM>(acc, row, c0, c1, xo);
-    return;
-  }
-  if constexpr (HI + 1 < R)
-    coh_dispatch<R, SMEM, LO, HI + 1>(lo, hi, acc, row, c0, c1, xo);
-  else if constexpr (LO + 1 < R)
-    coh_dispatch<R, SMEM, LO + 1, LO + 1>(lo, hi, acc, row, c0, c1, xo);
+  if (lo == 0)
+    coh_prefix<R, SMEM>(hi, acc, row, c0, c1, xo);
+  else if (hi == R - 1)
+    coh_suffix<R, SMEM>(lo, acc, row, c0, c1, xo);
+  else
+    coh_row_any<R, SMEM>(lo, hi, acc, row, c0, c1, xo);
 }
 
 template <int R, bool SMEM>
