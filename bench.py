@@ -535,14 +535,15 @@ def run_c4(args):
     fp64 = ctypes_fp64_peak(ctx)
     tc_tf = TC_FLOPS(n_it) * px_step / (tc_ms / 1e3) / 1e12 if tc_ms else None
     sp_ms = kt.get("k_speckle_tiles", (0.0, 0))[0]
-    hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    hbm = _hbm_peak()
     sp_gbs = 9.0 * px_step / (sp_ms / 1e3) / 1e9 if sp_ms else None
     roofline = {"bound": "fp64", "kernel": "tile geocoding (" + "+".join(sorted(k for k in kt if k.startswith(TC_STAGE))) + ")",
                 "achieved": tc_tf, "peak": fp64, "unit": "TFLOP/s",
                 "frac": tc_tf / fp64 if (tc_tf and fp64) else None, "traffic": None,
                 "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
                 "speckle_stage": {"kernel": "k_speckle_tiles", "bound": "hbm", "achieved": sp_gbs,
-                                  "peak": hbm, "unit": "GB/s", "frac": sp_gbs / hbm if sp_gbs else None,
+                                  "peak": hbm, "peak_source": _hbm_peak_source(), "unit": "GB/s",
+                                  "frac": sp_gbs / hbm if sp_gbs else None,
                                   "bytes_per_px": 9.0, "ms": sp_ms}}
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_k, 4)}
                for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
@@ -588,7 +589,7 @@ def _tile_roofline(sd, tiles, ctx, reqs):
     tc_ms = sum(v[0] for k, v in kt.items() if k.startswith(TC_STAGE))
     sp_ms = kt.get("k_speckle_tiles", (0.0, 0))[0]
     fp64 = ctypes_fp64_peak(ctx)
-    hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
+    hbm = _hbm_peak()
     tf = TC_FLOPS(n_it) * px / (tc_ms / 1e3) / 1e12 if tc_ms else None
     gbs = 9.0 * px / (sp_ms / 1e3) / 1e9 if sp_ms else None
     total = sum(v[0] for v in kt.values()) or 1.0
@@ -597,7 +598,8 @@ def _tile_roofline(sd, tiles, ctx, reqs):
             "traffic": None, "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
             "batch": f"{len(reqs)} tiles, {px} px",
             "speckle_stage": {"kernel": "k_speckle_tiles", "bound": "hbm", "achieved": gbs, "peak": hbm,
-                              "unit": "GB/s", "frac": gbs / hbm if gbs else None, "bytes_per_px": 9.0,
+                              "peak_source": _hbm_peak_source(), "unit": "GB/s",
+                              "frac": gbs / hbm if gbs else None, "bytes_per_px": 9.0,
                               "ms": sp_ms}}
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total, 4)}
                for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
@@ -1195,11 +1197,17 @@ def run_insar(args):
 
 
 def _hbm_peak():
-    """Measured HBM copy bandwidth (GB/s), else the fallback figure."""
+    """Measured HBM copy bandwidth (GB/s), else the fallback figure (6650 GB/s,
+    an earlier STREAM-style copy on this kind of B200)."""
     try:
         return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs", 6650.0))
     except Exception:
         return 6650.0
+
+
+def _hbm_peak_source():
+    return ("measured (MEASURED_PEAKS.json hbm_gbs)" if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json"))
+            else "fallback 6650 GB/s (no measured peaks file)")
 
 
 def run_export(args):
