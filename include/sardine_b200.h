@@ -94,7 +94,8 @@ typedef enum sd_status {
     SD_ERR_INSAR_NO_DC_ESTIMATES = 90,
     SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC = 91,
     SD_ERR_INSAR_INVALID_WINDOW_SIZE = 92,
-    SD_ERR_INSAR_ORBIT = 93
+    SD_ERR_INSAR_ORBIT = 93,
+    SD_ERR_INSAR_COREG_GRID_TOO_SMALL = 94
 } sd_status;
 
 /* ── Enumerations mirroring the reference's enums ─────────────────────── */
@@ -619,6 +620,29 @@ int sd_deramp_subswath(sd_ctx *ctx, const int16_t *iq, uint64_t lines, uint64_t 
 int sd_resample_secondary(sd_ctx *ctx, const float *sec, uint64_t sec_lines, uint64_t sec_samples,
                           uint64_t lines, uint64_t samples, const double *az_poly, const double *rg_poly,
                           float *out);
+
+/* compute_coreg_offsets (insar/coreg.rs:128-223): a 20 x 50 grid of reference
+ * pixels ((i+1) lines / 21, (j+1) samples / 51), each forward-geocoded to the
+ * WGS84 ellipsoid (ecef_from_slant_range_doppler, 20 iterations, 1 mm),
+ * then solve_zero_doppler on the secondary orbit from sec_first_us (20
+ * iterations, 1e-9 s) to its secondary line and column (column offset
+ * sec_first_sample); failed points are skipped.  The degree-2 fits of the
+ * line and column offsets (normal equations, Gaussian elimination with
+ * partial pivoting) fill *out.  The grid runs on the device, the fit on
+ * the host.  SD_ERR_INSAR_COREG_GRID_TOO_SMALL with fewer than 6 points or
+ * a singular system. */
+typedef struct sd_coreg_result {     /* CoregResult (coreg.rs:102-109) */
+    double az_poly[6];
+    double rg_poly[6];
+    double fit_residual_rms;
+    uint64_t n_valid;
+} sd_coreg_result;
+int sd_coreg_offsets(sd_ctx *ctx, const sd_state_vector *ref_orbit, uint64_t n_ref, int64_t ref_first_us,
+                     uint64_t ref_lines, uint64_t ref_samples, uint64_t ref_valid_sample_offset,
+                     double ref_azimuth_time_interval_s, double ref_slant_range_time_s,
+                     double ref_range_pixel_spacing_m, const sd_state_vector *sec_orbit, uint64_t n_sec,
+                     int64_t sec_first_us, double sec_azimuth_time_interval_s, double sec_slant_range_time_s,
+                     double sec_range_pixel_spacing_m, uint64_t sec_first_sample, sd_coreg_result *out);
 
 /* form_interferogram (insar/interferogram.rs:165-398) of a co-registered
  * pair ref, sec (lines x samples complex f32, host or device): per pixel the

@@ -77,6 +77,8 @@ def _declare(L):
         "orc_multilook": (C.c_int, [P, P, u64, u64, C.c_uint32, C.c_uint32, P, P]),
         "orc_to_ground_range": (C.c_int, [P, u64, u64, d, d, d, P, C.c_int32, d, d, P, P]),
         "orc_deramp": (C.c_int, [P, u64, u64, u64, d, d, d, P, u64, i64, P, P]),
+        "orc_fit_poly6": (C.c_int, [P, u64, C.c_int, P, P]),
+        "orc_coreg_offsets": (C.c_int, [P, u64, i64, u64, u64, u64, d, d, d, P, u64, i64, d, d, d, u64, P, P, P, P]),
         "orc_resample_secondary": (C.c_int, [P, u64, u64, u64, u64, P, P, P]),
         "orc_ecef_from_slant_range_doppler": (C.c_int, [P, P, d, u64, d, P]),
         "orc_form_interferogram": (C.c_int, [P, P, u64, u64, u64, d, d, d, P, u64, i64, P, u64, d, u64, u64, P,
@@ -503,3 +505,27 @@ def form_interferogram(coreg: T.Coregistered, ref_swath: T.SubSwathMetadata, ref
     if rc:
         return rc, None
     return rc, T.Interferogram(coh, ph, lines, samples, int(cfg.az_looks), int(cfg.rg_looks))
+
+
+def fit_poly6(pts, which: int):
+    """fit_poly6 (insar/coreg.rs:478-517) of column `which` (2: dl, 3: dc) of
+    (l, c, dl, dc) points: (status, coefficients, residual rms)."""
+    a = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1)
+    coef, rms = (C.c_double * 6)(), C.c_double()
+    rc = lib().orc_fit_poly6(a.ctypes.data, a.size // 4, which, coef, C.byref(rms))
+    return rc, list(coef), rms.value
+
+
+def compute_coreg_offsets(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us):
+    """compute_coreg_offsets (insar/coreg.rs:128-223): (status, CoregResult or None)."""
+    az, rg, rms, nv = (C.c_double * 6)(), (C.c_double * 6)(), C.c_double(), C.c_uint64()
+    rc = lib().orc_coreg_offsets(ref_orbit.to_c(), len(ref_orbit.times_us), int(ref_first_us), int(ref_deburst.lines),
+                                 int(ref_deburst.samples), int(ref_deburst.valid_sample_offset),
+                                 float(ref_swath.azimuth_time_interval_s), float(ref_swath.slant_range_time_s),
+                                 float(ref_swath.range_pixel_spacing_m), sec_orbit.to_c(), len(sec_orbit.times_us),
+                                 int(sec_first_us), float(sec_swath.azimuth_time_interval_s),
+                                 float(sec_swath.slant_range_time_s), float(sec_swath.range_pixel_spacing_m),
+                                 int(sec_swath.first_sample), az, rg, C.byref(rms), C.byref(nv))
+    if rc:
+        return rc, None
+    return rc, T.CoregResult(T.CoregPoly(list(az), list(rg)), rms.value, int(nv.value))

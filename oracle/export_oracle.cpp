@@ -19,6 +19,7 @@
 //   resample_secondary     sardine/src/insar/coreg.rs:230-264, 428-466
 //   ecef_from_slant_range_doppler  sardine/src/insar/coreg.rs:280-362
 //   form_interferogram     sardine/src/insar/interferogram.rs:165-398
+//   compute_coreg_offsets  sardine/src/insar/coreg.rs:128-223, 371-414, 478-568
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -801,5 +802,93 @@ extern "C" int orc_form_interferogram(const float *ref, const float *sec, uint64
       if (phase) phase[l * samples + c] = (float)std::atan2(sim, sre);
     }
   }
+  return SD_OK;
+}
+
+// compute_coreg_offsets (coreg.rs:128-223): the sparse grid in order, then
+// fit_poly6 (478-517) with gaussian_elimination (522-568).
+extern "C" int orc_solve_zero_doppler(const double *target, const sd_state_vector *svs, uint64_t n, int64_t guess,
+                                      uint64_t max_iter, double tol, int64_t *t_out, int32_t *iters_out,
+                                      double *residual_out);
+
+extern "C" int orc_fit_poly6(const double *pts, uint64_t n, int which, double *coef, double *rms) {
+  double a[6][6] = {}, b[6] = {};
+  for (uint64_t p = 0; p < n; ++p) {
+    const double l = pts[4 * p], c = pts[4 * p + 1], y = pts[4 * p + which];
+    const double bs[6] = {1.0, l, c, l * l, l * c, c * c};
+    for (int i = 0; i < 6; ++i) {
+      b[i] += bs[i] * y;
+      for (int j = 0; j < 6; ++j) a[i][j] += bs[i] * bs[j];
+    }
+  }
+  for (int col = 0; col < 6; ++col) {
+    int piv = col;  // Iterator::max_by keeps the last of equal maxima
+    for (int r = col + 1; r < 6; ++r)
+      if (std::fabs(a[r][col]) >= std::fabs(a[piv][col])) piv = r;
+    for (int k = 0; k < 6; ++k) std::swap(a[col][k], a[piv][k]);
+    std::swap(b[col], b[piv]);
+    if (std::fabs(a[col][col]) < 1e-12) return SD_ERR_INSAR_COREG_GRID_TOO_SMALL;
+    const double inv = 1.0 / a[col][col];
+    for (int r = col + 1; r < 6; ++r) {
+      const double f = a[r][col] * inv;
+      for (int k = col; k < 6; ++k) a[r][k] -= f * a[col][k];
+      b[r] -= f * b[col];
+    }
+  }
+  for (int i = 5; i >= 0; --i) {
+    double sum = b[i];
+    for (int j = i + 1; j < 6; ++j) sum -= a[i][j] * coef[j];
+    coef[i] = sum / a[i][i];
+  }
+  double sse = 0.0;
+  for (uint64_t p = 0; p < n; ++p) {
+    const double l = pts[4 * p], c = pts[4 * p + 1], y = pts[4 * p + which];
+    const double res = y - orc_poly6(coef, l, c);
+    sse += res * res;
+  }
+  *rms = std::sqrt(sse / (double)n);
+  return SD_OK;
+}
+
+extern "C" int orc_coreg_offsets(const sd_state_vector *ro, uint64_t nr, int64_t ref_first, uint64_t lines,
+                                 uint64_t samples, uint64_t ref_off, double ref_ati, double ref_tau0, double ref_rps,
+                                 const sd_state_vector *so, uint64_t ns, int64_t sec_first, double sec_ati,
+                                 double sec_tau0, double sec_rps, uint64_t sec_first_sample, double *az, double *rg,
+                                 double *rms, uint64_t *n_valid) {
+  const double c_light = 299792458.0;
+  const double ref_dtau = 2.0 * ref_rps / c_light, sec_dtau = 2.0 * sec_rps / c_light;
+  const double az_step = (double)lines / 21.0, rg_step = (double)samples / 51.0;
+  std::vector<double> pts;
+  for (int gi = 0; gi < 20; ++gi) {
+    const double l = (double)(gi + 1) * az_step;
+    for (int gj = 0; gj < 50; ++gj) {
+      const double c = (double)(gj + 1) * rg_step;
+      const int64_t t_ref = ref_first + (int64_t)(l * ref_ati * 1e6);
+      const double range_m = (ref_tau0 + (c + (double)ref_off) * ref_dtau) * c_light / 2.0;
+      double pos[3], vel[3], acc[3], P[3];
+      if (orc_interpolate_orbit_and_accel(ro, nr, t_ref, pos, vel, acc) != 0) continue;
+      if (orc_ecef_from_slant_range_doppler(pos, vel, range_m, 20, 1e-3, P) != 0) continue;
+      int64_t t;
+      int32_t it;
+      double resid;
+      if (orc_solve_zero_doppler(P, so, ns, sec_first, 20, 1e-9, &t, &it, &resid) != 0) continue;
+      double sp[3], sv[3], sa[3];
+      if (orc_interpolate_orbit_and_accel(so, ns, t, sp, sv, sa) != 0) continue;
+      const double l_sec = (double)(t - sec_first) / (sec_ati * 1e6);
+      const double rng = std::sqrt((P[0] - sp[0]) * (P[0] - sp[0]) + (P[1] - sp[1]) * (P[1] - sp[1]) +
+                                   (P[2] - sp[2]) * (P[2] - sp[2]));
+      const double c_sec = (2.0 * rng / c_light - sec_tau0) / sec_dtau - (double)sec_first_sample;
+      pts.insert(pts.end(), {l, c, l_sec - l, c_sec - c});
+    }
+  }
+  const uint64_t n = pts.size() / 4;
+  *n_valid = n;
+  if (n < 6) return SD_ERR_INSAR_COREG_GRID_TOO_SMALL;
+  double ra, rr;
+  if (orc_fit_poly6(pts.data(), n, 2, az, &ra) || orc_fit_poly6(pts.data(), n, 3, rg, &rr)) {
+    *n_valid = 0;
+    return SD_ERR_INSAR_COREG_GRID_TOO_SMALL;
+  }
+  *rms = std::sqrt((ra * ra + rr * rr) / 2.0);
   return SD_OK;
 }

@@ -31,7 +31,7 @@ import numpy as np
 from . import _abi
 from . import types as T
 from ._lib import Context, default_context, lib
-from .types import (BoundingBox, BurstEntry, CalibrationVector, CoregPoly, Coregistered, DcEstimate, DeburstArray, Deramped, DemGrid,
+from .types import (BoundingBox, BurstEntry, CalibrationVector, CoregPoly, CoregResult, Coregistered, DcEstimate, DeburstArray, Deramped, DemGrid,
                     GeocodedImage, GroundRangeImage, Interferogram, InterferogramConfig, GeoidModel, GeolocationGridPoint, MergedSigma0, NoiseAzimuthVector,
                     NoiseRangeVector, OrbitData, OutputCrs, Precision, ResamplingKernel, SceneMetadata,
                     Sigma0Array, SpeckleFilter, SubSwathMetadata, SwathCalibration, SwathInput,
@@ -45,6 +45,7 @@ __all__ = [
     "tc_output_grid", "to_db_inplace", "write_cog_with_crs", "downsample_2x", "ExportError",
     "SlcReader", "SlcReadError", "apply_multilook", "to_ground_range", "GroundRangeError",
     "deramp_subswath", "InsarError", "resample_secondary", "form_interferogram",
+    "compute_coreg_offsets",
 ] + [n for n in dir(T) if n[:1].isupper() and getattr(getattr(T, n), "__module__", "") == T.__name__]
 
 
@@ -135,6 +136,7 @@ _KINDS = {
     _abi.SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC: (InsarError, "AzimuthTimeBeforeDcEstimates"),
     _abi.SD_ERR_INSAR_INVALID_WINDOW_SIZE: (InsarError, "InvalidWindowSize"),
     _abi.SD_ERR_INSAR_ORBIT: (InsarError, "Orbit"),
+    _abi.SD_ERR_INSAR_COREG_GRID_TOO_SMALL: (InsarError, "CoregGridTooSmall"),
 }
 
 
@@ -676,3 +678,21 @@ def form_interferogram(coreg: T.Coregistered, ref_swath: SubSwathMetadata, ref_o
                                      int(cfg.az_looks), int(cfg.rg_looks), T.ptr(coh), T.ptr(ph))
     _check(ctx, rc, InsarError)
     return T.Interferogram(coh, ph, lines, samples, int(cfg.az_looks), int(cfg.rg_looks))
+
+
+def compute_coreg_offsets(ref_swath: SubSwathMetadata, ref_orbit: OrbitData, ref_first_us: int,
+                          ref_deburst: DeburstArray, sec_swath: SubSwathMetadata, sec_orbit: OrbitData,
+                          sec_first_us: int, ctx: Optional[Context] = None) -> T.CoregResult:
+    """compute_coreg_offsets (insar/coreg.rs:128-223): the 20 x 50 sparse grid
+    geocoded on the device, the degree-2 offset fits on the host."""
+    ctx = _ctx(ctx)
+    r = _abi.CoregResultC()
+    rc = lib().sd_coreg_offsets(ctx.handle, ref_orbit.to_c(), len(ref_orbit.times_us), int(ref_first_us),
+                                int(ref_deburst.lines), int(ref_deburst.samples),
+                                int(ref_deburst.valid_sample_offset), float(ref_swath.azimuth_time_interval_s),
+                                float(ref_swath.slant_range_time_s), float(ref_swath.range_pixel_spacing_m),
+                                sec_orbit.to_c(), len(sec_orbit.times_us), int(sec_first_us),
+                                float(sec_swath.azimuth_time_interval_s), float(sec_swath.slant_range_time_s),
+                                float(sec_swath.range_pixel_spacing_m), int(sec_swath.first_sample), C.byref(r))
+    _check(ctx, rc, InsarError)
+    return T.CoregResult(T.CoregPoly(list(r.az_poly), list(r.rg_poly)), r.fit_residual_rms, int(r.n_valid))

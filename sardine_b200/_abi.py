@@ -59,6 +59,7 @@ SD_ERR_INSAR_NO_DC_ESTIMATES = 90
 SD_ERR_INSAR_AZIMUTH_TIME_BEFORE_DC = 91
 SD_ERR_INSAR_INVALID_WINDOW_SIZE = 92
 SD_ERR_INSAR_ORBIT = 93
+SD_ERR_INSAR_COREG_GRID_TOO_SMALL = 94
 
 RESAMPLE_BILINEAR, RESAMPLE_BICUBIC, RESAMPLE_LANCZOS3 = 0, 1, 2
 CRS_WGS84, CRS_UTM_NORTH, CRS_UTM_SOUTH = 0, 1, 2
@@ -118,6 +119,11 @@ class GrdInfo(C.Structure):
 
 class DcEstimateC(C.Structure):
     _fields_ = [("azimuth_time_us", C.c_int64), ("t0_s", C.c_double), ("data_dc_poly", C.c_double * 3)]
+
+
+class CoregResultC(C.Structure):
+    _fields_ = [("az_poly", C.c_double * 6), ("rg_poly", C.c_double * 6), ("fit_residual_rms", C.c_double),
+                ("n_valid", C.c_uint64)]
 
 
 class TcConfig(C.Structure):

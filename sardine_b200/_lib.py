@@ -64,6 +64,9 @@ _SIGS = {
     "sd_to_ground_range": (C.c_int, [P, P, C.c_uint64, C.c_uint64, C.c_double, C.c_double, C.c_double, P,
                                      C.c_int32, C.c_double, C.c_double, P, P]),
     "sd_slc_read_burst_raw": (C.c_int, [P, P, C.c_uint64, C.c_uint64, P]),
+    "sd_coreg_offsets": (C.c_int, [P, P, C.c_uint64, C.c_int64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_double,
+                                   C.c_double, C.c_double, P, C.c_uint64, C.c_int64, C.c_double, C.c_double,
+                                   C.c_double, C.c_uint64, P]),
     "sd_resample_secondary": (C.c_int, [P, P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, P, P, P]),
     "sd_form_interferogram": (C.c_int, [P, P, P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_double, C.c_double,
                                         C.c_double, P, C.c_uint64, C.c_int64, P, C.c_uint64, C.c_double,

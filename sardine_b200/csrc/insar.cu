@@ -70,14 +70,15 @@ __global__ void k_coreg_resample(const float2 *__restrict__ sec, uint64_t sl, ui
   }
 }
 
-// ecef_from_slant_range_doppler (coreg.rs:280-362) with max_iter 10, tol 1 m.
-__device__ bool flat_point(const double *sp, const double *sv, double r, double *t) {
+// ecef_from_slant_range_doppler (coreg.rs:280-362).
+__device__ bool flat_point(const double *sp, const double *sv, double r, double *t, int max_iter = 10,
+                           double tol_m = 1.0) {
   const double px = sp[0], py = sp[1], pz = sp[2], vx = sv[0], vy = sv[1], vz = sv[2];
   const double a = kA, b = kB;
   const double sat_r = sqrt(px * px + py * py + pz * pz);
   const double scale = a / sat_r;
   double tx = px * scale, ty = py * scale, tz = pz * scale * (b / a);
-  for (int it = 0; it < 10; ++it) {
+  for (int it = 0; it < max_iter; ++it) {
     const double dx = tx - px, dy = ty - py, dz = tz - pz;
     const double f1 = dx * vx + dy * vy + dz * vz;
     const double f2 = dx * dx + dy * dy + dz * dz - r * r;
@@ -93,12 +94,65 @@ __device__ bool flat_point(const double *sp, const double *sv, double r, double 
     tx -= dxt;
     ty -= dyt;
     tz -= dzt;
-    if (sqrt(dxt * dxt + dyt * dyt + dzt * dzt) < 1.0) {
+    if (sqrt(dxt * dxt + dyt * dyt + dzt * dzt) < tol_m) {
       t[0] = tx, t[1] = ty, t[2] = tz;
       return true;
     }
   }
   return false;
+}
+
+
+constexpr int kGridAz = 20, kGridRg = 50;  // GRID_AZ, GRID_RG (coreg.rs:54-56)
+
+struct CoregGeom {
+  const sd_state_vector *ro, *so;
+  uint64_t nr, ns;
+  int64_t ref_first, sec_first;
+  double ref_ati, ref_tau0, ref_dtau, ref_off, sec_ati, sec_tau0, sec_dtau, sec_off, az_step, rg_step;
+};
+
+// One sparse grid point of compute_coreg_offsets (coreg.rs:159-207): forward
+// geocoding of the reference pixel (20 iterations, 1 mm), solve_zero_doppler
+// on the secondary orbit from its first line (20 iterations, 1e-9 s;
+// terrain_correction.rs:1010-1073) and secondary_sar_coords (coreg.rs:371-414).
+__global__ void k_coreg_grid(CoregGeom g, double4 *pts, int *ok) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kGridAz * kGridRg) return;
+  ok[i] = 0;
+  const int gi = i / kGridRg, gj = i - gi * kGridRg;
+  const double l = (double)(gi + 1) * g.az_step, c = (double)(gj + 1) * g.rg_step;
+  const int64_t t_ref = g.ref_first + f2i64(l * g.ref_ati * 1e6);
+  const double range_m = (g.ref_tau0 + (c + g.ref_off) * g.ref_dtau) * kC / 2.0;
+  OrbitState s;
+  if (orbit_eval(g.ro, g.nr, t_ref, &s) != ORB_OK) return;
+  const double sp[3] = {s.pos.x, s.pos.y, s.pos.z}, sv[3] = {s.vel.x, s.vel.y, s.vel.z};
+  double P[3];
+  if (!flat_point(sp, sv, range_m, P, 20, 1e-3)) return;
+  int64_t t = g.sec_first;
+  bool conv = false;
+  OrbitState q;
+  for (int it = 0; it < 20; ++it) {
+    if (orbit_eval(g.so, g.ns, t, &q) != ORB_OK) return;
+    const double rx = P[0] - q.pos.x, ry = P[1] - q.pos.y, rz = P[2] - q.pos.z;
+    const double f = rx * q.vel.x + ry * q.vel.y + rz * q.vel.z;
+    const double vsq = q.vel.x * q.vel.x + q.vel.y * q.vel.y + q.vel.z * q.vel.z;
+    const double fp = -vsq + (rx * q.acc.x + ry * q.acc.y + rz * q.acc.z);
+    if (fabs(fp) < 1.0) return;
+    const double delta = -f / fp;
+    if (fabs(delta) < 1e-9) {
+      conv = true;
+      break;
+    }
+    t = t + f2i64(delta * 1e6);
+  }
+  if (!conv) return;
+  const double l_sec = (double)(t - g.sec_first) / (g.sec_ati * 1e6);
+  const double dx = P[0] - q.pos.x, dy = P[1] - q.pos.y, dz = P[2] - q.pos.z;
+  const double rng = sqrt(dx * dx + dy * dy + dz * dz);
+  const double c_sec = (2.0 * rng / kC - g.sec_tau0) / g.sec_dtau - g.sec_off;
+  pts[i] = make_double4(l, c, l_sec - l, c_sec - c);
+  ok[i] = 1;
 }
 
 __global__ void __launch_bounds__(128, 7) k_igram(const float2 *__restrict__ ref, const float2 *__restrict__ sec,
@@ -339,4 +393,106 @@ extern "C" int sd_form_interferogram(sd_ctx *ctx, const float *ref, const float 
   SD_TRY(finish_out(ctx, coherence, dcoh, n * 4));
   if (phase) SD_TRY(finish_out(ctx, phase, dph, n * 4));
   return sync(ctx);  // the host state table lives until here
+}
+
+namespace sd {
+namespace {
+// gaussian_elimination (coreg.rs:522-568): partial pivoting (the last row of
+// the largest magnitude, as Iterator::max_by), 1e-12 pivot floor.
+bool gauss6(double a[6][6], double b[6], double x[6]) {
+  for (int col = 0; col < 6; ++col) {
+    int p = col;
+    for (int r = col + 1; r < 6; ++r)
+      if (fabs(a[r][col]) >= fabs(a[p][col])) p = r;
+    for (int k = 0; k < 6; ++k) std::swap(a[col][k], a[p][k]);
+    std::swap(b[col], b[p]);
+    if (fabs(a[col][col]) < 1e-12) return false;
+    const double inv = 1.0 / a[col][col];
+    for (int r = col + 1; r < 6; ++r) {
+      const double f = a[r][col] * inv;
+      for (int k = col; k < 6; ++k) a[r][k] -= f * a[col][k];
+      b[r] -= f * b[col];
+    }
+  }
+  for (int i = 5; i >= 0; --i) {
+    double sum = b[i];
+    for (int j = i + 1; j < 6; ++j) sum -= a[i][j] * x[j];
+    x[i] = sum / a[i][i];
+  }
+  return true;
+}
+
+// fit_poly6 (coreg.rs:478-517) of value k (2: dl, 3: dc) of the points.
+bool fit6(const std::vector<double4> &pts, int k, double coef[6], double *rms) {
+  double ata[6][6] = {}, atb[6] = {};
+  for (const double4 &q : pts) {
+    const double l = q.x, c = q.y, y = k == 2 ? q.z : q.w;
+    const double bs[6] = {1.0, l, c, l * l, l * c, c * c};
+    for (int i = 0; i < 6; ++i) {
+      atb[i] += bs[i] * y;
+      for (int j = 0; j < 6; ++j) ata[i][j] += bs[i] * bs[j];
+    }
+  }
+  if (!gauss6(ata, atb, coef)) return false;
+  double sse = 0.0;
+  for (const double4 &q : pts) {
+    const double l = q.x, c = q.y, y = k == 2 ? q.z : q.w;
+    const double res = y - (coef[0] + coef[1] * l + coef[2] * c + coef[3] * l * l + coef[4] * l * c + coef[5] * c * c);
+    sse += res * res;
+  }
+  *rms = std::sqrt(sse / (double)pts.size());
+  return true;
+}
+}  // namespace
+}  // namespace sd
+
+extern "C" int sd_coreg_offsets(sd_ctx *ctx, const sd_state_vector *ref_orbit, uint64_t n_ref, int64_t ref_first_us,
+                                uint64_t ref_lines, uint64_t ref_samples, uint64_t ref_valid_sample_offset,
+                                double ref_azimuth_time_interval_s, double ref_slant_range_time_s,
+                                double ref_range_pixel_spacing_m, const sd_state_vector *sec_orbit, uint64_t n_sec,
+                                int64_t sec_first_us, double sec_azimuth_time_interval_s,
+                                double sec_slant_range_time_s, double sec_range_pixel_spacing_m,
+                                uint64_t sec_first_sample, sd_coreg_result *out) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!ref_orbit || !sec_orbit || !out) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null argument");
+  SD_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const void *dro, *dso;
+  double4 *dpts;
+  int *dok;
+  SD_TRY(stage_in(ctx, "cg.ro", ref_orbit, n_ref * sizeof(sd_state_vector), &dro));
+  SD_TRY(stage_in(ctx, "cg.so", sec_orbit, n_sec * sizeof(sd_state_vector), &dso));
+  SD_TRY(scratch_t(ctx, "cg.pts", kGridAz * kGridRg, &dpts));
+  SD_TRY(scratch_t(ctx, "cg.ok", kGridAz * kGridRg, &dok));
+  CoregGeom g;
+  g.ro = (const sd_state_vector *)dro, g.so = (const sd_state_vector *)dso, g.nr = n_ref, g.ns = n_sec;
+  g.ref_first = ref_first_us, g.sec_first = sec_first_us;
+  g.ref_ati = ref_azimuth_time_interval_s, g.ref_tau0 = ref_slant_range_time_s;
+  g.ref_dtau = 2.0 * ref_range_pixel_spacing_m / kC, g.ref_off = (double)ref_valid_sample_offset;
+  g.sec_ati = sec_azimuth_time_interval_s, g.sec_tau0 = sec_slant_range_time_s;
+  g.sec_dtau = 2.0 * sec_range_pixel_spacing_m / kC, g.sec_off = (double)sec_first_sample;
+  g.az_step = (double)ref_lines / (double)(kGridAz + 1), g.rg_step = (double)ref_samples / (double)(kGridRg + 1);
+  SD_TIMED_BEGIN(ctx, "k_coreg_grid");
+  k_coreg_grid<<<(kGridAz * kGridRg + 127) / 128, 128, 0, s>>>(g, dpts, dok);
+  SD_LAUNCHED(ctx);
+  std::vector<double4> pts(kGridAz * kGridRg);
+  std::vector<int> ok(kGridAz * kGridRg);
+  SD_CUDA(ctx, cudaMemcpyAsync(pts.data(), dpts, pts.size() * sizeof(double4), cudaMemcpyDeviceToHost, s));
+  SD_CUDA(ctx, cudaMemcpyAsync(ok.data(), dok, ok.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+  SD_TRY(sync(ctx));
+  std::vector<double4> valid;  // grid order, as the reference's collect
+  for (size_t i = 0; i < pts.size(); ++i)
+    if (ok[i]) valid.push_back(pts[i]);
+  out->n_valid = valid.size();
+  if (valid.size() < 6)
+    return set_error(ctx, SD_ERR_INSAR_COREG_GRID_TOO_SMALL,
+                     "co-registration: need at least 6 valid grid points for polynomial fit, got %zu", valid.size());
+  double ra, rr;
+  if (!fit6(valid, 2, out->az_poly, &ra) || !fit6(valid, 3, out->rg_poly, &rr)) {
+    out->n_valid = 0;
+    return set_error(ctx, SD_ERR_INSAR_COREG_GRID_TOO_SMALL,
+                     "co-registration: need at least 6 valid grid points for polynomial fit, got 0");
+  }
+  out->fit_residual_rms = std::sqrt((ra * ra + rr * rr) / 2.0);
+  return SD_OK;
 }

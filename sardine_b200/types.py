@@ -125,6 +125,7 @@ class SubSwathMetadata:
     range_pixel_spacing_m: float
     slant_range_time_s: float
     dc_estimates: list = None  # [DcEstimate]; deramp_subswath needs them
+    first_sample: int = 0      # full-image column of the first valid pixel (compute_coreg_offsets)
 
     def to_c(self) -> _abi.SubSwath:
         return _abi.SubSwath(self.burst_count, self.lines_per_burst, self.azimuth_time_interval_s,
@@ -197,6 +198,14 @@ class CoregPoly:
     """insar/coreg.rs:73-90: offsets (dl, dc) = p0 + p1 l + p2 c + p3 l^2 + p4 l c + p5 c^2."""
     az: Sequence[float]
     rg: Sequence[float]
+
+
+@dataclass
+class CoregResult:
+    """insar/coreg.rs:102-109."""
+    poly: Any
+    fit_residual_rms: float
+    n_valid: int
 
 
 @dataclass

@@ -275,3 +275,66 @@ def test_gpu_interferogram_reference_cases_and_errors(ctx):
     with pytest.raises(sd.InsarError) as e:
         sd.form_interferogram(co, _minimal_swath(), orb, T0_US + 60_000_000, orb, 0.0555, ctx=ctx)
     assert e.value.kind == "Orbit"
+
+
+# ── sparse co-registration offsets (compute_coreg_offsets) ──────────────────
+def test_oracle_poly_fit_recovers_linear_offset():
+    # coreg.rs:683-706
+    pts = [(i * 10.0, j * 50.0, 0.5, 0.0) for i in range(100) for j in range(10)]
+    rc, coef, rms = oracle.fit_poly6(pts, 2)
+    assert rc == 0 and abs(coef[0] - 0.5) < 1e-9 and rms < 1e-10
+
+
+def _coreg_case(realistic=False, lines=1500, samples=4000):
+    """realistic: the inclined circular orbits (200 m baseline), secondary
+    0.31 s later.  Otherwise the reference tests' fixed-position orbit for
+    both passes (interferogram.rs:508-521, moved off the equator), where the zero-Doppler residual
+    after forward geocoding is far below 1 ns, so every point converges."""
+    if realistic:
+        sw = SubSwathMetadata("IW1", 1, lines, samples, 2.055556e-3, 20.0, 2.0 * 712_000.0 / 299_792_458.0)
+        ro, so, ts = _circular_orbit(), _circular_orbit((110.0, -60.0, 150.0)), T0_US + 310_000
+    else:
+        sw = SubSwathMetadata("IW1", 1, lines, samples, 2.055556e-3, 20.0, 2.0 * 712_000.0 / 299_792_458.0)
+        ro = so = _orbit_at(6_000_000.0, 0.0, 3_741_857.0)  # 7071 km out, off the equator
+        ts = T0_US
+    sec_sw = SubSwathMetadata("IW1", 1, lines, samples, sw.azimuth_time_interval_s, 20.0, sw.slant_range_time_s,
+                              first_sample=3)
+    return sw, ro, T0_US, Deramped(None, lines, samples, 5), sec_sw, so, ts
+
+
+def test_oracle_coreg_offsets_fixed_orbit():
+    """Same fixed state for every line of both passes: the secondary line is
+    0, so dl = -l, and dc = ref offset - first_sample; the fit recovers them."""
+    rc, r = oracle.compute_coreg_offsets(*_coreg_case())
+    assert rc == 0 and r.n_valid == 1000
+    assert np.allclose(r.poly.az, [0, -1, 0, 0, 0, 0], atol=1e-6) and abs(r.poly.rg[0] - 2.0) < 1e-3
+    assert r.fit_residual_rms < 1e-6
+
+
+def test_oracle_coreg_offsets_realistic_orbit_fails_like_the_reference():
+    """solve_zero_doppler steps in whole microseconds (terrain_correction.rs
+    :1066) but asks for |delta| < 1e-9 s (coreg.rs:381), so on real orbits a
+    point converges only when its zero-Doppler time lies within 1 ns of a
+    whole microsecond: the grid comes out too small."""
+    rc, _ = oracle.compute_coreg_offsets(*_coreg_case(realistic=True))
+    assert rc == _abi.SD_ERR_INSAR_COREG_GRID_TOO_SMALL
+
+
+@pytest.mark.gpu
+def test_gpu_coreg_offsets_match_oracle(ctx):
+    case = _coreg_case()
+    rc, want = oracle.compute_coreg_offsets(*case)
+    assert rc == 0
+    got = sd.compute_coreg_offsets(*case, ctx=ctx)
+    assert got.n_valid == want.n_valid
+    assert got.poly.az == want.poly.az and got.poly.rg == want.poly.rg
+    assert got.fit_residual_rms == want.fit_residual_rms
+
+
+@pytest.mark.gpu
+def test_gpu_coreg_grid_too_small(ctx):
+    for case in (_coreg_case(realistic=True), _coreg_case()[:2] + (T0_US + 500_000_000,) + _coreg_case()[3:]):
+        assert oracle.compute_coreg_offsets(*case)[0] == _abi.SD_ERR_INSAR_COREG_GRID_TOO_SMALL
+        with pytest.raises(sd.InsarError) as e:
+            sd.compute_coreg_offsets(*case, ctx=ctx)
+        assert e.value.kind == "CoregGridTooSmall"
