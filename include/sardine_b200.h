@@ -371,8 +371,13 @@ int sd_apply_calibration(sd_ctx *ctx, const int16_t *deburst_iq, uint64_t lines,
  *    <= 64 LUT vectors and <= 65536 LUT knots per family (sigma0, range
  *    noise), <= 32768 lines, <= 32768 samples; larger inputs are rejected
  *    with SD_ERR_INVALID_ARGUMENT and a message;
- *  - the first call on a device resolves the array's address on that device
- *    (cudaGetSymbolAddress); make that first call before any stream capture;
+ *  - every call looks up the array's address on the current device
+ *    (cudaGetSymbolAddress), and the first call on a device loads the
+ *    library's module there: make that first call before any stream
+ *    capture.  The call stages its LUT tables from host memory that lives
+ *    only for the call, so it refuses a capturing stream
+ *    (SD_ERR_INVALID_ARGUMENT);
+ *  - a null LUT array with a non-zero count is rejected the same way;
  *  - every call shares the one array and leaves its contents behind (nothing
  *    in it needs to start at zero): calls whose work overlaps on the GPU race
  *    with each other, so serialise them (one stream, or events);

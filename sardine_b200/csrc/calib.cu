@@ -342,6 +342,17 @@ struct CalPlan {
 int cal_plan(sd_ctx *ctx, const sd_lut_vector *cal, uint64_t n_cal, const sd_lut_vector *nr, uint64_t n_nr,
              const sd_noise_azimuth *az, uint64_t col_offset, uint64_t samples, uint64_t tiff_line_origin,
              uint64_t lines, CalPlan *P) {
+  if ((n_cal && !cal) || (n_nr && !nr))
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null LUT vector array with a non-zero count");
+  for (uint64_t i = 0; i < n_cal + n_nr; ++i) {
+    const sd_lut_vector &v = i < n_cal ? cal[i] : nr[i - n_cal];
+    if (v.n && (!v.pixels || !v.values))
+      return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "LUT vector at line %d has %llu knots but a null array",
+                       v.line, (unsigned long long)v.n);
+  }
+  if (az && az->n && (!az->lines || !az->values))
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "azimuth noise vector has %llu knots but a null array",
+                     (unsigned long long)az->n);
   if (n_cal == 0) return set_error(ctx, SD_ERR_CAL_NO_CALIBRATION_VECTORS, "calibration LUT has no vectors");
   if (n_nr == 0) return set_error(ctx, SD_ERR_CAL_NO_NOISE_RANGE_VECTORS, "noise range LUT has no vectors");
   const uint32_t SLACK = 600;
@@ -753,11 +764,6 @@ constexpr size_t NA_SCRATCH_BYTES = 20u << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_SCRATCH_BYTES];
 
-// Device address of g_noalloc_scratch per device, resolved once per device
-// (with that device current) by the first call on it.
-std::mutex g_na_mu;
-void *g_na_ptr[64] = {nullptr};
-
 struct NaLayout {  // byte offsets inside the static array
   size_t off[2][5];  // per family: px, pm, val, off, cnt
   size_t tab[2];
@@ -827,6 +833,19 @@ int noalloc_run(sd_ctx *c, const int16_t *iq, uint64_t lines, uint64_t samples, 
                 const sd_lut_vector *cal, uint64_t n_cal, const sd_lut_vector *nr, uint64_t n_nr,
                 const sd_noise_azimuth *az, uint64_t tiff_line_origin, float *out, float *nesz,
                 uint32_t *cal_gap, uint32_t *nr_gap) {
+  // The LUT tables, line parameters and azimuth vector are staged from host
+  // vectors that live only for this call: a capturing stream would record
+  // copies from memory that is gone when the graph replays.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(c->stream, &cap) != cudaSuccess) {
+    const cudaError_t e = cudaGetLastError();
+    return set_error(c, SD_ERR_CUDA, "cudaStreamIsCapturing failed: %s", cudaGetErrorString(e));
+  }
+  if (cap != cudaStreamCaptureStatusNone)
+    return set_error(c, SD_ERR_INVALID_ARGUMENT,
+                     "allocation-free calibration stages host data per call and cannot run on a capturing stream");
+  if ((n_cal && !cal) || (n_nr && !nr))
+    return set_error(c, SD_ERR_INVALID_ARGUMENT, "null LUT vector array with a non-zero count");
   // size limits first: the static working memory is fixed
   if (n_cal > NA_MAX_VECTORS || n_nr > NA_MAX_VECTORS)
     return set_error(c, SD_ERR_INVALID_ARGUMENT,
@@ -857,22 +876,21 @@ int noalloc_run(sd_ctx *c, const int16_t *iq, uint64_t lines, uint64_t samples, 
   if (L.total > NA_SCRATCH_BYTES)
     return set_error(c, SD_ERR_INVALID_ARGUMENT, "working set %zu B exceeds the %zu B static scratch", L.total,
                      NA_SCRATCH_BYTES);
-  // resolve the array's device address once per device (this device is current)
+  // The array's device address on the current device.  It is looked up on
+  // every call (a table lookup, not a stream operation): an address cached
+  // across calls would go stale after cudaDeviceReset or a recreated primary
+  // context, when the module reloads elsewhere.  The first call on a device
+  // also loads the module there.
   unsigned char *base = nullptr;
   {
-    std::lock_guard<std::mutex> lk(g_na_mu);
-    void *&slot = g_na_ptr[c->device & 63];
-    if (!slot) {
-      void *p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        cudaGetLastError();
-        return set_error(c, SD_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s",
-                         cudaGetErrorString(e));
-      }
-      slot = p;
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return set_error(c, SD_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch) failed: %s",
+                       cudaGetErrorString(e));
     }
-    base = (unsigned char *)slot;
+    base = (unsigned char *)p;
   }
   CalSwathDev s{};
   for (int f = 0; f < 2; ++f) {

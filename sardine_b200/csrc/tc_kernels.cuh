@@ -479,13 +479,26 @@ __device__ float sample_bicubic(const float *d, uint64_t nl, uint64_t ns, double
 // The build compiles with --fmad=false (the FP64 path must not contract);
 // the FP32 code contracts explicitly with fmaf.
 
+// The fractional tap position f and its complement g = 1 - f, both formed in
+// FP64 and then rounded, so each carries its own relative accuracy.  Weights
+// that vanish as f -> 1 are proportional to g; a g formed in FP32 from the
+// rounded f carries f's absolute error (2^-25) and loses its relative
+// accuracy there, which the error bound below does not allow for.
+struct FracF {
+  float f, g;
+};
+__device__ __forceinline__ FracF frac_f(double x, int64_t base) {
+  const double fd = x - (double)base;
+  return {(float)fd, (float)(1.0 - fd)};
+}
+
 // keys_weight (a = -0.5) of the taps -1, 0, 1, 2 at offsets k - f, in
 // factored form: 1.5u^3 - 2.5u^2 + 1 = (1 - u)(1 + u - 1.5u^2) on [0, 1) and
 // -0.5u^3 + 2.5u^2 - 4u + 2 = -0.5(u - 1)(u - 2)^2 on [1, 2).  Expanded, the
 // cubics cancel near their roots and a small weight loses its leading
 // digits; factored, every weight keeps its relative accuracy.
-__device__ __forceinline__ void keys4_f(float f, float w[4]) {
-  const float g = 1.f - f;
+__device__ __forceinline__ void keys4_f(FracF q, float w[4]) {
+  const float f = q.f, g = q.g;
   w[0] = -0.5f * f * g * g;
   w[1] = g * fmaf(-1.5f * f, f, 1.f + f);
   w[2] = f * fmaf(-1.5f * g, g, 1.f + g);
@@ -495,16 +508,18 @@ __device__ __forceinline__ void keys4_f(float f, float w[4]) {
 // Lanczos-3 weights (terrain_correction.rs:938-952) of the taps li = -2..3
 // at x = f - li.  sin(pi x) = (-1)^li sin(pi f) and sin(pi x/3) =
 // sin(pi f/3) cos(pi li/3) - cos(pi f/3) sin(pi li/3), so the six weights
-// take two sinpi and one sincospi.
+// take two sinpi and one sincospi.  In FP32 every factor that vanishes as
+// f -> 1 is taken from g = 1 - f (sin(pi f) = sin(pi g), x = f - 1 = -g).
 template <typename T>
-__device__ __forceinline__ void lanczos6(T f, T w[6]);
+__device__ __forceinline__ void lanczos6(double fd, T w[6]);
 
 template <>
-__device__ __forceinline__ void lanczos6<float>(float f, float w[6]) {
-  const float s1 = sinpif(f);
+__device__ __forceinline__ void lanczos6<float>(double fd, float w[6]) {
+  const float f = (float)fd, g = (float)(1.0 - fd);
+  const float s1 = sinpif(f <= 0.5f ? f : g);
   float s3, c3;
   sincospif(f * (1.f / 3.f), &s3, &c3);
-  const float q = sinpif((1.f - f) * (1.f / 3.f));
+  const float q = sinpif(g * (1.f / 3.f));
   const float h = 0.866025403784438647f;  // sin(pi/3)
   const float cl[6] = {-0.5f, 0.5f, 1.f, 0.5f, -0.5f, -1.f};
   const float sl[6] = {-h, -h, 0.f, h, h, 0.f};
@@ -512,7 +527,7 @@ __device__ __forceinline__ void lanczos6<float>(float f, float w[6]) {
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
     const int li = j - 2;
-    const float x = f - (float)li;
+    const float x = li == 1 ? -g : f - (float)li;
     const float ax = fabsf(x);
     const float s = (li & 1) ? -s1 : s1;
     // taps li = -2 and 1: the angle-addition form cancels as f -> 1, so
@@ -546,7 +561,10 @@ __device__ __forceinline__ void lanczos6<double>(double f, double w[6]) {
 // The FP32 samplers also return the magnitude sum A = sum |v w|.  Their
 // error is at most kSampErr * A: two nested fma chains of <= 6 terms
 // (12 u of A) plus the FP32 weights' own rounding (a few ulps each, 2e-6 for
-// a weight product).  The bound travels with the value (CandPre::serr) to
+// a weight product).  That needs every weight to keep its relative accuracy,
+// so the weights are formed from f and g = 1 - f each rounded from FP64
+// (frac_f): a weight proportional to g is then exact to a few ulps also as
+// f -> 1.  The bound travels with the value (CandPre::serr) to
 // the mask decisions, so an inexact sum (negative lobes cancelling) costs an
 // FP64 re-sample only where it can change the output: a valid pixel whose
 // bound exceeds kSampRel of its value, or a noise-floor test within it.
@@ -572,15 +590,17 @@ __device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, dou
   int64_t l1 = l0 + 1 < max_line ? l0 + 1 : max_line;
   int64_t s0 = clampi(f2i64(floor(sample)), 0, max_sample);
   int64_t s1 = s0 + 1 < max_sample ? s0 + 1 : max_sample;
-  const float dl = (float)(line - (double)l0), ds = (float)(sample - (double)s0);
+  // dl may be negative (line in [-0.5, 0)) or beyond 1 at the far edge
+  const FracF ql = frac_f(line, l0), qs = frac_f(sample, s0);
+  const float dl = ql.f, ds = qs.f;
   float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
   float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
   if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
   // explicit weights, as the reference forms them: with non-negative
   // weights and samples every term is non-negative and the sum keeps its
   // relative accuracy even near zero (the lerp form a + t(b - a) does not)
-  const float w00 = (1.f - dl) * (1.f - ds), w01 = (1.f - dl) * ds;
-  const float w10 = dl * (1.f - ds), w11 = dl * ds;
+  const float w00 = ql.g * qs.g, w01 = ql.g * ds;
+  const float w10 = dl * qs.g, w11 = dl * ds;
   const float r = fmaf(v00, w00, fmaf(v01, w01, fmaf(v10, w10, v11 * w11)));
   const float a = fmaf(fabsf(v00), fabsf(w00), fmaf(fabsf(v01), fabsf(w01),
                        fmaf(fabsf(v10), fabsf(w10), fabsf(v11) * fabsf(w11))));
@@ -592,10 +612,9 @@ __device__ float sample_bicubic_f(const float *d, uint64_t nl, uint64_t ns, doub
                                   float *amag) {
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
-  const float dl = (float)(line - (double)lf), ds = (float)(sample - (double)sf);
   float ws[4], wls[4];
-  keys4_f(ds, ws);
-  keys4_f(dl, wls);
+  keys4_f(frac_f(sample, sf), ws);
+  keys4_f(frac_f(line, lf), wls);
   int64_t cols[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) cols[k] = clampi(sf + k - 1, 0, max_s);
@@ -625,8 +644,8 @@ __device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, doub
   int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
   int64_t lf = f2i64(floor(line)), sf = f2i64(floor(sample));
   T wl[6], ws[6];
-  lanczos6<T>((T)(line - (double)lf), wl);
-  lanczos6<T>((T)(sample - (double)sf), ws);
+  lanczos6<T>(line - (double)lf, wl);
+  lanczos6<T>(sample - (double)sf, ws);
   int64_t cols[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) cols[k] = clampi(sf + k - 2, 0, max_s);
@@ -697,10 +716,10 @@ __device__ bool sample_bicubic_pair_f(const float *d, uint64_t nl, uint64_t ns, 
   const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
   if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
   float ws0[4], ws1[4], wl0[4], wl1[4];
-  keys4_f((float)(sample[0] - (double)sf), ws0);
-  keys4_f((float)(sample[1] - (double)sf), ws1);
-  keys4_f((float)(line[0] - (double)lf), wl0);
-  keys4_f((float)(line[1] - (double)lf), wl1);
+  keys4_f(frac_f(sample[0], sf), ws0);
+  keys4_f(frac_f(sample[1], sf), ws1);
+  keys4_f(frac_f(line[0], lf), wl0);
+  keys4_f(frac_f(line[1], lf), wl1);
   int64_t cols[4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) cols[k] = clampi(sf + k - 1, 0, max_s);
@@ -740,10 +759,10 @@ __device__ bool sample_lanczos_pair(const float *d, uint64_t nl, uint64_t ns, co
   const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
   if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
   T wl0[6], ws0[6], wl1[6], ws1[6];
-  lanczos6<T>((T)(line[0] - (double)lf), wl0);
-  lanczos6<T>((T)(sample[0] - (double)sf), ws0);
-  lanczos6<T>((T)(line[1] - (double)lf), wl1);
-  lanczos6<T>((T)(sample[1] - (double)sf), ws1);
+  lanczos6<T>(line[0] - (double)lf, wl0);
+  lanczos6<T>(sample[0] - (double)sf, ws0);
+  lanczos6<T>(line[1] - (double)lf, wl1);
+  lanczos6<T>(sample[1] - (double)sf, ws1);
   int64_t cols[6];
 #pragma unroll
   for (int k = 0; k < 6; ++k) cols[k] = clampi(sf + k - 2, 0, max_s);
@@ -1097,10 +1116,17 @@ __device__ CandOut cand_post(const TcDev &p, const CandPre &c, V3 P, V3 S, const
 //        An = cos(phi) (hn - hs + N'(c + d)) - sin(phi) ((N + hn) c + (N + hs) d)
 //        Zn = sin(phi) (hn - hs + B'(c + d)) + cos(phi) ((B + hn) c + (B + hs) d)
 //        B = N (1 - e^2), N' = dN/dphi = N e^2 sin cos / (1 - e^2 sin^2).
+// en = |E-W chord| x |N-S chord| scales the normal's rounding error: every
+// component of the FP32 cross product is within ~10 u en of the exact one
+// (u = 2^-24), so the local projection lp = n . look is within
+// kLpErr * en + kLpRel * |lp| of its FP64 value.
 struct FacetF {
   bool ok;
-  float nx, ny, nz, area;
+  float nx, ny, nz, area, en;
 };
+constexpr float kLpErr = 1e-6f;   // ~16 u, plus the chord expansion's ~1e-8
+constexpr float kLpRel = 4e-7f;   // look vector and its rsqrt
+constexpr float kWRelFull = 2e-5f;  // beyond: the flattening weight itself is redone in FP64
 
 __device__ FacetF facetf_from(const TcDev &p, const PixGeo &g, const float h[4]) {
   FacetF f{};
@@ -1127,6 +1153,7 @@ __device__ FacetF facetf_from(const TcDev &p, const PixGeo &g, const float h[4])
   f.ny = ez * nx - ex * nz;
   f.nz = ex * ny - ey * nx;
   f.area = sqrtf(f.nx * f.nx + f.ny * f.ny + f.nz * f.nz);
+  f.en = sqrtf((ex * ex + ey * ey + ez * ez) * (nx * nx + ny * ny + nz * nz));
   return f;
 }
 
@@ -1152,19 +1179,30 @@ __device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g
       const float lx = (float)(S.x - g.P.x), ly = (float)(S.y - g.P.y), lz = (float)(S.z - g.P.z);
       const float il = rsqrtf(lx * lx + ly * ly + lz * lz);
       const float lp = (f.nx * lx + f.ny * ly + f.nz * lz) * il;
-      if (fabsf(lp) <= 1e-4f * f.area) { *redo = RD_FULL; return o; }
+      const float dlp = kLpErr * f.en + kLpRel * fabsf(lp);  // bound on |lp - lp_fp64|
+      if (fabsf(lp) <= fmaxf(1e-4f * f.area, 8.f * dlp)) { *redo = RD_FULL; return o; }
       if (lp <= 0.f || f.area == 0.f) {
         if (p.flatten) return {NAN, cosv, (uint8_t)SD_MASK_SHADOW, 5};
       } else {
         const float w = lp / flat_area;
-        if (fabsf(w - 0.05f) <= 5e-6f || fabsf(w - 2.0f) <= 2e-4f) { *redo = RD_FULL; return o; }
+        // relative error of w: that of lp, the division and flat_area's rounding
+        const float ew = dlp / lp + 2.4e-7f;
+        if (fabsf(w - 0.05f) <= 0.05f * fmaxf(1e-4f, 4.f * ew) ||
+            fabsf(w - 2.0f) <= 2.0f * fmaxf(1e-4f, 4.f * ew)) {
+          *redo = RD_FULL;
+          return o;
+        }
         cosv = fminf(fmaxf(lp / f.area, 0.f), 1.f);
         if (w < 0.05f || w > 2.0f) {
           if (p.flatten) return {NAN, cosv, (uint8_t)(w > 2.0f ? SD_MASK_LAYOVER : SD_MASK_FORESHORTENING), 5};
         } else if (p.flatten) {
           sigma0 /= w;
-          serr /= w;
+          // gamma0 = sigma0 / w: the sampling bound scales by 1 / w and the
+          // weight's own relative error adds; a weight too inexact to be
+          // reused by the FP64 re-sample sends the candidate to k_redo
+          serr = serr / w + fabsf(sigma0) * ew;
           wd = w;
+          if (ew > kWRelFull && serr > kSampRel * fabsf(sigma0)) { *redo = RD_FULL; return o; }
         }
       }
     }

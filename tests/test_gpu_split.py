@@ -135,3 +135,33 @@ def test_split_zero_clipped_sigma0(ctx, resampling):
     # 35 % zeros make many values near-zero interpolations, ill-conditioned in
     # relative terms for any implementation: judged against the noise floor
     assert rep["sigma_floor_over_1e-4_px"] <= cap, rep
+
+
+@pytest.mark.parametrize("resampling", [sd.ResamplingKernel.Bilinear, sd.ResamplingKernel.Bicubic,
+                                        sd.ResamplingKernel.Lanczos3])
+def test_split_matches_fp64_path_zero_clipped_full_shape(ctx, resampling):
+    """Split vs the FP64 path on the config-1 shape (4096 x 8192 sigma0,
+    1024^2 DEM) geocoded at a quarter of the DEM posting (4096^2 output px),
+    flattening on, with 35 % of the sigma0 samples clipped to zero as the
+    noise subtraction does.  Both paths share the microsecond chain, so
+    times, masks, counters and the NaN pattern are equal, and every
+    sigma0/gamma0 is within 1e-4 relative of the FP64 value: no pixel is
+    excepted and no noise-floor metric is used."""
+    sc = synth.config1_scene(seed=39, resampling=resampling, flatten=True)
+    img = np.array(sc.merged.data)
+    rng = np.random.default_rng(10)
+    img[rng.uniform(size=img.shape) < 0.35] = 0.0
+    sc.merged.data = img
+    sc.config.pixel_spacing_deg = sc.config.pixel_spacing_deg / 4
+    ref = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx, return_times=True)
+    sc.config.precision = SPLIT
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx, return_times=True)
+    rep = compare_geocoded(gpu, ref, gpu.azimuth_time_us, ref.azimuth_time_us,
+                           sc.scene.sub_swaths[0].azimuth_time_interval_s)
+    assert rep["compared_px"] > 4_000_000, rep
+    assert rep["time_mismatch_px"] == 0, rep
+    assert rep["nan_pattern_equal"] and rep["mask_equal"], rep
+    assert rep["sigma_rel_over_1e-4_px"] == 0, rep
+    assert rep["cos_lia_abs_err_max"] <= 1e-5, rep
+    assert gpu.newton_iter_histogram == ref.newton_iter_histogram
+    assert gpu.valid_pixel_count == ref.valid_pixel_count

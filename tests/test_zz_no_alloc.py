@@ -82,3 +82,37 @@ def test_noalloc_rejects_oversize_and_host_buffers():
     out_h = torch.empty((4, 100))
     rc, msg, _, _ = _call_noalloc(host.data, host, sw.cal, sw.noise, 0, out_h, out_h.clone())
     assert rc == sd._abi.SD_ERR_INVALID_ARGUMENT and "device" in msg
+
+
+def test_noalloc_refuses_capture_and_null_luts():
+    """Its LUT tables are staged from host memory that lives only for the
+    call, so a capturing stream is refused before any work is enqueued; a
+    null LUT array with a non-zero count is an argument error, not a crash."""
+    import torch
+    dev = torch.device("cuda", 0)
+    ctx = sd.Context(0)
+    sw = _case(44)
+    deb = sd.deburst_subswath(torch.from_numpy(np.asarray(sw.slc)).to(dev), sw.sw, sw.bursts, ctx=ctx)
+    out = torch.empty((deb.lines, deb.samples), device=dev)
+    nesz = torch.empty_like(out)
+    torch.cuda.synchronize()
+    err = C.create_string_buffer(512)
+    cg, ng = C.c_uint32(), C.c_uint32()
+    rc = _lib.lib().sd_apply_calibration_noalloc(
+        None, deb.data.data_ptr(), deb.lines, deb.samples, deb.valid_sample_offset, None, 3, None, 2,
+        None, 0, out.data_ptr(), nesz.data_ptr(), C.byref(cg), C.byref(ng), err, len(err))
+    assert rc == sd._abi.SD_ERR_INVALID_ARGUMENT and b"null" in err.value
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=side):
+        rc, msg, _, _ = _call_noalloc(deb.data, deb, sw.cal, sw.noise, sw.bursts[0].first_line, out, nesz,
+                                      stream=C.c_void_p(side.cuda_stream))
+    assert rc == sd._abi.SD_ERR_INVALID_ARGUMENT and "capturing" in msg
+    del graph
+    # the stream works as before once the capture has ended
+    rc, msg, _, _ = _call_noalloc(deb.data, deb, sw.cal, sw.noise, sw.bursts[0].first_line, out, nesz)
+    torch.cuda.synchronize()
+    assert rc == 0, msg
+    want = sd.apply_calibration(deb, sw.cal, sw.noise, sw.bursts[0].first_line, ctx=ctx)
+    assert torch.equal(out, want.data) and torch.equal(nesz, want.nesz)
+    ctx.close()
