@@ -429,17 +429,58 @@ def cpu_baseline(args, sc, res_gpu, merged_px, threads=None, budget_s=12.0, gpu_
                            f"{band} of {rows} output rows (rows {r0}..{r0 + band}); value = output px / "
                            f"(prep time + per-row TC time x rows)")})
     if gpu_band is not None:
-        # the GPU product path on the same rows of the full-size scene, against the oracle
-        from sardine_b200.accuracy import compare_geocoded
+        # the GPU product path on the same rows of the full-size scene, against
+        # the oracle with glibc's sines and cosines (as timed) and with
+        # correctly rounded ones (untimed)
+        with oracle.libm("cr"):
+            ref_cr, ref_cr_t, _ = oracle.terrain_correction(merged, sc.scene, dem_h, sc.grids, sc.config,
+                                                            row_begin=r0, row_end=r0 + band, return_times=True)
         g = gpu_band(r0, r0 + band)
-        rep = compare_geocoded(g, ref, g.azimuth_time_us, ref_t,
-                               sc.scene.sub_swaths[0].azimuth_time_interval_s)
-        rep["rows"] = [r0, r0 + band]
-        rep["counters_equal"] = (g.valid_pixel_count == ref.valid_pixel_count and
-                                 g.newton_iter_histogram == ref.newton_iter_histogram and
-                                 g.flat_masked_count == ref.flat_masked_count)
-        out["parity_vs_oracle"] = rep
+        out["parity_vs_oracle"] = parity_both(g, ref, ref_t, ref_cr, ref_cr_t,
+                                              sc.scene.sub_swaths[0].azimuth_time_interval_s)
+        out["parity_vs_oracle"]["rows"] = [r0, r0 + band]
     return out
+
+
+def _neq(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return ~((a == b) | (np.isnan(a) & np.isnan(b)))
+
+
+def parity_both(g, gl, gl_t, cr, cr_t, ati_s):
+    """GPU result against the oracle run with glibc's sines and cosines and
+    with correctly rounded ones: the full report against the latter, the
+    count of pixels where the two oracle runs differ (glibc not correctly
+    rounded) and, outside those, time flips and pixels beyond 1e-4 against
+    the former."""
+    from sardine_b200.accuracy import compare_geocoded
+    rep_cr = compare_geocoded(g, cr, g.azimuth_time_us, cr_t, ati_s)
+    rep_cr["counters_equal"] = (g.valid_pixel_count == cr.valid_pixel_count and
+                                g.newton_iter_histogram == cr.newton_iter_histogram and
+                                g.flat_masked_count == cr.flat_masked_count and
+                                g.noise_masked_count == cr.noise_masked_count)
+    libm = _neq(gl.data, cr.data) | (np.asarray(gl_t) != np.asarray(cr_t))
+    if gl.mask is not None:
+        libm |= (np.asarray(gl.mask) != np.asarray(cr.mask)) | _neq(gl.cos_lia, cr.cos_lia)
+    keep = ~libm
+    a = np.asarray(g.data, np.float64)[keep]
+    b = np.asarray(gl.data, np.float64)[keep]
+    both = np.isfinite(a) & np.isfinite(b)
+    rel = np.abs(a[both] - b[both]) / np.maximum(np.abs(b[both]), 1e-30)
+    outside = {
+        "px": int(keep.sum()),
+        "time_mismatch_px": int((np.asarray(g.azimuth_time_us)[keep] != np.asarray(gl_t)[keep]).sum()),
+        "nan_pattern_equal": bool(np.array_equal(np.isfinite(a), np.isfinite(b))),
+        "sigma_rel_over_1e-4_px": int((rel > 1e-4).sum()),
+        "mask_equal": bool(gl.mask is None or np.array_equal(np.asarray(g.mask)[keep], np.asarray(gl.mask)[keep])),
+    }
+    keys = ("compared_px", "time_mismatch_px", "geoloc_err_px_max", "nan_pattern_equal", "mask_equal",
+            "sigma_rel_over_1e-4_px", "sigma_rel_err_max", "sigma_rel_err_mean", "cos_lia_abs_err_max",
+            "counters_equal")
+    return {"vs_correctly_rounded_oracle": {k: rep_cr.get(k) for k in keys},
+            "oracle_glibc_vs_correctly_rounded_px": int(libm.sum()),
+            "oracle_glibc_vs_correctly_rounded_time_px": int((np.asarray(gl_t) != np.asarray(cr_t)).sum()),
+            "vs_glibc_oracle_outside_those_px": outside}
 
 
 # ── config 4: batched multi-scene tiles ─────────────────────────────────────

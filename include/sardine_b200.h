@@ -703,6 +703,12 @@ int sd_write_cog(sd_ctx *ctx, const char *path, const float *data, uint64_t cols
 int sd_measure_fp64_peak(sd_ctx *ctx, int32_t iters, double *tflops);
 int sd_measure_fp32_peak(sd_ctx *ctx, int32_t iters, double *tflops);
 
+/* Correctly rounded sin and cos (the device's copy of the function the
+ * terrain correction takes its target ECEF sines and cosines from) of n
+ * doubles in device memory; no counterpart in the reference, which calls the
+ * platform libm (geodesy.rs:42-45). */
+int sd_cr_sincos(sd_ctx *ctx, const double *x, uint64_t n, double *s, double *c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,9 @@ def _declare(L):
     d, f, i32, i64, u64 = C.c_double, C.c_float, C.c_int32, C.c_int64, C.c_uint64
     sig = {
         "orc_set_threads": (None, [C.c_int]),
+        "orc_set_libm": (None, [C.c_int]),
+        "orc_get_libm": (C.c_int, []),
+        "orc_cr_sincos": (None, [P, C.c_uint64, P, P]),
         "orc_get_threads": (C.c_int, []),
         "orc_interpolate_orbit_and_accel": (C.c_int, [P, u64, i64, P, P, P]),
         "orc_solve_zero_doppler": (C.c_int, [P, P, u64, i64, u64, d, P, P, P]),
@@ -107,6 +110,36 @@ def _a(x):
 
 def set_threads(n: int) -> None:
     lib().orc_set_threads(n)
+
+
+class libm:
+    """Context manager selecting the oracle's libm for the sines and cosines
+    of geodetic_to_ecef and the forward UTM projection: "glibc" (the platform
+    libm, as the reference calls it; the default) or "cr" (correctly rounded
+    sin/cos: the reference on a platform whose libm rounds correctly)."""
+
+    def __init__(self, kind: str):
+        if kind not in ("glibc", "cr"):
+            raise ValueError(kind)
+        self.kind = kind
+
+    def __enter__(self):
+        self.prev = lib().orc_get_libm()
+        lib().orc_set_libm(1 if self.kind == "cr" else 0)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_libm(self.prev)
+        return False
+
+
+def cr_sincos(x):
+    """Correctly rounded sin and cos of a float64 array."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    s = np.empty_like(x)
+    c = np.empty_like(x)
+    lib().orc_cr_sincos(x.ctypes.data, x.size, s.ctypes.data, c.ctypes.data)
+    return s, c
 
 
 def threads() -> int:

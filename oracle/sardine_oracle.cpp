@@ -15,8 +15,19 @@
 //     Krueger's n-series as given by Karney (2011), "Transverse Mercator with
 //     an accuracy of a few nanometers", J. Geodesy 85, eqs. 7-11, 35-36.
 //     Pinned only to the reference's own UTM tests (output_crs.rs:597-628).
+//     Its inverse (the anchors of a projected output row) always takes its
+//     elementary functions from sardine_b200/csrc/crmath.cuh, one arithmetic
+//     for host and device: proj4rs's own arithmetic is not available here,
+//     and with one libm on both sides the anchors are the same bits in the
+//     oracle and on the device.  The forward projection of DEM lookups
+//     follows the libm setting below.
 //   * libm sin/cos/sqrt: the reference calls the platform libm (glibc on
-//     Linux); this file calls the same functions.
+//     Linux); this file calls the same functions by default.  orc_set_libm(1)
+//     switches the sines and cosines of geodetic_to_ecef and the functions of
+//     the forward UTM projection to crmath.cuh (correctly rounded sin/cos):
+//     the reference as it would run on a platform whose libm rounds
+//     correctly.  The two settings differ exactly where glibc's results are
+//     not correctly rounded (~1.4e-3 of its sin/cos results).
 //
 // Arithmetic follows the reference operation by operation: f32 where the
 // reference uses f32, f64 where it uses f64, left-to-right evaluation, no
@@ -36,8 +47,14 @@
 #include <vector>
 
 #include "../include/sardine_b200.h"
+#include "../sardine_b200/csrc/crmath.cuh"
 
 namespace {
+
+// 0: the platform libm (the reference's); 1: crmath.cuh (correctly rounded
+// sin/cos) for geodetic_to_ecef and the forward UTM projection.
+std::atomic<int> g_cr_libm{0};
+inline bool cr_libm() { return g_cr_libm.load(std::memory_order_relaxed) != 0; }
 
 // ── constants (geodesy.rs:13-25, types.rs:11) ─────────────────────────────
 constexpr double kPi = 3.14159265358979323846;  // std::f64::consts::PI
@@ -124,8 +141,14 @@ inline V3 normalize3(V3 v) {
 inline V3 geodetic_to_ecef(double lat_deg, double lon_deg, double h) {
   double lat = lat_deg * kPi / 180.0;
   double lon = lon_deg * kPi / 180.0;
-  double sin_lat = std::sin(lat), cos_lat = std::cos(lat);
-  double sin_lon = std::sin(lon), cos_lon = std::cos(lon);
+  double sin_lat, cos_lat, sin_lon, cos_lon;
+  if (cr_libm()) {
+    sd::crm::sincos(lat, &sin_lat, &cos_lat);
+    sd::crm::sincos(lon, &sin_lon, &cos_lon);
+  } else {
+    sin_lat = std::sin(lat), cos_lat = std::cos(lat);
+    sin_lon = std::sin(lon), cos_lon = std::cos(lon);
+  }
   double n = WGS84_A / std::sqrt(1.0 - WGS84_E2 * sin_lat * sin_lat);
   return {(n + h) * cos_lat * cos_lon, (n + h) * cos_lat * sin_lon,
           (n * (1.0 - WGS84_E2) + h) * sin_lat};
@@ -177,9 +200,11 @@ inline double adjlon(double lam) {  // wrap to [-pi, pi]
 }
 
 // sum_j c[j] * sin(2 j (xi + i eta)), returned as (re, im)
-inline void krueger_sum(const double *c, double xi, double eta, double *re, double *im) {
-  double s1 = std::sin(2.0 * xi), c1 = std::cos(2.0 * xi);
-  double sh1 = std::sinh(2.0 * eta), ch1 = std::cosh(2.0 * eta);
+inline void krueger_sum(const double *c, double xi, double eta, double *re, double *im, bool crl) {
+  double s1 = crl ? sd::crm::sin(2.0 * xi) : std::sin(2.0 * xi);
+  double c1 = crl ? sd::crm::cos(2.0 * xi) : std::cos(2.0 * xi);
+  double sh1 = crl ? sd::crm::sinh(2.0 * eta) : std::sinh(2.0 * eta);
+  double ch1 = crl ? sd::crm::cosh(2.0 * eta) : std::cosh(2.0 * eta);
   // sin(2 zeta) and cos(2 zeta) for zeta = xi + i eta
   double sr = s1 * ch1, si = c1 * sh1;    // sin(2z)
   double cr = c1 * ch1, ci = -s1 * sh1;   // cos(2z)
@@ -198,7 +223,12 @@ inline void krueger_sum(const double *c, double xi, double eta, double *re, doub
   *im = acci;
 }
 
-inline double taupf(double tau, double e) {  // tau' from tau (Karney eq. 7-9)
+inline double taupf(double tau, double e, bool cr) {  // tau' from tau (Karney eq. 7-9)
+  if (cr) {
+    double tau1 = sd::crm::hypot(1.0, tau);
+    double sig = sd::crm::sinh(e * sd::crm::atanh(e * tau / tau1));
+    return sd::crm::hypot(1.0, sig) * tau - sig * tau1;
+  }
   double tau1 = std::hypot(1.0, tau);
   double sig = std::sinh(e * std::atanh(e * tau / tau1));
   return std::hypot(1.0, sig) * tau - sig * tau1;
@@ -207,9 +237,9 @@ inline double taupf(double tau, double e) {  // tau' from tau (Karney eq. 7-9)
 inline double tauf(double taup, double e, double e2m) {  // inverse of taupf (eq. 19-21)
   double tau = taup / e2m;
   for (int i = 0; i < 6; ++i) {
-    double taupa = taupf(tau, e);
+    double taupa = taupf(tau, e, true);
     double dtau = (taup - taupa) * (1.0 + e2m * tau * tau) /
-                  (e2m * std::hypot(1.0, tau) * std::hypot(1.0, taupa));
+                  (e2m * sd::crm::hypot(1.0, tau) * sd::crm::hypot(1.0, taupa));
     tau += dtau;
     if (!(std::fabs(dtau) >= 1e-15 * std::max(1.0, std::fabs(tau)))) break;
   }
@@ -218,13 +248,20 @@ inline double tauf(double taup, double e, double e2m) {  // inverse of taupf (eq
 
 // lon, lat in radians -> easting, northing (m)
 void utm_forward(const Utm &u, double lon, double lat, double *x, double *y) {
+  const bool cr = cr_libm();
   double lam = adjlon(lon - u.lon0);
-  double tau = std::tan(lat);
-  double taup = taupf(tau, u.e);
-  double xip = std::atan2(taup, std::cos(lam));
-  double etap = std::asinh(std::sin(lam) / std::hypot(taup, std::cos(lam)));
+  double tau = cr ? sd::crm::tan(lat) : std::tan(lat);
+  double taup = taupf(tau, u.e, cr);
+  double xip, etap;
+  if (cr) {
+    xip = sd::crm::atan2(taup, sd::crm::cos(lam));
+    etap = sd::crm::asinh(sd::crm::sin(lam) / sd::crm::hypot(taup, sd::crm::cos(lam)));
+  } else {
+    xip = std::atan2(taup, std::cos(lam));
+    etap = std::asinh(std::sin(lam) / std::hypot(taup, std::cos(lam)));
+  }
   double sr, si;
-  krueger_sum(u.alp, xip, etap, &sr, &si);
+  krueger_sum(u.alp, xip, etap, &sr, &si, cr);
   double xi = xip + sr, eta = etap + si;
   *x = 500000.0 + u.k0A * eta;
   *y = (u.south ? 10000000.0 : 0.0) + u.k0A * xi;
@@ -235,13 +272,13 @@ void utm_inverse(const Utm &u, double x, double y, double *lon, double *lat) {
   double xi = (y - (u.south ? 10000000.0 : 0.0)) / u.k0A;
   double eta = (x - 500000.0) / u.k0A;
   double sr, si;
-  krueger_sum(u.bet, xi, eta, &sr, &si);
+  krueger_sum(u.bet, xi, eta, &sr, &si, true);
   double xip = xi - sr, etap = eta - si;
-  double s = std::sinh(etap), c = std::cos(xip);
-  double taup = std::sin(xip) / std::hypot(s, c);
+  double s = sd::crm::sinh(etap), c = sd::crm::cos(xip);
+  double taup = sd::crm::sin(xip) / sd::crm::hypot(s, c);
   double tau = tauf(taup, u.e, u.e2m);
-  *lat = std::atan(tau);
-  *lon = adjlon(std::atan2(s, c) + u.lon0);
+  *lat = sd::crm::atan(tau);
+  *lon = adjlon(sd::crm::atan2(s, c) + u.lon0);
 }
 
 // Projector::lonlat_to_xy / xy_to_lonlat (output_crs.rs:301-340): degrees in
@@ -618,6 +655,16 @@ extern "C" {
 // Worker threads for the parallel loops (0 = all hardware threads).
 void orc_set_threads(int n) { g_threads.store(n < 0 ? 0 : n); }
 int orc_get_threads(void) { return n_threads(); }
+
+// Sines and cosines of geodetic_to_ecef and the forward UTM projection's
+// functions: 0 = the platform libm (default, the reference's), 1 = crmath.cuh.
+void orc_set_libm(int correctly_rounded) { g_cr_libm.store(correctly_rounded ? 1 : 0); }
+int orc_get_libm(void) { return g_cr_libm.load(); }
+
+// Correctly rounded sin and cos of n doubles (the checker of the device's).
+void orc_cr_sincos(const double *x, uint64_t n, double *s, double *c) {
+  for (uint64_t i = 0; i < n; ++i) sd::crm::sincos(x[i], s + i, c + i);
+}
 
 int orc_interpolate_orbit_and_accel(const sd_state_vector *svs, uint64_t n, int64_t t,
                                     double *pos, double *vel, double *acc) {

@@ -76,6 +76,7 @@ _SIGS = {
     "sd_downsample_2x": (C.c_int, [P, P, C.c_uint64, C.c_uint64, P]),
     "sd_write_cog": (C.c_int, [P, C.c_char_p, P, C.c_uint64, C.c_uint64, P, C.c_int32, C.c_int32, C.c_uint32]),
     "sd_measure_fp64_peak": (C.c_int, [P, C.c_int32, P]),
+    "sd_cr_sincos": (C.c_int, [P, P, C.c_uint64, P, P]),
     "sd_measure_fp32_peak": (C.c_int, [P, C.c_int32, P]),
 }
 

@@ -38,8 +38,12 @@
 
 #if defined(__CUDACC__)
 #define CRM_HD __host__ __device__ __forceinline__
+#define CRM_HD_CALL __host__ __device__ inline
+#define CRM_HD_COLD static __host__ __device__ __noinline__
 #else
 #define CRM_HD inline
+#define CRM_HD_CALL inline
+#define CRM_HD_COLD inline
 #endif
 
 namespace sd {
@@ -177,7 +181,7 @@ CRM_HD void sincos_fast(double ah, double al, DD *s, DD *c) {
 
 // sin and cos of r = (rh, rl), |r| <= pi/4 + 2^-9, by their Taylor series in
 // double-double arithmetic (terms to r^29: error ~2^-100).
-CRM_HD void sincos_slow(double rh, double rl, DD *s, DD *c) {
+CRM_HD_COLD void sincos_slow(double rh, double rl, DD *s, DD *c) {
   const DD r{rh, rl};
   const DD r2 = dd_mul(r, r);
   DD ps{invfact(2 * 29), invfact(2 * 29 + 1)};
@@ -196,8 +200,9 @@ CRM_HD void sincos_slow(double rh, double rl, DD *s, DD *c) {
   *c = pc;
 }
 
-// Correctly rounded sin(x) and cos(x).
-CRM_HD void sincos(double x, double *so, double *co) {
+// Correctly rounded sin(x) and cos(x).  The slow path is not inlined at the
+// call sites (it runs for ~1 call in 4000).
+CRM_HD_CALL void sincos(double x, double *so, double *co) {
   if (!(fabs(x) <= 1e5)) {  // outside the reduction's range, NaN, infinities
     *so = ::sin(x);
     *co = ::cos(x);
@@ -245,7 +250,7 @@ CRM_HD double tan(double x) {
 
 // ── functions of the UTM projection (a few ulps; identical on host and device)
 // e^x - 1 for |x| <= 0.35: Taylor series to x^18.
-CRM_HD double expm1_small(double x) {
+CRM_HD_CALL double expm1_small(double x) {
   double p = invfact(2 * 18);
   for (int n = 17; n >= 1; --n) p = p * x + invfact(2 * n);
   return p * x;
@@ -275,7 +280,7 @@ CRM_HD double cosh(double x) {
 // atanh(x) = sum x^(2n+1) / (2n+1) for |x| <= 0.125 (terms to x^61); the
 // platform's atanh beyond (the UTM transform's arguments stay below the
 // eccentricity, 0.082).
-CRM_HD double atanh(double x) {
+CRM_HD_CALL double atanh(double x) {
   if (!(fabs(x) <= 0.125)) return ::atanh(x);
   const double x2 = x * x;
   double p = invodd(30);
@@ -292,7 +297,7 @@ CRM_HD double asinh(double x) {
 // atan by two half-angle reductions, atan(x) = 2 atan(x / (1 + sqrt(1 + x^2))),
 // to |x| <= tan(pi/16), then its Taylor series to x^61; |x| > 1 through
 // pi/2 - atan(1/x).
-CRM_HD double atan(double x) {
+CRM_HD_CALL double atan(double x) {
   if (x != x) return x;
   const double ax = fabs(x);
   const bool inv = ax > 1.0;

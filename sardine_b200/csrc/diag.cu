@@ -1,6 +1,7 @@
 // diag.cu — FP64 / FP32 FMA-chain throughput probes.  The roofline of the
 // terrain correction is the FP64 pipe, whose peak is not among the measured
 // HBM / tensor figures; this measures it on the device at run time.
+#include "crmath.cuh"
 #include "runtime.cuh"
 
 namespace sd {
@@ -43,8 +44,25 @@ int measure(sd_ctx *ctx, int iters, double *tflops) {
   return SD_OK;
 }
 
+__global__ void k_cr_sincos(const double *x, uint64_t n, double *s, double *c) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) crm::sincos(x[i], s + i, c + i);
+}
+
 }  // namespace
 }  // namespace sd
+
+extern "C" int sd_cr_sincos(sd_ctx *ctx, const double *x, uint64_t n, double *s, double *c) {
+  if (!ctx || (n && (!x || !s || !c))) return SD_ERR_INVALID_ARGUMENT;
+  if (n == 0) return SD_OK;
+  if (!sd::is_device_ptr(x) || !sd::is_device_ptr(s) || !sd::is_device_ptr(c))
+    return sd::set_error(ctx, SD_ERR_INVALID_ARGUMENT, "sd_cr_sincos needs device buffers");
+  SD_CUDA(ctx, cudaSetDevice(ctx->device));
+  SD_TIMED_BEGIN(ctx, "k_cr_sincos");
+  sd::k_cr_sincos<<<sd::grid_for(n, 256), 256, 0, ctx->stream>>>(x, n, s, c);
+  SD_LAUNCHED(ctx);
+  return SD_OK;
+}
 
 extern "C" int sd_measure_fp64_peak(sd_ctx *ctx, int32_t iters, double *tflops) {
   if (!ctx || !tflops || iters <= 0) return SD_ERR_INVALID_ARGUMENT;

@@ -12,11 +12,14 @@
 #include <cstdint>
 
 #include "../../include/sardine_b200.h"
+#include "crmath.cuh"
 
 #if defined(__CUDACC__)
 #define SD_HD __host__ __device__ __forceinline__
+#define SD_HD_COLD static __host__ __device__ __noinline__  // rare paths, kept out of line
 #else
 #define SD_HD inline
+#define SD_HD_COLD inline
 #endif
 
 namespace sd {
@@ -68,12 +71,15 @@ SD_HD V3 normalize3(V3 v) {
   return {v.x / n, v.y / n, v.z / n};
 }
 
-// geodetic_to_ecef (geodesy.rs:38-55)
+// geodetic_to_ecef (geodesy.rs:38-55), with correctly rounded sines and
+// cosines (crmath.cuh): equal to the reference's wherever its libm rounds
+// correctly.
 SD_HD V3 geodetic_to_ecef(double lat_deg, double lon_deg, double h) {
   double lat = lat_deg * kPi / 180.0;
   double lon = lon_deg * kPi / 180.0;
-  double sin_lat = sin(lat), cos_lat = cos(lat);
-  double sin_lon = sin(lon), cos_lon = cos(lon);
+  double sin_lat, cos_lat, sin_lon, cos_lon;
+  crm::sincos(lat, &sin_lat, &cos_lat);
+  crm::sincos(lon, &sin_lon, &cos_lon);
   double n = WGS84_A / sqrt(1.0 - WGS84_E2 * sin_lat * sin_lat);
   return {(n + h) * cos_lat * cos_lon, (n + h) * cos_lat * sin_lon,
           (n * (1.0 - WGS84_E2) + h) * sin_lat};
@@ -126,10 +132,13 @@ SD_HD double adjlon(double lam) {
   return lam;
 }
 
+// The exact forward and inverse transforms take their elementary functions
+// from crmath.cuh, the arithmetic the oracle's restatement uses for them.
 // sum_{j=1..6} c[j] sin(2 j zeta), zeta = xi + i eta  (complex Chebyshev recurrence)
 SD_HD void krueger_sum(const double *c, double xi, double eta, double *re, double *im) {
-  double s1 = sin(2.0 * xi), c1 = cos(2.0 * xi);
-  double sh1 = sinh(2.0 * eta), ch1 = cosh(2.0 * eta);
+  double s1, c1;
+  crm::sincos(2.0 * xi, &s1, &c1);
+  double sh1 = crm::sinh(2.0 * eta), ch1 = crm::cosh(2.0 * eta);
   double sr = s1 * ch1, si = c1 * sh1;
   double cr = c1 * ch1, ci = -s1 * sh1;
   double pr = 0.0, pi = 0.0, qr = sr, qi = si, ar = 0.0, ai = 0.0;
@@ -145,16 +154,16 @@ SD_HD void krueger_sum(const double *c, double xi, double eta, double *re, doubl
 }
 
 SD_HD double taupf(double tau, double e) {
-  double tau1 = hypot(1.0, tau);
-  double sig = sinh(e * atanh(e * tau / tau1));
-  return hypot(1.0, sig) * tau - sig * tau1;
+  double tau1 = crm::hypot(1.0, tau);
+  double sig = crm::sinh(e * crm::atanh(e * tau / tau1));
+  return crm::hypot(1.0, sig) * tau - sig * tau1;
 }
 
 SD_HD double tauf(double taup, double e, double e2m) {
   double tau = taup / e2m;
   for (int i = 0; i < 6; ++i) {
     double taupa = taupf(tau, e);
-    double dtau = (taup - taupa) * (1.0 + e2m * tau * tau) / (e2m * hypot(1.0, tau) * hypot(1.0, taupa));
+    double dtau = (taup - taupa) * (1.0 + e2m * tau * tau) / (e2m * crm::hypot(1.0, tau) * crm::hypot(1.0, taupa));
     tau += dtau;
     double lim = fabs(tau) > 1.0 ? fabs(tau) : 1.0;
     if (!(fabs(dtau) >= 1e-15 * lim)) break;
@@ -165,11 +174,12 @@ SD_HD double tauf(double taup, double e, double e2m) {
 // lon/lat in degrees -> easting/northing (Projector::lonlat_to_xy, output_crs.rs:301-315)
 SD_HD void utm_lonlat_to_xy(const Utm &u, double lon_deg, double lat_deg, double *x, double *y) {
   double lam = adjlon(lon_deg * (kPi / 180.0) - u.lon0);
-  double tau = tan(lat_deg * (kPi / 180.0));
+  double tau = crm::tan(lat_deg * (kPi / 180.0));
   double taup = taupf(tau, u.e);
-  double cl = cos(lam);
-  double xip = atan2(taup, cl);
-  double etap = asinh(sin(lam) / hypot(taup, cl));
+  double sl, cl;
+  crm::sincos(lam, &sl, &cl);
+  double xip = crm::atan2(taup, cl);
+  double etap = crm::asinh(sl / crm::hypot(taup, cl));
   double sr, si;
   krueger_sum(u.alp, xip, etap, &sr, &si);
   *x = 500000.0 + u.k0A * (etap + si);
@@ -183,11 +193,13 @@ SD_HD void utm_xy_to_lonlat(const Utm &u, double x, double y, double *lon_deg, d
   double sr, si;
   krueger_sum(u.bet, xi, eta, &sr, &si);
   double xip = xi - sr, etap = eta - si;
-  double s = sinh(etap), c = cos(xip);
-  double taup = sin(xip) / hypot(s, c);
+  double sx, c;
+  crm::sincos(xip, &sx, &c);
+  double s = crm::sinh(etap);
+  double taup = sx / crm::hypot(s, c);
   double tau = tauf(taup, u.e, u.e2m);
-  *lat_deg = atan(tau) * (180.0 / kPi);
-  *lon_deg = adjlon(atan2(s, c) + u.lon0) * (180.0 / kPi);
+  *lat_deg = crm::atan(tau) * (180.0 / kPi);
+  *lon_deg = adjlon(crm::atan2(s, c) + u.lon0) * (180.0 / kPi);
 }
 
 // The forward projection split into its latitude-only and longitude-only
@@ -289,6 +301,30 @@ SD_HD void utm_local_step(const Utm &u, const UtmLocal &l, double dphi, double d
   *y = l.y + u.k0A * dz_re;
 }
 
+// Projected point (and local expansion) at position t of the segment between
+// two anchors A, B whose lon/lat differ by (dphi, dlam) radians: a cubic
+// Hermite through the anchors' projected points and their derivatives along
+// the segment (d/dt = dzeta/dw . (psi' dphi + i dlam)); the local-expansion
+// terms are interpolated linearly.
+SD_HD void utm_local_hermite(const UtmLocal &A, const UtmLocal &B, double dphi, double dlam, double k0A,
+                             double t, UtmLocal *o) {
+  const double aw = A.dpsi1 * dphi, bw = B.dpsi1 * dphi;
+  const double ax_ = k0A * (A.zw_re * dlam + A.zw_im * aw), ay_ = k0A * (A.zw_re * aw - A.zw_im * dlam);
+  const double bx_ = k0A * (B.zw_re * dlam + B.zw_im * bw), by_ = k0A * (B.zw_re * bw - B.zw_im * dlam);
+  const double t2 = t * t, t3 = t2 * t;
+  const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
+  const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+  o->x = h00 * A.x + h10 * ax_ + h01 * B.x + h11 * bx_;
+  o->y = h00 * A.y + h10 * ay_ + h01 * B.y + h11 * by_;
+  const double u = 1.0 - t;
+  o->zw_re = u * A.zw_re + t * B.zw_re;
+  o->zw_im = u * A.zw_im + t * B.zw_im;
+  o->zww_re = u * A.zww_re + t * B.zww_re;
+  o->zww_im = u * A.zww_im + t * B.zww_im;
+  o->dpsi1 = u * A.dpsi1 + t * B.dpsi1;
+  o->dpsi2 = u * A.dpsi2 + t * B.dpsi2;
+}
+
 // sin/cos of a + b from sin/cos of a, for |b| < 1e-4 (series to b^4).
 SD_HD void sincos_add(double sa, double ca, double b, double *s, double *c) {
   const double b2 = b * b;
@@ -367,6 +403,102 @@ SD_HD bool dem_sample(const DemView &d, double row_f, double col_f, float *h) {
              (double)v10 * dr * (1.0 - dc) + (double)v11 * dr * dc;
   *h = (float)v;
   return true;
+}
+
+// ── certified lookups ──────────────────────────────────────────────────────
+// The device forms the DEM position of a UTM pixel by interpolation (the
+// centre by a cubic Hermite between its row's anchors, the cardinal
+// neighbours by a second-order local step) and fractional indices by
+// multiplying with the reciprocal of the pixel size; the reference projects
+// every lookup and divides.  The positions agree to ~9e-9 m (measured on a
+// 250 km UTM row at 5,200 km northing, where the rounding of ~5e6 m northings
+// dominates); kDemPosEps allows for northings up to 1e7 m.  A lookup is
+// "decided" when the height the exact position gives is certain to be the
+// same f32: no f32 rounding boundary lies within the bilinear value's
+// uncertainty, and no cell edge, clamp or DEM margin lies within the
+// position's.  An undecided lookup (~1e-4 of them) is redone exactly
+// (dem_elevation).
+constexpr double kDemPosEps = 3e-8;  // m
+
+// 1 = decided (*inside = the lookup is inside the DEM; *h its height, NaN
+// for a void), 0 = undecided.  eps_px: position uncertainty in pixels,
+// to which the reciprocal's rounding is added here.
+SD_HD int dem_sample_cert(const DemView &d, double row_f, double col_f, double eps_px, bool *inside, float *h) {
+  if (row_f != row_f || col_f != col_f) return 0;
+  const double eps = eps_px + 5e-16 * (fabs(row_f) + fabs(col_f));
+  const double max_row = (double)(d.height - 1);
+  const double max_col = (double)(d.width - 1);
+  // the +-0.5 px margin (dem.rs:351-371)
+  if (row_f < -0.5 - eps || row_f > max_row + 0.5 + eps || col_f < -0.5 - eps || col_f > max_col + 0.5 + eps) {
+    *inside = false;
+    return 1;
+  }
+  if (row_f < -0.5 + eps || row_f > max_row + 0.5 - eps || col_f < -0.5 + eps || col_f > max_col + 0.5 - eps)
+    return 0;
+  // the clamps to [0, max]
+  if (fabs(row_f) <= eps || fabs(row_f - max_row) <= eps || fabs(col_f) <= eps || fabs(col_f - max_col) <= eps)
+    return 0;
+  *inside = true;
+  row_f = clampd(row_f, 0.0, max_row);
+  col_f = clampd(col_f, 0.0, max_col);
+  uint64_t max_rc = d.height - 1;
+  uint64_t r0 = f2u64(row_f);
+  uint64_t rlim = max_rc == 0 ? 0 : max_rc - 1;
+  if (r0 > rlim) r0 = rlim;
+  uint64_t c0 = f2u64(col_f);
+  uint64_t clim = d.width < 2 ? 0 : d.width - 2;
+  if (c0 > clim) c0 = clim;
+  const uint64_t r1 = r0 + 1, c1 = c0 + 1;
+  const double dr = row_f - (double)r0;
+  const double dc = col_f - (double)c0;
+  if (dr <= eps || dr >= 1.0 - eps || dc <= eps || dc >= 1.0 - eps) return 0;  // a cell edge
+#if defined(__CUDA_ARCH__)
+  const float v00 = __ldg(&d.data[r0 * d.width + c0]), v01 = __ldg(&d.data[r0 * d.width + c1]);
+  const float v10 = __ldg(&d.data[r1 * d.width + c0]), v11 = __ldg(&d.data[r1 * d.width + c1]);
+#else
+  const float v00 = d.data[r0 * d.width + c0], v01 = d.data[r0 * d.width + c1];
+  const float v10 = d.data[r1 * d.width + c0], v11 = d.data[r1 * d.width + c1];
+#endif
+  if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) {
+    *h = NAN;
+    return 1;
+  }
+  const double v = (double)v00 * (1.0 - dr) * (1.0 - dc) + (double)v01 * (1.0 - dr) * dc +
+                   (double)v10 * dr * (1.0 - dc) + (double)v11 * dr * dc;
+  // the value's uncertainty: its slopes over eps, plus the rounding of this
+  // sum and of the exact position's (a few ulps of the corner magnitudes)
+  const double gr = fmax(fabs((double)v10 - (double)v00), fabs((double)v11 - (double)v01));
+  const double gc = fmax(fabs((double)v01 - (double)v00), fabs((double)v11 - (double)v10));
+  const double dv = (gr + gc) * eps +
+                    2e-15 * (fabs((double)v00) + fabs((double)v01) + fabs((double)v10) + fabs((double)v11));
+  const float lo = (float)(v - dv), hi = (float)(v + dv);
+  if (lo != hi) return 0;
+  *h = (float)v;
+  return 1;
+}
+
+SD_HD bool dem_elevation(const DemView &d, double lat_deg, double lon_deg, float *h);
+SD_HD_COLD bool dem_elevation_exact(const DemView &d, double lat_deg, double lon_deg, float *h) {
+  return dem_elevation(d, lat_deg, lon_deg, h);
+}
+
+// Height at an interpolated projected position (x, y) of the geodetic point
+// (lat, lon): decided from the position when possible, else the exact lookup.
+SD_HD bool dem_at_xy_checked(const DemView &d, double x, double y, double lat_deg, double lon_deg, float *h) {
+  bool inside = false;
+  if (dem_sample_cert(d, (d.origin_y - y) * d.inv_ps, (x - d.origin_x) * d.inv_ps, kDemPosEps * d.inv_ps,
+                      &inside, h))
+    return inside;
+  return dem_elevation_exact(d, lat_deg, lon_deg, h);
+}
+// Height at an exact lon/lat on a geographic DEM (only the reciprocal's
+// rounding to allow for).
+SD_HD bool dem_at_lonlat_checked(const DemView &d, double lon_deg, double lat_deg, float *h) {
+  bool inside = false;
+  const double lon_norm = lon_deg >= 180.0 ? lon_deg - 360.0 : lon_deg;
+  if (dem_sample_cert(d, (d.origin_y - lat_deg) * d.inv_ps, (lon_norm - d.origin_x) * d.inv_ps, 0.0, &inside, h))
+    return inside;
+  return dem_elevation_exact(d, lat_deg, lon_deg, h);
 }
 
 // The reference divides by the pixel size; the product with its reciprocal

@@ -259,24 +259,7 @@ __device__ void dem_local_from_anchors(const TcDev &p, uint64_t r, int g, double
   const UtmLocal &A = p.aloc[r * p.n_pts + g], &B = p.aloc[r * p.n_pts + g + 1];
   const double *lo = p.alon + r * p.n_pts, *la = p.alat + r * p.n_pts;
   const double k = kPi / 180.0;
-  const double dphi = (la[g + 1] - la[g]) * k, dlam = (lo[g + 1] - lo[g]) * k;
-  const double k0A = p.dem.utm.k0A;
-  // derivatives along the segment at both ends
-  const double aw = A.dpsi1 * dphi, bw = B.dpsi1 * dphi;
-  const double ax_ = k0A * (A.zw_re * dlam + A.zw_im * aw), ay_ = k0A * (A.zw_re * aw - A.zw_im * dlam);
-  const double bx_ = k0A * (B.zw_re * dlam + B.zw_im * bw), by_ = k0A * (B.zw_re * bw - B.zw_im * dlam);
-  const double t2 = t * t, t3 = t2 * t;
-  const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
-  const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
-  o->x = h00 * A.x + h10 * ax_ + h01 * B.x + h11 * bx_;
-  o->y = h00 * A.y + h10 * ay_ + h01 * B.y + h11 * by_;
-  const double u = 1.0 - t;
-  o->zw_re = u * A.zw_re + t * B.zw_re;
-  o->zw_im = u * A.zw_im + t * B.zw_im;
-  o->zww_re = u * A.zww_re + t * B.zww_re;
-  o->zww_im = u * A.zww_im + t * B.zww_im;
-  o->dpsi1 = u * A.dpsi1 + t * B.dpsi1;
-  o->dpsi2 = u * A.dpsi2 + t * B.dpsi2;
+  utm_local_hermite(A, B, (la[g + 1] - la[g]) * k, (lo[g + 1] - lo[g]) * k, p.dem.utm.k0A, t, o);
 }
 
 // guess_azimuth_time (terrain_correction.rs:1107-1137)
@@ -857,9 +840,9 @@ __device__ bool pixel_height(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g, 
     const Utm &u = p.dem.utm;
     if (p.aloc) dem_local_from_anchors(p, r, seg, t, &g->loc);
     else utm_local(u, g->lat, utm_taup(u, g->lat), utm_lam(u, g->lon), &g->loc);
-    ok = dem_at_xy(p.dem, g->loc.x, g->loc.y, hf);
+    ok = dem_at_xy_checked(p.dem, g->loc.x, g->loc.y, g->lat, g->lon, hf);
   } else {
-    ok = dem_at_lonlat(p.dem, g->lon, g->lat, hf);
+    ok = dem_at_lonlat_checked(p.dem, g->lon, g->lat, hf);
   }
   return ok && isfinite(*hf);
 }
@@ -869,10 +852,8 @@ __device__ __forceinline__ void pixel_ecef(const TcDev &p, PixGeo *g, float hf) 
   double h_ell = (double)hf + geoid_undulation(p.geoid, g->lat, g->lon);
   g->la = deg2rad_ecef(g->lat);
   g->lo = deg2rad_ecef(g->lon);
-  g->sla = sin(g->la);
-  g->cla = cos(g->la);
-  g->slo = sin(g->lo);
-  g->clo = cos(g->lo);
+  crm::sincos(g->la, &g->sla, &g->cla);  // correctly rounded (crmath.cuh)
+  crm::sincos(g->lo, &g->slo, &g->clo);
   g->P = ecef_sc(g->sla, g->cla, g->slo, g->clo, h_ell);
 }
 
@@ -905,18 +886,18 @@ __device__ bool facet_heights(const TcDev &p, const PixGeo &g, float h[4]) {
     const double k = kPi / 180.0;
     double x, y;
     utm_local_step(u, g.loc, 0.0, (lon_e - g.lon) * k, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &he);
+    ok = dem_at_xy_checked(p.dem, x, y, g.lat, lon_e, &he);
     utm_local_step(u, g.loc, 0.0, (lon_w - g.lon) * k, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &hw) && ok;
+    ok = dem_at_xy_checked(p.dem, x, y, g.lat, lon_w, &hw) && ok;
     utm_local_step(u, g.loc, (lat_n - g.lat) * k, 0.0, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &hn) && ok;
+    ok = dem_at_xy_checked(p.dem, x, y, lat_n, g.lon, &hn) && ok;
     utm_local_step(u, g.loc, (lat_s - g.lat) * k, 0.0, &x, &y);
-    ok = dem_at_xy(p.dem, x, y, &hs) && ok;
+    ok = dem_at_xy_checked(p.dem, x, y, lat_s, g.lon, &hs) && ok;
   } else {
-    ok = dem_at_lonlat(p.dem, lon_e, g.lat, &he);
-    ok = dem_at_lonlat(p.dem, lon_w, g.lat, &hw) && ok;
-    ok = dem_at_lonlat(p.dem, g.lon, lat_n, &hn) && ok;
-    ok = dem_at_lonlat(p.dem, g.lon, lat_s, &hs) && ok;
+    ok = dem_at_lonlat_checked(p.dem, lon_e, g.lat, &he);
+    ok = dem_at_lonlat_checked(p.dem, lon_w, g.lat, &hw) && ok;
+    ok = dem_at_lonlat_checked(p.dem, g.lon, lat_n, &hn) && ok;
+    ok = dem_at_lonlat_checked(p.dem, g.lon, lat_s, &hs) && ok;
   }
   h[0] = he, h[1] = hw, h[2] = hn, h[3] = hs;
   return ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);

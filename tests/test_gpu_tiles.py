@@ -48,10 +48,18 @@ def _host(res):
 
 
 def _oracle_tile(sc, req, halo=0):
+    """The oracle on the tile's grid, with glibc's and with correctly rounded
+    sines and cosines (see test_gpu_tc)."""
     sp = req.config.pixel_spacing_deg
-    return oracle.terrain_correction_grid(sc.merged, sc.scene, sc.dem, sc.grids, req.config,
-                                          req.origin_x - halo * sp, req.origin_y + halo * sp,
-                                          req.rows + 2 * halo, req.cols + 2 * halo)
+
+    def run():
+        return oracle.terrain_correction_grid(sc.merged, sc.scene, sc.dem, sc.grids, req.config,
+                                              req.origin_x - halo * sp, req.origin_y + halo * sp,
+                                              req.rows + 2 * halo, req.cols + 2 * halo)
+    gl = run()
+    with oracle.libm("cr"):
+        cr = run()
+    return gl, cr
 
 
 def test_tiles_match_oracle(ctx):
@@ -80,10 +88,10 @@ def test_tiles_two_scenes_split_precision(ctx):
         ref = _oracle_tile(sc, req)
         r = _host(r)
         if req.config.precision == sd.Precision.SPLIT:
-            rep = compare_geocoded(r, ref)
+            rep = compare_geocoded(r, ref[1])
             assert rep["nan_pattern_equal"] and rep["mask_equal"], rep
-            assert rep["sigma_rel_over_1e-4_px"] <= 1, rep
-            assert r.newton_iter_histogram == ref.newton_iter_histogram
+            assert rep["sigma_rel_over_1e-4_px"] == 0, rep
+            assert r.newton_iter_histogram == ref[1].newton_iter_histogram
         else:
             assert_tc_parity(r, ref)
     rs1.close()
@@ -97,15 +105,14 @@ def test_tiles_speckle_halo_crop(ctx, filt, halo):
     req = _req(sc, rs, g, 40, 50, 90, 120, K.Bicubic, speckle=filt)
     assert req.halo() == halo
     r = _host(tiles.tc_tiles([req], ctx)[0])
-    big = _oracle_tile(sc, req, halo)
+    big = _oracle_tile(sc, req, halo)[1]
     rows, cols = req.rows + 2 * halo, req.cols + 2 * halo
     ref = oracle.apply_speckle_filter(big.data, cols, rows, filt)
     crop = np.asarray(ref).reshape(rows, cols)[halo:halo + req.rows, halo:halo + req.cols]
     assert np.array_equal(np.isnan(r.data), np.isnan(crop))
     ok = np.isfinite(crop)
     rel = np.abs(r.data[ok].astype(np.float64) - crop[ok]) / np.maximum(np.abs(crop[ok]), 1e-30)
-    # a 1 us flip of one geocoded pixel reaches every output whose window holds it
-    assert (rel > 1e-4).sum() <= max(1, 1e-3 * ok.sum()), rel.max()
+    assert (rel > 1e-4).sum() == 0, rel.max()
     assert np.array_equal(r.mask, big.mask[halo:halo + req.rows, halo:halo + req.cols])
     rs.close()
 
