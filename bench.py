@@ -55,7 +55,7 @@ UNIT = "px/s"
 #    ECEF + facet normal + flattening/LIA), N_it = mean Newton iterations.
 PREP_BYTES_PER_PX = 12.0
 # every kernel of the terrain-correction stage (the FP64 roofline's time)
-TC_STAGE = ("k_main", "k_heights", "k_resample", "k_redo", "k_scan", "k_select", "k_row")
+TC_STAGE = ("k_main", "k_heights", "k_resample", "k_redo", "k_scan", "k_cand", "k_row")
 TC_FLOPS = lambda n_it: n_it * 430.0 + 90.0 + 150.0
 
 

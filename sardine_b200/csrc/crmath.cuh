@@ -202,7 +202,7 @@ CRM_HD_COLD void sincos_slow(double rh, double rl, DD *s, DD *c) {
 
 // Correctly rounded sin(x) and cos(x).  The slow path is not inlined at the
 // call sites (it runs for ~1 call in 4000).
-CRM_HD_CALL void sincos(double x, double *so, double *co) {
+CRM_HD void sincos(double x, double *so, double *co) {
   if (!(fabs(x) <= 1e5)) {  // outside the reduction's range, NaN, infinities
     *so = ::sin(x);
     *co = ::cos(x);

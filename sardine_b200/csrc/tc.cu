@@ -68,20 +68,18 @@ extern "C" int sd_tc_output_grid(sd_ctx *ctx, const sd_scene *scene, const sd_tc
 namespace sd {
 namespace {
 
-// Single job: k_main with the job record as a kernel parameter, specialised
-// per resampling kernel.
+// Single job: k_main with the job record as a kernel parameter; the later
+// stages specialised per resampling kernel.
 int launch_pixels_single(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, int kernel, bool split,
                          const TcDev *job) {
-  {
-    if (kernel == SD_RESAMPLE_BICUBIC)
-      return split ? launch_pixels_t<SD_RESAMPLE_BICUBIC, true>(ctx, d_work, totals, "k_main<BICUBIC,SPLIT>", job)
-                   : launch_pixels_t<SD_RESAMPLE_BICUBIC, false>(ctx, d_work, totals, "k_main<BICUBIC>", job);
-    if (kernel == SD_RESAMPLE_LANCZOS3)
-      return split ? launch_pixels_t<SD_RESAMPLE_LANCZOS3, true>(ctx, d_work, totals, "k_main<LANCZOS3,SPLIT>", job)
-                   : launch_pixels_t<SD_RESAMPLE_LANCZOS3, false>(ctx, d_work, totals, "k_main<LANCZOS3>", job);
-    return split ? launch_pixels_t<SD_RESAMPLE_BILINEAR, true>(ctx, d_work, totals, "k_main<BILINEAR,SPLIT>", job)
-                 : launch_pixels_t<SD_RESAMPLE_BILINEAR, false>(ctx, d_work, totals, "k_main<BILINEAR>", job);
-  }
+  if (kernel == SD_RESAMPLE_BICUBIC)
+    return split ? launch_pixels_t<SD_RESAMPLE_BICUBIC, true>(ctx, d_work, totals, job)
+                 : launch_pixels_t<SD_RESAMPLE_BICUBIC, false>(ctx, d_work, totals, job);
+  if (kernel == SD_RESAMPLE_LANCZOS3)
+    return split ? launch_pixels_t<SD_RESAMPLE_LANCZOS3, true>(ctx, d_work, totals, job)
+                 : launch_pixels_t<SD_RESAMPLE_LANCZOS3, false>(ctx, d_work, totals, job);
+  return split ? launch_pixels_t<SD_RESAMPLE_BILINEAR, true>(ctx, d_work, totals, job)
+               : launch_pixels_t<SD_RESAMPLE_BILINEAR, false>(ctx, d_work, totals, job);
 }
 
 }  // namespace
@@ -92,17 +90,7 @@ int launch_main_param(sd_ctx *ctx, const void *job, cudaStream_t st) {
   if (items == 0) return SD_OK;
   if (items > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "tile too large");
   const unsigned g = (unsigned)items;
-#define SD_MAIN_PARAM(K)                                                              \
-  if (p.split) k_main<K, true><<<g, MAIN_THREADS, 0, st>>>(p);                         \
-  else k_main<K, false><<<g, MAIN_THREADS, 0, st>>>(p);
-  if (p.resampling == SD_RESAMPLE_BICUBIC) {
-    SD_MAIN_PARAM(SD_RESAMPLE_BICUBIC)
-  } else if (p.resampling == SD_RESAMPLE_LANCZOS3) {
-    SD_MAIN_PARAM(SD_RESAMPLE_LANCZOS3)
-  } else {
-    SD_MAIN_PARAM(SD_RESAMPLE_BILINEAR)
-  }
-#undef SD_MAIN_PARAM
+  k_main<<<g, MAIN_THREADS, 0, st>>>(p);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return set_error(ctx, SD_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
@@ -270,7 +258,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   SD_TRY(scratch_t(ctx, "tc.hnb", npx, &d_hnb));
   p.hc = d_hc;
   p.hnb = d_hnb;
-  SD_TRY(scratch_t(ctx, "tc.rec", npx, &p.rec));
+  SD_TRY(scratch_t(ctx, "tc.fb", npx, &p.fb));
   SD_TRY(scratch_t(ctx, "tc.cc", npx, &p.cc));
   SD_TRY(scratch_t(ctx, "tc.sel", npx, &p.sel));
   void *d_out, *d_cos = nullptr, *d_mask = nullptr;
@@ -295,9 +283,10 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   p.fast = (p.tol <= 1e-6) ? 1 : 0;
   p.bpr = (p.cols + MAIN_PIX - 1) / MAIN_PIX;
   p.split = cfg->precision == SD_PRECISION_SPLIT;
-  if (p.split) {  // FP64 re-sample queue of every k_main item
-    SD_TRY(scratch_t(ctx, "tc.rs_cnt", p.rows * p.bpr, &p.rs_cnt));
-    SD_TRY(scratch_t(ctx, "tc.rs_ent", p.rows * p.bpr * RS_CAP, &p.rs_ent));
+  if (p.split) {  // FP64 re-sample queue of every k_cand item
+    const uint64_t items = stage_items(WK_SEL, p);
+    SD_TRY(scratch_t(ctx, "tc.rs_cnt", items, &p.rs_cnt));
+    SD_TRY(scratch_t(ctx, "tc.rs_ent", items * RS_CAP, &p.rs_ent));
   }
 
   // ── one-job work table ──

@@ -19,19 +19,25 @@
 //  k_row_*         per-row set-up: UTM anchors (output_crs.rs:364-417),
 //                  latitude seed, LUT guess, flat-cell area, and a coarse
 //                  azimuth-time model (17 knots per row).
-//  k_main          per pixel: DEM, geoid, target ECEF; the reference
-//                  iteration from the model time gives one converged time
-//                  t*; the set F = {t : |delta(t)| < tol} of possible
-//                  converged times (a pair {fb, fb+1}); the outcome of the
-//                  reference iteration from every member of the left
-//                  neighbour's F (the only seeds the chain can hand it); and
-//                  the outputs (resampling, Small-2011 geometry, mask, NESZ)
-//                  for both members of F.
+//  k_heights       per pixel: the DEM heights of the centre and of the four
+//                  cardinal neighbours, decided as the exact projection
+//                  would decide them (geo.cuh: dem_sample_cert).
+//  k_main          per pixel: geoid, target ECEF; the reference iteration
+//                  from the model time gives one converged time t*; the set
+//                  F = {t : |delta(t)| < tol} of possible converged times (a
+//                  pair {fb, fb+1}); and the outcome of the reference
+//                  iteration from every member of the left neighbour's F (the
+//                  only seeds the chain can hand it).  Decisions taken on an
+//                  approximate orbit state near a threshold are re-taken on
+//                  the reference's state.
 //  k_scan          per row: a warp walks the columns composing the per-pixel
 //                  outcome maps, selects each pixel's member of F, and runs
 //                  the reference iteration in place for any seed outside the
 //                  precomputed set.
-//  k_select        per pixel: final rasters, counters and Newton histogram.
+//  k_cand          per pixel: the outputs (resampling, Small-2011 geometry,
+//                  mask, NESZ) of the one selected converged time, final
+//                  rasters, counters and Newton histogram; split precision
+//                  defers what FP32 cannot settle to k_resample and k_redo.
 #pragma once
 #include <algorithm>
 #include <limits>
@@ -64,9 +70,12 @@ struct OrbitDev {
 
 // State at integer microsecond t: the table (the reference's Lagrange sums,
 // evaluated once per microsecond) inside its span, the window polynomials
-// outside it, the Lagrange sums directly when neither exists.
-__device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
+// outside it, the Lagrange sums directly when neither exists.  *exact: the
+// state is the reference's Lagrange sums (not the polynomial form).
+__device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq,
+                                        bool *exact = nullptr) {
   const int64_t i = t - o.tab_t0;
+  if (exact) *exact = !(o.poly && !(i >= 0 && i < o.tab_n));
   if (i >= 0 && i < o.tab_n) {
     const double2 *e = o.tab + 5 * i;
     double2 a = __ldg(e), b = __ldg(e + 1), c = __ldg(e + 2), d = __ldg(e + 3), f = __ldg(e + 4);
@@ -81,24 +90,56 @@ __device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState
   return rc;
 }
 
+// The reference's own state at t: the table inside its span, else the
+// Lagrange sums (orbit_eval, the reference's formula).
+__device__ __noinline__ int orbit_exact(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
+  const int64_t i = t - o.tab_t0;
+  if (i >= 0 && i < o.tab_n) return orbit_at(o, t, s, vsq);
+  const int rc = orbit_eval(o.svs, o.n, t, s);
+  if (rc == ORB_OK) *vsq = dot3(s->vel, s->vel);
+  return rc;
+}
+
+// A Newton decision (the |delta| < tol test or the microsecond truncation of
+// the step, 1045-1067) taken on an approximate state (the window polynomials,
+// or a warp's Taylor expansion: within ~2e-8 m and ~2e-11 m/s of the
+// reference's sums, which moves delta by <= ~3e-12 s) is re-taken on the
+// reference's state when it lies within kZdEps of its threshold.
+constexpr double kZdEps = 1e-11;  // s
+__device__ __forceinline__ bool zd_marginal(double d, double tol) {
+  const double ad = fabs(d);
+  const double m = ad * 1e6, fr = m - floor(m);
+  return fabs(ad - tol) <= kZdEps || fr <= kZdEps * 1e6 || fr >= 1.0 - kZdEps * 1e6;
+}
+
 struct ZdRes {
   uint8_t st;
   int64_t t;
   int it;
 };
 
-// solve_zero_doppler (terrain_correction.rs:1010-1073), bit-exact.
+// solve_zero_doppler (terrain_correction.rs:1010-1073), bit-exact: a decision
+// taken on a polynomial state near its threshold is re-taken on the
+// reference's state.
 __device__ ZdRes newton(const OrbitDev &o, V3 P, int64_t seed, int max_iter, double tol) {
   int64_t t = seed;
   for (int i = 0; i < max_iter; ++i) {
     OrbitState s;
     double vsq;
-    if (orbit_at(o, t, &s, &vsq) != ORB_OK) return {ST_ORBIT, t, i};
+    bool exact;
+    if (orbit_at(o, t, &s, &vsq, &exact) != ORB_OK) return {ST_ORBIT, t, i};
     V3 r = sub3(P, s.pos);
     double f = dot3(r, s.vel);
     double fp = -vsq + dot3(r, s.acc);
     if (fabs(fp) < 1.0) return {ST_DEGEN, t, i};
     double delta = -f / fp;
+    if (!exact && zd_marginal(delta, tol) && orbit_exact(o, t, &s, &vsq) == ORB_OK) {
+      r = sub3(P, s.pos);
+      f = dot3(r, s.vel);
+      fp = -vsq + dot3(r, s.acc);
+      if (fabs(fp) < 1.0) return {ST_DEGEN, t, i};
+      delta = -f / fp;
+    }
     if (fabs(delta) < tol) return {ST_CONV, t, i + 1};
     t = t + f2i64(delta * 1e6);
   }
@@ -139,7 +180,7 @@ struct TcDev {
   int flatten, compute_lia, need_geom, resampling, nesz_mask;
   float nesz_factor;
   // per-pixel scratch
-  struct Rec *rec;
+  int64_t *fb;
   uint32_t *cc;
   uint8_t *sel;
   // outputs
@@ -156,8 +197,8 @@ struct TcDev {
   uint64_t row0;               // grid row of the job's first row (row bands)
   const float *hc;             // per pixel: DEM height of the centre (NaN: none), from k_heights
   const float4 *hnb;           // per pixel: heights of the E, W, N, S neighbours (NaN: facet missing)
-  uint32_t *rs_cnt;            // split: per k_main item, FP64 re-samples queued (may exceed RS_CAP)
-  struct RsEnt *rs_ent;        // split: per k_main item, RS_CAP queued re-samples
+  uint32_t *rs_cnt;            // split: per k_cand item (256 px), FP64 re-samples queued (may exceed RS_CAP)
+  struct RsEnt *rs_ent;        // split: per k_cand item, RS_CAP queued re-samples
 };
 
 // ── work table ──────────────────────────────────────────────────────────────
@@ -331,8 +372,6 @@ __global__ void k_row_setup(const TcWork *__restrict__ wp) {
       for (int k = 0; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; ++k) p.counters[k] = 0;
       for (int k = 0; k < 5; ++k) p.flags[k] = 0;
     }
-    if (p.rs_cnt)
-      for (uint64_t b = 0; b < p.bpr; ++b) p.rs_cnt[r * p.bpr + b] = 0;
     const double y = row_y(p, r);
     double lat_seed = y;
     if (p.utm) {
@@ -561,9 +600,9 @@ enum { RD_NONE = 0, RD_FULL = 1, RD_SAMPLE = 2 };
 struct RsEnt {
   double line, sample;  // FP64 image coordinates of the candidate
   float wdiv;           // flattening weight the value is divided by (1: none)
-  uint32_t meta;        // thread of the k_main item (1..255) | member << 8
+  uint32_t thread;      // pixel within the k_cand item (0..255)
 };
-constexpr int RS_CAP = 64;  // queued re-samples per k_main item (beyond: k_redo)
+constexpr int RS_CAP = 64;  // queued re-samples per k_cand item (beyond: k_redo)
 
 __device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, double line, double sample,
                                    float *amag) {
@@ -649,139 +688,6 @@ __device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, doub
   }
   if (amag) *amag = (float)aacc;
   return (float)acc;
-}
-
-// ── both members of F at once ─────────────────────────────────────────────────
-// The two members' image coordinates differ by 1 us of azimuth time (~5e-4
-// line) and nanometres of slant range, so they almost always share their tap
-// window: one pass over the window then feeds both sums, each in the order
-// of its single-candidate sampler.  They return false (nothing done) when
-// the windows differ.
-__device__ bool sample_bicubic_pair(const float *d, uint64_t nl, uint64_t ns, const double *line,
-                                    const double *sample, float *out) {
-  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
-  const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
-  if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
-  double ws0[4], ws1[4];
-  int64_t cols[4];
-  const double ds0 = sample[0] - (double)sf, ds1 = sample[1] - (double)sf;
-  const double dl0 = line[0] - (double)lf, dl1 = line[1] - (double)lf;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    ws0[k] = keys_weight((double)(k - 1) - ds0);
-    ws1[k] = keys_weight((double)(k - 1) - ds1);
-    cols[k] = clampi(sf + k - 1, 0, max_s);
-  }
-  double acc0 = 0.0, acc1 = 0.0;
-#pragma unroll
-  for (int li = -1; li <= 2; ++li) {
-    const int64_t row = clampi(lf + li, 0, max_l);
-    const double wl0 = keys_weight((double)li - dl0), wl1 = keys_weight((double)li - dl1);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const float v = ldf(d, row * (int64_t)ns + cols[k]);
-      if (v != v) {
-        out[0] = out[1] = NAN;
-        return true;
-      }
-      acc0 += (double)v * wl0 * ws0[k];
-      acc1 += (double)v * wl1 * ws1[k];
-    }
-  }
-  out[0] = (float)acc0;
-  out[1] = (float)acc1;
-  return true;
-}
-
-__device__ bool sample_bicubic_pair_f(const float *d, uint64_t nl, uint64_t ns, const double *line,
-                                      const double *sample, float *out, float *amag) {
-  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
-  const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
-  if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
-  float ws0[4], ws1[4], wl0[4], wl1[4];
-  keys4_f(frac_f(sample[0], sf), ws0);
-  keys4_f(frac_f(sample[1], sf), ws1);
-  keys4_f(frac_f(line[0], lf), wl0);
-  keys4_f(frac_f(line[1], lf), wl1);
-  int64_t cols[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) cols[k] = clampi(sf + k - 1, 0, max_s);
-  float acc0 = 0.f, acc1 = 0.f, aac0 = 0.f, aac1 = 0.f;
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int64_t row = clampi(lf + j - 1, 0, max_l);
-    float r0 = 0.f, r1 = 0.f, a0 = 0.f, a1 = 0.f;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const float v = ldf(d, row * (int64_t)ns + cols[k]);
-      if (v != v) {
-        out[0] = out[1] = NAN;
-        return true;
-      }
-      r0 = fmaf(v, ws0[k], r0);
-      r1 = fmaf(v, ws1[k], r1);
-      a0 = fmaf(fabsf(v), fabsf(ws0[k]), a0);
-      a1 = fmaf(fabsf(v), fabsf(ws1[k]), a1);
-    }
-    acc0 = fmaf(r0, wl0[j], acc0);
-    acc1 = fmaf(r1, wl1[j], acc1);
-    aac0 = fmaf(a0, fabsf(wl0[j]), aac0);
-    aac1 = fmaf(a1, fabsf(wl1[j]), aac1);
-  }
-  out[0] = acc0;
-  out[1] = acc1;
-  amag[0] = aac0;
-  amag[1] = aac1;
-  return true;
-}
-
-template <typename T>
-__device__ bool sample_lanczos_pair(const float *d, uint64_t nl, uint64_t ns, const double *line,
-                                    const double *sample, float *out, float *amag) {
-  int64_t max_l = (int64_t)nl - 1, max_s = (int64_t)ns - 1;
-  const int64_t lf = f2i64(floor(line[0])), sf = f2i64(floor(sample[0]));
-  if (f2i64(floor(line[1])) != lf || f2i64(floor(sample[1])) != sf) return false;
-  T wl0[6], ws0[6], wl1[6], ws1[6];
-  lanczos6<T>(line[0] - (double)lf, wl0);
-  lanczos6<T>(sample[0] - (double)sf, ws0);
-  lanczos6<T>(line[1] - (double)lf, wl1);
-  lanczos6<T>(sample[1] - (double)sf, ws1);
-  int64_t cols[6];
-#pragma unroll
-  for (int k = 0; k < 6; ++k) cols[k] = clampi(sf + k - 2, 0, max_s);
-  T acc0 = 0, acc1 = 0, aac0 = 0, aac1 = 0;
-#pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    const int64_t row = clampi(lf + j - 2, 0, max_l);
-    T r0 = 0, r1 = 0, a0 = 0, a1 = 0;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const float v = ldf(d, row * (int64_t)ns + cols[k]);
-      if (v != v) {
-        out[0] = out[1] = NAN;
-        return true;
-      }
-      r0 += (T)v * ws0[k];
-      r1 += (T)v * ws1[k];
-      if (amag) {
-        a0 += fabs((T)v * ws0[k]);
-        a1 += fabs((T)v * ws1[k]);
-      }
-    }
-    acc0 += r0 * wl0[j];
-    acc1 += r1 * wl1[j];
-    if (amag) {
-      aac0 += a0 * fabs(wl0[j]);
-      aac1 += a1 * fabs(wl1[j]);
-    }
-  }
-  out[0] = (float)acc0;
-  out[1] = (float)acc1;
-  if (amag) {
-    amag[0] = (float)aac0;
-    amag[1] = (float)aac1;
-  }
-  return true;
 }
 
 // KDYN: the resampling kernel is read from the job record (batches whose
@@ -988,48 +894,6 @@ __device__ __forceinline__ CandPre cand_geom(const TcDev &p, V3 P, V3 S, int64_t
   return c;
 }
 
-// Resamples both members of F (pre[k] from cand_geom), sharing the tap window
-// when they can; members the pair samplers do not cover go one by one.
-// Split precision samples in FP32 and leaves the error bound in serr for
-// cand_post_f to judge (a few lanes taking an FP64 path here would hold
-// their whole warp).
-template <int KERNEL, bool SPLIT>
-__device__ void resample_members(const TcDev &p, CandPre pre[2], int fmask) {
-  const int kind = KERNEL == KDYN ? p.resampling : KERNEL;
-  bool done = false;
-  if (fmask == 3 && pre[0].inside && pre[1].inside && kind != SD_RESAMPLE_BILINEAR) {
-    const double line[2] = {pre[0].line, pre[1].line}, sample[2] = {pre[0].sample, pre[1].sample};
-    float out[2], amag[2] = {0.f, 0.f};
-    if (kind == SD_RESAMPLE_BICUBIC)
-      done = SPLIT ? sample_bicubic_pair_f(p.img, p.lines, p.samples, line, sample, out, amag)
-                   : sample_bicubic_pair(p.img, p.lines, p.samples, line, sample, out);
-    else
-      done = SPLIT ? sample_lanczos_pair<float>(p.img, p.lines, p.samples, line, sample, out, amag)
-                   : sample_lanczos_pair<double>(p.img, p.lines, p.samples, line, sample, out, nullptr);
-    if (done) {
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        pre[k].sigma0 = out[k];
-        if (SPLIT) pre[k].serr = kSampErr * amag[k];
-        if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
-      }
-    }
-  }
-  if (done) return;
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    if (!((fmask >> k) & 1) || !pre[k].inside) continue;
-    if (SPLIT) {
-      float amag = 0.f;
-      pre[k].sigma0 = resample_f<KERNEL>(p, pre[k].line, pre[k].sample, &amag);
-      pre[k].serr = kSampErr * amag;
-    } else {
-      pre[k].sigma0 = resample<KERNEL>(p, pre[k].line, pre[k].sample);
-    }
-    if (pre[k].sigma0 != pre[k].sigma0) pre[k].inside = false;
-  }
-}
-
 template <int KERNEL, bool SPLIT>
 __device__ CandPre cand_pre(const TcDev &p, V3 P, V3 S, int64_t t) {
   CandPre c = cand_geom(p, P, S, t);
@@ -1229,35 +1093,13 @@ __device__ CandOut cand_fp64(const TcDev &p, const PixGeo &g, V3 S, int64_t t, d
   return cand_post(p, pre, g.P, S, f, flat_area);
 }
 
-template <int KERNEL, bool SPLIT>
-__device__ CandOut cand_full(const TcDev &p, const PixGeo &g, V3 S, int64_t t, double flat_area,
-                             const float *h4) {
-  if (!SPLIT) return cand_fp64<KERNEL>(p, g, S, t, flat_area, h4);
-  CandPre pre = cand_pre<KERNEL, true>(p, g.P, S, t);
-  FacetF f{};
-  if (pre.inside && p.need_geom)
-    f = h4 ? (heights_ok(h4) ? facetf_from(p, g, h4) : FacetF{}) : pixel_facet_f(p, g);
-  int redo;
-  float wd;
-  CandOut o = cand_post_f(p, pre, g, S, f, (float)flat_area, &redo, &wd);
-  return redo != RD_NONE ? cand_fp64<KERNEL>(p, g, S, t, flat_area, h4) : o;
-}
-
 // ── per-pixel stores ─────────────────────────────────────────────────────────
-// Rec: the fixed-point pair F = {fb, fb+1} and the pixel's output for each
-// member.  cc: codes (outcome of the reference iteration seeded at each
-// member of the left neighbour's F), F membership and flags.
-struct __align__(16) Rec {
-  int64_t fb;
-  float data[2];
-  float cos[2];
-  uint8_t omask[2];
-  uint8_t ocls[2];
-  uint32_t pad;
-};
-enum : uint32_t { CF_DEMMISS = 1u << 18, CF_HASF = 1u << 19, CF_HASOUT = 1u << 20,
-                  CF_REDO = 1u << 21 /* split: outputs to be redone in FP64 (k_redo) */,
-                  CF_OUT0 = 1u << 22 /* bits 22-23: members whose outputs Rec holds */ };
+// fb: the base of the fixed-point pair F = {fb, fb+1} (k_main), or the
+// converged time of an exact-path pixel (k_scan).  cc: codes (outcome of the
+// reference iteration seeded at each member of the left neighbour's F), F
+// membership and flags.
+enum : uint32_t { CF_DEMMISS = 1u << 18, CF_HASF = 1u << 19, CF_CODES = 1u << 20 /* F and codes recorded */,
+                  CF_REDO = 1u << 21 /* split: outputs to be redone in FP64 (k_redo) */ };
 // sel byte written by the scan: low 3 bits = outcome, high 4 bits = iterations
 enum : uint8_t { SEL_M0 = 0, SEL_M1 = 1, SEL_DONE = 2, SEL_NONCONV = 3, SEL_DEGEN = 4, SEL_DEMMISS = 5,
                  SEL_ORBIT = 6 };
@@ -1266,10 +1108,18 @@ struct Ent {  // one orbit-table record
   double px, py, pz, vx, vy, vz, ax, ay, az, vsq;
 };
 
-__device__ __forceinline__ int ent_at(const OrbitDev &o, int64_t t, Ent *e) {
+__device__ __forceinline__ int ent_at(const OrbitDev &o, int64_t t, Ent *e, bool *exact = nullptr) {
   OrbitState s;
   double vsq;
-  int rc = orbit_at(o, t, &s, &vsq);
+  int rc = orbit_at(o, t, &s, &vsq, exact);
+  if (rc != ORB_OK) return rc;
+  *e = {s.pos.x, s.pos.y, s.pos.z, s.vel.x, s.vel.y, s.vel.z, s.acc.x, s.acc.y, s.acc.z, vsq};
+  return ORB_OK;
+}
+__device__ __forceinline__ int ent_exact(const OrbitDev &o, int64_t t, Ent *e) {
+  OrbitState s;
+  double vsq;
+  int rc = orbit_exact(o, t, &s, &vsq);
   if (rc != ORB_OK) return rc;
   *e = {s.pos.x, s.pos.y, s.pos.z, s.vel.x, s.vel.y, s.vel.z, s.acc.x, s.acc.y, s.acc.z, vsq};
   return ORB_OK;
@@ -1287,10 +1137,22 @@ __device__ __forceinline__ int zd_eval(V3 P, const Ent &e, double tol, double *d
   return fabs(d) < tol ? 0 : 1;
 }
 
+// zd_eval on *e, re-evaluated on the reference's state at t (which replaces
+// *e; *exact becomes true) when e is approximate and the decision marginal.
+__device__ __forceinline__ int zd_step(const OrbitDev &o, V3 P, Ent *e, bool *exact, int64_t t, double tol,
+                                       double *delta) {
+  int st = zd_eval(P, *e, tol, delta);
+  if (!*exact && st != 2 && zd_marginal(*delta, tol) && ent_exact(o, t, e) == ORB_OK) {
+    *exact = true;
+    st = zd_eval(P, *e, tol, delta);
+  }
+  return st;
+}
+
 struct Slot {  // shared-memory record exchanged with the right-hand neighbour
   int64_t fb;
   int32_t fmask;
-  int32_t pad;
+  int32_t exact;  // bit k: e[k] is the reference's state
   Ent e[2];
 };
 
@@ -1318,6 +1180,7 @@ __global__ void __launch_bounds__(SEL_THREADS, 4) k_heights(const TcWork *__rest
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
     const int jb = find_job(pre, w.n_jobs, item);
     const TcDev &p = w.jobs[jb];
+    if (p.rs_cnt && threadIdx.x == 0) p.rs_cnt[item - pre[jb]] = 0;  // k_cand's queue of this item
     if (!p.hc) continue;
     const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
     if (i >= p.rows * p.cols) continue;
@@ -1407,8 +1270,8 @@ __device__ __forceinline__ void orb_taylor_build(const OrbitDev &o, int64_t uw, 
   T->v3[d] = v[3];
 }
 
-// State at t from the warp's expansion, or from the table.
-__device__ __forceinline__ int ent_lane(const OrbitDev &o, const OrbTaylor &T, int64_t t, Ent *e) {
+// State at t from the warp's expansion (*exact = false), or from the table.
+__device__ __forceinline__ int ent_lane(const OrbitDev &o, const OrbTaylor &T, int64_t t, Ent *e, bool *exact) {
   const int64_t dt = t - T.uw;
   if (T.ok && t > T.lo && t < T.hi && dt <= 20000 && dt >= -20000) {
     const double h = (double)dt * 1e-6;
@@ -1420,14 +1283,17 @@ __device__ __forceinline__ int ent_lane(const OrbitDev &o, const OrbTaylor &T, i
       A[d] = fma(h, fma(h, 3.0 * T.v3[d], 2.0 * T.v2[d]), T.a0[d]);
     }
     *e = {P[0], P[1], P[2], V[0], V[1], V[2], A[0], A[1], A[2], V[0] * V[0] + V[1] * V[1] + V[2] * V[2]};
+    *exact = false;
     return ORB_OK;
   }
-  return ent_at(o, t, e);
+  return ent_at(o, t, e, exact);
 }
 
 // One k_main work item: MAIN_PIX pixels of row r starting at chunk * MAIN_PIX
 // (plus the left neighbour on thread 0).  Every thread of the block calls it.
-template <int KERNEL, bool SPLIT>
+// It records F and the codes only: the outputs of the one member the row
+// walk selects are computed after the walk (k_cand), so this kernel holds no
+// resampling or facet state.
 __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t chunk, Slot *slot,
                                           OrbTaylor *tw) {
   const int tid = threadIdx.x;
@@ -1439,7 +1305,10 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   bool geo_ok = false;
   int fmask = 0;
   int64_t fb = 0;
-  Ent e0{}, e1{};
+  // The pair's orbit states go to this thread's slot as soon as they are
+  // known, so they do not stay live in registers across the block barrier.
+  Slot &my = slot[tid];
+  int exm = 0;  // bit k: my.e[k] is the reference's state
   // The warp's 32 pixels lie within ~10 ms of azimuth time: all lanes take
   // their first Newton step from one shared state (one broadcast read), the
   // landing point is within a few ns of each lane's own root.
@@ -1447,11 +1316,11 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   const uint64_t cq = c < 0 ? 0 : ((uint64_t)c < p.cols ? (uint64_t)c : p.cols - 1);
   const int64_t uw = __shfl_sync(0xffffffffu, predicted_time(p, rr, cq), 16);
   Ent ew;
-  const bool ew_ok = fast && ent_at(p.orb, uw, &ew) == ORB_OK;
+  bool ew_exact = false;
+  const bool ew_ok = fast && ent_at(p.orb, uw, &ew, &ew_exact) == ORB_OK;
   OrbTaylor &T = tw[tid >> 5];
   orb_taylor_build(p.orb, uw, ew, ew_ok, tid & 31, &T);
   __syncwarp();
-  float h4[4] = {NAN, NAN, NAN, NAN};
   if (in_row && r < p.rows) {
     if (p.hc) {  // heights from k_heights
       pixel_lonlat(p, r, (uint64_t)c, &g.lon, &g.lat);
@@ -1465,60 +1334,76 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
       // reference iteration from the shared state: one converged t*
       int64_t t = ew_ok ? uw : predicted_time(p, r, (uint64_t)c);
       Ent e;
+      bool ex = false;
       double d = 0.0;
       int st = 1;
       for (int it = 0; it < 40 && st == 1; ++it) {
-        if (it == 0 && ew_ok) e = ew;
-        else if (ent_lane(p.orb, T, t, &e) != ORB_OK) { st = 3; break; }
-        st = zd_eval(g.P, e, p.tol, &d);
+        if (it == 0 && ew_ok) {
+          e = ew;
+          ex = ew_exact;
+        } else if (ent_lane(p.orb, T, t, &e, &ex) != ORB_OK) {
+          st = 3;
+          break;
+        }
+        st = zd_step(p.orb, g.P, &e, &ex, t, p.tol, &d);
         if (st == 1) t = t + f2i64(d * 1e6);
       }
       if (st == 0) {
         // F = {t : |delta(t)| < tol} lies in {t*-1, t*, t*+1}.  The root sits
         // at t* + d; delta carries ~1e-13 s of rounding noise (the dot
-        // product cancels terms of ~6e9), so for |d| >= 1e-11 s only
-        // t* + sign(d) can join t*, while for smaller |d| both neighbours are
-        // evaluated.  A three-member F is left to the exact path.
-        Ent ea, eb;
-        double da = 0.0, db = 0.0;
-        const int64_t ta = d > 0.0 ? t + 1 : t - 1;   // the likely member
-        const bool ma = ent_lane(p.orb, T, ta, &ea) == ORB_OK && zd_eval(g.P, ea, p.tol, &da) == 0;
+        // product cancels terms of ~6e9) and the states' approximation up to
+        // ~3e-12 s, so for |d| >= 1e-11 s only t* + sign(d) can join t*,
+        // while for smaller |d| both neighbours are evaluated.  A
+        // three-member F is left to the exact path.
+        const int64_t ta = d > 0.0 ? t + 1 : t - 1;  // the likely member
+        const int kt = ta > t ? 0 : 1;                // position of t* in the pair {ta, t*}
+        my.e[kt] = e;
+        int ex_t = ex ? 1 : 0;
+        bool ma;
+        {
+          Ent ea;
+          bool exa = false;
+          double da = 0.0;
+          ma = ent_lane(p.orb, T, ta, &ea, &exa) == ORB_OK && zd_step(p.orb, g.P, &ea, &exa, ta, p.tol, &da) == 0;
+          my.e[1 - kt] = ea;
+          exm = (ex_t << kt) | ((exa ? 1 : 0) << (1 - kt));
+        }
         bool mb = false;
-        const int64_t tb = d > 0.0 ? t - 1 : t + 1;
-        if (fabs(d) < 1e-11) mb = ent_lane(p.orb, T, tb, &eb) == ORB_OK && zd_eval(g.P, eb, p.tol, &db) == 0;
+        if (fabs(d) < 1e-11) {
+          const int64_t tb = d > 0.0 ? t - 1 : t + 1;
+          Ent eb;
+          bool exb = false;
+          double db = 0.0;
+          mb = ent_lane(p.orb, T, tb, &eb, &exb) == ORB_OK && zd_step(p.orb, g.P, &eb, &exb, tb, p.tol, &db) == 0;
+          if (mb && !ma) {  // the pair {t*, tb}: t* moves to the other position
+            my.e[1 - kt] = my.e[kt];
+            my.e[kt] = eb;
+            exm = (ex_t << (1 - kt)) | ((exb ? 1 : 0) << kt);
+          }
+        }
         if (!(ma && mb)) {
-          const bool use_b = mb;                      // pair {t*, tb} when only tb joins
-          const int64_t other = use_b ? tb : ta;
-          const Ent &eo = use_b ? eb : ea;
-          const bool om = use_b ? mb : ma;
-          if (other > t) {
-            fb = t; e0 = e; e1 = eo; fmask = 1 | (om ? 2 : 0);
-          } else {
-            fb = other; e0 = eo; e1 = e; fmask = 2 | (om ? 1 : 0);
+          if (mb) {  // {t*, tb}, tb on the other side of t* than ta
+            fb = kt == 0 ? t - 1 : t;
+            fmask = 3;
+          } else {   // {t*, ta}
+            fb = kt == 0 ? t : ta;
+            fmask = (1 << kt) | (ma ? 1 << (1 - kt) : 0);
           }
         }
       }
     }
   }
-  slot[tid].fb = fb;
-  slot[tid].fmask = fmask;
-  slot[tid].e[0] = e0;
-  slot[tid].e[1] = e1;
+  my.fb = fb;
+  my.fmask = fmask;
+  my.exact = exm;
   __syncthreads();
   if (tid == 0 || !in_row || r >= p.rows) return;
 
   uint32_t cc = 0xFFFFu;
-  Rec rec;
-  rec.fb = fb;
-  rec.pad = 0;
-  rec.data[0] = rec.data[1] = NAN;
-  rec.cos[0] = rec.cos[1] = NAN;
-  rec.omask[0] = rec.omask[1] = SD_MASK_OUTSIDE_FOOTPRINT;
-  rec.ocls[0] = rec.ocls[1] = 2;
   if (!geo_ok) {
     cc |= CF_DEMMISS;
   } else if (fmask) {
-    cc |= CF_HASF | ((uint32_t)fmask << 16);
+    cc |= CF_HASF | CF_CODES | ((uint32_t)fmask << 16);
     // outcome of the reference iteration seeded at each member of the left
     // neighbour's F (the only seeds the row walk can hand this pixel)
     const Slot &L = slot[tid - 1];
@@ -1536,12 +1421,17 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
             break;
           }
           Ent e;
+          bool exact = false;
           bool have = true;
-          if (t == L.fb + k) e = L.e[k];
-          else have = ent_lane(p.orb, T, t, &e) == ORB_OK;
+          if (t == L.fb + k) {
+            e = L.e[k];
+            exact = (L.exact >> k) & 1;
+          } else {
+            have = ent_lane(p.orb, T, t, &e, &exact) == ORB_OK;
+          }
           if (!have) break;  // orbit error: the walk redoes it
           double d;
-          int st = zd_eval(g.P, e, p.tol, &d);
+          int st = zd_step(p.orb, g.P, &e, &exact, t, p.tol, &d);
           if (st == 0) {
             int64_t m = t - fb;
             if ((m == 0 || m == 1) && ((fmask >> m) & 1)) code = (uint32_t)m | ((uint32_t)min(it + 1, 15) << 4);
@@ -1557,114 +1447,21 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
         cc = (cc & ~(0xFFu << (8 * k))) | (code << (8 * k));
       }
     }
-    // Outputs only for the members the row walk can select through the codes
-    // (the left neighbour's F members that converge here); both at a row
-    // start, after a void or when no code converges.  A walk from an
-    // explicit seed that lands on a member without outputs computes it
-    // there (exact_pixel).
-    int outm = fmask;
-    if (c > 0 && L.fmask) {
-      int reach = 0;
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const uint32_t code = (cc >> (8 * k)) & 0xFFu;
-        if (((L.fmask >> k) & 1) && code != 0xFFu && (code & 3u) < 2u) reach |= 1 << (code & 1u);
-      }
-      if (reach & fmask) outm = reach & fmask;
-    }
-    cc |= (uint32_t)outm * CF_OUT0;
-    CandPre pre[2];
-    bool need = false;
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const Ent &e = k == 0 ? e0 : e1;
-      if ((outm >> k) & 1) {
-        pre[k] = cand_geom(p, g.P, V3{e.px, e.py, e.pz}, fb + k);
-      } else {
-        pre[k].inside = false;
-      }
-    }
-    bool defer = false;
-    resample_members<KERNEL, SPLIT>(p, pre, outm);
-    need = pre[0].inside || pre[1].inside;
-    const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
-    if constexpr (SPLIT) {
-      FacetF f{};
-      if (need && p.need_geom) {
-        if (p.hnb) {
-          const float4 q4 = __ldg(p.hnb + i);
-          h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
-          if (heights_ok(h4)) f = facetf_from(p, g, h4);
-        } else if (facet_heights(p, g, h4)) {
-          f = facetf_from(p, g, h4);
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const Ent &e = k == 0 ? e0 : e1;
-        if (!((outm >> k) & 1)) continue;
-        const V3 S{e.px, e.py, e.pz};
-        int redo;
-        float wd;
-        CandOut o = cand_post_f(p, pre[k], g, S, f, (float)flat_area, &redo, &wd);
-        if (redo == RD_SAMPLE) {  // queue the FP64 re-sample in this item's slots
-          const uint64_t item = r * p.bpr + chunk;
-          const uint32_t q = atomicAdd(p.rs_cnt + item, 1u);
-          if (q < (uint32_t)RS_CAP)
-            p.rs_ent[item * RS_CAP + q] = RsEnt{pre[k].line, pre[k].sample, wd, (uint32_t)tid | ((uint32_t)k << 8)};
-          else
-            redo = RD_FULL;
-        }
-        defer = defer || redo == RD_FULL;
-        rec.data[k] = o.data;
-        rec.cos[k] = o.cos;
-        rec.omask[k] = o.mask;
-        rec.ocls[k] = o.cls;
-      }
-    } else {
-      Facet f{};
-      if (need && p.need_geom) {
-        if (p.hnb) {
-          const float4 q4 = __ldg(p.hnb + i);
-          h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
-          if (heights_ok(h4)) f = facet_from(p, g, h4);
-        } else {
-          f = pixel_facet(p, g);
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const Ent &e = k == 0 ? e0 : e1;
-        if (!((outm >> k) & 1)) continue;
-        CandOut o = cand_post(p, pre[k], g.P, V3{e.px, e.py, e.pz}, f, flat_area);
-        rec.data[k] = o.data;
-        rec.cos[k] = o.cos;
-        rec.omask[k] = o.mask;
-        rec.ocls[k] = o.cls;
-      }
-    }
-    cc |= CF_HASOUT;
-    if (defer) {
-      cc |= CF_REDO;
-      atomicAdd(&p.flags[3], 1);
-    }
   }
-  p.rec[i] = rec;
+  p.fb[i] = fb;
   p.cc[i] = cc;
 }
 
 // Single job: the job record is a kernel parameter (constant-bank operands)
 // and the grid covers its rows x bpr items.
-template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main(TcDev p) {
   __shared__ Slot slot[MAIN_THREADS];
   __shared__ OrbTaylor tw[MAIN_THREADS / 32];
-  main_item<KERNEL, SPLIT>(p, blockIdx.x / p.bpr, blockIdx.x % p.bpr, slot, tw);
+  main_item(p, blockIdx.x / p.bpr, blockIdx.x % p.bpr, slot, tw);
 }
 
 // Tile batches: persistent CTAs over the work table; the current job's
 // record is staged in shared memory.
-template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const TcWork *__restrict__ wp) {
   __shared__ Slot slot[MAIN_THREADS];
   __shared__ __align__(16) unsigned char s_job[sizeof(TcDev)];
@@ -1687,133 +1484,7 @@ __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const
       cur = jb;
     }
     const uint64_t li = item - pre[jb];
-    main_item<KERNEL, SPLIT>(p, li / p.bpr, li % p.bpr, slot, tw);
-  }
-}
-
-// ── k_resample (split precision): FP64 values of the queued candidates ────────
-// k_main queues a candidate (RD_SAMPLE) whose geometry, masks and flattening
-// weight FP32 settled but whose resampling sum cancelled past its error
-// bound.  One warp per k_main item, one lane per queued candidate: the FP64
-// sampler, the flattening division and the NESZ test of cand_post; a NESZ
-// test within its margin sends the pixel to k_redo instead.
-template <int KERNEL>
-__global__ void __launch_bounds__(SEL_THREADS) k_resample(const TcWork *__restrict__ wp) {
-  const TcWork w = *wp;
-  const uint64_t *pre = stage_pre(w, WK_MAIN);
-  const uint64_t total = pre[w.n_jobs];
-  const int lane = threadIdx.x & 31;
-  const uint64_t nwarps = (uint64_t)gridDim.x * (SEL_THREADS / 32);
-  for (uint64_t item = (uint64_t)blockIdx.x * (SEL_THREADS / 32) + (threadIdx.x >> 5); item < total;
-       item += nwarps) {
-    const int jb = find_job(pre, w.n_jobs, item);
-    const TcDev &p = w.jobs[jb];
-    if (!p.rs_cnt) continue;
-    const uint64_t li = item - pre[jb];
-    const uint32_t n = min(p.rs_cnt[li], (uint32_t)RS_CAP);
-    if (n == 0) continue;
-    const uint64_t r = li / p.bpr, chunk = li % p.bpr;
-    for (uint32_t q = lane; q < n; q += 32) {
-      const RsEnt e = p.rs_ent[li * RS_CAP + q];
-      const uint64_t c = chunk * MAIN_PIX + (e.meta & 0xFFu) - 1;
-      const int k = (int)(e.meta >> 8);
-      const uint64_t i = r * p.cols + c;
-      Rec &rec = p.rec[i];
-      float sigma0 = resample<KERNEL>(p, e.line, e.sample);
-      if (sigma0 != sigma0) {
-        rec.data[k] = NAN;
-        rec.cos[k] = NAN;
-        rec.omask[k] = SD_MASK_OUTSIDE_FOOTPRINT;
-        rec.ocls[k] = 2;
-        continue;
-      }
-      sigma0 /= e.wdiv;
-      uint8_t m = SD_MASK_VALID, cls = 0;
-      if (p.nesz_mask) {
-        const float nz = sample_bilinear(p.nesz, p.lines, p.samples, e.line, e.sample);
-        if (nz == nz) {
-          const float thr = nz * p.nesz_factor;
-          if (fabsf(sigma0 - thr) <= 1e-5f * fabsf(thr)) {
-            atomicOr(p.cc + i, (uint32_t)CF_REDO);
-            atomicAdd(&p.flags[3], 1);
-            continue;
-          }
-          if (sigma0 <= thr) {
-            sigma0 = NAN;
-            m = SD_MASK_NOISE_MASKED;
-            cls = 6;
-          }
-        }
-      }
-      rec.data[k] = sigma0;
-      rec.omask[k] = m;
-      rec.ocls[k] = cls;
-    }
-    if (lane == 0) atomicAdd(&p.flags[4], (int)n);
-  }
-}
-
-// ── k_redo (split precision): FP64 outputs for the flagged pixels ──────────
-// Pixels with a mask decision inside its FP32 margin (or more queued
-// re-samples than their item holds) get both members of F recomputed with
-// the FP64 candidate here, outside k_main's warps; flags[3] counts them.
-template <int KERNEL>
-__global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__ wp) {
-  // flagged pixels are sparse: each block first compacts the flagged pixels
-  // of a REDO_CHUNK into shared memory, then runs them densely
-  __shared__ uint16_t list[REDO_CHUNK];
-  __shared__ int n_list;
-  const TcWork w = *wp;
-  const uint64_t *pre = stage_pre(w, WK_REDO);
-  const uint64_t total = pre[w.n_jobs];
-  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    const int jb = find_job(pre, w.n_jobs, item);
-    const TcDev &p = w.jobs[jb];
-    if (p.flags[3] == 0) continue;  // nothing flagged in this job (uniform over the block)
-    const uint64_t npx = p.rows * p.cols;
-    const uint64_t base = (item - pre[jb]) * REDO_CHUNK;
-    __syncthreads();  // the previous item is done with the list
-    if (threadIdx.x == 0) n_list = 0;
-    __syncthreads();
-    for (int k = 0; k < REDO_CHUNK / SEL_THREADS; ++k) {
-      const uint64_t i = base + (uint64_t)k * SEL_THREADS + threadIdx.x;
-      if (i < npx && (p.cc[i] & CF_REDO)) list[atomicAdd(&n_list, 1)] = (uint16_t)(i - base);
-    }
-    __syncthreads();
-    const int n = n_list;
-    if (n > 0 && threadIdx.x == 0) atomicAdd(&p.flags[2], n);
-    for (int q = threadIdx.x; q < n; q += SEL_THREADS) {
-      const uint64_t i = base + list[q];
-      const uint32_t cc = p.cc[i];
-      const uint64_t r = i / p.cols, c = i % p.cols;
-      PixGeo g;
-      float h4[4] = {NAN, NAN, NAN, NAN};
-      const float *hp = nullptr;
-      if (p.hc) {
-        pixel_lonlat(p, r, c, &g.lon, &g.lat);
-        pixel_ecef(p, &g, p.hc[i]);
-        const float4 q4 = p.hnb[i];
-        h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
-        hp = h4;
-      } else if (!pixel_geo(p, r, c, &g)) {
-        continue;
-      }
-      Rec rec = p.rec[i];
-      const int outm = (int)((cc >> 22) & 3u);  // members k_main gave outputs
-      const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
-      for (int k = 0; k < 2; ++k) {
-        if (!((outm >> k) & 1)) continue;
-        OrbitState os;
-        double vsq;
-        if (orbit_at(p.orb, rec.fb + k, &os, &vsq) != ORB_OK) continue;
-        const CandOut o = cand_fp64<KERNEL>(p, g, os.pos, rec.fb + k, flat_area, hp);
-        rec.data[k] = o.data;
-        rec.cos[k] = o.cos;
-        rec.omask[k] = o.mask;
-        rec.ocls[k] = o.cls;
-      }
-      p.rec[i] = rec;
-    }
+    main_item(p, li / p.bpr, li % p.bpr, slot, tw);
   }
 }
 
@@ -1828,9 +1499,10 @@ struct WState {
 };
 
 // The reference solve of pixel (r, c) from seed s, for pixels the
-// precomputed records do not cover.  With `write`, it also stores the
-// pixel's outputs when the converged time has none precomputed.
-template <int KERNEL, bool SPLIT>
+// precomputed records do not cover.  A converged time that is not a member
+// of the pixel's F is selected as SEL_DONE and, with `write`, stored in fb
+// (nothing reads that pixel's F afterwards: the walk leaves it with an
+// explicit seed).
 __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s, uint32_t cc, int64_t fb,
                               bool write, uint8_t *sel) {
   const uint64_t i = r * p.cols + c;
@@ -1850,21 +1522,10 @@ __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s,
     return {1, s};
   }
   const int it = z.it > 15 ? 15 : z.it;
-  if (cc & CF_HASOUT) {
+  if (cc & CF_CODES) {
     const uint32_t fm = (cc >> 16) & 3u;
     const int64_t m = z.t - fb;
     if ((m == 0 || m == 1) && ((fm >> m) & 1)) {
-      if (write && !((cc >> (22 + m)) & 1u)) {  // k_main left this member's outputs out
-        OrbitState os;
-        double vsq;
-        orbit_at(p.orb, z.t, &os, &vsq);
-        const CandOut o = cand_full<KERNEL, SPLIT>(p, g, os.pos, z.t, p.need_geom ? p.row_flat[r] : 0.0, nullptr);
-        Rec &rc = p.rec[i];
-        rc.data[m] = o.data;
-        rc.cos[m] = o.cos;
-        rc.omask[m] = o.mask;
-        rc.ocls[m] = o.cls;
-      }
       *sel = (uint8_t)(m | (it << 4));
       return {0, m};
     }
@@ -1872,24 +1533,13 @@ __device__ WState exact_pixel(const TcDev &p, uint64_t r, uint64_t c, int64_t s,
   *sel = (uint8_t)(SEL_DONE | (it << 4));
   if (write) {
     atomicAdd(&p.flags[1], 1);
-    OrbitState os;
-    double vsq;
-    orbit_at(p.orb, z.t, &os, &vsq);
-    CandOut o = cand_full<KERNEL, SPLIT>(p, g, os.pos, z.t, p.need_geom ? p.row_flat[r] : 0.0, nullptr);
-    p.out[i] = o.data;
-    if (p.compute_lia) {
-      p.cos_lia[i] = o.cos;
-      p.mask[i] = o.mask;
-    }
-    if (p.az_time) p.az_time[i] = z.t;
-    p.rec[i].ocls[0] = o.cls;
+    p.fb[i] = z.t;
   }
   return {1, z.t};
 }
 
 // Walk columns [b, e) of row r from state st (terrain_correction.rs:
 // 1443-1580), any pixel kind.  fb is read only where a seed value is needed.
-template <int KERNEL, bool SPLIT>
 __device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, WState st, bool write) {
   const uint64_t base = r * p.cols;
   uint32_t prev_cc = b > 0 ? p.cc[base + b - 1] : CF_DEMMISS;
@@ -1898,20 +1548,20 @@ __device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, W
     const uint32_t cc = p.cc[base + c];
     uint8_t sel;
     if (cc & CF_DEMMISS) {
-      if (st.kind == 0) st = {1, p.rec[base + c - 1].fb + st.v};  // the seed passes through the void
+      if (st.kind == 0) st = {1, p.fb[base + c - 1] + st.v};  // the seed passes through the void
       sel = SEL_DEMMISS;
     } else {
       uint32_t code = 0xFF;
-      if (st.kind == 0 && (prev_cc & CF_HASF) && (cc & CF_HASOUT)) code = (cc >> (8 * st.v)) & 0xFFu;
+      if (st.kind == 0 && (prev_cc & CF_HASF) && (cc & CF_CODES)) code = (cc >> (8 * st.v)) & 0xFFu;
       if (code != 0xFF && (code & 3u) != 3u) {
         st = {0, (int64_t)(code & 3u)};
         sel = (uint8_t)((code & 3u) | (code & 0xF0u));
       } else if (code != 0xFF) {
-        st = {1, p.rec[base + c - 1].fb + st.v};  // not converged: seed unchanged
+        st = {1, p.fb[base + c - 1] + st.v};  // not converged: seed unchanged
         sel = (uint8_t)((((code >> 2) & 3u) == 1u ? SEL_NONCONV : SEL_DEGEN) | (code & 0xF0u));
       } else {
-        const int64_t s = st.kind == 0 ? p.rec[base + c - 1].fb + st.v : st.v;
-        st = exact_pixel<KERNEL, SPLIT>(p, r, c, s, cc, p.rec[base + c].fb, write, &sel);
+        const int64_t s = st.kind == 0 ? p.fb[base + c - 1] + st.v : st.v;
+        st = exact_pixel(p, r, c, s, cc, p.fb[base + c], write, &sel);
       }
     }
     if (write) p.sel[base + c] = sel;
@@ -1931,7 +1581,6 @@ __device__ WState walk_seg(const TcDev &p, uint64_t r, uint64_t b, uint64_t e, W
 // kind is (re)done by walk_seg.
 constexpr int SCAN_WARPS = 4;
 
-template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restrict__ wp) {
   __shared__ uint32_t sbuf[SCAN_WARPS][32][33];
   __shared__ __align__(16) unsigned char s_job[SCAN_WARPS][sizeof(TcDev)];
@@ -1964,7 +1613,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
       ++c;
     }
     if (c < n) {
-      st0 = walk_seg<KERNEL, SPLIT>(p, r, c, c + 1, WState{1, p.row_guess[r]}, true);
+      st0 = walk_seg(p, r, c, c + 1, WState{1, p.row_guess[r]}, true);
       c0 = c + 1;
     }
   }
@@ -1994,7 +1643,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
     const int cnt = b + 32 * (uint64_t)k < e ? (int)min((uint64_t)32, e - b - 32 * (uint64_t)k) : 0;
     for (int t = 0; t < cnt; ++t) {
       const uint32_t w = buf[lane][t];
-      if ((w & (CF_DEMMISS | CF_HASOUT)) != CF_HASOUT) bad = 3;
+      if ((w & (CF_DEMMISS | CF_CODES)) != CF_CODES) bad = 3;
       const uint32_t x0 = (w >> (8 * s0)) & 0xFFu, x1 = (w >> (8 * s1)) & 0xFFu;
       if (x0 == 0xFFu || (x0 & 3u) == 3u) bad |= 1;
       if (x1 == 0xFFu || (x1 & 3u) == 3u) bad |= 2;
@@ -2005,8 +1654,8 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
   }
   WState ex0 = {0, 0}, ex1 = {0, 1};
   if (b < e) {
-    ex0 = (bad & 1) ? walk_seg<KERNEL, SPLIT>(p, r, b, e, WState{0, 0}, false) : WState{0, s0};
-    ex1 = (bad & 2) ? walk_seg<KERNEL, SPLIT>(p, r, b, e, WState{0, 1}, false) : WState{0, s1};
+    ex0 = (bad & 1) ? walk_seg(p, r, b, e, WState{0, 0}, false) : WState{0, s0};
+    ex1 = (bad & 2) ? walk_seg(p, r, b, e, WState{0, 1}, false) : WState{0, s1};
   }
   // phase 2: compose the lanes' maps in order
   WState st = st0, entry{2, 0};
@@ -2016,7 +1665,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
       entry = st;
       if (b < e) {
         if (st.kind == 0) nx = st.v == 0 ? ex0 : ex1;
-        else nx = walk_seg<KERNEL, SPLIT>(p, r, b, e, st, false);
+        else nx = walk_seg(p, r, b, e, st, false);
       }
     }
     st.kind = __shfl_sync(0xffffffffu, nx.kind, j);
@@ -2050,58 +1699,260 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
     }
     __syncwarp();
   }
-  if (b < e && !regular) walk_seg<KERNEL, SPLIT>(p, r, b, e, entry, true);
+  if (b < e && !regular) walk_seg(p, r, b, e, entry, true);
   }
 }
 
-// ── K5: final rasters, counters and Newton histogram ────────────────────────
-__global__ void __launch_bounds__(SEL_THREADS) k_select(const TcWork *__restrict__ wp) {
+// ── K5: outputs of the selected member, rasters, counters, histogram ───────
+// After the walk every pixel with a converged time has exactly one: fb +
+// member (SEL_M0/SEL_M1) or fb itself (an exact-path pixel).  One thread per
+// pixel recomputes the pixel's geometry (lon/lat, the DEM heights k_heights
+// left, geoid, target ECEF), reads the satellite position at that time from
+// the orbit table (the reference's own sums, so the slant range and image
+// coordinates are the reference's) and forms the reference's outputs (1585-1739:
+// resampling, facet, flattening, masks, NESZ).  Split precision: a candidate
+// FP32 cannot settle is queued for an FP64 re-sample (RD_SAMPLE, k_resample)
+// or flagged for the FP64 candidate (RD_FULL, k_redo), which write and count
+// it instead.
+#ifndef SD_CAND_MINB
+#define SD_CAND_MINB 2  // blocks of 256 per SM the register budget is cut for
+#endif
+
+__device__ __forceinline__ void pixel_from_heights(const TcDev &p, uint64_t i, uint64_t r, uint64_t c, PixGeo *g,
+                                                   float h4[4], bool *ok) {
+  if (p.hc) {
+    pixel_lonlat(p, r, c, &g->lon, &g->lat);
+    const float hf = __ldg(p.hc + i);
+    *ok = isfinite(hf);
+    if (*ok) pixel_ecef(p, g, hf);
+    if (p.need_geom) {
+      const float4 q4 = __ldg(p.hnb + i);
+      h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
+    }
+  } else {
+    *ok = pixel_geo(p, r, c, g);
+    if (*ok && p.need_geom && !facet_heights(p, *g, h4)) h4[0] = h4[1] = h4[2] = h4[3] = NAN;
+  }
+}
+
+template <int KERNEL, bool SPLIT>
+__global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork *__restrict__ wp) {
   __shared__ unsigned int s_cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
   const TcWork w = *wp;
   const uint64_t *pre = stage_pre(w, WK_SEL);
   const uint64_t total = pre[w.n_jobs];
+  const int tid = threadIdx.x;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
     const int jb = find_job(pre, w.n_jobs, item);
     const TcDev &p = w.jobs[jb];
     __syncthreads();  // the previous item's flush is done
-    for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
+    for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
     __syncthreads();
     const uint64_t npx = p.rows * p.cols;
-    const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
-    if (i < npx) {
-      const uint8_t sel = p.sel[i];
-      const int code = sel & 7, it = sel >> 4;
-      int counter = -1;
-      if (code == SEL_M0 || code == SEL_M1) {
-        const Rec &rc = p.rec[i];
-        counter = rc.ocls[code];
-        atomicAdd(&s_cnt[kCounters + it], 1u);
-        p.out[i] = rc.data[code];
-        if (p.compute_lia) {
-          p.cos_lia[i] = rc.cos[code];
-          p.mask[i] = rc.omask[code];
-        }
-        if (p.az_time) p.az_time[i] = rc.fb + code;
-      } else if (code == SEL_DONE) {
-        counter = p.rec[i].ocls[0];
-        atomicAdd(&s_cnt[kCounters + it], 1u);
-      } else if (code != SEL_ORBIT) {
-        uint8_t m = code == SEL_NONCONV ? SD_MASK_NON_CONVERGED
-                    : code == SEL_DEGEN ? SD_MASK_DEGENERATE_GEOMETRY
-                                        : SD_MASK_DEM_MISSING;
-        counter = code == SEL_NONCONV ? 3 : (code == SEL_DEGEN ? 4 : 1);
-        if (p.az_time) p.az_time[i] = INT64_MIN;
-        p.out[i] = NAN;
-        if (p.compute_lia) {
-          p.cos_lia[i] = NAN;
-          p.mask[i] = m;
+    const uint64_t li = item - pre[jb];
+    const uint64_t i = li * SEL_THREADS + tid;
+    const uint8_t sel = i < npx ? p.sel[i] : (uint8_t)SEL_ORBIT;
+    const int code = sel & 7, it = sel >> 4;
+    const bool has_t = code == SEL_M0 || code == SEL_M1 || code == SEL_DONE;
+    const int64_t t = has_t ? p.fb[i] + (code == SEL_M1 ? 1 : 0) : 0;
+    int counter = -1;
+    if (has_t) {
+      atomicAdd(&s_cnt[kCounters + it], 1u);
+      const uint64_t r = i / p.cols, c = i % p.cols;
+      PixGeo g;
+      float h4[4] = {NAN, NAN, NAN, NAN};
+      bool ok;
+      pixel_from_heights(p, i, r, c, &g, h4, &ok);
+      OrbitState os;
+      double vsq;
+      const bool orb_ok = ok && orbit_exact(p.orb, t, &os, &vsq) == ORB_OK;
+      if (!orb_ok) atomicOr(&p.flags[0], ok ? 1 : 2);  // cannot happen for a converged time
+      CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
+      bool deferred = false;
+      if (orb_ok) {
+        const V3 S = os.pos;
+        const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+        if constexpr (SPLIT) {
+          const CandPre cp = cand_pre<KERNEL, true>(p, g.P, S, t);
+          FacetF f{};
+          if (cp.inside && p.need_geom && heights_ok(h4)) f = facetf_from(p, g, h4);
+          int redo;
+          float wd = 1.f;
+          o = cand_post_f(p, cp, g, S, f, (float)flat_area, &redo, &wd);
+          if (redo == RD_SAMPLE) {  // queue the FP64 re-sample in this item's slots
+            const uint32_t q = atomicAdd(p.rs_cnt + li, 1u);
+            if (q < (uint32_t)RS_CAP) {
+              p.rs_ent[li * RS_CAP + q] = RsEnt{cp.line, cp.sample, wd, (uint32_t)tid};
+              if (p.compute_lia) p.cos_lia[i] = o.cos;
+              deferred = true;
+            } else {
+              redo = RD_FULL;
+            }
+          }
+          if (redo == RD_FULL) {
+            p.cc[i] |= CF_REDO;
+            atomicAdd(&p.flags[3], 1);
+            deferred = true;
+          }
+        } else {
+          const CandPre cp = cand_pre<KERNEL, false>(p, g.P, S, t);
+          Facet f{};
+          if (cp.inside && p.need_geom && heights_ok(h4)) f = facet_from(p, g, h4);
+          o = cand_post(p, cp, g.P, S, f, flat_area);
         }
       }
-      if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
+      if (!deferred) {
+        p.out[i] = o.data;
+        if (p.compute_lia) {
+          p.cos_lia[i] = o.cos;
+          p.mask[i] = o.mask;
+        }
+        counter = o.cls;
+      }
+      if (p.az_time) p.az_time[i] = t;
+    } else if (i < npx && code != SEL_ORBIT) {
+      const uint8_t m = code == SEL_NONCONV ? SD_MASK_NON_CONVERGED
+                        : code == SEL_DEGEN ? SD_MASK_DEGENERATE_GEOMETRY
+                                            : SD_MASK_DEM_MISSING;
+      counter = code == SEL_NONCONV ? 3 : (code == SEL_DEGEN ? 4 : 1);
+      if (p.az_time) p.az_time[i] = INT64_MIN;
+      p.out[i] = NAN;
+      if (p.compute_lia) {
+        p.cos_lia[i] = NAN;
+        p.mask[i] = m;
+      }
+    }
+    if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
+    __syncthreads();
+    for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
+      if (s_cnt[k]) atomicAdd(&p.counters[k], (unsigned long long)s_cnt[k]);
+  }
+}
+
+// ── k_resample (split precision): FP64 values of the queued candidates ────────
+// k_cand queues a candidate (RD_SAMPLE) whose geometry, masks and flattening
+// weight FP32 settled but whose resampling sum cancelled past its error
+// bound.  One warp per k_cand item, one lane per queued candidate: the FP64
+// sampler, the flattening division and the NESZ test of cand_post; a NESZ
+// test within its margin sends the pixel to k_redo instead.  Counters are
+// added per warp.
+template <int KERNEL>
+__global__ void __launch_bounds__(SEL_THREADS) k_resample(const TcWork *__restrict__ wp) {
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_SEL);
+  const uint64_t total = pre[w.n_jobs];
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (SEL_THREADS / 32);
+  for (uint64_t item = (uint64_t)blockIdx.x * (SEL_THREADS / 32) + (threadIdx.x >> 5); item < total;
+       item += nwarps) {
+    const int jb = find_job(pre, w.n_jobs, item);
+    const TcDev &p = w.jobs[jb];
+    if (!p.rs_cnt) continue;
+    const uint64_t li = item - pre[jb];
+    const uint32_t n = min(p.rs_cnt[li], (uint32_t)RS_CAP);
+    if (n == 0) continue;
+    for (uint32_t q0 = 0; q0 < n; q0 += 32) {  // warp-uniform: the ballots below
+      const uint32_t q = q0 + lane;
+      int cls = -1;
+      if (q < n) {
+        const RsEnt e = p.rs_ent[li * RS_CAP + q];
+        const uint64_t i = li * SEL_THREADS + e.thread;
+        float sigma0 = resample<KERNEL>(p, e.line, e.sample);
+        uint8_t m = SD_MASK_VALID;
+        cls = 0;
+        if (sigma0 != sigma0) {
+          m = SD_MASK_OUTSIDE_FOOTPRINT;
+          cls = 2;
+          if (p.compute_lia) p.cos_lia[i] = NAN;
+        } else {
+          sigma0 /= e.wdiv;
+          if (p.nesz_mask) {
+            const float nz = sample_bilinear(p.nesz, p.lines, p.samples, e.line, e.sample);
+            if (nz == nz) {
+              const float thr = nz * p.nesz_factor;
+              if (fabsf(sigma0 - thr) <= 1e-5f * fabsf(thr)) {
+                atomicOr(p.cc + i, (uint32_t)CF_REDO);
+                atomicAdd(&p.flags[3], 1);
+                cls = -1;
+              } else if (sigma0 <= thr) {
+                sigma0 = NAN;
+                m = SD_MASK_NOISE_MASKED;
+                cls = 6;
+              }
+            }
+          }
+        }
+        if (cls >= 0) {
+          p.out[i] = sigma0;
+          if (p.compute_lia) p.mask[i] = m;
+        }
+      }
+      const int n0 = __popc(__ballot_sync(0xffffffffu, cls == 0));
+      const int n2 = __popc(__ballot_sync(0xffffffffu, cls == 2));
+      const int n6 = __popc(__ballot_sync(0xffffffffu, cls == 6));
+      if (lane == 0) {
+        if (n0) atomicAdd(&p.counters[0], (unsigned long long)n0);
+        if (n2) atomicAdd(&p.counters[2], (unsigned long long)n2);
+        if (n6) atomicAdd(&p.counters[6], (unsigned long long)n6);
+      }
+    }
+    if (lane == 0) atomicAdd(&p.flags[4], (int)n);
+  }
+}
+
+// ── k_redo (split precision): FP64 outputs for the flagged pixels ──────────
+// Pixels with a mask decision inside its FP32 margin (or more queued
+// re-samples than their item holds) get the FP64 candidate of their
+// selected member here, outside k_cand's warps; flags[2] counts them.
+template <int KERNEL>
+__global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__ wp) {
+  // flagged pixels are sparse: each block first compacts the flagged pixels
+  // of a REDO_CHUNK into shared memory, then runs them densely
+  __shared__ uint16_t list[REDO_CHUNK];
+  __shared__ int n_list;
+  const TcWork w = *wp;
+  const uint64_t *pre = stage_pre(w, WK_REDO);
+  const uint64_t total = pre[w.n_jobs];
+  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
+    const int jb = find_job(pre, w.n_jobs, item);
+    const TcDev &p = w.jobs[jb];
+    if (p.flags[3] == 0) continue;  // nothing flagged in this job (uniform over the block)
+    const uint64_t npx = p.rows * p.cols;
+    const uint64_t base = (item - pre[jb]) * REDO_CHUNK;
+    __syncthreads();  // the previous item is done with the list
+    if (threadIdx.x == 0) n_list = 0;
+    __syncthreads();
+    for (int k = 0; k < REDO_CHUNK / SEL_THREADS; ++k) {
+      const uint64_t i = base + (uint64_t)k * SEL_THREADS + threadIdx.x;
+      if (i < npx && (p.cc[i] & CF_REDO)) list[atomicAdd(&n_list, 1)] = (uint16_t)(i - base);
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
-      if (s_cnt[k]) atomicAdd(&p.counters[k], (unsigned long long)s_cnt[k]);
+    const int n = n_list;
+    if (n > 0 && threadIdx.x == 0) atomicAdd(&p.flags[2], n);
+    for (int q = threadIdx.x; q < n; q += SEL_THREADS) {
+      const uint64_t i = base + list[q];
+      const uint64_t r = i / p.cols, c = i % p.cols;
+      const int code = p.sel[i] & 7;
+      const int64_t t = p.fb[i] + (code == SEL_M1 ? 1 : 0);
+      PixGeo g;
+      float h4[4] = {NAN, NAN, NAN, NAN};
+      bool ok;
+      pixel_from_heights(p, i, r, c, &g, h4, &ok);
+      OrbitState os;
+      double vsq;
+      if (!ok || orbit_exact(p.orb, t, &os, &vsq) != ORB_OK) {
+        atomicOr(&p.flags[0], 2);
+        continue;
+      }
+      const CandOut o = cand_fp64<KERNEL>(p, g, os.pos, t, p.need_geom ? p.row_flat[r] : 0.0,
+                                          p.need_geom ? h4 : nullptr);
+      p.out[i] = o.data;
+      if (p.compute_lia) {
+        p.cos_lia[i] = o.cos;
+        p.mask[i] = o.mask;
+      }
+      atomicAdd(&p.counters[o.cls], 1ull);
+    }
   }
 }
 
@@ -2194,45 +2045,48 @@ int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
 }
 
 // job: the single job's record (parameter form of k_main), or null for the
-// persistent work-table form.
+// persistent work-table form.  Stages: k_main (F and codes), k_scan (the row
+// walk), k_cand (outputs of the selected members), and in split precision
+// k_resample and k_redo (the candidates FP32 could not settle).
 template <int K, bool S>
-int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const char *name,
-                    const TcDev *job, bool with_main = true) {
+int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const TcDev *job,
+                    bool with_main = true) {
   cudaStream_t st = ctx->stream;
   if (with_main) {
-  SD_TIMED_BEGIN(ctx, name);
-  if (job) {
-    if (totals[WK_MAIN] > 0x7FFFFFFFull)
-      return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "output grid too large");
-    k_main<K, S><<<(unsigned)std::max<uint64_t>(totals[WK_MAIN], 1), MAIN_THREADS, 0, st>>>(*job);
-  } else {
-    unsigned g = persistent_grid(k_main_batch<K, S>, MAIN_THREADS, 0, totals[WK_MAIN]);
-    if (ctx->main_cps > 0) {
-      int dev = 0, sms = 1;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      g = std::min<unsigned>(g, (unsigned)(ctx->main_cps * sms));
+    if (job) {
+      if (totals[WK_MAIN] > 0x7FFFFFFFull)
+        return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "output grid too large");
+      SD_TIMED_BEGIN(ctx, "k_main");
+      k_main<<<(unsigned)std::max<uint64_t>(totals[WK_MAIN], 1), MAIN_THREADS, 0, st>>>(*job);
+    } else {
+      unsigned g = persistent_grid(k_main_batch, MAIN_THREADS, 0, totals[WK_MAIN]);
+      if (ctx->main_cps > 0) {
+        int dev = 0, sms = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g = std::min<unsigned>(g, (unsigned)(ctx->main_cps * sms));
+      }
+      SD_TIMED_BEGIN(ctx, "k_main_batch");
+      k_main_batch<<<g, MAIN_THREADS, 0, st>>>(d_work);
     }
-    k_main_batch<K, S><<<g, MAIN_THREADS, 0, st>>>(d_work);
+    SD_LAUNCHED(ctx);
   }
+  SD_TIMED_BEGIN(ctx, "k_scan");
+  k_scan<<<persistent_grid(k_scan, SCAN_WARPS * 32, 0, blocks_for(totals[WK_SCAN], SCAN_WARPS)),
+           SCAN_WARPS * 32, 0, st>>>(d_work);
   SD_LAUNCHED(ctx);
-  }
+  SD_TIMED_BEGIN(ctx, S ? "k_cand<SPLIT>" : "k_cand");
+  k_cand<K, S><<<persistent_grid(k_cand<K, S>, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
+  SD_LAUNCHED(ctx);
   if (S) {
     SD_TIMED_BEGIN(ctx, "k_resample");
-    k_resample<K><<<persistent_grid(k_resample<K>, SEL_THREADS, 0, blocks_for(totals[WK_MAIN], SEL_THREADS / 32)),
+    k_resample<K><<<persistent_grid(k_resample<K>, SEL_THREADS, 0, blocks_for(totals[WK_SEL], SEL_THREADS / 32)),
                     SEL_THREADS, 0, st>>>(d_work);
     SD_LAUNCHED(ctx);
     SD_TIMED_BEGIN(ctx, "k_redo");
     k_redo<K><<<persistent_grid(k_redo<K>, SEL_THREADS, 0, totals[WK_REDO]), SEL_THREADS, 0, st>>>(d_work);
     SD_LAUNCHED(ctx);
   }
-  SD_TIMED_BEGIN(ctx, "k_scan");
-  k_scan<K, S><<<persistent_grid(k_scan<K, S>, SCAN_WARPS * 32, 0, blocks_for(totals[WK_SCAN], SCAN_WARPS)),
-                 SCAN_WARPS * 32, 0, st>>>(d_work);
-  SD_LAUNCHED(ctx);
-  SD_TIMED_BEGIN(ctx, "k_select");
-  k_select<<<persistent_grid(k_select, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
-  SD_LAUNCHED(ctx);
   return SD_OK;
 }
 

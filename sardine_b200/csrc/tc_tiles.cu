@@ -12,11 +12,11 @@ namespace sd {
 namespace {
 
 // Tile batches: the persistent work-table kernels; the resampler is read
-// per job.  with_main false: k_scan and k_select only (k_main ran per tile).
+// per job.  with_main false: the stages after k_main only (k_main ran per tile).
 int launch_pixels_batch(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, bool split,
                         bool with_main = true) {
-  return split ? launch_pixels_t<KDYN, true>(ctx, d_work, totals, "k_main_batch<SPLIT>", nullptr, with_main)
-               : launch_pixels_t<KDYN, false>(ctx, d_work, totals, "k_main_batch", nullptr, with_main);
+  return split ? launch_pixels_t<KDYN, true>(ctx, d_work, totals, nullptr, with_main)
+               : launch_pixels_t<KDYN, false>(ctx, d_work, totals, nullptr, with_main);
 }
 
 // k_main per tile in its parameter form (job record in the kernel's
@@ -397,7 +397,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     return o;
   };
   struct Offs {
-    size_t guess, flat, knots, alon, alat, aloc, hc, hnb, rec, cc, sel, rscnt, rsent, hout[3], fin[3];
+    size_t guess, flat, knots, alon, alat, aloc, hc, hnb, fb, cc, sel, rscnt, rsent, hout[3], fin[3];
   };
   std::vector<Offs> of(n);
   size_t ax_total = 0;
@@ -417,13 +417,13 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     }
     o.hc = take(npx * sizeof(float));
     o.hnb = take(npx * sizeof(float4));
-    o.rec = take(npx * sizeof(Rec));
+    o.fb = take(npx * sizeof(int64_t));
     o.cc = take(npx * 4);
     o.sel = take(npx);
     o.rscnt = o.rsent = SIZE_MAX;
     if (tiles[i].cfg.precision == SD_PRECISION_SPLIT) {
-      o.rscnt = take(p.rows * p.bpr * 4);
-      o.rsent = take(p.rows * p.bpr * RS_CAP * sizeof(RsEnt));
+      o.rscnt = take(stage_items(WK_SEL, p) * 4);
+      o.rsent = take(stage_items(WK_SEL, p) * RS_CAP * sizeof(RsEnt));
     }
     for (int k = 0; k < 3; ++k) {
       o.hout[k] = o.fin[k] = SIZE_MAX;
@@ -477,7 +477,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     }
     p.hc = (const float *)(arena + o.hc);
     p.hnb = (const float4 *)(arena + o.hnb);
-    p.rec = (Rec *)(arena + o.rec);
+    p.fb = (int64_t *)(arena + o.fb);
     p.cc = (uint32_t *)(arena + o.cc);
     p.sel = (uint8_t *)(arena + o.sel);
     p.rs_cnt = o.rscnt != SIZE_MAX ? (uint32_t *)(arena + o.rscnt) : nullptr;
