@@ -424,34 +424,23 @@ constexpr double kDemPosEps = 3e-8;  // m
 // for a void), 0 = undecided.  eps_px: position uncertainty in pixels,
 // to which the reciprocal's rounding is added here.
 SD_HD int dem_sample_cert(const DemView &d, double row_f, double col_f, double eps_px, bool *inside, float *h) {
-  if (row_f != row_f || col_f != col_f) return 0;
-  const double eps = eps_px + 5e-16 * (fabs(row_f) + fabs(col_f));
   const double max_row = (double)(d.height - 1);
   const double max_col = (double)(d.width - 1);
-  // the +-0.5 px margin (dem.rs:351-371)
-  if (row_f < -0.5 - eps || row_f > max_row + 0.5 + eps || col_f < -0.5 - eps || col_f > max_col + 0.5 + eps) {
+  // Within a pixel of the DEM's border the margin test (+-0.5 px,
+  // dem.rs:351-371) and the clamps to [0, max] are near: left to the exact
+  // lookup, as is anything non-finite.  Far outside is decided here.
+  if (row_f < -1.0 || row_f > max_row + 1.0 || col_f < -1.0 || col_f > max_col + 1.0) {
     *inside = false;
     return 1;
   }
-  if (row_f < -0.5 + eps || row_f > max_row + 0.5 - eps || col_f < -0.5 + eps || col_f > max_col + 0.5 - eps)
-    return 0;
-  // the clamps to [0, max]
-  if (fabs(row_f) <= eps || fabs(row_f - max_row) <= eps || fabs(col_f) <= eps || fabs(col_f - max_col) <= eps)
-    return 0;
+  if (!(row_f >= 1.0 && row_f <= max_row - 1.0 && col_f >= 1.0 && col_f <= max_col - 1.0)) return 0;
+  const double eps = eps_px + 5e-16 * (row_f + col_f);
   *inside = true;
-  row_f = clampd(row_f, 0.0, max_row);
-  col_f = clampd(col_f, 0.0, max_col);
-  uint64_t max_rc = d.height - 1;
-  uint64_t r0 = f2u64(row_f);
-  uint64_t rlim = max_rc == 0 ? 0 : max_rc - 1;
-  if (r0 > rlim) r0 = rlim;
-  uint64_t c0 = f2u64(col_f);
-  uint64_t clim = d.width < 2 ? 0 : d.width - 2;
-  if (c0 > clim) c0 = clim;
-  const uint64_t r1 = r0 + 1, c1 = c0 + 1;
+  uint64_t r0 = (uint64_t)row_f, c0 = (uint64_t)col_f;  // in [1, max - 1]: no clamp applies
   const double dr = row_f - (double)r0;
   const double dc = col_f - (double)c0;
   if (dr <= eps || dr >= 1.0 - eps || dc <= eps || dc >= 1.0 - eps) return 0;  // a cell edge
+  const uint64_t r1 = r0 + 1, c1 = c0 + 1;
 #if defined(__CUDA_ARCH__)
   const float v00 = __ldg(&d.data[r0 * d.width + c0]), v01 = __ldg(&d.data[r0 * d.width + c1]);
   const float v10 = __ldg(&d.data[r1 * d.width + c0]), v11 = __ldg(&d.data[r1 * d.width + c1]);
@@ -465,12 +454,11 @@ SD_HD int dem_sample_cert(const DemView &d, double row_f, double col_f, double e
   }
   const double v = (double)v00 * (1.0 - dr) * (1.0 - dc) + (double)v01 * (1.0 - dr) * dc +
                    (double)v10 * dr * (1.0 - dc) + (double)v11 * dr * dc;
-  // the value's uncertainty: its slopes over eps, plus the rounding of this
-  // sum and of the exact position's (a few ulps of the corner magnitudes)
-  const double gr = fmax(fabs((double)v10 - (double)v00), fabs((double)v11 - (double)v01));
-  const double gc = fmax(fabs((double)v01 - (double)v00), fabs((double)v11 - (double)v10));
-  const double dv = (gr + gc) * eps +
-                    2e-15 * (fabs((double)v00) + fabs((double)v01) + fabs((double)v10) + fabs((double)v11));
+  // the value's uncertainty: the corners' spread times the position's
+  // uncertainty in both axes, plus the rounding of this sum and of the exact
+  // position's (a few ulps of the corner magnitudes)
+  const float lo4 = fminf(fminf(v00, v01), fminf(v10, v11)), hi4 = fmaxf(fmaxf(v00, v01), fmaxf(v10, v11));
+  const double dv = 2.0 * ((double)hi4 - (double)lo4) * eps + 8e-15 * fmax(fabs((double)lo4), fabs((double)hi4));
   const float lo = (float)(v - dv), hi = (float)(v + dv);
   if (lo != hi) return 0;
   *h = (float)v;

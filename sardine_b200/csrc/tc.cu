@@ -321,6 +321,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   SD_CUDA(ctx, cudaMemcpyAsync(flags, ctx->d_flags, sizeof flags, cudaMemcpyDeviceToHost, st));
   SD_CUDA(ctx, cudaMemcpyAsync(cnt, ctx->d_counters, sizeof cnt, cudaMemcpyDeviceToHost, st));
   SD_TRY(sync(ctx));
+  if (flags[5]) return set_error(ctx, SD_ERR_INTERNAL, "terrain correction: a converged pixel lost its DEM height");
   if (flags[0]) {
     return set_error(ctx, SD_ERR_TC_ORBIT,
                      "orbit interpolation failed: interpolation time outside orbit window; "

@@ -90,14 +90,34 @@ __device__ __forceinline__ int orbit_at(const OrbitDev &o, int64_t t, OrbitState
   return rc;
 }
 
+// The Lagrange sums out of line (taken rarely: times outside the table).
+__device__ __noinline__ int orbit_eval_cold(const sd_state_vector *svs, uint64_t n, int64_t t, OrbitState *s) {
+  return orbit_eval(svs, n, t, s);
+}
+
 // The reference's own state at t: the table inside its span, else the
 // Lagrange sums (orbit_eval, the reference's formula).
-__device__ __noinline__ int orbit_exact(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
+__device__ __forceinline__ int orbit_exact(const OrbitDev &o, int64_t t, OrbitState *s, double *vsq) {
   const int64_t i = t - o.tab_t0;
   if (i >= 0 && i < o.tab_n) return orbit_at(o, t, s, vsq);
-  const int rc = orbit_eval(o.svs, o.n, t, s);
+  const int rc = orbit_eval_cold(o.svs, o.n, t, s);
   if (rc == ORB_OK) *vsq = dot3(s->vel, s->vel);
   return rc;
+}
+
+// The reference's satellite position at t (the first 24 B of the table entry).
+__device__ __forceinline__ bool orbit_pos_exact(const OrbitDev &o, int64_t t, V3 *S) {
+  const int64_t i = t - o.tab_t0;
+  if (i >= 0 && i < o.tab_n) {
+    const double2 *e = o.tab + 5 * i;
+    const double2 a = __ldg(e), b = __ldg(e + 1);
+    *S = {a.x, a.y, b.x};
+    return true;
+  }
+  OrbitState s;
+  if (orbit_eval_cold(o.svs, o.n, t, &s) != ORB_OK) return false;
+  *S = s.pos;
+  return true;
 }
 
 // A Newton decision (the |delta| < tol test or the microsecond truncation of
@@ -249,17 +269,17 @@ __device__ __forceinline__ double row_y(const TcDev &p, uint64_t r) {
 // UTM (output_crs.rs:383-415).
 // Pixel centre as in pixel_lonlat, plus the anchor segment g and the
 // position t in it (UTM grids only).
-__device__ void pixel_seg(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat, int *gs,
-                          double *ts);
+__device__ __forceinline__ void pixel_seg(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat,
+                                          int *gs, double *ts);
 
-__device__ void pixel_lonlat(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat) {
+__device__ __forceinline__ void pixel_lonlat(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat) {
   int g;
   double t;
   pixel_seg(p, r, c, lon, lat, &g, &t);
 }
 
-__device__ void pixel_seg(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat, int *gs,
-                          double *ts) {
+__device__ __forceinline__ void pixel_seg(const TcDev &p, uint64_t r, uint64_t c, double *lon, double *lat,
+                                          int *gs, double *ts) {
   *gs = 0;
   *ts = 0.0;
   if (!p.utm) {
@@ -296,7 +316,7 @@ __device__ void pixel_seg(const TcDev &p, uint64_t r, uint64_t c, double *lon, d
 // dlam)) reproduces the exact projection to ~1e-11 m.  The local-expansion
 // terms used for the cardinal neighbours move by ~1e-4 relative over a
 // segment and are interpolated linearly (effect ~3e-8 m on a 10 m step).
-__device__ void dem_local_from_anchors(const TcDev &p, uint64_t r, int g, double t, UtmLocal *o) {
+__device__ __forceinline__ void dem_local_from_anchors(const TcDev &p, uint64_t r, int g, double t, UtmLocal *o) {
   const UtmLocal &A = p.aloc[r * p.n_pts + g], &B = p.aloc[r * p.n_pts + g + 1];
   const double *lo = p.alon + r * p.n_pts, *la = p.alat + r * p.n_pts;
   const double k = kPi / 180.0;
@@ -370,7 +390,7 @@ __global__ void k_row_setup(const TcWork *__restrict__ wp) {
     const uint64_t r = i - pre[j];
     if (r == 0) {  // the job's counters and flags start at zero
       for (int k = 0; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; ++k) p.counters[k] = 0;
-      for (int k = 0; k < 5; ++k) p.flags[k] = 0;
+      for (int k = 0; k < 6; ++k) p.flags[k] = 0;
     }
     const double y = row_y(p, r);
     double lat_seed = y;
@@ -424,7 +444,7 @@ __global__ void k_row_model(const TcWork *__restrict__ wp) {
   }
 }
 
-__device__ int64_t predicted_time(const TcDev &p, uint64_t r, uint64_t c) {
+__device__ __forceinline__ int64_t predicted_time(const TcDev &p, uint64_t r, uint64_t c) {
   const int64_t *k = p.knot_t + r * KNOTS;
   if (p.cols <= 1) return k[0] != INT64_MIN ? k[0] : p.row_guess[r];
   int j = (int)((c * (KNOTS - 1)) / (p.cols - 1));
@@ -737,7 +757,7 @@ struct PixGeo {
 // Returns false when the DEM has no finite height there.
 // Centre of the pixel: lon/lat, the UTM local expansion for a projected DEM,
 // and the DEM height; false when there is no finite height.
-__device__ bool pixel_height(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g, float *hf) {
+__device__ __forceinline__ bool pixel_height(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g, float *hf) {
   int seg;
   double t;
   pixel_seg(p, r, c, &g->lon, &g->lat, &seg, &t);
@@ -782,7 +802,7 @@ struct Facet {
 
 // Heights of the east, west, north and south neighbours (1642-1675: DEM
 // heights without the geoid); false when any lies outside the DEM or on a void.
-__device__ bool facet_heights(const TcDev &p, const PixGeo &g, float h[4]) {
+__device__ __forceinline__ bool facet_heights(const TcDev &p, const PixGeo &g, float h[4]) {
   const double sd = p.step_deg;
   const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
   float he, hw, hn, hs;
@@ -1173,7 +1193,10 @@ static_assert(MAIN_THREADS <= 256, "RsEnt::meta holds the k_main thread in 8 bit
 // (NaN when any is missing).  These are the latency-bound gathers and
 // projections; done here at low register pressure they overlap well, and
 // k_main reads 20 B per pixel instead.
-__global__ void __launch_bounds__(SEL_THREADS, 4) k_heights(const TcWork *__restrict__ wp) {
+#ifndef SD_HEIGHTS_MINB
+#define SD_HEIGHTS_MINB 4
+#endif
+__global__ void __launch_bounds__(SEL_THREADS, SD_HEIGHTS_MINB) k_heights(const TcWork *__restrict__ wp) {
   const TcWork w = *wp;
   const uint64_t *pre = stage_pre(w, WK_SEL);
   const uint64_t total = pre[w.n_jobs];
@@ -1181,7 +1204,6 @@ __global__ void __launch_bounds__(SEL_THREADS, 4) k_heights(const TcWork *__rest
     const int jb = find_job(pre, w.n_jobs, item);
     const TcDev &p = w.jobs[jb];
     if (p.rs_cnt && threadIdx.x == 0) p.rs_cnt[item - pre[jb]] = 0;  // k_cand's queue of this item
-    if (!p.hc) continue;
     const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
     if (i >= p.rows * p.cols) continue;
     const uint64_t r = i / p.cols, c = i % p.cols;
@@ -1322,14 +1344,12 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   orb_taylor_build(p.orb, uw, ew, ew_ok, tid & 31, &T);
   __syncwarp();
   if (in_row && r < p.rows) {
-    if (p.hc) {  // heights from k_heights
-      pixel_lonlat(p, r, (uint64_t)c, &g.lon, &g.lat);
-      const float hf = __ldg(p.hc + i);
-      geo_ok = isfinite(hf);
-      if (geo_ok) pixel_ecef(p, &g, hf);
-    } else {
-      geo_ok = pixel_geo(p, r, (uint64_t)c, &g);
-    }
+    // heights from k_heights (every job has them; computing them here
+    // instead would put the pixel's geometry in local memory)
+    pixel_lonlat(p, r, (uint64_t)c, &g.lon, &g.lat);
+    const float hf = __ldg(p.hc + i);
+    geo_ok = isfinite(hf);
+    if (geo_ok) pixel_ecef(p, &g, hf);
     if (geo_ok && fast) {
       // reference iteration from the shared state: one converged t*
       int64_t t = ew_ok ? uw : predicted_time(p, r, (uint64_t)c);
@@ -1718,20 +1738,16 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
 #define SD_CAND_MINB 2  // blocks of 256 per SM the register budget is cut for
 #endif
 
+// The pixel's geometry from the heights k_heights left (every job has them).
 __device__ __forceinline__ void pixel_from_heights(const TcDev &p, uint64_t i, uint64_t r, uint64_t c, PixGeo *g,
                                                    float h4[4], bool *ok) {
-  if (p.hc) {
-    pixel_lonlat(p, r, c, &g->lon, &g->lat);
-    const float hf = __ldg(p.hc + i);
-    *ok = isfinite(hf);
-    if (*ok) pixel_ecef(p, g, hf);
-    if (p.need_geom) {
-      const float4 q4 = __ldg(p.hnb + i);
-      h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
-    }
-  } else {
-    *ok = pixel_geo(p, r, c, g);
-    if (*ok && p.need_geom && !facet_heights(p, *g, h4)) h4[0] = h4[1] = h4[2] = h4[3] = NAN;
+  pixel_lonlat(p, r, c, &g->lon, &g->lat);
+  const float hf = __ldg(p.hc + i);
+  *ok = isfinite(hf);
+  if (*ok) pixel_ecef(p, g, hf);
+  if (p.need_geom) {
+    const float4 q4 = __ldg(p.hnb + i);
+    h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
   }
 }
 
@@ -1742,12 +1758,24 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
   const uint64_t *pre = stage_pre(w, WK_SEL);
   const uint64_t total = pre[w.n_jobs];
   const int tid = threadIdx.x;
+  // counters accumulate in shared memory over the block's items of one job
+  // and go to the job's counters when the job changes or the block ends
+  for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
+  int cur = -1;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
     const int jb = find_job(pre, w.n_jobs, item);
+    if (jb != cur) {  // block-uniform
+      __syncthreads();
+      if (cur >= 0)
+        for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
+          if (s_cnt[k]) {
+            atomicAdd(&w.jobs[cur].counters[k], (unsigned long long)s_cnt[k]);
+            s_cnt[k] = 0;
+          }
+      __syncthreads();
+      cur = jb;
+    }
     const TcDev &p = w.jobs[jb];
-    __syncthreads();  // the previous item's flush is done
-    for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
-    __syncthreads();
     const uint64_t npx = p.rows * p.cols;
     const uint64_t li = item - pre[jb];
     const uint64_t i = li * SEL_THREADS + tid;
@@ -1763,14 +1791,12 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
       float h4[4] = {NAN, NAN, NAN, NAN};
       bool ok;
       pixel_from_heights(p, i, r, c, &g, h4, &ok);
-      OrbitState os;
-      double vsq;
-      const bool orb_ok = ok && orbit_exact(p.orb, t, &os, &vsq) == ORB_OK;
-      if (!orb_ok) atomicOr(&p.flags[0], ok ? 1 : 2);  // cannot happen for a converged time
+      V3 S;
+      const bool orb_ok = ok && orbit_pos_exact(p.orb, t, &S);
+      if (!orb_ok) atomicOr(&p.flags[ok ? 0 : 5], 1);  // cannot happen for a converged time
       CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
       bool deferred = false;
       if (orb_ok) {
-        const V3 S = os.pos;
         const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
         if constexpr (SPLIT) {
           const CandPre cp = cand_pre<KERNEL, true>(p, g.P, S, t);
@@ -1823,10 +1849,11 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
       }
     }
     if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
-    __syncthreads();
-    for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
-      if (s_cnt[k]) atomicAdd(&p.counters[k], (unsigned long long)s_cnt[k]);
   }
+  __syncthreads();
+  if (cur >= 0)
+    for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
+      if (s_cnt[k]) atomicAdd(&w.jobs[cur].counters[k], (unsigned long long)s_cnt[k]);
 }
 
 // ── k_resample (split precision): FP64 values of the queued candidates ────────
@@ -1941,7 +1968,7 @@ __global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__
       OrbitState os;
       double vsq;
       if (!ok || orbit_exact(p.orb, t, &os, &vsq) != ORB_OK) {
-        atomicOr(&p.flags[0], 2);
+        atomicOr(&p.flags[ok ? 0 : 5], 1);
         continue;
       }
       const CandOut o = cand_fp64<KERNEL>(p, g, os.pos, t, p.need_geom ? p.row_flat[r] : 0.0,

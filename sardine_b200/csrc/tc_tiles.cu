@@ -626,6 +626,7 @@ extern "C" int sd_tc_tiles_finish(sd_ctx *ctx, sd_geocoded_info *infos, uint64_t
   SD_CUDA(ctx, cudaEventSynchronize(ctx->tiles_done));
   SD_TRY(sync(ctx));
   int orbit_bad = -1;
+  bool internal_bad = false;
   for (uint64_t i = 0; i < n; ++i) {
     sd_geocoded_info f = ctx->tile_info[i];
     const unsigned long long *c = ctx->h_tile_counters + 32 * i;
@@ -641,8 +642,10 @@ extern "C" int sd_tc_tiles_finish(sd_ctx *ctx, sd_geocoded_info *infos, uint64_t
     f.diag_fp64_redo_pixels = (uint64_t)ctx->h_tile_flags[8 * i + 2];
     f.diag_fp64_resampled = (uint64_t)ctx->h_tile_flags[8 * i + 4];
     if (ctx->h_tile_flags[8 * i] && orbit_bad < 0) orbit_bad = (int)i;
+    if (ctx->h_tile_flags[8 * i + 5]) internal_bad = true;
     infos[i] = f;
   }
+  if (internal_bad) return set_error(ctx, SD_ERR_INTERNAL, "tiles: a converged pixel lost its DEM height");
   if (orbit_bad >= 0)
     return set_error(ctx, SD_ERR_TC_ORBIT,
                      "tile %d: orbit interpolation failed: interpolation time outside orbit window; "
