@@ -10,6 +10,11 @@ at any time; each scheduler step
   3. launches that batch asynchronously (one persistent launch per stage,
      replayed from a CUDA graph).
 
+A request can be cancelled (`cancel`): a queued one leaves the queue, an
+in-flight one still runs with its batch but its result is dropped when the
+batch is collected.  A request submitted with a deadline that has passed by
+the time a slot could take it is cancelled the same way (`Cancelled`).
+
 A slot is a context (CUDA stream + reserved scratch arena); with two or more
 slots, a batch admitted while another is on the GPU runs concurrently with
 it.  Requests never wait for a batch boundary longer than one in-flight
@@ -28,6 +33,10 @@ from ._lib import Context, lib
 from .tiles import TileBatch, TileRequest
 
 
+class Cancelled(Exception):
+    """The request was cancelled (by `cancel` or its deadline) and has no result."""
+
+
 @dataclass
 class Ticket:
     """One submitted request and, once done, its result and timings."""
@@ -37,6 +46,12 @@ class Ticket:
     t_done: float = 0.0
     result: object = None
     error: Optional[BaseException] = None
+    deadline: float = float("inf")  # latest admission time (the clock's units)
+    cancel_requested: bool = False
+
+    @property
+    def cancelled(self) -> bool:
+        return isinstance(self.error, Cancelled)
 
     @property
     def latency_s(self) -> float:
@@ -123,8 +138,12 @@ class GeocodingServer:
         self.completed: List[Ticket] = []
 
     # ── client side ──
-    def submit(self, req: TileRequest) -> Ticket:
+    def submit(self, req: TileRequest, deadline_s: Optional[float] = None) -> Ticket:
+        """Queues a request; with deadline_s it is cancelled if no slot has
+        taken it within deadline_s of its submission."""
         t = Ticket(req, self.clock())
+        if deadline_s is not None:
+            t.deadline = t.t_submit + deadline_s
         out_cap = getattr(self.slots[0], "out_capacity", None)
         if req.device_bytes() > self.slots[0].capacity or \
                 (out_cap is not None and output_bytes(req) > out_cap):
@@ -135,6 +154,22 @@ class GeocodingServer:
             return t
         self.queue.append(t)
         return t
+
+    def cancel(self, t: Ticket) -> bool:
+        """Cancels a request that has not completed: a queued one is removed
+        at once; an in-flight one runs on with its batch and its result is
+        dropped at collection.  Returns False when it had already completed."""
+        if t.done:
+            return False
+        try:
+            self.queue.remove(t)
+        except ValueError:  # in flight
+            t.cancel_requested = True
+            return True
+        t.error = Cancelled("cancelled before launch")
+        t.t_done = self.clock()
+        self.completed.append(t)
+        return True
 
     # ── scheduler ──
     def step(self) -> int:
@@ -154,8 +189,11 @@ class GeocodingServer:
             results = s.batch.finish()
             now = self.clock()
             for t, r in zip(s.tickets, results):
-                t.result = r
                 t.t_done = now
+                if t.cancel_requested:  # ran with its batch; the result is dropped
+                    t.error = Cancelled("cancelled in flight")
+                    continue
+                t.result = r
                 if self.on_done is not None:
                     self.on_done(t)
                 if not self.keep_results and hasattr(r, "data"):
@@ -174,6 +212,12 @@ class GeocodingServer:
         take: List[Ticket] = []
         used = used_out = 0
         out_cap = getattr(s, "out_capacity", float("inf"))
+        now = self.clock()
+        while self.queue and self.queue[0].deadline < now:  # expired before any slot took it
+            t = self.queue.popleft()
+            t.error = Cancelled("deadline passed before launch")
+            t.t_done = now
+            self.completed.append(t)
         while self.queue and len(take) < self.max_batch:
             need = self.queue[0].request.device_bytes()
             need_out = output_bytes(self.queue[0].request) if out_cap != float("inf") else 0

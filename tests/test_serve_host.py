@@ -8,7 +8,7 @@ import numpy as np
 import oracle
 import sardine_b200 as sd
 from sardine_b200 import synth
-from sardine_b200.serve import GeocodingServer, latency_summary
+from sardine_b200.serve import Cancelled, GeocodingServer, latency_summary
 from sardine_b200.tiles import TileRequest
 
 
@@ -107,6 +107,34 @@ def test_fifo_head_of_line_and_oversize():
     assert slots[0].launched == [["x"]]
     srv.drain()
     assert slots[0].launched == [["x"], ["y", "z"]]
+
+
+def test_cancel_queued_and_in_flight():
+    srv, slots = _server(budget=100, slots=1, max_batch=1, polls=3)
+    a = srv.submit(FakeReq("a", 50))
+    b = srv.submit(FakeReq("b", 50))
+    c = srv.submit(FakeReq("c", 50))
+    srv.step()                       # a in flight, b and c queued
+    assert srv.cancel(a) and srv.cancel(b)
+    assert b.done and b.cancelled and not a.done
+    srv.drain()
+    assert a.cancelled and a.result is None       # ran with its batch, result dropped
+    assert c.result == ("result", "c") and c.error is None
+    assert slots[0].launched == [["a"], ["c"]]     # b never launched
+    assert not srv.cancel(c)                      # already completed
+    s = latency_summary(srv.completed)
+    assert s["completed"] == 1 and s["failed"] == 2
+
+
+def test_deadline_expires_in_queue():
+    srv, slots = _server(budget=100, slots=1, max_batch=1, polls=5)
+    srv.submit(FakeReq("a", 50))
+    late = srv.submit(FakeReq("late", 50), deadline_s=2.0)   # the fake clock ticks 1 per call
+    ok = srv.submit(FakeReq("ok", 50), deadline_s=1e9)
+    srv.drain()
+    assert isinstance(late.error, Cancelled) and late.result is None
+    assert ok.result == ("result", "ok")
+    assert ["late"] not in slots[0].launched
 
 
 def test_latency_summary():
