@@ -1735,7 +1735,7 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
 // or flagged for the FP64 candidate (RD_FULL, k_redo), which write and count
 // it instead.
 #ifndef SD_CAND_MINB
-#define SD_CAND_MINB 3  // blocks of 256 per SM the register budget is cut for (latency-bound: warps over spills)
+#define SD_CAND_MINB 4  // blocks of 256 per SM the register budget is cut for (latency-bound: warps over spills)
 #endif
 
 // The pixel's geometry from the heights k_heights left (every job has them).
