@@ -252,12 +252,11 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
       p.aloc = d_aloc;
     }
   }
-  float *d_hc;
-  float4 *d_hnb;
-  SD_TRY(scratch_t(ctx, "tc.hc", npx, &d_hc));
-  SD_TRY(scratch_t(ctx, "tc.hnb", npx, &d_hnb));
-  p.hc = d_hc;
-  p.hnb = d_hnb;
+  double *d_tp, *d_fct = nullptr;
+  SD_TRY(scratch_t(ctx, "tc.target", 3 * npx, &d_tp));
+  if (p.need_geom) SD_TRY(scratch_t(ctx, "tc.facet", 4 * npx, &d_fct));
+  p.tp = d_tp;
+  p.fct = d_fct;
   SD_TRY(scratch_t(ctx, "tc.fb", npx, &p.fb));
   SD_TRY(scratch_t(ctx, "tc.cc", npx, &p.cc));
   SD_TRY(scratch_t(ctx, "tc.sel", npx, &p.sel));

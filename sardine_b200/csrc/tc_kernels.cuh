@@ -215,8 +215,11 @@ struct TcDev {
   int fast;                    // tolerance allows the fixed-point-pair scheme
   int split;                   // SD_PRECISION_SPLIT
   uint64_t row0;               // grid row of the job's first row (row bands)
-  const float *hc;             // per pixel: DEM height of the centre (NaN: none), from k_heights
-  const float4 *hnb;           // per pixel: heights of the E, W, N, S neighbours (NaN: facet missing)
+  // per pixel, from k_heights (structure of arrays, npx apart): the target
+  // ECEF x, y, z (x NaN: no DEM height) and, when the facet is needed, the
+  // facet normal x, y, z and area (area NaN: a neighbour height missing)
+  const double *tp;
+  const double *fct;
   uint32_t *rs_cnt;            // split: per k_cand item (256 px), FP64 re-samples queued (may exceed RS_CAP)
   struct RsEnt *rs_ent;        // split: per k_cand item, RS_CAP queued re-samples
 };
@@ -1030,7 +1033,7 @@ __device__ FacetF pixel_facet_f(const TcDev &p, const PixGeo &g) {
 
 // cand_post in split precision; *redo is set when a mask decision falls
 // inside the FP32 error margin and the FP64 candidate must decide.
-__device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g, V3 S, const FacetF &f,
+__device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, V3 P, V3 S, const FacetF &f,
                                float flat_area, int *redo, float *wdiv) {
   CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
   *redo = RD_NONE;
@@ -1041,7 +1044,7 @@ __device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g
     if (!f.ok) {
       if (p.flatten) return {NAN, cosv, (uint8_t)SD_MASK_DEM_NEIGHBOUR_MISSING, 5};
     } else {
-      const float lx = (float)(S.x - g.P.x), ly = (float)(S.y - g.P.y), lz = (float)(S.z - g.P.z);
+      const float lx = (float)(S.x - P.x), ly = (float)(S.y - P.y), lz = (float)(S.z - P.z);
       const float il = rsqrtf(lx * lx + ly * ly + lz * lz);
       const float lp = (f.nx * lx + f.ny * ly + f.nz * lz) * il;
       const float dlp = kLpErr * f.en + kLpRel * fabsf(lp);  // bound on |lp - lp_fp64|
@@ -1102,6 +1105,13 @@ __device__ CandOut cand_post_f(const TcDev &p, const CandPre &c, const PixGeo &g
 // missing), else null to look them up.
 __device__ __forceinline__ bool heights_ok(const float *h4) {
   return isfinite(h4[0]) && isfinite(h4[1]) && isfinite(h4[2]) && isfinite(h4[3]);
+}
+
+// One candidate's output in FP64 from the stored target and facet.
+template <int KERNEL>
+__device__ CandOut cand_fp64_tf(const TcDev &p, V3 P, const Facet &f, V3 S, int64_t t, double flat_area) {
+  CandPre pre = cand_pre<KERNEL, false>(p, P, S, t);
+  return cand_post(p, pre, P, S, f, flat_area);
 }
 
 template <int KERNEL>
@@ -1187,12 +1197,12 @@ constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
 static_assert(MAIN_THREADS <= 256, "RsEnt::meta holds the k_main thread in 8 bits");
 
 // ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
-// ── k_heights: the DEM side of every pixel ahead of k_main ─────────────────
-// Per pixel: the centre height (DEM lookup of 1529-1536, NaN where the DEM
-// has none) and, where the facet is needed, the four neighbour heights
-// (NaN when any is missing).  These are the latency-bound gathers and
-// projections; done here at low register pressure they overlap well, and
-// k_main reads 20 B per pixel instead.
+// ── k_heights: the geometry of every pixel ahead of k_main ─────────────────
+// Per pixel: the centre height (DEM lookup of 1529-1536), geoid and target
+// ECEF (1545-1546), and, where the facet is needed, the four neighbour
+// heights and the facet normal and area (1642-1675).  None of it depends on
+// the azimuth time, so k_main reads the target (24 B) and k_cand the target
+// and facet (56 B) instead of recomputing them.
 #ifndef SD_HEIGHTS_MINB
 #define SD_HEIGHTS_MINB 4
 #endif
@@ -1207,17 +1217,33 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_HEIGHTS_MINB) k_heights(const 
     const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
     if (i >= p.rows * p.cols) continue;
     const uint64_t r = i / p.cols, c = i % p.cols;
+    const uint64_t npx = p.rows * p.cols;
     PixGeo g;
     float hf;
     const bool ok = pixel_height(p, r, c, &g, &hf);
-    float h[4] = {NAN, NAN, NAN, NAN};
-    if (ok && p.need_geom) {
-      g.lo = deg2rad_ecef(g.lon);
-      g.la = deg2rad_ecef(g.lat);
-      if (!facet_heights(p, g, h)) h[0] = h[1] = h[2] = h[3] = NAN;
+    double *tp = (double *)p.tp;
+    if (!ok) {
+      tp[i] = NAN;
+      if (p.fct) ((double *)p.fct)[3 * npx + i] = NAN;
+      continue;
     }
-    ((float *)p.hc)[i] = ok ? hf : NAN;
-    ((float4 *)p.hnb)[i] = make_float4(h[0], h[1], h[2], h[3]);
+    pixel_ecef(p, &g, hf);
+    tp[i] = g.P.x;
+    tp[npx + i] = g.P.y;
+    tp[2 * npx + i] = g.P.z;
+    if (p.fct) {
+      double *f = (double *)p.fct;
+      float h[4];
+      if (facet_heights(p, g, h)) {
+        const Facet fc = facet_from(p, g, h);
+        f[i] = fc.normal.x;
+        f[npx + i] = fc.normal.y;
+        f[2 * npx + i] = fc.normal.z;
+        f[3 * npx + i] = fc.area;
+      } else {
+        f[3 * npx + i] = NAN;
+      }
+    }
   }
 }
 
@@ -1344,12 +1370,14 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   orb_taylor_build(p.orb, uw, ew, ew_ok, tid & 31, &T);
   __syncwarp();
   if (in_row && r < p.rows) {
-    // heights from k_heights (every job has them; computing them here
-    // instead would put the pixel's geometry in local memory)
-    pixel_lonlat(p, r, (uint64_t)c, &g.lon, &g.lat);
-    const float hf = __ldg(p.hc + i);
-    geo_ok = isfinite(hf);
-    if (geo_ok) pixel_ecef(p, &g, hf);
+    // the target from k_heights (every job has it)
+    const uint64_t npx = p.rows * p.cols;
+    g.P.x = __ldg(p.tp + i);
+    geo_ok = isfinite(g.P.x);
+    if (geo_ok) {
+      g.P.y = __ldg(p.tp + npx + i);
+      g.P.z = __ldg(p.tp + 2 * npx + i);
+    }
     if (geo_ok && fast) {
       // reference iteration from the shared state: one converged t*
       int64_t t = ew_ok ? uw : predicted_time(p, r, (uint64_t)c);
@@ -1738,17 +1766,23 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
 #define SD_CAND_MINB 4  // blocks of 256 per SM the register budget is cut for (latency-bound: warps over spills)
 #endif
 
-// The pixel's geometry from the heights k_heights left (every job has them).
-__device__ __forceinline__ void pixel_from_heights(const TcDev &p, uint64_t i, uint64_t r, uint64_t c, PixGeo *g,
-                                                   float h4[4], bool *ok) {
-  pixel_lonlat(p, r, c, &g->lon, &g->lat);
-  const float hf = __ldg(p.hc + i);
-  *ok = isfinite(hf);
-  if (*ok) pixel_ecef(p, g, hf);
-  if (p.need_geom) {
-    const float4 q4 = __ldg(p.hnb + i);
-    h4[0] = q4.x, h4[1] = q4.y, h4[2] = q4.z, h4[3] = q4.w;
+// The pixel's target and facet as k_heights left them (every job has them).
+__device__ __forceinline__ bool target_facet(const TcDev &p, uint64_t i, V3 *P, Facet *f) {
+  const uint64_t npx = p.rows * p.cols;
+  P->x = __ldg(p.tp + i);
+  if (!isfinite(P->x)) return false;
+  P->y = __ldg(p.tp + npx + i);
+  P->z = __ldg(p.tp + 2 * npx + i);
+  f->ok = false;
+  if (p.fct) {
+    const double area = __ldg(p.fct + 3 * npx + i);
+    if (isfinite(area)) {
+      f->ok = true;
+      f->normal = {__ldg(p.fct + i), __ldg(p.fct + npx + i), __ldg(p.fct + 2 * npx + i)};
+      f->area = area;
+    }
   }
+  return true;
 }
 
 template <int KERNEL, bool SPLIT>
@@ -1786,11 +1820,10 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
     int counter = -1;
     if (has_t) {
       atomicAdd(&s_cnt[kCounters + it], 1u);
-      const uint64_t r = i / p.cols, c = i % p.cols;
-      PixGeo g;
-      float h4[4] = {NAN, NAN, NAN, NAN};
-      bool ok;
-      pixel_from_heights(p, i, r, c, &g, h4, &ok);
+      const uint64_t r = i / p.cols;
+      V3 P;
+      Facet fc;
+      const bool ok = target_facet(p, i, &P, &fc);
       V3 S;
       const bool orb_ok = ok && orbit_pos_exact(p.orb, t, &S);
       if (!orb_ok) atomicOr(&p.flags[ok ? 0 : 5], 1);  // cannot happen for a converged time
@@ -1799,12 +1832,19 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
       if (orb_ok) {
         const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
         if constexpr (SPLIT) {
-          const CandPre cp = cand_pre<KERNEL, true>(p, g.P, S, t);
+          const CandPre cp = cand_pre<KERNEL, true>(p, P, S, t);
+          // the FP64 facet rounded to FP32: within 2^-24 |n| per component,
+          // inside the bound cand_post_f allows (kLpErr en, en = area)
           FacetF f{};
-          if (cp.inside && p.need_geom && heights_ok(h4)) f = facetf_from(p, g, h4);
+          if (fc.ok) {
+            f.ok = true;
+            f.nx = (float)fc.normal.x, f.ny = (float)fc.normal.y, f.nz = (float)fc.normal.z;
+            f.area = (float)fc.area;
+            f.en = f.area;
+          }
           int redo;
           float wd = 1.f;
-          o = cand_post_f(p, cp, g, S, f, (float)flat_area, &redo, &wd);
+          o = cand_post_f(p, cp, P, S, f, (float)flat_area, &redo, &wd);
           if (redo == RD_SAMPLE) {  // queue the FP64 re-sample in this item's slots
             const uint32_t q = atomicAdd(p.rs_cnt + li, 1u);
             if (q < (uint32_t)RS_CAP) {
@@ -1821,10 +1861,8 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
             deferred = true;
           }
         } else {
-          const CandPre cp = cand_pre<KERNEL, false>(p, g.P, S, t);
-          Facet f{};
-          if (cp.inside && p.need_geom && heights_ok(h4)) f = facet_from(p, g, h4);
-          o = cand_post(p, cp, g.P, S, f, flat_area);
+          const CandPre cp = cand_pre<KERNEL, false>(p, P, S, t);
+          o = cand_post(p, cp, P, S, fc, flat_area);
         }
       }
       if (!deferred) {
@@ -1958,21 +1996,19 @@ __global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__
     if (n > 0 && threadIdx.x == 0) atomicAdd(&p.flags[2], n);
     for (int q = threadIdx.x; q < n; q += SEL_THREADS) {
       const uint64_t i = base + list[q];
-      const uint64_t r = i / p.cols, c = i % p.cols;
+      const uint64_t r = i / p.cols;
       const int code = p.sel[i] & 7;
       const int64_t t = p.fb[i] + (code == SEL_M1 ? 1 : 0);
-      PixGeo g;
-      float h4[4] = {NAN, NAN, NAN, NAN};
-      bool ok;
-      pixel_from_heights(p, i, r, c, &g, h4, &ok);
+      V3 P;
+      Facet fc;
+      const bool ok = target_facet(p, i, &P, &fc);
       OrbitState os;
       double vsq;
       if (!ok || orbit_exact(p.orb, t, &os, &vsq) != ORB_OK) {
         atomicOr(&p.flags[ok ? 0 : 5], 1);
         continue;
       }
-      const CandOut o = cand_fp64<KERNEL>(p, g, os.pos, t, p.need_geom ? p.row_flat[r] : 0.0,
-                                          p.need_geom ? h4 : nullptr);
+      const CandOut o = cand_fp64_tf<KERNEL>(p, P, fc, os.pos, t, p.need_geom ? p.row_flat[r] : 0.0);
       p.out[i] = o.data;
       if (p.compute_lia) {
         p.cos_lia[i] = o.cos;

@@ -397,7 +397,7 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     return o;
   };
   struct Offs {
-    size_t guess, flat, knots, alon, alat, aloc, hc, hnb, fb, cc, sel, rscnt, rsent, hout[3], fin[3];
+    size_t guess, flat, knots, alon, alat, aloc, tp, fct, fb, cc, sel, rscnt, rsent, hout[3], fin[3];
   };
   std::vector<Offs> of(n);
   size_t ax_total = 0;
@@ -415,8 +415,8 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
       if (p.dem.kind == SD_DEM_PROJECTED_UTM) o.aloc = take(p.rows * p.n_pts * sizeof(UtmLocal));
       ax_total += p.n_pts;
     }
-    o.hc = take(npx * sizeof(float));
-    o.hnb = take(npx * sizeof(float4));
+    o.tp = take(3 * npx * sizeof(double));
+    o.fct = p.need_geom ? take(4 * npx * sizeof(double)) : SIZE_MAX;
     o.fb = take(npx * sizeof(int64_t));
     o.cc = take(npx * 4);
     o.sel = take(npx);
@@ -475,8 +475,8 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
       p.alat = (const double *)(arena + o.alat);
       p.aloc = o.aloc != SIZE_MAX ? (const UtmLocal *)(arena + o.aloc) : nullptr;
     }
-    p.hc = (const float *)(arena + o.hc);
-    p.hnb = (const float4 *)(arena + o.hnb);
+    p.tp = (const double *)(arena + o.tp);
+    p.fct = o.fct != SIZE_MAX ? (const double *)(arena + o.fct) : nullptr;
     p.fb = (int64_t *)(arena + o.fb);
     p.cc = (uint32_t *)(arena + o.cc);
     p.sel = (uint8_t *)(arena + o.sel);

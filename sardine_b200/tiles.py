@@ -101,9 +101,10 @@ class TileRequest:
 
     def device_bytes(self) -> int:
         """Device scratch this tile needs inside a batch (admission budget):
-        per-pixel heights (20 B), pair base / time (8 B), codes (4 B),
-        selection (1 B) and halo'd outputs (9 B) over the halo'd grid, plus
-        per-row state and the final rasters when they are staged."""
+        per-pixel target (24 B) and facet (32 B, with flattening or LIA),
+        pair base / time (8 B), codes (4 B), selection (1 B) and halo'd
+        outputs (9 B) over the halo'd grid, plus per-row state and the final
+        rasters when they are staged."""
         h = self.halo()
         r, c = self.rows + 2 * h, self.cols + 2 * h
         anchors = min(256, c) + 1 if self.config.crs.kind != _abi.CRS_WGS84 else 0
@@ -112,7 +113,8 @@ class TileRequest:
         if self.config.precision == T.Precision.SPLIT:
             # FP64 re-sample queue: per k_cand item (256 px) a count and 64 x 24 B
             extra = -(-(r * c) // 256) * (4 + 64 * 24) + 512
-        return r * c * (20 + 8 + 4 + 1 + 9) + r * per_row + self.rows * self.cols * 9 + 8192 + extra
+        geom = 32 if (self.config.flatten or self.config.compute_lia) else 0
+        return r * c * (24 + geom + 8 + 4 + 1 + 9) + r * per_row + self.rows * self.cols * 9 + 8192 + extra
 
 
 def _tile_to_c(req: TileRequest, outs, anchors: int) -> _abi.Tile:

@@ -153,9 +153,9 @@ def test_tile_request_halo_and_budget():
     r1 = TileRequest(None, sc.config, 0.0, 0.0, 100, 50, sd.SpeckleFilter.RefinedLee(4.4))
     r2 = TileRequest(None, sc.config, 0.0, 0.0, 100, 50, sd.SpeckleFilter.GammaMap(5, 4.4))
     assert (r0.halo(), r1.halo(), r2.halo()) == (0, 3, 2)
-    # per-pixel heights, pair bases, codes, selection and halo'd outputs:
-    # 42 B per halo'd pixel
-    assert r1.device_bytes() >= 106 * 56 * 42 and r1.device_bytes() > r0.device_bytes()
+    # per-pixel target, facet, pair bases, codes, selection and halo'd
+    # outputs: 78 B per halo'd pixel
+    assert r1.device_bytes() >= 106 * 56 * 78 and r1.device_bytes() > r0.device_bytes()
 
 
 def test_oracle_explicit_grid_equals_scene_grid():
