@@ -639,7 +639,16 @@ def run_c4(args):
             "e2e": None,
         }
         if args.cpu_baseline and world == 1:
-            out["cpu_baseline"] = _tiles_cpu_baseline(scenes, reqs)
+            def gpu_tiles(rs):  # the same requests through the GPU path, results on the host
+                got = []
+                for i in range(0, len(rs), 16):
+                    for x in tiles.tc_tiles(rs[i:i + 16], ctx):
+                        x.data = x.data.cpu().numpy()
+                        x.mask = x.mask.cpu().numpy() if x.mask is not None else None
+                        x.cos_lia = None
+                        got.append(x)
+                return got
+            out["cpu_baseline"] = _tiles_cpu_baseline(scenes, reqs, gpu_tiles=gpu_tiles)
         print(json.dumps(out), flush=True)
     _finish_dist(dist)
     ctx.close()

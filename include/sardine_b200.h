@@ -681,6 +681,24 @@ int sd_form_interferogram(sd_ctx *ctx, const float *ref, const float *sec, uint6
 int sd_to_db(sd_ctx *ctx, float *data, uint64_t n, float noise_floor_linear, uint64_t *counts,
              float *stats);
 
+/* dB output fused into the producing kernel: after
+ * sd_ctx_set_db_output(ctx, 1, noise_floor_linear), sd_terrain_correction
+ * (and its _rows/_with_times forms) and sd_speckle on this context write
+ * their sigma0/gamma0 (resp. filtered) raster in dB exactly as sd_to_db
+ * would convert it afterwards (to_db_inplace, export.rs:59-99, as run.rs:
+ * 395-403 applies it to the last stage's output), so the separate
+ * read-modify-write pass over the raster disappears.  sd_ctx_db_result then
+ * returns that call's {converted, noise_masked} counts and the
+ * compute_db_stats (run.rs:63-97) {min, max, mean, median} of the raster it
+ * wrote (of the band, for sd_terrain_correction_rows).  enable = 0 restores
+ * linear output.  SD_ERR_EXPORT_INVALID_NOISE_FLOOR when noise_floor_linear
+ * < 0.  No reference counterpart: the reference converts in a separate
+ * pass. */
+int sd_ctx_set_db_output(sd_ctx *ctx, int32_t enable, float noise_floor_linear);
+/* counts: {converted, noise_masked}; stats: {min, max, mean, median}.
+ * SD_ERR_INVALID_ARGUMENT if no call with dB output has completed. */
+int sd_ctx_db_result(sd_ctx *ctx, uint64_t *counts, float *stats);
+
 /* downsample_2x (export.rs:362-392): dst ((cols+1)/2 x (rows+1)/2) holds the
  * f64 mean of the non-NaN pixels of each 2x2 patch of src, NaN when all
  * are NaN.  The overview step of sd_write_cog. */

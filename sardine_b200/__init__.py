@@ -460,6 +460,24 @@ def to_db_inplace(data, noise_floor_linear: float, ctx: Optional[Context] = None
     return (out, tuple(float(x) for x in st)) if stats else out
 
 
+def set_db_output(ctx: Context, enable: bool, noise_floor_linear: float = 0.0) -> None:
+    """Makes terrain_correction and apply_speckle_filter on `ctx` write their
+    raster in dB, converted in the producing kernel as to_db_inplace
+    (export.rs:59-99) would convert it afterwards; db_result(ctx) returns
+    the last such call's counts and compute_db_stats (run.rs:63-97)."""
+    rc = lib().sd_ctx_set_db_output(ctx.handle, int(bool(enable)), float(noise_floor_linear))
+    _check(ctx, rc, ExportError)
+
+
+def db_result(ctx: Context):
+    """((converted, noise_masked), (min, max, mean, median)) of the last call
+    on `ctx` that wrote dB output."""
+    counts = (C.c_uint64 * 2)()
+    st = (C.c_float * 4)()
+    _check(ctx, lib().sd_ctx_db_result(ctx.handle, counts, st))
+    return (int(counts[0]), int(counts[1])), tuple(float(x) for x in st)
+
+
 def downsample_2x(src, cols: int, rows: int, ctx: Optional[Context] = None):
     """downsample_2x (export.rs:362-392): ((rows+1)//2, (cols+1)//2) raster
     of 2x2 NaN-skipping f64 means."""

@@ -556,6 +556,7 @@ extern "C" int sd_deburst_plan(sd_ctx *ctx, const sd_subswath *sw, const sd_burs
 
 extern "C" int sd_deburst_subswath(sd_ctx *ctx, const int16_t *slc, uint64_t tiff_width, uint64_t tiff_height,
                                    const sd_subswath *sw, const sd_burst *bursts, uint64_t n, int16_t *out) {
+  SD_STAGE("deburst");
   if (!ctx || !sw || !slc || !out) return SD_ERR_INVALID_ARGUMENT;
   SD_CUDA(ctx, cudaSetDevice(ctx->device));
   DeburstPlan p;
@@ -582,6 +583,7 @@ extern "C" int sd_apply_calibration(sd_ctx *ctx, const int16_t *iq, uint64_t lin
                                     const sd_lut_vector *nr, uint64_t n_nr, const sd_noise_azimuth *az,
                                     uint64_t tiff_line_origin, float *out, float *nesz, uint32_t *cal_gap,
                                     uint32_t *nr_gap) {
+  SD_STAGE("calibration");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   SD_CUDA(ctx, cudaSetDevice(ctx->device));
   CalPlan P;
@@ -618,6 +620,7 @@ extern "C" int sd_merge_subswaths(sd_ctx *ctx, int32_t n, const float *const *si
                                   const uint64_t *lines, const uint64_t *samples, const uint64_t *voff,
                                   const uint32_t *cal_gap, const uint32_t *nr_gap, const sd_subswath *sw,
                                   const int64_t *az_start, float *out, float *out_nesz, sd_merged_info *info) {
+  SD_STAGE("merge_subswaths");
   if (!ctx || !info) return SD_ERR_INVALID_ARGUMENT;
   FillRange fr[8];
   SD_TRY(merge_plan(ctx, n, lines, samples, voff, sw, az_start, info, fr));
@@ -662,6 +665,7 @@ extern "C" int sd_merge_subswaths(sd_ctx *ctx, int32_t n, const float *const *si
 
 extern "C" int sd_calibrate_deburst_merge(sd_ctx *ctx, int32_t n, const sd_swath_input *sw, float *out,
                                           float *out_nesz, sd_merged_info *info) {
+  SD_STAGE("cal_deburst_merge");
   if (!ctx || !sw || !info) return SD_ERR_INVALID_ARGUMENT;
   if (n <= 0) return set_error(ctx, SD_ERR_MERGE_EMPTY_INPUTS, "at least 1 subswath input is required, got 0");
   if (n > 8) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "at most 8 sub-swaths are supported");
@@ -947,6 +951,7 @@ extern "C" int sd_apply_calibration_noalloc(void *stream, const int16_t *deburst
                                             const sd_noise_azimuth *noise_azimuth, uint64_t tiff_line_origin,
                                             float *out_sigma0, float *out_nesz, uint32_t *cal_gap_px,
                                             uint32_t *noise_gap_px, char *err, uint64_t err_len) {
+  SD_STAGE("calibration");
   sd_ctx c;  // host-side bookkeeping only; owns no device memory
   int dev = 0;
   int rc;

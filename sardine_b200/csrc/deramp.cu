@@ -52,6 +52,7 @@ extern "C" int sd_deramp_subswath(sd_ctx *ctx, const int16_t *iq, uint64_t lines
                                   double range_pixel_spacing_m, double azimuth_time_interval_s,
                                   const sd_dc_estimate *estimates, uint64_t n_estimates, int64_t burst_start_us,
                                   int32_t swath_id, float *out) {
+  SD_STAGE("deramp");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (n_estimates == 0 || !estimates)
     return set_error(ctx, SD_ERR_INSAR_NO_DC_ESTIMATES,

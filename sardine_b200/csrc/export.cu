@@ -45,6 +45,8 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 // to_db_inplace on one DB_CHUNK per block (NaN kept; v <= floor -> NaN and
 // counted as noise-masked; else 10 log10 v), with the block's statistics of
 // the finite results.
+// CONVERT false: the statistics of a raster already in dB (read only).
+template <bool CONVERT>
 __global__ void __launch_bounds__(DB_THREADS) k_to_db(float *__restrict__ d, uint64_t n, float floor_lin,
                                                       DbPart *__restrict__ part) {
   __shared__ double s_sum[DB_THREADS / 32];
@@ -59,21 +61,20 @@ __global__ void __launch_bounds__(DB_THREADS) k_to_db(float *__restrict__ d, uin
 #pragma unroll
   for (int k = 0; k < DB_PER_THREAD; ++k) {  // all loads in flight before any use
     const uint64_t i = base + (uint64_t)k * DB_THREADS + tid;
-    x[k] = i < n ? __ldcs(d + i) : NAN;
+    x[k] = i < n ? (CONVERT ? __ldcs(d + i) : __ldg(d + i)) : NAN;
   }
 #pragma unroll
   for (int k = 0; k < DB_PER_THREAD; ++k) {
     const uint64_t i = base + (uint64_t)k * DB_THREADS + tid;
     float v = x[k];
     if (i >= n || v != v) continue;
-    if (v <= floor_lin) {
-      v = NAN;
-      ++nm;
-    } else {
-      v = 10.0f * log10f(v);
-      ++cv;
+    if (CONVERT) {
+      int cls;
+      v = db_value(v, floor_lin, &cls);
+      if (cls == 1) ++nm;
+      else ++cv;
+      d[i] = v;
     }
-    d[i] = v;
     if (isfinite(v)) {
       mn = fminf(mn, v);
       mx = fmaxf(mx, v);
@@ -248,8 +249,89 @@ struct PinnedBufs {
 
 using namespace sd;
 
+namespace sd {
+namespace {
+
+// compute_db_stats from the dB pass's block partials: min, max and the f64
+// sum in block order; the median of every max(cnt / 100000, 1)-th finite
+// value in element order (k_db_sample) by nth_element on the host.
+int db_stats_parts(sd_ctx *ctx, const float *d, uint64_t n, const std::vector<DbPart> &part, float st[4]) {
+  const uint64_t nb = part.size();
+  double sum = 0.0;
+  uint64_t cnt = 0;
+  float mn = INFINITY, mx = -INFINITY;
+  std::vector<uint64_t> first(nb);
+  for (uint64_t b = 0; b < nb; ++b) {
+    first[b] = cnt;
+    sum += part[b].sum;
+    cnt += part[b].cnt;
+    mn = std::min(mn, part[b].mn);
+    mx = std::max(mx, part[b].mx);
+  }
+  st[0] = st[1] = st[2] = st[3] = NAN;
+  if (cnt == 0) return SD_OK;
+  cudaStream_t s = ctx->stream;
+  const uint64_t stride = std::max<uint64_t>(cnt / 100000, 1);
+  const uint64_t n_sample = (cnt + stride - 1) / stride;
+  uint64_t *d_first;
+  float *d_sample;
+  SD_TRY(scratch_t(ctx, "db.first", nb, &d_first));
+  SD_TRY(scratch_t(ctx, "db.sample", n_sample, &d_sample));
+  SD_CUDA(ctx, cudaMemcpyAsync(d_first, first.data(), nb * 8, cudaMemcpyHostToDevice, s));
+  SD_TIMED_BEGIN(ctx, "k_db_sample");
+  k_db_sample<<<(unsigned)nb, DB_THREADS, 0, s>>>(d, n, d_first, stride, d_sample, n_sample);
+  SD_LAUNCHED(ctx);
+  std::vector<float> sample(n_sample);
+  SD_CUDA(ctx, cudaMemcpyAsync(sample.data(), d_sample, n_sample * 4, cudaMemcpyDeviceToHost, s));
+  SD_TRY(sync(ctx));
+  std::nth_element(sample.begin(), sample.begin() + n_sample / 2, sample.end());
+  st[0] = mn;
+  st[1] = mx;
+  st[2] = (float)(sum / (double)cnt);
+  st[3] = sample[n_sample / 2];
+  return SD_OK;
+}
+
+// The dB pass (CONVERT: to_db_inplace; else the statistics only) over device
+// memory d, its partials copied back.
+template <bool CONVERT>
+int db_pass(sd_ctx *ctx, float *d, uint64_t n, float floor_lin, std::vector<DbPart> *part) {
+  const uint64_t nb = (n + DB_CHUNK - 1) / DB_CHUNK;
+  if (nb > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "raster too large");
+  DbPart *d_part;
+  SD_TRY(scratch_t(ctx, "db.part", nb, &d_part));
+  SD_TIMED_BEGIN(ctx, CONVERT ? "k_to_db" : "k_db_stats");
+  k_to_db<CONVERT><<<(unsigned)nb, DB_THREADS, 0, ctx->stream>>>(d, n, floor_lin, d_part);
+  SD_LAUNCHED(ctx);
+  part->resize(nb);
+  SD_CUDA(ctx, cudaMemcpyAsync(part->data(), d_part, nb * sizeof(DbPart), cudaMemcpyDeviceToHost, ctx->stream));
+  return sync(ctx);
+}
+
+}  // namespace
+
+int db_stats_device(sd_ctx *ctx, const float *d, uint64_t n, float st[4]) {
+  st[0] = st[1] = st[2] = st[3] = NAN;
+  if (n == 0) return SD_OK;
+  std::vector<DbPart> part;
+  SD_TRY(db_pass<false>(ctx, const_cast<float *>(d), n, 0.0f, &part));
+  return db_stats_parts(ctx, d, n, part, st);
+}
+
+int db_finish(sd_ctx *ctx, const float *d_out, uint64_t n, uint64_t converted, uint64_t masked) {
+  ctx->db_valid = false;
+  ctx->db_counts[0] = converted;
+  ctx->db_counts[1] = masked;
+  SD_TRY(db_stats_device(ctx, d_out, n, ctx->db_stats));
+  ctx->db_valid = true;
+  return SD_OK;
+}
+
+}  // namespace sd
+
 extern "C" int sd_to_db(sd_ctx *ctx, float *data, uint64_t n, float noise_floor_linear, uint64_t *counts,
                         float *stats) {
+  SD_STAGE("db_conversion");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!(noise_floor_linear >= 0.0f))
     return set_error(ctx, SD_ERR_EXPORT_INVALID_NOISE_FLOOR, "noise_floor_linear must be non-negative; got %g",
@@ -259,64 +341,18 @@ extern "C" int sd_to_db(sd_ctx *ctx, float *data, uint64_t n, float noise_floor_
   float st[4] = {NAN, NAN, NAN, NAN};
   if (n > 0) {
     SD_CUDA(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = ctx->stream;
     const void *din;
     SD_TRY(stage_in(ctx, "db.data", data, n * sizeof(float), &din));
     float *d = (float *)din;
-    const uint64_t nb = (n + DB_CHUNK - 1) / DB_CHUNK;
-    if (nb > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "raster too large");
-    DbPart *d_part;
-    SD_TRY(scratch_t(ctx, "db.part", nb, &d_part));
-    SD_TIMED_BEGIN(ctx, "k_to_db");
-    k_to_db<<<(unsigned)nb, DB_THREADS, 0, s>>>(d, n, noise_floor_linear, d_part);
-    SD_LAUNCHED(ctx);
-    std::vector<DbPart> part(nb);
-    SD_CUDA(ctx, cudaMemcpyAsync(part.data(), d_part, nb * sizeof(DbPart), cudaMemcpyDeviceToHost, s));
-    SD_TRY(sync(ctx));
+    std::vector<DbPart> part;
+    SD_TRY(db_pass<true>(ctx, d, n, noise_floor_linear, &part));
     for (const DbPart &q : part) {
       cv += q.cv;
       nm += q.nm;
     }
-    if (stats) {
-      double sum = 0.0;
-      uint64_t cnt = 0;
-      float mn = INFINITY, mx = -INFINITY;
-      std::vector<uint64_t> first(nb);
-      for (uint64_t b = 0; b < nb; ++b) {
-        first[b] = cnt;
-        sum += part[b].sum;
-        cnt += part[b].cnt;
-        mn = std::min(mn, part[b].mn);
-        mx = std::max(mx, part[b].mx);
-      }
-      if (cnt > 0) {
-        const uint64_t stride = std::max<uint64_t>(cnt / 100000, 1);
-        const uint64_t n_sample = (cnt + stride - 1) / stride;
-        uint64_t *d_first;
-        float *d_sample;
-        SD_TRY(scratch_t(ctx, "db.first", nb, &d_first));
-        SD_TRY(scratch_t(ctx, "db.sample", n_sample, &d_sample));
-        SD_CUDA(ctx, cudaMemcpyAsync(d_first, first.data(), nb * 8, cudaMemcpyHostToDevice, s));
-        SD_TIMED_BEGIN(ctx, "k_db_sample");
-        k_db_sample<<<(unsigned)nb, DB_THREADS, 0, s>>>(d, n, d_first, stride, d_sample, n_sample);
-        SD_LAUNCHED(ctx);
-        std::vector<float> sample(n_sample);
-        SD_CUDA(ctx, cudaMemcpyAsync(sample.data(), d_sample, n_sample * 4, cudaMemcpyDeviceToHost, s));
-        SD_TRY(finish_out(ctx, data, d, n * sizeof(float)));
-        SD_TRY(sync(ctx));
-        std::nth_element(sample.begin(), sample.begin() + n_sample / 2, sample.end());
-        st[0] = mn;
-        st[1] = mx;
-        st[2] = (float)(sum / (double)cnt);
-        st[3] = sample[n_sample / 2];
-      } else {
-        SD_TRY(finish_out(ctx, data, d, n * sizeof(float)));
-        SD_TRY(sync(ctx));
-      }
-    } else {
-      SD_TRY(finish_out(ctx, data, d, n * sizeof(float)));
-      SD_TRY(sync(ctx));
-    }
+    if (stats) SD_TRY(db_stats_parts(ctx, d, n, part, st));
+    SD_TRY(finish_out(ctx, data, d, n * sizeof(float)));
+    SD_TRY(sync(ctx));
   }
   if (counts) {
     counts[0] = cv;
@@ -326,7 +362,28 @@ extern "C" int sd_to_db(sd_ctx *ctx, float *data, uint64_t n, float noise_floor_
   return SD_OK;
 }
 
+extern "C" int sd_ctx_set_db_output(sd_ctx *ctx, int32_t enable, float noise_floor_linear) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (enable && !(noise_floor_linear >= 0.0f))
+    return set_error(ctx, SD_ERR_EXPORT_INVALID_NOISE_FLOOR, "noise_floor_linear must be non-negative; got %g",
+                     (double)noise_floor_linear);
+  ctx->db_out = enable != 0;
+  ctx->db_floor = enable ? noise_floor_linear : 0.0f;
+  ctx->db_valid = false;
+  return SD_OK;
+}
+
+extern "C" int sd_ctx_db_result(sd_ctx *ctx, uint64_t *counts, float *stats) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!ctx->db_valid)
+    return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "no call with dB output has completed on this context");
+  if (counts) counts[0] = ctx->db_counts[0], counts[1] = ctx->db_counts[1];
+  if (stats) std::memcpy(stats, ctx->db_stats, sizeof ctx->db_stats);
+  return SD_OK;
+}
+
 extern "C" int sd_downsample_2x(sd_ctx *ctx, const float *src, uint64_t cols, uint64_t rows, float *dst) {
+  SD_STAGE("export_overviews");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (cols == 0 || rows == 0) return SD_OK;
   if (!src || !dst) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null buffer");
@@ -346,6 +403,7 @@ extern "C" int sd_downsample_2x(sd_ctx *ctx, const float *src, uint64_t cols, ui
 
 extern "C" int sd_write_cog(sd_ctx *ctx, const char *path, const float *data, uint64_t cols, uint64_t rows,
                             const double *gt, int32_t crs, int32_t utm_zone, uint32_t tile_size) {
+  SD_STAGE("export_geotiff");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!path || !gt) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null path or geotransform");
   const double pw = gt[1], ph = -gt[5];

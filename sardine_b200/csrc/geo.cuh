@@ -439,16 +439,37 @@ SD_HD int dem_sample_cert(const DemView &d, double row_f, double col_f, double e
   uint64_t r0 = (uint64_t)row_f, c0 = (uint64_t)col_f;  // in [1, max - 1]: no clamp applies
   const double dr = row_f - (double)r0;
   const double dc = col_f - (double)c0;
-  if (dr <= eps || dr >= 1.0 - eps || dc <= eps || dc >= 1.0 - eps) return 0;  // a cell edge
   const uint64_t r1 = r0 + 1, c1 = c0 + 1;
 #if defined(__CUDA_ARCH__)
-  const float v00 = __ldg(&d.data[r0 * d.width + c0]), v01 = __ldg(&d.data[r0 * d.width + c1]);
-  const float v10 = __ldg(&d.data[r1 * d.width + c0]), v11 = __ldg(&d.data[r1 * d.width + c1]);
+#define SD_DEM_AT(R, C) __ldg(&d.data[(R) * d.width + (C)])
 #else
-  const float v00 = d.data[r0 * d.width + c0], v01 = d.data[r0 * d.width + c1];
-  const float v10 = d.data[r1 * d.width + c0], v11 = d.data[r1 * d.width + c1];
+#define SD_DEM_AT(R, C) d.data[(R) * d.width + (C)]
 #endif
-  if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) {
+  const float v00 = SD_DEM_AT(r0, c0), v01 = SD_DEM_AT(r0, c1);
+  const float v10 = SD_DEM_AT(r1, c0), v11 = SD_DEM_AT(r1, c1);
+  float lo4 = fminf(fminf(v00, v01), fminf(v10, v11)), hi4 = fmaxf(fmaxf(v00, v01), fmaxf(v10, v11));
+  const bool nan4 = v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11;
+  // Within eps of a cell edge the exact position may fall in the next cell:
+  // row er (r0 - 1 or r0 + 2) and column ec join the corners.  The bilinear
+  // surface is continuous across the edge, so the value either cell gives
+  // differs from this cell's by the corners' spread times eps plus rounding:
+  // the spread is taken over the union.  (Output grids aligned with the DEM
+  // put every lookup on a node, within rounding, so this is the common case.)
+  const int64_t er = dr <= eps ? -1 : (dr >= 1.0 - eps ? 2 : 0);
+  const int64_t ec = dc <= eps ? -1 : (dc >= 1.0 - eps ? 2 : 0);
+  if (er | ec) {
+    if (nan4) return 0;  // a void the other cell may not hold
+    const uint64_t rr = (uint64_t)((int64_t)r0 + er), cc = (uint64_t)((int64_t)c0 + ec);
+    float e0 = v00, e1 = v00, e2 = v00, e3 = v00, e4 = v00;
+    if (er) e0 = SD_DEM_AT(rr, c0), e1 = SD_DEM_AT(rr, c1);
+    if (ec) e2 = SD_DEM_AT(r0, cc), e3 = SD_DEM_AT(r1, cc);
+    if (er && ec) e4 = SD_DEM_AT(rr, cc);
+    if (e0 != e0 || e1 != e1 || e2 != e2 || e3 != e3 || e4 != e4) return 0;
+    lo4 = fminf(lo4, fminf(fminf(e0, e1), fminf(fminf(e2, e3), e4)));
+    hi4 = fmaxf(hi4, fmaxf(fmaxf(e0, e1), fmaxf(fmaxf(e2, e3), e4)));
+  }
+#undef SD_DEM_AT
+  if (nan4) {
     *h = NAN;
     return 1;
   }
@@ -457,7 +478,6 @@ SD_HD int dem_sample_cert(const DemView &d, double row_f, double col_f, double e
   // the value's uncertainty: the corners' spread times the position's
   // uncertainty in both axes, plus the rounding of this sum and of the exact
   // position's (a few ulps of the corner magnitudes)
-  const float lo4 = fminf(fminf(v00, v01), fminf(v10, v11)), hi4 = fmaxf(fmaxf(v00, v01), fmaxf(v10, v11));
   const double dv = 2.0 * ((double)hi4 - (double)lo4) * eps + 8e-15 * fmax(fabs((double)lo4), fabs((double)hi4));
   const float lo = (float)(v - dv), hi = (float)(v + dv);
   if (lo != hi) return 0;
@@ -487,6 +507,24 @@ SD_HD bool dem_at_lonlat_checked(const DemView &d, double lon_deg, double lat_de
   if (dem_sample_cert(d, (d.origin_y - lat_deg) * d.inv_ps, (lon_norm - d.origin_x) * d.inv_ps, 0.0, &inside, h))
     return inside;
   return dem_elevation_exact(d, lat_deg, lon_deg, h);
+}
+
+// The same two lookups without the exact fallback: 1 = inside (*h the
+// height, NaN on a void), 0 = outside the DEM, -1 = undecided (the caller
+// defers the pixel to a pass that runs the checked form).
+SD_HD int dem_at_xy_try(const DemView &d, double x, double y, float *h) {
+  bool inside = false;
+  if (!dem_sample_cert(d, (d.origin_y - y) * d.inv_ps, (x - d.origin_x) * d.inv_ps, kDemPosEps * d.inv_ps, &inside,
+                       h))
+    return -1;
+  return inside ? 1 : 0;
+}
+SD_HD int dem_at_lonlat_try(const DemView &d, double lon_deg, double lat_deg, float *h) {
+  bool inside = false;
+  const double lon_norm = lon_deg >= 180.0 ? lon_deg - 360.0 : lon_deg;
+  if (!dem_sample_cert(d, (d.origin_y - lat_deg) * d.inv_ps, (lon_norm - d.origin_x) * d.inv_ps, 0.0, &inside, h))
+    return -1;
+  return inside ? 1 : 0;
 }
 
 // The reference divides by the pixel size; the product with its reciprocal

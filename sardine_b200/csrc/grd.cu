@@ -113,6 +113,7 @@ extern "C" int sd_to_ground_range(sd_ctx *ctx, const float *data, uint64_t lines
                                   double range_pixel_spacing_m, const sd_grd_swath_grid *grids, int32_t n_grids,
                                   double target_spacing_m, double azimuth_pixel_spacing_m, float *out,
                                   sd_grd_info *info) {
+  SD_STAGE("ground_range_projection");
   if (!ctx || !info) return SD_ERR_INVALID_ARGUMENT;
   if (lines == 0 || samples == 0)
     return set_error(ctx, SD_ERR_GRD_EMPTY_IMAGE, "merged image is empty (%llu lines x %llu samples)",

@@ -305,6 +305,7 @@ using namespace sd;
 extern "C" int sd_resample_secondary(sd_ctx *ctx, const float *sec, uint64_t sec_lines, uint64_t sec_samples,
                                      uint64_t lines, uint64_t samples, const double *az_poly, const double *rg_poly,
                                      float *out) {
+  SD_STAGE("resample_secondary");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!az_poly || !rg_poly) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null polynomial");
   if (samples > 0xffffffffull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "too many samples per line");
@@ -332,6 +333,7 @@ extern "C" int sd_form_interferogram(sd_ctx *ctx, const float *ref, const float 
                                      const sd_state_vector *ref_orbit, uint64_t n_ref, int64_t ref_first_us,
                                      const sd_state_vector *sec_orbit, uint64_t n_sec, double wavelength_m,
                                      uint32_t az_looks, uint32_t rg_looks, float *coherence, float *phase) {
+  SD_STAGE("interferogram");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (az_looks == 0 || rg_looks == 0)
     return set_error(ctx, SD_ERR_INSAR_INVALID_WINDOW_SIZE,
@@ -453,6 +455,7 @@ extern "C" int sd_coreg_offsets(sd_ctx *ctx, const sd_state_vector *ref_orbit, u
                                 int64_t sec_first_us, double sec_azimuth_time_interval_s,
                                 double sec_slant_range_time_s, double sec_range_pixel_spacing_m,
                                 uint64_t sec_first_sample, sd_coreg_result *out) {
+  SD_STAGE("coreg_offsets");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!ref_orbit || !sec_orbit || !out) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null argument");
   SD_CUDA(ctx, cudaSetDevice(ctx->device));

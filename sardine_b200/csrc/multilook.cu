@@ -40,6 +40,7 @@ using namespace sd;
 
 extern "C" int sd_multilook(sd_ctx *ctx, const float *data, const float *nesz, uint64_t lines, uint64_t samples,
                             uint32_t range_looks, uint32_t azimuth_looks, float *out_data, float *out_nesz) {
+  SD_STAGE("multilook");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (range_looks == 0 || azimuth_looks == 0)
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "multilook factors must be >= 1 (range=%u, azimuth=%u)",

@@ -1,7 +1,46 @@
 // runtime.cu — context lifecycle, error reporting and staging.
 #include "runtime.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
+#include <chrono>
+#include <cstdlib>
+
 namespace sd {
+
+namespace {
+bool timing_log_on() {
+  static const bool on = [] {
+    const char *e = std::getenv("SARDINE_B200_TIMING");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
+
+StageScope::StageScope(const char *stage) : name(stage), t0(0.0), log(timing_log_on()) {
+  nvtxRangePushA(stage);
+  if (log) t0 = now_s();
+}
+
+StageScope::~StageScope() {
+  nvtxRangePop();
+  if (log) std::fprintf(stderr, "[timing] %s = %.3f s\n", name, now_s() - t0);
+}
+
+void log_newton_hist(const unsigned long long *hist, int n) {
+  if (!timing_log_on() || !hist) return;
+  unsigned long long total = 0;
+  for (int i = 0; i < n; ++i) total += hist[i];
+  if (total == 0) return;
+  std::string parts;
+  for (int i = 1; i < n; ++i)
+    if (hist[i]) parts += (parts.empty() ? "" : " ") + std::to_string(i) + "=" + std::to_string(hist[i]);
+  std::fprintf(stderr, "[timing] newton_iter_hist (total=%llu): %s\n", total, parts.c_str());
+}
 
 int set_error(sd_ctx *ctx, int code, const char *fmt, ...) {
   if (ctx) {

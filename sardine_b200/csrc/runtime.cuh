@@ -56,11 +56,59 @@ struct sd_ctx {
     uint64_t launches;  // kernels per replay
   };
   std::unordered_map<int, GraphRec> graph_exec;
+  // dB output fused into the producing kernels (sd_ctx_set_db_output): the
+  // terrain correction and the speckle filter write 10 log10 v, and the
+  // counts and statistics of the last such call are kept for sd_ctx_db_result
+  bool db_out = false;
+  float db_floor = 0.0f;
+  bool db_valid = false;
+  uint64_t db_counts[2] = {0, 0};  // converted, noise-masked
+  float db_stats[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 };
 
 namespace sd {
 
 int set_error(sd_ctx *ctx, int code, const char *fmt, ...);
+
+// One call of an entry point as a stage of the reference's pipeline, under
+// the reference's [timing] stage name (run.rs:54-60, scene_prep.rs:680-700):
+// an NVTX range for profilers (nvtx3 is header-only and costs nothing when
+// no tool is attached) and, when SARDINE_B200_TIMING=1 is set, the
+// reference's "[timing] <stage> = <s> s" line on stderr when the call
+// returns (wall clock; the entry points synchronise before returning).
+struct StageScope {
+  const char *name;
+  double t0;
+  bool log;
+  explicit StageScope(const char *stage);
+  ~StageScope();
+};
+// The reference's Newton histogram line (run.rs:319-339), when logging.
+void log_newton_hist(const unsigned long long *hist, int n);
+
+// to_db_inplace (export.rs:80-90) on one value: NaN stays NaN (*cls -1);
+// v <= floor_lin becomes NaN (*cls 1, noise-masked); anything else becomes
+// 10 log10 v (*cls 0, converted).
+__device__ __forceinline__ float db_value(float v, float floor_lin, int *cls) {
+  if (v != v) {
+    *cls = -1;
+    return v;
+  }
+  if (v <= floor_lin) {
+    *cls = 1;
+    return __int_as_float(0x7fc00000);
+  }
+  *cls = 0;
+  return 10.0f * log10f(v);
+}
+
+// compute_db_stats (run.rs:63-97) of the device raster d[0..n) into st:
+// {min, max, mean, median}, NaN when no value is finite (export.cu).
+int db_stats_device(sd_ctx *ctx, const float *d, uint64_t n, float st[4]);
+// After a producing call that wrote dB values: the counts (from the
+// kernels' counters) and the statistics of the device raster d_out.
+int db_finish(sd_ctx *ctx, const float *d_out, uint64_t n, uint64_t converted, uint64_t masked);
+#define SD_STAGE(stage) ::sd::StageScope sd_stage_scope__(stage)
 
 #define SD_CUDA(ctx, call)                                                               \
   do {                                                                                   \

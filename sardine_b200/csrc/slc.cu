@@ -219,6 +219,7 @@ extern "C" void sd_slc_close(sd_slc_reader *r) {
 
 extern "C" int sd_slc_read_burst_raw(sd_ctx *ctx, sd_slc_reader *r, uint64_t first_line, uint64_t line_count,
                                      int16_t *out) {
+  SD_STAGE("read_burst");
   if (!ctx || !r) return SD_ERR_INVALID_ARGUMENT;
   if (first_line > r->height || line_count > (uint64_t)r->height - first_line)
     return set_error(ctx, SD_ERR_SLC_LINE_OUT_OF_BOUNDS, "line range [%llu, %llu) is out of image bounds [0, %u)",

@@ -1,12 +1,15 @@
 // speckle.cu — the five SpeckleKernel filters on sm_100a.
 //
 // Replaces apply_speckle_filter / SpeckleKernel::apply (sardine/src/speckle.rs:
-// 131-180, 218-569, 586-603).  One thread per output pixel; the block's
-// window footprint (tile + halo) is staged once in shared memory, out-of-image
-// cells stored as NaN so the reference's "in bounds and finite" filter is a
-// single isfinite test.  Window sums are accumulated in f64 in the
-// reference's row-major tap order and cast to f32 exactly as speckle.rs:
-// 226-240 does, so the f32 filter arithmetic sees the same inputs.
+// 131-180, 218-569, 586-603).  A thread owns SP_ROWS outputs of one column;
+// the block's window footprint (tile + halo) is staged once in shared memory,
+// out-of-image cells stored as NaN so the reference's "in bounds and finite"
+// filter is a single isfinite test.  Window sums are accumulated in f64 in
+// the reference's row-major tap order (each tap converted once and added to
+// every output of the thread whose window holds it) and cast to f32 exactly
+// as speckle.rs:226-240 does, so the f32 filter arithmetic sees the same
+// inputs.  The sums are sequential per output, so neither a sliding window
+// nor a shuffle tree (which re-associates the adds) would reproduce them.
 #include <cmath>
 
 #include "geo.cuh"
@@ -18,45 +21,6 @@ namespace {
 
 constexpr int TX = 32, TY = 8;
 
-// Refined Lee directional masks (speckle.rs:432-457) as row-major tap lists.
-struct RlMasks {
-  int8_t n[8];
-  int8_t dy[8][24];
-  int8_t dx[8][24];
-};
-__constant__ RlMasks c_rl;
-
-bool rl_in_mask(int dir, int dy, int dx) {
-  if (dy == 0 && dx == 0) return false;
-  switch (dir) {
-    case 0: return dy >= 1 && dy <= 3;
-    case 1: return dy >= -3 && dy <= -1;
-    case 2: return dx >= 1 && dx <= 3;
-    case 3: return dx >= -3 && dx <= -1;
-    case 4: return std::abs(dy - dx) <= 1 && (dy + dx) >= 1;
-    case 5: return std::abs(dy - dx) <= 1 && (dy + dx) <= -1;
-    case 6: return std::abs(dy + dx) <= 1 && (dx - dy) >= 1;
-    case 7: return std::abs(dy + dx) <= 1 && (dx - dy) <= -1;
-  }
-  return false;
-}
-
-RlMasks make_masks() {
-  RlMasks m{};
-  for (int d = 0; d < 8; ++d) {
-    int k = 0;
-    for (int dy = -3; dy <= 3; ++dy)
-      for (int dx = -3; dx <= 3; ++dx)
-        if (rl_in_mask(d, dy, dx)) {
-          m.dy[d][k] = (int8_t)dy;
-          m.dx[d][k] = (int8_t)dx;
-          ++k;
-        }
-    m.n[d] = (int8_t)k;
-  }
-  return m;
-}
-
 struct SpParams {
   const float *in;
   float *out;
@@ -64,6 +28,9 @@ struct SpParams {
   int half;
   int kind;
   float enl, damping, cv_n_sq, cv_max_sq;
+  int db;                    // write the filtered value in dB (to_db_inplace)
+  float db_floor;
+  unsigned long long *dbc;   // db: converted, noise-masked counts
 };
 
 __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
@@ -79,43 +46,7 @@ __device__ float speckle_px(const float *tile, int tw, int lx, int ly, int h, co
   const float centre = tile[ly * tw + lx];
   float o = NAN;
   if (!finitef(centre)) return o;
-  if (KIND == SD_SPECKLE_REFINED_LEE) {
-    float best_cv = INFINITY, best_mean = centre, best_var = 0.0f;
-    for (int d = 0; d < 8; ++d) {
-      double sum = 0.0, sum_sq = 0.0;
-      int n = 0;
-      const int nt = c_rl.n[d];
-      for (int k = 0; k < nt; ++k) {
-        float v = tile[(ly + c_rl.dy[d][k]) * tw + lx + c_rl.dx[d][k]];
-        if (!finitef(v)) continue;
-        double vd = (double)v;
-        sum += vd;
-        sum_sq += vd * vd;
-        ++n;
-      }
-      if (n == 0) continue;
-      double md = sum / (double)n;
-      double vard = maxd_nan(sum_sq / (double)n - md * md, 0.0);
-      float mean = (float)md, var = (float)vard;
-      if (!(mean > 0.0f)) continue;
-      float cv = var / (mean * mean);
-      if (cv < best_cv) {
-        best_cv = cv;
-        best_mean = mean;
-        best_var = var;
-      }
-    }
-    if (!isfinite(best_cv)) {
-      o = centre;
-    } else {
-      float noise_var = best_mean * best_mean * p.cv_n_sq;
-      float signal_var = maxf_nan(best_var - noise_var, 0.0f);
-      float denom = signal_var + noise_var;
-      float k = denom > 0.0f ? signal_var / denom : 0.0f;
-      o = best_mean + k * (centre - best_mean);
-    }
-    return o;
-  }
+  static_assert(KIND != SD_SPECKLE_REFINED_LEE, "Refined Lee: rl_rows");
   double sum = 0.0, sum_sq = 0.0;
   int n = 0;
   for (int dy = -h; dy <= h; ++dy) {
@@ -173,12 +104,248 @@ __device__ float speckle_px(const float *tile, int tw, int lx, int ly, int h, co
   return o;
 }
 
+// ── several outputs per thread ────────────────────────────────────────────────
+// A thread owns SP_ROWS outputs of one column.  Each staged tap is converted
+// to f64 (and squared) once and added to every one of those outputs whose
+// window holds it; an output still receives its taps in the reference's
+// row-major order.  A tap the reference skips (outside the image, or not
+// finite) adds -0.0, which leaves every IEEE sum unchanged (x + -0.0 == x,
+// also for x == +0.0), so the sums are bit-identical to the filtered loop
+// while the add sequence stays the same for every lane.
+constexpr int SP_ROWS = 2;
+// slots of the context's device counters that hold sd_speckle's dB counts
+constexpr int SP_DB_COUNTERS = 48;
+// largest tile-batch block (Refined Lee holds 2 x 8 directional sums per thread)
+constexpr int SP_MAX_THREADS = 512;
+
+template <int R>
+struct WinAcc {
+  double s[R], q[R];
+  int n[R];
+};
+
+__device__ __forceinline__ void tap_f64(float v, bool &f, double &d, double &q) {
+  f = isfinite(v);
+  d = f ? (double)v : -0.0;
+  q = f ? d * d : -0.0;
+}
+
+// the w taps of one window row into outputs LO..HI
+template <int R, int LO, int HI>
+__device__ __forceinline__ void win_row(WinAcc<R> &a, const float *row, int w) {
+  int nf = 0;
+  for (int x = 0; x < w; ++x) {
+    bool f;
+    double d, q;
+    tap_f64(row[x], f, d, q);
+    nf += f;
+#pragma unroll
+    for (int r = LO; r <= HI; ++r) {
+      a.s[r] += d;
+      a.q[r] += q;
+    }
+  }
+#pragma unroll
+  for (int r = LO; r <= HI; ++r) a.n[r] += nf;
+}
+
+// outputs lo..hi with a runtime range (predicated adds; ranges strictly
+// inside 0..R-1 only, which windows smaller than the thread's rows produce)
+template <int R>
+__device__ __forceinline__ void win_row_any(int lo, int hi, WinAcc<R> &a, const float *row, int w) {
+  int nf = 0;
+  for (int x = 0; x < w; ++x) {
+    bool f;
+    double d, q;
+    tap_f64(row[x], f, d, q);
+    nf += f;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (r >= lo && r <= hi) {
+        a.s[r] += d;
+        a.q[r] += q;
+      }
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+    if (r >= lo && r <= hi) a.n[r] += nf;
+}
+
+template <int R, int K = 0>
+__device__ __forceinline__ void win_prefix(int hi, WinAcc<R> &a, const float *row, int w) {
+  if (hi == K) return win_row<R, 0, K>(a, row, w);
+  if constexpr (K + 1 < R) win_prefix<R, K + 1>(hi, a, row, w);
+}
+template <int R, int K = 1>
+__device__ __forceinline__ void win_suffix(int lo, WinAcc<R> &a, const float *row, int w) {
+  if constexpr (K < R) {
+    if (lo == K) return win_row<R, K, R - 1>(a, row, w);
+    win_suffix<R, K + 1>(lo, a, row, w);
+  }
+}
+
+// Window sums of outputs (ly0 + r, lx), r < R, over a (2h+1)^2 window of
+// the staged tile (row stride tw).  Window row k (tile row ly0 - h + k)
+// feeds outputs max(0, k - 2h) .. min(R - 1, k).
+template <int R>
+__device__ __forceinline__ void win_stats(const float *tile, int tw, int lx, int ly0, int h, WinAcc<R> &a) {
+#pragma unroll
+  for (int r = 0; r < R; ++r) a.s[r] = a.q[r] = 0.0, a.n[r] = 0;
+  const int w = 2 * h + 1;
+  for (int k = 0; k < R + 2 * h; ++k) {
+    const int lo = k - 2 * h > 0 ? k - 2 * h : 0, hi = k < R - 1 ? k : R - 1;
+    const float *row = tile + (ly0 - h + k) * tw + lx - h;
+    if (lo == 0) win_prefix<R>(hi, a, row, w);
+    else if (hi == R - 1) win_suffix<R>(lo, a, row, w);
+    else win_row_any<R>(lo, hi, a, row, w);
+  }
+}
+
+// The filter of KIND (not Refined Lee, not Frost) from one output's window
+// sums, as speckle_px forms it.
+template <int KIND>
+__device__ __forceinline__ float filt_stats(float centre, double sum, double sum_sq, int n, const SpCoef &p) {
+  if (!finitef(centre) || n == 0) return NAN;
+  const double md = sum / (double)n;
+  const double vard = maxd_nan(sum_sq / (double)n - md * md, 0.0);
+  const float mean = (float)md, var = (float)vard;
+  if (KIND == SD_SPECKLE_BOXCAR) return mean;
+  if (KIND == SD_SPECKLE_LEE) {
+    const float noise_var = mean * mean * p.cv_n_sq;
+    const float signal_var = maxf_nan(var - noise_var, 0.0f);
+    const float denom = signal_var + noise_var;
+    const float k = denom > 0.0f ? signal_var / denom : 0.0f;
+    return mean + k * (centre - mean);
+  }
+  // Gamma-MAP (speckle.rs:348-411)
+  const float cv_sq = mean > 0.0f ? var / (mean * mean) : 0.0f;
+  if (cv_sq <= p.cv_n_sq) return mean;
+  if (cv_sq >= p.cv_max_sq) return centre;
+  const float alpha = (1.0f + p.cv_n_sq) / (cv_sq - p.cv_n_sq);
+  const float b = (alpha - p.enl - 1.0f) * mean;
+  const float disc = b * b + 4.0f * alpha * p.enl * mean * centre;
+  return disc >= 0.0f ? ((p.enl - alpha + 1.0f) * mean + sqrtf(disc)) / (2.0f * p.enl) : mean;
+}
+
+// Refined Lee masks (speckle.rs:432-457) at compile time.
+__host__ __device__ constexpr bool rl_mask(int d, int dy, int dx) {
+  if (dy == 0 && dx == 0) return false;
+  const int a = dy - dx < 0 ? dx - dy : dy - dx, b = dy + dx < 0 ? -(dy + dx) : dy + dx;
+  switch (d) {
+    case 0: return dy >= 1 && dy <= 3;
+    case 1: return dy >= -3 && dy <= -1;
+    case 2: return dx >= 1 && dx <= 3;
+    case 3: return dx >= -3 && dx <= -1;
+    case 4: return a <= 1 && (dy + dx) >= 1;
+    case 5: return a <= 1 && (dy + dx) <= -1;
+    case 6: return b <= 1 && (dx - dy) >= 1;
+    case 7: return b <= 1 && (dx - dy) <= -1;
+  }
+  return false;
+}
+// bit x (dx = x - 3) of window row dy in direction d
+__host__ __device__ constexpr uint32_t rl_rowbits(int d, int dy) {
+  uint32_t m = 0;
+  for (int x = 0; x < 7; ++x)
+    if (rl_mask(d, dy, x - 3)) m |= 1u << x;
+  return m;
+}
+
+// Refined Lee for outputs (ly0 + r, lx), r < R: the 8 directional sums of
+// every output in one pass over the R + 6 staged rows (all membership tests
+// resolved at compile time), the counts from per-row finite bits.
+template <int R>
+__device__ __forceinline__ void rl_rows(const float *tile, int tw, int lx, int ly0, const SpCoef &p, float *o) {
+  double s[R][8], q[R][8];
+  uint32_t fin[R + 6];
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int d = 0; d < 8; ++d) s[r][d] = q[r][d] = 0.0;
+#pragma unroll
+  for (int k = 0; k < R + 6; ++k) {
+    const float *row = tile + (ly0 - 3 + k) * tw + lx - 3;
+    uint32_t bits = 0;
+#pragma unroll
+    for (int x = 0; x < 7; ++x) {
+      bool f;
+      double dv, qv;
+      tap_f64(row[x], f, dv, qv);
+      bits |= (uint32_t)f << x;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int dy = k - 3 - r;
+        if (dy < -3 || dy > 3) continue;
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+          if (rl_mask(d, dy, x - 3)) {
+            s[r][d] += dv;
+            q[r][d] += qv;
+          }
+      }
+    }
+    fin[k] = bits;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const float centre = tile[(ly0 + r) * tw + lx];
+    if (!finitef(centre)) {
+      o[r] = NAN;
+      continue;
+    }
+    float best_cv = INFINITY, best_mean = centre, best_var = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+      int n = 0;
+#pragma unroll
+      for (int dy = -3; dy <= 3; ++dy) n += __popc(fin[r + 3 + dy] & rl_rowbits(d, dy));
+      if (n == 0) continue;
+      const double md = s[r][d] / (double)n;
+      const double vard = maxd_nan(q[r][d] / (double)n - md * md, 0.0);
+      const float mean = (float)md, var = (float)vard;
+      if (!(mean > 0.0f)) continue;
+      const float cv = var / (mean * mean);
+      if (cv < best_cv) {
+        best_cv = cv;
+        best_mean = mean;
+        best_var = var;
+      }
+    }
+    if (!isfinite(best_cv)) {
+      o[r] = centre;
+    } else {
+      const float noise_var = best_mean * best_mean * p.cv_n_sq;
+      const float signal_var = maxf_nan(best_var - noise_var, 0.0f);
+      const float denom = signal_var + noise_var;
+      const float k = denom > 0.0f ? signal_var / denom : 0.0f;
+      o[r] = best_mean + k * (centre - best_mean);
+    }
+  }
+}
+
+// SP_ROWS outputs (ly0 + r, lx) of filter KIND from the staged tile.
+template <int KIND>
+__device__ __forceinline__ void speckle_rows(const float *tile, int tw, int lx, int ly0, int h, const SpCoef &p,
+                                             float *o) {
+  if (KIND == SD_SPECKLE_REFINED_LEE) {
+    rl_rows<SP_ROWS>(tile, tw, lx, ly0, p, o);
+  } else if (KIND == SD_SPECKLE_FROST) {  // per-output weights: one output at a time
+#pragma unroll
+    for (int r = 0; r < SP_ROWS; ++r) o[r] = speckle_px<SD_SPECKLE_FROST>(tile, tw, lx, ly0 + r, h, p);
+  } else {
+    WinAcc<SP_ROWS> a;
+    win_stats<SP_ROWS>(tile, tw, lx, ly0, h, a);
+#pragma unroll
+    for (int r = 0; r < SP_ROWS; ++r) o[r] = filt_stats<KIND>(tile[(ly0 + r) * tw + lx], a.s[r], a.q[r], a.n[r], p);
+  }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
   extern __shared__ float tile[];
   const int h = p.half;
-  const int tw = TX + 2 * h, th = TY + 2 * h;
-  const int64_t c0 = (int64_t)blockIdx.x * TX - h, r0 = (int64_t)blockIdx.y * TY - h;
+  const int tw = TX + 2 * h, th = TY * SP_ROWS + 2 * h;
+  const int64_t c0 = (int64_t)blockIdx.x * TX - h, r0 = (int64_t)blockIdx.y * (TY * SP_ROWS) - h;
   for (int k = threadIdx.y * TX + threadIdx.x; k < tw * th; k += TX * TY) {
     int ty = k / tw, tx = k % tw;
     int64_t rr = r0 + ty, cc = c0 + tx;
@@ -187,10 +354,30 @@ __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
     tile[k] = v;
   }
   __syncthreads();
-  const int64_t c = (int64_t)blockIdx.x * TX + threadIdx.x, r = (int64_t)blockIdx.y * TY + threadIdx.y;
+  // this thread: column c, rows r .. r + SP_ROWS - 1
+  const int64_t c = (int64_t)blockIdx.x * TX + threadIdx.x;
+  const int64_t r = (int64_t)blockIdx.y * (TY * SP_ROWS) + threadIdx.y * SP_ROWS;
   if (c >= p.cols || r >= p.rows) return;
   const SpCoef cf{p.enl, p.damping, p.cv_n_sq, p.cv_max_sq};
-  p.out[r * p.cols + c] = speckle_px<KIND>(tile, tw, threadIdx.x + h, threadIdx.y + h, h, cf);
+  float o[SP_ROWS];
+  speckle_rows<KIND>(tile, tw, threadIdx.x + h, threadIdx.y * SP_ROWS + h, h, cf, o);
+  unsigned ncv = 0, nnm = 0;
+#pragma unroll
+  for (int k = 0; k < SP_ROWS; ++k)
+    if (r + k < p.rows) {
+      float v = o[k];
+      if (p.db) {  // the dB conversion of the filtered raster, in this epilogue
+        int dc;
+        v = db_value(v, p.db_floor, &dc);
+        ncv += dc == 0;
+        nnm += dc == 1;
+      }
+      p.out[(r + k) * p.cols + c] = v;
+    }
+  if (p.db) {
+    if (ncv) atomicAdd(p.dbc, (unsigned long long)ncv);
+    if (nnm) atomicAdd(p.dbc + 1, (unsigned long long)nnm);
+  }
 }
 
 // ── batched form: many tiles, each a halo'd geocoded raster ──────────────────
@@ -199,7 +386,7 @@ __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
 // tile's halo'd raster (cells outside it are NaN, which the filters skip like
 // out-of-image cells), filters the data plane with the tile's kind (or
 // copies it when kind < 0) and crops cos(LIA) and the mask.
-__global__ void __launch_bounds__(1024) k_speckle_tiles(const SpWork *__restrict__ wp) {
+__global__ void __launch_bounds__(SP_MAX_THREADS) k_speckle_tiles(const SpWork *__restrict__ wp) {
   extern __shared__ float tile[];
   const SpWork w = *wp;
   const int bx = (int)blockDim.x, by = (int)blockDim.y, nt = bx * by;
@@ -217,10 +404,11 @@ __global__ void __launch_bounds__(1024) k_speckle_tiles(const SpWork *__restrict
     const int64_t nbx = (jb.cols + bx - 1) / bx;
     const int64_t tr = (int64_t)li / nbx, tc = (int64_t)li % nbx;
     const int h = jb.kind >= 0 ? jb.half : 0;
-    const int tw = bx + 2 * h, th = by + 2 * h;
+    const int tw = bx + 2 * h, th = by * SP_ROWS + 2 * h;
     const int64_t in_cols = jb.cols + 2 * jb.halo, in_rows = jb.rows + 2 * jb.halo;
-    // output (r, c) is input (r + halo, c + halo)
-    const int64_t c0 = tc * bx + jb.halo - h, r0 = tr * by + jb.halo - h;
+    // output (r, c) is input (r + halo, c + halo); the block covers bx
+    // columns and by * SP_ROWS rows
+    const int64_t c0 = tc * bx + jb.halo - h, r0 = tr * by * SP_ROWS + jb.halo - h;
     __syncthreads();
     for (int k = tid; k < tw * th; k += nt) {
       const int ty = k / tw, tx = k % tw;
@@ -230,39 +418,35 @@ __global__ void __launch_bounds__(1024) k_speckle_tiles(const SpWork *__restrict
       tile[k] = v;
     }
     __syncthreads();
-    const int64_t c = tc * bx + threadIdx.x, r = tr * by + threadIdx.y;
+    // this thread: column c, rows r .. r + SP_ROWS - 1
+    const int64_t c = tc * bx + threadIdx.x, r = (tr * by + threadIdx.y) * SP_ROWS;
     if (c < jb.cols && r < jb.rows) {
       const SpCoef cf{jb.enl, jb.damping, jb.cv_n_sq, jb.cv_max_sq};
-      const int lx = threadIdx.x + h, ly = threadIdx.y + h;
-      float o;
+      const int lx = threadIdx.x + h, ly = threadIdx.y * SP_ROWS + h;
+      float o[SP_ROWS];
       switch (jb.kind) {
-        case SD_SPECKLE_BOXCAR: o = speckle_px<SD_SPECKLE_BOXCAR>(tile, tw, lx, ly, h, cf); break;
-        case SD_SPECKLE_LEE: o = speckle_px<SD_SPECKLE_LEE>(tile, tw, lx, ly, h, cf); break;
-        case SD_SPECKLE_FROST: o = speckle_px<SD_SPECKLE_FROST>(tile, tw, lx, ly, h, cf); break;
-        case SD_SPECKLE_GAMMA_MAP: o = speckle_px<SD_SPECKLE_GAMMA_MAP>(tile, tw, lx, ly, h, cf); break;
-        case SD_SPECKLE_REFINED_LEE: o = speckle_px<SD_SPECKLE_REFINED_LEE>(tile, tw, lx, ly, h, cf); break;
-        default: o = tile[ly * tw + lx];
+        case SD_SPECKLE_BOXCAR: speckle_rows<SD_SPECKLE_BOXCAR>(tile, tw, lx, ly, h, cf, o); break;
+        case SD_SPECKLE_LEE: speckle_rows<SD_SPECKLE_LEE>(tile, tw, lx, ly, h, cf, o); break;
+        case SD_SPECKLE_FROST: speckle_rows<SD_SPECKLE_FROST>(tile, tw, lx, ly, h, cf, o); break;
+        case SD_SPECKLE_GAMMA_MAP: speckle_rows<SD_SPECKLE_GAMMA_MAP>(tile, tw, lx, ly, h, cf, o); break;
+        case SD_SPECKLE_REFINED_LEE: speckle_rows<SD_SPECKLE_REFINED_LEE>(tile, tw, lx, ly, h, cf, o); break;
+        default:
+#pragma unroll
+          for (int k = 0; k < SP_ROWS; ++k) o[k] = tile[(ly + k) * tw + lx];
       }
-      const int64_t oi = r * jb.cols + c, ii = (r + jb.halo) * in_cols + (c + jb.halo);
-      jb.out[oi] = o;
-      if (jb.cos_out) jb.cos_out[oi] = __ldg(jb.cos_in + ii);
-      if (jb.mask_out) jb.mask_out[oi] = __ldg(jb.mask_in + ii);
+#pragma unroll
+      for (int k = 0; k < SP_ROWS; ++k) {
+        if (r + k >= jb.rows) break;
+        const int64_t oi = (r + k) * jb.cols + c, ii = (r + k + jb.halo) * in_cols + (c + jb.halo);
+        jb.out[oi] = o[k];
+        if (jb.cos_out) jb.cos_out[oi] = __ldg(jb.cos_in + ii);
+        if (jb.mask_out) jb.mask_out[oi] = __ldg(jb.mask_in + ii);
+      }
     }
   }
 }
 
-bool g_masks_uploaded[64] = {false};
-
 }  // namespace
-
-int speckle_masks(sd_ctx *ctx) {
-  if (!g_masks_uploaded[ctx->device & 63]) {
-    RlMasks m = make_masks();
-    SD_CUDA(ctx, cudaMemcpyToSymbol(c_rl, &m, sizeof m));
-    g_masks_uploaded[ctx->device & 63] = true;
-  }
-  return SD_OK;
-}
 
 void speckle_coefs(int kind, uint64_t window, float enl, float damping, SpJob *j) {
   const uint64_t win = kind == SD_SPECKLE_REFINED_LEE ? 7 : window;
@@ -275,12 +459,11 @@ void speckle_coefs(int kind, uint64_t window, float enl, float damping, SpJob *j
 }
 
 bool speckle_shape_ok(int tx, int ty) {
-  return tx >= 8 && ty >= 1 && tx <= 256 && tx * ty <= 1024 && (tx * ty) % 32 == 0;
+  return tx >= 8 && ty >= 1 && tx <= 256 && tx * ty <= SP_MAX_THREADS && (tx * ty) % 32 == 0;
 }
 
 int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool full_grid, int tx, int ty) {
-  SD_TRY(speckle_masks(ctx));
-  const size_t smem = (size_t)(tx + 2 * SP_MAX_HALF) * (ty + 2 * SP_MAX_HALF) * sizeof(float);
+  const size_t smem = (size_t)(tx + 2 * SP_MAX_HALF) * (ty * SP_ROWS + 2 * SP_MAX_HALF) * sizeof(float);
   const unsigned g = persistent_grid(k_speckle_tiles, tx * ty, smem, full_grid ? ~0ull : total);
   SD_TIMED_BEGIN(ctx, "k_speckle_tiles");
   k_speckle_tiles<<<g, dim3(tx, ty), smem, ctx->stream>>>(d_work);
@@ -289,7 +472,7 @@ int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool
 }
 
 uint64_t speckle_tile_items(const SpJob &j, int tx, int ty) {
-  return (uint64_t)((j.cols + tx - 1) / tx) * (uint64_t)((j.rows + ty - 1) / ty);
+  return (uint64_t)((j.cols + tx - 1) / tx) * (uint64_t)((j.rows + ty * SP_ROWS - 1) / (ty * SP_ROWS));
 }
 
 // Validation in the reference's order (speckle.rs:137-178).
@@ -311,7 +494,6 @@ int speckle_validate(uint64_t len, uint64_t cols, uint64_t rows, int kind, uint6
 int speckle_launch(sd_ctx *ctx, const float *d_in, float *d_out, uint64_t cols, uint64_t rows,
                    int kind, uint64_t window, float enl, float damping, cudaStream_t st) {
   if (cols == 0 || rows == 0) return SD_OK;
-  SD_TRY(speckle_masks(ctx));
   uint64_t win = kind == SD_SPECKLE_REFINED_LEE ? 7 : window;
   SpParams p;
   p.in = d_in;
@@ -324,11 +506,15 @@ int speckle_launch(sd_ctx *ctx, const float *d_in, float *d_out, uint64_t cols, 
   p.damping = damping;
   p.cv_n_sq = 1.0f / enl;
   p.cv_max_sq = p.cv_n_sq < 1.0f ? 2.0f * p.cv_n_sq / (1.0f - p.cv_n_sq) : INFINITY;
+  p.db = ctx->db_out;
+  p.db_floor = ctx->db_floor;
+  p.dbc = ctx->d_counters + SP_DB_COUNTERS;
+  if (p.db) SD_CUDA(ctx, cudaMemsetAsync(p.dbc, 0, 2 * sizeof(unsigned long long), st));
   const int h = p.half;
-  size_t smem = (size_t)(TX + 2 * h) * (TY + 2 * h) * sizeof(float);
+  size_t smem = (size_t)(TX + 2 * h) * (TY * SP_ROWS + 2 * h) * sizeof(float);
   if (smem > 200 * 1024)
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "speckle window %llu too large", (unsigned long long)win);
-  dim3 grid((unsigned)((cols + TX - 1) / TX), (unsigned)((rows + TY - 1) / TY));
+  dim3 grid((unsigned)((cols + TX - 1) / TX), (unsigned)((rows + TY * SP_ROWS - 1) / (TY * SP_ROWS)));
   dim3 block(TX, TY);
   switch (kind) {
 #define SD_LAUNCH_SPECKLE(K)                                                                 \
@@ -356,6 +542,7 @@ using namespace sd;
 extern "C" int sd_speckle(sd_ctx *ctx, const float *data, uint64_t data_len, uint64_t cols,
                           uint64_t rows, int32_t kind, uint64_t window, float enl, float damping,
                           float *out) {
+  SD_STAGE("speckle");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   int rc = speckle_validate(data_len, cols, rows, kind, window, enl, damping);
   if (rc != SD_OK) {
@@ -383,6 +570,13 @@ extern "C" int sd_speckle(sd_ctx *ctx, const float *data, uint64_t data_len, uin
   SD_TRY(stage_out(ctx, "sp.out", out, data_len * sizeof(float), &d_out));
   SD_TRY(speckle_launch(ctx, (const float *)d_in, (float *)d_out, cols, rows, kind, window, enl,
                         damping, ctx->stream));
+  if (ctx->db_out) {
+    unsigned long long c[2];
+    SD_CUDA(ctx, cudaMemcpyAsync(c, ctx->d_counters + SP_DB_COUNTERS, sizeof c, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    SD_TRY(sync(ctx));
+    SD_TRY(db_finish(ctx, (const float *)d_out, data_len, c[0], c[1]));
+  }
   SD_TRY(finish_out(ctx, out, d_out, data_len * sizeof(float)));
   return sync(ctx);
 }

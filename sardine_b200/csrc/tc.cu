@@ -274,6 +274,8 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   p.az_time = (int64_t *)d_times;
   p.flags = ctx->d_flags;
   p.counters = ctx->d_counters;
+  p.db = ctx->db_out;
+  p.db_floor = ctx->db_floor;
   SD_CUDA(ctx, cudaMemsetAsync(ctx->d_flags, 0, 64 * sizeof(int), st));
   SD_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 64 * sizeof(unsigned long long), st));
   // The candidate-set scheme needs tol <= 1 us (then at most three
@@ -326,6 +328,8 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
                      "orbit interpolation failed: interpolation time outside orbit window; "
                      "refusing to extrapolate");
   }
+  // dB output: the statistics of the converted raster while it is on the device
+  if (p.db) SD_TRY(db_finish(ctx, (const float *)d_out, npx, cnt[kCntDb], cnt[kCntDb + 1]));
   SD_TRY(finish_out(ctx, out_data, d_out, npx * sizeof(float)));
   if (p.compute_lia) {
     SD_TRY(finish_out(ctx, out_cos_lia, d_cos, npx * sizeof(float)));
@@ -340,6 +344,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   info->flat_masked_count = cnt[5];
   info->noise_masked_count = cnt[6];
   for (int k = 0; k < SD_NEWTON_ITER_HIST_SIZE; ++k) info->newton_iter_histogram[k] = cnt[kCounters + k];
+  log_newton_hist(cnt + kCounters, SD_NEWTON_ITER_HIST_SIZE);
   info->diag_exact_path_pixels = (uint64_t)flags[1];
   info->diag_fp64_redo_pixels = (uint64_t)flags[2];
   info->diag_fp64_resampled = (uint64_t)flags[4];
@@ -352,6 +357,7 @@ extern "C" int sd_terrain_correction(sd_ctx *ctx, const sd_radar_image *image, c
                                      const sd_geo_grid_point *grid, uint64_t n_grid,
                                      const sd_tc_config *cfg, float *out_data, float *out_cos_lia,
                                      uint8_t *out_mask, sd_geocoded_info *info) {
+  SD_STAGE("terrain_correction");
   return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, 0, 0, out_data, out_cos_lia, out_mask,
                 nullptr, info);
 }
@@ -362,6 +368,7 @@ extern "C" int sd_terrain_correction_with_times(sd_ctx *ctx, const sd_radar_imag
                                                 uint64_t n_grid, const sd_tc_config *cfg, float *out_data,
                                                 float *out_cos_lia, uint8_t *out_mask,
                                                 int64_t *out_azimuth_time_us, sd_geocoded_info *info) {
+  SD_STAGE("terrain_correction");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!out_azimuth_time_us) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null time buffer");
   return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, 0, 0, out_data, out_cos_lia, out_mask,
@@ -374,6 +381,7 @@ extern "C" int sd_terrain_correction_rows(sd_ctx *ctx, const sd_radar_image *ima
                                           const sd_tc_config *cfg, uint64_t row_begin, uint64_t row_end,
                                           float *out_data, float *out_cos_lia, uint8_t *out_mask,
                                           int64_t *out_azimuth_time_us, sd_geocoded_info *info) {
+  SD_STAGE("terrain_correction");
   return tc_run(ctx, image, scene, dem, geoid, grid, n_grid, cfg, row_begin, row_end, out_data, out_cos_lia,
                 out_mask, out_azimuth_time_us, info);
 }

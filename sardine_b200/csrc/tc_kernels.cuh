@@ -57,7 +57,8 @@ namespace {
 
 enum : uint8_t { ST_CONV = 0, ST_NONCONV = 1, ST_DEGEN = 2, ST_ORBIT = 3, ST_DEMMISS = 4 };
 constexpr int KNOTS = 17;
-constexpr int kCounters = 8;  // valid, dem, outside, nonconv, degen, flat, noise, spare
+constexpr int kCounters = 10;  // valid, dem, outside, nonconv, degen, flat, noise, spare, dB converted, dB masked
+constexpr int kCntDb = 8;      // counters[kCntDb + cls] for db_value's class cls (0 converted, 1 noise-masked)
 
 struct OrbitDev {
   const sd_state_vector *svs;
@@ -220,6 +221,8 @@ struct TcDev {
   // facet normal x, y, z and area (area NaN: a neighbour height missing)
   const double *tp;
   const double *fct;
+  int db;                      // write sigma0/gamma0 in dB (to_db_inplace), below db_floor as NaN
+  float db_floor;
   uint32_t *rs_cnt;            // split: per k_cand item (256 px), FP64 re-samples queued (may exceed RS_CAP)
   struct RsEnt *rs_ent;        // split: per k_cand item, RS_CAP queued re-samples
 };
@@ -236,9 +239,13 @@ constexpr int REDO_CHUNK = SEL_THREADS * 32;  // pixels one k_redo block compact
 
 struct TcWork {
   int n_jobs;
-  int pad;
+  uint32_t hq_cap;      // capacity of hq
   const TcDev *jobs;
   const uint64_t *pre;  // kWk x (n_jobs + 1)
+  // k_heights' deferred pixels (a DEM lookup undecided): job << 40 | pixel;
+  // *hq_cnt counts every deferral, also those past hq_cap (done in place)
+  unsigned long long *hq;
+  unsigned int *hq_cnt;
 };
 
 __device__ __forceinline__ const uint64_t *stage_pre(const TcWork &w, int stage) {
@@ -786,6 +793,25 @@ __device__ __forceinline__ void pixel_ecef(const TcDev &p, PixGeo *g, float hf) 
   g->P = ecef_sc(g->sla, g->cla, g->slo, g->clo, h_ell);
 }
 
+// pixel_height with decided lookups only: 1 = a finite height, 0 = none
+// (outside the DEM or a void), -1 = the lookup is undecided.
+__device__ __forceinline__ int pixel_height_try(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g, float *hf) {
+  int seg;
+  double t;
+  pixel_seg(p, r, c, &g->lon, &g->lat, &seg, &t);
+  int st;
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    if (p.aloc) dem_local_from_anchors(p, r, seg, t, &g->loc);
+    else utm_local(u, g->lat, utm_taup(u, g->lat), utm_lam(u, g->lon), &g->loc);
+    st = dem_at_xy_try(p.dem, g->loc.x, g->loc.y, hf);
+  } else {
+    st = dem_at_lonlat_try(p.dem, g->lon, g->lat, hf);
+  }
+  if (st < 0) return -1;
+  return st > 0 && isfinite(*hf) ? 1 : 0;
+}
+
 __device__ bool pixel_geo(const TcDev &p, uint64_t r, uint64_t c, PixGeo *g) {
   float hf;
   if (!pixel_height(p, r, c, g, &hf)) return false;
@@ -830,6 +856,37 @@ __device__ __forceinline__ bool facet_heights(const TcDev &p, const PixGeo &g, f
   }
   h[0] = he, h[1] = hw, h[2] = hn, h[3] = hs;
   return ok && isfinite(he) && isfinite(hw) && isfinite(hn) && isfinite(hs);
+}
+
+// facet_heights with decided lookups only: 1 = four finite heights, 0 = a
+// neighbour outside the DEM or on a void, -1 = a lookup is undecided.
+__device__ __forceinline__ int facet_heights_try(const TcDev &p, const PixGeo &g, float h[4]) {
+  const double sd = p.step_deg;
+  const double lon_e = g.lon + sd, lon_w = g.lon - sd, lat_n = g.lat + sd, lat_s = g.lat - sd;
+  int s[4];
+  if (p.dem.kind == SD_DEM_PROJECTED_UTM) {
+    const Utm &u = p.dem.utm;
+    const double k = kPi / 180.0;
+    double x, y;
+    utm_local_step(u, g.loc, 0.0, (lon_e - g.lon) * k, &x, &y);
+    s[0] = dem_at_xy_try(p.dem, x, y, &h[0]);
+    utm_local_step(u, g.loc, 0.0, (lon_w - g.lon) * k, &x, &y);
+    s[1] = dem_at_xy_try(p.dem, x, y, &h[1]);
+    utm_local_step(u, g.loc, (lat_n - g.lat) * k, 0.0, &x, &y);
+    s[2] = dem_at_xy_try(p.dem, x, y, &h[2]);
+    utm_local_step(u, g.loc, (lat_s - g.lat) * k, 0.0, &x, &y);
+    s[3] = dem_at_xy_try(p.dem, x, y, &h[3]);
+  } else {
+    s[0] = dem_at_lonlat_try(p.dem, lon_e, g.lat, &h[0]);
+    s[1] = dem_at_lonlat_try(p.dem, lon_w, g.lat, &h[1]);
+    s[2] = dem_at_lonlat_try(p.dem, g.lon, lat_n, &h[2]);
+    s[3] = dem_at_lonlat_try(p.dem, g.lon, lat_s, &h[3]);
+  }
+  if (s[0] < 0 || s[1] < 0 || s[2] < 0 || s[3] < 0) return -1;
+  return s[0] > 0 && s[1] > 0 && s[2] > 0 && s[3] > 0 && isfinite(h[0]) && isfinite(h[1]) && isfinite(h[2]) &&
+                 isfinite(h[3])
+             ? 1
+             : 0;
 }
 
 // Normal and area of the facet from the four neighbour heights.
@@ -1206,6 +1263,50 @@ static_assert(MAIN_THREADS <= 256, "RsEnt::meta holds the k_main thread in 8 bit
 #ifndef SD_HEIGHTS_MINB
 #define SD_HEIGHTS_MINB 4
 #endif
+
+// Target and facet of pixel i once its heights are known (ok: the centre
+// height hf is finite; fs: the four neighbour heights h are).
+__device__ __forceinline__ void heights_store(const TcDev &p, uint64_t i, PixGeo &g, bool ok, float hf, bool fs,
+                                              const float h[4]) {
+  const uint64_t npx = p.rows * p.cols;
+  double *tp = (double *)p.tp;
+  if (!ok) {
+    tp[i] = NAN;
+    if (p.fct) ((double *)p.fct)[3 * npx + i] = NAN;
+    return;
+  }
+  pixel_ecef(p, &g, hf);
+  tp[i] = g.P.x;
+  tp[npx + i] = g.P.y;
+  tp[2 * npx + i] = g.P.z;
+  if (p.fct) {
+    double *f = (double *)p.fct;
+    if (fs) {
+      const Facet fc = facet_from(p, g, h);
+      f[i] = fc.normal.x;
+      f[npx + i] = fc.normal.y;
+      f[2 * npx + i] = fc.normal.z;
+      f[3 * npx + i] = fc.area;
+    } else {
+      f[3 * npx + i] = NAN;
+    }
+  }
+}
+
+// Pixel i with the checked lookups (an undecided lookup is redone exactly).
+__device__ __noinline__ void heights_exact(const TcDev &p, uint64_t i) {
+  const uint64_t r = i / p.cols, c = i % p.cols;
+  PixGeo g;
+  float hf, h[4];
+  const bool ok = pixel_height(p, r, c, &g, &hf);
+  const bool fs = ok && p.fct && facet_heights(p, g, h);
+  heights_store(p, i, g, ok, hf, fs, h);
+}
+
+// The exact lookup behind an undecided one costs a full UTM projection;
+// taken inline by ~1 pixel in 200 it stalls the other 31 lanes of the warp
+// and the instruction cache.  Such pixels are queued instead and k_heights_fix
+// runs them 32 to a warp.
 __global__ void __launch_bounds__(SEL_THREADS, SD_HEIGHTS_MINB) k_heights(const TcWork *__restrict__ wp) {
   const TcWork w = *wp;
   const uint64_t *pre = stage_pre(w, WK_SEL);
@@ -1215,35 +1316,55 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_HEIGHTS_MINB) k_heights(const 
     const TcDev &p = w.jobs[jb];
     if (p.rs_cnt && threadIdx.x == 0) p.rs_cnt[item - pre[jb]] = 0;  // k_cand's queue of this item
     const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
-    if (i >= p.rows * p.cols) continue;
-    const uint64_t r = i / p.cols, c = i % p.cols;
-    const uint64_t npx = p.rows * p.cols;
-    PixGeo g;
-    float hf;
-    const bool ok = pixel_height(p, r, c, &g, &hf);
-    double *tp = (double *)p.tp;
-    if (!ok) {
-      tp[i] = NAN;
-      if (p.fct) ((double *)p.fct)[3 * npx + i] = NAN;
-      continue;
+    bool defer = false;
+    if (i < p.rows * p.cols) {
+      const uint64_t r = i / p.cols, c = i % p.cols;
+      PixGeo g;
+      float hf, h[4];
+      const int st = pixel_height_try(p, r, c, &g, &hf);
+      const int fs = st > 0 && p.fct ? facet_heights_try(p, g, h) : 0;
+      if (st >= 0 && fs >= 0) heights_store(p, i, g, st > 0, hf, fs > 0, h);
+      else defer = true;
     }
-    pixel_ecef(p, &g, hf);
-    tp[i] = g.P.x;
-    tp[npx + i] = g.P.y;
-    tp[2 * npx + i] = g.P.z;
-    if (p.fct) {
-      double *f = (double *)p.fct;
-      float h[4];
-      if (facet_heights(p, g, h)) {
-        const Facet fc = facet_from(p, g, h);
-        f[i] = fc.normal.x;
-        f[npx + i] = fc.normal.y;
-        f[2 * npx + i] = fc.normal.z;
-        f[3 * npx + i] = fc.area;
-      } else {
-        f[3 * npx + i] = NAN;
+    // queue the deferred lanes, one atomic per warp (the item loop is
+    // uniform over the block, so every lane arrives here)
+    const unsigned m = __ballot_sync(0xffffffffu, defer);
+    if (m) {
+      const int lane = threadIdx.x & 31;
+      unsigned base = 0;
+      if (lane == 0) base = atomicAdd(w.hq_cnt, (unsigned)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (defer) {
+        const unsigned slot = base + __popc(m & ((1u << lane) - 1u));
+        if (slot < w.hq_cap) w.hq[slot] = ((unsigned long long)jb << 40) | i;
+        ((double *)p.tp)[i] = -INFINITY;  // the mark k_heights_fix scans for when the queue overflowed
       }
     }
+  }
+}
+
+// The deferred pixels of k_heights, with the checked lookups: the queue, or
+// after an overflow every pixel k_heights marked.
+__global__ void __launch_bounds__(128) k_heights_fix(const TcWork *__restrict__ wp) {
+  const TcWork w = *wp;
+  const unsigned cnt = *w.hq_cnt;
+  if (cnt <= w.hq_cap) {
+    for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+      const unsigned long long e = w.hq[k];
+      const int jb = (int)(e >> 40);
+      const uint64_t i = e & ((1ull << 40) - 1);
+      if (jb < w.n_jobs && i < w.jobs[jb].rows * w.jobs[jb].cols) heights_exact(w.jobs[jb], i);
+    }
+    return;
+  }
+  const uint64_t *pre = stage_pre(w, WK_SEL);
+  const uint64_t total = pre[w.n_jobs] * SEL_THREADS;
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t item = k / SEL_THREADS;
+    const int jb = find_job(pre, w.n_jobs, item);
+    const TcDev &p = w.jobs[jb];
+    const uint64_t i = (item - pre[jb]) * SEL_THREADS + k % SEL_THREADS;
+    if (i < p.rows * p.cols && p.tp[i] == -INFINITY) heights_exact(p, i);
   }
 }
 
@@ -1866,7 +1987,13 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
         }
       }
       if (!deferred) {
-        p.out[i] = o.data;
+        float v = o.data;
+        if (p.db) {
+          int dc;
+          v = db_value(v, p.db_floor, &dc);
+          if (dc >= 0) atomicAdd(&s_cnt[kCntDb + dc], 1u);
+        }
+        p.out[i] = v;
         if (p.compute_lia) {
           p.cos_lia[i] = o.cos;
           p.mask[i] = o.mask;
@@ -1948,6 +2075,11 @@ __global__ void __launch_bounds__(SEL_THREADS) k_resample(const TcWork *__restri
           }
         }
         if (cls >= 0) {
+          if (p.db) {
+            int dc;
+            sigma0 = db_value(sigma0, p.db_floor, &dc);
+            if (dc >= 0) atomicAdd(&p.counters[kCntDb + dc], 1ull);
+          }
           p.out[i] = sigma0;
           if (p.compute_lia) p.mask[i] = m;
         }
@@ -2009,7 +2141,13 @@ __global__ void __launch_bounds__(SEL_THREADS) k_redo(const TcWork *__restrict__
         continue;
       }
       const CandOut o = cand_fp64_tf<KERNEL>(p, P, fc, os.pos, t, p.need_geom ? p.row_flat[r] : 0.0);
-      p.out[i] = o.data;
+      float v = o.data;
+      if (p.db) {
+        int dc;
+        v = db_value(v, p.db_floor, &dc);
+        if (dc >= 0) atomicAdd(&p.counters[kCntDb + dc], 1ull);
+      }
+      p.out[i] = v;
       if (p.compute_lia) {
         p.cos_lia[i] = o.cos;
         p.mask[i] = o.mask;
@@ -2079,6 +2217,17 @@ int work_upload(sd_ctx *ctx, const char *name, const TcDev *jobs, int n, TcWorkH
   SD_TRY(scratch(ctx, name, bytes, &d));
   std::vector<unsigned char> h(bytes);
   work_layout(jobs, n, h.data(), (unsigned char *)d, wk);
+  // k_heights' queue: 1 entry per 64 pixels (~1 in 200 defers), its count
+  // zeroed ahead of the stages
+  const uint64_t px = wk->totals[WK_SEL] * SEL_THREADS;
+  const uint64_t cap = std::min<uint64_t>(px / 64 + 4096, 0x7FFFFFFFull);
+  unsigned char *q = nullptr;
+  SD_TRY(scratch_t(ctx, (std::string(name) + ".hq").c_str(), 16 + cap * 8, &q));
+  TcWork *hw = reinterpret_cast<TcWork *>(h.data());
+  hw->hq_cnt = reinterpret_cast<unsigned int *>(q);
+  hw->hq = reinterpret_cast<unsigned long long *>(q + 16);
+  hw->hq_cap = (uint32_t)cap;
+  SD_CUDA(ctx, cudaMemsetAsync(q, 0, 4, ctx->stream));
   // pageable source: the copy is staged before the call returns
   SD_CUDA(ctx, cudaMemcpyAsync(d, h.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
   *d_work = (TcWork *)d;
@@ -2103,6 +2252,11 @@ int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
   SD_LAUNCHED(ctx);
   SD_TIMED_BEGIN(ctx, "k_heights");
   k_heights<<<persistent_grid(k_heights, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
+  SD_LAUNCHED(ctx);
+  // the deferred pixels (their count is known on the device only)
+  SD_TIMED_BEGIN(ctx, "k_heights_fix");
+  k_heights_fix<<<persistent_grid(k_heights_fix, 128, 0, blocks_for(totals[WK_SEL] == ~0ull ? ~0ull : totals[WK_SEL] * 4, 128)), 128, 0, st>>>(
+      d_work);
   SD_LAUNCHED(ctx);
   return SD_OK;
 }

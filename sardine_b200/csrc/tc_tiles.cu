@@ -172,6 +172,7 @@ int run_graph(sd_ctx *ctx, int key, const void *tag, F body) {
 extern "C" int sd_scene_create(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scene,
                                const sd_dem *dem, const sd_geoid *geoid, const sd_geo_grid_point *grid,
                                uint64_t n_grid, sd_scene_dev **out) {
+  SD_STAGE("scene_upload");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!image || !scene || !dem || !geoid || !out || (n_grid && !grid))
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null argument");
@@ -378,6 +379,7 @@ int tile_plan(sd_ctx *ctx, const sd_tile &t, uint64_t i, TilePlan *pl) {
 }  // namespace sd
 
 extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n) {
+  SD_STAGE("terrain_correction_tiles");
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (ctx->tiles_pending)
     return set_error(ctx, SD_ERR_BUSY, "the previous tile batch has not been collected (sd_tc_tiles_finish)");
@@ -571,7 +573,6 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     pre[m] = acc;
     SD_CUDA(ctx, cudaMemcpyAsync(d_sw, h.data(), h.size(), cudaMemcpyHostToDevice, st));
     if (use_graph && m < 1024) {
-      SD_TRY(speckle_masks(ctx));
       SD_TRY(run_graph(ctx, 1 << 20 | tx << 10 | ty, d_sw, [&]() -> int {
         return speckle_tiles_launch(ctx, (const SpWork *)d_sw, acc, true, tx, ty);
       }));
@@ -655,6 +656,7 @@ extern "C" int sd_tc_tiles_finish(sd_ctx *ctx, sd_geocoded_info *infos, uint64_t
 }
 
 extern "C" int sd_tc_tiles(sd_ctx *ctx, const sd_tile *tiles, uint64_t n, sd_geocoded_info *infos) {
+  SD_STAGE("terrain_correction_tiles");
   SD_TRY(sd_tc_tiles_launch(ctx, tiles, n));
   return sd_tc_tiles_finish(ctx, infos, n);
 }

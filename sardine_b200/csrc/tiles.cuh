@@ -33,7 +33,6 @@ struct SpWork {
   const uint64_t *pre;  // n_jobs + 1: exclusive prefix of tx x ty blocks
 };
 
-int speckle_masks(sd_ctx *ctx);
 // k_main in its parameter form for one terrain-correction job record (the
 // TcDev layout of tc_kernels.cuh), on stream st.
 int launch_main_param(sd_ctx *ctx, const void *job, cudaStream_t st);

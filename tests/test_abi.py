@@ -33,3 +33,23 @@ def test_ctx_create_without_gpu_fails_cleanly():
     h = ctypes.c_void_p()
     rc = _lib.lib().sd_ctx_create(0, ctypes.byref(h))
     assert rc != 0 and not h.value
+
+
+def test_stage_timing_lines_in_the_reference_format():
+    """With SARDINE_B200_TIMING=1 every entry point reports its stage on
+    stderr as the reference's report_timing does ("[timing] <stage> = <s> s",
+    run.rs:54-60), also when it returns an error status; each call is an
+    NVTX range under the same name.  A null context needs no GPU."""
+    import subprocess
+    import sys
+    code = ("import ctypes; from sardine_b200 import _lib; L = _lib.lib(); "
+            "rc = L.sd_speckle(None, None, 0, 0, 0, 0, 3, ctypes.c_float(1.0), ctypes.c_float(0.0), None); "
+            "rc2 = L.sd_to_db(None, None, 0, ctypes.c_float(0.0), None, None); print(rc, rc2)")
+    env = dict(os.environ, SARDINE_B200_TIMING="1")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert re.search(r"^\[timing\] speckle = \d+\.\d{3} s$", out.stderr, re.M), out.stderr
+    assert re.search(r"^\[timing\] db_conversion = \d+\.\d{3} s$", out.stderr, re.M), out.stderr
+    env.pop("SARDINE_B200_TIMING")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=120)
+    assert "[timing]" not in out.stderr

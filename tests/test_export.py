@@ -232,3 +232,74 @@ def test_gpu_cog_errors(ctx, tmp_path):
         sd.write_cog_with_crs(str(tmp_path / "no_such_dir" / "c.tif"), d, 2, 2, GT, WGS, 512, ctx=ctx)
     assert e.value.kind == "Io"
     assert not os.path.exists(str(tmp_path / "no_such_dir"))
+
+
+def _fused_vs_separate(ctx, run, floor):
+    """run() on ctx with dB output fused into its last kernel, against run()
+    in linear followed by to_db_inplace on the same context: the same bits,
+    counts and statistics (both convert with the same device function)."""
+    lin = np.array(run(), dtype=np.float32)
+    c_sep, s_sep = sd.to_db_inplace(lin, floor, ctx=ctx, stats=True)
+    sd.set_db_output(ctx, True, floor)
+    try:
+        fused = np.array(run(), dtype=np.float32)
+        c_f, s_f = sd.db_result(ctx)
+    finally:
+        sd.set_db_output(ctx, False)
+    assert np.array_equal(fused.view(np.uint32), lin.view(np.uint32)), "fused dB raster differs"
+    assert c_f == c_sep
+    assert np.array_equal(np.array(s_f, np.float32).view(np.uint32), np.array(s_sep, np.float32).view(np.uint32))
+    assert c_f[0] > 0 and c_f[1] > 0
+    return fused
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "split"])
+def test_gpu_db_fused_into_terrain_correction(ctx, precision):
+    """to_db_inplace fused into the terrain correction's last kernels
+    (k_cand, and k_resample / k_redo in split precision)."""
+    from sardine_b200 import synth
+    sc = synth.config1_scene(seed=21, n_lines=512, n_samples=1024, dem_n=160, flatten=True,
+                             resampling=sd.ResamplingKernel.Lanczos3)
+    if precision == "split":
+        sc.config.precision = sd.Precision.SPLIT
+    floor = 0.02
+
+    def run():
+        return sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx).data
+
+    fused = _fused_vs_separate(ctx, run, floor)
+    # and against the oracle's to_db of the same linear raster
+    lin = np.array(run(), dtype=np.float32)
+    ref = lin.copy()
+    oracle.to_db_inplace(ref, floor)
+    fin = np.isfinite(ref)
+    assert np.array_equal(np.isnan(fused), np.isnan(ref))
+    assert _ulps(fused[fin], ref[fin]).max() <= 4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flt", [sd.SpeckleFilter.RefinedLee(4.4), sd.SpeckleFilter.GammaMap(5, 4.4)],
+                         ids=["refined_lee", "gamma_map"])
+def test_gpu_db_fused_into_speckle(ctx, flt):
+    rng = np.random.default_rng(8)
+    rows, cols = 301, 257
+    img = rng.exponential(0.05, size=(rows, cols)).astype(np.float32)
+    img[5:9, 30:60] = np.nan
+    img[200:230, 100:140] = 0.0
+
+    def run():
+        return sd.apply_speckle_filter(img, cols, rows, flt, ctx=ctx)
+
+    _fused_vs_separate(ctx, run, 0.01)
+
+
+@pytest.mark.gpu
+def test_gpu_db_output_errors(ctx):
+    with pytest.raises(sd.ExportError) as e:
+        sd.set_db_output(ctx, True, -1.0)
+    assert e.value.kind == "InvalidNoiseFloor"
+    fresh = sd.Context(ctx.device)
+    with pytest.raises(sd.SardineError):
+        sd.db_result(fresh)
+    fresh.close()

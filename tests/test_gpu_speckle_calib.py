@@ -16,6 +16,8 @@ FILTERS = [
     sd.SpeckleFilter.RefinedLee(4.4),
     sd.SpeckleFilter.Boxcar(3),
     sd.SpeckleFilter.GammaMap(9, 1.0),
+    sd.SpeckleFilter.Lee(3, 1.0),
+    sd.SpeckleFilter.Boxcar(15),
 ]
 
 
@@ -27,6 +29,12 @@ def test_speckle_parity(ctx, flt):
     img[10:14, 20:40] = np.nan
     img[100, 7] = np.inf
     img[150:, 290:] = 0.0
+    # negative zeros: a window of -0.0 alone sums to +0.0 in the reference's
+    # loop, and skipped taps must not change any sum's sign
+    img[60:75, 100:118] = -0.0
+    img[62, 130:140] = -0.0
+    img[80, 200] = -np.inf
+    img[0, :] = np.nan  # a void edge row
     ref = oracle.apply_speckle_filter(img, cols, rows, flt).reshape(rows, cols)
     out = np.asarray(sd.apply_speckle_filter(img, cols, rows, flt, ctx=ctx)).reshape(rows, cols)
     assert np.array_equal(np.isnan(out), np.isnan(ref))
@@ -36,6 +44,8 @@ def test_speckle_parity(ctx, flt):
         assert rel.max() < 1e-5
     else:
         assert np.array_equal(out[m], ref[m]), "bit-exact expected (same f64 sums, same f32 ops)"
+        # the same bits, signed zeros included
+        assert np.array_equal(out[m].view(np.uint32), ref[m].view(np.uint32))
 
 
 @pytest.mark.parametrize("kind,window,enl,damp,code", [

@@ -112,6 +112,19 @@ def test_config1_shape_parity(ctx, resampling, flatten):
     assert_tc_parity(gpu, ref)
 
 
+def test_config1_full_shape_parity(ctx):
+    """Plain terrain correction at its full stated shape: a 4096 x 8192
+    sigma0 image, a 1024 x 1024 EPSG:4326 DEM, bilinear, LIA, no flattening."""
+    sc = synth.config1_scene(seed=1)
+    assert (sc.merged.lines, sc.merged.samples) == (4096, 8192)
+    assert np.asarray(sc.dem.data).shape == (1024, 1024)
+    assert sc.config.resampling == sd.ResamplingKernel.Bilinear and not sc.config.flatten
+    ref = oracle_tc(sc.merged, sc.scene, sc.dem, sc.grids, sc.config)
+    gpu = sd.terrain_correction(sc.merged, sc.scene, sc.dem, sc.grids, sc.config, ctx=ctx)
+    assert ref[1].valid_pixel_count > 0.5 * ref[1].total_pixel_count
+    assert_tc_parity(gpu, ref)
+
+
 def test_config1_partial_footprint_and_voids(ctx):
     """DEM larger than the radar footprint (outside-footprint pixels) with
     NaN voids (DEM_MISSING and DEM_NEIGHBOUR_MISSING)."""
