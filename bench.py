@@ -966,20 +966,15 @@ def run_c5(args):
             clk_summary = clk.summary()
     # end to end: the headline stream again, each result copied to host memory
     # as it completes (the D2H is inside the latency)
-    host_buf = torch.empty(3 * 2048 * 2048 * 4 + 4096, dtype=torch.uint8, pin_memory=True)
     d2h = [0]
 
-    def to_host(t):
-        off = 0
+    def on_host(t):  # the result planes are in pinned host memory when the request completes
         for plane in (t.result.data, t.result.cos_lia, t.result.mask):
-            if plane is None:
-                continue
-            nb = plane.numel() * plane.element_size()
-            host_buf[off:off + nb].copy_(plane.reshape(-1).view(torch.uint8))
-            off += nb
-        d2h[0] += off
+            if plane is not None:
+                assert not plane.is_cuda
+                d2h[0] += plane.numel() * plane.element_size()
     e2e_server = GeocodingServer(local, hbm_budget=budget // 2, slots=2, max_batch=64, graphs=True,
-                                 on_done=to_host)
+                                 on_done=on_host, host_results=True)
     for s in e2e_server.slots:
         autotune.apply(s.ctx, tune)
     n = args.burst * args.steps
@@ -995,6 +990,21 @@ def run_c5(args):
     e2e_s = _max_over_ranks(dist, e2e_s)
     e2e_px = _sum_over_ranks(dist, esum["px"])
     e2e_server.close()
+    # the same batched loop with every request in FP64: what split precision
+    # itself contributes (same tiles; the arms alternate, best of two each)
+    arm_px_s = {"fp64": 0.0, "split": 0.0}
+    for _ in range(2):
+        for arm, prec in (("split", sd.Precision.SPLIT), ("fp64", sd.Precision.FP64)):
+            rq = _c5_requests(sd, scenes, np.random.default_rng(58 + rank), args.burst, prec)
+            torch.cuda.synchronize()
+            a0 = time.perf_counter()
+            asum = latency_summary(_serve(server, rq, np.zeros(len(rq))))
+            torch.cuda.synchronize()
+            arm_px_s[arm] = max(arm_px_s[arm], asum["px"] / (time.perf_counter() - a0))
+    batched_fp64 = {"what": (f"the same {args.burst} requests queued at once through the same 2-slot batched loop "
+                             "in FP64 and in split precision (arms alternated, best of two, wall clock)"),
+                    "fp64_px_per_s": arm_px_s["fp64"], "split_px_per_s": arm_px_s["split"],
+                    "split_over_fp64": arm_px_s["split"] / arm_px_s["fp64"]}
     # plain per-request FP64 path on the same GPU: one tile per launch, no graphs
     base = GeocodingServer(local, hbm_budget=4 << 30, slots=1, max_batch=1, graphs=False)
     nb = max(64, args.burst * args.steps // 2)
@@ -1032,14 +1042,16 @@ def run_c5(args):
             "e2e": {"value": e2e_px / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": int(d2h[0] / max(1, args.steps)),
                     "p50_ms": esum["p50_ms"], "p99_ms": esum["p99_ms"],
-                    "api": "GeocodingServer with every result copied to pinned host memory on completion "
-                           "(scenes resident; request inputs are descriptors only)",
+                    "api": "GeocodingServer(host_results=True): each batch's result planes copied to pinned "
+                           "host memory on the slot's stream behind its kernels; a request completes when its "
+                           "results are on the host (scenes resident; request inputs are descriptors only)",
                     "scene_prepare_s": round(t_prep, 3),
                     "scene_prepare": (f"{args.scenes} scenes synthesised on the device, calibrated + debursted + "
                                       "merged and made resident before the timed region")},
             "roofline": roofline, "cpu_baseline": cpu,
             "accuracy_split_vs_fp64": acc,
             "per_request_fp64": bsum,
+            "batched_fp64_vs_split": batched_fp64,
             "run_details": {"autotune": tune,
                             "scene_device_gb": round(sum(s["rs"].device_bytes for s in scenes) / 2**30, 2)},
             "served_by_rate": by_rate,

@@ -500,6 +500,12 @@ typedef struct {
  * scenes, sizes, resampling kernels, precisions and filters.  One batch per
  * context is in flight at a time (SD_ERR_BUSY otherwise). */
 int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n);
+/* Host delivery of a batch in flight: one copy of `bytes` from device
+ * memory dev_src (normally the results' arena) to host memory host_dst
+ * (pinned for an asynchronous copy), enqueued on the context's stream
+ * behind the batch's kernels; the batch completes (sd_tc_tiles_poll /
+ * _finish) once the copy has landed.  No reference counterpart (serving). */
+int sd_tc_tiles_copy_out(sd_ctx *ctx, void *host_dst, const void *dev_src, uint64_t bytes);
 /* SD_OK when the batch in flight has finished (or none is), SD_ERR_BUSY if not. */
 int sd_tc_tiles_poll(sd_ctx *ctx);
 /* Waits for the batch and fills infos[0..n) (counters, histogram, grid). */
@@ -514,7 +520,7 @@ int sd_ctx_set_graphs(sd_ctx *ctx, int enable);
  * that fit it run without device allocations. */
 int sd_ctx_reserve(sd_ctx *ctx, uint64_t tile_arena_bytes);
 /* Launch shapes of the tile stages: the speckle/crop block (tx x ty
- * threads, tx >= 8, tx*ty <= 1024 and a multiple of 32; default 32 x 8) and
+ * threads, tx >= 8, tx*ty <= 512 and a multiple of 32; default 32 x 8) and
  * the geocoding kernel: CTAs per SM of its persistent form (0 = as many as
  * fit), or -1 for one launch per tile with the job in parameter space over
  * four forked streams.  Results do not depend on them;

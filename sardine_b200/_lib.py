@@ -49,6 +49,7 @@ _SIGS = {
     "sd_scene_device_bytes": (C.c_uint64, [P]),
     "sd_scene_destroy": (None, [P]),
     "sd_tc_tiles_launch": (C.c_int, [P, P, C.c_uint64]),
+    "sd_tc_tiles_copy_out": (C.c_int, [P, P, P, C.c_uint64]),
     "sd_tc_tiles_poll": (C.c_int, [P]),
     "sd_tc_tiles_finish": (C.c_int, [P, P, C.c_uint64]),
     "sd_tc_tiles": (C.c_int, [P, P, C.c_uint64, P]),

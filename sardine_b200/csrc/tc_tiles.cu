@@ -608,6 +608,18 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
   return SD_OK;
 }
 
+extern "C" int sd_tc_tiles_copy_out(sd_ctx *ctx, void *host_dst, const void *dev_src, uint64_t bytes) {
+  if (!ctx) return SD_ERR_INVALID_ARGUMENT;
+  if (!ctx->tiles_pending) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "no tile batch in flight");
+  if (bytes == 0) return SD_OK;
+  if (!host_dst || !dev_src) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "null buffer");
+  SD_CUDA(ctx, cudaSetDevice(ctx->device));
+  // behind the batch's kernels on its stream; the batch completes after it
+  SD_CUDA(ctx, cudaMemcpyAsync(host_dst, dev_src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  SD_CUDA(ctx, cudaEventRecord(ctx->tiles_done, ctx->stream));
+  return SD_OK;
+}
+
 extern "C" int sd_tc_tiles_poll(sd_ctx *ctx) {
   if (!ctx) return SD_ERR_INVALID_ARGUMENT;
   if (!ctx->tiles_pending) return SD_OK;

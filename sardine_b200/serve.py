@@ -74,9 +74,10 @@ class _Slot:
     """A context (stream) with its scratch arena reserved up front and a
     result arena the batch's outputs are carved from."""
 
-    def __init__(self, device: int, arena_bytes: int, graphs: bool, out_bytes: int):
+    def __init__(self, device: int, arena_bytes: int, graphs: bool, out_bytes: int, host: bool = False):
         import torch
         self.ctx = Context(device)
+        self.device = device
         self.capacity = arena_bytes
         self.out_capacity = out_bytes
         lib().sd_ctx_set_graphs(self.ctx.handle, int(graphs))
@@ -85,26 +86,49 @@ class _Slot:
             if rc != 0:
                 raise MemoryError(self.ctx.last_error())
         self.out_arena = torch.empty(out_bytes, dtype=torch.uint8, device=f"cuda:{device}")
+        # host delivery: a pinned mirror of the result arena, filled by one
+        # copy on the slot's stream behind each batch's kernels
+        self.host_arena = torch.empty(out_bytes, dtype=torch.uint8, pin_memory=True) if host else None
+        self.host_views = None
         self.batch: Optional[TileBatch] = None
         self.tickets: List[Ticket] = []
         self.bytes = 0
 
     def launch(self, requests):
         import torch
-        outs, off = [], 0
+        outs, hviews, off = [], [], 0
         for r in requests:
             n = r.rows * r.cols
-            views = []
+            views, hv = [], []
             for k, (dt, esz) in enumerate(((torch.float32, 4), (torch.float32, 4), (torch.uint8, 1))):
                 if k > 0 and not r.config.compute_lia:
                     views.append(None)
+                    hv.append(None)
                     continue
                 views.append(self.out_arena[off:off + esz * n].view(dt).view(r.rows, r.cols))
+                if self.host_arena is not None:
+                    hv.append(self.host_arena[off:off + esz * n].view(dt).view(r.rows, r.cols))
                 off += (esz * n + 255) // 256 * 256
             outs.append(tuple(views))
-        return TileBatch(self.ctx, requests, outs).launch()
+            hviews.append(tuple(hv))
+        batch = TileBatch(self.ctx, requests, outs).launch()
+        self.host_views = None
+        if self.host_arena is not None and off:
+            # one copy behind the batch on its stream (the library's, so no
+            # torch stream bookkeeping outlives the context); the batch is
+            # done once the copy has landed
+            rc = lib().sd_tc_tiles_copy_out(self.ctx.handle, C.c_void_p(self.host_arena.data_ptr()),
+                                            C.c_void_p(self.out_arena.data_ptr()), C.c_uint64(off))
+            if rc != 0:
+                raise RuntimeError(f"sd_tc_tiles_copy_out: {self.ctx.last_error()}")
+            self.host_views = hviews
+        return batch
 
     def close(self):
+        # the result arenas go before the context whose stream filled them
+        self.host_views = None
+        self.host_arena = None
+        self.out_arena = None
         self.ctx.close()
 
 
@@ -119,12 +143,17 @@ class GeocodingServer:
     def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, slots: int = 2,
                  max_batch: int = 64, graphs: bool = True,
                  clock: Callable[[], float] = time.perf_counter, slot_factory=None,
-                 on_done: Optional[Callable[[Ticket], None]] = None, keep_results: bool = False):
+                 on_done: Optional[Callable[[Ticket], None]] = None, keep_results: bool = False,
+                 host_results: bool = False):
         """hbm_budget covers each slot's scratch arena (4/5 of its share) and
         result arena (1/5).  Results live in the slot's result arena until
         that slot's next batch: `on_done(ticket)` runs as each request
         completes (copy out what must outlive it); unless keep_results, the
-        completed ticket keeps only counters and timings."""
+        completed ticket keeps only counters and timings.  host_results:
+        results are delivered in pinned host memory (the slot's host mirror,
+        copied behind the batch on its stream, so the transfer overlaps the
+        other slots' kernels); a request completes when its results are on
+        the host."""
         if slots < 1:
             raise ValueError("slots must be >= 1")
         self.clock = clock
@@ -132,7 +161,7 @@ class GeocodingServer:
         self.on_done = on_done
         self.keep_results = keep_results
         share = hbm_budget // slots
-        make = slot_factory or (lambda cap: _Slot(device, cap * 4 // 5, graphs, cap // 5))
+        make = slot_factory or (lambda cap: _Slot(device, cap * 4 // 5, graphs, cap // 5, host_results))
         self.slots = [make(share) for _ in range(slots)]
         self.queue: Deque[Ticket] = deque()
         self.completed: List[Ticket] = []
@@ -188,7 +217,10 @@ class GeocodingServer:
         try:
             results = s.batch.finish()
             now = self.clock()
-            for t, r in zip(s.tickets, results):
+            host = getattr(s, "host_views", None)
+            for k, (t, r) in enumerate(zip(s.tickets, results)):
+                if host is not None and hasattr(r, "data"):  # the planes as they landed on the host
+                    r.data, r.cos_lia, r.mask = host[k]
                 t.t_done = now
                 if t.cancel_requested:  # ran with its batch; the result is dropped
                     t.error = Cancelled("cancelled in flight")

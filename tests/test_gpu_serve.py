@@ -43,9 +43,10 @@ def _requests(scenes, rng, n):
     return out
 
 
-def _saver(saved):
+def _saver(saved, host=False):
     def on_done(t):
         r = t.result
+        assert r.data.is_cuda != host  # host_results: the planes arrive in pinned host memory
         saved[id(t)] = (r.data.cpu().numpy().copy(), None if r.mask is None else r.mask.cpu().numpy().copy(),
                         r.valid_pixel_count, list(r.newton_iter_histogram))
     return on_done
@@ -63,12 +64,14 @@ def _same(x, y):
     assert x[2] == y[2] and x[3] == y[3]
 
 
-def test_served_results_equal_alone_with_overlapping_slots(ctx):
+@pytest.mark.parametrize("host", [False, True], ids=["device_results", "host_results"])
+def test_served_results_equal_alone_with_overlapping_slots(ctx, host):
     scenes = [_scene(ctx, 61), _scene(ctx, 62)]
     rng = np.random.default_rng(3)
     reqs = _requests(scenes, rng, 40)
     saved = {}
-    srv = GeocodingServer(0, hbm_budget=2 << 30, slots=2, max_batch=6, graphs=True, on_done=_saver(saved))
+    srv = GeocodingServer(0, hbm_budget=2 << 30, slots=2, max_batch=6, graphs=True, on_done=_saver(saved, host),
+                          host_results=host)
     # a burst fills both slots, then Poisson arrivals at ~2000 req/s while
     # batches are on the device
     tickets = [srv.submit(r) for r in reqs[:12]]
