@@ -676,6 +676,13 @@ def _speckle_adds(sd, filt):
     return 4 * w * w if filt.kind == sd._abi.SPECKLE_FROST else 2 * w * w
 
 
+# DRAM bytes per output pixel of the TC stage and of the speckle/crop stage on
+# the config-5 tile batch, from one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum of every stage kernel, profiles/tc_c5_traffic.md)
+C5_TC_TRAFFIC_B_PER_PX = 359.4
+C5_SP_TRAFFIC_B_PER_PX = 10.2
+
+
 def _tile_roofline(sd, tiles, ctx, reqs):
     """Per-stage CUDA-event times of one batch of `reqs` on `ctx` (timing
     replaces graph replay for that batch): the geocoding stage against the
@@ -699,14 +706,18 @@ def _tile_roofline(sd, tiles, ctx, reqs):
     total = sum(v[0] for v in kt.values()) or 1.0
     roof = {"bound": "fp64", "kernel": "tile geocoding (" + "+".join(sorted(k for k in kt if k.startswith(TC_STAGE))) + ")",
             "achieved": tf, "peak": fp64, "unit": "TFLOP/s", "frac": tf / fp64 if (tf and fp64) else None,
-            "traffic": None, "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
+            "traffic": C5_TC_TRAFFIC_B_PER_PX * px,
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of every TC-stage kernel on this "
+                               "batch's tile sizes, 359.4 B/px x the batch's px (profiles/tc_c5_traffic.md)"),
+            "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
             "batch": f"{len(reqs)} tiles, {px} px",
             "speckle_stage": {"kernel": "k_speckle_tiles", "bound": "fp64_add", "achieved": add_rate,
                               "peak": add_peak, "unit": "T adds/s",
                               "frac": add_rate / add_peak if (add_rate and add_peak) else None,
                               "adds": adds, "peak_source": "measured FP64 FMA-chain rate / 2 (adds per s)",
                               "hbm_gbs": gbs, "hbm_frac": gbs / hbm if gbs else None,
-                              "hbm_peak_source": _hbm_peak_source(), "bytes_per_px": 9.0, "ms": sp_ms}}
+                              "hbm_peak_source": _hbm_peak_source(), "bytes_per_px": 9.0, "ms": sp_ms,
+                              "traffic": C5_SP_TRAFFIC_B_PER_PX * px}}
     kernels = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total, 4)}
                for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
     return roof, kernels

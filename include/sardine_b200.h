@@ -705,6 +705,15 @@ int sd_ctx_set_db_output(sd_ctx *ctx, int32_t enable, float noise_floor_linear);
  * SD_ERR_INVALID_ARGUMENT if no call with dB output has completed. */
 int sd_ctx_db_result(sd_ctx *ctx, uint64_t *counts, float *stats);
 
+/* Debug builds (compiled with -DSD_BOUNDS_CHECK=1) test every radar-image
+ * and DEM gather of the terrain-correction kernels against the buffer's
+ * extent, skip an access outside it and record the first one.  word[0..4):
+ * {site (1 radar image, 2 DEM; 0 = none since the last call), index,
+ * extent, 1 if this build has the checks else 0}; reading clears the
+ * record.  No reference counterpart (the reference relies on Rust's bounds
+ * checks). */
+int sd_debug_bounds(sd_ctx *ctx, uint64_t *word);
+
 /* downsample_2x (export.rs:362-392): dst ((cols+1)/2 x (rows+1)/2) holds the
  * f64 mean of the non-NaN pixels of each 2x2 patch of src, NaN when all
  * are NaN.  The overview step of sd_write_cog. */

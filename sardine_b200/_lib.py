@@ -60,6 +60,7 @@ _SIGS = {
     "sd_to_db": (C.c_int, [P, P, C.c_uint64, C.c_float, P, P]),
     "sd_ctx_set_db_output": (C.c_int, [P, C.c_int32, C.c_float]),
     "sd_ctx_db_result": (C.c_int, [P, P, P]),
+    "sd_debug_bounds": (C.c_int, [P, P]),
     "sd_slc_open": (C.c_int, [P, C.c_char_p, P]),
     "sd_slc_dims": (C.c_int, [P, P, P, P]),
     "sd_slc_close": (None, [P]),

@@ -182,8 +182,8 @@ struct FuLine {
   uint32_t col_end, vs, ve, in_start;
 };
 
-__global__ void __launch_bounds__(FU_THREADS) k_fused(MergeDev m, uint64_t lines, uint64_t cols,
-                                                     float *__restrict__ out, float *__restrict__ nesz) {
+__global__ void __launch_bounds__(FU_THREADS) k_fused(MergeDev m, uint64_t lines, uint64_t cols, float *out,
+                                                     float *nesz) {
   __shared__ FuLine sl[8];
   const uint64_t chunks = (cols + FU_COLS - 1) / FU_COLS;
   const uint64_t l = blockIdx.x / chunks;
@@ -206,54 +206,34 @@ __global__ void __launch_bounds__(FU_THREADS) k_fused(MergeDev m, uint64_t lines
   __syncthreads();
   float *orow = out + l * cols;
   float *nrow = nesz + l * cols;
-  // Phase 1: every pixel's owning swath and all of its loads (sample word
-  // and LUT values), issued before any result is formed or stored, so the
-  // thread keeps FU_PER_THREAD gathers in flight.
-  int own[FU_PER_THREAD];
-  uint32_t iqw[FU_PER_THREAD];
-  float k0[FU_PER_THREAD], k1[FU_PER_THREAD], n0[FU_PER_THREAD], n1[FU_PER_THREAD];
-#pragma unroll
-  for (int j = 0; j < FU_PER_THREAD; ++j) {
-    const uint32_t c = c0 + (uint32_t)(j * FU_THREADS) + threadIdx.x;
-    own[j] = -1;
-    if (c >= cols) continue;
-    for (int k = 0; k < m.n; ++k) {
-      const FuLine &f = sl[k];
-      if (c < f.col_end) {
-        if (c >= f.vs && c < f.ve) own[j] = k;
-        break;
-      }
-    }
-    if (own[j] < 0) continue;
-    const FuLine &f = sl[own[j]];
-    const CalSwathDev &s = m.sw[own[j]];
-    const uint32_t cc = f.in_start + (c - f.vs);
-    iqw[j] = __ldg(f.row + cc);
-    k0[j] = __ldg(s.cal_tab + (uint64_t)f.cal.lo * s.tab_cols + cc);
-    k1[j] = f.cal.lo != f.cal.hi ? __ldg(s.cal_tab + (uint64_t)f.cal.hi * s.tab_cols + cc) : k0[j];
-    n0[j] = __ldg(s.nr_tab + (uint64_t)f.nr.lo * s.tab_cols + cc);
-    n1[j] = f.nr.lo != f.nr.hi ? __ldg(s.nr_tab + (uint64_t)f.nr.hi * s.tab_cols + cc) : n0[j];
-  }
-  // Phase 2: apply_cal_row (apply_calibration.rs:288-309) and the stores.
 #pragma unroll
   for (int j = 0; j < FU_PER_THREAD; ++j) {
     const uint32_t c = c0 + (uint32_t)(j * FU_THREADS) + threadIdx.x;
     if (c >= cols) break;
     float a = NAN, b = NAN;
-    if (own[j] >= 0) {
-      const FuLine &f = sl[own[j]];
-      const int32_t i = (int32_t)(int16_t)(iqw[j] & 0xFFFF), q = (int32_t)(int16_t)(iqw[j] >> 16);
-      const float power = (float)(int32_t)((uint32_t)(i * i) + (uint32_t)(q * q));
-      float kk = k0[j];
-      if (f.cal.lo != f.cal.hi) kk = lerpf(kk, k1[j], f.cal.t);
-      float nr = n0[j];
-      if (f.nr.lo != f.nr.hi) nr = lerpf(nr, n1[j], f.nr.t);
-      const float k2 = kk * kk;
-      const float valid = (k2 > 0.0f) ? 1.0f : 0.0f;
-      const float inv_k2 = (k2 > 0.0f) ? 1.0f / k2 : 0.0f;
-      const float noise_val = nr * f.az;
-      a = maxf_nan(power - noise_val, 0.0f) * inv_k2 * valid;
-      b = noise_val * inv_k2 * valid;
+    for (int k = 0; k < m.n; ++k) {
+      const FuLine &f = sl[k];
+      if (c < f.col_end) {
+        if (c >= f.vs && c < f.ve) {
+          const uint32_t cc = f.in_start + (c - f.vs);
+          const CalSwathDev &s = m.sw[k];
+          const uint32_t iqw = __ldg(f.row + cc);
+          const int32_t i = (int32_t)(int16_t)(iqw & 0xFFFF), q = (int32_t)(int16_t)(iqw >> 16);
+          const float power = (float)(int32_t)((uint32_t)(i * i) + (uint32_t)(q * q));
+          float kk = __ldg(s.cal_tab + (uint64_t)f.cal.lo * s.tab_cols + cc);
+          if (f.cal.lo != f.cal.hi) kk = lerpf(kk, __ldg(s.cal_tab + (uint64_t)f.cal.hi * s.tab_cols + cc), f.cal.t);
+          float nr = __ldg(s.nr_tab + (uint64_t)f.nr.lo * s.tab_cols + cc);
+          if (f.nr.lo != f.nr.hi) nr = lerpf(nr, __ldg(s.nr_tab + (uint64_t)f.nr.hi * s.tab_cols + cc), f.nr.t);
+          // apply_cal_row (apply_calibration.rs:288-309)
+          const float k2 = kk * kk;
+          const float valid = (k2 > 0.0f) ? 1.0f : 0.0f;
+          const float inv_k2 = (k2 > 0.0f) ? 1.0f / k2 : 0.0f;
+          const float noise_val = nr * f.az;
+          a = maxf_nan(power - noise_val, 0.0f) * inv_k2 * valid;
+          b = noise_val * inv_k2 * valid;
+        }
+        break;
+      }
     }
     orow[c] = a;
     nrow[c] = b;

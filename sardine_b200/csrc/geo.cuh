@@ -352,6 +352,13 @@ struct DemView {
   Utm utm;
 };
 
+// A DEM cell read on the device (bounds-checked in SD_BOUNDS_CHECK builds).
+#if defined(__CUDA_ARCH__) && defined(SD_IN_BOUNDS)
+#define SD_DEM_LD(d, i)                                                                          \
+  (SD_IN_BOUNDS(::sd::BS_DEM, (i), (d).width * (d).height) ? __ldg(&(d).data[(i)]) : __int_as_float(0x7fc00000))
+#else
+#define SD_DEM_LD(d, i) __ldg(&(d).data[(i)])
+#endif
 SD_HD bool dem_sample(const DemView &d, double row_f, double col_f, float *h);
 
 // returns false for Err(OutOfBounds); *h = NaN for voids.
@@ -389,8 +396,8 @@ SD_HD bool dem_sample(const DemView &d, double row_f, double col_f, float *h) {
   double dr = row_f - (double)r0;
   double dc = col_f - (double)c0;
 #if defined(__CUDA_ARCH__)
-  float v00 = __ldg(&d.data[r0 * d.width + c0]), v01 = __ldg(&d.data[r0 * d.width + c1]);
-  float v10 = __ldg(&d.data[r1 * d.width + c0]), v11 = __ldg(&d.data[r1 * d.width + c1]);
+  float v00 = SD_DEM_LD(d, r0 * d.width + c0), v01 = SD_DEM_LD(d, r0 * d.width + c1);
+  float v10 = SD_DEM_LD(d, r1 * d.width + c0), v11 = SD_DEM_LD(d, r1 * d.width + c1);
 #else
   float v00 = d.data[r0 * d.width + c0], v01 = d.data[r0 * d.width + c1];
   float v10 = d.data[r1 * d.width + c0], v11 = d.data[r1 * d.width + c1];
@@ -441,7 +448,7 @@ SD_HD int dem_sample_cert(const DemView &d, double row_f, double col_f, double e
   const double dc = col_f - (double)c0;
   const uint64_t r1 = r0 + 1, c1 = c0 + 1;
 #if defined(__CUDA_ARCH__)
-#define SD_DEM_AT(R, C) __ldg(&d.data[(R) * d.width + (C)])
+#define SD_DEM_AT(R, C) SD_DEM_LD(d, (R) * d.width + (C))
 #else
 #define SD_DEM_AT(R, C) d.data[(R) * d.width + (C)]
 #endif

@@ -257,3 +257,19 @@ int sd_ctx_kernel_times(sd_ctx *ctx, char *names, uint64_t names_len, double *ms
 }
 
 }  // extern "C"
+
+// The first out-of-bounds gather the checked kernels recorded since the last
+// call: word = {site (1 radar image, 2 DEM; 0 none), index, extent, checks
+// compiled in (1) or not (0)}; the words are cleared.
+extern "C" int sd_debug_bounds(sd_ctx *ctx, uint64_t *word) {
+  if (!ctx || !word) return SD_ERR_INVALID_ARGUMENT;
+  unsigned long long a[3], b[3];
+  if (cudaSetDevice(ctx->device) != cudaSuccess || sd::bounds_read_tc(a) != 0 || sd::bounds_read_tiles(b) != 0)
+    return sd::set_error(ctx, SD_ERR_CUDA, "reading the bounds-check words failed");
+  const unsigned long long *w = a[0] ? a : b;
+  word[0] = w[0];
+  word[1] = w[1];
+  word[2] = w[2];
+  word[3] = SD_BOUNDS_CHECK ? 1 : 0;
+  return SD_OK;
+}

@@ -86,6 +86,47 @@ struct StageScope {
 // The reference's Newton histogram line (run.rs:319-339), when logging.
 void log_newton_hist(const unsigned long long *hist, int n);
 
+// ── debug bounds checks ─────────────────────────────────────────────────────
+// Built with -DSD_BOUNDS_CHECK=1, every gather of the radar image and the
+// DEM in the terrain-correction kernels tests its index against the
+// buffer's extent.  The first violation in a translation unit is recorded
+// in that unit's error word {site, index, extent} and the access is skipped
+// (the value reads as NaN): a faulty index shows up as a status the host
+// reads (sd_debug_bounds), never as a memory fault.  Default builds compile
+// the checks out.
+#ifndef SD_BOUNDS_CHECK
+#define SD_BOUNDS_CHECK 0
+#endif
+enum BoundsSite : int { BS_IMAGE = 1, BS_DEM = 2 };
+#if SD_BOUNDS_CHECK
+static __device__ unsigned long long sd_bounds_word[3];
+__device__ __noinline__ static bool sd_bounds_fail(int site, unsigned long long i, unsigned long long n) {
+  if (atomicCAS(&sd_bounds_word[0], 0ull, (unsigned long long)site) == 0ull) {
+    sd_bounds_word[1] = i;
+    sd_bounds_word[2] = n;
+  }
+  return false;
+}
+#define SD_IN_BOUNDS(site, i, n) \
+  ((unsigned long long)(i) < (unsigned long long)(n) || ::sd::sd_bounds_fail((site), (i), (n)))
+// the unit's word, read and cleared by the host (one per checked unit)
+#define SD_BOUNDS_ACCESSOR(fn)                                                  \
+  int fn(unsigned long long out[3]) {                                           \
+    if (cudaMemcpyFromSymbol(out, sd_bounds_word, 3 * sizeof(unsigned long long)) != cudaSuccess) return -1; \
+    const unsigned long long z[3] = {0, 0, 0};                                  \
+    return cudaMemcpyToSymbol(sd_bounds_word, z, sizeof z) == cudaSuccess ? 0 : -1; \
+  }
+#else
+#define SD_IN_BOUNDS(site, i, n) true
+#define SD_BOUNDS_ACCESSOR(fn) \
+  int fn(unsigned long long out[3]) { \
+    out[0] = out[1] = out[2] = 0;     \
+    return 0;                         \
+  }
+#endif
+int bounds_read_tc(unsigned long long out[3]);
+int bounds_read_tiles(unsigned long long out[3]);
+
 // to_db_inplace (export.rs:80-90) on one value: NaN stays NaN (*cls -1);
 // v <= floor_lin becomes NaN (*cls 1, noise-masked); anything else becomes
 // 10 log10 v (*cls 0, converted).

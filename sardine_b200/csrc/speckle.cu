@@ -386,41 +386,94 @@ __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
 // tile's halo'd raster (cells outside it are NaN, which the filters skip like
 // out-of-image cells), filters the data plane with the tile's kind (or
 // copies it when kind < 0) and crops cos(LIA) and the mask.
+// Where one work item's window sits: its job, block position and the
+// staged footprint (rows r0.., columns c0.. of the job's halo'd raster).
+struct SpItem {
+  const SpJob *jb;
+  int64_t tr, tc, r0, c0, in_cols, in_rows;
+  int h, tw, th;
+};
+
+__device__ __forceinline__ SpItem sp_item(const SpWork &w, uint64_t item, int bx, int by) {
+  int lo = 0, hi = w.n_jobs;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (w.pre[mid] <= item) lo = mid;
+    else hi = mid;
+  }
+  SpItem it;
+  it.jb = &w.jobs[lo];
+  const SpJob &jb = *it.jb;
+  const uint64_t li = item - w.pre[lo];
+  const int64_t nbx = (jb.cols + bx - 1) / bx;
+  it.tr = (int64_t)li / nbx;
+  it.tc = (int64_t)li % nbx;
+  it.h = jb.kind >= 0 ? jb.half : 0;
+  it.tw = bx + 2 * it.h;
+  it.th = by * SP_ROWS + 2 * it.h;
+  it.in_cols = jb.cols + 2 * jb.halo;
+  it.in_rows = jb.rows + 2 * jb.halo;
+  // output (r, c) is input (r + halo, c + halo); the block covers bx
+  // columns and by * SP_ROWS rows
+  it.c0 = it.tc * bx + jb.halo - it.h;
+  it.r0 = it.tr * by * SP_ROWS + jb.halo - it.h;
+  return it;
+}
+
+// Issues the item's window into buf: asynchronous 4-byte copies
+// (cp.async, completed by the caller's wait) for cells inside the raster,
+// plain NaN stores for the rest.
+__device__ __forceinline__ void sp_stage_async(const SpItem &it, float *buf, int tid, int nt) {
+  const float *in = it.jb->in;
+  for (int k = tid; k < it.tw * it.th; k += nt) {
+    const int ty = k / it.tw, tx = k % it.tw;
+    const int64_t rr = it.r0 + ty, cc = it.c0 + tx;
+    if (rr >= 0 && cc >= 0 && rr < it.in_rows && cc < it.in_cols) {
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(buf + k);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(in + rr * it.in_cols + cc)
+                   : "memory");
+    } else {
+      buf[k] = NAN;
+    }
+  }
+}
+
+// Items are strided over a persistent grid; each block double-buffers its
+// window: the next item's copies are in flight while the current item is
+// filtered.
 __global__ void __launch_bounds__(SP_MAX_THREADS) k_speckle_tiles(const SpWork *__restrict__ wp) {
-  extern __shared__ float tile[];
+  extern __shared__ float smem[];
   const SpWork w = *wp;
   const int bx = (int)blockDim.x, by = (int)blockDim.y, nt = bx * by;
   const int tid = threadIdx.y * bx + threadIdx.x;
+  const int buf_floats = (bx + 2 * SP_MAX_HALF) * (by * SP_ROWS + 2 * SP_MAX_HALF);
   const uint64_t total = w.pre[w.n_jobs];
-  for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    int lo = 0, hi = w.n_jobs;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (w.pre[mid] <= item) lo = mid;
-      else hi = mid;
-    }
-    const SpJob &jb = w.jobs[lo];
-    const uint64_t li = item - w.pre[lo];
-    const int64_t nbx = (jb.cols + bx - 1) / bx;
-    const int64_t tr = (int64_t)li / nbx, tc = (int64_t)li % nbx;
-    const int h = jb.kind >= 0 ? jb.half : 0;
-    const int tw = bx + 2 * h, th = by * SP_ROWS + 2 * h;
-    const int64_t in_cols = jb.cols + 2 * jb.halo, in_rows = jb.rows + 2 * jb.halo;
-    // output (r, c) is input (r + halo, c + halo); the block covers bx
-    // columns and by * SP_ROWS rows
-    const int64_t c0 = tc * bx + jb.halo - h, r0 = tr * by * SP_ROWS + jb.halo - h;
+  uint64_t item = blockIdx.x;
+  if (item < total) sp_stage_async(sp_item(w, item, bx, by), smem, tid, nt);
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  for (int b = 0; item < total; item += gridDim.x, b ^= 1) {
+    const SpItem it = sp_item(w, item, bx, by);
+    const uint64_t next = item + gridDim.x;
+    if (next < total) sp_stage_async(sp_item(w, next, bx, by), smem + (b ^ 1) * buf_floats, tid, nt);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this item's copies have landed
     __syncthreads();
-    for (int k = tid; k < tw * th; k += nt) {
-      const int ty = k / tw, tx = k % tw;
-      const int64_t rr = r0 + ty, cc = c0 + tx;
-      float v = NAN;
-      if (rr >= 0 && cc >= 0 && rr < in_rows && cc < in_cols) v = __ldg(jb.in + rr * in_cols + cc);
-      tile[k] = v;
-    }
-    __syncthreads();
+    const float *tile = smem + b * buf_floats;
+    const SpJob &jb = *it.jb;
+    const int h = it.h, tw = it.tw;
     // this thread: column c, rows r .. r + SP_ROWS - 1
-    const int64_t c = tc * bx + threadIdx.x, r = (tr * by + threadIdx.y) * SP_ROWS;
+    const int64_t c = it.tc * bx + threadIdx.x, r = (it.tr * by + threadIdx.y) * SP_ROWS;
     if (c < jb.cols && r < jb.rows) {
+      // the cropped cos(LIA) and mask travel while the filter computes
+      float cz[SP_ROWS];
+      uint8_t mz[SP_ROWS];
+#pragma unroll
+      for (int k = 0; k < SP_ROWS; ++k) {
+        const int64_t ii = (r + k + jb.halo) * it.in_cols + (c + jb.halo);
+        const bool in = r + k < jb.rows;
+        cz[k] = in && jb.cos_out ? __ldg(jb.cos_in + ii) : 0.0f;
+        mz[k] = in && jb.mask_out ? __ldg(jb.mask_in + ii) : 0;
+      }
       const SpCoef cf{jb.enl, jb.damping, jb.cv_n_sq, jb.cv_max_sq};
       const int lx = threadIdx.x + h, ly = threadIdx.y * SP_ROWS + h;
       float o[SP_ROWS];
@@ -437,13 +490,15 @@ __global__ void __launch_bounds__(SP_MAX_THREADS) k_speckle_tiles(const SpWork *
 #pragma unroll
       for (int k = 0; k < SP_ROWS; ++k) {
         if (r + k >= jb.rows) break;
-        const int64_t oi = (r + k) * jb.cols + c, ii = (r + k + jb.halo) * in_cols + (c + jb.halo);
+        const int64_t oi = (r + k) * jb.cols + c;
         jb.out[oi] = o[k];
-        if (jb.cos_out) jb.cos_out[oi] = __ldg(jb.cos_in + ii);
-        if (jb.mask_out) jb.mask_out[oi] = __ldg(jb.mask_in + ii);
+        if (jb.cos_out) jb.cos_out[oi] = cz[k];
+        if (jb.mask_out) jb.mask_out[oi] = mz[k];
       }
     }
+    __syncthreads();  // every thread is done with this buffer before it is refilled
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 }  // namespace
@@ -463,7 +518,8 @@ bool speckle_shape_ok(int tx, int ty) {
 }
 
 int speckle_tiles_launch(sd_ctx *ctx, const SpWork *d_work, uint64_t total, bool full_grid, int tx, int ty) {
-  const size_t smem = (size_t)(tx + 2 * SP_MAX_HALF) * (ty * SP_ROWS + 2 * SP_MAX_HALF) * sizeof(float);
+  // two window buffers (double-buffered staging)
+  const size_t smem = 2 * (size_t)(tx + 2 * SP_MAX_HALF) * (ty * SP_ROWS + 2 * SP_MAX_HALF) * sizeof(float);
   const unsigned g = persistent_grid(k_speckle_tiles, tx * ty, smem, full_grid ? ~0ull : total);
   SD_TIMED_BEGIN(ctx, "k_speckle_tiles");
   k_speckle_tiles<<<g, dim3(tx, ty), smem, ctx->stream>>>(d_work);

@@ -56,6 +56,11 @@ int tc_output_grid_host(const sd_scene *scene, const sd_tc_config *cfg, sd_geoco
 
 }  // namespace sd
 
+namespace sd {
+// this unit's bounds-check word (see runtime.cuh)
+SD_BOUNDS_ACCESSOR(bounds_read_tc)
+}  // namespace sd
+
 using namespace sd;
 
 extern "C" int sd_tc_output_grid(sd_ctx *ctx, const sd_scene *scene, const sd_tc_config *cfg,

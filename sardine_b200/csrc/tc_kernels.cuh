@@ -469,7 +469,10 @@ __device__ __forceinline__ int64_t predicted_time(const TcDev &p, uint64_t r, ui
 }
 
 // ── resampling (terrain_correction.rs:770-983) ───────────────────────────────
-__device__ __forceinline__ float ldf(const float *p, int64_t i) { return __ldg(p + i); }
+// One radar-image sample; n = lines x samples bounds it in SD_BOUNDS_CHECK builds.
+__device__ __forceinline__ float ldf(const float *p, int64_t i, uint64_t n) {
+  return SD_IN_BOUNDS(BS_IMAGE, i, n) ? __ldg(p + i) : __int_as_float(0x7fc00000);
+}
 
 __device__ float sample_bilinear(const float *d, uint64_t nl, uint64_t ns, double line, double sample) {
   int64_t max_line = nl == 0 ? 0 : (int64_t)nl - 1;
@@ -480,8 +483,8 @@ __device__ float sample_bilinear(const float *d, uint64_t nl, uint64_t ns, doubl
   int64_t s1 = s0 + 1 < max_sample ? s0 + 1 : max_sample;
   double dl = line - (double)l0;
   double ds = sample - (double)s0;
-  float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
-  float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
+  float v00 = ldf(d, l0 * (int64_t)ns + s0, nl * ns), v01 = ldf(d, l0 * (int64_t)ns + s1, nl * ns);
+  float v10 = ldf(d, l1 * (int64_t)ns + s0, nl * ns), v11 = ldf(d, l1 * (int64_t)ns + s1, nl * ns);
   if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
   double w00 = (1.0 - dl) * (1.0 - ds);
   double w01 = (1.0 - dl) * ds;
@@ -508,7 +511,7 @@ __device__ float sample_bicubic(const float *d, uint64_t nl, uint64_t ns, double
     double wl = keys_weight((double)li - dl);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      float v = ldf(d, row * (int64_t)ns + cols[k], nl * ns);
       if (v != v) return NAN;
       acc += (double)v * wl * ws[k];
     }
@@ -645,8 +648,8 @@ __device__ float sample_bilinear_f(const float *d, uint64_t nl, uint64_t ns, dou
   // dl may be negative (line in [-0.5, 0)) or beyond 1 at the far edge
   const FracF ql = frac_f(line, l0), qs = frac_f(sample, s0);
   const float dl = ql.f, ds = qs.f;
-  float v00 = ldf(d, l0 * (int64_t)ns + s0), v01 = ldf(d, l0 * (int64_t)ns + s1);
-  float v10 = ldf(d, l1 * (int64_t)ns + s0), v11 = ldf(d, l1 * (int64_t)ns + s1);
+  float v00 = ldf(d, l0 * (int64_t)ns + s0, nl * ns), v01 = ldf(d, l0 * (int64_t)ns + s1, nl * ns);
+  float v10 = ldf(d, l1 * (int64_t)ns + s0, nl * ns), v11 = ldf(d, l1 * (int64_t)ns + s1, nl * ns);
   if (v00 != v00 || v01 != v01 || v10 != v10 || v11 != v11) return NAN;
   // explicit weights, as the reference forms them: with non-negative
   // weights and samples every term is non-negative and the sum keeps its
@@ -678,7 +681,7 @@ __device__ float sample_bicubic_f(const float *d, uint64_t nl, uint64_t ns, doub
     float racc = 0.f, rabs = 0.f;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      float v = ldf(d, row * (int64_t)ns + cols[k], nl * ns);
       if (v != v) return NAN;
       racc = fmaf(v, ws[k], racc);
       rabs = fmaf(fabsf(v), fabsf(ws[k]), rabs);
@@ -708,7 +711,7 @@ __device__ float sample_lanczos_t(const float *d, uint64_t nl, uint64_t ns, doub
     T racc = 0, rabs = 0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      float v = ldf(d, row * (int64_t)ns + cols[k]);
+      float v = ldf(d, row * (int64_t)ns + cols[k], nl * ns);
       if (v != v) return NAN;
       racc += (T)v * ws[k];
       if (amag) rabs += fabs((T)v * ws[k]);

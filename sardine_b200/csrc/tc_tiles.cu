@@ -6,6 +6,11 @@
 
 #include "tc_kernels.cuh"
 
+namespace sd {
+// this unit's bounds-check word (see runtime.cuh)
+SD_BOUNDS_ACCESSOR(bounds_read_tiles)
+}  // namespace sd
+
 using namespace sd;
 
 namespace sd {
