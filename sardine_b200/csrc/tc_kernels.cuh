@@ -1497,11 +1497,9 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
     // the target from k_heights (every job has it)
     const uint64_t npx = p.rows * p.cols;
     g.P.x = __ldg(p.tp + i);
+    g.P.y = __ldg(p.tp + npx + i);  // all three at once: one round trip
+    g.P.z = __ldg(p.tp + 2 * npx + i);
     geo_ok = isfinite(g.P.x);
-    if (geo_ok) {
-      g.P.y = __ldg(p.tp + npx + i);
-      g.P.z = __ldg(p.tp + 2 * npx + i);
-    }
     if (geo_ok && fast) {
       // reference iteration from the shared state: one converged t*
       int64_t t = ew_ok ? uw : predicted_time(p, r, (uint64_t)c);
@@ -1891,6 +1889,35 @@ __global__ void __launch_bounds__(SCAN_WARPS * 32) k_scan(const TcWork *__restri
 #endif
 
 // The pixel's target and facet as k_heights left them (every job has them).
+// A pixel's k_heights planes, loaded together (one memory round trip: no
+// load waits on another's value).
+struct PixPlanes {
+  double t[3], f[4];
+};
+__device__ __forceinline__ PixPlanes load_planes(const TcDev &p, uint64_t i) {
+  const uint64_t npx = p.rows * p.cols;
+  PixPlanes q;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) q.t[k] = __ldg(p.tp + k * npx + i);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) q.f[k] = p.fct ? __ldg(p.fct + k * npx + i) : NAN;
+  return q;
+}
+// target_facet from preloaded planes
+__device__ __forceinline__ bool target_facet_of(const TcDev &p, const PixPlanes &q, V3 *P, Facet *f) {
+  P->x = q.t[0];
+  if (!isfinite(P->x)) return false;
+  P->y = q.t[1];
+  P->z = q.t[2];
+  f->ok = false;
+  if (p.fct && isfinite(q.f[3])) {
+    f->ok = true;
+    f->normal = {q.f[0], q.f[1], q.f[2]};
+    f->area = q.f[3];
+  }
+  return true;
+}
+
 __device__ __forceinline__ bool target_facet(const TcDev &p, uint64_t i, V3 *P, Facet *f) {
   const uint64_t npx = p.rows * p.cols;
   P->x = __ldg(p.tp + i);
@@ -1937,17 +1964,25 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
     const uint64_t npx = p.rows * p.cols;
     const uint64_t li = item - pre[jb];
     const uint64_t i = li * SEL_THREADS + tid;
-    const uint8_t sel = i < npx ? p.sel[i] : (uint8_t)SEL_ORBIT;
+    // the pixel's walk outcome, base time and geometry in one round trip
+    uint8_t sel = (uint8_t)SEL_ORBIT;
+    int64_t fbv = 0;
+    PixPlanes pl;
+    if (i < npx) {
+      sel = p.sel[i];
+      fbv = p.fb[i];
+      pl = load_planes(p, i);
+    }
     const int code = sel & 7, it = sel >> 4;
     const bool has_t = code == SEL_M0 || code == SEL_M1 || code == SEL_DONE;
-    const int64_t t = has_t ? p.fb[i] + (code == SEL_M1 ? 1 : 0) : 0;
+    const int64_t t = has_t ? fbv + (code == SEL_M1 ? 1 : 0) : 0;
     int counter = -1;
     if (has_t) {
       atomicAdd(&s_cnt[kCounters + it], 1u);
       const uint64_t r = i / p.cols;
       V3 P;
       Facet fc;
-      const bool ok = target_facet(p, i, &P, &fc);
+      const bool ok = target_facet_of(p, pl, &P, &fc);
       V3 S;
       const bool orb_ok = ok && orbit_pos_exact(p.orb, t, &S);
       if (!orb_ok) atomicOr(&p.flags[ok ? 0 : 5], 1);  // cannot happen for a converged time
