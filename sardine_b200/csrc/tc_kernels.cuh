@@ -1486,6 +1486,15 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   // landing point is within a few ns of each lane's own root.
   const uint64_t rr = r < p.rows ? r : p.rows - 1;
   const uint64_t cq = c < 0 ? 0 : ((uint64_t)c < p.cols ? (uint64_t)c : p.cols - 1);
+  // the target from k_heights (every job has it), loaded ahead of the warp's
+  // orbit expansion, which does not depend on it
+  const bool px_in = in_row && r < p.rows;
+  if (px_in) {
+    const uint64_t npx = p.rows * p.cols;
+    g.P.x = __ldg(p.tp + i);
+    g.P.y = __ldg(p.tp + npx + i);
+    g.P.z = __ldg(p.tp + 2 * npx + i);
+  }
   const int64_t uw = __shfl_sync(0xffffffffu, predicted_time(p, rr, cq), 16);
   Ent ew;
   bool ew_exact = false;
@@ -1493,12 +1502,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   OrbTaylor &T = tw[tid >> 5];
   orb_taylor_build(p.orb, uw, ew, ew_ok, tid & 31, &T);
   __syncwarp();
-  if (in_row && r < p.rows) {
-    // the target from k_heights (every job has it)
-    const uint64_t npx = p.rows * p.cols;
-    g.P.x = __ldg(p.tp + i);
-    g.P.y = __ldg(p.tp + npx + i);  // all three at once: one round trip
-    g.P.z = __ldg(p.tp + 2 * npx + i);
+  if (px_in) {
     geo_ok = isfinite(g.P.x);
     if (geo_ok && fast) {
       // reference iteration from the shared state: one converged t*
