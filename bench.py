@@ -1155,7 +1155,7 @@ def _write_slc_tiff(path, iq):
 def run_ingest(args):
     """SLC ingest feeding the fused calibrate+deburst+merge: the three
     sub-swath measurement TIFFs of a config-2 scene (3 x 13,500 x 21,000
-    CInt16, 3.4 GB, on the box's local disk, in its page cache after the
+    CInt16, 3.4 GB, on the machine's local disk, in its page cache after the
     warm-up) are read through SlcReader straight into device buffers, then
     calibrated, debursted and merged.  value = merged pixels per second of
     the whole step; the read alone is reported in GB/s."""

@@ -1,7 +1,7 @@
 """ctypes binding of the CPU oracle (oracle/sardine_oracle.cpp).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
-the checker, and by bench.py for the CPU-baseline leg.  The product package
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() to
+check its results, and by bench.py for the CPU-baseline leg.  The product package
 never imports this module.
 """
 from __future__ import annotations

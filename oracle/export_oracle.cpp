@@ -2,7 +2,7 @@
 // dB conversion, dB statistics, overview downsampling and the
 // Cloud-Optimised GeoTIFF writer.
 //
-// TEST INFRASTRUCTURE ONLY (the checker and the CPU baseline): a plain
+// TEST INFRASTRUCTURE ONLY (the parity tests' reference results and the CPU baseline): a plain
 // sequential restatement of the reference's arithmetic and file layout,
 // never linked into the product library.
 //

@@ -661,7 +661,7 @@ int orc_get_threads(void) { return n_threads(); }
 void orc_set_libm(int correctly_rounded) { g_cr_libm.store(correctly_rounded ? 1 : 0); }
 int orc_get_libm(void) { return g_cr_libm.load(); }
 
-// Correctly rounded sin and cos of n doubles (the checker of the device's).
+// Correctly rounded sin and cos of n doubles (the reference values the device's are tested against).
 void orc_cr_sincos(const double *x, uint64_t n, double *s, double *c) {
   for (uint64_t i = 0; i < n; ++i) sd::crm::sincos(x[i], s + i, c + i);
 }
