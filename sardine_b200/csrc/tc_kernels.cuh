@@ -2253,18 +2253,23 @@ void work_layout(const TcDev *jobs, int n, unsigned char *h, unsigned char *d, T
   wk->d_jobs = reinterpret_cast<TcDev *>(d + o_jobs);
 }
 
+// k_heights' deferral queue for `px` pixels: 1 entry per 64 pixels plus
+// 4096 (deferrals are rare; an overflow falls back to a scan), after a
+// 16-byte count.
+uint64_t heights_queue_cap(uint64_t px) { return std::min<uint64_t>(px / 64 + 4096, 0x7FFFFFFFull); }
+size_t heights_queue_bytes(uint64_t px) { return 16 + heights_queue_cap(px) * 8; }
+
 int work_upload(sd_ctx *ctx, const char *name, const TcDev *jobs, int n, TcWorkHost *wk, TcWork **d_work) {
   const size_t bytes = work_bytes(n);
   void *d = nullptr;
   SD_TRY(scratch(ctx, name, bytes, &d));
   std::vector<unsigned char> h(bytes);
   work_layout(jobs, n, h.data(), (unsigned char *)d, wk);
-  // k_heights' queue: 1 entry per 64 pixels (~1 in 200 defers), its count
-  // zeroed ahead of the stages
+  // k_heights' queue (heights_queue_bytes), its count zeroed ahead of the stages
   const uint64_t px = wk->totals[WK_SEL] * SEL_THREADS;
-  const uint64_t cap = std::min<uint64_t>(px / 64 + 4096, 0x7FFFFFFFull);
+  const uint64_t cap = heights_queue_cap(px);
   unsigned char *q = nullptr;
-  SD_TRY(scratch_t(ctx, (std::string(name) + ".hq").c_str(), 16 + cap * 8, &q));
+  SD_TRY(scratch_t(ctx, (std::string(name) + ".hq").c_str(), heights_queue_bytes(px), &q));
   TcWork *hw = reinterpret_cast<TcWork *>(h.data());
   hw->hq_cnt = reinterpret_cast<unsigned int *>(q);
   hw->hq = reinterpret_cast<unsigned long long *>(q + 16);

@@ -696,6 +696,12 @@ extern "C" int sd_ctx_reserve(sd_ctx *ctx, uint64_t tile_arena_bytes) {
   SD_TRY(scratch(ctx, "tiles.counters", 1024 * 32 * 8, &p));
   SD_TRY(scratch(ctx, "tiles.flags", 1024 * 8 * 4, &p));
   SD_TRY(scratch(ctx, "tiles.ax", 1024 * 257 * 8, &p));
+  // k_heights' deferral queues at the capacity work_upload asks for a batch
+  // that fills the arena (a tile pixel takes at least 37 arena bytes), so an
+  // admitted batch never regrows them (a regrow frees memory, which
+  // synchronises the device and would stall the other contexts' batches)
+  SD_TRY(scratch(ctx, "tiles.work0.hq", heights_queue_bytes(tile_arena_bytes / 37), &p));
+  SD_TRY(scratch(ctx, "tiles.work1.hq", heights_queue_bytes(tile_arena_bytes / 37), &p));
   return SD_OK;
 }
 
