@@ -1535,6 +1535,41 @@ def run_export(args):
             "frac": per_k[dom]["gbs"] / peak, "traffic": None,
             "bytes_per_step": alg[dom], "stage_gbs": round(sum(alg.values()) / (dev_ms / 1e3) / 1e9, 1)}
     file_bytes = os.path.getsize(path)
+    # the dB conversion fused into the stage that produces the raster (here
+    # a Gamma-MAP 5 x 5 filter, as run.rs applies speckle before to_db): the
+    # filter then to_db_inplace, against the filter writing dB itself
+    flt = sd.SpeckleFilter.GammaMap(5, 4.4)
+
+    def dev_ms_of(fn):
+        fn()  # warm
+        ctx.set_timing(True)
+        fn()
+        t = ctx.kernel_times()
+        ctx.set_timing(False)
+        return {k: round(v[0], 3) for k, v in t.items()}
+
+    def separate():
+        filtered = sd.apply_speckle_filter(src, cols, rows, flt, ctx=ctx)
+        return sd.to_db_inplace(filtered, 0.0, ctx=ctx, stats=True)
+
+    def fused():
+        sd.set_db_output(ctx, True, 0.0)
+        try:
+            sd.apply_speckle_filter(src, cols, rows, flt, ctx=ctx)
+            return sd.db_result(ctx)
+        finally:
+            sd.set_db_output(ctx, False)
+    sep_k = dev_ms_of(separate)
+    sep_res = separate()
+    fus_k = dev_ms_of(fused)
+    fus_res = fused()
+    db_fusion = {"what": (f"Gamma-MAP 5x5 of the {rows}x{cols} raster, then to_db_inplace + stats, against the "
+                          "filter writing dB itself (statistics from a read-only pass)"),
+                 "separate_kernels_ms": sep_k, "fused_kernels_ms": fus_k,
+                 "separate_ms": round(sum(sep_k.values()), 3), "fused_ms": round(sum(fus_k.values()), 3),
+                 "same_counts_and_stats": bool(sep_res[0] == fus_res[0] and
+                                               np.array_equal(np.array(sep_res[1], np.float32).view(np.uint32),
+                                                              np.array(fus_res[1], np.float32).view(np.uint32)))}
     cpu = None
     if args.cpu_baseline and world == 1 and rank == 0:
         import oracle
@@ -1559,6 +1594,7 @@ def run_export(args):
                                    + (" (REDUCED SHAPE)" if args.small else ""),
                        "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
             "kernels": per_k, "roofline": roof, "counts": list(counts), "db_stats": list(stats),
+            "db_fused_into_speckle": db_fusion,
             "cpu_baseline": cpu, "gpu_launches": sum(v["launches"] for v in per_k.values()),
             "clocks": clk.summary(),
             "e2e": {"value": world * n / (wall / args.steps), "unit": "px/s", "h2d_bytes_per_step": 0,

@@ -354,29 +354,44 @@ __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
     tile[k] = v;
   }
   __syncthreads();
-  // this thread: column c, rows r .. r + SP_ROWS - 1
+  // this thread: column c, rows r .. r + SP_ROWS - 1 (threads past the
+  // raster's edge stay for the block's count reduction)
   const int64_t c = (int64_t)blockIdx.x * TX + threadIdx.x;
   const int64_t r = (int64_t)blockIdx.y * (TY * SP_ROWS) + threadIdx.y * SP_ROWS;
-  if (c >= p.cols || r >= p.rows) return;
-  const SpCoef cf{p.enl, p.damping, p.cv_n_sq, p.cv_max_sq};
-  float o[SP_ROWS];
-  speckle_rows<KIND>(tile, tw, threadIdx.x + h, threadIdx.y * SP_ROWS + h, h, cf, o);
   unsigned ncv = 0, nnm = 0;
+  if (c < p.cols && r < p.rows) {
+    const SpCoef cf{p.enl, p.damping, p.cv_n_sq, p.cv_max_sq};
+    float o[SP_ROWS];
+    speckle_rows<KIND>(tile, tw, threadIdx.x + h, threadIdx.y * SP_ROWS + h, h, cf, o);
 #pragma unroll
-  for (int k = 0; k < SP_ROWS; ++k)
-    if (r + k < p.rows) {
-      float v = o[k];
-      if (p.db) {  // the dB conversion of the filtered raster, in this epilogue
-        int dc;
-        v = db_value(v, p.db_floor, &dc);
-        ncv += dc == 0;
-        nnm += dc == 1;
+    for (int k = 0; k < SP_ROWS; ++k)
+      if (r + k < p.rows) {
+        float v = o[k];
+        if (p.db) {  // the dB conversion of the filtered raster, in this epilogue
+          int dc;
+          v = db_value(v, p.db_floor, &dc);
+          ncv += dc == 0;
+          nnm += dc == 1;
+        }
+        p.out[(r + k) * p.cols + c] = v;
       }
-      p.out[(r + k) * p.cols + c] = v;
+  }
+  if (p.db) {  // the block's counts: warp sums, then one global atomic per block
+    __shared__ unsigned s_db[2];
+    const int tid = threadIdx.y * TX + threadIdx.x;
+    if (tid == 0) s_db[0] = s_db[1] = 0;
+    __syncthreads();
+    ncv = __reduce_add_sync(0xffffffffu, ncv);
+    nnm = __reduce_add_sync(0xffffffffu, nnm);
+    if ((tid & 31) == 0) {
+      atomicAdd(&s_db[0], ncv);
+      atomicAdd(&s_db[1], nnm);
     }
-  if (p.db) {
-    if (ncv) atomicAdd(p.dbc, (unsigned long long)ncv);
-    if (nnm) atomicAdd(p.dbc + 1, (unsigned long long)nnm);
+    __syncthreads();
+    if (tid == 0) {
+      if (s_db[0]) atomicAdd(p.dbc, (unsigned long long)s_db[0]);
+      if (s_db[1]) atomicAdd(p.dbc + 1, (unsigned long long)s_db[1]);
+    }
   }
 }
 

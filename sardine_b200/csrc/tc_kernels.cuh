@@ -2087,7 +2087,7 @@ __global__ void __launch_bounds__(SEL_THREADS) k_resample(const TcWork *__restri
     if (n == 0) continue;
     for (uint32_t q0 = 0; q0 < n; q0 += 32) {  // warp-uniform: the ballots below
       const uint32_t q = q0 + lane;
-      int cls = -1;
+      int cls = -1, dbc = -1;
       if (q < n) {
         const RsEnt e = p.rs_ent[li * RS_CAP + q];
         const uint64_t i = li * SEL_THREADS + e.thread;
@@ -2117,11 +2117,7 @@ __global__ void __launch_bounds__(SEL_THREADS) k_resample(const TcWork *__restri
           }
         }
         if (cls >= 0) {
-          if (p.db) {
-            int dc;
-            sigma0 = db_value(sigma0, p.db_floor, &dc);
-            if (dc >= 0) atomicAdd(&p.counters[kCntDb + dc], 1ull);
-          }
+          if (p.db) sigma0 = db_value(sigma0, p.db_floor, &dbc);
           p.out[i] = sigma0;
           if (p.compute_lia) p.mask[i] = m;
         }
@@ -2129,10 +2125,14 @@ __global__ void __launch_bounds__(SEL_THREADS) k_resample(const TcWork *__restri
       const int n0 = __popc(__ballot_sync(0xffffffffu, cls == 0));
       const int n2 = __popc(__ballot_sync(0xffffffffu, cls == 2));
       const int n6 = __popc(__ballot_sync(0xffffffffu, cls == 6));
+      const int d0 = __popc(__ballot_sync(0xffffffffu, dbc == 0));  // dB converted / noise-masked
+      const int d1 = __popc(__ballot_sync(0xffffffffu, dbc == 1));
       if (lane == 0) {
         if (n0) atomicAdd(&p.counters[0], (unsigned long long)n0);
         if (n2) atomicAdd(&p.counters[2], (unsigned long long)n2);
         if (n6) atomicAdd(&p.counters[6], (unsigned long long)n6);
+        if (d0) atomicAdd(&p.counters[kCntDb], (unsigned long long)d0);
+        if (d1) atomicAdd(&p.counters[kCntDb + 1], (unsigned long long)d1);
       }
     }
     if (lane == 0) atomicAdd(&p.flags[4], (int)n);
