@@ -57,15 +57,27 @@ __global__ void __launch_bounds__(DB_THREADS) k_to_db(float *__restrict__ d, uin
   uint32_t cv = 0, nm = 0, cnt = 0;
   double sum = 0.0;
   float mn = INFINITY, mx = -INFINITY;
+  // element of slot k: base + 4 (g DB_THREADS + tid) + j with g = k / 4,
+  // j = k % 4, so a thread's four consecutive elements are one 16-byte word
+  // (128-bit loads and stores when the raster is 16-byte aligned)
+  constexpr int G = DB_PER_THREAD / 4;
+  const bool vec = (reinterpret_cast<uintptr_t>(d) & 15) == 0;
   float x[DB_PER_THREAD];
 #pragma unroll
-  for (int k = 0; k < DB_PER_THREAD; ++k) {  // all loads in flight before any use
-    const uint64_t i = base + (uint64_t)k * DB_THREADS + tid;
-    x[k] = i < n ? (CONVERT ? __ldcs(d + i) : __ldg(d + i)) : NAN;
+  for (int g = 0; g < G; ++g) {  // all loads in flight before any use
+    const uint64_t i0 = base + 4 * ((uint64_t)g * DB_THREADS + tid);
+    if (vec && i0 + 3 < n) {
+      const float4 q = CONVERT ? __ldcs(reinterpret_cast<const float4 *>(d + i0))
+                               : __ldg(reinterpret_cast<const float4 *>(d + i0));
+      x[4 * g] = q.x, x[4 * g + 1] = q.y, x[4 * g + 2] = q.z, x[4 * g + 3] = q.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[4 * g + j] = i0 + j < n ? (CONVERT ? __ldcs(d + i0 + j) : __ldg(d + i0 + j)) : NAN;
+    }
   }
 #pragma unroll
   for (int k = 0; k < DB_PER_THREAD; ++k) {
-    const uint64_t i = base + (uint64_t)k * DB_THREADS + tid;
+    const uint64_t i = base + 4 * ((uint64_t)(k / 4) * DB_THREADS + tid) + k % 4;
     float v = x[k];
     if (i >= n || v != v) continue;
     if (CONVERT) {
@@ -73,13 +85,26 @@ __global__ void __launch_bounds__(DB_THREADS) k_to_db(float *__restrict__ d, uin
       v = db_value(v, floor_lin, &cls);
       if (cls == 1) ++nm;
       else ++cv;
-      d[i] = v;
+      x[k] = v;
     }
     if (isfinite(v)) {
       mn = fminf(mn, v);
       mx = fmaxf(mx, v);
       sum += (double)v;
       ++cnt;
+    }
+  }
+  if (CONVERT) {  // the converted words back (NaN elements unchanged)
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const uint64_t i0 = base + 4 * ((uint64_t)g * DB_THREADS + tid);
+      if (vec && i0 + 3 < n) {
+        __stcs(reinterpret_cast<float4 *>(d + i0), make_float4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]));
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (i0 + j < n) d[i0 + j] = x[4 * g + j];
+      }
     }
   }
   sum = warp_sum_d(sum);
@@ -121,46 +146,71 @@ __global__ void __launch_bounds__(DB_THREADS) k_to_db(float *__restrict__ d, uin
 __global__ void __launch_bounds__(DB_THREADS) k_db_sample(const float *__restrict__ d, uint64_t n,
                                                           const uint64_t *__restrict__ first, uint64_t stride,
                                                           float *__restrict__ sample, uint64_t n_sample) {
-  constexpr int NW = DB_THREADS / 32;
-  __shared__ uint32_t s_c[DB_PER_THREAD][NW];
-  __shared__ uint64_t s_first[DB_PER_THREAD];  // first sample rank at or after each round's start
+  // Round g of the block covers elements base + g * 1024 .. + 1024; lane l of
+  // warp w holds four consecutive ones, base + g * 1024 + 4 (32 w + l) + j
+  // (one 16-byte load).  A finite value's rank in element order is: the
+  // block's first rank, the counts of earlier rounds, of earlier warps in the
+  // round, of earlier lanes in the warp, and of the lane's earlier elements.
+  constexpr int NW = DB_THREADS / 32, G = DB_PER_THREAD / 4, RND = 4 * DB_THREADS;
+  __shared__ uint32_t s_c[G][NW];
+  __shared__ uint64_t s_first[G];  // first sample rank at or after each round's start
   const uint64_t base = (uint64_t)blockIdx.x * DB_CHUNK;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const bool vec = (reinterpret_cast<uintptr_t>(d) & 15) == 0;
   float x[DB_PER_THREAD];
   unsigned m[DB_PER_THREAD];
 #pragma unroll
-  for (int k = 0; k < DB_PER_THREAD; ++k) {
-    const uint64_t i = base + (uint64_t)k * DB_THREADS + tid;
-    x[k] = i < n ? __ldcs(d + i) : NAN;
+  for (int g = 0; g < G; ++g) {
+    const uint64_t i0 = base + (uint64_t)g * RND + 4 * (uint64_t)tid;
+    if (vec && i0 + 3 < n) {
+      const float4 q = __ldcs(reinterpret_cast<const float4 *>(d + i0));
+      x[4 * g] = q.x, x[4 * g + 1] = q.y, x[4 * g + 2] = q.z, x[4 * g + 3] = q.w;
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[4 * g + j] = i0 + j < n ? __ldcs(d + i0 + j) : NAN;
+    }
   }
 #pragma unroll
-  for (int k = 0; k < DB_PER_THREAD; ++k) {
-    m[k] = __ballot_sync(0xffffffffu, isfinite(x[k]));
-    if (lane == 0) s_c[k][wid] = __popc(m[k]);
+  for (int g = 0; g < G; ++g) {
+    uint32_t wc = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      m[4 * g + j] = __ballot_sync(0xffffffffu, isfinite(x[4 * g + j]));
+      wc += __popc(m[4 * g + j]);
+    }
+    if (lane == 0) s_c[g][wid] = wc;
   }
   __syncthreads();
-  if (tid < DB_PER_THREAD) {  // thread k: the rank at round k's start (uniform over the block)
+  if (tid < G) {  // thread g: the rank at round g's start (uniform over the block)
     uint64_t rk = first[blockIdx.x];
     for (int j = 0; j < tid; ++j)
       for (int w = 0; w < NW; ++w) rk += s_c[j][w];
     s_first[tid] = rk + (stride - rk % stride) % stride;
   }
   __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
   uint64_t rank = first[blockIdx.x];
 #pragma unroll
-  for (int k = 0; k < DB_PER_THREAD; ++k) {  // element k * 256 + tid: rounds before, then warps before
-    uint32_t before = __popc(m[k] & ((1u << lane) - 1u)), total = 0;
+  for (int g = 0; g < G; ++g) {
+    uint32_t before = 0, total = 0;
 #pragma unroll
     for (int w = 0; w < NW; ++w) {
-      const uint32_t c = s_c[k][w];
+      const uint32_t c = s_c[g][w];
       before += w < wid ? c : 0u;
       total += c;
     }
-    if ((m[k] >> lane) & 1u) {
-      const uint64_t rk = rank + before, f = s_first[k];
-      // stride >= 256: at most one sample per round, the one at rank f
-      const bool take = stride >= DB_THREADS ? rk == f : (rk >= f && (rk - f) % stride == 0);
-      if (take && rk / stride < n_sample) sample[rk / stride] = x[k];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) before += __popc(m[4 * g + j] & lt);  // earlier lanes' elements
+    const uint64_t f = s_first[g];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if ((m[4 * g + j] >> lane) & 1u) {
+        const uint64_t rk = rank + before;
+        // stride >= 1024: at most one sample per round, the one at rank f
+        const bool take = stride >= (uint64_t)RND ? rk == f : (rk >= f && (rk - f) % stride == 0);
+        if (take && rk / stride < n_sample) sample[rk / stride] = x[4 * g + j];
+        ++before;  // this lane's next element comes after this one
+      }
     }
     rank += total;
   }
