@@ -10,7 +10,11 @@
 // as speckle.rs:226-240 does, so the f32 filter arithmetic sees the same
 // inputs.  The sums are sequential per output, so neither a sliding window
 // nor a shuffle tree (which re-associates the adds) would reproduce them.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
+#include <cstdlib>
 
 #include "geo.cuh"
 #include "runtime.cuh"
@@ -31,6 +35,7 @@ struct SpParams {
   int db;                    // write the filtered value in dB (to_db_inplace)
   float db_floor;
   unsigned long long *dbc;   // db: converted, noise-masked counts
+  int *err;                  // set when a staging wait timed out (k_speckle_tma)
 };
 
 __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
@@ -115,6 +120,8 @@ __device__ float speckle_px(const float *tile, int tw, int lx, int ly, int h, co
 constexpr int SP_ROWS = 2;
 // slots of the context's device counters that hold sd_speckle's dB counts
 constexpr int SP_DB_COUNTERS = 48;
+// slot of the context's device error words for a timed-out staging wait
+constexpr int SP_ERR_FLAG = 40;
 // largest tile-batch block (Refined Lee holds 2 x 8 directional sums per thread)
 constexpr int SP_MAX_THREADS = 512;
 
@@ -395,6 +402,99 @@ __global__ void __launch_bounds__(TX *TY) k_speckle(SpParams p) {
   }
 }
 
+// ── the same filter with the window staged by the tensor-memory accelerator ─
+// For rasters whose rows are 16-byte aligned (cols % 4 == 0, base 16-byte
+// aligned) one 2-D `cp.async.bulk.tensor` load stages the block's window.
+// The window's first column is rounded down to a multiple of 4 floats (the
+// copy's x coordinate must be a 16-byte multiple) and the box is widened to
+// bw columns to cover the remainder; cells outside the raster arrive as NaN
+// (the tensor map's fill mode), exactly the "outside the image" cell the
+// filters skip.  The copy completes on a shared-memory mbarrier; the wait is
+// bounded and reports a timeout in *p.err instead of spinning forever.
+
+// true once phase `phase` of the mbarrier at shared address `bar` has
+// completed, false after `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if (it > 32) __nanosleep(256);
+  }
+  return false;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(TX *TY) k_speckle_tma(SpParams p, const __grid_constant__ CUtensorMap tm, int bw) {
+  extern __shared__ __align__(128) float tile[];
+  __shared__ __align__(8) unsigned long long mbar;
+  const int h = p.half, th = TY * SP_ROWS + 2 * h;
+  const int tid = threadIdx.y * TX + threadIdx.x;
+  const int x = (int)blockIdx.x * TX - h;          // the window's first column (may be negative)
+  const int x0 = x - (((x % 4) + 4) % 4);          // rounded down to 4 floats
+  const int y0 = (int)blockIdx.y * (TY * SP_ROWS) - h;
+  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&mbar);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bw * th * 4)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+            "r"((uint32_t)__cvta_generic_to_shared(tile)),
+        "l"(reinterpret_cast<uint64_t>(&tm)), "r"(x0), "r"(y0), "r"(bar)
+        : "memory");
+  }
+  if (!mbar_wait(bar, 0, 1u << 22)) {  // never expected: the copy is a few KB
+    if (tid == 0) atomicExch(p.err, 1);
+    return;
+  }
+  // this thread: column c, rows r .. r + SP_ROWS - 1
+  const int64_t c = (int64_t)blockIdx.x * TX + threadIdx.x;
+  const int64_t r = (int64_t)blockIdx.y * (TY * SP_ROWS) + threadIdx.y * SP_ROWS;
+  unsigned ncv = 0, nnm = 0;
+  if (c < p.cols && r < p.rows) {
+    const SpCoef cf{p.enl, p.damping, p.cv_n_sq, p.cv_max_sq};
+    float o[SP_ROWS];
+    speckle_rows<KIND>(tile, bw, threadIdx.x + h + (x - x0), threadIdx.y * SP_ROWS + h, h, cf, o);
+#pragma unroll
+    for (int k = 0; k < SP_ROWS; ++k)
+      if (r + k < p.rows) {
+        float v = o[k];
+        if (p.db) {
+          int dc;
+          v = db_value(v, p.db_floor, &dc);
+          ncv += dc == 0;
+          nnm += dc == 1;
+        }
+        p.out[(r + k) * p.cols + c] = v;
+      }
+  }
+  if (p.db) {  // the block's counts, as k_speckle forms them
+    __shared__ unsigned s_db[2];
+    if (tid == 0) s_db[0] = s_db[1] = 0;
+    __syncthreads();
+    ncv = __reduce_add_sync(0xffffffffu, ncv);
+    nnm = __reduce_add_sync(0xffffffffu, nnm);
+    if ((tid & 31) == 0) {
+      atomicAdd(&s_db[0], ncv);
+      atomicAdd(&s_db[1], nnm);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      if (s_db[0]) atomicAdd(p.dbc, (unsigned long long)s_db[0]);
+      if (s_db[1]) atomicAdd(p.dbc + 1, (unsigned long long)s_db[1]);
+    }
+  }
+}
+
 // ── batched form: many tiles, each a halo'd geocoded raster ──────────────────
 // Item = one tx x ty block (the launch's block shape, chosen by the tile
 // autotuner) of one tile's output.  The block stages its window from the
@@ -562,6 +662,43 @@ int speckle_validate(uint64_t len, uint64_t cols, uint64_t rows, int kind, uint6
 }
 
 // Launch on device buffers (shared with the tile path).
+// The driver's tensor-map encoder, looked up once through the runtime (no
+// link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// SARDINE_B200_SPECKLE_TMA=0 keeps every call on the scalar staging.
+bool tma_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("SARDINE_B200_SPECKLE_TMA");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// A 2-D map of the f32 raster (cols x rows, row pitch cols floats) with a
+// bw x th box, cells outside the raster filled with NaN.
+bool encode_window_map(CUtensorMap *tm, const float *d, uint64_t cols, uint64_t rows, int bw, int th) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {cols, rows};
+  const cuuint64_t strides[1] = {cols * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)th};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(d), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NAN_REQUEST_ZERO_FMA) == CUDA_SUCCESS;
+}
+
 int speckle_launch(sd_ctx *ctx, const float *d_in, float *d_out, uint64_t cols, uint64_t rows,
                    int kind, uint64_t window, float enl, float damping, cudaStream_t st) {
   if (cols == 0 || rows == 0) return SD_OK;
@@ -581,12 +718,39 @@ int speckle_launch(sd_ctx *ctx, const float *d_in, float *d_out, uint64_t cols, 
   p.db_floor = ctx->db_floor;
   p.dbc = ctx->d_counters + SP_DB_COUNTERS;
   if (p.db) SD_CUDA(ctx, cudaMemsetAsync(p.dbc, 0, 2 * sizeof(unsigned long long), st));
+  p.err = ctx->d_flags + SP_ERR_FLAG;
+  SD_CUDA(ctx, cudaMemsetAsync(p.err, 0, sizeof(int), st));
   const int h = p.half;
   size_t smem = (size_t)(TX + 2 * h) * (TY * SP_ROWS + 2 * h) * sizeof(float);
   if (smem > 200 * 1024)
     return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "speckle window %llu too large", (unsigned long long)win);
   dim3 grid((unsigned)((cols + TX - 1) / TX), (unsigned)((rows + TY * SP_ROWS - 1) / (TY * SP_ROWS)));
   dim3 block(TX, TY);
+  // the TMA-staged form where the raster's rows are 16-byte aligned and the
+  // widened window fits one box (at most 256 per dimension)
+  const int bw = (TX + 2 * h + 3 + 3) & ~3, th = TY * SP_ROWS + 2 * h;
+  CUtensorMap tm;
+  if (tma_enabled() && cols % 4 == 0 && (reinterpret_cast<uintptr_t>(d_in) & 15) == 0 && bw <= 256 && th <= 256 &&
+      cols < (1ull << 32) && rows < (1ull << 31) && encode_window_map(&tm, d_in, cols, rows, bw, th)) {
+    const size_t tsmem = (size_t)bw * th * sizeof(float);
+    switch (kind) {
+#define SD_LAUNCH_SPECKLE_TMA(K)                                                              \
+  case K:                                                                                     \
+    if (tsmem > 48 * 1024)                                                                    \
+      SD_CUDA(ctx, cudaFuncSetAttribute(k_speckle_tma<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem)); \
+    SD_TIMED_BEGIN(ctx, "k_speckle_tma_" #K);                                            \
+    k_speckle_tma<K><<<grid, block, tsmem, st>>>(p, tm, bw);                                  \
+    break;
+      SD_LAUNCH_SPECKLE_TMA(SD_SPECKLE_BOXCAR)
+      SD_LAUNCH_SPECKLE_TMA(SD_SPECKLE_LEE)
+      SD_LAUNCH_SPECKLE_TMA(SD_SPECKLE_FROST)
+      SD_LAUNCH_SPECKLE_TMA(SD_SPECKLE_GAMMA_MAP)
+      SD_LAUNCH_SPECKLE_TMA(SD_SPECKLE_REFINED_LEE)
+#undef SD_LAUNCH_SPECKLE_TMA
+    }
+    SD_LAUNCHED(ctx);
+    return SD_OK;
+  }
   switch (kind) {
 #define SD_LAUNCH_SPECKLE(K)                                                                 \
   case K:                                                                                    \
@@ -649,5 +813,9 @@ extern "C" int sd_speckle(sd_ctx *ctx, const float *data, uint64_t data_len, uin
     SD_TRY(db_finish(ctx, (const float *)d_out, data_len, c[0], c[1]));
   }
   SD_TRY(finish_out(ctx, out, d_out, data_len * sizeof(float)));
-  return sync(ctx);
+  int err = 0;
+  SD_CUDA(ctx, cudaMemcpyAsync(&err, ctx->d_flags + SP_ERR_FLAG, sizeof err, cudaMemcpyDeviceToHost, ctx->stream));
+  SD_TRY(sync(ctx));
+  if (err) return set_error(ctx, SD_ERR_TIMEOUT, "speckle: a window's staging copy did not complete");
+  return SD_OK;
 }

@@ -21,19 +21,24 @@ FILTERS = [
 ]
 
 
+# 301 columns: rows not 16-byte aligned, the window is staged with loads;
+# 300 and 40: aligned rows, staged by one tensor-memory copy per block (40 x
+# 20 is smaller than one block's window, so the fill covers every side)
+@pytest.mark.parametrize("shape", [(173, 301), (173, 300), (20, 40)], ids=lambda s: f"{s[0]}x{s[1]}")
 @pytest.mark.parametrize("flt", FILTERS, ids=lambda f: f"k{f.kind}w{f.window}")
-def test_speckle_parity(ctx, flt):
+def test_speckle_parity(ctx, flt, shape):
     rng = np.random.default_rng(3)
-    rows, cols = 173, 301
+    rows, cols = shape
     img = rng.exponential(0.05, size=(rows, cols)).astype(np.float32)
-    img[10:14, 20:40] = np.nan
-    img[100, 7] = np.inf
+    img[10:14, 20:40] = np.nan  # slices clip to small shapes
     img[150:, 290:] = 0.0
     # negative zeros: a window of -0.0 alone sums to +0.0 in the reference's
     # loop, and skipped taps must not change any sum's sign
     img[60:75, 100:118] = -0.0
-    img[62, 130:140] = -0.0
-    img[80, 200] = -np.inf
+    img[62:63, 130:140] = -0.0
+    img[100:101, 7:8] = np.inf
+    img[80:81, 200:201] = -np.inf
+    img[5:7, 3:9] = -0.0
     img[0, :] = np.nan  # a void edge row
     ref = oracle.apply_speckle_filter(img, cols, rows, flt).reshape(rows, cols)
     out = np.asarray(sd.apply_speckle_filter(img, cols, rows, flt, ctx=ctx)).reshape(rows, cols)
