@@ -91,7 +91,7 @@ int launch_pixels_single(sd_ctx *ctx, const TcWork *d_work, const uint64_t *tota
 
 int launch_main_param(sd_ctx *ctx, const void *job, cudaStream_t st) {
   const TcDev &p = *static_cast<const TcDev *>(job);
-  const uint64_t items = p.rows * p.bpr;
+  const uint64_t items = main_items(p);
   if (items == 0) return SD_OK;
   if (items > 0x7FFFFFFFull) return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "tile too large");
   const unsigned g = (unsigned)items;
@@ -287,7 +287,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   // consecutive microseconds can satisfy |delta| < tol).  Larger tolerances
   // leave every pixel to the row walk's exact path.
   p.fast = (p.tol <= 1e-6) ? 1 : 0;
-  p.bpr = (p.cols + MAIN_PIX - 1) / MAIN_PIX;
+  set_main_segments(&p);
   p.split = cfg->precision == SD_PRECISION_SPLIT;
   if (p.split) {  // FP64 re-sample queue of every k_cand item
     const uint64_t items = stage_items(WK_SEL, p);

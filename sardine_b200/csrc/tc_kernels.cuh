@@ -212,7 +212,9 @@ struct TcDev {
   int *flags;
   unsigned long long *counters;
   unsigned long long *trange;  // [0] = min, [1] = max (biased by 2^63), or null
-  uint64_t bpr;                // k_main work items per row
+  uint64_t bpr;                // k_main row segments per row
+  int seg_px;                  // pixels per k_main row segment (a segment is seg_px + 1 threads: the
+  int seg_per_item;            // first is the left neighbour), and segments per k_main item
   int fast;                    // tolerance allows the fixed-point-pair scheme
   int split;                   // SD_PRECISION_SPLIT
   uint64_t row0;               // grid row of the job's first row (row bands)
@@ -1253,7 +1255,27 @@ struct Slot {  // shared-memory record exchanged with the right-hand neighbour
 #define SD_MAIN_MINB 2  // blocks per SM the register budget is cut for (128 regs)
 #endif
 constexpr int MAIN_THREADS = SD_MAIN_THREADS;
-constexpr int MAIN_PIX = MAIN_THREADS - 1;  // thread 0 is the left halo pixel
+constexpr int MAIN_PIX = MAIN_THREADS - 1;  // widest segment: thread 0 is the left halo pixel
+
+// k_main's segment length for a row of `cols` pixels: 255, 127 or 63 pixels
+// (one item holds 1, 2 or 4 segments), the one that leaves the fewest
+// threads idle; a shorter segment must gain more than 2 % of utilisation
+// (each segment spends a thread on its left neighbour).
+inline void set_main_segments(TcDev *p) {
+  int best = MAIN_PIX;
+  double best_u = 0.0;
+  for (int seg = MAIN_PIX; seg >= (MAIN_THREADS / 4) - 1; seg = (seg + 1) / 2 - 1) {
+    const uint64_t spr = (p->cols + seg - 1) / seg;
+    const double u = spr ? (double)p->cols / (double)(spr * (uint64_t)(seg + 1)) : 0.0;
+    if (u > best_u + 0.02) best = seg, best_u = u;
+  }
+  p->seg_px = best;
+  p->seg_per_item = MAIN_THREADS / (best + 1);
+  p->bpr = (p->cols + best - 1) / best;
+}
+inline uint64_t main_items(const TcDev &p) {
+  return (p.rows * p.bpr + p.seg_per_item - 1) / p.seg_per_item;
+}
 static_assert(MAIN_THREADS <= 256, "RsEnt::meta holds the k_main thread in 8 bits");
 
 // ── K3: per-pixel solve, candidate outcomes and candidate outputs ───────────
@@ -1461,17 +1483,22 @@ __device__ __forceinline__ int ent_lane(const OrbitDev &o, const OrbTaylor &T, i
   return ent_at(o, t, e, exact);
 }
 
-// One k_main work item: MAIN_PIX pixels of row r starting at chunk * MAIN_PIX
-// (plus the left neighbour on thread 0).  Every thread of the block calls it.
-// It records F and the codes only: the outputs of the one member the row
-// walk selects are computed after the walk (k_cand), so this kernel holds no
-// resampling or facet state.
-__device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t chunk, Slot *slot,
-                                          OrbTaylor *tw) {
+// One k_main work item: seg_per_item consecutive row segments of seg_px
+// pixels (the first thread of each segment holds the segment's left
+// neighbour).  Narrow rows use shorter segments, so a 256-pixel row is not
+// one full item and one nearly empty one.  Every thread of the block calls
+// it.  It records F and the codes only: the outputs of the one member the
+// row walk selects are computed after the walk (k_cand), so this kernel
+// holds no resampling or facet state.
+__device__ __forceinline__ void main_item(const TcDev &p, uint64_t item, Slot *slot, OrbTaylor *tw) {
   const int tid = threadIdx.x;
   const int fast = p.fast;
-  const int64_t c = (int64_t)chunk * MAIN_PIX + tid - 1;
-  const bool in_row = c >= 0 && c < (int64_t)p.cols;
+  const int segw = p.seg_px + 1, pos = tid % segw;
+  const uint64_t sg = item * (uint64_t)p.seg_per_item + (uint64_t)(tid / segw);  // the thread's segment
+  const bool seg_ok = sg < p.rows * p.bpr;
+  const uint64_t r = seg_ok ? sg / p.bpr : p.rows;  // r == rows: no pixel
+  const int64_t c = (int64_t)(seg_ok ? sg % p.bpr : 0) * p.seg_px + pos - 1;
+  const bool in_row = seg_ok && c >= 0 && c < (int64_t)p.cols;
   const uint64_t i = r * p.cols + (uint64_t)(c < 0 ? 0 : c);
   PixGeo g;
   bool geo_ok = false;
@@ -1571,7 +1598,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
   my.fmask = fmask;
   my.exact = exm;
   __syncthreads();
-  if (tid == 0 || !in_row || r >= p.rows) return;
+  if (pos == 0 || !in_row || r >= p.rows) return;
 
   uint32_t cc = 0xFFFFu;
   if (!geo_ok) {
@@ -1631,7 +1658,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t r, uint64_t c
 __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main(TcDev p) {
   __shared__ Slot slot[MAIN_THREADS];
   __shared__ OrbTaylor tw[MAIN_THREADS / 32];
-  main_item(p, blockIdx.x / p.bpr, blockIdx.x % p.bpr, slot, tw);
+  main_item(p, blockIdx.x, slot, tw);
 }
 
 // Tile batches: persistent CTAs over the work table; the current job's
@@ -1658,7 +1685,7 @@ __global__ void __launch_bounds__(MAIN_THREADS, SD_MAIN_MINB) k_main_batch(const
       cur = jb;
     }
     const uint64_t li = item - pre[jb];
-    main_item(p, li / p.bpr, li % p.bpr, slot, tw);
+    main_item(p, li, slot, tw);
   }
 }
 
@@ -2222,7 +2249,7 @@ uint64_t stage_items(int stage, const TcDev &p) {
     case WK_ANCH: return p.utm ? p.rows * (uint64_t)p.n_pts : 0;
     case WK_ROWS: return p.rows;
     case WK_KNOT: return p.rows * KNOTS;
-    case WK_MAIN: return p.rows * p.bpr;
+    case WK_MAIN: return main_items(p);
     case WK_SCAN: return p.rows;
     case WK_REDO: return (p.rows * p.cols + REDO_CHUNK - 1) / REDO_CHUNK;
     default: return (p.rows * p.cols + SEL_THREADS - 1) / SEL_THREADS;

@@ -368,7 +368,7 @@ int tile_plan(sd_ctx *ctx, const sd_tile &t, uint64_t i, TilePlan *pl) {
   p.nesz = p.nesz_mask ? s.nesz : nullptr;
   p.nesz_factor = p.nesz_mask ? std::pow(10.0f, cfg.noise_floor_margin_db / 10.0f) : 0.0f;
   p.fast = (p.tol <= 1e-6) ? 1 : 0;
-  p.bpr = (cols + MAIN_PIX - 1) / MAIN_PIX;
+  set_main_segments(&p);
   pl->crop = pl->halo > 0 || t.speckle >= 0;
   pl->user[0] = t.out_data;
   pl->user[1] = p.compute_lia ? t.out_cos_lia : nullptr;
