@@ -1002,7 +1002,7 @@ def run_c5(args):
             if plane is not None:
                 assert not plane.is_cuda
                 d2h[0] += plane.numel() * plane.element_size()
-    e2e_server = GeocodingServer(local, hbm_budget=budget // 2, slots=2, max_batch=64, graphs=True,
+    e2e_server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=64, graphs=True,
                                  on_done=on_host, host_results=True)
     for s in e2e_server.slots:
         autotune.apply(s.ctx, tune)
