@@ -314,8 +314,8 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
     int64_t t1 = std::min(scene->state_vectors[nsv - 1].time_us, tmax + 100000);
     // a table larger than the grid costs more to build than it saves
     if (t1 >= t0 && (uint64_t)(t1 - t0 + 1) <= npx) {
-      SD_TRY(build_orbit_table(ctx, "tc.orbit_table", (const sd_state_vector *)d_svs, nsv, t0, t1, tmin, tmax,
-                               &p.orb));
+      SD_TRY(build_orbit_table(ctx, "tc.orbit_table", "tc.orbit_taylor", (const sd_state_vector *)d_svs, nsv, t0,
+                               t1, tmin, tmax, &p.orb));
       // the job record on the device carries the table
       SD_CUDA(ctx, cudaMemcpyAsync((void *)wk.d_jobs, &p, sizeof(TcDev), cudaMemcpyHostToDevice, st));
     }

@@ -60,6 +60,8 @@ constexpr int KNOTS = 17;
 constexpr int kCounters = 10;  // valid, dem, outside, nonconv, degen, flat, noise, spare, dB converted, dB masked
 constexpr int kCntDb = 8;      // counters[kCntDb + cls] for db_value's class cls (0 converted, 1 noise-masked)
 
+struct OrbTaylor;
+
 struct OrbitDev {
   const sd_state_vector *svs;
   uint64_t n;
@@ -67,6 +69,8 @@ struct OrbitDev {
   int64_t tab_t0;
   int64_t tab_n;
   const OrbPoly *poly;  // n - 7 window polynomials for times outside the table
+  const OrbTaylor *tay;  // expansions about tab_t0 + k * TAY_STEP, k < tay_n (k_orbit_taylor)
+  int64_t tay_n;
 };
 
 // State at integer microsecond t: the table (the reference's Lagrange sums,
@@ -1464,6 +1468,56 @@ __device__ __forceinline__ void orb_taylor_build(const OrbitDev &o, int64_t uw, 
   T->v3[d] = v[3];
 }
 
+// Expansions about every TAY_STEP-th microsecond of the orbit table's span,
+// built once per table: a warp copies the one nearest its shared time
+// (|uw - centre| <= 2 ms, so its lanes' times stay well inside the 20 ms
+// bound) instead of searching the state vectors and shifting the window
+// polynomial on the way to its first Newton step.
+constexpr int64_t TAY_STEP = 4000;
+constexpr int TAY_WORDS = (int)(sizeof(OrbTaylor) / 8);
+static_assert(sizeof(OrbTaylor) % 8 == 0 && TAY_WORDS <= 32, "one 8-byte word of OrbTaylor per lane");
+
+inline int64_t tay_count(int64_t tab_n) { return tab_n > 0 ? (tab_n - 1) / TAY_STEP + 1 : 0; }
+
+// Thread 3k + d fills coordinate d of expansion k (o.tab must be built).
+__global__ void k_orbit_taylor(OrbitDev o, int64_t n, OrbTaylor *out) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * n) return;
+  const int64_t k = i / 3;
+  const int64_t u = o.tab_t0 + k * TAY_STEP;
+  Ent e;
+  const bool ok = ent_at(o, u, &e) == ORB_OK;
+  orb_taylor_build(o, u, e, ok, (int)(i % 3), out + k);
+}
+
+// Every lane of the warp calls it with the warp's shared time uw.
+__device__ __forceinline__ void orb_taylor_fetch(const OrbitDev &o, int64_t uw, const Ent &ew, bool ew_ok,
+                                                 int lane, OrbTaylor *T) {
+  const int64_t q = uw - o.tab_t0 + TAY_STEP / 2;
+  if (o.tay && q >= 0 && q / TAY_STEP < o.tay_n) {
+    if (lane < TAY_WORDS)
+      reinterpret_cast<uint64_t *>(T)[lane] = __ldg(reinterpret_cast<const uint64_t *>(o.tay + q / TAY_STEP) + lane);
+  } else {
+    orb_taylor_build(o, uw, ew, ew_ok, lane, T);
+  }
+}
+
+// Expansions over orb's table into d_out (tay_count(orb->tab_n) entries);
+// sets orb->tay.
+inline int launch_orbit_taylor(sd_ctx *ctx, OrbitDev *orb, OrbTaylor *d_out) {
+  const int64_t n = tay_count(orb->tab_n);
+  orb->tay = nullptr;
+  orb->tay_n = 0;
+  if (n == 0) return SD_OK;
+  OrbitDev o = *orb;
+  SD_TIMED_BEGIN(ctx, "k_orbit_taylor");
+  k_orbit_taylor<<<grid_for((size_t)(3 * n), 128), 128, 0, ctx->stream>>>(o, n, d_out);
+  SD_LAUNCHED(ctx);
+  orb->tay = d_out;
+  orb->tay_n = n;
+  return SD_OK;
+}
+
 // State at t from the warp's expansion (*exact = false), or from the table.
 __device__ __forceinline__ int ent_lane(const OrbitDev &o, const OrbTaylor &T, int64_t t, Ent *e, bool *exact) {
   const int64_t dt = t - T.uw;
@@ -1527,7 +1581,7 @@ __device__ __forceinline__ void main_item(const TcDev &p, uint64_t item, Slot *s
   bool ew_exact = false;
   const bool ew_ok = fast && ent_at(p.orb, uw, &ew, &ew_exact) == ORB_OK;
   OrbTaylor &T = tw[tid >> 5];
-  orb_taylor_build(p.orb, uw, ew, ew_ok, tid & 31, &T);
+  orb_taylor_fetch(p.orb, uw, ew, ew_ok, tid & 31, &T);
   __syncwarp();
   if (px_in) {
     geo_ok = isfinite(g.P.x);
@@ -2382,9 +2436,10 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
 }
 
 // FP64 Lagrange state at every microsecond of [t0, t1] into scratch `name`
-// (capped at 96 M entries, 7.7 GB, centred on [tmin, tmax]).
-int build_orbit_table(sd_ctx *ctx, const char *name, const sd_state_vector *d_svs, uint64_t nsv, int64_t t0,
-                      int64_t t1, int64_t tmin, int64_t tmax, OrbitDev *orb) {
+// (capped at 96 M entries, 7.7 GB, centred on [tmin, tmax]), and the orbit
+// expansions over it into scratch `tay_name`.
+int build_orbit_table(sd_ctx *ctx, const char *name, const char *tay_name, const sd_state_vector *d_svs,
+                      uint64_t nsv, int64_t t0, int64_t t1, int64_t tmin, int64_t tmax, OrbitDev *orb) {
   const int64_t max_entries = 96ll * 1000 * 1000;
   if (t1 - t0 + 1 > max_entries) {
     const int64_t mid = (tmin / 2 + tmax / 2);
@@ -2400,7 +2455,9 @@ int build_orbit_table(sd_ctx *ctx, const char *name, const sd_state_vector *d_sv
   orb->tab = d_tab;
   orb->tab_t0 = t0;
   orb->tab_n = t1 - t0 + 1;
-  return SD_OK;
+  OrbTaylor *d_tay;
+  SD_TRY(scratch_t(ctx, tay_name, (size_t)tay_count(orb->tab_n), &d_tay));
+  return launch_orbit_taylor(ctx, orb, d_tay);
 }
 
 // Window polynomials of the orbit (orbit_poly_build) in scratch `name`.

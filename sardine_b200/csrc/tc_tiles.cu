@@ -273,6 +273,16 @@ extern "C" int sd_scene_create(sd_ctx *ctx, const sd_radar_image *image, const s
       s->orb.tab = (const double2 *)tab;
       s->orb.tab_t0 = t0;
       s->orb.tab_n = (int64_t)n;
+      const size_t tay_bytes = (size_t)tay_count(s->orb.tab_n) * sizeof(OrbTaylor);
+      void *tay = nullptr;
+      e = cudaMalloc(&tay, tay_bytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(ctx, SD_ERR_OUT_OF_MEMORY, "scene orbit expansions: cudaMalloc failed");
+      }
+      s->owned.push_back(tay);
+      s->bytes += tay_bytes;
+      SD_TRY(launch_orbit_taylor(ctx, &s->orb, (OrbTaylor *)tay));
     }
   }
   SD_TRY(sync(ctx));
