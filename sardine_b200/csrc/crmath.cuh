@@ -1,7 +1,9 @@
 // crmath.cuh — elementary functions written once for host and device, built
 // from IEEE double additions, multiplications, divisions and square roots
 // only, so the host compiler (gcc, no contraction) and the device compiler
-// (nvcc --fmad=false) produce the same bits from the same inputs.
+// (nvcc --fmad=false) produce the same bits from the same inputs.  The one
+// exception is sincos' fast path, which fuses its tail terms on the device:
+// its results are correctly rounded on both sides, hence equal.
 //
 // * sincos: correctly rounded (round to nearest) sine and cosine for
 //   |x| <= 1e5.  Method (Ziv's two-step strategy, as used by correctly
@@ -163,10 +165,28 @@ CRM_HD void sincos_fast(double ah, double al, DD *s, DD *c) {
   const double Sh = sincos_tab(4 * j), Sl = sincos_tab(4 * j + 1);
   const double Ch = sincos_tab(4 * j + 2), Cl = sincos_tab(4 * j + 3);
   const double d2 = dh * dh;
+  double p, pe, m, me;
+#if defined(__CUDA_ARCH__)
+  // The same terms in the same order with fused multiply-adds: one rounding
+  // per term instead of two, so the error bound holds a fortiori and a
+  // result that passes the rounding test is the correctly rounded value,
+  // equal to the host's.  (The FP64 pipe bounds the terrain kernels, and
+  // this halves the multiply-add count of the tails.)
+  const double pc = d2 * fma(d2, fma(-d2, 1.0 / 720.0, 1.0 / 24.0), -0.5);
+  const double ps = d2 * fma(d2, fma(-d2, 1.0 / 5040.0, 1.0 / 120.0), -1.0 / 6.0);
+  const double dps = dh * ps, ddl = dh * dl;
+  two_prod(Ch, dh, p, pe);
+  two_sum(Sh, p, m, me);
+  double t = fma(-Sh, ddl, fma(Ch, dps, fma(Sh, pc, fma(Ch, dl, fma(Cl, dh, me + pe + Sl)))));
+  fast_two_sum(m, t, s->h, s->l);
+  two_prod(Sh, dh, p, pe);
+  two_sum(Ch, -p, m, me);
+  t = fma(-Ch, ddl, fma(-Sh, dps, fma(Ch, pc, fma(-Sh, dl, fma(-Sl, dh, me - pe + Cl)))));
+  fast_two_sum(m, t, c->h, c->l);
+#else
   const double pc = d2 * (-0.5 + d2 * ((1.0 / 24.0) - d2 * (1.0 / 720.0)));
   const double ps = d2 * ((-1.0 / 6.0) + d2 * ((1.0 / 120.0) - d2 * (1.0 / 5040.0)));
   const double dps = dh * ps, ddl = dh * dl;
-  double p, pe, m, me;
   // sine
   two_prod(Ch, dh, p, pe);
   two_sum(Sh, p, m, me);
@@ -177,6 +197,7 @@ CRM_HD void sincos_fast(double ah, double al, DD *s, DD *c) {
   two_sum(Ch, -p, m, me);
   t = me - pe + Cl - Sl * dh - Sh * dl + Ch * pc - Sh * dps - Ch * ddl;
   fast_two_sum(m, t, c->h, c->l);
+#endif
 }
 
 // sin and cos of r = (rh, rl), |r| <= pi/4 + 2^-9, by their Taylor series in

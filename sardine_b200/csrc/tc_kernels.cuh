@@ -1337,12 +1337,22 @@ __device__ __noinline__ void heights_exact(const TcDev &p, uint64_t i) {
 // and the instruction cache.  Such pixels are queued instead and k_heights_fix
 // runs them 32 to a warp.
 __global__ void __launch_bounds__(SEL_THREADS, SD_HEIGHTS_MINB) k_heights(const TcWork *__restrict__ wp) {
+  // the current job's record in shared memory (restaged when the block's
+  // item stride crosses into the next job)
+  __shared__ __align__(16) unsigned char s_job[sizeof(TcDev)];
   const TcWork w = *wp;
   const uint64_t *pre = stage_pre(w, WK_SEL);
   const uint64_t total = pre[w.n_jobs];
+  const TcDev &p = *reinterpret_cast<const TcDev *>(s_job);
+  int cur = -1;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    const int jb = find_job(pre, w.n_jobs, item);
-    const TcDev &p = w.jobs[jb];
+    const int jb = find_job(pre, w.n_jobs, item);  // uniform over the block
+    if (jb != cur) {
+      __syncthreads();  // every thread is done with the previous record
+      load_job(s_job, w.jobs + jb, threadIdx.x, SEL_THREADS);
+      __syncthreads();
+      cur = jb;
+    }
     if (p.rs_cnt && threadIdx.x == 0) p.rs_cnt[item - pre[jb]] = 0;  // k_cand's queue of this item
     const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
     bool defer = false;
