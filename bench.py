@@ -1790,6 +1790,41 @@ def run_reference(args):
     }), flush=True)
 
 
+def run_tile_batch(args):
+    """A profiling aid, not a bench number: the config-5 scenes and 64 seeded
+    requests of the served arm geocoded as one `tc_tiles` batch (after a
+    warm-up batch of 8), twice per group: all tiles, the narrow ones
+    (<= 512 columns) and the wide ones (>= 1024).  Prints the per-kernel
+    device time of the second pass of each group, in ms and ps per output
+    pixel, as one JSON line."""
+    import numpy as np
+    import torch
+    import sardine_b200 as sd
+    from sardine_b200 import tiles
+    torch.cuda.set_device(0)
+    ctx = sd.Context(0)
+    scenes = _c5_setup(sd, ctx, "cuda:0", 0, args.tile_batch)
+    reqs = _c5_requests(sd, scenes, np.random.default_rng(5), 64, sd.Precision.SPLIT)
+    groups = {"all": reqs, "narrow<=512": [r for r in reqs if r.cols <= 512],
+              "wide>=1024": [r for r in reqs if r.cols >= 1024]}
+    tiles.tc_tiles(reqs[:8], ctx)
+    out = {"tile_batch": {"scenes": args.tile_batch, "requests": len(reqs)}}
+    for name, g in groups.items():
+        if not g:
+            continue
+        for _ in range(2):
+            ctx.set_timing(True)
+            tiles.tc_tiles(g, ctx)
+            kt = ctx.kernel_times()
+            ctx.set_timing(False)
+        px = sum(r.rows * r.cols for r in g)
+        out[name] = {"tiles": len(g), "px": px,
+                     "ps_per_px": {k: round(v[0] * 1e9 / px, 1)
+                                   for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])},
+                     "ms": {k: round(v[0], 3) for k, v in kt.items()}}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1807,10 +1842,15 @@ def main():
     ap.add_argument("--ref-rows", type=int, default=16)
     ap.add_argument("--small", action="store_true",
                     help="reduced IW shape (profiler captures); not a bench number")
+    ap.add_argument("--tile-batch", dest="tile_batch", type=int, default=0, metavar="N_SCENES",
+                    help="time one config-5 tile batch over N_SCENES scenes per kernel (profiler captures); "
+                         "not a bench number")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.tile_batch:
+        run_tile_batch(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.config == "c4":
         run_c4(args)

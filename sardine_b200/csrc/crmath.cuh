@@ -229,8 +229,10 @@ CRM_HD void sincos(double x, double *so, double *co) {
     *co = ::cos(x);
     return;
   }
-  double rh, rl;
-  int q = reduce_pio2(x, false, rh, rl);
+  double rh = x, rl = 0.0;
+  // |x| < 0.78 < pi/4: k = 0, and every step of the reduction is exact, so it
+  // would return (x, 0) itself.
+  int q = fabs(x) < 0.78 ? 0 : reduce_pio2(x, false, rh, rl);
   const bool neg = rh < 0.0;
   DD s, c;
   sincos_fast(neg ? -rh : rh, neg ? -rl : rl, &s, &c);
