@@ -679,7 +679,7 @@ def _speckle_adds(sd, filt):
 # DRAM bytes per output pixel of the TC stage and of the speckle/crop stage on
 # the config-5 tile batch, from one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum of every stage kernel, profiles/tc_c5_traffic.md)
-C5_TC_TRAFFIC_B_PER_PX = 359.4
+C5_TC_TRAFFIC_B_PER_PX = 380.7
 C5_SP_TRAFFIC_B_PER_PX = 10.2
 
 
@@ -708,7 +708,7 @@ def _tile_roofline(sd, tiles, ctx, reqs):
             "achieved": tf, "peak": fp64, "unit": "TFLOP/s", "frac": tf / fp64 if (tf and fp64) else None,
             "traffic": C5_TC_TRAFFIC_B_PER_PX * px,
             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of every TC-stage kernel on this "
-                               "batch's tile sizes, 359.4 B/px x the batch's px (profiles/tc_c5_traffic.md)"),
+                               "batch's tile sizes, %.1f B/px x the batch's px (profiles/tc_c5_traffic.md)" % C5_TC_TRAFFIC_B_PER_PX),
             "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
             "batch": f"{len(reqs)} tiles, {px} px",
             "speckle_stage": {"kernel": "k_speckle_tiles", "bound": "fp64_add", "achieved": add_rate,
