@@ -308,8 +308,16 @@ def split_accuracy(sd, sc, ctx, stream):
     from sardine_b200.accuracy import compare_geocoded
     rep = compare_geocoded(split, ref, split.azimuth_time_us, ref.azimuth_time_us,
                            sc.scene.sub_swaths[0].azimuth_time_interval_s)
+    # the whole FP64 call (host work and the azimuth-time copy included)
     rep["fp64_tc_ms"] = e0.elapsed_time(e1)
     rep["fp64_tc_px_per_s"] = ref.total_pixel_count / (rep["fp64_tc_ms"] / 1e3)
+    # like for like with roofline.stage_ms: the FP64 call's TC-stage kernels
+    ctx.set_timing(True)
+    sd.terrain_correction(m, sc.scene, sc.dem, sc.grids, cfg64, ctx=ctx)
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    rep["fp64_tc_stage_ms"] = sum(v[0] for k, v in kt.items() if k.startswith(TC_STAGE + ("k_orbit",)))
+    rep["fp64_kernels_ms"] = {k: round(v[0], 3) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
     rep["counters_equal"] = (split.newton_iter_histogram == ref.newton_iter_histogram and
                              split.valid_pixel_count == ref.valid_pixel_count and
                              split.flat_masked_count == ref.flat_masked_count)

@@ -2034,13 +2034,16 @@ __device__ __forceinline__ bool target_facet(const TcDev &p, uint64_t i, V3 *P, 
 template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork *__restrict__ wp) {
   __shared__ unsigned int s_cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
+  __shared__ __align__(16) unsigned char s_job[sizeof(TcDev)];
   const TcWork w = *wp;
   const uint64_t *pre = stage_pre(w, WK_SEL);
   const uint64_t total = pre[w.n_jobs];
   const int tid = threadIdx.x;
   // counters accumulate in shared memory over the block's items of one job
-  // and go to the job's counters when the job changes or the block ends
+  // and go to the job's counters when the job changes or the block ends;
+  // the job's record is staged in shared memory at the same change
   for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
+  const TcDev &p = *reinterpret_cast<const TcDev *>(s_job);
   int cur = -1;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
     const int jb = find_job(pre, w.n_jobs, item);
@@ -2052,10 +2055,10 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
             atomicAdd(&w.jobs[cur].counters[k], (unsigned long long)s_cnt[k]);
             s_cnt[k] = 0;
           }
+      load_job(s_job, w.jobs + jb, tid, blockDim.x);
       __syncthreads();
       cur = jb;
     }
-    const TcDev &p = w.jobs[jb];
     const uint64_t npx = p.rows * p.cols;
     const uint64_t li = item - pre[jb];
     const uint64_t i = li * SEL_THREADS + tid;
