@@ -317,6 +317,8 @@ def split_accuracy(sd, sc, ctx, stream):
     kt = ctx.kernel_times()
     ctx.set_timing(False)
     rep["fp64_tc_stage_ms"] = sum(v[0] for k, v in kt.items() if k.startswith(TC_STAGE + ("k_orbit",)))
+    # split candidates whose FP32 resampling sum failed its error bound (re-sampled in FP64)
+    rep["split_fp64_resampled_px"] = int(split.diag_fp64_resampled)
     rep["fp64_kernels_ms"] = {k: round(v[0], 3) for k, v in sorted(kt.items(), key=lambda kv: -kv[1][0])}
     rep["counters_equal"] = (split.newton_iter_histogram == ref.newton_iter_histogram and
                              split.valid_pixel_count == ref.valid_pixel_count and

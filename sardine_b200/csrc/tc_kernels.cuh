@@ -16,6 +16,9 @@
 //                  Newton iteration is one table read instead of an 8-point
 //                  Lagrange evaluation with 56 divisions; outside the table
 //                  the window polynomials (geo.cuh: OrbPoly) stand in.
+//  k_orbit_taylor  the orbit's Taylor expansion about every 4th ms of the
+//                  table's span, from which k_main's warps take their
+//                  approximate states between table reads.
 //  k_row_*         per-row set-up: UTM anchors (output_crs.rs:364-417),
 //                  latitude seed, LUT guess, flat-cell area, and a coarse
 //                  azimuth-time model (17 knots per row).
