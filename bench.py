@@ -867,7 +867,8 @@ def _c5_config(args, world):
                          "over 2 slots, HBM-budget admission; value at the last rate ('max': "
                          "every request queued at once = saturated throughput)"),
             "rates_req_s": args.rates.split(","), "burst_per_step": args.burst,
-            "hbm_budget_gb": args.budget_gb, "parallelism": f"replicas x{world}"}
+            "hbm_budget_gb": args.budget_gb, "max_batch": args.max_batch,
+            "parallelism": f"replicas x{world}"}
 
 
 
@@ -958,7 +959,7 @@ def run_c5(args):
     rng = np.random.default_rng(5 + rank)
     rates = [math.inf if r.strip() == "max" else float(r) for r in args.rates.split(",")]
     budget = args.budget_gb << 30
-    server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=64, graphs=True)
+    server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=args.max_batch, graphs=True)
     sample = _c5_requests(sd, scenes, rng, 64, sd.Precision.SPLIT)
     tune = None
     for s in server.slots:
@@ -1012,7 +1013,7 @@ def run_c5(args):
             if plane is not None:
                 assert not plane.is_cuda
                 d2h[0] += plane.numel() * plane.element_size()
-    e2e_server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=64, graphs=True,
+    e2e_server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=args.max_batch, graphs=True,
                                  on_done=on_host, host_results=True)
     for s in e2e_server.slots:
         autotune.apply(s.ctx, tune)
@@ -1847,6 +1848,7 @@ def main():
     ap.add_argument("--burst", type=int, default=512, help="config5 requests per step")
     ap.add_argument("--scenes", type=int, default=8, help="config5 resident scenes")
     ap.add_argument("--budget-gb", dest="budget_gb", type=int, default=16, help="config5 HBM budget")
+    ap.add_argument("--max-batch", dest="max_batch", type=int, default=64, help="config5 requests per batch at most")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--ref-rows", type=int, default=16)

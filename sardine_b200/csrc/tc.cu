@@ -299,7 +299,7 @@ static int tc_run(sd_ctx *ctx, const sd_radar_image *image, const sd_scene *scen
   TcWorkHost wk;
   TcWork *d_work = nullptr;
   SD_TRY(work_upload(ctx, "tc.work", &p, 1, &wk, &d_work));
-  SD_TRY(launch_rows(ctx, d_work, wk.totals));
+  SD_TRY(launch_rows(ctx, d_work, wk.totals, &p));  // k_heights in its parameter form
   unsigned long long tr[2];
   SD_CUDA(ctx, cudaMemcpyAsync(tr, d_trange, sizeof tr, cudaMemcpyDeviceToHost, st));
   SD_TRY(sync(ctx));

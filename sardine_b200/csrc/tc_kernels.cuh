@@ -43,6 +43,7 @@
 //                  defers what FP32 cannot settle to k_resample and k_redo.
 #pragma once
 #include <algorithm>
+#include <cstdlib>
 #include <limits>
 #include <memory>
 
@@ -1339,50 +1340,64 @@ __device__ __noinline__ void heights_exact(const TcDev &p, uint64_t i) {
 // taken inline by ~1 pixel in 200 it stalls the other 31 lanes of the warp
 // and the instruction cache.  Such pixels are queued instead and k_heights_fix
 // runs them 32 to a warp.
+// One k_heights item: SEL_THREADS pixels of job jb from local item li.
+// Every thread of the block calls it (the deferral ballot needs all lanes);
+// wp's deferral queue is read only when a lane defers.
+__device__ __forceinline__ void heights_item(const TcDev &p, int jb, uint64_t li, const TcWork *__restrict__ wp) {
+  if (p.rs_cnt && threadIdx.x == 0) p.rs_cnt[li] = 0;  // k_cand's queue of this item
+  const uint64_t i = li * SEL_THREADS + threadIdx.x;
+  bool defer = false;
+  if (i < p.rows * p.cols) {
+    const uint64_t r = i / p.cols, c = i % p.cols;
+    PixGeo g;
+    float hf, h[4];
+    const int st = pixel_height_try(p, r, c, &g, &hf);
+    const int fs = st > 0 && p.fct ? facet_heights_try(p, g, h) : 0;
+    if (st >= 0 && fs >= 0) heights_store(p, i, g, st > 0, hf, fs > 0, h);
+    else defer = true;
+  }
+  // queue the deferred lanes, one atomic per warp
+  const unsigned m = __ballot_sync(0xffffffffu, defer);
+  if (m) {
+    const int lane = threadIdx.x & 31;
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(wp->hq_cnt, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (defer) {
+      const unsigned slot = base + __popc(m & ((1u << lane) - 1u));
+      if (slot < wp->hq_cap) wp->hq[slot] = ((unsigned long long)jb << 40) | i;
+      ((double *)p.tp)[i] = -INFINITY;  // the mark k_heights_fix scans for when the queue overflowed
+    }
+  }
+}
+
+// Persistent form over the work table: the current job's record in shared
+// memory (restaged when the block's item stride crosses into the next job).
 __global__ void __launch_bounds__(SEL_THREADS, SD_HEIGHTS_MINB) k_heights(const TcWork *__restrict__ wp) {
-  // the current job's record in shared memory (restaged when the block's
-  // item stride crosses into the next job)
   __shared__ __align__(16) unsigned char s_job[sizeof(TcDev)];
-  const TcWork w = *wp;
-  const uint64_t *pre = stage_pre(w, WK_SEL);
-  const uint64_t total = pre[w.n_jobs];
+  const uint64_t *pre = stage_pre(*wp, WK_SEL);
+  const int n_jobs = wp->n_jobs;
+  const uint64_t total = pre[n_jobs];
   const TcDev &p = *reinterpret_cast<const TcDev *>(s_job);
   int cur = -1;
   for (uint64_t item = blockIdx.x; item < total; item += gridDim.x) {
-    const int jb = find_job(pre, w.n_jobs, item);  // uniform over the block
+    const int jb = find_job(pre, n_jobs, item);  // uniform over the block
     if (jb != cur) {
       __syncthreads();  // every thread is done with the previous record
-      load_job(s_job, w.jobs + jb, threadIdx.x, SEL_THREADS);
+      load_job(s_job, wp->jobs + jb, threadIdx.x, SEL_THREADS);
       __syncthreads();
       cur = jb;
     }
-    if (p.rs_cnt && threadIdx.x == 0) p.rs_cnt[item - pre[jb]] = 0;  // k_cand's queue of this item
-    const uint64_t i = (item - pre[jb]) * SEL_THREADS + threadIdx.x;
-    bool defer = false;
-    if (i < p.rows * p.cols) {
-      const uint64_t r = i / p.cols, c = i % p.cols;
-      PixGeo g;
-      float hf, h[4];
-      const int st = pixel_height_try(p, r, c, &g, &hf);
-      const int fs = st > 0 && p.fct ? facet_heights_try(p, g, h) : 0;
-      if (st >= 0 && fs >= 0) heights_store(p, i, g, st > 0, hf, fs > 0, h);
-      else defer = true;
-    }
-    // queue the deferred lanes, one atomic per warp (the item loop is
-    // uniform over the block, so every lane arrives here)
-    const unsigned m = __ballot_sync(0xffffffffu, defer);
-    if (m) {
-      const int lane = threadIdx.x & 31;
-      unsigned base = 0;
-      if (lane == 0) base = atomicAdd(w.hq_cnt, (unsigned)__popc(m));
-      base = __shfl_sync(0xffffffffu, base, 0);
-      if (defer) {
-        const unsigned slot = base + __popc(m & ((1u << lane) - 1u));
-        if (slot < w.hq_cap) w.hq[slot] = ((unsigned long long)jb << 40) | i;
-        ((double *)p.tp)[i] = -INFINITY;  // the mark k_heights_fix scans for when the queue overflowed
-      }
-    }
+    heights_item(p, jb, item - pre[jb], wp);
   }
+}
+
+// Parameter form: one job (work-table index jb), one block per item.  The
+// record sits in the kernel's parameter bank, so its fields are instruction
+// operands rather than loads into registers.
+__global__ void __launch_bounds__(SEL_THREADS, SD_HEIGHTS_MINB) k_heights_param(TcDev p, int jb,
+                                                                              const TcWork *__restrict__ wp) {
+  heights_item(p, jb, blockIdx.x, wp);
 }
 
 // The deferred pixels of k_heights, with the checked lookups: the queue, or
@@ -2381,7 +2396,41 @@ int work_upload(sd_ctx *ctx, const char *name, const TcDev *jobs, int n, TcWorkH
 // work blocks of `items` items, `per` per block (~0 = a full resident grid)
 uint64_t blocks_for(uint64_t items, unsigned per) { return items == ~0ull ? ~0ull : grid_for(items, per); }
 
-int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
+// SARDINE_B200_HEIGHTS_PARAM=0 keeps k_heights in its persistent
+// work-table form where the parameter form would run.
+inline bool heights_param_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("SARDINE_B200_HEIGHTS_PARAM");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// k_heights in its parameter form for job `job` (work-table index jb) on st.
+inline int launch_heights_param(sd_ctx *ctx, const TcDev &job, int jb, const TcWork *d_work, cudaStream_t st) {
+  const uint64_t items = stage_items(WK_SEL, job);
+  if (items == 0) return SD_OK;
+  k_heights_param<<<(unsigned)items, SEL_THREADS, 0, st>>>(job, jb, d_work);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(ctx, SD_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  ctx->launches++;
+  return SD_OK;
+}
+
+// The pixels k_heights deferred (their count is known on the device only).
+int launch_heights_fix(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
+  SD_TIMED_BEGIN(ctx, "k_heights_fix");
+  k_heights_fix<<<persistent_grid(k_heights_fix, 128, 0, blocks_for(totals[WK_SEL] == ~0ull ? ~0ull : totals[WK_SEL] * 4, 128)), 128, 0, ctx->stream>>>(
+      d_work);
+  SD_LAUNCHED(ctx);
+  return SD_OK;
+}
+
+// Row stages, then k_heights and k_heights_fix unless `heights` is false
+// (the caller launches them itself).  single: the one job's record, for the
+// parameter form of k_heights.
+int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const TcDev *single = nullptr,
+                bool heights = true) {
   cudaStream_t st = ctx->stream;
   if (totals[WK_ANCH]) {
     SD_TIMED_BEGIN(ctx, "k_row_anchors");
@@ -2394,15 +2443,16 @@ int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals) {
   SD_TIMED_BEGIN(ctx, "k_row_model");
   k_row_model<<<persistent_grid(k_row_model, 128, 0, blocks_for(totals[WK_KNOT], 128)), 128, 0, st>>>(d_work);
   SD_LAUNCHED(ctx);
+  if (!heights) return SD_OK;
   SD_TIMED_BEGIN(ctx, "k_heights");
-  k_heights<<<persistent_grid(k_heights, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
-  SD_LAUNCHED(ctx);
-  // the deferred pixels (their count is known on the device only)
-  SD_TIMED_BEGIN(ctx, "k_heights_fix");
-  k_heights_fix<<<persistent_grid(k_heights_fix, 128, 0, blocks_for(totals[WK_SEL] == ~0ull ? ~0ull : totals[WK_SEL] * 4, 128)), 128, 0, st>>>(
-      d_work);
-  SD_LAUNCHED(ctx);
-  return SD_OK;
+  if (single && heights_param_enabled()) {
+    SD_TRY(launch_heights_param(ctx, *single, 0, d_work, st));
+    ::sd::timing_end(ctx);
+  } else {
+    k_heights<<<persistent_grid(k_heights, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
+    SD_LAUNCHED(ctx);
+  }
+  return launch_heights_fix(ctx, d_work, totals);
 }
 
 // job: the single job's record (parameter form of k_main), or null for the

@@ -24,18 +24,18 @@ int launch_pixels_batch(sd_ctx *ctx, const TcWork *d_work, const uint64_t *total
                : launch_pixels_t<KDYN, false>(ctx, d_work, totals, nullptr, with_main);
 }
 
-// k_main per tile in its parameter form (job record in the kernel's
-// parameter space rather than in shared memory), the tiles spread largest
-// first over four side streams forked from and joined back to the
-// context's stream so that small tiles overlap.
-int fork_main_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs) {
+// One launch per tile over four side streams (largest tiles first, each to
+// the least loaded stream), joined back into the context's stream; timed as
+// `name`.  launch(i, stream) launches tile i's kernel.
+template <class F>
+int fork_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, const char *name, F launch) {
   for (int k = 0; k < 4; ++k) {
     if (!ctx->side[k]) SD_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
     if (!ctx->ev_join[k]) SD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_join[k], cudaEventDisableTiming));
   }
   if (!ctx->ev_fork) SD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
   const int ns = (int)std::min<size_t>(4, jobs.size());
-  SD_TIMED_BEGIN(ctx, "k_main (per tile)");
+  SD_TIMED_BEGIN(ctx, name);
   SD_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
   for (int k = 0; k < ns; ++k) SD_CUDA(ctx, cudaStreamWaitEvent(ctx->side[k], ctx->ev_fork, 0));
   std::vector<size_t> order(jobs.size());
@@ -47,7 +47,7 @@ int fork_main_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs) {
     int k = 0;
     for (int q = 1; q < ns; ++q)
       if (load[q] < load[k]) k = q;
-    SD_TRY(launch_main_param(ctx, &jobs[i], ctx->side[k]));
+    SD_TRY(launch(i, ctx->side[k]));
     load[k] += jobs[i].rows * jobs[i].cols;
   }
   for (int k = 0; k < ns; ++k) {
@@ -56,6 +56,22 @@ int fork_main_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs) {
   }
   ::sd::timing_end(ctx);
   return SD_OK;
+}
+
+// k_main per tile in its parameter form (job record in the kernel's
+// parameter space rather than in shared memory); small tiles overlap on
+// the side streams.
+int fork_main_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs) {
+  return fork_per_tile(ctx, jobs, "k_main (per tile)",
+                       [&](size_t i, cudaStream_t s) { return launch_main_param(ctx, &jobs[i], s); });
+}
+
+// k_heights in its parameter form, one launch per tile (d_work: the batch's
+// work table, whose deferral queue the tiles share).
+int fork_heights_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, const TcWork *d_work) {
+  return fork_per_tile(ctx, jobs, "k_heights (per tile)", [&](size_t i, cudaStream_t s) {
+    return launch_heights_param(ctx, jobs[i], (int)i, d_work, s);
+  });
 }
 
 }  // namespace
@@ -547,8 +563,13 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     }
     SD_TRY(work_upload(ctx, wname, grp[g].data(), (int)grp[g].size(), &wk, &d_work));
     const bool split = g == 1;
-    if (ctx->main_cps < 0) {  // per-tile parameter launches of k_main
-      SD_TRY(launch_rows(ctx, d_work, wk.totals));
+    if (ctx->main_cps < 0) {  // per-tile parameter launches of k_heights and k_main
+      const bool hp = heights_param_enabled();
+      SD_TRY(launch_rows(ctx, d_work, wk.totals, nullptr, !hp));
+      if (hp) {
+        SD_TRY(fork_heights_per_tile(ctx, grp[g], d_work));
+        SD_TRY(launch_heights_fix(ctx, d_work, wk.totals));
+      }
       SD_TRY(fork_main_per_tile(ctx, grp[g]));
       SD_TRY(launch_pixels_batch(ctx, d_work, wk.totals, split, false));
     } else if (use_graph) {
