@@ -2049,6 +2049,103 @@ __device__ __forceinline__ bool target_facet(const TcDev &p, uint64_t i, V3 *P, 
   return true;
 }
 
+// One k_cand item: the outputs of SEL_THREADS pixels of job p from local
+// item li; counts go to the block's s_cnt.
+template <int KERNEL, bool SPLIT>
+__device__ __forceinline__ void cand_item(const TcDev &p, uint64_t li, unsigned int *s_cnt) {
+  const int tid = threadIdx.x;
+  const uint64_t npx = p.rows * p.cols;
+  const uint64_t i = li * SEL_THREADS + tid;
+  // the pixel's walk outcome, base time and geometry in one round trip
+  uint8_t sel = (uint8_t)SEL_ORBIT;
+  int64_t fbv = 0;
+  PixPlanes pl;
+  if (i < npx) {
+    sel = p.sel[i];
+    fbv = p.fb[i];
+    pl = load_planes(p, i);
+  }
+  const int code = sel & 7, it = sel >> 4;
+  const bool has_t = code == SEL_M0 || code == SEL_M1 || code == SEL_DONE;
+  const int64_t t = has_t ? fbv + (code == SEL_M1 ? 1 : 0) : 0;
+  int counter = -1;
+  if (has_t) {
+    atomicAdd(&s_cnt[kCounters + it], 1u);
+    const uint64_t r = i / p.cols;
+    V3 P;
+    Facet fc;
+    const bool ok = target_facet_of(p, pl, &P, &fc);
+    V3 S;
+    const bool orb_ok = ok && orbit_pos_exact(p.orb, t, &S);
+    if (!orb_ok) atomicOr(&p.flags[ok ? 0 : 5], 1);  // cannot happen for a converged time
+    CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
+    bool deferred = false;
+    if (orb_ok) {
+      const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
+      if constexpr (SPLIT) {
+        const CandPre cp = cand_pre<KERNEL, true>(p, P, S, t);
+        // the FP64 facet rounded to FP32: within 2^-24 |n| per component,
+        // inside the bound cand_post_f allows (kLpErr en, en = area)
+        FacetF f{};
+        if (fc.ok) {
+          f.ok = true;
+          f.nx = (float)fc.normal.x, f.ny = (float)fc.normal.y, f.nz = (float)fc.normal.z;
+          f.area = (float)fc.area;
+          f.en = f.area;
+        }
+        int redo;
+        float wd = 1.f;
+        o = cand_post_f(p, cp, P, S, f, (float)flat_area, &redo, &wd);
+        if (redo == RD_SAMPLE) {  // queue the FP64 re-sample in this item's slots
+          const uint32_t q = atomicAdd(p.rs_cnt + li, 1u);
+          if (q < (uint32_t)RS_CAP) {
+            p.rs_ent[li * RS_CAP + q] = RsEnt{cp.line, cp.sample, wd, (uint32_t)tid};
+            if (p.compute_lia) p.cos_lia[i] = o.cos;
+            deferred = true;
+          } else {
+            redo = RD_FULL;
+          }
+        }
+        if (redo == RD_FULL) {
+          p.cc[i] |= CF_REDO;
+          atomicAdd(&p.flags[3], 1);
+          deferred = true;
+        }
+      } else {
+        const CandPre cp = cand_pre<KERNEL, false>(p, P, S, t);
+        o = cand_post(p, cp, P, S, fc, flat_area);
+      }
+    }
+    if (!deferred) {
+      float v = o.data;
+      if (p.db) {
+        int dc;
+        v = db_value(v, p.db_floor, &dc);
+        if (dc >= 0) atomicAdd(&s_cnt[kCntDb + dc], 1u);
+      }
+      p.out[i] = v;
+      if (p.compute_lia) {
+        p.cos_lia[i] = o.cos;
+        p.mask[i] = o.mask;
+      }
+      counter = o.cls;
+    }
+    if (p.az_time) p.az_time[i] = t;
+  } else if (i < npx && code != SEL_ORBIT) {
+    const uint8_t m = code == SEL_NONCONV ? SD_MASK_NON_CONVERGED
+                      : code == SEL_DEGEN ? SD_MASK_DEGENERATE_GEOMETRY
+                                          : SD_MASK_DEM_MISSING;
+    counter = code == SEL_NONCONV ? 3 : (code == SEL_DEGEN ? 4 : 1);
+    if (p.az_time) p.az_time[i] = INT64_MIN;
+    p.out[i] = NAN;
+    if (p.compute_lia) {
+      p.cos_lia[i] = NAN;
+      p.mask[i] = m;
+    }
+  }
+  if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
+}
+
 template <int KERNEL, bool SPLIT>
 __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork *__restrict__ wp) {
   __shared__ unsigned int s_cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
@@ -2077,102 +2174,27 @@ __global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand(const TcWork
       __syncthreads();
       cur = jb;
     }
-    const uint64_t npx = p.rows * p.cols;
-    const uint64_t li = item - pre[jb];
-    const uint64_t i = li * SEL_THREADS + tid;
-    // the pixel's walk outcome, base time and geometry in one round trip
-    uint8_t sel = (uint8_t)SEL_ORBIT;
-    int64_t fbv = 0;
-    PixPlanes pl;
-    if (i < npx) {
-      sel = p.sel[i];
-      fbv = p.fb[i];
-      pl = load_planes(p, i);
-    }
-    const int code = sel & 7, it = sel >> 4;
-    const bool has_t = code == SEL_M0 || code == SEL_M1 || code == SEL_DONE;
-    const int64_t t = has_t ? fbv + (code == SEL_M1 ? 1 : 0) : 0;
-    int counter = -1;
-    if (has_t) {
-      atomicAdd(&s_cnt[kCounters + it], 1u);
-      const uint64_t r = i / p.cols;
-      V3 P;
-      Facet fc;
-      const bool ok = target_facet_of(p, pl, &P, &fc);
-      V3 S;
-      const bool orb_ok = ok && orbit_pos_exact(p.orb, t, &S);
-      if (!orb_ok) atomicOr(&p.flags[ok ? 0 : 5], 1);  // cannot happen for a converged time
-      CandOut o{NAN, NAN, SD_MASK_OUTSIDE_FOOTPRINT, 2};
-      bool deferred = false;
-      if (orb_ok) {
-        const double flat_area = p.need_geom ? p.row_flat[r] : 0.0;
-        if constexpr (SPLIT) {
-          const CandPre cp = cand_pre<KERNEL, true>(p, P, S, t);
-          // the FP64 facet rounded to FP32: within 2^-24 |n| per component,
-          // inside the bound cand_post_f allows (kLpErr en, en = area)
-          FacetF f{};
-          if (fc.ok) {
-            f.ok = true;
-            f.nx = (float)fc.normal.x, f.ny = (float)fc.normal.y, f.nz = (float)fc.normal.z;
-            f.area = (float)fc.area;
-            f.en = f.area;
-          }
-          int redo;
-          float wd = 1.f;
-          o = cand_post_f(p, cp, P, S, f, (float)flat_area, &redo, &wd);
-          if (redo == RD_SAMPLE) {  // queue the FP64 re-sample in this item's slots
-            const uint32_t q = atomicAdd(p.rs_cnt + li, 1u);
-            if (q < (uint32_t)RS_CAP) {
-              p.rs_ent[li * RS_CAP + q] = RsEnt{cp.line, cp.sample, wd, (uint32_t)tid};
-              if (p.compute_lia) p.cos_lia[i] = o.cos;
-              deferred = true;
-            } else {
-              redo = RD_FULL;
-            }
-          }
-          if (redo == RD_FULL) {
-            p.cc[i] |= CF_REDO;
-            atomicAdd(&p.flags[3], 1);
-            deferred = true;
-          }
-        } else {
-          const CandPre cp = cand_pre<KERNEL, false>(p, P, S, t);
-          o = cand_post(p, cp, P, S, fc, flat_area);
-        }
-      }
-      if (!deferred) {
-        float v = o.data;
-        if (p.db) {
-          int dc;
-          v = db_value(v, p.db_floor, &dc);
-          if (dc >= 0) atomicAdd(&s_cnt[kCntDb + dc], 1u);
-        }
-        p.out[i] = v;
-        if (p.compute_lia) {
-          p.cos_lia[i] = o.cos;
-          p.mask[i] = o.mask;
-        }
-        counter = o.cls;
-      }
-      if (p.az_time) p.az_time[i] = t;
-    } else if (i < npx && code != SEL_ORBIT) {
-      const uint8_t m = code == SEL_NONCONV ? SD_MASK_NON_CONVERGED
-                        : code == SEL_DEGEN ? SD_MASK_DEGENERATE_GEOMETRY
-                                            : SD_MASK_DEM_MISSING;
-      counter = code == SEL_NONCONV ? 3 : (code == SEL_DEGEN ? 4 : 1);
-      if (p.az_time) p.az_time[i] = INT64_MIN;
-      p.out[i] = NAN;
-      if (p.compute_lia) {
-        p.cos_lia[i] = NAN;
-        p.mask[i] = m;
-      }
-    }
-    if (counter >= 0) atomicAdd(&s_cnt[counter], 1u);
+    cand_item<KERNEL, SPLIT>(p, item - pre[jb], s_cnt);
   }
   __syncthreads();
   if (cur >= 0)
     for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
       if (s_cnt[k]) atomicAdd(&w.jobs[cur].counters[k], (unsigned long long)s_cnt[k]);
+}
+
+// Parameter form for one job (the record in the parameter bank), persistent
+// over the job's items.
+template <int KERNEL, bool SPLIT>
+__global__ void __launch_bounds__(SEL_THREADS, SD_CAND_MINB) k_cand_param(TcDev p) {
+  __shared__ unsigned int s_cnt[kCounters + SD_NEWTON_ITER_HIST_SIZE];
+  const int tid = threadIdx.x;
+  for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x) s_cnt[k] = 0;
+  __syncthreads();
+  const uint64_t items = (p.rows * p.cols + SEL_THREADS - 1) / SEL_THREADS;
+  for (uint64_t li = blockIdx.x; li < items; li += gridDim.x) cand_item<KERNEL, SPLIT>(p, li, s_cnt);
+  __syncthreads();
+  for (int k = tid; k < kCounters + SD_NEWTON_ITER_HIST_SIZE; k += blockDim.x)
+    if (s_cnt[k]) atomicAdd(&p.counters[k], (unsigned long long)s_cnt[k]);
 }
 
 // ── k_resample (split precision): FP64 values of the queued candidates ────────
@@ -2455,15 +2477,53 @@ int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const
   return launch_heights_fix(ctx, d_work, totals);
 }
 
+// Stages of launch_pixels_t.
+enum : unsigned { PX_MAIN = 1, PX_SCAN = 2, PX_CAND = 4, PX_POST = 8, PX_ALL = 15 };
+
+// SARDINE_B200_CAND_PARAM=0 keeps k_cand in its persistent work-table form
+// where the parameter form would run.
+inline bool cand_param_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("SARDINE_B200_CAND_PARAM");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// k_cand in its parameter form for one job on st, specialised on the job's
+// own resampling kernel.
+template <bool S>
+int launch_cand_param(sd_ctx *ctx, const TcDev &job, cudaStream_t st) {
+  const uint64_t items = stage_items(WK_SEL, job);
+  if (items == 0) return SD_OK;
+  switch (job.resampling) {
+    case SD_RESAMPLE_BICUBIC:
+      k_cand_param<SD_RESAMPLE_BICUBIC, S>
+          <<<persistent_grid(k_cand_param<SD_RESAMPLE_BICUBIC, S>, SEL_THREADS, 0, items), SEL_THREADS, 0, st>>>(job);
+      break;
+    case SD_RESAMPLE_LANCZOS3:
+      k_cand_param<SD_RESAMPLE_LANCZOS3, S>
+          <<<persistent_grid(k_cand_param<SD_RESAMPLE_LANCZOS3, S>, SEL_THREADS, 0, items), SEL_THREADS, 0, st>>>(job);
+      break;
+    default:
+      k_cand_param<SD_RESAMPLE_BILINEAR, S>
+          <<<persistent_grid(k_cand_param<SD_RESAMPLE_BILINEAR, S>, SEL_THREADS, 0, items), SEL_THREADS, 0, st>>>(job);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(ctx, SD_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  ctx->launches++;
+  return SD_OK;
+}
+
 // job: the single job's record (parameter form of k_main), or null for the
 // persistent work-table form.  Stages: k_main (F and codes), k_scan (the row
 // walk), k_cand (outputs of the selected members), and in split precision
 // k_resample and k_redo (the candidates FP32 could not settle).
 template <int K, bool S>
 int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const TcDev *job,
-                    bool with_main = true) {
+                    unsigned stages = PX_ALL) {
   cudaStream_t st = ctx->stream;
-  if (with_main) {
+  if (stages & PX_MAIN) {
     if (job) {
       if (totals[WK_MAIN] > 0x7FFFFFFFull)
         return set_error(ctx, SD_ERR_INVALID_ARGUMENT, "output grid too large");
@@ -2482,14 +2542,23 @@ int launch_pixels_t(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, c
     }
     SD_LAUNCHED(ctx);
   }
-  SD_TIMED_BEGIN(ctx, "k_scan");
-  k_scan<<<persistent_grid(k_scan, SCAN_WARPS * 32, 0, blocks_for(totals[WK_SCAN], SCAN_WARPS)),
-           SCAN_WARPS * 32, 0, st>>>(d_work);
-  SD_LAUNCHED(ctx);
-  SD_TIMED_BEGIN(ctx, S ? "k_cand<SPLIT>" : "k_cand");
-  k_cand<K, S><<<persistent_grid(k_cand<K, S>, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
-  SD_LAUNCHED(ctx);
-  if (S) {
+  if (stages & PX_SCAN) {
+    SD_TIMED_BEGIN(ctx, "k_scan");
+    k_scan<<<persistent_grid(k_scan, SCAN_WARPS * 32, 0, blocks_for(totals[WK_SCAN], SCAN_WARPS)),
+             SCAN_WARPS * 32, 0, st>>>(d_work);
+    SD_LAUNCHED(ctx);
+  }
+  if (stages & PX_CAND) {
+    SD_TIMED_BEGIN(ctx, S ? "k_cand<SPLIT>" : "k_cand");
+    if (job && K != KDYN && cand_param_enabled())
+      k_cand_param<K == KDYN ? 0 : K, S>
+          <<<persistent_grid(k_cand_param<K == KDYN ? 0 : K, S>, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(
+              *job);
+    else
+      k_cand<K, S><<<persistent_grid(k_cand<K, S>, SEL_THREADS, 0, totals[WK_SEL]), SEL_THREADS, 0, st>>>(d_work);
+    SD_LAUNCHED(ctx);
+  }
+  if (S && (stages & PX_POST)) {
     SD_TIMED_BEGIN(ctx, "k_resample");
     k_resample<K><<<persistent_grid(k_resample<K>, SEL_THREADS, 0, blocks_for(totals[WK_SEL], SEL_THREADS / 32)),
                     SEL_THREADS, 0, st>>>(d_work);

@@ -17,11 +17,11 @@ namespace sd {
 namespace {
 
 // Tile batches: the persistent work-table kernels; the resampler is read
-// per job.  with_main false: the stages after k_main only (k_main ran per tile).
+// per job.  stages: the PX_* stages to launch (the others run per tile).
 int launch_pixels_batch(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, bool split,
-                        bool with_main = true) {
-  return split ? launch_pixels_t<KDYN, true>(ctx, d_work, totals, nullptr, with_main)
-               : launch_pixels_t<KDYN, false>(ctx, d_work, totals, nullptr, with_main);
+                        unsigned stages = PX_ALL) {
+  return split ? launch_pixels_t<KDYN, true>(ctx, d_work, totals, nullptr, stages)
+               : launch_pixels_t<KDYN, false>(ctx, d_work, totals, nullptr, stages);
 }
 
 // One launch per tile over four side streams (largest tiles first, each to
@@ -64,6 +64,16 @@ int fork_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, const char *name,
 int fork_main_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs) {
   return fork_per_tile(ctx, jobs, "k_main (per tile)",
                        [&](size_t i, cudaStream_t s) { return launch_main_param(ctx, &jobs[i], s); });
+}
+
+// k_cand in its parameter form, one launch per tile, each specialised on
+// the tile's resampling kernel.
+int fork_cand_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, bool split) {
+  return fork_per_tile(ctx, jobs, split ? "k_cand<SPLIT> (per tile)" : "k_cand (per tile)",
+                       [&](size_t i, cudaStream_t s) {
+                         return split ? launch_cand_param<true>(ctx, jobs[i], s)
+                                      : launch_cand_param<false>(ctx, jobs[i], s);
+                       });
 }
 
 // k_heights in its parameter form, one launch per tile (d_work: the batch's
@@ -571,7 +581,13 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
         SD_TRY(launch_heights_fix(ctx, d_work, wk.totals));
       }
       SD_TRY(fork_main_per_tile(ctx, grp[g]));
-      SD_TRY(launch_pixels_batch(ctx, d_work, wk.totals, split, false));
+      if (cand_param_enabled()) {
+        SD_TRY(launch_pixels_batch(ctx, d_work, wk.totals, split, PX_SCAN));
+        SD_TRY(fork_cand_per_tile(ctx, grp[g], split));
+        SD_TRY(launch_pixels_batch(ctx, d_work, wk.totals, split, PX_POST));
+      } else {
+        SD_TRY(launch_pixels_batch(ctx, d_work, wk.totals, split, PX_ALL & ~PX_MAIN));
+      }
     } else if (use_graph) {
       static const uint64_t kFull[kWk] = {~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull, ~0ull};
       SD_TRY(run_graph(ctx, g + 2 * ctx->main_cps, d_work, [&]() -> int {
