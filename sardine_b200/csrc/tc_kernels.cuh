@@ -386,21 +386,33 @@ __global__ void k_orbit_table(const sd_state_vector *svs, uint64_t n, int64_t t0
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;              \
        i += (uint64_t)gridDim.x * blockDim.x)
 
+// Anchor li of job p: the exact inverse projection of its grid point and,
+// for a UTM DEM, the forward projection's local expansion there.
+__device__ __forceinline__ void anchor_item(const TcDev &p, uint64_t li) {
+  const uint64_t r = li / p.n_pts, a = li % p.n_pts;
+  double lon, lat;
+  utm_xy_to_lonlat(p.proj, p.ax[a], row_y(p, r), &lon, &lat);
+  ((double *)p.alon)[li] = lon;
+  ((double *)p.alat)[li] = lat;
+  if (p.aloc) {
+    const Utm &u = p.dem.utm;
+    utm_local(u, lat, utm_taup(u, lat), utm_lam(u, lon), (UtmLocal *)p.aloc + li);
+  }
+}
+
 __global__ void k_row_anchors(const TcWork *__restrict__ wp) {
   SD_FOR_ITEMS(WK_ANCH) {
     const int j = find_job(pre, w.n_jobs, i);
-    const TcDev &p = w.jobs[j];
-    const uint64_t li = i - pre[j];
-    const uint64_t r = li / p.n_pts, a = li % p.n_pts;
-    double lon, lat;
-    utm_xy_to_lonlat(p.proj, p.ax[a], row_y(p, r), &lon, &lat);
-    ((double *)p.alon)[li] = lon;
-    ((double *)p.alat)[li] = lat;
-    if (p.aloc) {
-      const Utm &u = p.dem.utm;
-      utm_local(u, lat, utm_taup(u, lat), utm_lam(u, lon), (UtmLocal *)p.aloc + li);
-    }
+    anchor_item(w.jobs[j], i - pre[j]);
   }
+}
+
+// Parameter form for one job: the projections' series coefficients sit in
+// the parameter bank and enter the FP64 instructions as operands.
+__global__ void k_row_anchors_param(TcDev p) {
+  const uint64_t n = p.utm ? p.rows * (uint64_t)p.n_pts : 0;
+  for (uint64_t li = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; li < n; li += (uint64_t)gridDim.x * blockDim.x)
+    anchor_item(p, li);
 }
 
 __global__ void k_row_setup(const TcWork *__restrict__ wp) {
@@ -2428,6 +2440,27 @@ inline bool heights_param_enabled() {
   return on;
 }
 
+// SARDINE_B200_ANCHORS_PARAM=0 keeps k_row_anchors in its persistent
+// work-table form where the parameter form would run.
+inline bool anchors_param_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("SARDINE_B200_ANCHORS_PARAM");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// k_row_anchors in its parameter form for one job on st.
+inline int launch_anchors_param(sd_ctx *ctx, const TcDev &job, cudaStream_t st) {
+  const uint64_t items = stage_items(WK_ANCH, job);
+  if (items == 0) return SD_OK;
+  k_row_anchors_param<<<persistent_grid(k_row_anchors_param, 128, 0, blocks_for(items, 128)), 128, 0, st>>>(job);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(ctx, SD_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  ctx->launches++;
+  return SD_OK;
+}
+
 // k_heights in its parameter form for job `job` (work-table index jb) on st.
 inline int launch_heights_param(sd_ctx *ctx, const TcDev &job, int jb, const TcWork *d_work, cudaStream_t st) {
   const uint64_t items = stage_items(WK_SEL, job);
@@ -2452,11 +2485,15 @@ int launch_heights_fix(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals
 // (the caller launches them itself).  single: the one job's record, for the
 // parameter form of k_heights.
 int launch_rows(sd_ctx *ctx, const TcWork *d_work, const uint64_t *totals, const TcDev *single = nullptr,
-                bool heights = true) {
+                bool heights = true, bool anchors = true) {
   cudaStream_t st = ctx->stream;
-  if (totals[WK_ANCH]) {
+  if (anchors && totals[WK_ANCH]) {
     SD_TIMED_BEGIN(ctx, "k_row_anchors");
-    k_row_anchors<<<persistent_grid(k_row_anchors, 128, 0, blocks_for(totals[WK_ANCH], 128)), 128, 0, st>>>(d_work);
+    if (single && anchors_param_enabled())
+      k_row_anchors_param<<<persistent_grid(k_row_anchors_param, 128, 0, blocks_for(totals[WK_ANCH], 128)), 128, 0,
+                            st>>>(*single);
+    else
+      k_row_anchors<<<persistent_grid(k_row_anchors, 128, 0, blocks_for(totals[WK_ANCH], 128)), 128, 0, st>>>(d_work);
     SD_LAUNCHED(ctx);
   }
   SD_TIMED_BEGIN(ctx, "k_row_setup");

@@ -76,6 +76,12 @@ int fork_cand_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, bool split) 
                        });
 }
 
+// k_row_anchors in its parameter form, one launch per tile.
+int fork_anchors_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs) {
+  return fork_per_tile(ctx, jobs, "k_row_anchors (per tile)",
+                       [&](size_t i, cudaStream_t s) { return launch_anchors_param(ctx, jobs[i], s); });
+}
+
 // k_heights in its parameter form, one launch per tile (d_work: the batch's
 // work table, whose deferral queue the tiles share).
 int fork_heights_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, const TcWork *d_work) {
@@ -574,8 +580,9 @@ extern "C" int sd_tc_tiles_launch(sd_ctx *ctx, const sd_tile *tiles, uint64_t n)
     SD_TRY(work_upload(ctx, wname, grp[g].data(), (int)grp[g].size(), &wk, &d_work));
     const bool split = g == 1;
     if (ctx->main_cps < 0) {  // per-tile parameter launches of k_heights and k_main
-      const bool hp = heights_param_enabled();
-      SD_TRY(launch_rows(ctx, d_work, wk.totals, nullptr, !hp));
+      const bool hp = heights_param_enabled(), ap = anchors_param_enabled() && wk.totals[WK_ANCH];
+      if (ap) SD_TRY(fork_anchors_per_tile(ctx, grp[g]));
+      SD_TRY(launch_rows(ctx, d_work, wk.totals, nullptr, !hp, !ap));
       if (hp) {
         SD_TRY(fork_heights_per_tile(ctx, grp[g], d_work));
         SD_TRY(launch_heights_fix(ctx, d_work, wk.totals));
