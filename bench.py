@@ -687,9 +687,12 @@ def _speckle_adds(sd, filt):
 
 
 # DRAM bytes per output pixel of the TC stage and of the speckle/crop stage on
-# the config-5 tile batch, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum of every stage kernel, profiles/tc_c5_traffic.md)
-C5_TC_TRAFFIC_B_PER_PX = 380.7
+# the config-5 tile batch in the per-tile kernel forms the served arm runs,
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of every
+# stage launch, profiles/tc_c5_traffic.md).  Reads are complete; writes are a
+# lower bound (a small tile's output still in L2 when its launch ends is
+# written back outside any launch's count).
+C5_TC_TRAFFIC_B_PER_PX = 270.9
 C5_SP_TRAFFIC_B_PER_PX = 10.2
 
 
@@ -717,8 +720,9 @@ def _tile_roofline(sd, tiles, ctx, reqs):
     roof = {"bound": "fp64", "kernel": "tile geocoding (" + "+".join(sorted(k for k in kt if k.startswith(TC_STAGE))) + ")",
             "achieved": tf, "peak": fp64, "unit": "TFLOP/s", "frac": tf / fp64 if (tf and fp64) else None,
             "traffic": C5_TC_TRAFFIC_B_PER_PX * px,
-            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of every TC-stage kernel on this "
-                               "batch's tile sizes, %.1f B/px x the batch's px (profiles/tc_c5_traffic.md)" % C5_TC_TRAFFIC_B_PER_PX),
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of every TC-stage launch (per-tile "
+                               "forms) on this batch's tile sizes, %.1f B/px x the batch's px "
+                               "(profiles/tc_c5_traffic.md); writes a lower bound" % C5_TC_TRAFFIC_B_PER_PX),
             "flops_per_px": TC_FLOPS(n_it), "newton_iters_mean": n_it, "stage_ms": tc_ms,
             "batch": f"{len(reqs)} tiles, {px} px",
             "speckle_stage": {"kernel": "k_speckle_tiles", "bound": "fp64_add", "achieved": add_rate,
@@ -1804,7 +1808,7 @@ def run_reference(args):
 def run_tile_batch(args):
     """A profiling aid, not a bench number: the config-5 scenes and 64 seeded
     requests of the served arm geocoded as one `tc_tiles` batch (after a
-    warm-up batch of 8), twice per group: all tiles, the narrow ones
+    warm-up batch of 8) in the kernel form `--tile-form` names, twice per group: all tiles, the narrow ones
     (<= 512 columns) and the wide ones (>= 1024).  Prints the per-kernel
     device time of the second pass of each group, in ms and ps per output
     pixel, as one JSON line."""
@@ -1814,12 +1818,15 @@ def run_tile_batch(args):
     from sardine_b200 import tiles
     torch.cuda.set_device(0)
     ctx = sd.Context(0)
+    if args.tile_form == "tile":  # the per-tile parameter forms the served arm's autotuner picks
+        from sardine_b200 import autotune
+        autotune.apply(ctx, {"speckle": [32, 8], "main_cps": -1})
     scenes = _c5_setup(sd, ctx, "cuda:0", 0, args.tile_batch)
     reqs = _c5_requests(sd, scenes, np.random.default_rng(5), 64, sd.Precision.SPLIT)
     groups = {"all": reqs, "narrow<=512": [r for r in reqs if r.cols <= 512],
               "wide>=1024": [r for r in reqs if r.cols >= 1024]}
     tiles.tc_tiles(reqs[:8], ctx)
-    out = {"tile_batch": {"scenes": args.tile_batch, "requests": len(reqs)}}
+    out = {"tile_batch": {"scenes": args.tile_batch, "requests": len(reqs), "form": args.tile_form}}
     for name, g in groups.items():
         if not g:
             continue
@@ -1857,6 +1864,8 @@ def main():
     ap.add_argument("--tile-batch", dest="tile_batch", type=int, default=0, metavar="N_SCENES",
                     help="time one config-5 tile batch over N_SCENES scenes per kernel (profiler captures); "
                          "not a bench number")
+    ap.add_argument("--tile-form", dest="tile_form", default="batch", choices=["batch", "tile"],
+                    help="--tile-batch: persistent work-table kernels (batch) or the per-tile parameter forms (tile)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
