@@ -291,14 +291,26 @@ SD_HD void utm_local(const Utm &u, double lat_deg, double taup, LamSC L, UtmLoca
 }
 
 // Projected coordinates of a point displaced by (dphi, dlam) radians.
+// The device fuses its multiply-adds here and in utm_local_hermite: these
+// positions only feed certified DEM lookups, whose allowance (kDemPosEps,
+// 3e-8 m) is far above the rounding of either form (~1e-9 m).
 SD_HD void utm_local_step(const Utm &u, const UtmLocal &l, double dphi, double dlam, double *x, double *y) {
-  const double dw_re = l.dpsi1 * dphi + 0.5 * l.dpsi2 * dphi * dphi;
   const double dw_im = dlam;
+#if defined(__CUDA_ARCH__)
+  const double dw_re = fma(0.5 * l.dpsi2 * dphi, dphi, l.dpsi1 * dphi);
+  const double w2_re = fma(dw_re, dw_re, -dw_im * dw_im), w2_im = 2.0 * dw_re * dw_im;
+  const double dz_re = fma(l.zw_re, dw_re, fma(-l.zw_im, dw_im, 0.5 * fma(l.zww_re, w2_re, -l.zww_im * w2_im)));
+  const double dz_im = fma(l.zw_re, dw_im, fma(l.zw_im, dw_re, 0.5 * fma(l.zww_re, w2_im, l.zww_im * w2_re)));
+  *x = fma(u.k0A, dz_im, l.x);
+  *y = fma(u.k0A, dz_re, l.y);
+#else
+  const double dw_re = l.dpsi1 * dphi + 0.5 * l.dpsi2 * dphi * dphi;
   const double w2_re = dw_re * dw_re - dw_im * dw_im, w2_im = 2.0 * dw_re * dw_im;
   const double dz_re = l.zw_re * dw_re - l.zw_im * dw_im + 0.5 * (l.zww_re * w2_re - l.zww_im * w2_im);
   const double dz_im = l.zw_re * dw_im + l.zw_im * dw_re + 0.5 * (l.zww_re * w2_im + l.zww_im * w2_re);
   *x = l.x + u.k0A * dz_im;
   *y = l.y + u.k0A * dz_re;
+#endif
 }
 
 // Projected point (and local expansion) at position t of the segment between
@@ -314,15 +326,26 @@ SD_HD void utm_local_hermite(const UtmLocal &A, const UtmLocal &B, double dphi, 
   const double t2 = t * t, t3 = t2 * t;
   const double h00 = 2.0 * t3 - 3.0 * t2 + 1.0, h10 = t3 - 2.0 * t2 + t;
   const double h01 = -2.0 * t3 + 3.0 * t2, h11 = t3 - t2;
+  const double u = 1.0 - t;
+#if defined(__CUDA_ARCH__)
+  o->x = fma(h00, A.x, fma(h01, B.x, fma(h10, ax_, h11 * bx_)));
+  o->y = fma(h00, A.y, fma(h01, B.y, fma(h10, ay_, h11 * by_)));
+  o->zw_re = fma(u, A.zw_re, t * B.zw_re);
+  o->zw_im = fma(u, A.zw_im, t * B.zw_im);
+  o->zww_re = fma(u, A.zww_re, t * B.zww_re);
+  o->zww_im = fma(u, A.zww_im, t * B.zww_im);
+  o->dpsi1 = fma(u, A.dpsi1, t * B.dpsi1);
+  o->dpsi2 = fma(u, A.dpsi2, t * B.dpsi2);
+#else
   o->x = h00 * A.x + h10 * ax_ + h01 * B.x + h11 * bx_;
   o->y = h00 * A.y + h10 * ay_ + h01 * B.y + h11 * by_;
-  const double u = 1.0 - t;
   o->zw_re = u * A.zw_re + t * B.zw_re;
   o->zw_im = u * A.zw_im + t * B.zw_im;
   o->zww_re = u * A.zww_re + t * B.zww_re;
   o->zww_im = u * A.zww_im + t * B.zww_im;
   o->dpsi1 = u * A.dpsi1 + t * B.dpsi1;
   o->dpsi2 = u * A.dpsi2 + t * B.dpsi2;
+#endif
 }
 
 // sin/cos of a + b from sin/cos of a, for |b| < 1e-4 (series to b^4).
@@ -480,8 +503,15 @@ SD_HD int dem_sample_cert(const DemView &d, double row_f, double col_f, double e
     *h = NAN;
     return 1;
   }
+#if defined(__CUDA_ARCH__)
+  // fused on the device: within a few ulps of the corner magnitudes of the
+  // unfused sum, inside the 8e-15 allowance below
+  const double wr = 1.0 - dr, wc = 1.0 - dc;
+  const double v = fma((double)v11 * dr, dc, fma((double)v10 * dr, wc, fma((double)v01 * wr, dc, (double)v00 * wr * wc)));
+#else
   const double v = (double)v00 * (1.0 - dr) * (1.0 - dc) + (double)v01 * (1.0 - dr) * dc +
                    (double)v10 * dr * (1.0 - dc) + (double)v11 * dr * dc;
+#endif
   // the value's uncertainty: the corners' spread times the position's
   // uncertainty in both axes, plus the rounding of this sum and of the exact
   // position's (a few ulps of the corner magnitudes)
