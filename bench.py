@@ -868,10 +868,10 @@ def _c5_config(args, world):
     return {"workload": (f"config5: {args.scenes} config-2-shape scenes resident (merged sigma0+NESZ, "
                          "DEM, orbit table); Poisson tile requests, sides 256-2048 log-uniform, "
                          "random scene/bbox/resampler/speckle, split precision, continuous batching "
-                         "over 2 slots, HBM-budget admission; value at the last rate ('max': "
+                         f"over {args.slots} slots, HBM-budget admission; value at the last rate ('max': "
                          "every request queued at once = saturated throughput)"),
             "rates_req_s": args.rates.split(","), "burst_per_step": args.burst,
-            "hbm_budget_gb": args.budget_gb, "max_batch": args.max_batch,
+            "hbm_budget_gb": args.budget_gb, "max_batch": args.max_batch, "slots": args.slots,
             "parallelism": f"replicas x{world}"}
 
 
@@ -963,7 +963,7 @@ def run_c5(args):
     rng = np.random.default_rng(5 + rank)
     rates = [math.inf if r.strip() == "max" else float(r) for r in args.rates.split(",")]
     budget = args.budget_gb << 30
-    server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=args.max_batch, graphs=True)
+    server = GeocodingServer(local, hbm_budget=budget, slots=args.slots, max_batch=args.max_batch, graphs=True)
     sample = _c5_requests(sd, scenes, rng, 64, sd.Precision.SPLIT)
     tune = None
     for s in server.slots:
@@ -1017,7 +1017,7 @@ def run_c5(args):
             if plane is not None:
                 assert not plane.is_cuda
                 d2h[0] += plane.numel() * plane.element_size()
-    e2e_server = GeocodingServer(local, hbm_budget=budget, slots=2, max_batch=args.max_batch, graphs=True,
+    e2e_server = GeocodingServer(local, hbm_budget=budget, slots=args.slots, max_batch=args.max_batch, graphs=True,
                                  on_done=on_host, host_results=True)
     for s in e2e_server.slots:
         autotune.apply(s.ctx, tune)
@@ -1856,6 +1856,7 @@ def main():
     ap.add_argument("--scenes", type=int, default=8, help="config5 resident scenes")
     ap.add_argument("--budget-gb", dest="budget_gb", type=int, default=16, help="config5 HBM budget")
     ap.add_argument("--max-batch", dest="max_batch", type=int, default=64, help="config5 requests per batch at most")
+    ap.add_argument("--slots", type=int, default=2, help="config5 concurrent batches (server slots)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--ref-rows", type=int, default=16)
