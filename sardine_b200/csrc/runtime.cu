@@ -203,7 +203,7 @@ void sd_ctx_destroy(sd_ctx *ctx) {
   if (ctx->d_counters) cudaFree(ctx->d_counters);
   for (auto &kv : ctx->graph_exec) cudaGraphExecDestroy(kv.second.exec);
   if (ctx->tiles_done) cudaEventDestroy(ctx->tiles_done);
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < SD_SIDE_STREAMS; ++k) {
     if (ctx->side[k]) cudaStreamDestroy(ctx->side[k]);
     if (ctx->ev_join[k]) cudaEventDestroy(ctx->ev_join[k]);
   }

@@ -24,17 +24,17 @@ int launch_pixels_batch(sd_ctx *ctx, const TcWork *d_work, const uint64_t *total
                : launch_pixels_t<KDYN, false>(ctx, d_work, totals, nullptr, stages);
 }
 
-// One launch per tile over four side streams (largest tiles first, each to
+// One launch per tile over the side streams (largest tiles first, each to
 // the least loaded stream), joined back into the context's stream; timed as
 // `name`.  launch(i, stream) launches tile i's kernel.
 template <class F>
 int fork_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, const char *name, F launch) {
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < SD_SIDE_STREAMS; ++k) {
     if (!ctx->side[k]) SD_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
     if (!ctx->ev_join[k]) SD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_join[k], cudaEventDisableTiming));
   }
   if (!ctx->ev_fork) SD_CUDA(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
-  const int ns = (int)std::min<size_t>(4, jobs.size());
+  const int ns = (int)std::min<size_t>(SD_SIDE_STREAMS, jobs.size());
   SD_TIMED_BEGIN(ctx, name);
   SD_CUDA(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
   for (int k = 0; k < ns; ++k) SD_CUDA(ctx, cudaStreamWaitEvent(ctx->side[k], ctx->ev_fork, 0));
@@ -42,7 +42,7 @@ int fork_per_tile(sd_ctx *ctx, const std::vector<TcDev> &jobs, const char *name,
   for (size_t i = 0; i < order.size(); ++i) order[i] = i;
   std::sort(order.begin(), order.end(),
             [&](size_t a, size_t b) { return jobs[a].rows * jobs[a].cols > jobs[b].rows * jobs[b].cols; });
-  uint64_t load[4] = {0, 0, 0, 0};
+  uint64_t load[SD_SIDE_STREAMS] = {};
   for (size_t i : order) {
     int k = 0;
     for (int q = 1; q < ns; ++q)
