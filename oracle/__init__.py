@@ -551,6 +551,18 @@ def fit_poly6(pts, which: int):
 
 def compute_coreg_offsets(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us):
     """compute_coreg_offsets (insar/coreg.rs:128-223): (status, CoregResult or None)."""
+    rc, res, _ = _coreg_offsets(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us)
+    return rc, res
+
+
+def coreg_n_valid(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us):
+    """(status, number of converged grid points), the count also on the
+    grid-too-small error, which carries it (coreg.rs:207-208)."""
+    rc, _, nv = _coreg_offsets(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us)
+    return rc, nv
+
+
+def _coreg_offsets(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us):
     az, rg, rms, nv = (C.c_double * 6)(), (C.c_double * 6)(), C.c_double(), C.c_uint64()
     rc = lib().orc_coreg_offsets(ref_orbit.to_c(), len(ref_orbit.times_us), int(ref_first_us), int(ref_deburst.lines),
                                  int(ref_deburst.samples), int(ref_deburst.valid_sample_offset),
@@ -560,5 +572,5 @@ def compute_coreg_offsets(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_s
                                  float(sec_swath.slant_range_time_s), float(sec_swath.range_pixel_spacing_m),
                                  int(sec_swath.first_sample), az, rg, C.byref(rms), C.byref(nv))
     if rc:
-        return rc, None
-    return rc, T.CoregResult(T.CoregPoly(list(az), list(rg)), rms.value, int(nv.value))
+        return rc, None, int(nv.value)
+    return rc, T.CoregResult(T.CoregPoly(list(az), list(rg)), rms.value, int(nv.value)), int(nv.value)

@@ -704,6 +704,17 @@ def compute_coreg_offsets(ref_swath: SubSwathMetadata, ref_orbit: OrbitData, ref
     """compute_coreg_offsets (insar/coreg.rs:128-223): the 20 x 50 sparse grid
     geocoded on the device, the degree-2 offset fits on the host."""
     ctx = _ctx(ctx)
+    rc, r = _coreg_offsets_raw(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us,
+                               ctx)
+    _check(ctx, rc, InsarError)
+    return T.CoregResult(T.CoregPoly(list(r.az_poly), list(r.rg_poly)), r.fit_residual_rms, int(r.n_valid))
+
+
+def _coreg_offsets_raw(ref_swath, ref_orbit, ref_first_us, ref_deburst, sec_swath, sec_orbit, sec_first_us,
+                       ctx: Context):
+    """sd_coreg_offsets' status and result record; n_valid is set on the
+    grid-too-small error too (the reference's error carries it,
+    insar/coreg.rs:207-208)."""
     r = _abi.CoregResultC()
     rc = lib().sd_coreg_offsets(ctx.handle, ref_orbit.to_c(), len(ref_orbit.times_us), int(ref_first_us),
                                 int(ref_deburst.lines), int(ref_deburst.samples),
@@ -712,5 +723,4 @@ def compute_coreg_offsets(ref_swath: SubSwathMetadata, ref_orbit: OrbitData, ref
                                 sec_orbit.to_c(), len(sec_orbit.times_us), int(sec_first_us),
                                 float(sec_swath.azimuth_time_interval_s), float(sec_swath.slant_range_time_s),
                                 float(sec_swath.range_pixel_spacing_m), int(sec_swath.first_sample), C.byref(r))
-    _check(ctx, rc, InsarError)
-    return T.CoregResult(T.CoregPoly(list(r.az_poly), list(r.rg_poly)), r.fit_residual_rms, int(r.n_valid))
+    return rc, r

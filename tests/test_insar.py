@@ -318,6 +318,7 @@ def test_oracle_coreg_offsets_realistic_orbit_fails_like_the_reference():
     whole microsecond: the grid comes out too small."""
     rc, _ = oracle.compute_coreg_offsets(*_coreg_case(realistic=True))
     assert rc == _abi.SD_ERR_INSAR_COREG_GRID_TOO_SMALL
+    assert oracle.coreg_n_valid(*_coreg_case(realistic=True)) == (rc, 4)
 
 
 @pytest.mark.gpu
@@ -333,8 +334,17 @@ def test_gpu_coreg_offsets_match_oracle(ctx):
 
 @pytest.mark.gpu
 def test_gpu_coreg_grid_too_small(ctx):
-    for case in (_coreg_case(realistic=True), _coreg_case()[:2] + (T0_US + 500_000_000,) + _coreg_case()[3:]):
-        assert oracle.compute_coreg_offsets(*case)[0] == _abi.SD_ERR_INSAR_COREG_GRID_TOO_SMALL
+    """The error kind and the number of grid points that converged before it:
+    on the realistic orbit the microsecond stepping lets 4 of 1000 converge,
+    and the device must find the same 4."""
+    from sardine_b200 import _coreg_offsets_raw
+    for case, n in ((_coreg_case(realistic=True), 4),
+                    (_coreg_case()[:2] + (T0_US + 500_000_000,) + _coreg_case()[3:], 0)):
+        rc, n_oracle = oracle.coreg_n_valid(*case)
+        assert rc == _abi.SD_ERR_INSAR_COREG_GRID_TOO_SMALL and n_oracle == n
         with pytest.raises(sd.InsarError) as e:
             sd.compute_coreg_offsets(*case, ctx=ctx)
         assert e.value.kind == "CoregGridTooSmall"
+        rc, r = _coreg_offsets_raw(*case, ctx)
+        assert rc == _abi.SD_ERR_INSAR_COREG_GRID_TOO_SMALL
+        assert int(r.n_valid) == n_oracle
